@@ -1,0 +1,343 @@
+"""Benchmark of the B200 mutual-interaction engine (one JSON line on rank 0).
+
+Workload (one "step"): one gravity evaluation (vector_field, brute-force
+branch + central mass) of the 65,536-body disk: masses log-uniform over
+[1e-9, 1e-6], all radii 1e-5, softening_parameter 0.5 (epsilon = 1e-5), G = 1.
+``value`` is pair-interactions/s (N(N-1) ordered interactions per step) of the
+mixed-precision kernel with inputs resident in HBM; ``e2e`` is the same metric
+through ncgpu_vector_field with pinned host buffers (copies inside the timed
+region).  The all-FP64 kernels (exact reference order, and tiled) are timed on
+the same input for the mixed-vs-FP64 ratio, and the mixed kernel's error is
+measured against the exact FP64 result.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank evaluates its own copy of the workload (replicas,
+weak scaling); times are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_BODIES = 65536
+SOFTENING = 0.5
+FLOP_PER_INTERACTION = 20  # 3 sub, 3 FMA (r^2+eps^2), rsqrt (2), 3 mul, 3 FMA accumulate
+METRIC = "Pair-interactions/s mixed vs FP64 (rel err<1e-6); mesh collision steps/s at N=1M"
+WORKLOAD = ("gravity-only single-step accelerations, N=65,536 disk (a~U[0.8,1.2], e~Rayleigh 0.01, "
+            "i~Rayleigh 0.005), masses log-uniform [1e-9,1e-6], R=1e-5, softening 0.5*(R_k+R_p)")
+REF_SAMPLE = 16384  # bodies per reference-arm step (bounded CPU sample)
+
+
+def dist_info():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload():
+    from ncorpion_b200 import disks
+    b = disks.gravity_disk(N_BODIES, seed=0)
+    ex = np.ones(N_BODIES, np.int32)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    return b, ex, cm
+
+
+def params(mode, central=1):
+    from ncorpion_b200 import api
+    return api.default_params(G=1.0, softening_parameter=SOFTENING, central_mass_bool=central,
+                              collision_bool=0, brute_force_bool=1, gravity_mode=mode)
+
+
+def cpu_reference_rate(b, ex, cm, nsample):
+    """The reference's own vector_field (compiled from its sources into
+    oracle/_ref) on the first `nsample` bodies; falls back to the C port of
+    it when the reference build is absent.  Returns (rate, seconds, kind)."""
+    import oracle
+    sub, exs = b[:nsample], ex[:nsample]
+    if oracle.ref_available("bf_grav_s05"):
+        ref = oracle.Ref("bf_grav_s05")
+        ref.set_state(sub, exs, cm)
+        t0 = time.perf_counter()
+        ref.vector_field()
+        dt = time.perf_counter() - t0
+        kind = "reference"
+    else:
+        from ncorpion_b200.api import Params
+        p = Params()
+        p.G, p.softening_parameter, p.central_mass_bool, p.mutual_bool = 1.0, SOFTENING, 1, 1
+        port = oracle.Port()
+        t0 = time.perf_counter()
+        port.vector_field(sub, exs, cm, p)
+        dt = time.perf_counter() - t0
+        kind = "port"
+    return nsample * (nsample - 1) / dt, dt, kind
+
+
+def run_reference_arm(a, ws, rank):
+    if rank != 0:
+        return 0
+    b, ex, cm = make_workload()
+    times = []
+    for i in range(a.warmup + a.steps):
+        rate, dt, kind = cpu_reference_rate(b, ex, cm, REF_SAMPLE)
+        if i >= a.warmup:
+            times.append(dt)
+    t = float(np.mean(times))
+    v = REF_SAMPLE * (REF_SAMPLE - 1) / t
+    out = {"metric": METRIC, "value": v, "unit": "pair-interactions/s", "n_gpus": a.gpus, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+           "config": {"workload": WORKLOAD, "n": N_BODIES, "sample_bodies": REF_SAMPLE,
+                      "parallelism": "single thread (the reference has no threading)"},
+           "cpu_baseline": {"value": v, "unit": "pair-interactions/s", "cores": 1, "kind": kind,
+                            "sample": f"reference vector_field (gcc -O2, oracle/_ref/bf_grav_s05) on the first "
+                                      f"{REF_SAMPLE} of the {N_BODIES} bodies per step"},
+           "e2e": {"value": v, "unit": "pair-interactions/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args(argv)
+    a.warmup = max(a.warmup, 3)
+    ws, rank, local = dist_info()
+    if a.impl == "reference":
+        return run_reference_arm(a, ws, rank)
+
+    import torch
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from ncorpion_b200 import api, build
+    if not os.path.exists(api.LIB_PATH):
+        build.build()
+    lib = api.load()
+
+    b, ex, cm = make_workload()
+    n = N_BODIES
+    pairs = n * (n - 1)
+    api.init(n, params(api.GRAVITY_MIXED))
+    dev = torch.device("cuda", local)
+    d_b = torch.from_numpy(b).to(dev)
+    d_ex = torch.from_numpy(ex).to(dev)
+    d_acc = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    d_cma = torch.zeros(3, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    cmh = np.ascontiguousarray(cm)
+    sp = C.c_void_p(stream.cuda_stream)
+
+    def step(mode):
+        st = lib.ncgpu_vector_field_dev(C.c_void_p(d_b.data_ptr()), C.c_void_p(d_ex.data_ptr()), n - 1,
+                                        api.ptr(cmh), C.c_void_p(d_acc.data_ptr()), C.c_void_p(d_cma.data_ptr()),
+                                        mode, sp)
+        api.check(st, "ncgpu_vector_field_dev")
+
+    def timed(mode, steps, warmup):
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                step(mode)
+            torch.cuda.synchronize()
+            if ws > 1:
+                torch.distributed.barrier()
+            tot, kern, launches = 0.0, [], 0
+            for _ in range(steps):
+                flush.zero_()  # L2 flush between timed steps (outside the events)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                step(mode)
+                e1.record(stream)
+                launches += lib.ncgpu_last_launch_count()
+                e1.synchronize()
+                tot += e0.elapsed_time(e1)
+                kern.append(api.last_kernel_ms())
+            torch.cuda.synchronize()
+            if ws > 1:
+                torch.distributed.barrier()
+        ms = tot / steps
+        kms = float(np.mean(kern))
+        if ws > 1:
+            t = torch.tensor([ms, kms], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms, kms = float(t[0]), float(t[1])
+        return ms, kms, launches
+
+    clock = ClockSampler(local)
+    clock.start()
+    ms_mixed, kms_mixed, launches = timed(api.GRAVITY_MIXED, a.steps, a.warmup)
+    clocks = clock.stop()
+    ms_fp64t, kms_fp64t, _ = timed(api.GRAVITY_FP64, max(2, a.steps // 3), 1)
+    ms_exact, kms_exact, _ = timed(api.GRAVITY_EXACT, 2, 1)
+
+    # accuracy of the mixed kernel against the exact FP64 result
+    def accel(mode, central):
+        api.set_params(params(mode, central))
+        with torch.cuda.stream(stream):
+            step(mode)
+        torch.cuda.synchronize()
+        return d_acc.cpu().numpy().copy()
+
+    a_ex_mut = accel(api.GRAVITY_EXACT, 0)
+    a_mx_mut = accel(api.GRAVITY_MIXED, 0)
+    a_ex_tot = accel(api.GRAVITY_EXACT, 1)
+    a_mx_tot = accel(api.GRAVITY_MIXED, 1)
+    rel_mut = np.linalg.norm(a_mx_mut - a_ex_mut, axis=1) / np.linalg.norm(a_ex_mut, axis=1)
+    rel_tot = np.linalg.norm(a_mx_tot - a_ex_tot, axis=1) / np.linalg.norm(a_ex_tot, axis=1)
+    api.set_params(params(api.GRAVITY_MIXED))
+
+    # end to end through the host-buffer C ABI call (pinned host memory)
+    hb = b.copy()
+    hex_ = ex.copy()
+    api.check(lib.ncgpu_host_register(api.ptr(hb), hb.nbytes), "register")
+    api.check(lib.ncgpu_host_register(api.ptr(hex_), hex_.nbytes), "register")
+    cma = np.zeros(3)
+    for _ in range(2):
+        api.check(lib.ncgpu_vector_field(api.ptr(hb), api.ptr(hex_), n - 1, api.ptr(cmh), api.ptr(cma),
+                                         api.GRAVITY_MIXED), "e2e")
+        hb[:] = b
+    e2e_t = []
+    for _ in range(a.steps):
+        hb[:] = b
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        api.check(lib.ncgpu_vector_field(api.ptr(hb), api.ptr(hex_), n - 1, api.ptr(cmh), api.ptr(cma),
+                                         api.GRAVITY_MIXED), "e2e")
+        e2e_t.append(time.perf_counter() - t0)
+    lib.ncgpu_host_unregister(api.ptr(hb))
+    lib.ncgpu_host_unregister(api.ptr(hex_))
+    e2e_s = float(np.mean(e2e_t))
+    if ws > 1:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t[0])
+
+    fp32_peak = api.probe_fp32_peak()
+    achieved = FLOP_PER_INTERACTION * pairs / (kms_mixed * 1e-3) / 1e12
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        try:
+            rate, dt, kind = cpu_reference_rate(b, ex, cm, N_BODIES)
+            cpu = {"value": rate, "unit": "pair-interactions/s", "cores": 1, "kind": kind,
+                   "sample": f"one full vector_field call on all {N_BODIES} bodies ({dt:.1f} s, 1 thread, "
+                             "reference sources gcc -O2)"}
+        except Exception as e:  # reference build absent on this machine
+            cpu = {"value": None, "unit": "pair-interactions/s", "cores": 1, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        value = ws * pairs / (ms_mixed * 1e-3)
+        out = {
+            "metric": METRIC, "value": value, "unit": "pair-interactions/s", "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 pair terms, f64 state/accumulation", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": N_BODIES, "gravity_mode": "mixed",
+                       "l2": "flushed between timed steps (256 MiB write outside the events)",
+                       "parallelism": "replicas" if ws > 1 else "single GPU"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak, "traffic": None,
+                         "kernel": "k_grav_tiled<mixed>", "kernel_ms": kms_mixed,
+                         "flop_per_interaction": FLOP_PER_INTERACTION,
+                         "peak_source": "measured FFMA-chain probe (ncgpu_probe_fp32_peak) in this run"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": ws * pairs / e2e_s, "unit": "pair-interactions/s",
+                    "h2d_bytes_per_step": int(hb.nbytes + hex_.nbytes), "d2h_bytes_per_step": int(n * 24 + 24),
+                    "ms_per_step": e2e_s * 1e3},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "fp64_exact": {"value": ws * pairs / (ms_exact * 1e-3), "ms_per_step": ms_exact,
+                           "kernel_ms": kms_exact},
+            "fp64_tiled": {"value": ws * pairs / (ms_fp64t * 1e-3), "ms_per_step": ms_fp64t,
+                           "kernel_ms": kms_fp64t},
+            "speedup_mixed_vs_fp64_exact": ms_exact / ms_mixed,
+            "speedup_mixed_vs_fp64_tiled": ms_fp64t / ms_mixed,
+            "accuracy": {"mutual_rel_err_max": float(rel_mut.max()),
+                         "mutual_rel_err_median": float(np.median(rel_mut)),
+                         "total_rel_err_max": float(rel_tot.max()),
+                         "total_rel_err_median": float(np.median(rel_tot)),
+                         "reference": "exact FP64 kernel (bit-identical to the reference's vector_field)"},
+        }
+        print(json.dumps(out))
+    api.finalize()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,149 @@
+/*
+ * ncgpu.h - C ABI of the B200 engine for NcorpiON's mutual-interaction hot path.
+ *
+ * Plain C, no CUDA or torch types: every entry point takes host pointers,
+ * sizes and PODs (the *_dev variants take device pointers as void* / double*),
+ * and returns 0 (NCGPU_OK) or a negative NCGPU_E_* status.  The library owns a
+ * single, device-resident body state between calls (single host thread,
+ * single CUDA stream, not re-entrant), mirroring the reference's global state
+ * (src/structure.c:62-115).
+ *
+ * Body records use the reference's `struct moonlet` layout
+ * (src/structure.h:74-84): x, y, z, vx, vy, vz, mass, radius, all double.
+ */
+#ifndef NCGPU_H
+#define NCGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NCGPU_OK 0
+#define NCGPU_E_ARG (-1)       /* bad argument (null pointer, size, mode)            */
+#define NCGPU_E_CUDA (-2)      /* a CUDA runtime call failed                          */
+#define NCGPU_E_CAPACITY (-3)  /* a device append buffer (pairs, events) overflowed   */
+#define NCGPU_E_NMAX (-4)      /* a body append went past N_max (src/structure.c:860) */
+#define NCGPU_E_STATE (-5)     /* ncgpu_init was not called / state not uploaded      */
+#define NCGPU_E_TIMEOUT (-6)   /* a bounded device-side wait gave up                  */
+#define NCGPU_E_UNSUPPORTED (-7) /* configuration outside the implemented hot path    */
+
+/* Gravity arithmetic modes. */
+#define NCGPU_GRAVITY_EXACT 0  /* FP64, the reference's per-body summation order and
+                                  operation sequence: bit-identical to vector_field  */
+#define NCGPU_GRAVITY_FP64 1   /* FP64, space-filling-curve tiles, one rsqrt per pair */
+#define NCGPU_GRAVITY_MIXED 2  /* FP32 pair terms on tile-relative coordinates,
+                                  near tiles in FP64, compensated sums folded to FP64 */
+
+/* Collision resolution types, numbered as collision_treatment's
+   type_of_collision (src/physics.c:1043-1050). */
+#define NCGPU_COLLISION_ELASTIC 0
+#define NCGPU_COLLISION_INELASTIC 1
+#define NCGPU_COLLISION_MERGER 2
+#define NCGPU_COLLISION_FRAGMENTATION 3
+
+struct ncgpu_body {          /* = struct moonlet (src/structure.h:74-84) */
+      double x, y, z, vx, vy, vz, mass, radius;
+};
+
+struct ncgpu_pair {          /* = struct pair (src/structure.h, pairs[] of mesh()) */
+      int fst, snd;
+};
+
+struct ncgpu_event {         /* one collision_treatment(a, b, type) call, in order */
+      int a, b, type;
+};
+
+/* Mirror of the parameters.h macros that the hot path reads
+   (src/parameters.h:66-119, 171-201, 283-309). */
+struct ncgpu_params {
+      double G;                      /* G                                        */
+      double softening_parameter;    /* softening_parameter (x (R_k + R_p))      */
+      int central_mass_bool;         /* central_mass_bool                        */
+      int mutual_bool;               /* mutual_bool                              */
+      int collision_bool;            /* collision_bool                           */
+      int brute_force_bool;          /* brute_force_bool                         */
+      int mesh_bool;                 /* mesh_bool                                */
+      int collision_type;            /* NCGPU_COLLISION_*                        */
+      double collision_parameter;    /* collision_parameter (inelastic f)        */
+      int one_collision_only_bool;   /* one_collision_only_bool                  */
+      int collision_cube_cells;      /* collision_cube_cells (mesh)              */
+      double how_many_neighbours;    /* how_many_neighbours (mesh)               */
+      double collision_cube_min;     /* collision_cube_min (mesh)                */
+      int switch_to_brute_force;     /* switch_to_brute_force                    */
+      int gravity_mode;              /* NCGPU_GRAVITY_*                          */
+      double near_theta;             /* MIXED: tile pairs whose boxes are closer
+                                        than near_theta x the larger box diagonal
+                                        are summed in FP64 (default 0.5 if <= 0) */
+};
+
+/* Fills *p with the reference's default values for the fields above
+   (G = 39.478..., softening 0, central mass on, mutual on, ...). */
+void ncgpu_default_params(struct ncgpu_params *p);
+
+/* Allocates device state for n_max body slots (N_max, src/parameters.h:171)
+   and copies the parameters.  Replaces array_initialization's allocations
+   (src/structure.c:553-647). */
+int ncgpu_init(int n_max, const struct ncgpu_params *params);
+void ncgpu_finalize(void);
+/* Replaces the parameters of an initialised library (no reallocation). */
+int ncgpu_set_params(const struct ncgpu_params *params);
+const char *ncgpu_strerror(int status);
+/* Last CUDA error string recorded by the library (for NCGPU_E_CUDA). */
+const char *ncgpu_last_error(void);
+
+/* ---- stateless force evaluation ------------------------------------------ */
+
+/* vector_field (src/physics.c:63-441), brute-force branch with the central
+   mass term: for every slot k <= largest_id with exists[k] != 0, writes the
+   acceleration of body k into bodies[k].vx, vy, vz (the reference stores
+   accelerations in the velocity fields, src/physics.c:264-266) and the central
+   mass back-reaction into cm_acc[3] (CM_acc, src/physics.c:137-139).  Host
+   buffers; copies in and out on the library stream. */
+int ncgpu_vector_field(struct ncgpu_body *bodies, const int *exists, int largest_id,
+                       const struct ncgpu_body *cm, double *cm_acc, int gravity_mode);
+
+/* Same computation on device-resident buffers: d_bodies holds 8 doubles per
+   slot (struct moonlet layout), d_exists one int per slot, d_acc receives
+   3 doubles per slot (zero for empty slots), d_cm_acc 3 doubles.  cm points to
+   host memory.  stream is a cudaStream_t (NULL = the library stream). */
+int ncgpu_vector_field_dev(const double *d_bodies, const int *d_exists, int largest_id,
+                           const struct ncgpu_body *cm, double *d_acc, double *d_cm_acc,
+                           int gravity_mode, void *stream);
+
+/* Number of kernel launches issued by the last API call. */
+int ncgpu_last_launch_count(void);
+/* Device time (CUDA events on the launching stream) of the dominant kernel of
+   the last gravity evaluation (the pair-sum kernel), in milliseconds. */
+int ncgpu_last_kernel_ms(double *ms);
+
+/* Page-locks a host buffer (e.g. the reference's moonlets array) so the
+   library's host<->device copies of it run at full bus speed. */
+int ncgpu_host_register(void *ptr, unsigned long bytes);
+int ncgpu_host_unregister(void *ptr);
+
+/* Diagnostic: measures this GPU's FP32 FFMA throughput with a dependent-chain
+   kernel (2 flops per FFMA) and returns it in *tflops; used as the roofline
+   denominator of the FP32 gravity kernel. */
+int ncgpu_probe_fp32_peak(double *tflops);
+
+/* ---- device-resident integrator state ------------------------------------ */
+
+/* Uploads slots 0..largest_id (bodies + exists) and the central mass. */
+int ncgpu_upload(const struct ncgpu_body *bodies, const int *exists, int largest_id,
+                 const struct ncgpu_body *cm);
+/* Downloads slots 0..*largest_id into host arrays of at least n_max slots. */
+int ncgpu_download(struct ncgpu_body *bodies, int *exists, int *largest_id,
+                   struct ncgpu_body *cm);
+/* timestep global (src/structure.c, used by kick/drift/closest_approach). */
+int ncgpu_set_timestep(double dt);
+
+/* kick (src/rk4.c:68-106) with F = vector_field in the configured gravity
+   mode: v += timestep * a for existing bodies, CM.v += timestep * CM_acc. */
+int ncgpu_kick(void);
+/* drift (src/rk4.c:109-127): x += timestep * v, CM too. */
+int ncgpu_drift(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NCGPU_H */

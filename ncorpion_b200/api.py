@@ -1,0 +1,198 @@
+"""ctypes binding of the C ABI declared in ``include/ncgpu.h``.
+
+This is the Python face of the same library a C host links against.  It loads
+``ncorpion_b200/libncgpu.so`` and raises if it is missing: there is no CPU or
+PyTorch fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import LIB_PATH
+
+OK = 0
+E_ARG, E_CUDA, E_CAPACITY, E_NMAX, E_STATE, E_TIMEOUT, E_UNSUPPORTED = -1, -2, -3, -4, -5, -6, -7
+
+GRAVITY_EXACT, GRAVITY_FP64, GRAVITY_MIXED = 0, 1, 2
+GRAVITY_MODES = {"exact": GRAVITY_EXACT, "fp64": GRAVITY_FP64, "mixed": GRAVITY_MIXED}
+COLLISION_ELASTIC, COLLISION_INELASTIC, COLLISION_MERGER, COLLISION_FRAGMENTATION = 0, 1, 2, 3
+
+
+class Params(C.Structure):
+    """Mirror of ``struct ncgpu_params`` (the parameters.h macros on the path)."""
+
+    _fields_ = [
+        ("G", C.c_double),
+        ("softening_parameter", C.c_double),
+        ("central_mass_bool", C.c_int),
+        ("mutual_bool", C.c_int),
+        ("collision_bool", C.c_int),
+        ("brute_force_bool", C.c_int),
+        ("mesh_bool", C.c_int),
+        ("collision_type", C.c_int),
+        ("collision_parameter", C.c_double),
+        ("one_collision_only_bool", C.c_int),
+        ("collision_cube_cells", C.c_int),
+        ("how_many_neighbours", C.c_double),
+        ("collision_cube_min", C.c_double),
+        ("switch_to_brute_force", C.c_int),
+        ("gravity_mode", C.c_int),
+        ("near_theta", C.c_double),
+    ]
+
+
+class NcgpuError(RuntimeError):
+    def __init__(self, status, where, lib=None):
+        msg = f"{where}: status {status}"
+        if lib is not None:
+            msg += f" ({lib.ncgpu_strerror(status).decode()})"
+            if status == E_CUDA:
+                msg += f": {lib.ncgpu_last_error().decode()}"
+        super().__init__(msg)
+        self.status = status
+
+
+_lib = None
+
+P = C.c_void_p
+EXPORTS = {
+    # name: (restype, argtypes)
+    "ncgpu_default_params": (None, [P]),
+    "ncgpu_init": (C.c_int, [C.c_int, P]),
+    "ncgpu_finalize": (None, []),
+    "ncgpu_strerror": (C.c_char_p, [C.c_int]),
+    "ncgpu_last_error": (C.c_char_p, []),
+    "ncgpu_vector_field": (C.c_int, [P, P, C.c_int, P, P, C.c_int]),
+    "ncgpu_vector_field_dev": (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P]),
+    "ncgpu_last_launch_count": (C.c_int, []),
+    "ncgpu_upload": (C.c_int, [P, P, C.c_int, P]),
+    "ncgpu_download": (C.c_int, [P, P, P, P]),
+    "ncgpu_set_timestep": (C.c_int, [C.c_double]),
+    "ncgpu_kick": (C.c_int, []),
+    "ncgpu_set_params": (C.c_int, [P]),
+    "ncgpu_host_register": (C.c_int, [P, C.c_ulong]),
+    "ncgpu_host_unregister": (C.c_int, [P]),
+    "ncgpu_probe_fp32_peak": (C.c_int, [P]),
+    "ncgpu_last_kernel_ms": (C.c_int, [P]),
+    "ncgpu_drift": (C.c_int, []),
+}
+
+
+def load(path: str | None = None):
+    """Load libncgpu.so (once) and declare the exported signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -m ncorpion_b200.build` "
+            "(the GPU path has no fallback)")
+    lib = C.CDLL(path)
+    for name, (res, args) in EXPORTS.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+def check(status: int, where: str):
+    if status != OK:
+        raise NcgpuError(status, where, _lib)
+
+
+def default_params(**kw) -> Params:
+    lib = load()
+    p = Params()
+    lib.ncgpu_default_params(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    return p
+
+
+def init(n_max: int, params: Params):
+    lib = load()
+    check(lib.ncgpu_init(int(n_max), C.byref(params)), "ncgpu_init")
+
+
+def set_params(params: Params):
+    check(load().ncgpu_set_params(C.byref(params)), "ncgpu_set_params")
+
+
+def probe_fp32_peak() -> float:
+    v = C.c_double(0.0)
+    check(load().ncgpu_probe_fp32_peak(C.byref(v)), "ncgpu_probe_fp32_peak")
+    return v.value
+
+
+def last_kernel_ms() -> float:
+    v = C.c_double(0.0)
+    check(load().ncgpu_last_kernel_ms(C.byref(v)), "ncgpu_last_kernel_ms")
+    return v.value
+
+
+def finalize():
+    load().ncgpu_finalize()
+
+
+def _bodies(b):
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    assert b.ndim == 2 and b.shape[1] == 8
+    return b
+
+
+def vector_field(bodies, exists=None, cm=None, mode="exact"):
+    """Accelerations of all existing bodies (copy of ``bodies``' layout with
+    vx, vy, vz replaced by the acceleration) and the central-mass CM_acc."""
+    lib = load()
+    b = _bodies(bodies).copy()
+    n = b.shape[0]
+    ex = np.ones(n, np.int32) if exists is None else np.ascontiguousarray(exists, dtype=np.int32)
+    cmv = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0]) if cm is None else np.ascontiguousarray(cm, np.float64)
+    cma = np.zeros(3)
+    st = lib.ncgpu_vector_field(ptr(b), ptr(ex), n - 1, ptr(cmv), ptr(cma), GRAVITY_MODES.get(mode, mode))
+    check(st, "ncgpu_vector_field")
+    acc = b[:, 3:6].copy()
+    acc[ex == 0] = 0.0
+    return acc, cma
+
+
+def upload(bodies, exists, cm):
+    lib = load()
+    b = _bodies(bodies)
+    ex = np.ascontiguousarray(exists, dtype=np.int32)
+    cmv = np.ascontiguousarray(cm, np.float64)
+    check(lib.ncgpu_upload(ptr(b), ptr(ex), b.shape[0] - 1, ptr(cmv)), "ncgpu_upload")
+
+
+def download(n_max: int):
+    lib = load()
+    b = np.zeros((n_max, 8))
+    ex = np.zeros(n_max, np.int32)
+    lid = C.c_int(0)
+    cm = np.zeros(8)
+    check(lib.ncgpu_download(ptr(b), ptr(ex), C.byref(lid), ptr(cm)), "ncgpu_download")
+    k = lid.value + 1
+    return b[:k].copy(), ex[:k].copy(), cm
+
+
+def set_timestep(dt: float):
+    check(load().ncgpu_set_timestep(float(dt)), "ncgpu_set_timestep")
+
+
+def kick():
+    check(load().ncgpu_kick(), "ncgpu_kick")
+
+
+def drift():
+    check(load().ncgpu_drift(), "ncgpu_drift")

@@ -1,0 +1,467 @@
+// C-ABI entry points of libncgpu: context lifetime, state transfer, the
+// stateless vector_field replacement and the leapfrog kick / drift.
+#include <string.h>
+#include <stdlib.h>
+#include <algorithm>
+#include "common.cuh"
+
+namespace ncg {
+
+static Ctx g_ctx;
+static char g_last_error[512] = "";
+static int g_launches = 0;
+
+Ctx &ctx() { return g_ctx; }
+
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line)
+{
+      snprintf(g_last_error, sizeof g_last_error, "%s: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+      return NCGPU_E_CUDA;
+}
+void note_launch() { ++g_launches; }
+void reset_launches() { g_launches = 0; }
+int launches() { return g_launches; }
+
+int ensure_partial(size_t doubles)
+{
+      Ctx &c = ctx();
+      if (doubles <= c.partial_cap) return NCGPU_OK;
+      if (c.partial) NCG_CK(cudaFree(c.partial));
+      c.partial = nullptr;
+      c.partial_cap = 0;
+      NCG_CK(cudaMalloc(&c.partial, doubles * sizeof(double)));
+      c.partial_cap = doubles;
+      return NCGPU_OK;
+}
+
+int check_err_word()
+{
+      Ctx &c = ctx();
+      unsigned h = 0;
+      NCG_CK(cudaMemcpyAsync(&h, c.err, sizeof h, cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaStreamSynchronize(c.s));
+      if (h) NCG_CK(cudaMemsetAsync(c.err, 0, sizeof(unsigned), c.s));
+      if (h & ERR_TIMEOUT) return NCGPU_E_TIMEOUT;
+      if (h & ERR_NMAX) return NCGPU_E_NMAX;
+      if (h & ERR_CAPACITY) return NCGPU_E_CAPACITY;
+      if (h) return NCGPU_E_CUDA;
+      return NCGPU_OK;
+}
+
+namespace {
+
+template <class Tp>
+int dalloc(Tp **p, size_t count)
+{
+      NCG_CK(cudaMalloc((void **)p, count * sizeof(Tp)));
+      return NCGPU_OK;
+}
+
+void free_all()
+{
+      Ctx &c = ctx();
+      void *ptrs[] = {c.x, c.y, c.z, c.vx, c.vy, c.vz, c.m, c.R, c.ex, c.cm, c.cm_acc, c.acc, c.cmterm,
+                      c.partial, c.cidx, c.cnt, c.n_dev, c.src64, c.srcR, c.src32, c.srcR32, c.tilebox,
+                      c.keys, c.keys2, c.vals, c.vals2, c.hist, c.red, c.err, c.aos, c.exs};
+      for (void *p : ptrs)
+            if (p) cudaFree(p);
+      if (c.pinned) cudaFreeHost(c.pinned);
+      if (c.kev0) cudaEventDestroy(c.kev0);
+      if (c.kev1) cudaEventDestroy(c.kev1);
+      if (c.s) cudaStreamDestroy(c.s);
+      c = Ctx{};
+}
+
+__global__ void k_aos_to_soa(const double *__restrict__ aos, int n, double *x, double *y, double *z, double *vx,
+                             double *vy, double *vz, double *m, double *R)
+{
+      int i = blockIdx.x * blockDim.x + threadIdx.x;
+      if (i >= n) return;
+      const double *b = aos + 8 * (size_t)i;
+      x[i] = b[0]; y[i] = b[1]; z[i] = b[2];
+      vx[i] = b[3]; vy[i] = b[4]; vz[i] = b[5];
+      m[i] = b[6]; R[i] = b[7];
+}
+
+__global__ void k_soa_to_aos(double *__restrict__ aos, int n, const double *x, const double *y, const double *z,
+                             const double *vx, const double *vy, const double *vz, const double *m, const double *R)
+{
+      int i = blockIdx.x * blockDim.x + threadIdx.x;
+      if (i >= n) return;
+      double *b = aos + 8 * (size_t)i;
+      b[0] = x[i]; b[1] = y[i]; b[2] = z[i];
+      b[3] = vx[i]; b[4] = vy[i]; b[5] = vz[i];
+      b[6] = m[i]; b[7] = R[i];
+}
+
+// kick, src/rk4.c:96-105: v += timestep * a for existing bodies, then the
+// central mass with CM_acc.  Explicit _rn operations: no FMA contraction.
+__global__ void k_kick(const int *__restrict__ ex, int n, double dt, const double *__restrict__ ax,
+                       const double *__restrict__ ay, const double *__restrict__ az, double *vx, double *vy,
+                       double *vz, double *cm, const double *__restrict__ cm_acc, int kick_cm)
+{
+      int i = blockIdx.x * blockDim.x + threadIdx.x;
+      if (i < n && ex[i]) {
+            vx[i] = __dadd_rn(vx[i], __dmul_rn(dt, ax[i]));
+            vy[i] = __dadd_rn(vy[i], __dmul_rn(dt, ay[i]));
+            vz[i] = __dadd_rn(vz[i], __dmul_rn(dt, az[i]));
+      }
+      if (i == 0 && kick_cm) {
+            cm[3] = __dadd_rn(cm[3], __dmul_rn(dt, cm_acc[0]));
+            cm[4] = __dadd_rn(cm[4], __dmul_rn(dt, cm_acc[1]));
+            cm[5] = __dadd_rn(cm[5], __dmul_rn(dt, cm_acc[2]));
+      }
+}
+
+// drift, src/rk4.c:115-126: x += timestep * v.
+__global__ void k_drift(const int *__restrict__ ex, int n, double dt, double *x, double *y, double *z,
+                        const double *__restrict__ vx, const double *__restrict__ vy,
+                        const double *__restrict__ vz, double *cm, int drift_cm)
+{
+      int i = blockIdx.x * blockDim.x + threadIdx.x;
+      if (i < n && ex[i]) {
+            x[i] = __dadd_rn(x[i], __dmul_rn(dt, vx[i]));
+            y[i] = __dadd_rn(y[i], __dmul_rn(dt, vy[i]));
+            z[i] = __dadd_rn(z[i], __dmul_rn(dt, vz[i]));
+      }
+      if (i == 0 && drift_cm) {
+            cm[0] = __dadd_rn(cm[0], __dmul_rn(dt, cm[3]));
+            cm[1] = __dadd_rn(cm[1], __dmul_rn(dt, cm[4]));
+            cm[2] = __dadd_rn(cm[2], __dmul_rn(dt, cm[5]));
+      }
+}
+
+}  // namespace
+
+BodyView state_view()
+{
+      Ctx &c = ctx();
+      BodyView v{c.x, c.y, c.z, c.vx, c.vy, c.vz, c.m, c.R, 1, c.ex};
+      return v;
+}
+
+int state_cm_host(double *cm8)
+{
+      Ctx &c = ctx();
+      NCG_CK(cudaMemcpyAsync(cm8, c.cm, 8 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaStreamSynchronize(c.s));
+      return NCGPU_OK;
+}
+
+int kick_state()
+{
+      Ctx &c = ctx();
+      double cm8[8];
+      NCG_TRY(state_cm_host(cm8));
+      const int nslots = c.largest_id + 1;
+      NCG_TRY(gravity_eval(state_view(), c.largest_id, cm8, c.acc, c.n_max, c.cm_acc, c.P.gravity_mode, c.s));
+      int nb = nslots > 0 ? (nslots + 255) / 256 : 1;
+      k_kick<<<nb, 256, 0, c.s>>>(c.ex, nslots, c.dt, c.acc, c.acc + c.n_max, c.acc + 2 * (size_t)c.n_max, c.vx,
+                                  c.vy, c.vz, c.cm, c.cm_acc, c.P.central_mass_bool);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
+
+int drift_state()
+{
+      Ctx &c = ctx();
+      const int nslots = c.largest_id + 1;
+      int nb = nslots > 0 ? (nslots + 255) / 256 : 1;
+      k_drift<<<nb, 256, 0, c.s>>>(c.ex, nslots, c.dt, c.x, c.y, c.z, c.vx, c.vy, c.vz, c.cm,
+                                   c.P.central_mass_bool);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
+
+}  // namespace ncg
+
+using namespace ncg;
+
+extern "C" {
+
+void ncgpu_default_params(struct ncgpu_params *p)
+{
+      if (!p) return;
+      memset(p, 0, sizeof *p);
+      p->G = 39.47841760435743447533796;  // src/parameters.h:131
+      p->softening_parameter = 0.;
+      p->central_mass_bool = 1;
+      p->mutual_bool = 1;
+      p->collision_bool = 1;
+      p->brute_force_bool = 1;
+      p->mesh_bool = 0;
+      p->collision_type = NCGPU_COLLISION_MERGER;
+      p->collision_parameter = 2.;
+      p->one_collision_only_bool = 0;
+      p->collision_cube_cells = 1024;
+      p->how_many_neighbours = 16.;
+      p->collision_cube_min = 80.;
+      p->switch_to_brute_force = 110;
+      p->gravity_mode = NCGPU_GRAVITY_EXACT;
+      p->near_theta = 0.5;
+}
+
+const char *ncgpu_strerror(int s)
+{
+      switch (s) {
+      case NCGPU_OK: return "ok";
+      case NCGPU_E_ARG: return "bad argument";
+      case NCGPU_E_CUDA: return "CUDA error";
+      case NCGPU_E_CAPACITY: return "device buffer capacity exceeded";
+      case NCGPU_E_NMAX: return "Cannot add a body to the simulation. Try increasing the value of N_max.";
+      case NCGPU_E_STATE: return "library not initialised or state not uploaded";
+      case NCGPU_E_TIMEOUT: return "device-side wait timed out";
+      case NCGPU_E_UNSUPPORTED: return "configuration not supported by the GPU path";
+      default: return "unknown status";
+      }
+}
+
+const char *ncgpu_last_error(void) { return g_last_error; }
+int ncgpu_last_launch_count(void) { return launches(); }
+
+int ncgpu_init(int n_max, const struct ncgpu_params *params)
+{
+      if (n_max <= 0 || !params) return NCGPU_E_ARG;
+      if (params->gravity_mode < 0 || params->gravity_mode > 2) return NCGPU_E_ARG;
+      if (g_ctx.inited) ncgpu_finalize();
+      Ctx &c = g_ctx;
+      c.P = *params;
+      c.n_max = n_max;
+      size_t N = (size_t)n_max;
+      size_t npad = ((N + 127) / 128) * 128;
+      int st = NCGPU_OK;
+#define A(ptr, cnt)                                          \
+      do {                                                   \
+            if ((st = dalloc(&(ptr), (cnt))) != NCGPU_OK) {  \
+                  free_all();                                \
+                  return st;                                 \
+            }                                                \
+      } while (0)
+      A(c.x, N); A(c.y, N); A(c.z, N); A(c.vx, N); A(c.vy, N); A(c.vz, N); A(c.m, N); A(c.R, N);
+      A(c.ex, N); A(c.exs, N);
+      A(c.cm, 8); A(c.cm_acc, 3);
+      A(c.acc, 3 * N);
+      A(c.cmterm, 3 * N);
+      A(c.cidx, N);
+      A(c.cnt, (N + 1023) / 1024 + 1);
+      A(c.n_dev, 8);
+      {
+            double *p = nullptr;
+            A(p, 4 * npad);
+            c.src64 = p;
+      }
+      A(c.srcR, npad);
+      {
+            float *p = nullptr;
+            A(p, 4 * npad);
+            c.src32 = p;
+      }
+      A(c.srcR32, npad);
+      A(c.tilebox, 6 * (npad / 128));
+      A(c.keys, N); A(c.keys2, N); A(c.vals, N); A(c.vals2, N);
+      c.hist_cap = 256 * ((N + 2047) / 2048);
+      A(c.hist, c.hist_cap);
+      A(c.red, 4096);
+      A(c.err, 1);
+      A(c.aos, 8 * N);
+#undef A
+      if (cudaMallocHost((void **)&c.pinned, 8 * N * sizeof(double)) != cudaSuccess) {
+            free_all();
+            return NCGPU_E_CUDA;
+      }
+      if (cudaEventCreate(&c.kev0) != cudaSuccess || cudaEventCreate(&c.kev1) != cudaSuccess) {
+            free_all();
+            return NCGPU_E_CUDA;
+      }
+      if (cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking) != cudaSuccess) {
+            free_all();
+            return NCGPU_E_CUDA;
+      }
+      if ((st = ensure_partial(3 * std::max(npad, (size_t)4096 * 128))) != NCGPU_OK) {
+            free_all();
+            return st;
+      }
+      cudaMemsetAsync(c.err, 0, sizeof(unsigned), c.s);
+      cudaMemsetAsync(c.ex, 0, N * sizeof(int), c.s);
+      double cm0[8] = {0., 0., 0., 0., 0., 0., 1., 1.};
+      cudaMemcpyAsync(c.cm, cm0, sizeof cm0, cudaMemcpyHostToDevice, c.s);
+      if (cudaStreamSynchronize(c.s) != cudaSuccess) {
+            free_all();
+            return NCGPU_E_CUDA;
+      }
+      c.inited = 1;
+      return NCGPU_OK;
+}
+
+int ncgpu_last_kernel_ms(double *ms)
+{
+      if (!ms) return NCGPU_E_ARG;
+      if (!g_ctx.inited || !g_ctx.kev_valid) return NCGPU_E_STATE;
+      NCG_CK(cudaEventSynchronize(g_ctx.kev1));
+      float f = 0.f;
+      NCG_CK(cudaEventElapsedTime(&f, g_ctx.kev0, g_ctx.kev1));
+      *ms = f;
+      return NCGPU_OK;
+}
+
+int ncgpu_set_params(const struct ncgpu_params *params)
+{
+      if (!g_ctx.inited) return NCGPU_E_STATE;
+      if (!params || params->gravity_mode < 0 || params->gravity_mode > 2) return NCGPU_E_ARG;
+      g_ctx.P = *params;
+      return NCGPU_OK;
+}
+
+int ncgpu_host_register(void *ptr, unsigned long bytes)
+{
+      if (!ptr || bytes == 0) return NCGPU_E_ARG;
+      NCG_CK(cudaHostRegister(ptr, (size_t)bytes, cudaHostRegisterDefault));
+      return NCGPU_OK;
+}
+
+int ncgpu_host_unregister(void *ptr)
+{
+      if (!ptr) return NCGPU_E_ARG;
+      NCG_CK(cudaHostUnregister(ptr));
+      return NCGPU_OK;
+}
+
+void ncgpu_finalize(void)
+{
+      if (g_ctx.s) cudaStreamSynchronize(g_ctx.s);
+      free_all();
+}
+
+int ncgpu_vector_field_dev(const double *d_bodies, const int *d_exists, int largest_id,
+                           const struct ncgpu_body *cm, double *d_acc, double *d_cm_acc, int gravity_mode,
+                           void *stream)
+{
+      Ctx &c = g_ctx;
+      reset_launches();
+      if (!c.inited) return NCGPU_E_STATE;
+      if (!d_bodies || !d_exists || !cm || !d_acc || !d_cm_acc) return NCGPU_E_ARG;
+      if (largest_id < -1 || largest_id >= c.n_max) return NCGPU_E_ARG;
+      cudaStream_t st = stream ? (cudaStream_t)stream : c.s;
+      BodyView bv{d_bodies, d_bodies + 1, d_bodies + 2, d_bodies + 3, d_bodies + 4, d_bodies + 5,
+                  d_bodies + 6, d_bodies + 7, 8, d_exists};
+      // d_acc is 3 consecutive blocks of (largest_id + 1) doubles
+      long bs = largest_id + 1;
+      // gravity_eval writes ax, ay, az blocks; repack to xyz triples
+      NCG_TRY(gravity_eval(bv, largest_id, (const double *)cm, c.acc, c.n_max, d_cm_acc, gravity_mode, st));
+      if (bs > 0) {
+            // interleave into d_acc[3*k + d]
+            NCG_CK(cudaMemcpy2DAsync(d_acc, 3 * sizeof(double), c.acc, sizeof(double), sizeof(double), bs,
+                                     cudaMemcpyDeviceToDevice, st));
+            NCG_CK(cudaMemcpy2DAsync(d_acc + 1, 3 * sizeof(double), c.acc + c.n_max, sizeof(double),
+                                     sizeof(double), bs, cudaMemcpyDeviceToDevice, st));
+            NCG_CK(cudaMemcpy2DAsync(d_acc + 2, 3 * sizeof(double), c.acc + 2 * (size_t)c.n_max, sizeof(double),
+                                     sizeof(double), bs, cudaMemcpyDeviceToDevice, st));
+      }
+      return NCGPU_OK;
+}
+
+int ncgpu_vector_field(struct ncgpu_body *bodies, const int *exists, int largest_id, const struct ncgpu_body *cm,
+                       double *cm_acc, int gravity_mode)
+{
+      Ctx &c = g_ctx;
+      reset_launches();
+      if (!c.inited) return NCGPU_E_STATE;
+      if (!bodies || !exists || !cm || !cm_acc) return NCGPU_E_ARG;
+      if (largest_id < -1 || largest_id >= c.n_max) return NCGPU_E_ARG;
+      const int ns = largest_id + 1;
+      cudaStream_t st = c.s;
+      if (ns > 0) {
+            NCG_CK(cudaMemcpyAsync(c.aos, bodies, sizeof(struct ncgpu_body) * (size_t)ns, cudaMemcpyHostToDevice, st));
+            NCG_CK(cudaMemcpyAsync(c.exs, exists, sizeof(int) * (size_t)ns, cudaMemcpyHostToDevice, st));
+      }
+      BodyView bv{c.aos, c.aos + 1, c.aos + 2, c.aos + 3, c.aos + 4, c.aos + 5, c.aos + 6, c.aos + 7, 8, c.exs};
+      NCG_TRY(gravity_eval(bv, largest_id, (const double *)cm, c.acc, c.n_max, c.cm_acc, gravity_mode, st));
+      double *h = c.pinned;
+      if (ns > 0) {
+            NCG_CK(cudaMemcpyAsync(h, c.acc, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaMemcpyAsync(h + ns, c.acc + c.n_max, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaMemcpyAsync(h + 2 * ns, c.acc + 2 * (size_t)c.n_max, sizeof(double) * ns,
+                                   cudaMemcpyDeviceToHost, st));
+      }
+      NCG_CK(cudaMemcpyAsync(h + 3 * ns, c.cm_acc, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      NCG_TRY(check_err_word());
+      for (int k = 0; k < ns; k++) {
+            if (!exists[k]) continue;
+            bodies[k].vx = h[k];
+            bodies[k].vy = h[ns + k];
+            bodies[k].vz = h[2 * ns + k];
+      }
+      cm_acc[0] = h[3 * ns];
+      cm_acc[1] = h[3 * ns + 1];
+      cm_acc[2] = h[3 * ns + 2];
+      return NCGPU_OK;
+}
+
+int ncgpu_upload(const struct ncgpu_body *bodies, const int *exists, int largest_id, const struct ncgpu_body *cm)
+{
+      Ctx &c = g_ctx;
+      reset_launches();
+      if (!c.inited) return NCGPU_E_STATE;
+      if ((!bodies && largest_id >= 0) || (!exists && largest_id >= 0) || !cm) return NCGPU_E_ARG;
+      if (largest_id < -1 || largest_id >= c.n_max) return NCGPU_E_ARG;
+      const int ns = largest_id + 1;
+      cudaStream_t st = c.s;
+      NCG_CK(cudaMemsetAsync(c.ex, 0, sizeof(int) * (size_t)c.n_max, st));
+      if (ns > 0) {
+            NCG_CK(cudaMemcpyAsync(c.aos, bodies, sizeof(struct ncgpu_body) * (size_t)ns, cudaMemcpyHostToDevice, st));
+            NCG_CK(cudaMemcpyAsync(c.ex, exists, sizeof(int) * (size_t)ns, cudaMemcpyHostToDevice, st));
+            k_aos_to_soa<<<(ns + 255) / 256, 256, 0, st>>>(c.aos, ns, c.x, c.y, c.z, c.vx, c.vy, c.vz, c.m, c.R);
+            NCG_LAUNCHED();
+      }
+      NCG_CK(cudaMemcpyAsync(c.cm, cm, 8 * sizeof(double), cudaMemcpyHostToDevice, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      c.largest_id = largest_id;
+      c.uploaded = 1;
+      return NCGPU_OK;
+}
+
+int ncgpu_download(struct ncgpu_body *bodies, int *exists, int *largest_id, struct ncgpu_body *cm)
+{
+      Ctx &c = g_ctx;
+      reset_launches();
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      if (!bodies || !exists || !largest_id || !cm) return NCGPU_E_ARG;
+      const int ns = c.largest_id + 1;
+      cudaStream_t st = c.s;
+      if (ns > 0) {
+            k_soa_to_aos<<<(ns + 255) / 256, 256, 0, st>>>(c.aos, ns, c.x, c.y, c.z, c.vx, c.vy, c.vz, c.m, c.R);
+            NCG_LAUNCHED();
+            NCG_CK(cudaMemcpyAsync(bodies, c.aos, sizeof(struct ncgpu_body) * (size_t)ns, cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaMemcpyAsync(exists, c.ex, sizeof(int) * (size_t)ns, cudaMemcpyDeviceToHost, st));
+      }
+      NCG_CK(cudaMemcpyAsync(cm, c.cm, 8 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      *largest_id = c.largest_id;
+      return check_err_word();
+}
+
+int ncgpu_set_timestep(double dt)
+{
+      if (!g_ctx.inited) return NCGPU_E_STATE;
+      g_ctx.dt = dt;
+      return NCGPU_OK;
+}
+
+int ncgpu_kick(void)
+{
+      reset_launches();
+      if (!g_ctx.inited || !g_ctx.uploaded) return NCGPU_E_STATE;
+      NCG_TRY(kick_state());
+      return check_err_word();
+}
+
+int ncgpu_drift(void)
+{
+      reset_launches();
+      if (!g_ctx.inited || !g_ctx.uploaded) return NCGPU_E_STATE;
+      NCG_TRY(drift_state());
+      return NCGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,117 @@
+// Shared internals of libncgpu: the device-resident context, error plumbing
+// and small device helpers.  Host code is single-threaded by contract (the
+// reference itself is a single-threaded program with global state).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include "../../include/ncgpu.h"
+
+namespace ncg {
+
+// Records a CUDA failure (text kept for ncgpu_last_error) and returns the
+// library status.
+int cuda_fail(cudaError_t e, const char *what, const char *file, int line);
+void note_launch();          // counts kernel launches of the current API call
+void reset_launches();
+int launches();
+
+#define NCG_CK(call)                                                          \
+      do {                                                                    \
+            cudaError_t e_ = (call);                                          \
+            if (e_ != cudaSuccess) return ncg::cuda_fail(e_, #call, __FILE__, __LINE__); \
+      } while (0)
+
+// After a <<<>>> launch: count it and surface launch-configuration errors.
+#define NCG_LAUNCHED()                                                        \
+      do {                                                                    \
+            ncg::note_launch();                                               \
+            cudaError_t e_ = cudaGetLastError();                              \
+            if (e_ != cudaSuccess) return ncg::cuda_fail(e_, "kernel launch", __FILE__, __LINE__); \
+      } while (0)
+
+#define NCG_TRY(call)                                                         \
+      do {                                                                    \
+            int s_ = (call);                                                  \
+            if (s_ != NCGPU_OK) return s_;                                    \
+      } while (0)
+
+// Strided read-only view of body fields: AoS (struct moonlet, stride 8) or
+// SoA (stride 1).
+struct BodyView {
+      const double *x, *y, *z, *vx, *vy, *vz, *m, *R;
+      long stride;
+      const int *ex;
+};
+
+// Device error word bits (set by kernels instead of trapping).
+enum : unsigned {
+      ERR_CAPACITY = 1u,
+      ERR_NMAX = 2u,
+      ERR_TIMEOUT = 4u,
+      ERR_INTERNAL = 8u,
+};
+
+// Scratch and state owned by the library, sized from n_max at ncgpu_init.
+struct Ctx {
+      int inited = 0;
+      int n_max = 0;
+      ncgpu_params P{};
+      cudaStream_t s = nullptr;
+
+      // device-resident body state (SoA, FP64) + exists flags
+      double *x = nullptr, *y = nullptr, *z = nullptr;
+      double *vx = nullptr, *vy = nullptr, *vz = nullptr;
+      double *m = nullptr, *R = nullptr;
+      int *ex = nullptr;
+      int *exs = nullptr;          // scratch exists flags for stateless calls
+      int largest_id = -1;
+      int uploaded = 0;
+      double *cm = nullptr;        // 8 doubles: central mass record
+      double *cm_acc = nullptr;    // 3 doubles
+      double dt = 0.0;
+
+      // gravity scratch
+      double *acc = nullptr;       // 3 * n_max (x block, y block, z block)
+      double *cmterm = nullptr;    // 3 * n_max
+      double *partial = nullptr;   // gravity partial sums (chunks x 3 x n_max)
+      size_t partial_cap = 0;      // doubles
+      int *cidx = nullptr;         // compacted existing slot ids
+      int *cnt = nullptr;          // block counts for compaction/scans
+      int *n_dev = nullptr;        // small device scalars
+      void *src64 = nullptr;       // packed FP64 sources (double4 per body)
+      double *srcR = nullptr;      // softening * R per body (FP64)
+      void *src32 = nullptr;       // packed FP32 sources (float4 per body)
+      float *srcR32 = nullptr;
+      double *tilebox = nullptr;   // per tile: cx,cy,cz,hx,hy,hz (6 doubles)
+      uint32_t *keys = nullptr, *keys2 = nullptr;
+      int *vals = nullptr, *vals2 = nullptr;
+      int *hist = nullptr;         // radix histogram scratch
+      size_t hist_cap = 0;
+      double *red = nullptr;       // reduction scratch (bbox etc.)
+      unsigned *err = nullptr;     // device error word
+      double *aos = nullptr;       // 8 * n_max staging for host AoS copies
+      double *pinned = nullptr;    // pinned host staging (8 * n_max doubles)
+      cudaEvent_t kev0 = nullptr, kev1 = nullptr;  // bracket the dominant kernel
+      int kev_valid = 0;
+};
+
+Ctx &ctx();
+int ensure_partial(size_t doubles);
+int check_err_word();        // syncs the stream, reads and clears the device error word
+
+// Gravity driver (gravity.cu).  Reads bodies through `bv` for slots
+// 0..largest_id, writes acc (3 blocks of n_max: ax, ay, az, zero for empty
+// slots) and cm_acc (3 doubles, device).
+int gravity_eval(const BodyView &bv, int largest_id, const double *cm_host8, double *d_acc,
+                 long acc_stride_block, double *d_cm_acc, int mode, cudaStream_t st);
+
+// LSD radix sort of (key, value) pairs, stable; keys use `bits` low bits.
+// Result ends in (keys, vals) buffers passed in (ping-pong through ctx scratch).
+int radix_sort_pairs(uint32_t *keys, int *vals, int n, int bits, cudaStream_t st);
+
+// Stream compaction of existing slots 0..largest_id into ctx().cidx (ascending).
+// Returns the count through *n_host (synchronises).
+int compact_existing(const int *ex, int largest_id, int *n_host, cudaStream_t st);
+
+}  // namespace ncg

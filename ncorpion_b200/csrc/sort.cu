@@ -1,0 +1,193 @@
+// Order-preserving primitives: stream compaction of existing slots and a
+// stable LSD radix sort of (uint32 key, int value) pairs.  Both are used by the
+// tiled gravity (space-filling-curve ordering) and the mesh search (sort of
+// bodies by mesh cell, which replaces the reference's hash-table chains,
+// src/structure.c:577-610 and :712-841).
+#include "common.cuh"
+
+namespace ncg {
+
+namespace {
+
+constexpr int CB = 1024;  // compaction block (one slot per thread)
+
+__global__ void k_count_flags(const int *__restrict__ ex, int n, int *__restrict__ cnt)
+{
+      int i = blockIdx.x * CB + threadIdx.x;
+      int f = (i < n && ex[i] != 0) ? 1 : 0;
+      int c = __syncthreads_count(f);
+      if (threadIdx.x == 0) cnt[blockIdx.x] = c;
+}
+
+// Exclusive scan of a[0..n) in place with one block of 1024 threads; writes
+// the total to *total.
+__global__ void k_scan_single(int *__restrict__ a, int n, int *__restrict__ total)
+{
+      __shared__ int part[1024];
+      int t = threadIdx.x;
+      int seg = (n + 1023) / 1024;
+      int lo = t * seg, hi = min(n, lo + seg);
+      int s = 0;
+      for (int i = lo; i < hi; i++) s += a[i];
+      part[t] = s;
+      __syncthreads();
+      for (int off = 1; off < 1024; off <<= 1) {
+            int v = t >= off ? part[t - off] : 0;
+            __syncthreads();
+            part[t] += v;
+            __syncthreads();
+      }
+      int run = part[t] - s;  // exclusive prefix of this segment
+      for (int i = lo; i < hi; i++) {
+            int v = a[i];
+            a[i] = run;
+            run += v;
+      }
+      if (t == 1023) *total = part[1023];
+}
+
+__global__ void k_scatter_flags(const int *__restrict__ ex, int n, const int *__restrict__ off,
+                                int *__restrict__ out)
+{
+      __shared__ int wsum[CB / 32];
+      int i = blockIdx.x * CB + threadIdx.x;
+      int f = (i < n && ex[i] != 0) ? 1 : 0;
+      unsigned b = __ballot_sync(0xffffffffu, f);
+      int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+      int r = __popc(b & ((1u << lane) - 1u));
+      if (lane == 0) wsum[w] = __popc(b);
+      __syncthreads();
+      if (threadIdx.x < 32) {
+            int v = wsum[threadIdx.x];
+            for (int o = 1; o < 32; o <<= 1) {
+                  int u = __shfl_up_sync(0xffffffffu, v, o);
+                  if (threadIdx.x >= o) v += u;
+            }
+            wsum[threadIdx.x] = v - wsum[threadIdx.x];
+      }
+      __syncthreads();
+      if (f) out[off[blockIdx.x] + wsum[w] + r] = i;
+}
+
+// ---- radix sort -------------------------------------------------------------
+constexpr int RT = 256;           // threads per block
+constexpr int RK = 8;             // keys per thread
+constexpr int RB = RT * RK;       // keys per block
+constexpr int RADIX = 256;
+
+__global__ void k_radix_hist(const uint32_t *__restrict__ keys, int n, int shift,
+                             int *__restrict__ hist, int nblocks)
+{
+      __shared__ int h[RADIX];
+      h[threadIdx.x] = 0;
+      __syncthreads();
+      int base = blockIdx.x * RB;
+#pragma unroll
+      for (int r = 0; r < RK; r++) {
+            int i = base + r * RT + threadIdx.x;
+            if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xffu], 1);
+      }
+      __syncthreads();
+      hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void k_radix_scatter(const uint32_t *__restrict__ kin, const int *__restrict__ vin,
+                                uint32_t *__restrict__ kout, int *__restrict__ vout, int n,
+                                int shift, const int *__restrict__ hist, int nblocks)
+{
+      __shared__ int run[RADIX];
+      __shared__ int gofs[RADIX];
+      __shared__ int wc[RT / 32][RADIX];
+      int t = threadIdx.x, lane = t & 31, w = t >> 5;
+      run[t] = 0;
+      gofs[t] = hist[t * nblocks + blockIdx.x];
+      int base = blockIdx.x * RB;
+      for (int r = 0; r < RK; r++) {
+            for (int q = 0; q < RT / 32; q++) wc[q][t] = 0;
+            __syncthreads();
+            int i = base + r * RT + t;
+            uint32_t key = 0;
+            int val = 0;
+            int d = RADIX;  // sentinel: no key
+            if (i < n) {
+                  key = kin[i];
+                  val = vin[i];
+                  d = (key >> shift) & 0xffu;
+            }
+            unsigned peers = __match_any_sync(0xffffffffu, d);
+            int rk = __popc(peers & ((1u << lane) - 1u));
+            int leader = __ffs(peers) - 1;
+            if (lane == leader && d < RADIX) wc[w][d] = __popc(peers);
+            __syncthreads();
+            {
+                  int acc = run[t];
+#pragma unroll
+                  for (int q = 0; q < RT / 32; q++) {
+                        int c = wc[q][t];
+                        wc[q][t] = acc;
+                        acc += c;
+                  }
+                  run[t] = acc;
+            }
+            __syncthreads();
+            if (d < RADIX) {
+                  int dst = gofs[d] + wc[w][d] + rk;
+                  kout[dst] = key;
+                  vout[dst] = val;
+            }
+            __syncthreads();
+      }
+}
+
+}  // namespace
+
+int compact_existing(const int *ex, int largest_id, int *n_host, cudaStream_t st)
+{
+      Ctx &c = ctx();
+      int n = largest_id + 1;
+      if (n <= 0) {
+            *n_host = 0;
+            return NCGPU_OK;
+      }
+      int nb = (n + CB - 1) / CB;
+      k_count_flags<<<nb, CB, 0, st>>>(ex, n, c.cnt);
+      NCG_LAUNCHED();
+      k_scan_single<<<1, 1024, 0, st>>>(c.cnt, nb, c.n_dev);
+      NCG_LAUNCHED();
+      k_scatter_flags<<<nb, CB, 0, st>>>(ex, n, c.cnt, c.cidx);
+      NCG_LAUNCHED();
+      NCG_CK(cudaMemcpyAsync(n_host, c.n_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      return NCGPU_OK;
+}
+
+int radix_sort_pairs(uint32_t *keys, int *vals, int n, int bits, cudaStream_t st)
+{
+      Ctx &c = ctx();
+      if (n <= 1) return NCGPU_OK;
+      int nb = (n + RB - 1) / RB;
+      size_t need = (size_t)RADIX * nb;
+      if (need > c.hist_cap) return NCGPU_E_CAPACITY;
+      uint32_t *ka = keys, *kb = c.keys2;
+      int *va = vals, *vb = c.vals2;
+      if (keys == c.keys2 || vals == c.vals2) return NCGPU_E_ARG;
+      int passes = (bits + 7) / 8;
+      for (int p = 0; p < passes; p++) {
+            int shift = 8 * p;
+            k_radix_hist<<<nb, RT, 0, st>>>(ka, n, shift, c.hist, nb);
+            NCG_LAUNCHED();
+            k_scan_single<<<1, 1024, 0, st>>>(c.hist, (int)need, c.n_dev + 1);
+            NCG_LAUNCHED();
+            k_radix_scatter<<<nb, RT, 0, st>>>(ka, va, kb, vb, n, shift, c.hist, nb);
+            NCG_LAUNCHED();
+            uint32_t *tk = ka; ka = kb; kb = tk;
+            int *tv = va; va = vb; vb = tv;
+      }
+      if (ka != keys) {  // odd number of passes: result is in the scratch pair
+            NCG_CK(cudaMemcpyAsync(keys, ka, sizeof(uint32_t) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+            NCG_CK(cudaMemcpyAsync(vals, va, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+      }
+      return NCGPU_OK;
+}
+
+}  // namespace ncg

@@ -1,0 +1,145 @@
+"""TEST INFRASTRUCTURE ONLY: CPU oracles for the parity tests and the CPU
+baseline.  Never imported by the product package ``ncorpion_b200``.
+
+* ``Port``   the plain-C restatement ``oracle/ncorpion_oracle.c`` (runtime
+             parameters), built with gcc into ``oracle/_build/liboracle.so``.
+* ``Ref``    the reference's own sources compiled per profile by
+             ``oracle/ref_build.py`` into ``oracle/_ref/<profile>/libref.so``
+             (available where the reference tree was present at build time).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SRC = os.path.join(HERE, "ncorpion_oracle.c")
+PORT_LIB = os.path.join(HERE, "_build", "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+P = C.c_void_p
+
+
+def build_port(force: bool = False) -> str:
+    os.makedirs(os.path.dirname(PORT_LIB), exist_ok=True)
+    if force or not os.path.exists(PORT_LIB) or os.path.getmtime(PORT_LIB) < os.path.getmtime(PORT_SRC):
+        subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", PORT_SRC, "-o", PORT_LIB, "-lm"],
+                       check=True)
+    return PORT_LIB
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+class Port:
+    """ctypes face of the C restatement."""
+
+    def __init__(self):
+        self.lib = C.CDLL(build_port())
+        L = self.lib
+        L.orc_vector_field.argtypes = [C.c_int, P, P, P, P, P, P]
+        L.orc_kick.argtypes = [C.c_int, P, P, P, C.c_double, P]
+        L.orc_drift.argtypes = [C.c_int, P, P, P, C.c_double, P]
+
+    def vector_field(self, bodies, exists, cm, params):
+        b = np.ascontiguousarray(bodies, np.float64)
+        ex = np.ascontiguousarray(exists, np.int32)
+        cmv = np.ascontiguousarray(cm, np.float64)
+        acc = np.zeros((b.shape[0], 3))
+        cma = np.zeros(3)
+        self.lib.orc_vector_field(b.shape[0] - 1, _p(b), _p(ex), _p(cmv), C.byref(params), _p(acc), _p(cma))
+        return acc, cma
+
+    def kick(self, bodies, exists, cm, dt, params):
+        b = np.ascontiguousarray(bodies, np.float64).copy()
+        cmv = np.ascontiguousarray(cm, np.float64).copy()
+        ex = np.ascontiguousarray(exists, np.int32)
+        self.lib.orc_kick(b.shape[0] - 1, _p(b), _p(ex), _p(cmv), C.c_double(dt), C.byref(params))
+        return b, cmv
+
+    def drift(self, bodies, exists, cm, dt, params):
+        b = np.ascontiguousarray(bodies, np.float64).copy()
+        cmv = np.ascontiguousarray(cm, np.float64).copy()
+        ex = np.ascontiguousarray(exists, np.int32)
+        self.lib.orc_drift(b.shape[0] - 1, _p(b), _p(ex), _p(cmv), C.c_double(dt), C.byref(params))
+        return b, cmv
+
+
+def ref_available(profile: str) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, profile, "libref.so"))
+
+
+class Ref:
+    """One profile of the reference compiled from source (global state: one
+    instance per process and profile)."""
+
+    _cache: dict = {}
+
+    def __new__(cls, profile: str):
+        if profile in cls._cache:
+            return cls._cache[profile]
+        self = super().__new__(cls)
+        path = os.path.join(REF_DIR, profile, "libref.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        L = C.CDLL(path)
+        self.lib = L
+        self.profile = profile
+        L.orc_init.restype = C.c_int
+        L.orc_set_state.argtypes = [C.c_int, P, P, P, C.c_double, C.c_double]
+        L.orc_get_state.argtypes = [P, P, P, P]
+        L.orc_get_state.restype = C.c_int
+        L.orc_vector_field.argtypes = [P, P]
+        L.orc_set_timestep.argtypes = [C.c_double]
+        L.orc_events.argtypes = [P, C.c_int]
+        L.orc_events.restype = C.c_int
+        L.orc_n_max.restype = C.c_int
+        if hasattr(L, "orc_pairs"):
+            L.orc_pairs.argtypes = [P, C.c_int]
+            L.orc_pairs.restype = C.c_int
+            L.orc_total_neighbours.restype = C.c_long
+            L.orc_three_largest.argtypes = [P]
+            L.orc_mesh_counts.argtypes = [P]
+        L.orc_set_free.argtypes = [C.c_int, P]
+        if L.orc_init() != 0:
+            raise MemoryError("reference init failed")
+        self.n_max = L.orc_n_max()
+        cls._cache[profile] = self
+        return self
+
+    def set_state(self, bodies, exists, cm, dt=1e-3, gam=0.0):
+        b = np.ascontiguousarray(bodies, np.float64)
+        ex = np.ascontiguousarray(exists, np.int32)
+        cmv = np.ascontiguousarray(cm, np.float64)
+        assert b.shape[0] <= self.n_max
+        self.lib.orc_set_state(b.shape[0] - 1, _p(b), _p(ex), _p(cmv), C.c_double(dt), C.c_double(gam))
+
+    def get_state(self):
+        b = np.zeros((self.n_max, 8))
+        ex = np.zeros(self.n_max, np.int32)
+        cm = np.zeros(8)
+        sc = np.zeros(8)
+        lid = self.lib.orc_get_state(_p(b), _p(ex), _p(cm), _p(sc))
+        return b[:lid + 1].copy(), ex[:lid + 1].copy(), cm, sc
+
+    def vector_field(self):
+        b, ex, cm, sc = self.get_state()
+        acc = np.zeros((b.shape[0], 3))
+        cma = np.zeros(3)
+        self.lib.orc_vector_field(_p(acc), _p(cma))
+        return acc, cma
+
+    def events(self):
+        n = self.lib.orc_events(None, 0)
+        out = np.zeros((max(n, 1), 3), np.int32)
+        self.lib.orc_events(_p(out), n)
+        return out[:n]
+
+    def pairs(self):
+        n = self.lib.orc_pairs(None, 0)
+        out = np.zeros((max(n, 1), 2), np.int32)
+        self.lib.orc_pairs(_p(out), n)
+        return out[:n]

@@ -1,0 +1,184 @@
+"""Recipe: compile the reference's own C sources into test oracles.
+
+The reference configures everything through ``#define``s in
+``src/parameters.h`` (every configuration is a recompile, ``src/makefile``).
+For each profile below this script
+
+1. copies ``<reference>/src/*.c|*.h`` into a temporary directory (the
+   reference tree is read-only and ``#include "parameters.h"`` would always
+   pick the copy next to the sources, so an out-of-tree ``-I`` cannot override
+   it),
+2. rewrites the profile's ``#define`` lines of that copy of ``parameters.h``,
+3. compiles with the reference's own flags (``gcc -O2``, ``src/makefile:10``)
+   plus ``-fPIC``, and links
+
+   * ``oracle/_ref/<profile>/libref.so`` = the reference objects (minus
+     ``main.c``) + ``oracle/ref_driver.c``, with ``collision_treatment``
+     wrapped to log the resolution order;
+   * ``oracle/_ref/<profile>/ncorpion`` = the full reference program
+     (``main.c`` included), reading ``./init.txt`` and writing its output
+     files into the working directory (``pth`` = ``"./"``).
+
+Only build outputs are written under ``oracle/_ref/`` (git-ignored); the
+temporary copy is deleted.  The shipped prebuilt ``src/ncorpion`` is never
+copied, read or run.
+
+Usage: ``python oracle/ref_build.py [--src DIR] [profile ...]``
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+DEFAULT_SRC = "/root/reference/src"
+
+COMMON = {
+    "write_to_files_bool": "0",
+    "make_animation_bool": "0",
+    "write_cartesian_bool": "0",
+    "write_elliptic_bool": "0",
+    "write_collisions_bool": "0",
+    "central_mass_bool": "1",
+    "reduce_to_COM_bool": "1",
+    "random_initial_bool": "0",
+    "initial_cartesian_bool": "1",
+    "seed_bool": "1",
+    "one_collision_only_bool": "0",
+    "openGL_bool": "0",
+    "resume_simulation_bool": "0",
+    "viscoelastic_bool": "0",
+    "J2_bool": "0",
+    "central_tides_bool": "0",
+    "inner_fluid_disk_bool": "0",
+    "mutual_bool": "1",
+    "brute_force_bool": "0",
+    "falcON_bool": "0",
+    "standard_tree_bool": "0",
+    "mesh_bool": "0",
+    "elastic_collision_bool": "0",
+    "inelastic_collision_bool": "0",
+    "instant_merger_bool": "0",
+    "fragmentation_bool": "0",
+    "G": "1.",
+    "pert_mass": "0.",
+    "disruption_threshold": "0.1",
+    "high_dumping_threshold": "100.",
+    "pth": '"./"',
+    "softening_parameter": "0.",
+    "t_init": "0.",
+}
+
+BF = dict(COMMON, brute_force_bool="1")
+MESH = dict(COMMON, mesh_bool="1", collision_cube_min="4.4", how_many_neighbours="16.0",
+            sma_min="0.5", sma_max="2.0", inclination_max="0.015")
+
+PROFILES = {
+    # brute-force gravity only (src/physics.c:174-202), softening 0 and 0.5
+    "bf_grav_s0": dict(BF, collision_bool="0", N_max="70000", N_0="2000",
+                       t_end="0.01", time_step="0.001"),
+    "bf_grav_s05": dict(BF, collision_bool="0", softening_parameter="0.5", N_max="70000",
+                        N_0="2000", t_end="0.01", time_step="0.001"),
+    # brute-force gravity + brute-force collisions, instant merger: N=2000, 200 steps
+    "bf_merge": dict(BF, collision_bool="1", instant_merger_bool="1", N_max="4096", N_0="2000",
+                     t_end="0.2", time_step="0.001", output_step="50",
+                     write_to_files_bool="1", write_cartesian_bool="1",
+                     write_collisions_bool="1"),
+    "bf_elastic": dict(BF, collision_bool="1", elastic_collision_bool="1", N_max="4096",
+                       N_0="2000", t_end="0.05", time_step="0.001"),
+    "bf_inelastic": dict(BF, collision_bool="1", inelastic_collision_bool="1",
+                         collision_parameter="1.5", N_max="4096", N_0="2000",
+                         t_end="0.05", time_step="0.001"),
+    # mesh search + mesh gravity, instant merger, small cube for tests
+    "mesh_merge_s": dict(MESH, collision_bool="1", instant_merger_bool="1",
+                         collision_cube_cells="256", N_max="70000", N_0="20000",
+                         t_end="0.005", time_step="0.0005"),
+    "mesh_inelastic_s": dict(MESH, collision_bool="1", inelastic_collision_bool="1",
+                             collision_parameter="1.5", collision_cube_cells="256",
+                             N_max="70000", N_0="20000", t_end="0.005", time_step="0.0005"),
+    "mesh_grav_s": dict(MESH, collision_bool="0", collision_cube_cells="256", N_max="70000",
+                        N_0="20000", t_end="0.005", time_step="0.0005"),
+    # the N = 1,048,576 mesh workload: 1024 cells per side (8.6 GB hash table)
+    "mesh_merge_1m": dict(MESH, collision_bool="1", instant_merger_bool="1",
+                          collision_cube_cells="1024", N_max="1100000", N_0="1048576",
+                          t_end="0.05", time_step="0.0005"),
+}
+
+CFLAGS = ["-O2", "-fPIC", "-w"]
+
+
+def write_params(src_params: str, dst_params: str, overrides: dict) -> None:
+    with open(src_params) as f:
+        lines = f.read().split("\n")
+    seen = set()
+    out = []
+    for line in lines:
+        m = re.match(r"^#define\s+(\w+)\s", line)
+        if m and m.group(1) in overrides:
+            name = m.group(1)
+            out.append(f"#define {name} {overrides[name]}")
+            seen.add(name)
+        else:
+            out.append(line)
+    missing = set(overrides) - seen
+    if missing:
+        raise RuntimeError(f"parameters.h has no #define for {sorted(missing)}")
+    with open(dst_params, "w") as f:
+        f.write("\n".join(out))
+
+
+def build(profile: str, src: str, verbose: bool = False) -> str:
+    ov = PROFILES[profile]
+    dst = os.path.join(OUT, profile)
+    os.makedirs(dst, exist_ok=True)
+    tmp = tempfile.mkdtemp(prefix=f"ncref_{profile}_")
+    try:
+        for p in glob.glob(os.path.join(src, "*.c")) + glob.glob(os.path.join(src, "*.h")):
+            shutil.copy(p, tmp)
+            os.chmod(os.path.join(tmp, os.path.basename(p)), 0o644)
+        write_params(os.path.join(src, "parameters.h"), os.path.join(tmp, "parameters.h"), ov)
+        shutil.copy(os.path.join(HERE, "ref_driver.c"), tmp)
+        units = ["structure", "physics", "collision", "ffm", "rk4", "display", "spring"]
+        objs = []
+        for u in units + ["ref_driver"]:
+            cmd = ["gcc", *CFLAGS, "-c", f"{u}.c", "-o", f"{u}.o"]
+            subprocess.run(cmd, cwd=tmp, check=True)
+            objs.append(f"{u}.o")
+        lib = os.path.join(dst, "libref.so")
+        subprocess.run(["gcc", "-shared", "-o", lib, *objs,
+                        "-Wl,--wrap=collision_treatment", "-lm"], cwd=tmp, check=True)
+        exe = os.path.join(dst, "ncorpion")
+        subprocess.run(["gcc", *CFLAGS, "main.c", *[f"{u}.o" for u in units], "-lm", "-o", exe],
+                       cwd=tmp, check=True)
+        with open(os.path.join(dst, "profile.txt"), "w") as f:
+            for k in sorted(ov):
+                f.write(f"{k} {ov[k]}\n")
+        if verbose:
+            print(f"built {profile} -> {dst}")
+        return dst
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--src", default=DEFAULT_SRC)
+    ap.add_argument("profiles", nargs="*")
+    a = ap.parse_args(argv)
+    if not os.path.isdir(a.src):
+        print(f"reference sources not found at {a.src}; nothing built", file=sys.stderr)
+        return 0
+    for p in a.profiles or sorted(PROFILES):
+        build(p, a.src, verbose=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,57 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); runs the sm_100a library")
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+@pytest.fixture(scope="session")
+def port():
+    import oracle
+    return oracle.Port()
+
+
+@pytest.fixture(scope="session")
+def lib():
+    from ncorpion_b200 import api, build
+    build.build()
+    return api.load()
+
+
+def make_params(**kw):
+    from ncorpion_b200 import api
+    p = api.Params()
+    # reference defaults for the path, as ncgpu_default_params sets them
+    p.G = 1.0
+    p.softening_parameter = 0.0
+    p.central_mass_bool = 1
+    p.mutual_bool = 1
+    p.collision_bool = 0
+    p.brute_force_bool = 1
+    p.mesh_bool = 0
+    p.collision_type = 2
+    p.collision_parameter = 2.0
+    p.one_collision_only_bool = 0
+    p.collision_cube_cells = 1024
+    p.how_many_neighbours = 16.0
+    p.collision_cube_min = 80.0
+    p.switch_to_brute_force = 110
+    p.gravity_mode = 0
+    p.near_theta = 0.5
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
