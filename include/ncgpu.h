@@ -73,7 +73,10 @@ struct ncgpu_params {
       int gravity_mode;              /* NCGPU_GRAVITY_*                          */
       double near_theta;             /* MIXED: tile pairs whose boxes are closer
                                         than near_theta x the larger box diagonal
-                                        are summed in FP64 (default 0.5 if <= 0) */
+                                        are summed in FP64 (default 0.25 if <= 0) */
+      double disruption_threshold;   /* disruption_threshold (dump into the CM)  */
+      double high_dumping_threshold; /* high_dumping_threshold (dump, unbound)   */
+      int reduce_to_COM_bool;        /* reduce_to_COM_bool                       */
 };
 
 /* Fills *p with the reference's default values for the fields above
@@ -126,6 +129,10 @@ int ncgpu_host_unregister(void *ptr);
    denominator of the FP32 gravity kernel. */
 int ncgpu_probe_fp32_peak(double *tflops);
 
+/* Diagnostic: out[i] = x[i]^(1.0/3.0), correctly rounded, as the device
+   merger computes the merged radius (src/physics.c:684). */
+int ncgpu_probe_pow_third(const double *x, double *out, int n);
+
 /* ---- device-resident integrator state ------------------------------------ */
 
 /* Uploads slots 0..largest_id (bodies + exists) and the central mass. */
@@ -142,6 +149,30 @@ int ncgpu_set_timestep(double dt);
 int ncgpu_kick(void);
 /* drift (src/rk4.c:109-127): x += timestep * v, CM too. */
 int ncgpu_drift(void);
+
+/* brute_force (src/collision.c:425-456): every pair i < j in the reference's
+   sweep order, FP64 closest_approach predicate, in-place resolution by
+   collision_treatment (src/physics.c:1043) with the configured type.
+   *n_events receives the number of collision_treatment calls. */
+int ncgpu_collide_brute(int *n_events);
+
+/* The events of the last sweep, in resolution order: (a, b, type) as passed to
+   collision_treatment, and optionally 8 doubles per event for the collision
+   output file: time_until_collision, m_A, m_B, R_A, R_B (A the heavier body,
+   values before the collision), DeltaV and dr.dv (src/physics.c:612-617). */
+int ncgpu_get_events(struct ncgpu_event *events, double *records, int cap, int *n_events);
+
+/* end_of_timestep (src/rk4.c:130-404), hot-path part: bodies inside
+   disruption_threshold merge into the central mass, bodies beyond
+   high_dumping_threshold are removed (then the barycentre is reduced when
+   reduce_to_COM_bool), did_collide is reset when collisions are limited, and
+   the body array is compacted by tidy_up when fewer than 9/10 of
+   largest_id slots are used.  *how_many_moonlets receives the body count. */
+int ncgpu_end_of_timestep(int *how_many_moonlets);
+
+/* One iteration of integration_brute_force_SABA1's loop (src/rk4.c:906-921):
+   kick, brute_force collisions (when collision_bool), drift, end_of_timestep. */
+int ncgpu_step_brute_force(int *how_many_moonlets);
 
 #ifdef __cplusplus
 }

@@ -41,6 +41,9 @@ class Params(C.Structure):
         ("switch_to_brute_force", C.c_int),
         ("gravity_mode", C.c_int),
         ("near_theta", C.c_double),
+        ("disruption_threshold", C.c_double),
+        ("high_dumping_threshold", C.c_double),
+        ("reduce_to_COM_bool", C.c_int),
     ]
 
 
@@ -77,6 +80,11 @@ EXPORTS = {
     "ncgpu_host_unregister": (C.c_int, [P]),
     "ncgpu_probe_fp32_peak": (C.c_int, [P]),
     "ncgpu_last_kernel_ms": (C.c_int, [P]),
+    "ncgpu_collide_brute": (C.c_int, [P]),
+    "ncgpu_probe_pow_third": (C.c_int, [P, P, C.c_int]),
+    "ncgpu_get_events": (C.c_int, [P, P, C.c_int, P]),
+    "ncgpu_end_of_timestep": (C.c_int, [P]),
+    "ncgpu_step_brute_force": (C.c_int, [P]),
     "ncgpu_drift": (C.c_int, []),
 }
 
@@ -196,3 +204,34 @@ def kick():
 
 def drift():
     check(load().ncgpu_drift(), "ncgpu_drift")
+
+
+def end_of_timestep() -> int:
+    n = C.c_int(0)
+    check(load().ncgpu_end_of_timestep(C.byref(n)), "ncgpu_end_of_timestep")
+    return n.value
+
+
+def step_brute_force() -> int:
+    n = C.c_int(0)
+    check(load().ncgpu_step_brute_force(C.byref(n)), "ncgpu_step_brute_force")
+    return n.value
+
+
+def collide_brute() -> int:
+    n = C.c_int(0)
+    check(load().ncgpu_collide_brute(C.byref(n)), "ncgpu_collide_brute")
+    return n.value
+
+
+def events(with_records=False):
+    """(n, 3) int array of (a, b, type) of the last sweep, plus the (n, 8)
+    records when asked."""
+    lib = load()
+    n = C.c_int(0)
+    check(lib.ncgpu_get_events(None, None, 0, C.byref(n)), "ncgpu_get_events")
+    k = n.value
+    ev = np.zeros((max(k, 1), 3), np.int32)
+    rec = np.zeros((max(k, 1), 8))
+    check(lib.ncgpu_get_events(ptr(ev), ptr(rec), k, C.byref(n)), "ncgpu_get_events")
+    return (ev[:k], rec[:k]) if with_records else ev[:k]

@@ -62,7 +62,8 @@ void free_all()
       Ctx &c = ctx();
       void *ptrs[] = {c.x, c.y, c.z, c.vx, c.vy, c.vz, c.m, c.R, c.ex, c.cm, c.cm_acc, c.acc, c.cmterm,
                       c.partial, c.cidx, c.cnt, c.n_dev, c.src64, c.srcR, c.src32, c.srcR32, c.tilebox,
-                      c.keys, c.keys2, c.vals, c.vals2, c.hist, c.red, c.err, c.aos, c.exs};
+                      c.keys, c.keys2, c.vals, c.vals2, c.hist, c.red, c.err, c.aos, c.exs,
+                      c.did, c.dirty, c.dlist, c.free_idx, c.scal, c.hi, c.hj, c.ev, c.evrec};
       for (void *p : ptrs)
             if (p) cudaFree(p);
       if (c.pinned) cudaFreeHost(c.pinned);
@@ -198,7 +199,10 @@ void ncgpu_default_params(struct ncgpu_params *p)
       p->collision_cube_min = 80.;
       p->switch_to_brute_force = 110;
       p->gravity_mode = NCGPU_GRAVITY_EXACT;
-      p->near_theta = 0.5;
+      p->near_theta = 0.25;
+      p->disruption_threshold = 1.8;     // src/parameters.h:150
+      p->high_dumping_threshold = 230.95;  // src/parameters.h:177
+      p->reduce_to_COM_bool = 1;
 }
 
 const char *ncgpu_strerror(int s)
@@ -264,6 +268,12 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
       A(c.red, 4096);
       A(c.err, 1);
       A(c.aos, 8 * N);
+      A(c.did, N); A(c.dirty, N); A(c.dlist, 3 * N); A(c.free_idx, N); A(c.scal, S_COUNT);
+      c.hit_cap = (int)N;
+      A(c.hi, N); A(c.hj, N);
+      c.ev_cap = (int)(2 * N + 1024);
+      A(c.ev, 3 * (size_t)c.ev_cap);
+      A(c.evrec, EVREC * (size_t)c.ev_cap);
 #undef A
       if (cudaMallocHost((void **)&c.pinned, 8 * N * sizeof(double)) != cudaSuccess) {
             free_all();
@@ -283,6 +293,9 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
       }
       cudaMemsetAsync(c.err, 0, sizeof(unsigned), c.s);
       cudaMemsetAsync(c.ex, 0, N * sizeof(int), c.s);
+      cudaMemsetAsync(c.did, 0, N * sizeof(int), c.s);
+      cudaMemsetAsync(c.dirty, 0, N, c.s);
+      cudaMemsetAsync(c.scal, 0, S_COUNT * sizeof(int), c.s);
       double cm0[8] = {0., 0., 0., 0., 0., 0., 1., 1.};
       cudaMemcpyAsync(c.cm, cm0, sizeof cm0, cudaMemcpyHostToDevice, c.s);
       if (cudaStreamSynchronize(c.s) != cudaSuccess) {
@@ -415,8 +428,14 @@ int ncgpu_upload(const struct ncgpu_body *bodies, const int *exists, int largest
             NCG_LAUNCHED();
       }
       NCG_CK(cudaMemcpyAsync(c.cm, cm, 8 * sizeof(double), cudaMemcpyHostToDevice, st));
+      NCG_CK(cudaMemsetAsync(c.did, 0, sizeof(int) * (size_t)c.n_max, st));
+      int sc[S_COUNT] = {0};
+      sc[S_LID] = largest_id;
+      NCG_CK(cudaMemcpyAsync(c.scal, sc, sizeof sc, cudaMemcpyHostToDevice, st));
       NCG_CK(cudaStreamSynchronize(st));
       c.largest_id = largest_id;
+      c.n_events = 0;
+      c.collision_count = 0;
       c.uploaded = 1;
       return NCGPU_OK;
 }

@@ -94,7 +94,40 @@ struct Ctx {
       double *pinned = nullptr;    // pinned host staging (8 * n_max doubles)
       cudaEvent_t kev0 = nullptr, kev1 = nullptr;  // bracket the dominant kernel
       int kev_valid = 0;
+
+      // collision state (device)
+      int *did = nullptr;          // did_collide[] (src/structure.c)
+      unsigned char *dirty = nullptr;  // bodies modified by an event of the current sweep
+      int *dlist = nullptr;        // their ids, in event order
+      int *free_idx = nullptr;     // free_indexes[] stack (src/structure.c:849-878)
+      int *scal = nullptr;         // device scalars, see enum Scal
+      int *hi = nullptr, *hj = nullptr;   // candidate hits (i, j) of a sweep
+      int hit_cap = 0;
+      int *ev = nullptr;           // events: (a, b, type) per collision_treatment call
+      double *evrec = nullptr;     // per-event record for the collision output file
+      int ev_cap = 0;
+      int n_events = 0;            // events of the last sweep (host copy)
+      int collision_count = 0;     // collision_count (host copy)
 };
+
+// Indices into Ctx::scal (device ints).
+enum Scal : int {
+      S_LID = 0,        // largest_id
+      S_NFREE = 1,      // how_many_free
+      S_NHITS = 2,      // hits appended by a sweep
+      S_NEV = 3,        // events of the current sweep
+      S_NDIRTY = 4,     // entries in dlist
+      S_CCOUNT = 5,     // collision_count
+      S_NPAIRS = 6,     // pairs appended (mesh)
+      S_HM = 7,         // how_many_moonlets
+      S_NFLAG = 8,      // bodies flagged for dumping
+      S_NEEDCOM = 9,    // need_to_reduce_COM_bool
+      S_COUNT = 16
+};
+
+// Per-event record fields (doubles) kept for the collision output file
+// (collisionData, src/display.c): t_coll, m_A, m_B, R_A, R_B, DeltaV, dr.dv.
+constexpr int EVREC = 8;
 
 Ctx &ctx();
 int ensure_partial(size_t doubles);

@@ -1,0 +1,204 @@
+// End of timestep on the device-resident state (src/rk4.c:130-404, the
+// parts the hot path needs): dumping into the central mass or beyond the
+// outer threshold, barycentre reduction, did_collide reset and tidy_up.
+// Order-dependent updates (the central mass absorbing dumped bodies, the
+// sequential momentum sums of total_momentum, src/structure.c:1193-1227) run
+// in slot order on one thread per sum, so results match the reference bit for
+// bit; the O(N) scans around them are parallel.
+#include "common.cuh"
+#include "physics.cuh"
+
+namespace ncg {
+
+DevState dev_state();
+int sync_scalars();
+int kick_state();
+int drift_state();
+int collide_brute_state();
+
+namespace {
+
+// flag[j] = 1 (inside disruption_threshold, central mass on), 2 (beyond
+// high_dumping_threshold), 0 otherwise; counts the bodies that stay.
+__global__ void k_eot_flag(const DevState S, int lid, const double *__restrict__ cm, int central, double dis,
+                           double high, int *__restrict__ flag)
+{
+      int j = blockIdx.x * blockDim.x + threadIdx.x;
+      int f = 0;
+      if (j <= lid && S.ex[j]) {
+            double XX = central ? cm[0] : 0., YY = central ? cm[1] : 0., ZZ = central ? cm[2] : 0.;
+            double DX = DSUB(S.x[j], XX), DY = DSUB(S.y[j], YY), DZ = DSUB(S.z[j], ZZ);
+            double r2 = DADD(DADD(DMUL(DX, DX), DMUL(DY, DY)), DMUL(DZ, DZ));
+            if (r2 < DMUL(dis, dis) && central) f = 1;
+            else if (r2 > DMUL(high, high)) f = 2;
+            else atomicAdd(S.scal + S_HM, 1);
+      }
+      if (j <= lid) flag[j] = f;
+      unsigned m = __ballot_sync(0xffffffffu, f != 0);
+      if ((threadIdx.x & 31) == 0 && m) atomicAdd(S.scal + S_NFLAG, __popc(m));
+}
+
+// The flagged bodies, in slot order (list from an order-preserving compaction).
+__global__ void k_eot_dump(const DevState S, const int *__restrict__ list, int n, const int *__restrict__ flag,
+                           double *cm, int mesh_bool)
+{
+      if (threadIdx.x != 0) return;
+      for (int q = 0; q < n; q++) {
+            int j = list[q];
+            if (flag[j] == 1) {
+                  double m = S.m[j];
+                  double X = S.x[j], Y = S.y[j], Z = S.z[j], vX = S.vx[j], vY = S.vy[j], vZ = S.vz[j];
+                  cm[6] = DADD(cm[6], m);
+                  double M = cm[6];
+                  double f = DDIV(DSUB(M, m), M);
+                  for (int d = 0; d < 6; d++) cm[d] = DMUL(cm[d], f);
+                  cm[0] = DADD(cm[0], DDIV(DMUL(m, X), M));
+                  cm[1] = DADD(cm[1], DDIV(DMUL(m, Y), M));
+                  cm[2] = DADD(cm[2], DDIV(DMUL(m, Z), M));
+                  cm[3] = DADD(cm[3], DDIV(DMUL(m, vX), M));
+                  cm[4] = DADD(cm[4], DDIV(DMUL(m, vY), M));
+                  cm[5] = DADD(cm[5], DDIV(DMUL(m, vZ), M));
+                  d_lose(S, j, mesh_bool);
+            } else {
+                  d_lose(S, j, mesh_bool);
+                  S.scal[S_NEEDCOM] = 1;
+            }
+      }
+}
+
+// total_momentum: lane d < 6 sums component d, lane 6 the mass, in slot order.
+__global__ void k_total_momentum(const DevState S, const int *__restrict__ list, int n, const double *__restrict__ cm,
+                                 int central, double *__restrict__ com)
+{
+      __shared__ double M_s;
+      int d = threadIdx.x;
+      double M = central ? cm[6] : 0.;
+      double s = 0.;
+      if (d < 6) s = DMUL(M, central ? cm[d] : 0.);
+      const double *f = d == 0 ? S.x : d == 1 ? S.y : d == 2 ? S.z : d == 3 ? S.vx : d == 4 ? S.vy : S.vz;
+      for (int q = 0; q < n; q++) {
+            int j = list[q];
+            double m = S.m[j];
+            if (d < 6) s = DADD(s, DMUL(m, f[j]));
+            else if (d == 6) M = DADD(M, m);
+      }
+      if (d == 6) M_s = M;
+      __syncthreads();
+      if (d < 6) com[d] = DDIV(s, M_s);
+}
+
+__global__ void k_sub_com(const DevState S, int lid, const double *__restrict__ com, double *cm, int central)
+{
+      int j = blockIdx.x * blockDim.x + threadIdx.x;
+      if (j == 0 && central)
+            for (int d = 0; d < 6; d++) cm[d] = DSUB(cm[d], com[d]);
+      if (j <= lid && S.ex[j]) {
+            S.x[j] = DSUB(S.x[j], com[0]); S.y[j] = DSUB(S.y[j], com[1]); S.z[j] = DSUB(S.z[j], com[2]);
+            S.vx[j] = DSUB(S.vx[j], com[3]); S.vy[j] = DSUB(S.vy[j], com[4]); S.vz[j] = DSUB(S.vz[j], com[5]);
+      }
+}
+
+// tidy_up (src/structure.c:881-911): existing bodies moved to slots 0..n-1
+// in order (gather through a staging copy).
+__global__ void k_tidy_gather(const DevState S, const int *__restrict__ list, int n, double *__restrict__ tmp,
+                              long N)
+{
+      int q = blockIdx.x * blockDim.x + threadIdx.x;
+      if (q >= n) return;
+      int j = list[q];
+      tmp[q] = S.x[j]; tmp[N + q] = S.y[j]; tmp[2 * N + q] = S.z[j];
+      tmp[3 * N + q] = S.vx[j]; tmp[4 * N + q] = S.vy[j]; tmp[5 * N + q] = S.vz[j];
+      tmp[6 * N + q] = S.m[j]; tmp[7 * N + q] = S.R[j];
+}
+
+__global__ void k_tidy_scatter(const DevState S, int n, int lid, const double *__restrict__ tmp, long N)
+{
+      int q = blockIdx.x * blockDim.x + threadIdx.x;
+      if (q < n) {
+            S.x[q] = tmp[q]; S.y[q] = tmp[N + q]; S.z[q] = tmp[2 * N + q];
+            S.vx[q] = tmp[3 * N + q]; S.vy[q] = tmp[4 * N + q]; S.vz[q] = tmp[5 * N + q];
+            S.m[q] = tmp[6 * N + q]; S.R[q] = tmp[7 * N + q];
+      }
+      if (q <= lid) S.ex[q] = q < n ? 1 : 0;
+      if (q == 0) {
+            S.scal[S_LID] = n - 1;
+            S.scal[S_NFREE] = 0;
+      }
+}
+
+}  // namespace
+
+int eot_state(int *hm_out)
+{
+      Ctx &c = ctx();
+      cudaStream_t st = c.s;
+      const ncgpu_params &P = c.P;
+      const int lid = c.largest_id;
+      DevState S = dev_state();
+      int zero[2] = {0, 0};
+      NCG_CK(cudaMemcpyAsync(c.scal + S_HM, zero, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+      const int nb = lid >= 0 ? (lid + 256) / 256 : 1;
+      int *flag = c.exs;
+      k_eot_flag<<<nb, 256, 0, st>>>(S, lid, c.cm, P.central_mass_bool, P.disruption_threshold,
+                                     P.high_dumping_threshold, flag);
+      NCG_LAUNCHED();
+      int h[S_COUNT];
+      NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      const int hm = h[S_HM];
+      if (h[S_NFLAG] > 0) {
+            int nf = 0;
+            NCG_TRY(compact_existing(flag, lid, &nf, st));
+            k_eot_dump<<<1, 32, 0, st>>>(S, c.cidx, nf, flag, c.cm, P.mesh_bool);
+            NCG_LAUNCHED();
+            NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaStreamSynchronize(st));
+      }
+      if (h[S_NEEDCOM] && P.reduce_to_COM_bool) {
+            int n = 0;
+            NCG_TRY(compact_existing(c.ex, lid, &n, st));
+            k_total_momentum<<<1, 32, 0, st>>>(S, c.cidx, n, c.cm, P.central_mass_bool, c.red + 3072);
+            NCG_LAUNCHED();
+            k_sub_com<<<nb, 256, 0, st>>>(S, lid, c.red + 3072, c.cm, P.central_mass_bool);
+            NCG_LAUNCHED();
+            NCG_CK(cudaMemsetAsync(c.scal + S_NEEDCOM, 0, sizeof(int), st));
+      }
+      if (P.collision_bool && (P.one_collision_only_bool || P.collision_type == NCGPU_COLLISION_FRAGMENTATION))
+            NCG_CK(cudaMemsetAsync(c.did, 0, sizeof(int) * (size_t)(lid + 1 > 0 ? lid + 1 : 1), st));
+      if (hm < 9 * lid / 10) {
+            int n = 0;
+            NCG_TRY(compact_existing(c.ex, lid, &n, st));
+            if (n > 0) {
+                  k_tidy_gather<<<(n + 255) / 256, 256, 0, st>>>(S, c.cidx, n, c.aos, c.n_max);
+                  NCG_LAUNCHED();
+            }
+            k_tidy_scatter<<<nb, 256, 0, st>>>(S, n, lid, c.aos, c.n_max);
+            NCG_LAUNCHED();
+      }
+      NCG_TRY(sync_scalars());
+      if (hm_out) *hm_out = hm;
+      return NCGPU_OK;
+}
+
+}  // namespace ncg
+
+using namespace ncg;
+
+extern "C" int ncgpu_end_of_timestep(int *how_many_moonlets)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      return eot_state(how_many_moonlets);
+}
+
+extern "C" int ncgpu_step_brute_force(int *how_many_moonlets)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      NCG_TRY(kick_state());
+      if (c.P.collision_bool) NCG_TRY(collide_brute_state());
+      NCG_TRY(drift_state());
+      return eot_state(how_many_moonlets);
+}

@@ -233,8 +233,10 @@ __global__ void k_morton(BodyView bv, const int *__restrict__ cidx, int n, const
       long s = (long)slot * bv.stride;
       double v[3] = {bv.x[s], bv.y[s], bv.z[s]};
       uint32_t q[3];
+      // one scale for all axes (the largest extent): cells stay cubic, so a
+      // thin disk gives compact tiles instead of slabs
+      const double ext = fmax(fmax(box[3] - box[0], box[4] - box[1]), box[5] - box[2]);
       for (int d = 0; d < 3; d++) {
-            double ext = box[3 + d] - box[d];
             double f = ext > 0. ? (v[d] - box[d]) / ext : 0.;
             int iq = (int)(f * 1023.999);
             q[d] = (uint32_t)min(max(iq, 0), 1023);
@@ -659,7 +661,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       // host side by the caller through near_theta's sibling field; general otherwise
       int sm = soft ? 2 : 0;
       double eps2 = 0.;
-      double theta = P.near_theta > 0. ? P.near_theta : 0.5;
+      double theta = P.near_theta > 0. ? P.near_theta : 0.25;
       dim3 grid(nchunks, ntiles);
       const float4 *s32 = (const float4 *)c.src32;
       NCG_CK(cudaEventRecord(c.kev0, st));

@@ -143,3 +143,59 @@ class Ref:
         out = np.zeros((max(n, 1), 2), np.int32)
         self.lib.orc_pairs(_p(out), n)
         return out[:n]
+
+
+class PortWorld:
+    """The port's stateful world: collisions, brute-force sweep and mesh."""
+
+    def __init__(self, n_max, params):
+        self.lib = C.CDLL(build_port())
+        L = self.lib
+        L.orc_w_init.argtypes = [C.c_int, P]
+        L.orc_w_set.argtypes = [C.c_int, P, P, P, C.c_double, C.c_double]
+        L.orc_w_get.argtypes = [P, P, P]
+        L.orc_w_get.restype = C.c_int
+        L.orc_w_events.argtypes = [P, C.c_int]
+        L.orc_w_events.restype = C.c_int
+        L.orc_w_pairs.argtypes = [P, C.c_long]
+        L.orc_w_pairs.restype = C.c_long
+        L.orc_w_total_neighbours.restype = C.c_long
+        L.orc_w_set_timestep.argtypes = [C.c_double]
+        L.orc_w_set_gam.argtypes = [C.c_double]
+        L.orc_w_three_largest.argtypes = [P]
+        L.orc_cell_index.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]
+        L.orc_cell_index.restype = C.c_long
+        self.n_max = n_max
+        self.params = params
+        if L.orc_w_init(n_max, C.byref(params)) != 0:
+            raise MemoryError("port world init failed")
+
+    def set_state(self, bodies, exists, cm, dt=1e-3, gam=0.0):
+        b = np.ascontiguousarray(bodies, np.float64)
+        ex = np.ascontiguousarray(exists, np.int32)
+        cmv = np.ascontiguousarray(cm, np.float64)
+        self.lib.orc_w_set(b.shape[0] - 1, _p(b), _p(ex), _p(cmv), C.c_double(dt), C.c_double(gam))
+
+    def get_state(self):
+        b = np.zeros((self.n_max, 8))
+        ex = np.zeros(self.n_max, np.int32)
+        cm = np.zeros(8)
+        lid = self.lib.orc_w_get(_p(b), _p(ex), _p(cm))
+        return b[:lid + 1].copy(), ex[:lid + 1].copy(), cm
+
+    def events(self):
+        n = self.lib.orc_w_events(None, 0)
+        out = np.zeros((max(n, 1), 3), np.int32)
+        self.lib.orc_w_events(_p(out), n)
+        return out[:n]
+
+    def pairs(self):
+        n = self.lib.orc_w_pairs(None, 0)
+        out = np.zeros((max(n, 1), 2), np.int32)
+        self.lib.orc_w_pairs(_p(out), n)
+        return out[:n]
+
+    def three_largest(self):
+        idx = np.zeros(3, np.int32)
+        self.lib.orc_w_three_largest(_p(idx))
+        return idx

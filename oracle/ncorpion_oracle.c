@@ -114,3 +114,526 @@ void orc_drift(int lid, body *b, const int *ex, body *cm, double dt, const struc
             cm->z += dt * cm->vz;
       }
 }
+
+/* ======================================================================== */
+/* Collisions and the mesh search.  A single "world" (the reference's global */
+/* state, src/structure.c:62-115) lives in this file.                       */
+/* ======================================================================== */
+
+static struct {
+      struct ncgpu_params P;
+      int n_max, lid;
+      body *b;
+      int *ex, *did, *free_idx;
+      int n_free;
+      body cm;
+      double dt;
+      double approach[6], t_coll;
+      int *ev;
+      int n_ev, ev_cap;
+      int collision_count;
+      /* mesh */
+      double gam;
+      int *pairs;
+      long n_pairs, pair_cap;
+      long total_neighbours;
+      int how_many_small, how_many_big;
+      /* hash: open addressing map cell index -> head/tail of an insertion-ordered list */
+      long *hkey;
+      int *hhead, *htail;
+      long hcap;
+      int *next_in_cell;
+      long *used_slots;
+      long n_used;
+      int three[3];
+} W;
+
+static void push_event(int a, int b, int type)
+{
+      if (W.n_ev >= W.ev_cap) {
+            W.ev_cap = W.ev_cap ? 2 * W.ev_cap : 1024;
+            W.ev = (int *)realloc(W.ev, sizeof(int) * 3 * (size_t)W.ev_cap);
+      }
+      W.ev[3 * W.n_ev] = a;
+      W.ev[3 * W.n_ev + 1] = b;
+      W.ev[3 * W.n_ev + 2] = type;
+      W.n_ev++;
+}
+
+int orc_w_init(int n_max, const struct ncgpu_params *P)
+{
+      free(W.b); free(W.ex); free(W.did); free(W.free_idx); free(W.pairs); free(W.hkey); free(W.hhead);
+      free(W.htail); free(W.next_in_cell); free(W.used_slots); free(W.ev);
+      memset(&W, 0, sizeof W);
+      W.P = *P;
+      W.n_max = n_max;
+      W.b = (body *)calloc((size_t)n_max, sizeof(body));
+      W.ex = (int *)calloc((size_t)n_max, sizeof(int));
+      W.did = (int *)calloc((size_t)n_max, sizeof(int));
+      W.free_idx = (int *)calloc((size_t)n_max, sizeof(int));
+      W.pair_cap = 5L * n_max * (long)P->how_many_neighbours + 64;
+      W.pairs = (int *)malloc(sizeof(int) * 2 * (size_t)W.pair_cap);
+      W.hcap = 1;
+      while (W.hcap < 4L * n_max) W.hcap <<= 1;
+      W.hkey = (long *)malloc(sizeof(long) * (size_t)W.hcap);
+      W.hhead = (int *)malloc(sizeof(int) * (size_t)W.hcap);
+      W.htail = (int *)malloc(sizeof(int) * (size_t)W.hcap);
+      for (long s = 0; s < W.hcap; s++) W.hkey[s] = -1;
+      W.next_in_cell = (int *)malloc(sizeof(int) * (size_t)n_max);
+      W.used_slots = (long *)malloc(sizeof(long) * (size_t)n_max);
+      return (W.b && W.ex && W.did && W.pairs && W.hkey) ? 0 : -1;
+}
+
+void orc_w_set(int lid, const body *b, const int *ex, const body *cm, double dt, double gam)
+{
+      int j;
+      W.lid = lid;
+      memcpy(W.b, b, sizeof(body) * (size_t)(lid + 1));
+      for (j = 0; j < W.n_max; j++) {
+            W.ex[j] = j <= lid ? ex[j] : 0;
+            W.did[j] = 0;
+      }
+      W.cm = *cm;
+      W.dt = dt;
+      W.gam = gam;
+      W.n_free = 0;
+      W.n_ev = 0;
+      W.n_pairs = 0;
+      W.total_neighbours = 0;
+      W.collision_count = 0;
+}
+
+void orc_w_set_timestep(double dt) { W.dt = dt; }
+void orc_w_set_gam(double gam) { W.gam = gam; }
+
+int orc_w_get(body *b, int *ex, body *cm)
+{
+      memcpy(b, W.b, sizeof(body) * (size_t)(W.lid + 1));
+      memcpy(ex, W.ex, sizeof(int) * (size_t)(W.lid + 1));
+      *cm = W.cm;
+      return W.lid;
+}
+
+int orc_w_events(int *out, int cap)
+{
+      int n = W.n_ev < cap ? W.n_ev : cap;
+      if (out && n) memcpy(out, W.ev, sizeof(int) * 3 * (size_t)n);
+      return W.n_ev;
+}
+void orc_w_events_reset(void) { W.n_ev = 0; }
+
+long orc_w_pairs(int *out, long cap)
+{
+      long n = W.n_pairs < cap ? W.n_pairs : cap;
+      if (out && n) memcpy(out, W.pairs, sizeof(int) * 2 * (size_t)n);
+      return W.n_pairs;
+}
+long orc_w_total_neighbours(void) { return W.total_neighbours; }
+int orc_w_collision_count(void) { return W.collision_count; }
+
+/* lose_moonlet (src/structure.c:1077-1087) */
+static void lose(int a)
+{
+      W.free_idx[W.n_free++] = a;
+      W.ex[a] = 0;
+      if (a <= 2 && W.P.mesh_bool) W.n_free--;
+}
+
+/* closest_approach (src/collision.c:63-172); returns 1 and fills W.approach
+   and W.t_coll when a and b collide within the timestep. */
+static int approach(int a, int b)
+{
+      if (!(W.ex[a] && W.ex[b])) return 0;
+      const body *A = W.b + a, *B = W.b + b;
+      double R_a = A->radius, R_b = B->radius;
+      double vx_a = A->vx, vy_a = A->vy, vz_a = A->vz, vx_b = B->vx, vy_b = B->vy, vz_b = B->vz;
+      double xa = A->x, ya = A->y, za = A->z, xb = B->x, yb = B->y, zb = B->z;
+      double dx = xa - xb, dy = ya - yb, dz = za - zb;
+      double dvx = vx_a - vx_b, dvy = vy_a - vy_b, dvz = vz_a - vz_b;
+      double dr_dot_dv = dx * dvx + dy * dvy + dz * dvz;
+      if (dr_dot_dv >= 0.0) return 0;
+      double dr2 = dx * dx + dy * dy + dz * dz;
+      double dv2 = dvx * dvx + dvy * dvy + dvz * dvz;
+      double R = R_a + R_b;
+      double disc = dr_dot_dv * dr_dot_dv + dv2 * (R * R - dr2);
+      if (disc <= 0.0) return 0;
+      double t = -(dr_dot_dv + sqrt(disc)) / dv2;
+      W.t_coll = t;
+      if (t > W.dt) return 0;
+      xa += t * vx_a; ya += t * vy_a; za += t * vz_a;
+      xb += t * vx_b; yb += t * vy_b; zb += t * vz_b;
+      if (A->mass > B->mass) {
+            W.approach[0] = xa; W.approach[1] = ya; W.approach[2] = za;
+            W.approach[3] = xb; W.approach[4] = yb; W.approach[5] = zb;
+      } else {
+            W.approach[0] = xb; W.approach[1] = yb; W.approach[2] = zb;
+            W.approach[3] = xa; W.approach[4] = ya; W.approach[5] = za;
+      }
+      return 1;
+}
+
+/* collision (src/physics.c:545-625): impulse with parameter f */
+static void impulse(int a, int b, double f)
+{
+      body *A = W.b + a, *B = W.b + b;
+      double R = A->radius + B->radius, m_a = A->mass, m_b = B->mass;
+      double vx_a = A->vx, vy_a = A->vy, vz_a = A->vz, vx_b = B->vx, vy_b = B->vy, vz_b = B->vz;
+      double xa = W.approach[0], ya = W.approach[1], za = W.approach[2];
+      double xb = W.approach[3], yb = W.approach[4], zb = W.approach[5];
+      double dr_dot_dv = (xa - xb) * (vx_a - vx_b) + (ya - yb) * (vy_a - vy_b) + (za - zb) * (vz_a - vz_b);
+      double alpha = f * m_a * m_b / ((m_a + m_b) * R * R);
+      double Jx = alpha * dr_dot_dv * (xb - xa), Jy = alpha * dr_dot_dv * (yb - ya), Jz = alpha * dr_dot_dv * (zb - za);
+      vx_a += Jx / m_a; vy_a += Jy / m_a; vz_a += Jz / m_a;
+      vx_b -= Jx / m_b; vy_b -= Jy / m_b; vz_b -= Jz / m_b;
+      double t = W.t_coll;
+      A->x = xa - t * vx_a; A->y = ya - t * vy_a; A->z = za - t * vz_a;
+      A->vx = vx_a; A->vy = vy_a; A->vz = vz_a;
+      B->x = xb - t * vx_b; B->y = yb - t * vy_b; B->z = zb - t * vz_b;
+      B->vx = vx_b; B->vy = vy_b; B->vz = vz_b;
+}
+
+/* merger (src/physics.c:628-708) */
+static void merge(int a, int b)
+{
+      body *A = W.b + a, *B = W.b + b;
+      double m_a = A->mass, m_b = B->mass, R_a = A->radius, R_b = B->radius;
+      double rho_a = 3. * m_a / (4. * M_PI * R_a * R_a * R_a);
+      double rho_b = 3. * m_b / (4. * M_PI * R_b * R_b * R_b);
+      double m = m_a + m_b;
+      double avg = (m_a * rho_a + m_b * rho_b) / m;
+      double vt0 = (m_a * A->vx + m_b * B->vx) / m, vt1 = (m_a * A->vy + m_b * B->vy) / m,
+             vt2 = (m_a * A->vz + m_b * B->vz) / m;
+      double rt0 = (m_a * W.approach[0] + m_b * W.approach[3]) / m;
+      double rt1 = (m_a * W.approach[1] + m_b * W.approach[4]) / m;
+      double rt2 = (m_a * W.approach[2] + m_b * W.approach[5]) / m;
+      double t = W.t_coll;
+      A->x = rt0 - t * vt0; A->y = rt1 - t * vt1; A->z = rt2 - t * vt2;
+      A->vx = vt0; A->vy = vt1; A->vz = vt2;
+      A->mass = m;
+      A->radius = pow(3.0 * m / (4.0 * M_PI * avg), 1.0 / 3.0);
+      lose(b);
+      W.did[a] = W.P.one_collision_only_bool;
+}
+
+/* collision_treatment (src/physics.c:1043-1091), types 0..2 */
+static void treat(int a, int b, int type)
+{
+      double m_a = W.b[a].mass, m_b = W.b[b].mass;
+      int A = m_a > m_b ? a : b, B = m_a > m_b ? b : a;
+      push_event(a, b, type);
+      if (!(W.ex[a] && W.ex[b])) return;
+      if (type == 0 || type == 1) {
+            impulse(A, B, type == 0 ? 2.0 : W.P.collision_parameter);
+            W.did[a] = W.P.one_collision_only_bool;
+            W.did[b] = W.P.one_collision_only_bool;
+            if (W.P.mutual_bool && W.P.mesh_bool) {
+                  W.pairs[2 * W.n_pairs] = a;
+                  W.pairs[2 * W.n_pairs + 1] = b;
+                  W.n_pairs++;
+            }
+      } else if (type == 2) {
+            merge(A, B);
+      }
+      W.collision_count++;
+}
+
+/* brute_force (src/collision.c:425-456) */
+void orc_w_brute_force(void)
+{
+      int i, j, cur = W.lid;
+      for (i = 0; i <= cur; i++) {
+            if (!W.ex[i]) continue;
+            for (j = i + 1; j <= W.lid; j++) {
+                  if (!W.ex[j]) continue;
+                  if (approach(i, j) && !W.did[i] && !W.did[j]) treat(i, j, W.P.collision_type);
+            }
+      }
+}
+
+/* ---- mesh ------------------------------------------------------------- */
+
+/* the linear cell index of hash_table_cell_index (src/collision.c:175-261):
+   -1 outside the cube, else i + j*d + k*d^2 with i = d/2 + 1 + floor(X/gam) */
+long orc_cell_index(double X, double Y, double Z, double gam, int d)
+{
+      double cube = gam * (double)d;
+      if (fabs(X) > cube / 2.0 || fabs(Y) > cube / 2.0 || fabs(Z) > cube / 2.0) return -1;
+      long i = d / 2 + 1 + (int)floor(X / gam);
+      long j = d / 2 + 1 + (int)floor(Y / gam);
+      long k = d / 2 + 1 + (int)floor(Z / gam);
+      return i + j * (long)d + k * (long)d * d;
+}
+
+static long hslot(long key)
+{
+      unsigned long h = (unsigned long)key * 0x9E3779B97F4A7C15ul;
+      long s = (long)(h >> 20) & (W.hcap - 1);
+      while (W.hkey[s] != -1 && W.hkey[s] != key) s = (s + 1) & (W.hcap - 1);
+      return s;
+}
+
+static void hash_clear(void)
+{
+      for (long u = 0; u < W.n_used; u++) W.hkey[W.used_slots[u]] = -1;
+      W.n_used = 0;
+}
+
+/* neighbours (src/collision.c:264-316) fused with the pop loop order: the
+   ids a query pushes (cells l = 0..26, each newest to oldest) are popped in
+   reverse, i.e. cells l = 26..0, each in insertion order.  Fills `out` with
+   that pop order and inserts k into its own cell. */
+static int query_insert(int k, int *out)
+{
+      int d = W.P.collision_cube_cells;
+      long L = orc_cell_index(W.b[k].x, W.b[k].y, W.b[k].z, W.gam, d);
+      if (L < 0) return 0;
+      int n = 0;
+      long dd = (long)d * d;
+      for (int l = 26; l >= 0; l--) {
+            int di = l % 3 - 1, dj = (l / 3) % 3 - 1, dk = l / 9 - 1;
+            long c = L + di + dj * (long)d + dk * dd;
+            long s = hslot(c);
+            if (W.hkey[s] != c) continue;
+            for (int p = W.hhead[s]; p >= 0; p = W.next_in_cell[p])
+                  if (W.ex[p]) out[n++] = p;
+      }
+      long s = hslot(L);
+      if (W.hkey[s] != L) {
+            W.hkey[s] = L;
+            W.hhead[s] = W.htail[s] = k;
+            W.used_slots[W.n_used++] = s;
+      } else {
+            W.next_in_cell[W.htail[s]] = k;
+            W.htail[s] = k;
+      }
+      W.next_in_cell[k] = -1;
+      return n;
+}
+
+static void add_pair(int a, int b)
+{
+      if (W.n_pairs < W.pair_cap) {
+            W.pairs[2 * W.n_pairs] = a;
+            W.pairs[2 * W.n_pairs + 1] = b;
+      }
+      W.n_pairs++;
+}
+
+/* mesh (src/collision.c:324-417) */
+void orc_w_mesh(void)
+{
+      int k, p, cur = W.lid;
+      int *nb = (int *)malloc(sizeof(int) * (size_t)(W.lid + 2));
+      double gam = W.gam;
+      for (k = 0; k <= cur; k++) {
+            if (!W.ex[k]) continue;
+            double R = W.b[k].radius;
+            if (R <= gam) {
+                  W.how_many_small++;
+                  int n = query_insert(k, nb);
+                  for (int q = 0; q < n; q++) {
+                        p = nb[q];
+                        int hit = approach(p, k);
+                        if (!hit || W.did[k] || W.did[p]) {
+                              if (W.P.mutual_bool) add_pair(k, p);
+                        } else {
+                              treat(p, k, W.P.collision_type);
+                        }
+                        W.total_neighbours++;
+                  }
+            } else {
+                  W.how_many_big++;
+                  for (p = 0; p <= W.lid; p++) {
+                        if (!W.ex[p] || p == k) continue;
+                        double Rp = W.b[p].radius;
+                        if (Rp < gam || (Rp >= gam && p > k)) {
+                              int hit = approach(p, k);
+                              if (!hit || W.did[k] || W.did[p]) {
+                                    if (W.P.mutual_bool) add_pair(k, p);
+                              } else {
+                                    treat(p, k, W.P.collision_type);
+                              }
+                        }
+                  }
+            }
+      }
+      free(nb);
+}
+
+/* get_neighbours_mesh (src/physics.c:1094-1118) */
+void orc_w_get_neighbours_mesh(void)
+{
+      int k, cur = W.lid;
+      int *nb = (int *)malloc(sizeof(int) * (size_t)(W.lid + 2));
+      for (k = 0; k <= cur; k++) {
+            if (!W.ex[k]) continue;
+            int n = query_insert(k, nb);
+            for (int q = 0; q < n; q++) {
+                  add_pair(k, nb[q]);
+                  W.total_neighbours++;
+            }
+      }
+      free(nb);
+}
+
+/* end of a mesh pass: hash cleared, counters reset (src/rk4.c:356-364) */
+void orc_w_mesh_reset(void)
+{
+      hash_clear();
+      W.n_pairs = 0;
+      W.total_neighbours = 0;
+      W.how_many_small = W.how_many_big = 0;
+}
+
+/* three_largest_moonlets + three_largest_three_first (src/structure.c:914-1063) */
+void orc_w_three_largest(int *idx)
+{
+      int i = 0, j;
+      double R_0 = 0., R_1 = 0., R_2 = 0., R = 0.;
+      int *t = W.three;
+      t[0] = t[1] = t[2] = -1;
+      for (j = 0; j <= W.lid; j++) {
+            if (!W.ex[j]) continue;
+            if (i == 0) {
+                  R_0 = W.b[j].radius;
+                  t[0] = j;
+            } else if (i == 1) {
+                  R_1 = W.b[j].radius;
+                  if (R_0 > R_1) t[1] = j;
+                  else { t[1] = t[0]; t[0] = j; R = R_1; R_1 = R_0; R_0 = R; }
+            } else if (i == 2) {
+                  R_2 = W.b[j].radius;
+                  if (R_1 >= R_2) t[2] = j;
+                  else if (R_2 > R_1 && R_2 <= R_0) { t[2] = t[1]; t[1] = j; R = R_2; R_2 = R_1; R_1 = R; }
+                  else { t[2] = t[1]; t[1] = t[0]; t[0] = j; R = R_2; R_2 = R_1; R_1 = R_0; R_0 = R; }
+            } else {
+                  R = W.b[j].radius;
+                  if (R > R_0) { t[2] = t[1]; t[1] = t[0]; t[0] = j; R_2 = R_1; R_1 = R_0; R_0 = R; }
+                  else if (R > R_1) { t[2] = t[1]; t[1] = j; R_2 = R_1; R_1 = R; }
+                  else if (R > R_2) { t[2] = j; R_2 = R; }
+            }
+            i++;
+      }
+      idx[0] = t[0]; idx[1] = t[1]; idx[2] = t[2];
+      /* three_largest_three_first */
+      int first = t[0], second = t[1], third = t[2];
+      body buf;
+      if (first != 0) {
+            if (W.ex[0]) { buf = W.b[0]; W.b[0] = W.b[first]; W.b[first] = buf; }
+            else { W.b[0] = W.b[first]; lose(first); W.ex[0] = 1; }
+            if (second == 0) second = first;
+            else if (third == 0) third = first;
+      }
+      if (second != 1) {
+            if (W.ex[1]) { buf = W.b[1]; W.b[1] = W.b[second]; W.b[second] = buf; }
+            else { W.b[1] = W.b[second]; lose(second); W.ex[1] = 1; }
+            if (third == 1) third = second;
+      }
+      if (third != 2) {
+            if (W.ex[2]) { buf = W.b[2]; W.b[2] = W.b[third]; W.b[third] = buf; }
+            else { W.b[2] = W.b[third]; lose(third); W.ex[2] = 1; }
+      }
+}
+
+/* ---- end of timestep -------------------------------------------------- */
+
+static int need_to_reduce_com = 0;
+
+/* total_momentum (src/structure.c:1193-1227) */
+static void total_momentum(double *mom)
+{
+      const int c = W.P.central_mass_bool;
+      double X = c ? W.cm.x : 0., Y = c ? W.cm.y : 0., Z = c ? W.cm.z : 0.;
+      double vX = c ? W.cm.vx : 0., vY = c ? W.cm.vy : 0., vZ = c ? W.cm.vz : 0.;
+      double M = c ? W.cm.mass : 0.;
+      mom[0] = M * X; mom[1] = M * Y; mom[2] = M * Z; mom[3] = M * vX; mom[4] = M * vY; mom[5] = M * vZ;
+      for (int j = 0; j <= W.lid; j++) {
+            if (!W.ex[j]) continue;
+            const body *B = W.b + j;
+            double m = B->mass;
+            M += m;
+            mom[0] += m * B->x; mom[1] += m * B->y; mom[2] += m * B->z;
+            mom[3] += m * B->vx; mom[4] += m * B->vy; mom[5] += m * B->vz;
+      }
+      for (int d = 0; d < 6; d++) mom[d] /= M;
+}
+
+/* tidy_up (src/structure.c:881-911) */
+static void tidy_up(void)
+{
+      int i = 0, j;
+      for (j = 0; j <= W.lid; j++) {
+            if (W.ex[j]) {
+                  if (j > i) W.b[i] = W.b[j];
+                  i++;
+            }
+      }
+      for (j = 0; j <= W.lid; j++) W.ex[j] = j < i ? 1 : 0;
+      W.lid = i - 1;
+      W.n_free = 0;
+}
+
+/* end_of_timestep (src/rk4.c:130-404), the parts on the hot path: dumping to
+   the central mass or beyond the outer threshold, COM reduction, did_collide
+   reset, tidy_up.  Returns how_many_moonlets. */
+int orc_w_end_of_timestep(void)
+{
+      int j, hm = 0;
+      const int c = W.P.central_mass_bool;
+      double XX = c ? W.cm.x : 0., YY = c ? W.cm.y : 0., ZZ = c ? W.cm.z : 0.;
+      for (j = 0; j <= W.lid; j++) {
+            if (!W.ex[j]) continue;
+            body *B = W.b + j;
+            double X = B->x, Y = B->y, Z = B->z, m = B->mass;
+            double DX = X - XX, DY = Y - YY, DZ = Z - ZZ;
+            int losing = 0;
+            if (DX * DX + DY * DY + DZ * DZ < W.P.disruption_threshold * W.P.disruption_threshold && c) {
+                  double vX = B->vx, vY = B->vy, vZ = B->vz;
+                  W.cm.mass += m;
+                  double M = W.cm.mass;
+                  W.cm.x *= (M - m) / M; W.cm.y *= (M - m) / M; W.cm.z *= (M - m) / M;
+                  W.cm.vx *= (M - m) / M; W.cm.vy *= (M - m) / M; W.cm.vz *= (M - m) / M;
+                  W.cm.x += m * X / M; W.cm.y += m * Y / M; W.cm.z += m * Z / M;
+                  W.cm.vx += m * vX / M; W.cm.vy += m * vY / M; W.cm.vz += m * vZ / M;
+                  lose(j);
+                  losing = 1;
+            } else if (DX * DX + DY * DY + DZ * DZ > W.P.high_dumping_threshold * W.P.high_dumping_threshold) {
+                  lose(j);
+                  losing = 1;
+                  need_to_reduce_com = 1;
+            }
+            if (!losing) hm++;
+      }
+      if (need_to_reduce_com && W.P.reduce_to_COM_bool) {
+            double com[6];
+            total_momentum(com);
+            if (c) {
+                  W.cm.x -= com[0]; W.cm.y -= com[1]; W.cm.z -= com[2];
+                  W.cm.vx -= com[3]; W.cm.vy -= com[4]; W.cm.vz -= com[5];
+            }
+            for (j = 0; j <= W.lid; j++) {
+                  if (!W.ex[j]) continue;
+                  W.b[j].x -= com[0]; W.b[j].y -= com[1]; W.b[j].z -= com[2];
+                  W.b[j].vx -= com[3]; W.b[j].vy -= com[4]; W.b[j].vz -= com[5];
+            }
+            need_to_reduce_com = 0;
+      }
+      if (W.P.collision_bool && (W.P.one_collision_only_bool || W.P.collision_type == 3))
+            for (j = 0; j <= W.lid; j++) W.did[j] = 0;
+      if (hm < 9 * W.lid / 10) tidy_up();
+      return hm;
+}
+
+/* the world's kick / drift (src/rk4.c:68-127) */
+void orc_w_kick(void) { orc_kick(W.lid, W.b, W.ex, &W.cm, W.dt, &W.P); }
+void orc_w_drift(void) { orc_drift(W.lid, W.b, W.ex, &W.cm, W.dt, &W.P); }
+
+/* one iteration of integration_brute_force_SABA1's loop (src/rk4.c:906-921):
+   kick, collisions, drift, end_of_timestep */
+int orc_w_step_brute_force(void)
+{
+      orc_w_kick();
+      if (W.P.collision_bool) orc_w_brute_force();
+      orc_w_drift();
+      return orc_w_end_of_timestep();
+}

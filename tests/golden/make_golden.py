@@ -54,6 +54,66 @@ def step_case(profile, n, seed, nsteps, dt, maker):
                 out_bodies=b2, out_exists=ex2, out_cm=cm2, events=ref.events())
 
 
+def digest(a):
+    import hashlib
+    return np.frombuffer(hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest(), np.uint8)
+
+
+def bf_sweep_case(profile, n, seed):
+    """One brute_force() call from a disk whose close pairs collide at once."""
+    b = disks.bf_collide_disk(n, seed=seed)
+    ex = np.ones(n, np.int32)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm, dt=1e-3)
+    ref.lib.orc_events_reset()
+    ref.lib.orc_brute_force()
+    b2, ex2, cm2, sc = ref.get_state()
+    return dict(bodies=b, exists=ex, cm=cm, dt=np.float64(1e-3), events=ref.events(),
+                out_digest=digest(b2), out_exists_digest=digest(ex2), out_cm=cm2)
+
+
+def bf_run_case(profile, n, seed, nsteps):
+    """nsteps iterations of the brute-force integrator loop with collisions."""
+    b = disks.bf_collide_disk(n, seed=seed)
+    ex = np.ones(n, np.int32)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm, dt=1e-3)
+    ref.lib.orc_events_reset()
+    for _ in range(nsteps):
+        ref.lib.orc_step_brute_force()
+    b2, ex2, cm2, sc = ref.get_state()
+    return dict(bodies=b, exists=ex, cm=cm, dt=np.float64(1e-3), nsteps=np.int64(nsteps), events=ref.events(),
+                out_digest=digest(b2), out_exists_digest=digest(ex2), out_cm=cm2,
+                out_largest_id=np.int64(b2.shape[0] - 1))
+
+
+def mesh_case(profile, n, seed, gam, dt):
+    """three_largest + one mesh() call: ordered pairs[], events and state."""
+    rng = np.random.default_rng(seed)
+    b = disks.mesh_disk(n, seed=seed)
+    b[:, 7] = rng.uniform(2e-3, 6e-3, n)
+    b[:, 6] = 4.0 / 3.0 * np.pi * 3.0 * b[:, 7] ** 3
+    ex = np.ones(n, np.int32)
+    ex[rng.choice(n, n // 50, replace=False)] = 0
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm, dt=dt, gam=gam)
+    ref.lib.orc_events_reset()
+    idx = np.zeros(3, np.int32)
+    ref.lib.orc_three_largest(idx.ctypes.data_as(oracle.P))
+    ref.lib.orc_mesh()
+    pairs = ref.pairs()
+    b2, ex2, cm2, sc = ref.get_state()
+    out = dict(bodies=b, exists=ex, cm=cm, dt=np.float64(dt), gam=np.float64(gam), three=idx,
+               events=ref.events(), n_pairs=np.int64(len(pairs)), pairs_digest=digest(pairs),
+               pairs_head=pairs[:256].copy(), total_neighbours=np.int64(ref.lib.orc_total_neighbours()),
+               out_digest=digest(b2), out_exists_digest=digest(ex2))
+    ref.lib.orc_mesh_reset()
+    return out
+
+
 def main():
     out = {}
     out["grav_s05_n512"] = gravity_case("bf_grav_s05", 512, 11, holes=(3, 100, 511))
@@ -61,6 +121,12 @@ def main():
     out["grav_s0_n2"] = gravity_case("bf_grav_s0", 2, 13)
     out["grav_s05_n3"] = gravity_case("bf_grav_s05", 3, 14)
     out["steps_s0_n256"] = step_case("bf_grav_s0", 256, 15, 5, 1e-3, lambda n, s: disks.gravity_disk(n, s))
+    out["bf_sweep_merge"] = bf_sweep_case("bf_merge", 2000, 0)
+    out["bf_sweep_elastic"] = bf_sweep_case("bf_elastic", 2000, 0)
+    out["bf_sweep_inelastic"] = bf_sweep_case("bf_inelastic", 2000, 0)
+    out["bf_run_merge"] = bf_run_case("bf_merge", 2000, 0, 40)
+    out["mesh_merge"] = mesh_case("mesh_merge_s", 6000, 21, 0.03, 5e-4)
+    out["mesh_inelastic"] = mesh_case("mesh_inelastic_s", 6000, 22, 0.03, 5e-4)
     for k, v in out.items():
         np.savez_compressed(os.path.join(HERE, k + ".npz"), **v)
         print("wrote", k)

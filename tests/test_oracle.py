@@ -45,3 +45,76 @@ def test_port_vs_reference_random_holes(port):
         a_ref, c_ref = ref.vector_field()
         a, c = port.vector_field(b, ex, cm, make_params(softening_parameter=0.5))
         assert np.array_equal(a, a_ref) and np.array_equal(c, c_ref)
+
+
+def _digest(a):
+    import hashlib
+    return np.frombuffer(hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest(), np.uint8)
+
+
+@pytest.mark.parametrize("name,ctype", [("bf_sweep_merge", 2), ("bf_sweep_elastic", 0), ("bf_sweep_inelastic", 1)])
+def test_port_brute_force_sweep_matches_golden(name, ctype):
+    g = golden(name)
+    w = oracle.PortWorld(4096, make_params(collision_bool=1, collision_type=ctype, collision_parameter=1.5))
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=float(g["dt"]))
+    w.lib.orc_w_brute_force()
+    b, ex, cm = w.get_state()
+    assert np.array_equal(w.events(), g["events"])
+    assert np.array_equal(_digest(b), g["out_digest"]) and np.array_equal(_digest(ex), g["out_exists_digest"])
+
+
+def test_port_brute_force_run_matches_golden():
+    g = golden("bf_run_merge")
+    w = oracle.PortWorld(4096, make_params(collision_bool=1, collision_type=2))
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=float(g["dt"]))
+    for _ in range(int(g["nsteps"])):
+        w.lib.orc_w_step_brute_force()
+    b, ex, cm = w.get_state()
+    assert np.array_equal(w.events(), g["events"])
+    assert np.array_equal(_digest(b), g["out_digest"])
+    assert np.array_equal(cm, g["out_cm"])
+
+
+@pytest.mark.parametrize("name,ctype", [("mesh_merge", 2), ("mesh_inelastic", 1)])
+def test_port_mesh_matches_golden(name, ctype):
+    g = golden(name)
+    p = make_params(mesh_bool=1, brute_force_bool=0, collision_bool=1, collision_type=ctype,
+                    collision_parameter=1.5, collision_cube_cells=256)
+    w = oracle.PortWorld(70000, p)
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=float(g["dt"]), gam=float(g["gam"]))
+    assert np.array_equal(w.three_largest(), g["three"])
+    w.lib.orc_w_mesh()
+    pairs = w.pairs()
+    assert len(pairs) == int(g["n_pairs"])
+    assert np.array_equal(pairs[:256], g["pairs_head"])
+    assert np.array_equal(_digest(pairs), g["pairs_digest"])
+    assert w.lib.orc_w_total_neighbours() == int(g["total_neighbours"])
+    assert np.array_equal(w.events(), g["events"])
+    b, ex, cm = w.get_state()
+    assert np.array_equal(_digest(b), g["out_digest"]) and np.array_equal(_digest(ex), g["out_exists_digest"])
+
+
+@pytest.mark.skipif(not oracle.ref_available("bf_grav_s0"), reason="reference not compiled here")
+def test_port_end_of_timestep_vs_reference():
+    """Dumping into the central mass, removal beyond the outer threshold with
+    the barycentre reduction, and tidy_up, against the reference's own
+    end_of_timestep (thresholds 0.1 and 100 in that profile)."""
+    import ctypes
+    from ncorpion_b200 import disks
+    b = disks.gravity_disk(1000, seed=9)
+    b[10:40, :3] *= 0.05
+    b[100:250, :3] *= 200.0
+    ex = np.ones(1000, np.int32)
+    ex[500:510] = 0
+    cm = np.array([1e-4, 0, 0, 0, 1e-5, 0, 1.0, 1.0])
+    ref = oracle.Ref("bf_grav_s0")
+    ref.set_state(b, ex, cm)
+    ref.lib.orc_end_of_timestep()
+    rb, rex, rcm, sc = ref.get_state()
+    w = oracle.PortWorld(2048, make_params())
+    w.set_state(b, ex, cm)
+    w.lib.orc_w_end_of_timestep.restype = ctypes.c_int
+    hm = w.lib.orc_w_end_of_timestep()
+    pb, pex, pcm = w.get_state()
+    assert hm == int(sc[2]) == 810
+    assert np.array_equal(rb, pb) and np.array_equal(rex, pex) and np.array_equal(rcm, pcm)
