@@ -170,6 +170,37 @@ int ncgpu_get_events(struct ncgpu_event *events, double *records, int cap, int *
    largest_id slots are used.  *how_many_moonlets receives the body count. */
 int ncgpu_end_of_timestep(int *how_many_moonlets);
 
+/* ---- mesh ------------------------------------------------------------------ */
+
+/* three_largest_moonlets + three_largest_three_first (src/structure.c:914-1063):
+   the three largest bodies (by radius) moved to slots 0, 1, 2; idx receives
+   three_largest_indexes before the moves (may be NULL). */
+int ncgpu_three_largest(int *idx);
+
+/* One pass of the mesh algorithm with mesh size gam (collision_cube =
+   gam * collision_cube_cells).  with_collisions = 1: mesh()
+   (src/collision.c:324-417): bodies with R <= gam, FP64 closest_approach on
+   every popped pair in the reference's pop order, collisions resolved in
+   place; 0: get_neighbours_mesh() (src/physics.c:1094): every body, no test.
+   Outputs: the length of pairs[] (how_many_pairs), the number of events and
+   total_neighbours.  Bodies larger than gam are not supported by the
+   parallel pass (NCGPU_E_UNSUPPORTED). The pass's cell table stays valid for
+   the next kick (mesh gravity) until end_of_timestep or ncgpu_mesh_reset. */
+int ncgpu_mesh(double gam, int with_collisions, int *n_pairs, int *n_events, long *total_neighbours);
+/* pairs[] of the last pass in the reference's order (struct pair). */
+int ncgpu_get_pairs(struct ncgpu_pair *pairs, int cap, int *n_pairs);
+/* Clears the cell table of the last pass (the hash reset of src/rk4.c:361). */
+int ncgpu_mesh_reset(void);
+/* force_naive_bool: 1 switches kicks and collisions to the brute-force path
+   (set by the host when N < switch_to_brute_force, src/rk4.c:388-393). */
+int ncgpu_set_force_naive(int on);
+
+/* One iteration of integration_mesh's loop (src/rk4.c:760-790): three largest
+   to slots 0-2, mesh() (or brute force when force_naive), drift, kick with
+   mesh gravity, end_of_timestep.  The host owns gamma and updates it from
+   total_neighbours with the reference's formula (src/rk4.c:367-372). */
+int ncgpu_step_mesh(double gam, int *how_many_moonlets, long *total_neighbours);
+
 /* One iteration of integration_brute_force_SABA1's loop (src/rk4.c:906-921):
    kick, brute_force collisions (when collision_bool), drift, end_of_timestep. */
 int ncgpu_step_brute_force(int *how_many_moonlets);

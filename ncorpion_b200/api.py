@@ -85,6 +85,12 @@ EXPORTS = {
     "ncgpu_get_events": (C.c_int, [P, P, C.c_int, P]),
     "ncgpu_end_of_timestep": (C.c_int, [P]),
     "ncgpu_step_brute_force": (C.c_int, [P]),
+    "ncgpu_three_largest": (C.c_int, [P]),
+    "ncgpu_mesh": (C.c_int, [C.c_double, C.c_int, P, P, P]),
+    "ncgpu_get_pairs": (C.c_int, [P, C.c_int, P]),
+    "ncgpu_mesh_reset": (C.c_int, []),
+    "ncgpu_set_force_naive": (C.c_int, [C.c_int]),
+    "ncgpu_step_mesh": (C.c_int, [C.c_double, P, P]),
     "ncgpu_drift": (C.c_int, []),
 }
 
@@ -235,3 +241,42 @@ def events(with_records=False):
     rec = np.zeros((max(k, 1), 8))
     check(lib.ncgpu_get_events(ptr(ev), ptr(rec), k, C.byref(n)), "ncgpu_get_events")
     return (ev[:k], rec[:k]) if with_records else ev[:k]
+
+
+def three_largest():
+    idx = np.zeros(3, np.int32)
+    check(load().ncgpu_three_largest(ptr(idx)), "ncgpu_three_largest")
+    return idx
+
+
+def mesh(gam: float, with_collisions: bool = True):
+    """(n_pairs, n_events, total_neighbours) of one mesh pass."""
+    np_, ne, tn = C.c_int(0), C.c_int(0), C.c_long(0)
+    check(load().ncgpu_mesh(float(gam), int(with_collisions), C.byref(np_), C.byref(ne), C.byref(tn)), "ncgpu_mesh")
+    return np_.value, ne.value, tn.value
+
+
+def pairs():
+    lib = load()
+    n = C.c_int(0)
+    check(lib.ncgpu_get_pairs(None, 0, C.byref(n)), "ncgpu_get_pairs")
+    out = np.zeros((max(n.value, 1), 2), np.int32)
+    check(lib.ncgpu_get_pairs(ptr(out), n.value, C.byref(n)), "ncgpu_get_pairs")
+    return out[:n.value]
+
+
+def mesh_reset():
+    check(load().ncgpu_mesh_reset(), "ncgpu_mesh_reset")
+
+
+def step_mesh(gam: float):
+    hm, tn = C.c_int(0), C.c_long(0)
+    check(load().ncgpu_step_mesh(float(gam), C.byref(hm), C.byref(tn)), "ncgpu_step_mesh")
+    return hm.value, tn.value
+
+
+def update_gamma(gam, total_neighbours, how_many_moonlets, how_many_neighbours, gam_min):
+    """Mesh-size update of src/rk4.c:367-372 (host side, libm pow)."""
+    average = 2.0 * float(total_neighbours) / float(how_many_moonlets)
+    gam = gam * (how_many_neighbours / average) ** (1.0 / 3.0)
+    return gam_min if gam < gam_min else gam

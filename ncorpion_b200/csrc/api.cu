@@ -57,9 +57,14 @@ int dalloc(Tp **p, size_t count)
       return NCGPU_OK;
 }
 
+}  // namespace
+void mesh_free();
+namespace {
+
 void free_all()
 {
       Ctx &c = ctx();
+      mesh_free();
       void *ptrs[] = {c.x, c.y, c.z, c.vx, c.vy, c.vz, c.m, c.R, c.ex, c.cm, c.cm_acc, c.acc, c.cmterm,
                       c.partial, c.cidx, c.cnt, c.n_dev, c.src64, c.srcR, c.src32, c.srcR32, c.tilebox,
                       c.keys, c.keys2, c.vals, c.vals2, c.hist, c.red, c.err, c.aos, c.exs,
@@ -149,13 +154,18 @@ int state_cm_host(double *cm8)
       return NCGPU_OK;
 }
 
+int mesh_gravity_state(const double *cm8);
+
 int kick_state()
 {
       Ctx &c = ctx();
       double cm8[8];
       NCG_TRY(state_cm_host(cm8));
       const int nslots = c.largest_id + 1;
-      NCG_TRY(gravity_eval(state_view(), c.largest_id, cm8, c.acc, c.n_max, c.cm_acc, c.P.gravity_mode, c.s));
+      if (c.P.mesh_bool && !c.force_naive)
+            NCG_TRY(mesh_gravity_state(cm8));
+      else
+            NCG_TRY(gravity_eval(state_view(), c.largest_id, cm8, c.acc, c.n_max, c.cm_acc, c.P.gravity_mode, c.s));
       int nb = nslots > 0 ? (nslots + 255) / 256 : 1;
       k_kick<<<nb, 256, 0, c.s>>>(c.ex, nslots, c.dt, c.acc, c.acc + c.n_max, c.acc + 2 * (size_t)c.n_max, c.vx,
                                   c.vy, c.vz, c.cm, c.cm_acc, c.P.central_mass_bool);
@@ -247,7 +257,7 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
       A(c.acc, 3 * N);
       A(c.cmterm, 3 * N);
       A(c.cidx, N);
-      A(c.cnt, (N + 1023) / 1024 + 1);
+      A(c.cnt, (std::max(N, (size_t)1 << 20) + 1023) / 1024 + 2);
       A(c.n_dev, 8);
       {
             double *p = nullptr;
@@ -262,15 +272,18 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
       }
       A(c.srcR32, npad);
       A(c.tilebox, 6 * (npad / 128));
-      A(c.keys, N); A(c.keys2, N); A(c.vals, N); A(c.vals2, N);
-      c.hist_cap = 256 * ((N + 2047) / 2048);
+      // sort scratch: at least 2^20 keys, so collision-hit lists of dense
+      // clusters sort even when n_max is small
+      const size_t NS = std::max(N, (size_t)1 << 20);
+      A(c.keys, NS); A(c.keys2, NS); A(c.vals, NS); A(c.vals2, NS);
+      c.hist_cap = 256 * ((NS + 2047) / 2048);
       A(c.hist, c.hist_cap);
       A(c.red, 4096);
       A(c.err, 1);
       A(c.aos, 8 * N);
       A(c.did, N); A(c.dirty, N); A(c.dlist, 3 * N); A(c.free_idx, N); A(c.scal, S_COUNT);
-      c.hit_cap = (int)N;
-      A(c.hi, N); A(c.hj, N);
+      c.hit_cap = (int)NS;
+      A(c.hi, NS); A(c.hj, NS);
       c.ev_cap = (int)(2 * N + 1024);
       A(c.ev, 3 * (size_t)c.ev_cap);
       A(c.evrec, EVREC * (size_t)c.ev_cap);
@@ -473,6 +486,13 @@ int ncgpu_kick(void)
       if (!g_ctx.inited || !g_ctx.uploaded) return NCGPU_E_STATE;
       NCG_TRY(kick_state());
       return check_err_word();
+}
+
+int ncgpu_set_force_naive(int on)
+{
+      if (!g_ctx.inited) return NCGPU_E_STATE;
+      g_ctx.force_naive = on ? 1 : 0;
+      return NCGPU_OK;
 }
 
 int ncgpu_drift(void)

@@ -272,7 +272,8 @@ int collide_brute_state()
       NCG_CK(cudaMemcpyAsync(&nh, c.scal + S_NHITS, sizeof(int), cudaMemcpyDeviceToHost, st));
       NCG_CK(cudaStreamSynchronize(st));
       if (nh > c.hit_cap) return NCGPU_E_CAPACITY;
-      int *si = c.dlist + c.n_max, *sj = c.dlist + 2 * (size_t)c.n_max;  // sorted hits
+      int *si = c.hi + c.hit_cap / 2, *sj = c.hj + c.hit_cap / 2;  // sorted hits (upper halves)
+      if (nh > c.hit_cap / 2) return NCGPU_E_CAPACITY;
       NCG_TRY(sort_hits(nh, si, sj, lid, st));
       EvArgs E{lid, c.dt, c.P.collision_type, c.P.collision_parameter, c.P.one_collision_only_bool,
                c.P.mesh_bool, c.ev_cap, c.n_max};

@@ -108,6 +108,28 @@ struct Ctx {
       int ev_cap = 0;
       int n_events = 0;            // events of the last sweep (host copy)
       int collision_count = 0;     // collision_count (host copy)
+
+      // mesh search (allocated on the first mesh pass)
+      int *cstart = nullptr;       // dense cell -> first sorted position (-1 empty)
+      size_t cell_cap = 0;
+      int mesh_d = 0;
+      uint32_t *mkeys = nullptr;   // cell index per sorted body (n + 1, sentinel)
+      int *mvals = nullptr;        // body index per sorted position
+      int *ckey = nullptr;         // insertion cell per slot (-1: not inserted)
+      int *mcnt = nullptr, *moff = nullptr;
+      int *cand_k = nullptr, *cand_p = nullptr;  // candidates in pop order
+      unsigned char *cflag = nullptr;
+      int *cpos = nullptr;         // output positions of kept candidates
+      int *msums = nullptr;        // scan scratch for candidate-sized scans
+      long pair_cap = 0;
+      int *occ = nullptr;
+      int occ_cap = 0;
+      int mesh_valid = 0;          // cell table populated by the last pass
+      int mesh_n = 0;              // sorted entries of the last pass (largest_id + 1)
+      int n_cand = 0, n_pairs = 0;
+      long total_neighbours = 0;
+      int how_many_small = 0, how_many_big = 0;
+      int force_naive = 0;         // force_naive_bool: brute force below switch_to_brute_force
 };
 
 // Indices into Ctx::scal (device ints).
@@ -122,6 +144,9 @@ enum Scal : int {
       S_HM = 7,         // how_many_moonlets
       S_NFLAG = 8,      // bodies flagged for dumping
       S_NEEDCOM = 9,    // need_to_reduce_COM_bool
+      S_NBIG = 10,      // bodies larger than the mesh size
+      S_NDROP = 11,     // candidates dropped by removals
+      S_NINS = 12,      // bodies inserted in the cell table
       S_COUNT = 16
 };
 
@@ -142,6 +167,9 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cm_host8, dou
 // LSD radix sort of (key, value) pairs, stable; keys use `bits` low bits.
 // Result ends in (keys, vals) buffers passed in (ping-pong through ctx scratch).
 int radix_sort_pairs(uint32_t *keys, int *vals, int n, int bits, cudaStream_t st);
+
+// Exclusive prefix sum; out has n + 1 entries (out[n] = total).
+int scan_exclusive(const int *in, int *out, int n, int *sums, cudaStream_t st);
 
 // Stream compaction of existing slots 0..largest_id into ctx().cidx (ascending).
 // Returns the count through *n_host (synchronises).

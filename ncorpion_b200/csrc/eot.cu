@@ -15,6 +15,9 @@ int sync_scalars();
 int kick_state();
 int drift_state();
 int collide_brute_state();
+int mesh_reset_state();
+int mesh_pass(double gam, int test);
+int three_largest_state(int *idx);
 
 namespace {
 
@@ -163,6 +166,7 @@ int eot_state(int *hm_out)
             NCG_LAUNCHED();
             NCG_CK(cudaMemsetAsync(c.scal + S_NEEDCOM, 0, sizeof(int), st));
       }
+      if (P.mesh_bool) NCG_TRY(mesh_reset_state());  // hash table cleared (src/rk4.c:356-364)
       if (P.collision_bool && (P.one_collision_only_bool || P.collision_type == NCGPU_COLLISION_FRAGMENTATION))
             NCG_CK(cudaMemsetAsync(c.did, 0, sizeof(int) * (size_t)(lid + 1 > 0 ? lid + 1 : 1), st));
       if (hm < 9 * lid / 10) {
@@ -200,5 +204,34 @@ extern "C" int ncgpu_step_brute_force(int *how_many_moonlets)
       NCG_TRY(kick_state());
       if (c.P.collision_bool) NCG_TRY(collide_brute_state());
       NCG_TRY(drift_state());
+      return eot_state(how_many_moonlets);
+}
+
+// One iteration of integration_mesh's loop (src/rk4.c:760-790) with mesh size
+// gam; *total_neighbours is the pass's count for the host's gamma update.
+extern "C" int ncgpu_step_mesh(double gam, int *how_many_moonlets, long *total_neighbours)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      if (!(gam > 0.)) return NCGPU_E_ARG;
+      long tn = 0;
+      if (c.P.collision_bool) {
+            if (c.force_naive) {
+                  NCG_TRY(collide_brute_state());
+            } else {
+                  NCG_TRY(three_largest_state(nullptr));
+                  NCG_TRY(mesh_pass(gam, 1));
+                  tn = c.total_neighbours;
+            }
+      }
+      NCG_TRY(drift_state());
+      if (!c.P.collision_bool && !c.force_naive) {
+            NCG_TRY(three_largest_state(nullptr));
+            NCG_TRY(mesh_pass(gam, 0));
+            tn = c.total_neighbours;
+      }
+      NCG_TRY(kick_state());
+      if (total_neighbours) *total_neighbours = tn;
       return eot_state(how_many_moonlets);
 }

@@ -1,0 +1,514 @@
+// Mesh collision search: the device replacement of mesh() and
+// get_neighbours_mesh() (src/collision.c:175-417, src/physics.c:1094-1118).
+//
+// The reference walks bodies k = 0..largest_id; a small body (R <= gam) first
+// collects every body already in the 27 cells around its own cell, then
+// inserts itself into its cell; the collected ids are popped in the order
+// cell slot l = 26..0, ascending index within a cell (the LIFO of
+// src/structure.c:712-841 reversed), each popped pair is tested by
+// closest_approach in FP64 and either resolved on the spot or appended to
+// pairs[].  Cells are identified by the reference's linear index
+// i + j*d + k*d^2 (d = collision_cube_cells, i = d/2 + 1 + floor(X/gam)), so
+// the neighbour aliasing of that index at the cube's x and y edges is kept.
+//
+// On the GPU:
+//   k_mesh_keys     cell index per inserted body (-1 outside the cube)
+//   radix sort      (cell, index) pairs; a dense cell -> first-position table
+//                   (the analogue of the reference's (d+2)^3 hash table) gives
+//                   O(1) access to a cell's bodies, in ascending index order
+//   k_mesh_count    candidates per body = bodies of lower index in its 27 cells
+//   scan            positions of every body's list in the global pop order
+//   k_mesh_write    candidates (k, p) written in pop order; the FP64 predicate
+//                   of the entry state marks hits
+//   k_mesh_events   one CTA replays the hits in order (mesh_events.cu)
+#include "common.cuh"
+#include "physics.cuh"
+
+namespace ncg {
+
+namespace {
+
+constexpr unsigned NOKEY = 0xffffffffu;
+
+// linear cell index of a body, -1 outside the cube (src/collision.c:192-202)
+__device__ __forceinline__ long long d_cell(double X, double Y, double Z, double gam, double half, int d)
+{
+      if (fabs(X) > half || fabs(Y) > half || fabs(Z) > half) return -1;
+      long long i = d / 2 + 1 + (int)floor(DDIV(X, gam));
+      long long j = d / 2 + 1 + (int)floor(DDIV(Y, gam));
+      long long k = d / 2 + 1 + (int)floor(DDIV(Z, gam));
+      return i + j * (long long)d + k * (long long)d * d;
+}
+
+// neighbour offset of cell slot l (l = 0 is (-1,-1,-1), x fastest)
+__device__ __forceinline__ long long d_noff(int l, int d)
+{
+      int di = l % 3 - 1, dj = (l / 3) % 3 - 1, dk = l / 9 - 1;
+      return di + dj * (long long)d + dk * (long long)d * d;
+}
+
+__global__ void k_mesh_keys(DevState S, int lid, double gam, double half, int d, int all_mode,
+                            uint32_t *__restrict__ keys, int *__restrict__ vals, int *__restrict__ ckey,
+                            int *__restrict__ nbig)
+{
+      int k = blockIdx.x * blockDim.x + threadIdx.x;
+      if (k > lid) return;
+      long long L = -1;
+      if (S.ex[k]) {
+            if (all_mode || S.R[k] <= gam) L = d_cell(S.x[k], S.y[k], S.z[k], gam, half, d);
+            else atomicAdd(nbig, 1);
+      }
+      ckey[k] = (int)L;
+      keys[k] = L >= 0 ? (uint32_t)L : NOKEY;
+      vals[k] = k;
+}
+
+__global__ void k_cell_heads(const uint32_t *__restrict__ keys, int n, int *__restrict__ cstart,
+                             int *__restrict__ n_ins)
+{
+      int q = blockIdx.x * blockDim.x + threadIdx.x;
+      if (q >= n) return;
+      uint32_t key = keys[q];
+      if (key == NOKEY) {
+            if (q == 0 || keys[q - 1] != NOKEY) *n_ins = q;
+            return;
+      }
+      if (q == 0 || keys[q - 1] != key) cstart[key] = q;
+      if (q == n - 1) *n_ins = n;
+}
+
+__global__ void k_cell_clear(const uint32_t *__restrict__ keys, int n, int *__restrict__ cstart)
+{
+      int q = blockIdx.x * blockDim.x + threadIdx.x;
+      if (q >= n) return;
+      uint32_t key = keys[q];
+      if (key != NOKEY && (q == 0 || keys[q - 1] != key)) cstart[key] = -1;
+}
+
+// number of candidates of body k: bodies of lower index in its 27 cells
+__global__ void k_mesh_count(const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
+                             const int *__restrict__ vals, const int *__restrict__ cstart, int lid, int d,
+                             long long cap, int *__restrict__ cnt)
+{
+      int k = blockIdx.x * blockDim.x + threadIdx.x;
+      if (k > lid) return;
+      int L = ckey[k];
+      int c = 0;
+      if (L >= 0) {
+            for (int l = 26; l >= 0; --l) {
+                  long long cell = L + d_noff(l, d);
+                  if (cell < 0 || cell >= cap) continue;  // i = 0 after rounding at -cube/2
+                  int s = cstart[cell];
+                  if (s < 0) continue;
+                  for (int q = s; keys[q] == (uint32_t)cell; ++q) {
+                        if (vals[q] >= k) break;
+                        c++;
+                  }
+            }
+      }
+      cnt[k] = c;
+}
+
+// candidates of body k in pop order; hit flag from the entry-state predicate
+__global__ void k_mesh_write(DevState S, const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
+                             const int *__restrict__ vals, const int *__restrict__ cstart,
+                             const int *__restrict__ off, int lid, int d, long long cap, double dt, int test,
+                             int *__restrict__ ck, int *__restrict__ cp, unsigned char *__restrict__ cflag,
+                             int *__restrict__ hitpos, int hit_cap, int *__restrict__ nhits, unsigned *err)
+{
+      int k = blockIdx.x * blockDim.x + threadIdx.x;
+      if (k > lid) return;
+      int L = ckey[k];
+      if (L < 0) return;
+      int pos = off[k];
+      const bool dk = test && S.did[k];
+      for (int l = 26; l >= 0; --l) {
+            long long cell = L + d_noff(l, d);
+            if (cell < 0 || cell >= cap) continue;
+            int s = cstart[cell];
+            if (s < 0) continue;
+            for (int q = s; keys[q] == (uint32_t)cell; ++q) {
+                  int p = vals[q];
+                  if (p >= k) break;
+                  ck[pos] = k;
+                  cp[pos] = p;
+                  unsigned char f = 0;
+                  if (test && !dk && !S.did[p] && d_approach(S, p, k, dt, nullptr)) {
+                        f = 1;
+                        int h = atomicAdd(nhits, 1);
+                        if (h < hit_cap) hitpos[h] = pos;
+                        else atomicOr(err, ERR_CAPACITY);
+                  }
+                  cflag[pos] = f;
+                  ++pos;
+            }
+      }
+}
+
+}  // namespace
+
+namespace {
+
+// cflag bits
+constexpr unsigned char F_HIT = 1, F_DROP = 2, F_MERGED = 4, F_SWAP = 8;
+constexpr int MEV = 1024;       // threads of the event kernel
+
+struct MeshEvArgs {
+      int lid0, d, type, one_only, mesh_bool, ev_cap, dcap, occ_cap, nsorted;
+      long long cell_cap;
+      double dt, f_inelastic;
+};
+
+// collision_treatment(p, k, type) at candidate position q (src/physics.c:1043)
+__device__ void d_mesh_treat(const DevState &S, int p, int k, int q, const MeshEvArgs &E, int *ev, double *evrec,
+                             unsigned char *cflag, unsigned *err, int *A_out, int *B_out)
+{
+      Approach ap;
+      d_approach(S, p, k, E.dt, &ap);
+      double m_a = S.m[p], m_b = S.m[k];
+      int A = m_a > m_b ? p : k, B = m_a > m_b ? k : p;
+      int ne = S.scal[S_NEV];
+      double *rec = nullptr;
+      if (ne < E.ev_cap) {
+            ev[3 * ne] = p;
+            ev[3 * ne + 1] = k;
+            ev[3 * ne + 2] = E.type;
+            rec = evrec + (size_t)EVREC * ne;
+            rec[0] = ap.t; rec[1] = S.m[A]; rec[2] = S.m[B]; rec[3] = S.R[A]; rec[4] = S.R[B];
+      } else {
+            atomicOr(err, ERR_CAPACITY);
+      }
+      S.scal[S_NEV] = ne + 1;
+      if (E.type == NCGPU_COLLISION_ELASTIC || E.type == NCGPU_COLLISION_INELASTIC) {
+            d_impulse(S, A, B, E.type == NCGPU_COLLISION_ELASTIC ? 2.0 : E.f_inelastic, ap, rec);
+            S.did[p] = E.one_only;
+            S.did[k] = E.one_only;
+            cflag[q] |= F_SWAP;   // pairs[] gets (p, k) at this position
+      } else if (E.type == NCGPU_COLLISION_MERGER) {
+            d_merge(S, A, B, ap, E.one_only, E.mesh_bool, rec);
+            cflag[q] |= F_MERGED;  // no pair appended
+      } else {
+            atomicOr(err, ERR_INTERNAL);
+      }
+      S.scal[S_CCOUNT] += 1;
+      *A_out = A;
+      *B_out = B;
+}
+
+// One CTA.  hitpos: entry-state hits sorted by position.  Modified bodies get
+// their later occurrences collected into a pool (own remaining pops, and the
+// lists of later bodies in the 27 cells around them); those occurrences are
+// re-tested against the current state after every event, the untouched hits
+// are taken as they are, and the smallest position wins.
+__global__ void __launch_bounds__(MEV) k_mesh_events(DevState S, const int *__restrict__ ck, const int *__restrict__ cp,
+                                                     unsigned char *cflag, const int *__restrict__ off,
+                                                     const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
+                                                     const int *__restrict__ vals, const int *__restrict__ cstart,
+                                                     const int *__restrict__ hitpos, int nh, MeshEvArgs E, int *ev,
+                                                     double *evrec, unsigned char *dirty, int *occ, int *ndrop,
+                                                     unsigned *err)
+{
+      __shared__ int best, hp_s, nocc, newb[2], newn, kq_s, q_s;
+      if (threadIdx.x == 0) {
+            hp_s = 0;
+            nocc = 0;
+      }
+      __syncthreads();
+      int cur = -1;
+      for (int iter = 0;; ++iter) {
+            if (iter > (1 << 26)) {
+                  if (threadIdx.x == 0) atomicOr(err, ERR_TIMEOUT);
+                  break;
+            }
+            if (threadIdx.x == 0) {
+                  int hp = hp_s;
+                  while (hp < nh) {
+                        int q = hitpos[hp];
+                        if (q > cur && !dirty[ck[q]] && !dirty[cp[q]] && !(cflag[q] & F_DROP)) break;
+                        hp++;
+                  }
+                  hp_s = hp;
+                  best = hp < nh ? hitpos[hp] : 0x7fffffff;
+            }
+            __syncthreads();
+            const int no = nocc;
+            for (int t = threadIdx.x; t < no; t += MEV) {
+                  int q = occ[t];
+                  if (q <= cur || q >= best || (cflag[q] & (F_DROP | F_MERGED | F_SWAP))) continue;
+                  int k = ck[q], p = cp[q];
+                  if (S.did[k] || S.did[p]) continue;
+                  if (d_approach(S, p, k, E.dt, nullptr)) atomicMin(&best, q);
+            }
+            __syncthreads();
+            const int q = best;
+            if (q == 0x7fffffff) break;
+            if (threadIdx.x == 0) {
+                  int A, B;
+                  int k = ck[q], p = cp[q];
+                  d_mesh_treat(S, p, k, q, E, ev, evrec, cflag, err, &A, &B);
+                  int nn = 0;
+                  if (!dirty[A]) { dirty[A] = 1; newb[nn++] = A; }
+                  if (!dirty[B]) { dirty[B] = 1; newb[nn++] = B; }
+                  newn = nn;
+                  kq_s = k;
+                  q_s = q;
+            }
+            __syncthreads();
+            // occurrences of the newly modified bodies after position q
+            const int kq = kq_s, nn = newn;
+            for (int w = 0; w < nn; ++w) {
+                  const int x = newb[w];
+                  const bool alive = S.ex[x];
+                  // remaining pops of the querying body itself
+                  if (x == kq && alive)
+                        for (int r = q_s + 1 + threadIdx.x; r < off[kq + 1]; r += MEV) {
+                              int o = atomicAdd(&nocc, 1);
+                              if (o < E.occ_cap) occ[o] = r;
+                              else atomicOr(err, ERR_CAPACITY);
+                        }
+                  // x in the lists of later bodies of its 27 cells
+                  const int Lx = ckey[x];
+                  if (Lx < 0) continue;
+                  for (int l = threadIdx.x >> 5; l < 27; l += MEV / 32) {
+                        long long cell = Lx + d_noff(l, E.d);
+                        if (cell < 0 || cell >= E.cell_cap) continue;
+                        int s = cstart[cell];
+                        if (s < 0) continue;
+                        for (int qq = s + (threadIdx.x & 31); qq < E.nsorted && keys[qq] == (uint32_t)cell; qq += 32) {
+                              int kk = vals[qq];
+                              if (kk <= kq) continue;
+                              for (int r = off[kk]; r < off[kk + 1]; ++r) {
+                                    if (cp[r] != x) continue;
+                                    if (alive) {
+                                          int o = atomicAdd(&nocc, 1);
+                                          if (o < E.occ_cap) occ[o] = r;
+                                          else atomicOr(err, ERR_CAPACITY);
+                                    } else {
+                                          cflag[r] |= F_DROP;  // removed before kk's query: never pushed
+                                          atomicAdd(ndrop, 1);
+                                    }
+                              }
+                        }
+                  }
+                  // a removed body does not query its own cells either
+                  if (!alive && x > kq)
+                        for (int r = off[x] + threadIdx.x; r < off[x + 1]; r += MEV) {
+                              cflag[r] |= F_DROP;
+                              atomicAdd(ndrop, 1);
+                        }
+            }
+            cur = q;
+            __syncthreads();
+      }
+}
+
+// pairs[] = candidates without dropped / merged entries, swapped ones as (p, k)
+__global__ void k_pairs_keep(const unsigned char *__restrict__ cflag, int n, int *__restrict__ keep)
+{
+      int q = blockIdx.x * blockDim.x + threadIdx.x;
+      if (q < n) keep[q] = (cflag[q] & (F_DROP | F_MERGED)) ? 0 : 1;
+}
+
+__global__ void k_pairs_emit(const int *__restrict__ ck, const int *__restrict__ cp,
+                             const unsigned char *__restrict__ cflag, const int *__restrict__ pos, int n,
+                             int *__restrict__ out)
+{
+      int q = blockIdx.x * blockDim.x + threadIdx.x;
+      if (q >= n) return;
+      unsigned char f = cflag[q];
+      if (f & (F_DROP | F_MERGED)) return;
+      int o = pos[q];
+      bool sw = f & F_SWAP;
+      out[2 * o] = sw ? cp[q] : ck[q];
+      out[2 * o + 1] = sw ? ck[q] : cp[q];
+}
+
+}  // namespace
+
+DevState dev_state();
+int sync_scalars();
+
+static int mesh_alloc(int d)
+{
+      Ctx &c = ctx();
+      if (d < 4 || d % 2 || d > 1200) return NCGPU_E_UNSUPPORTED;  // int cell index up to ~1.7e9
+      if (c.cstart && c.mesh_d == d) return NCGPU_OK;
+      if (c.cstart) cudaFree(c.cstart);
+      size_t dd = (size_t)d;
+      c.cell_cap = (dd + 3) * (1 + dd + dd * dd);
+      NCG_CK(cudaMalloc(&c.cstart, sizeof(int) * c.cell_cap));
+      NCG_CK(cudaMemsetAsync(c.cstart, 0xff, sizeof(int) * c.cell_cap, c.s));
+      c.mesh_d = d;
+      if (!c.mkeys) {
+            size_t N = (size_t)c.n_max;
+            NCG_CK(cudaMalloc(&c.mkeys, sizeof(uint32_t) * (N + 1)));
+            NCG_CK(cudaMalloc(&c.mvals, sizeof(int) * N));
+            NCG_CK(cudaMalloc(&c.ckey, sizeof(int) * N));
+            NCG_CK(cudaMalloc(&c.mcnt, sizeof(int) * (N + 1)));
+            NCG_CK(cudaMalloc(&c.moff, sizeof(int) * (N + 2)));
+            c.pair_cap = 5L * c.n_max * (long)(c.P.how_many_neighbours > 1. ? c.P.how_many_neighbours : 16.) + 1024;
+            if (c.pair_cap > 0x7fffff00L) c.pair_cap = 0x7fffff00L;
+            NCG_CK(cudaMalloc(&c.cand_k, sizeof(int) * c.pair_cap));
+            NCG_CK(cudaMalloc(&c.cand_p, sizeof(int) * c.pair_cap));
+            NCG_CK(cudaMalloc(&c.cflag, c.pair_cap));
+            NCG_CK(cudaMalloc(&c.cpos, sizeof(int) * (c.pair_cap + 1)));
+            NCG_CK(cudaMalloc(&c.msums, sizeof(int) * (c.pair_cap / 1024 + 2)));
+            c.occ_cap = 64 * c.n_max + 4096;
+            NCG_CK(cudaMalloc(&c.occ, sizeof(int) * (size_t)c.occ_cap));
+      }
+      return NCGPU_OK;
+}
+
+void mesh_free()
+{
+      Ctx &c = ctx();
+      void *ptrs[] = {c.cstart, c.mkeys, c.mvals, c.ckey, c.mcnt, c.moff, c.cand_k, c.cand_p, c.cflag, c.cpos,
+                      c.occ, c.msums};
+      for (void *p : ptrs)
+            if (p) cudaFree(p);
+}
+
+int mesh_reset_state()
+{
+      Ctx &c = ctx();
+      if (c.mesh_valid && c.mesh_n > 0) {
+            k_cell_clear<<<(c.mesh_n + 255) / 256, 256, 0, c.s>>>(c.mkeys, c.mesh_n, c.cstart);
+            NCG_LAUNCHED();
+      }
+      c.mesh_valid = 0;
+      return NCGPU_OK;
+}
+
+__global__ void k_clear_dirty_events(unsigned char *dirty, const int *ev, int n)
+{
+      int e = blockIdx.x * blockDim.x + threadIdx.x;
+      if (e < n) {
+            dirty[ev[3 * e]] = 0;
+            dirty[ev[3 * e + 1]] = 0;
+      }
+}
+
+// One mesh pass.  test = 1: mesh() (small bodies, predicate and resolution);
+// test = 0: get_neighbours_mesh() (every body, no predicate).
+int mesh_pass(double gam, int test)
+{
+      Ctx &c = ctx();
+      cudaStream_t st = c.s;
+      const int d = c.P.collision_cube_cells;
+      NCG_TRY(mesh_alloc(d));
+      NCG_TRY(mesh_reset_state());
+      const int lid = c.largest_id;
+      const int n = lid + 1;
+      int zero[S_COUNT] = {0};
+      NCG_CK(cudaMemcpyAsync(c.scal + S_NHITS, zero, 2 * sizeof(int), cudaMemcpyHostToDevice, st));  // NHITS, NEV
+      NCG_CK(cudaMemcpyAsync(c.scal + S_NBIG, zero, 3 * sizeof(int), cudaMemcpyHostToDevice, st));   // NBIG, NDROP, NINS
+      c.n_cand = c.n_pairs = 0;
+      c.total_neighbours = 0;
+      c.how_many_small = c.how_many_big = 0;
+      if (n <= 0) return sync_scalars();
+      DevState S = dev_state();
+      const double half = gam * (double)d / 2.0;
+      const int nb = (n + 255) / 256;
+      k_mesh_keys<<<nb, 256, 0, st>>>(S, lid, gam, half, d, !test, c.mkeys, c.mvals, c.ckey, c.scal + S_NBIG);
+      NCG_LAUNCHED();
+      NCG_TRY(radix_sort_pairs(c.mkeys, c.mvals, n, 32, st));
+      NCG_CK(cudaMemsetAsync(c.mkeys + n, 0xff, sizeof(uint32_t), st));
+      k_cell_heads<<<nb, 256, 0, st>>>(c.mkeys, n, c.cstart, c.scal + S_NINS);
+      NCG_LAUNCHED();
+      c.mesh_valid = 1;
+      c.mesh_n = n;
+      k_mesh_count<<<nb, 256, 0, st>>>(c.ckey, c.mkeys, c.mvals, c.cstart, lid, d, (long long)c.cell_cap, c.mcnt);
+      NCG_LAUNCHED();
+      NCG_TRY(scan_exclusive(c.mcnt, c.moff, n, c.cnt, st));
+      int h[S_COUNT];
+      int total = 0;
+      NCG_CK(cudaMemcpyAsync(&total, c.moff + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      if (test && h[S_NBIG] > 0) return NCGPU_E_UNSUPPORTED;  // bodies larger than the mesh size
+      if ((long)total > c.pair_cap) return NCGPU_E_CAPACITY;
+      c.n_cand = total;
+      k_mesh_write<<<nb, 256, 0, st>>>(S, c.ckey, c.mkeys, c.mvals, c.cstart, c.moff, lid, d, (long long)c.cell_cap,
+                                       c.dt, test, c.cand_k,
+                                       c.cand_p, c.cflag, c.hi, c.hit_cap, c.scal + S_NHITS, c.err);
+      NCG_LAUNCHED();
+      int nh = 0;
+      NCG_CK(cudaMemcpyAsync(&nh, c.scal + S_NHITS, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      if (nh > c.hit_cap) return NCGPU_E_CAPACITY;
+      if (nh > 0) {
+            NCG_CK(cudaMemcpyAsync(c.keys, c.hi, sizeof(int) * (size_t)nh, cudaMemcpyDeviceToDevice, st));
+            NCG_CK(cudaMemsetAsync(c.vals, 0, sizeof(int) * (size_t)nh, st));
+            NCG_TRY(radix_sort_pairs(c.keys, c.vals, nh, 31, st));
+            MeshEvArgs E{lid, d, c.P.collision_type, c.P.one_collision_only_bool, c.P.mesh_bool, c.ev_cap, c.n_max,
+                         c.occ_cap, n, (long long)c.cell_cap, c.dt, c.P.collision_parameter};
+            if (E.type == NCGPU_COLLISION_FRAGMENTATION) return NCGPU_E_UNSUPPORTED;
+            k_mesh_events<<<1, MEV, 0, st>>>(S, c.cand_k, c.cand_p, c.cflag, c.moff, c.ckey, c.mkeys, c.mvals,
+                                             c.cstart, (const int *)c.keys, nh, E, c.ev, c.evrec, c.dirty, c.occ,
+                                             c.scal + S_NDROP, c.err);
+            NCG_LAUNCHED();
+      }
+      NCG_TRY(sync_scalars());
+      NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      if (c.n_events > 0) {
+            k_clear_dirty_events<<<(c.n_events + 255) / 256, 256, 0, st>>>(c.dirty, c.ev, min(c.n_events, c.ev_cap));
+            NCG_LAUNCHED();
+      }
+      const int merged = c.P.collision_type == NCGPU_COLLISION_MERGER ? c.n_events : 0;
+      c.total_neighbours = (long)total - h[S_NDROP];
+      c.n_pairs = c.P.mutual_bool ? total - h[S_NDROP] - merged : 0;
+      c.how_many_big = h[S_NBIG];
+      return NCGPU_OK;
+}
+
+}  // namespace ncg
+
+using namespace ncg;
+
+extern "C" int ncgpu_mesh(double gam, int with_collisions, int *n_pairs, int *n_events, long *total_neighbours)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      if (!(gam > 0.)) return NCGPU_E_ARG;
+      NCG_TRY(mesh_pass(gam, with_collisions ? 1 : 0));
+      if (n_pairs) *n_pairs = c.n_pairs;
+      if (n_events) *n_events = with_collisions ? c.n_events : 0;
+      if (total_neighbours) *total_neighbours = c.total_neighbours;
+      return NCGPU_OK;
+}
+
+extern "C" int ncgpu_get_pairs(struct ncgpu_pair *out, int cap, int *n)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited) return NCGPU_E_STATE;
+      if (!n) return NCGPU_E_ARG;
+      *n = c.n_pairs;
+      if (!out || cap <= 0 || c.n_cand == 0 || c.n_pairs == 0) return NCGPU_OK;
+      cudaStream_t st = c.s;
+      const int nc = c.n_cand;
+      const int nb = (nc + 255) / 256;
+      k_pairs_keep<<<nb, 256, 0, st>>>(c.cflag, nc, c.cpos);
+      NCG_LAUNCHED();
+      NCG_TRY(scan_exclusive(c.cpos, c.cpos, nc, c.msums, st));  // in place
+      int *dst = nullptr;
+      NCG_CK(cudaMalloc(&dst, sizeof(int) * 2 * (size_t)c.n_pairs));
+      k_pairs_emit<<<nb, 256, 0, st>>>(c.cand_k, c.cand_p, c.cflag, c.cpos, nc, dst);
+      NCG_LAUNCHED();
+      const int k = c.n_pairs < cap ? c.n_pairs : cap;
+      cudaError_t e = cudaMemcpyAsync(out, dst, sizeof(int) * 2 * (size_t)k, cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      cudaFree(dst);
+      if (e != cudaSuccess) return cuda_fail(e, "ncgpu_get_pairs copy", __FILE__, __LINE__);
+      return NCGPU_OK;
+}
+
+extern "C" int ncgpu_mesh_reset(void)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited) return NCGPU_E_STATE;
+      return mesh_reset_state();
+}

@@ -1,0 +1,421 @@
+// Mesh-mode pieces of the step: the three largest bodies moved to slots 0-2
+// and the mesh gravity field.
+//
+// three_largest_moonlets (src/structure.c:914-1002) scans slots in order; the
+// first three existing bodies are ranked by special rules, every later body
+// displaces a ranked one only when strictly larger, so the result is the
+// first three of a stable sort (radius descending) of [ranked three, later
+// bodies in slot order].  The later bodies' top three by (radius desc, slot
+// asc) come from a parallel reduction; one thread merges and then applies
+// three_largest_three_first (src/structure.c:1005-1063).
+//
+// Mesh gravity (vector_field's mesh branches, src/physics.c:84-109, 205-261,
+// 297-379): central mass, the three largest bodies against every body, and
+// pairs[].  A body's pairs[] contributions are, in list order, its own pops
+// (cells 26..0, lower indices ascending) followed by the later bodies whose
+// pops found it, in ascending index.  Each thread walks the cells of its own
+// body in exactly that order, so the FP64 sums match the reference without
+// reading pairs[]; the three bodies 0-2 and CM_acc sum every body's term in
+// slot order (sequential chains in the exact mode).
+#include <algorithm>
+#include "common.cuh"
+#include "physics.cuh"
+
+namespace ncg {
+
+DevState dev_state();
+int sync_scalars();
+
+namespace {
+
+struct Top3 {
+      double R[3];
+      int i[3];
+};
+
+__device__ __forceinline__ bool better(double Ra, int ia, double Rb, int ib)
+{
+      return Ra > Rb || (Ra == Rb && ia < ib);
+}
+
+__device__ __forceinline__ void t3_insert(Top3 &t, double R, int i)
+{
+      if (i < 0) return;
+      if (t.i[0] < 0 || better(R, i, t.R[0], t.i[0])) {
+            t.R[2] = t.R[1]; t.i[2] = t.i[1]; t.R[1] = t.R[0]; t.i[1] = t.i[0]; t.R[0] = R; t.i[0] = i;
+      } else if (t.i[1] < 0 || better(R, i, t.R[1], t.i[1])) {
+            t.R[2] = t.R[1]; t.i[2] = t.i[1]; t.R[1] = R; t.i[1] = i;
+      } else if (t.i[2] < 0 || better(R, i, t.R[2], t.i[2])) {
+            t.R[2] = R; t.i[2] = i;
+      }
+}
+
+// first three existing slots (one warp, ballots over 32 slots at a time)
+__global__ void k_first3(const int *__restrict__ ex, int lid, int *__restrict__ out)
+{
+      int lane = threadIdx.x, found = 0;
+      int e[3] = {-1, -1, -1};
+      for (int base = 0; base <= lid && found < 3; base += 32) {
+            int j = base + lane;
+            unsigned m = __ballot_sync(0xffffffffu, j <= lid && ex[j]);
+            while (m && found < 3) {
+                  int b = __ffs(m) - 1;
+                  e[found++] = base + b;
+                  m &= m - 1;
+            }
+      }
+      if (lane == 0) {
+            out[0] = e[0];
+            out[1] = e[1];
+            out[2] = e[2];
+      }
+}
+
+constexpr int TB = 256;
+
+// top three by (radius desc, slot asc) of existing slots > first3[2]
+__global__ void k_top3_part(const DevState S, int lid, const int *__restrict__ first3, double *__restrict__ partR,
+                            int *__restrict__ parti)
+{
+      __shared__ double sR[3][TB];
+      __shared__ int si[3][TB];
+      Top3 t;
+      for (int q = 0; q < 3; q++) { t.R[q] = 0.; t.i[q] = -1; }
+      const int start = first3[2] + 1;
+      if (first3[2] >= 0)
+            for (int j = start + blockIdx.x * TB + threadIdx.x; j <= lid; j += gridDim.x * TB)
+                  if (S.ex[j]) t3_insert(t, S.R[j], j);
+      for (int q = 0; q < 3; q++) { sR[q][threadIdx.x] = t.R[q]; si[q][threadIdx.x] = t.i[q]; }
+      __syncthreads();
+      for (int o = TB / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o) {
+                  Top3 u;
+                  for (int q = 0; q < 3; q++) { u.R[q] = sR[q][threadIdx.x]; u.i[q] = si[q][threadIdx.x]; }
+                  for (int q = 0; q < 3; q++) t3_insert(u, sR[q][threadIdx.x + o], si[q][threadIdx.x + o]);
+                  for (int q = 0; q < 3; q++) { sR[q][threadIdx.x] = u.R[q]; si[q][threadIdx.x] = u.i[q]; }
+            }
+            __syncthreads();
+      }
+      if (threadIdx.x < 3) {
+            partR[blockIdx.x * 3 + threadIdx.x] = sR[threadIdx.x][0];
+            parti[blockIdx.x * 3 + threadIdx.x] = si[threadIdx.x][0];
+      }
+}
+
+__device__ void swap_bodies(const DevState &S, int a, int b)
+{
+      double *f[8] = {S.x, S.y, S.z, S.vx, S.vy, S.vz, S.m, S.R};
+      for (int q = 0; q < 8; q++) {
+            double t = f[q][a];
+            f[q][a] = f[q][b];
+            f[q][b] = t;
+      }
+}
+
+__device__ void move_body(const DevState &S, int dst, int src)
+{
+      double *f[8] = {S.x, S.y, S.z, S.vx, S.vy, S.vz, S.m, S.R};
+      for (int q = 0; q < 8; q++) f[q][dst] = f[q][src];
+}
+
+// merge + three_largest_three_first; out[0..2] = three_largest_indexes
+__global__ void k_top3_final(const DevState S, const int *__restrict__ first3, const double *__restrict__ partR,
+                             const int *__restrict__ parti, int nparts, int mesh_bool, int *__restrict__ out)
+{
+      if (threadIdx.x != 0) return;
+      int e0 = first3[0], e1 = first3[1], e2 = first3[2];
+      int t[3] = {-1, -1, -1};
+      double R0 = 0., R1 = 0., R2 = 0., R;
+      // the first three existing bodies (src/structure.c:933-978)
+      if (e0 >= 0) { R0 = S.R[e0]; t[0] = e0; }
+      if (e1 >= 0) {
+            R1 = S.R[e1];
+            if (R0 > R1) t[1] = e1;
+            else { t[1] = t[0]; t[0] = e1; R = R1; R1 = R0; R0 = R; }
+      }
+      if (e2 >= 0) {
+            R2 = S.R[e2];
+            if (R1 >= R2) t[2] = e2;
+            else if (R2 > R1 && R2 <= R0) { t[2] = t[1]; t[1] = e2; R = R2; R2 = R1; R1 = R; }
+            else { t[2] = t[1]; t[1] = t[0]; t[0] = e2; R = R2; R2 = R1; R1 = R0; R0 = R; }
+      }
+      // later bodies, strictly-larger insertion in (radius desc, slot asc) order
+      Top3 rest;
+      for (int q = 0; q < 3; q++) { rest.R[q] = 0.; rest.i[q] = -1; }
+      for (int b = 0; b < nparts; b++)
+            for (int q = 0; q < 3; q++) t3_insert(rest, partR[3 * b + q], parti[3 * b + q]);
+      for (int q = 0; q < 3; q++) {
+            int j = rest.i[q];
+            if (j < 0 || e2 < 0) continue;
+            double Rj = rest.R[q];
+            if (Rj > R0) { t[2] = t[1]; t[1] = t[0]; t[0] = j; R2 = R1; R1 = R0; R0 = Rj; }
+            else if (Rj > R1) { t[2] = t[1]; t[1] = j; R2 = R1; R1 = Rj; }
+            else if (Rj > R2) { t[2] = j; R2 = Rj; }
+      }
+      out[0] = t[0]; out[1] = t[1]; out[2] = t[2];
+      if (t[0] < 0 || t[1] < 0 || t[2] < 0) return;  // fewer than three bodies
+      // three_largest_three_first
+      int first = t[0], second = t[1], third = t[2];
+      if (first != 0) {
+            if (S.ex[0]) swap_bodies(S, 0, first);
+            else { move_body(S, 0, first); d_lose(S, first, mesh_bool); S.ex[0] = 1; }
+            if (second == 0) second = first;
+            else if (third == 0) third = first;
+      }
+      if (second != 1) {
+            if (S.ex[1]) swap_bodies(S, 1, second);
+            else { move_body(S, 1, second); d_lose(S, second, mesh_bool); S.ex[1] = 1; }
+            if (third == 1) third = second;
+      }
+      if (third != 2) {
+            if (S.ex[2]) swap_bodies(S, 2, third);
+            else { move_body(S, 2, third); d_lose(S, third, mesh_bool); S.ex[2] = 1; }
+      }
+}
+
+}  // namespace
+
+namespace {
+
+__device__ __forceinline__ long long g_noff(int l, int d)
+{
+      int di = l % 3 - 1, dj = (l / 3) % 3 - 1, dk = l / 9 - 1;
+      return di + dj * (long long)d + dk * (long long)d * d;
+}
+
+// a + ((G*m_o) * (x_o - x_b)) / D^3 with the reference's operation order
+__device__ __forceinline__ void pair_add(const DevState &S, int b, int o, double G, double sp, bool soft, double &ax,
+                                         double &ay, double &az)
+{
+      double dx = DSUB(S.x[o], S.x[b]), dy = DSUB(S.y[o], S.y[b]), dz = DSUB(S.z[o], S.z[b]);
+      double r2 = DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz));
+      if (soft) {
+            double s = DMUL(sp, DADD(S.R[b], S.R[o]));
+            r2 = DADD(r2, DMUL(s, s));
+      }
+      double D = __dsqrt_rn(r2);
+      double D3 = DMUL(DMUL(D, D), D);
+      double g = DMUL(G, S.m[o]);
+      ax = DADD(ax, DDIV(DMUL(g, dx), D3));
+      ay = DADD(ay, DDIV(DMUL(g, dy), D3));
+      az = DADD(az, DDIV(DMUL(g, dz), D3));
+}
+
+// The term body b adds to body i (0..2) in the k > 2 loop: G*mk*DX/D3 with
+// DX = X_b - X_i (src/physics.c:216-257).
+__device__ __forceinline__ void big_term(const DevState &S, int b, int i, double G, double sp, bool soft, double *t)
+{
+      double dx = DSUB(S.x[b], S.x[i]), dy = DSUB(S.y[b], S.y[i]), dz = DSUB(S.z[b], S.z[i]);
+      double r2 = DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz));
+      if (soft) {
+            double s = DMUL(sp, DADD(S.R[b], S.R[i]));
+            r2 = DADD(r2, DMUL(s, s));
+      }
+      double D = __dsqrt_rn(r2);
+      double D3 = DMUL(DMUL(D, D), D);
+      double g = DMUL(G, S.m[b]);
+      t[0] = DDIV(DMUL(g, dx), D3);
+      t[1] = DDIV(DMUL(g, dy), D3);
+      t[2] = DDIV(DMUL(g, dz), D3);
+}
+
+struct MGArgs {
+      int lid, d, central, mutual, soft;
+      long long cell_cap;
+      double G, sp, mu, cmx, cmy, cmz;
+};
+
+// Accelerations of bodies 3..lid (bodies 0..2 are finished by k_mesh_big3);
+// terms for bodies 0..2 and CM_acc go to `terms` (12 blocks of n_max).
+__global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
+                            const int *__restrict__ vals, const int *__restrict__ cstart, int have_cells,
+                            double *__restrict__ ax, double *__restrict__ ay, double *__restrict__ az,
+                            double *__restrict__ terms, long N)
+{
+      int b = blockIdx.x * blockDim.x + threadIdx.x;
+      if (b > A.lid || !S.ex[b]) return;
+      double a_x = 0., a_y = 0., a_z = 0.;
+      if (A.central) {
+            double DX = DSUB(S.x[b], A.cmx), DY = DSUB(S.y[b], A.cmy), DZ = DSUB(S.z[b], A.cmz);
+            double rk = __dsqrt_rn(DADD(DADD(DMUL(DX, DX), DMUL(DY, DY)), DMUL(DZ, DZ)));
+            double r3 = DMUL(DMUL(rk, rk), rk);
+            a_x = DDIV(DMUL(-A.mu, DX), r3);
+            a_y = DDIV(DMUL(-A.mu, DY), r3);
+            a_z = DDIV(DMUL(-A.mu, DZ), r3);
+            double g = DMUL(A.G, S.m[b]);
+            terms[9 * N + b] = DDIV(DMUL(g, DX), r3);
+            terms[10 * N + b] = DDIV(DMUL(g, DY), r3);
+            terms[11 * N + b] = DDIV(DMUL(g, DZ), r3);
+      }
+      if (b <= 2) {  // bodies 0..2: central term only here
+            ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
+            return;
+      }
+      if (A.mutual) {
+            for (int i = 0; i < 3; i++) {
+                  if (!S.ex[i]) continue;
+                  pair_add(S, b, i, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                  double t[3];
+                  big_term(S, b, i, A.G, A.sp, A.soft, t);
+                  terms[(3 * i) * N + b] = t[0];
+                  terms[(3 * i + 1) * N + b] = t[1];
+                  terms[(3 * i + 2) * N + b] = t[2];
+            }
+      }
+      const int L = have_cells ? ckey[b] : -1;
+      if (A.mutual && L >= 0) {
+            // own pops: cells 26..0, lower indices ascending
+            int cur[27];
+            for (int l = 26; l >= 0; --l) {
+                  long long cell = L + g_noff(l, A.d);
+                  cur[l] = -1;
+                  if (cell < 0 || cell >= A.cell_cap) continue;
+                  int s = cstart[cell];
+                  if (s < 0) continue;
+                  int q = s;
+                  for (; keys[q] == (uint32_t)cell; ++q) {
+                        int p = vals[q];
+                        if (p >= b) break;
+                        if (p > 2 && S.ex[p]) pair_add(S, b, p, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                  }
+                  cur[l] = (keys[q] == (uint32_t)cell) ? q : -1;  // first higher index, if any
+            }
+            // later bodies that found b, ascending index: 27-way merge
+            for (;;) {
+                  int best = 0x7fffffff, bl = -1;
+                  for (int l = 0; l < 27; ++l) {
+                        int q = cur[l];
+                        if (q < 0) continue;
+                        int v = vals[q];
+                        if (v < best) { best = v; bl = l; }
+                  }
+                  if (bl < 0) break;
+                  if (best > 2 && best != b && S.ex[best]) pair_add(S, b, best, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                  long long cell = L + g_noff(bl, A.d);
+                  int q = cur[bl] + 1;
+                  cur[bl] = (keys[q] == (uint32_t)cell) ? q : -1;
+            }
+      }
+      ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
+}
+
+// Bodies 0..2 and CM_acc.  exact: lanes 0..8 sum the k > 2 terms of body
+// i = lane/3, component lane%3, lanes 9..11 the CM_acc terms, each in slot
+// order, then lane 0 adds the (0,1), (0,2), (1,2) pairs (src/physics.c:297-341).
+__global__ void k_mesh_big3(DevState S, MGArgs A, const double *__restrict__ terms, long N, double *ax, double *ay,
+                            double *az, double *cm_acc)
+{
+      __shared__ double tot[12];
+      const int lane = threadIdx.x;
+      if (lane < 12) {
+            const int i = lane / 3;
+            const double *t = terms + (size_t)lane * N;
+            const bool cmlane = lane >= 9;
+            // body i's chain starts from its central term (it is accumulated
+            // on top of it in the k loop); CM_acc starts from 0
+            const int comp = lane % 3;
+            double s = cmlane ? 0. : (comp == 0 ? ax[i] : comp == 1 ? ay[i] : az[i]);
+            if (cmlane || (S.ex[i] && A.mutual)) {
+                  const int k0 = cmlane ? 0 : 3;
+                  double v[16];
+                  int k = k0;
+                  for (; k + 16 <= A.lid + 1; k += 16) {
+#pragma unroll
+                        for (int u = 0; u < 16; u++) v[u] = S.ex[k + u] ? t[k + u] : 0.;
+#pragma unroll
+                        for (int u = 0; u < 16; u++)
+                              if (S.ex[k + u]) s = DADD(s, v[u]);
+                  }
+                  for (; k <= A.lid; ++k)
+                        if (S.ex[k]) s = DADD(s, t[k]);
+            }
+            tot[lane] = s;
+      }
+      __syncthreads();
+      if (lane != 0) return;
+      if (A.central) {
+            cm_acc[0] = tot[9]; cm_acc[1] = tot[10]; cm_acc[2] = tot[11];
+      } else {
+            cm_acc[0] = cm_acc[1] = cm_acc[2] = 0.;
+      }
+      double a[3][3];
+      for (int i = 0; i < 3; i++) {
+            if (!S.ex[i]) continue;
+            a[i][0] = tot[3 * i];
+            a[i][1] = tot[3 * i + 1];
+            a[i][2] = tot[3 * i + 2];
+      }
+      if (A.mutual) {
+            const int pr[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+            for (int q = 0; q < 3; q++) {
+                  int u = pr[q][0], w = pr[q][1];
+                  if (!(S.ex[u] && S.ex[w])) continue;
+                  pair_add(S, u, w, A.G, A.sp, A.soft, a[u][0], a[u][1], a[u][2]);
+                  pair_add(S, w, u, A.G, A.sp, A.soft, a[w][0], a[w][1], a[w][2]);
+            }
+      }
+      for (int i = 0; i < 3; i++) {
+            if (!S.ex[i]) continue;
+            ax[i] = a[i][0]; ay[i] = a[i][1]; az[i] = a[i][2];
+      }
+}
+
+}  // namespace
+
+int three_largest_state(int *idx)
+{
+      Ctx &c = ctx();
+      cudaStream_t st = c.s;
+      const int lid = c.largest_id;
+      DevState S = dev_state();
+      int *first3 = c.n_dev + 2, *out = c.n_dev + 5;
+      k_first3<<<1, 32, 0, st>>>(c.ex, lid, first3);
+      NCG_LAUNCHED();
+      const int np = std::min(256, std::max(1, (lid + 1 + TB - 1) / TB));
+      double *partR = c.red + 1024;
+      int *parti = (int *)(c.red + 1792);
+      k_top3_part<<<np, TB, 0, st>>>(S, lid, first3, partR, parti);
+      NCG_LAUNCHED();
+      k_top3_final<<<1, 32, 0, st>>>(S, first3, partR, parti, np, c.P.mesh_bool, out);
+      NCG_LAUNCHED();
+      int h[3];
+      NCG_CK(cudaMemcpyAsync(h, out, sizeof h, cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      if (idx) { idx[0] = h[0]; idx[1] = h[1]; idx[2] = h[2]; }
+      return NCGPU_OK;
+}
+
+// vector_field in mesh mode on the device state; acc blocks + cm_acc.
+int mesh_gravity_state(const double *cm8)
+{
+      Ctx &c = ctx();
+      cudaStream_t st = c.s;
+      const int lid = c.largest_id;
+      const long N = c.n_max;
+      NCG_TRY(ensure_partial((size_t)12 * N));
+      DevState S = dev_state();
+      MGArgs A{lid, c.P.collision_cube_cells, c.P.central_mass_bool, c.P.mutual_bool,
+               c.P.softening_parameter != 0., (long long)c.cell_cap, c.P.G, c.P.softening_parameter, c.P.G * cm8[6], cm8[0], cm8[1], cm8[2]};
+      double *ax = c.acc, *ay = c.acc + N, *az = c.acc + 2 * N;
+      if (lid >= 0) {
+            k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.cstart, c.mesh_valid, ax,
+                                                          ay, az, c.partial, N);
+            NCG_LAUNCHED();
+      }
+      k_mesh_big3<<<1, 32, 0, st>>>(S, A, c.partial, N, ax, ay, az, c.cm_acc);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
+
+}  // namespace ncg
+
+using namespace ncg;
+
+extern "C" int ncgpu_three_largest(int *idx)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      NCG_TRY(three_largest_state(idx));
+      return sync_scalars();
+}

@@ -139,7 +139,59 @@ __global__ void k_radix_scatter(const uint32_t *__restrict__ kin, const int *__r
       }
 }
 
+// Exclusive scan of one 1024-element block; block total to sums[b].
+__global__ void k_block_scan(const int *__restrict__ in, int n, int *__restrict__ out, int *__restrict__ sums)
+{
+      __shared__ int ws[32];
+      int i = blockIdx.x * 1024 + threadIdx.x;
+      int v = i < n ? in[i] : 0;
+      int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+      int x = v;
+      for (int o = 1; o < 32; o <<= 1) {
+            int u = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += u;
+      }
+      if (lane == 31) ws[w] = x;
+      __syncthreads();
+      if (w == 0) {
+            int y = ws[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                  int u = __shfl_up_sync(0xffffffffu, y, o);
+                  if (lane >= o) y += u;
+            }
+            ws[lane] = y;
+      }
+      __syncthreads();
+      int excl = x - v + (w > 0 ? ws[w - 1] : 0);
+      if (i < n) out[i] = excl;
+      if (threadIdx.x == 1023) sums[blockIdx.x] = ws[31];
+}
+
+__global__ void k_add_block_offsets(int *__restrict__ out, int n, const int *__restrict__ sums)
+{
+      int i = blockIdx.x * 1024 + threadIdx.x;
+      if (i < n) out[i] += sums[blockIdx.x];
+}
+
 }  // namespace
+
+// out[i] = sum of in[0..i); out[n] = total (out has n + 1 entries).
+// `sums` is scratch of at least ceil(n / 1024) + 1 ints.
+int scan_exclusive(const int *in, int *out, int n, int *sums, cudaStream_t st)
+{
+      if (n <= 0) {
+            NCG_CK(cudaMemsetAsync(out, 0, sizeof(int), st));
+            return NCGPU_OK;
+      }
+      int nb = (n + 1023) / 1024;
+      k_block_scan<<<nb, 1024, 0, st>>>(in, n, out, sums);
+      NCG_LAUNCHED();
+      k_scan_single<<<1, 1024, 0, st>>>(sums, nb, out + n);
+      NCG_LAUNCHED();
+      k_add_block_offsets<<<nb, 1024, 0, st>>>(out, n, sums);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
 
 int compact_existing(const int *ex, int largest_id, int *n_host, cudaStream_t st)
 {

@@ -199,3 +199,20 @@ class PortWorld:
         idx = np.zeros(3, np.int32)
         self.lib.orc_w_three_largest(_p(idx))
         return idx
+
+
+def _pw_setup(L):
+    L.orc_w_step_mesh.restype = C.c_long
+    L.orc_w_end_of_timestep.restype = C.c_int
+    L.orc_w_step_brute_force.restype = C.c_int
+
+
+_orig_pw_init = PortWorld.__init__
+
+
+def _pw_init(self, n_max, params):
+    _orig_pw_init(self, n_max, params)
+    _pw_setup(self.lib)
+
+
+PortWorld.__init__ = _pw_init

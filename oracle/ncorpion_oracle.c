@@ -637,3 +637,115 @@ int orc_w_step_brute_force(void)
       orc_w_drift();
       return orc_w_end_of_timestep();
 }
+
+/* vector_field, mesh branches (src/physics.c:84-109, 205-261, 297-379):
+   central mass, the three largest bodies (slots 0-2) against every body,
+   their mutual pairs, then pairs[] in list order.  acc: 3 per slot. */
+void orc_w_vector_field_mesh(double *acc, double *cm_acc)
+{
+      int k, p, j;
+      const double G = W.P.G, sp = W.P.softening_parameter;
+      const int c = W.P.central_mass_bool, mut = W.P.mutual_bool;
+      const body *b = W.b;
+      const int *ex = W.ex;
+      double XX = c ? W.cm.x : 0., YY = c ? W.cm.y : 0., ZZ = c ? W.cm.z : 0.;
+      double M = W.cm.mass;
+      double X0 = 0, Y0 = 0, Z0 = 0, m0 = 0, R0 = 0, X1 = 0, Y1 = 0, Z1 = 0, m1 = 0, R1 = 0, X2 = 0, Y2 = 0, Z2 = 0, m2 = 0, R2 = 0;
+      if (ex[0]) { X0 = b[0].x; Y0 = b[0].y; Z0 = b[0].z; m0 = b[0].mass; R0 = b[0].radius; }
+      if (ex[1]) { X1 = b[1].x; Y1 = b[1].y; Z1 = b[1].z; m1 = b[1].mass; R1 = b[1].radius; }
+      if (ex[2]) { X2 = b[2].x; Y2 = b[2].y; Z2 = b[2].z; m2 = b[2].mass; R2 = b[2].radius; }
+      cm_acc[0] = cm_acc[1] = cm_acc[2] = 0.;
+      for (k = 0; k <= W.lid; k++) acc[3 * k] = acc[3 * k + 1] = acc[3 * k + 2] = 0.;
+      for (k = 0; k <= W.lid; k++) {
+            if (!ex[k]) continue;
+            double X = b[k].x, Y = b[k].y, Z = b[k].z, mk = b[k].mass;
+            double DX = X - XX, DY = Y - YY, DZ = Z - ZZ;
+            double rk = sqrt(DX * DX + DY * DY + DZ * DZ), r3 = rk * rk * rk, mu = G * M;
+            double aX = 0., aY = 0., aZ = 0.;
+            if (c) {
+                  aX = -mu * DX / r3; aY = -mu * DY / r3; aZ = -mu * DZ / r3;
+                  cm_acc[0] += G * mk * DX / r3; cm_acc[1] += G * mk * DY / r3; cm_acc[2] += G * mk * DZ / r3;
+            }
+            if (mut && k > 2) {
+                  double Rk = b[k].radius, soft, D, D3;
+                  double Xi[3] = {X0, X1, X2}, Yi[3] = {Y0, Y1, Y2}, Zi[3] = {Z0, Z1, Z2}, mi[3] = {m0, m1, m2},
+                         Ri[3] = {R0, R1, R2};
+                  for (int i = 0; i < 3; i++) {
+                        if (!ex[i]) continue;
+                        DX = X - Xi[i]; DY = Y - Yi[i]; DZ = Z - Zi[i];
+                        soft = sp * (Rk + Ri[i]);
+                        D = sqrt(DX * DX + DY * DY + DZ * DZ + soft * soft);
+                        D3 = D * D * D;
+                        aX -= G * mi[i] * DX / D3; aY -= G * mi[i] * DY / D3; aZ -= G * mi[i] * DZ / D3;
+                        acc[3 * i] += G * mk * DX / D3; acc[3 * i + 1] += G * mk * DY / D3; acc[3 * i + 2] += G * mk * DZ / D3;
+                  }
+            }
+            acc[3 * k] = aX; acc[3 * k + 1] = aY; acc[3 * k + 2] = aZ;
+      }
+      if (!mut) return;
+      int pr[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+      for (int q = 0; q < 3; q++) {
+            int u = pr[q][0], w = pr[q][1];
+            if (!(ex[u] && ex[w])) continue;
+            double DX = b[u].x - b[w].x, DY = b[u].y - b[w].y, DZ = b[u].z - b[w].z;
+            double soft = sp * (b[u].radius + b[w].radius);
+            double D = sqrt(DX * DX + DY * DY + DZ * DZ + soft * soft), D3 = D * D * D;
+            double mu_ = b[u].mass, mw = b[w].mass;
+            acc[3 * u] -= G * mw * DX / D3; acc[3 * u + 1] -= G * mw * DY / D3; acc[3 * u + 2] -= G * mw * DZ / D3;
+            acc[3 * w] += G * mu_ * DX / D3; acc[3 * w + 1] += G * mu_ * DY / D3; acc[3 * w + 2] += G * mu_ * DZ / D3;
+      }
+      for (j = 0; j < W.n_pairs; j++) {
+            k = W.pairs[2 * j];
+            p = W.pairs[2 * j + 1];
+            if (!(ex[k] && ex[p] && k > 2 && p > 2)) continue;
+            double DX = b[k].x - b[p].x, DY = b[k].y - b[p].y, DZ = b[k].z - b[p].z;
+            double soft = sp * (b[k].radius + b[p].radius);
+            double D = sqrt(DX * DX + DY * DY + DZ * DZ + soft * soft), D3 = D * D * D;
+            double mk = b[k].mass, mp = b[p].mass;
+            acc[3 * k] -= G * mp * DX / D3; acc[3 * k + 1] -= G * mp * DY / D3; acc[3 * k + 2] -= G * mp * DZ / D3;
+            acc[3 * p] += G * mk * DX / D3; acc[3 * p + 1] += G * mk * DY / D3; acc[3 * p + 2] += G * mk * DZ / D3;
+      }
+}
+
+void orc_w_kick_mesh(void)
+{
+      int i;
+      double *acc = (double *)malloc(sizeof(double) * 3 * (size_t)(W.lid + 1 > 0 ? W.lid + 1 : 1));
+      double cma[3];
+      orc_w_vector_field_mesh(acc, cma);
+      for (i = 0; i <= W.lid; i++) {
+            if (!W.ex[i]) continue;
+            W.b[i].vx += W.dt * acc[3 * i];
+            W.b[i].vy += W.dt * acc[3 * i + 1];
+            W.b[i].vz += W.dt * acc[3 * i + 2];
+      }
+      if (W.P.central_mass_bool) {
+            W.cm.vx += W.dt * cma[0];
+            W.cm.vy += W.dt * cma[1];
+            W.cm.vz += W.dt * cma[2];
+      }
+      free(acc);
+}
+
+/* one iteration of integration_mesh's loop (src/rk4.c:760-790) with a given
+   gamma; returns total_neighbours of the pass (for the host's gamma update) */
+long orc_w_step_mesh(void)
+{
+      int idx[3];
+      long tn;
+      orc_w_mesh_reset();
+      if (W.P.collision_bool) {
+            orc_w_three_largest(idx);
+            orc_w_mesh();
+      }
+      orc_w_drift();
+      if (!W.P.collision_bool) {
+            orc_w_three_largest(idx);
+            orc_w_get_neighbours_mesh();
+      }
+      orc_w_kick_mesh();
+      tn = W.total_neighbours;
+      orc_w_end_of_timestep();
+      orc_w_mesh_reset();
+      return tn;
+}
