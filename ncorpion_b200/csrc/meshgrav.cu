@@ -299,40 +299,92 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
       ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
 }
 
-// Bodies 0..2 and CM_acc.  exact: lanes 0..8 sum the k > 2 terms of body
-// i = lane/3, component lane%3, lanes 9..11 the CM_acc terms, each in slot
-// order, then lane 0 adds the (0,1), (0,2), (1,2) pairs (src/physics.c:297-341).
-__global__ void k_mesh_big3(DevState S, MGArgs A, const double *__restrict__ terms, long N, double *ax, double *ay,
-                            double *az, double *cm_acc)
+// Bodies 0..2 and CM_acc.  Chain w (0..8: body w/3, component w%3; 9..11:
+// CM_acc components) sums its terms in slot order.  exact: one warp per chain,
+// coalesced loads of 32 terms handed to the chain through shuffles, so the
+// FP64 sum is the reference's sequential one (a body that does not exist adds
+// +0.0, which leaves any sum other than -0.0 unchanged).  Body i's chain starts
+// from its central term, CM_acc from 0.
+__device__ __forceinline__ double chain_init(int w, const double *ax, const double *ay, const double *az)
 {
-      __shared__ double tot[12];
-      const int lane = threadIdx.x;
-      if (lane < 12) {
-            const int i = lane / 3;
-            const double *t = terms + (size_t)lane * N;
-            const bool cmlane = lane >= 9;
-            // body i's chain starts from its central term (it is accumulated
-            // on top of it in the k loop); CM_acc starts from 0
-            const int comp = lane % 3;
-            double s = cmlane ? 0. : (comp == 0 ? ax[i] : comp == 1 ? ay[i] : az[i]);
-            if (cmlane || (S.ex[i] && A.mutual)) {
-                  const int k0 = cmlane ? 0 : 3;
-                  double v[16];
-                  int k = k0;
-                  for (; k + 16 <= A.lid + 1; k += 16) {
+      if (w >= 9) return 0.;
+      int i = w / 3, comp = w % 3;
+      return comp == 0 ? ax[i] : comp == 1 ? ay[i] : az[i];
+}
+
+__device__ __forceinline__ bool chain_live(int w, const DevState &S, const MGArgs &A)
+{
+      return w >= 9 ? A.central : (S.ex[w / 3] && A.mutual);
+}
+
+__global__ void __launch_bounds__(384) k_mesh_chains(DevState S, MGArgs A, const double *__restrict__ terms, long N,
+                                                     const double *__restrict__ ax, const double *__restrict__ ay,
+                                                     const double *__restrict__ az, double *__restrict__ tot)
+{
+      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      double s = chain_init(w, ax, ay, az);
+      if (chain_live(w, S, A)) {
+            const double *t = terms + (size_t)w * N;
+            const int k0 = w >= 9 ? 0 : 3;
+            const int n = A.lid + 1;
+            int k = k0;
+            double v = (k + lane < n && S.ex[k + lane]) ? t[k + lane] : 0.;
+            for (; k < n; k += 32) {
+                  const int kn = k + 32 + lane;
+                  const double vn = (kn < n && S.ex[kn]) ? t[kn] : 0.;  // prefetch the next chunk
 #pragma unroll
-                        for (int u = 0; u < 16; u++) v[u] = S.ex[k + u] ? t[k + u] : 0.;
-#pragma unroll
-                        for (int u = 0; u < 16; u++)
-                              if (S.ex[k + u]) s = DADD(s, v[u]);
-                  }
-                  for (; k <= A.lid; ++k)
-                        if (S.ex[k]) s = DADD(s, t[k]);
+                  for (int u = 0; u < 32; u++) s = DADD(s, __shfl_sync(0xffffffffu, v, u));
+                  v = vn;
             }
-            tot[lane] = s;
+      }
+      if (lane == 0) tot[w] = s;
+}
+
+// Non-exact modes: deterministic two-level sums of the same 12 chains.
+constexpr int RB12 = 256;
+__global__ void k_mesh_chains_part(DevState S, MGArgs A, const double *__restrict__ terms, long N,
+                                   double *__restrict__ part)
+{
+      __shared__ double sh[12][RB12 / 32];
+      double s[12];
+      for (int w = 0; w < 12; w++) s[w] = 0.;
+      const int n = A.lid + 1;
+      for (int k = blockIdx.x * RB12 + threadIdx.x; k < n; k += gridDim.x * RB12) {
+            if (!S.ex[k]) continue;
+            for (int w = 0; w < 12; w++)
+                  if (k >= (w >= 9 ? 0 : 3)) s[w] += terms[(size_t)w * N + k];
+      }
+      const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+      for (int w = 0; w < 12; w++) {
+            double v = s[w];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) sh[w][wp] = v;
       }
       __syncthreads();
-      if (lane != 0) return;
+      if (threadIdx.x < 12) {
+            double v = 0.;
+            for (int q = 0; q < RB12 / 32; q++) v += sh[threadIdx.x][q];
+            part[blockIdx.x * 12 + threadIdx.x] = v;
+      }
+}
+
+__global__ void k_mesh_chains_fold(DevState S, MGArgs A, const double *__restrict__ part, int nparts,
+                                   const double *__restrict__ ax, const double *__restrict__ ay,
+                                   const double *__restrict__ az, double *__restrict__ tot)
+{
+      const int w = threadIdx.x;
+      if (w >= 12) return;
+      double s = 0.;
+      for (int b = 0; b < nparts; b++) s += part[12 * b + w];
+      tot[w] = chain_live(w, S, A) ? chain_init(w, ax, ay, az) + s : chain_init(w, ax, ay, az);
+}
+
+// CM_acc and bodies 0..2: chain totals, then the (0,1), (0,2), (1,2) pairs
+// (src/physics.c:297-341).
+__global__ void k_mesh_big3(DevState S, MGArgs A, const double *__restrict__ tot, double *ax, double *ay, double *az,
+                            double *cm_acc)
+{
+      if (threadIdx.x != 0) return;
       if (A.central) {
             cm_acc[0] = tot[9]; cm_acc[1] = tot[10]; cm_acc[2] = tot[11];
       } else {
@@ -402,7 +454,19 @@ int mesh_gravity_state(const double *cm8)
                                                           ay, az, c.partial, N);
             NCG_LAUNCHED();
       }
-      k_mesh_big3<<<1, 32, 0, st>>>(S, A, c.partial, N, ax, ay, az, c.cm_acc);
+      double *tot = c.red + 3584;
+      if (c.P.gravity_mode == NCGPU_GRAVITY_EXACT) {
+            k_mesh_chains<<<1, 384, 0, st>>>(S, A, c.partial, N, ax, ay, az, tot);
+            NCG_LAUNCHED();
+      } else {
+            const int np = std::min(148, std::max(1, (lid + RB12) / RB12));
+            double *part = c.red + 1024;  // up to 148 x 12 doubles
+            k_mesh_chains_part<<<np, RB12, 0, st>>>(S, A, c.partial, N, part);
+            NCG_LAUNCHED();
+            k_mesh_chains_fold<<<1, 32, 0, st>>>(S, A, part, np, ax, ay, az, tot);
+            NCG_LAUNCHED();
+      }
+      k_mesh_big3<<<1, 32, 0, st>>>(S, A, tot, ax, ay, az, c.cm_acc);
       NCG_LAUNCHED();
       return NCGPU_OK;
 }

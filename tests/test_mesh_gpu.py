@@ -38,8 +38,10 @@ def assert_state_equal(b, ex, b_ref, ex_ref):
 
 
 def mesh_params(ctype=2, cells=256, **kw):
-    return make_params(mesh_bool=1, brute_force_bool=0, collision_bool=1, collision_type=ctype,
-                       collision_parameter=1.5, collision_cube_cells=cells, **kw)
+    base = dict(mesh_bool=1, brute_force_bool=0, collision_bool=1, collision_type=ctype, collision_parameter=1.5,
+                collision_cube_cells=cells)
+    base.update(kw)
+    return make_params(**base)
 
 
 @pytest.fixture()
