@@ -205,6 +205,33 @@ int ncgpu_step_mesh(double gam, int *how_many_moonlets, long *total_neighbours);
    kick, brute_force collisions (when collision_bool), drift, end_of_timestep. */
 int ncgpu_step_brute_force(int *how_many_moonlets);
 
+/* ---- differentiable leapfrog (no reference counterpart) ------------------ */
+
+/* Host arrays, bodies as (n, 3) row-major triples. */
+struct ncgpu_leapfrog_args {
+      int n;                       /* bodies (all existing)                      */
+      const double *x0, *v0;       /* initial positions / velocities, 3n each     */
+      const double *m, *R;         /* masses, radii (softening), n each           */
+      const double *cm;            /* central mass record, 8 doubles              */
+      double dt;                   /* timestep                                    */
+      int nsteps;                  /* leapfrog steps                              */
+      int checkpoint;              /* steps between stored states (default 32)    */
+      double *x_final, *v_final;   /* outputs (3n each, may be NULL)              */
+      const double *adj_x_final;   /* dL/dx_final, 3n (ncgpu_leapfrog_vjp)        */
+      double *grad_x0, *grad_v0;   /* dL/dx0, dL/dv0, 3n each (ncgpu_leapfrog_vjp) */
+      double *grad_m;              /* dL/dm, n (ncgpu_leapfrog_vjp)                */
+};
+
+/* The brute-force integrator without collisions (src/rk4.c:873-936): half
+   drift, nsteps x (kick, drift), half back-drift of the output, the central
+   mass integrated as a body.  FP64 pair sums, one rsqrt per pair. */
+int ncgpu_leapfrog(const struct ncgpu_leapfrog_args *args);
+
+/* Reverse mode through ncgpu_leapfrog: given dL/dx_final returns dL/dx0,
+   dL/dv0 and dL/dm.  States are stored every `checkpoint` steps and each
+   segment is recomputed, so memory is O(n (nsteps/checkpoint + checkpoint)). */
+int ncgpu_leapfrog_vjp(const struct ncgpu_leapfrog_args *args);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,6 +47,18 @@ class Params(C.Structure):
     ]
 
 
+class LeapfrogArgs(C.Structure):
+    """Mirror of ``struct ncgpu_leapfrog_args``."""
+
+    _fields_ = [
+        ("n", C.c_int),
+        ("x0", C.c_void_p), ("v0", C.c_void_p), ("m", C.c_void_p), ("R", C.c_void_p), ("cm", C.c_void_p),
+        ("dt", C.c_double), ("nsteps", C.c_int), ("checkpoint", C.c_int),
+        ("x_final", C.c_void_p), ("v_final", C.c_void_p), ("adj_x_final", C.c_void_p),
+        ("grad_x0", C.c_void_p), ("grad_v0", C.c_void_p), ("grad_m", C.c_void_p),
+    ]
+
+
 class NcgpuError(RuntimeError):
     def __init__(self, status, where, lib=None):
         msg = f"{where}: status {status}"
@@ -91,6 +103,8 @@ EXPORTS = {
     "ncgpu_mesh_reset": (C.c_int, []),
     "ncgpu_set_force_naive": (C.c_int, [C.c_int]),
     "ncgpu_step_mesh": (C.c_int, [C.c_double, P, P]),
+    "ncgpu_leapfrog": (C.c_int, [P]),
+    "ncgpu_leapfrog_vjp": (C.c_int, [P]),
     "ncgpu_drift": (C.c_int, []),
 }
 
@@ -280,3 +294,37 @@ def update_gamma(gam, total_neighbours, how_many_moonlets, how_many_neighbours, 
     average = 2.0 * float(total_neighbours) / float(how_many_moonlets)
     gam = gam * (how_many_neighbours / average) ** (1.0 / 3.0)
     return gam_min if gam < gam_min else gam
+
+
+def _c3(a):
+    return np.ascontiguousarray(a, np.float64).reshape(-1, 3)
+
+
+def leapfrog(x0, v0, m, R, cm, dt, nsteps, checkpoint=32):
+    """Final positions and velocities of the collisionless brute-force
+    integrator (half drift, nsteps x (kick, drift), half back-drift)."""
+    x0, v0 = _c3(x0), _c3(v0)
+    n = x0.shape[0]
+    m = np.ascontiguousarray(m, np.float64)
+    R = np.ascontiguousarray(R, np.float64)
+    cm = np.ascontiguousarray(cm, np.float64)
+    xf, vf = np.zeros((n, 3)), np.zeros((n, 3))
+    a = LeapfrogArgs(n, x0.ctypes.data, v0.ctypes.data, m.ctypes.data, R.ctypes.data, cm.ctypes.data, float(dt),
+                     int(nsteps), int(checkpoint), xf.ctypes.data, vf.ctypes.data, None, None, None, None)
+    check(load().ncgpu_leapfrog(C.byref(a)), "ncgpu_leapfrog")
+    return xf, vf
+
+
+def leapfrog_vjp(x0, v0, m, R, cm, dt, nsteps, adj_x_final, checkpoint=32):
+    """(dL/dx0, dL/dv0, dL/dm) for a given dL/dx_final."""
+    x0, v0, adj = _c3(x0), _c3(v0), _c3(adj_x_final)
+    n = x0.shape[0]
+    m = np.ascontiguousarray(m, np.float64)
+    R = np.ascontiguousarray(R, np.float64)
+    cm = np.ascontiguousarray(cm, np.float64)
+    gx, gv, gm = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n)
+    a = LeapfrogArgs(n, x0.ctypes.data, v0.ctypes.data, m.ctypes.data, R.ctypes.data, cm.ctypes.data, float(dt),
+                     int(nsteps), int(checkpoint), None, None, adj.ctypes.data, gx.ctypes.data, gv.ctypes.data,
+                     gm.ctypes.data)
+    check(load().ncgpu_leapfrog_vjp(C.byref(a)), "ncgpu_leapfrog_vjp")
+    return gx, gv, gm

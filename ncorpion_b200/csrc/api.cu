@@ -277,7 +277,7 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
       const size_t NS = std::max(N, (size_t)1 << 20);
       A(c.keys, NS); A(c.keys2, NS); A(c.vals, NS); A(c.vals2, NS);
       c.hist_cap = 256 * ((NS + 2047) / 2048);
-      A(c.hist, c.hist_cap);
+      A(c.hist, c.hist_cap + 1);  // + total of the in-place scan
       A(c.red, 4096);
       A(c.err, 1);
       A(c.aos, 8 * N);

@@ -332,8 +332,11 @@ __global__ void __launch_bounds__(384) k_mesh_chains(DevState S, MGArgs A, const
             for (; k < n; k += 32) {
                   const int kn = k + 32 + lane;
                   const double vn = (kn < n && S.ex[kn]) ? t[kn] : 0.;  // prefetch the next chunk
+                  double w[32];
 #pragma unroll
-                  for (int u = 0; u < 32; u++) s = DADD(s, __shfl_sync(0xffffffffu, v, u));
+                  for (int u = 0; u < 32; u++) w[u] = __shfl_sync(0xffffffffu, v, u);  // off the add chain
+#pragma unroll
+                  for (int u = 0; u < 32; u++) s = DADD(s, w[u]);
                   v = vn;
             }
       }

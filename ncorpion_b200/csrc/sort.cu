@@ -228,8 +228,7 @@ int radix_sort_pairs(uint32_t *keys, int *vals, int n, int bits, cudaStream_t st
             int shift = 8 * p;
             k_radix_hist<<<nb, RT, 0, st>>>(ka, n, shift, c.hist, nb);
             NCG_LAUNCHED();
-            k_scan_single<<<1, 1024, 0, st>>>(c.hist, (int)need, c.n_dev + 1);
-            NCG_LAUNCHED();
+            NCG_TRY(scan_exclusive(c.hist, c.hist, (int)need, c.cnt, st));
             k_radix_scatter<<<nb, RT, 0, st>>>(ka, va, kb, vb, n, shift, c.hist, nb);
             NCG_LAUNCHED();
             uint32_t *tk = ka; ka = kb; kb = tk;
