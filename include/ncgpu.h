@@ -54,29 +54,31 @@ struct ncgpu_event {         /* one collision_treatment(a, b, type) call, in ord
 };
 
 /* Mirror of the parameters.h macros that the hot path reads
-   (src/parameters.h:66-119, 171-201, 283-309). */
+   (src/parameters.h:66-119, 171-201, 283-309).  Each field is the macro's
+   name with a par_ prefix, so this header can be included next to
+   parameters.h, whose macros would otherwise rewrite the field names. */
 struct ncgpu_params {
-      double G;                      /* G                                        */
-      double softening_parameter;    /* softening_parameter (x (R_k + R_p))      */
-      int central_mass_bool;         /* central_mass_bool                        */
-      int mutual_bool;               /* mutual_bool                              */
-      int collision_bool;            /* collision_bool                           */
-      int brute_force_bool;          /* brute_force_bool                         */
-      int mesh_bool;                 /* mesh_bool                                */
-      int collision_type;            /* NCGPU_COLLISION_*                        */
-      double collision_parameter;    /* collision_parameter (inelastic f)        */
-      int one_collision_only_bool;   /* one_collision_only_bool                  */
-      int collision_cube_cells;      /* collision_cube_cells (mesh)              */
-      double how_many_neighbours;    /* how_many_neighbours (mesh)               */
-      double collision_cube_min;     /* collision_cube_min (mesh)                */
-      int switch_to_brute_force;     /* switch_to_brute_force                    */
-      int gravity_mode;              /* NCGPU_GRAVITY_*                          */
-      double near_theta;             /* MIXED: tile pairs whose boxes are closer
+      double par_G;                      /* G                                        */
+      double par_softening_parameter;    /* softening_parameter (x (R_k + R_p))      */
+      int par_central_mass_bool;         /* central_mass_bool                        */
+      int par_mutual_bool;               /* mutual_bool                              */
+      int par_collision_bool;            /* collision_bool                           */
+      int par_brute_force_bool;          /* brute_force_bool                         */
+      int par_mesh_bool;                 /* mesh_bool                                */
+      int par_collision_type;            /* NCGPU_COLLISION_*                        */
+      double par_collision_parameter;    /* collision_parameter (inelastic f)        */
+      int par_one_collision_only_bool;   /* one_collision_only_bool                  */
+      int par_collision_cube_cells;      /* collision_cube_cells (mesh)              */
+      double par_how_many_neighbours;    /* how_many_neighbours (mesh)               */
+      double par_collision_cube_min;     /* collision_cube_min (mesh)                */
+      int par_switch_to_brute_force;     /* switch_to_brute_force                    */
+      int par_gravity_mode;              /* NCGPU_GRAVITY_*                          */
+      double par_near_theta;             /* MIXED: tile pairs whose boxes are closer
                                         than near_theta x the larger box diagonal
                                         are summed in FP64 (default 0.25 if <= 0) */
-      double disruption_threshold;   /* disruption_threshold (dump into the CM)  */
-      double high_dumping_threshold; /* high_dumping_threshold (dump, unbound)   */
-      int reduce_to_COM_bool;        /* reduce_to_COM_bool                       */
+      double par_disruption_threshold;   /* disruption_threshold (dump into the CM)  */
+      double par_high_dumping_threshold; /* high_dumping_threshold (dump, unbound)   */
+      int par_reduce_to_COM_bool;        /* reduce_to_COM_bool                       */
 };
 
 /* Fills *p with the reference's default values for the fields above
@@ -220,6 +222,8 @@ struct ncgpu_leapfrog_args {
       const double *adj_x_final;   /* dL/dx_final, 3n (ncgpu_leapfrog_vjp)        */
       double *grad_x0, *grad_v0;   /* dL/dx0, dL/dv0, 3n each (ncgpu_leapfrog_vjp) */
       double *grad_m;              /* dL/dm, n (ncgpu_leapfrog_vjp)                */
+      const double *tan_x0, *tan_v0, *tan_m;  /* input tangents (ncgpu_leapfrog_jvp)  */
+      double *tan_x_final;         /* output tangent of x_final, 3n (ncgpu_leapfrog_jvp) */
 };
 
 /* The brute-force integrator without collisions (src/rk4.c:873-936): half
@@ -231,6 +235,12 @@ int ncgpu_leapfrog(const struct ncgpu_leapfrog_args *args);
    dL/dv0 and dL/dm.  States are stored every `checkpoint` steps and each
    segment is recomputed, so memory is O(n (nsteps/checkpoint + checkpoint)). */
 int ncgpu_leapfrog_vjp(const struct ncgpu_leapfrog_args *args);
+
+/* Forward mode (tangent-linear) through ncgpu_leapfrog: the directional
+   derivative of x_final along (tan_x0, tan_v0, tan_m).  Exact to rounding, it
+   checks the adjoint through <w, J d> = <J^T w, d> where finite differences of
+   tiny masses drown in roundoff. */
+int ncgpu_leapfrog_jvp(const struct ncgpu_leapfrog_args *args);
 
 #ifdef __cplusplus
 }

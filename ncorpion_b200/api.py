@@ -56,6 +56,7 @@ class LeapfrogArgs(C.Structure):
         ("dt", C.c_double), ("nsteps", C.c_int), ("checkpoint", C.c_int),
         ("x_final", C.c_void_p), ("v_final", C.c_void_p), ("adj_x_final", C.c_void_p),
         ("grad_x0", C.c_void_p), ("grad_v0", C.c_void_p), ("grad_m", C.c_void_p),
+        ("tan_x0", C.c_void_p), ("tan_v0", C.c_void_p), ("tan_m", C.c_void_p), ("tan_x_final", C.c_void_p),
     ]
 
 
@@ -105,6 +106,7 @@ EXPORTS = {
     "ncgpu_step_mesh": (C.c_int, [C.c_double, P, P]),
     "ncgpu_leapfrog": (C.c_int, [P]),
     "ncgpu_leapfrog_vjp": (C.c_int, [P]),
+    "ncgpu_leapfrog_jvp": (C.c_int, [P]),
     "ncgpu_drift": (C.c_int, []),
 }
 
@@ -328,3 +330,19 @@ def leapfrog_vjp(x0, v0, m, R, cm, dt, nsteps, adj_x_final, checkpoint=32):
                      gm.ctypes.data)
     check(load().ncgpu_leapfrog_vjp(C.byref(a)), "ncgpu_leapfrog_vjp")
     return gx, gv, gm
+
+
+def leapfrog_jvp(x0, v0, m, R, cm, dt, nsteps, tan_x0, tan_v0, tan_m):
+    """Directional derivative of x_final along (tan_x0, tan_v0, tan_m)."""
+    x0, v0, tx, tv = _c3(x0), _c3(v0), _c3(tan_x0), _c3(tan_v0)
+    n = x0.shape[0]
+    m = np.ascontiguousarray(m, np.float64)
+    R = np.ascontiguousarray(R, np.float64)
+    cm = np.ascontiguousarray(cm, np.float64)
+    tm = np.ascontiguousarray(tan_m, np.float64)
+    out = np.zeros((n, 3))
+    a = LeapfrogArgs(n, x0.ctypes.data, v0.ctypes.data, m.ctypes.data, R.ctypes.data, cm.ctypes.data, float(dt),
+                     int(nsteps), 32, None, None, None, None, None, None, tx.ctypes.data, tv.ctypes.data,
+                     tm.ctypes.data, out.ctypes.data)
+    check(load().ncgpu_leapfrog_jvp(C.byref(a)), "ncgpu_leapfrog_jvp")
+    return out

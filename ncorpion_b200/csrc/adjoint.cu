@@ -25,21 +25,23 @@ namespace {
 constexpr int AT = 128;  // bodies per tile / threads per block
 
 struct Src {
-      const double *x, *y, *z, *m, *sR, *lx, *ly, *lz;
+      const double *x, *y, *z, *m, *sR, *lx, *ly, *lz;  // lx.. : adjoints (VJP) or position tangents (JVP)
+      const double *dm;                                 // mass tangents (JVP)
 };
 
-// Mutual forces (OP 0: 3 outputs) or their VJP (OP 1: 4 outputs) of target
-// block blockIdx.y against source chunk blockIdx.x.
+// Mutual forces (OP 0: 3 outputs), their VJP (OP 1: 4 outputs) or their JVP
+// (OP 2: 3 outputs, d a_k = sum_j G [dm_j r + m_j T_kj (dx_j - dx_k)] / ...)
+// of target block blockIdx.y against source chunk blockIdx.x.
 template <int OP, bool SOFT>
 __global__ void __launch_bounds__(AT) k_pairs(Src s, int n, int tpc, double *__restrict__ part, long stride)
 {
-      __shared__ double sx[AT], sy[AT], sz[AT], sm[AT], sr[AT], slx[AT], sly[AT], slz[AT];
+      __shared__ double sx[AT], sy[AT], sz[AT], sm[AT], sr[AT], slx[AT], sly[AT], slz[AT], sdm[AT];
       const int k = blockIdx.y * AT + threadIdx.x;
       const bool act = k < n;
       const int kk = act ? k : 0;
       const double xk = s.x[kk], yk = s.y[kk], zk = s.z[kk], mk = s.m[kk], rk = SOFT ? s.sR[kk] : 0.;
       double lxk = 0., lyk = 0., lzk = 0.;
-      if (OP == 1) { lxk = s.lx[kk]; lyk = s.ly[kk]; lzk = s.lz[kk]; }
+      if (OP >= 1) { lxk = s.lx[kk]; lyk = s.ly[kk]; lzk = s.lz[kk]; }
       double o0 = 0., o1 = 0., o2 = 0., o3 = 0.;
       const int ntiles = (n + AT - 1) / AT;
       const int t0 = blockIdx.x * tpc, t1 = min(ntiles, t0 + tpc);
@@ -50,7 +52,8 @@ __global__ void __launch_bounds__(AT) k_pairs(Src s, int n, int tpc, double *__r
                   sx[threadIdx.x] = s.x[j]; sy[threadIdx.x] = s.y[j]; sz[threadIdx.x] = s.z[j];
                   sm[threadIdx.x] = s.m[j];
                   if (SOFT) sr[threadIdx.x] = s.sR[j];
-                  if (OP == 1) { slx[threadIdx.x] = s.lx[j]; sly[threadIdx.x] = s.ly[j]; slz[threadIdx.x] = s.lz[j]; }
+                  if (OP >= 1) { slx[threadIdx.x] = s.lx[j]; sly[threadIdx.x] = s.ly[j]; slz[threadIdx.x] = s.lz[j]; }
+                  if (OP == 2) sdm[threadIdx.x] = s.dm[j];
             }
             __syncthreads();
             const int cnt = min(AT, n - t * AT);
@@ -65,6 +68,14 @@ __global__ void __launch_bounds__(AT) k_pairs(Src s, int n, int tpc, double *__r
                   if (OP == 0) {
                         const double w = sm[q] * i3;
                         o0 = fma(w, rx, o0); o1 = fma(w, ry, o1); o2 = fma(w, rz, o2);
+                  } else if (OP == 2) {
+                        const double i5 = i3 * ri * ri;
+                        const double dx = slx[q] - lxk, dy = sly[q] - lyk, dz = slz[q] - lzk;
+                        const double rd = rx * dx + ry * dy + rz * dz;
+                        const double mj = sm[q], c = 3.0 * rd * i5 * mj, g = sdm[q] * i3;
+                        o0 += g * rx + mj * i3 * dx - rx * c;
+                        o1 += g * ry + mj * i3 * dy - ry * c;
+                        o2 += g * rz + mj * i3 * dz - rz * c;
                   } else {
                         const double i5 = i3 * ri * ri;
                         const double mj = sm[q];
@@ -77,7 +88,7 @@ __global__ void __launch_bounds__(AT) k_pairs(Src s, int n, int tpc, double *__r
             }
       }
       if (act) {
-            double *p = part + (size_t)blockIdx.x * (OP == 0 ? 3 : 4) * stride;
+            double *p = part + (size_t)blockIdx.x * (OP == 1 ? 4 : 3) * stride;
             p[k] = o0; p[stride + k] = o1; p[2 * stride + k] = o2;
             if (OP == 1) p[3 * stride + k] = o3;
       }
@@ -140,6 +151,35 @@ __global__ void k_vjp_final(const double *__restrict__ part, int nch, long strid
       mux[k] = o[0]; muy[k] = o[1]; muz[k] = o[2]; nu[k] = o[3];
 }
 
+// JVP: d a = G * sum of chunk partials - G M J_k (dx_k - dX); per-body terms
+// of d A_cm = sum_k G [dm_k s_k/|s|^3 + m_k J_k (dx_k - dX)].
+__global__ void k_jvp_final(const double *__restrict__ part, int nch, long stride, Src s, int n,
+                            const double *__restrict__ cm, const double *__restrict__ dX, double G, double M,
+                            int central, double *dax, double *day, double *daz, double *cterm)
+{
+      int k = blockIdx.x * blockDim.x + threadIdx.x;
+      if (k >= n) return;
+      double o[3] = {0., 0., 0.};
+      for (int c = 0; c < nch; c++)
+            for (int d = 0; d < 3; d++) o[d] += part[(size_t)c * 3 * stride + d * stride + k];
+      for (int d = 0; d < 3; d++) o[d] *= G;
+      if (central) {
+            double sv[3] = {s.x[k] - cm[0], s.y[k] - cm[1], s.z[k] - cm[2]};
+            double r2 = sv[0] * sv[0] + sv[1] * sv[1] + sv[2] * sv[2];
+            double ri = rsqrt(r2), i3 = ri * ri * ri, i5 = i3 * ri * ri;
+            double u[3] = {s.lx[k] - dX[0], s.ly[k] - dX[1], s.lz[k] - dX[2]};
+            double su = sv[0] * u[0] + sv[1] * u[1] + sv[2] * u[2];
+            double Ju[3];
+            for (int d = 0; d < 3; d++) Ju[d] = u[d] * i3 - 3.0 * sv[d] * su * i5;
+            const double mk = s.m[k], dmk = s.dm[k];
+            for (int d = 0; d < 3; d++) {
+                  o[d] -= G * M * Ju[d];
+                  cterm[d * n + k] = G * (dmk * sv[d] * i3 + mk * Ju[d]);
+            }
+      }
+      dax[k] = o[0]; day[k] = o[1]; daz[k] = o[2];
+}
+
 constexpr int SB = 256;
 // out[d] = sum_k v[d*n + k], deterministic two levels (d < 3)
 __global__ void k_sum3p(const double *__restrict__ v, int n, double *__restrict__ part)
@@ -194,6 +234,7 @@ struct LF {
       double *X, *V, *m, *sR, *cm, *acc, *cterm, *part, *red, *acm;
       double *lx, *lv, *LX, *LV, *mu, *nu, *gm, *xterm, *muX;
       double *ckpt, *seg;
+      double *tx, *tv, *tm, *tX, *da, *dA;  // tangents (JVP)
       int C, ncp;
       cudaStream_t st;
 };
@@ -250,6 +291,36 @@ int lf_vjp(LF &L, const double *pos, const double *cmpos)
       return NCGPU_OK;
 }
 
+// One kick + drift of the state and of its tangents.
+int lf_step_jvp(LF &L, double dt)
+{
+      const int n = L.n, nb = (n + 255) / 256;
+      NCG_TRY(lf_force(L, L.X, L.cm));
+      Src s{L.X, L.X + n, L.X + 2 * n, L.m, L.sR, L.tx, L.tx + n, L.tx + 2 * n, L.tm};
+      dim3 grid(L.nch, L.ntiles);
+      if (L.soft) k_pairs<2, true><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
+      else k_pairs<2, false><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
+      NCG_LAUNCHED();
+      k_jvp_final<<<nb, 256, 0, L.st>>>(L.part, L.nch, n, s, n, L.cm, L.tX, L.G, L.M, L.central, L.da, L.da + n,
+                                        L.da + 2 * n, L.xterm);
+      NCG_LAUNCHED();
+      if (L.central) {
+            k_sum3p<<<L.np, SB, 0, L.st>>>(L.xterm, n, L.red);
+            NCG_LAUNCHED();
+            k_sum3f<<<1, 32, 0, L.st>>>(L.red, L.np, L.dA);
+            NCG_LAUNCHED();
+      }
+      k_axpy3<<<nb, 256, 0, L.st>>>(dt, L.acc, L.V, n, n, L.acm, L.central ? L.cm + 3 : nullptr);
+      NCG_LAUNCHED();
+      k_axpy3<<<nb, 256, 0, L.st>>>(dt, L.da, L.tv, n, n, L.dA, L.central ? L.tX + 3 : nullptr);
+      NCG_LAUNCHED();
+      k_axpy3<<<nb, 256, 0, L.st>>>(dt, L.V, L.X, n, n, L.cm + 3, L.central ? L.cm : nullptr);
+      NCG_LAUNCHED();
+      k_axpy3<<<nb, 256, 0, L.st>>>(dt, L.tv, L.tx, n, n, L.tX + 3, L.central ? L.tX : nullptr);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
+
 void split3(double *dst, const double *src, int n, cudaStream_t st, cudaError_t *e)
 {
       for (int d = 0; d < 3 && *e == cudaSuccess; d++)
@@ -278,19 +349,21 @@ __global__ void k_xf(const double *__restrict__ X, const double *__restrict__ V,
             for (int d = 0; d < 3; d++) out[(size_t)d * n + k] = X[(size_t)d * n + k] - h * V[(size_t)d * n + k];
 }
 
-int lf_run(const struct ncgpu_leapfrog_args *a, bool vjp)
+int lf_run(const struct ncgpu_leapfrog_args *a, int mode)
 {
+      const bool vjp = mode == 1, jvp = mode == 2;
       Ctx &c = ctx();
       const int n = a->n;
       if (n <= 0 || !a->x0 || !a->v0 || !a->m || !a->R || !a->cm || a->nsteps < 0) return NCGPU_E_ARG;
       if (vjp && (!a->adj_x_final || !a->grad_x0 || !a->grad_v0 || !a->grad_m)) return NCGPU_E_ARG;
+      if (jvp && (!a->tan_x0 || !a->tan_v0 || !a->tan_m || !a->tan_x_final)) return NCGPU_E_ARG;
       LF L{};
       L.n = n;
       L.st = c.s;
-      L.G = c.P.G;
+      L.G = c.P.par_G;
       L.M = a->cm[6];
-      L.central = c.P.central_mass_bool != 0;
-      L.soft = c.P.softening_parameter != 0.;
+      L.central = c.P.par_central_mass_bool != 0;
+      L.soft = c.P.par_softening_parameter != 0.;
       L.ntiles = (n + AT - 1) / AT;
       L.nch = std::max(1, std::min(L.ntiles, (2048 + L.ntiles - 1) / L.ntiles));
       L.tpc = (L.ntiles + L.nch - 1) / L.nch;
@@ -301,7 +374,8 @@ int lf_run(const struct ncgpu_leapfrog_args *a, bool vjp)
       const size_t N = (size_t)n, st = 6 * N + 6;
       size_t total = 3 * N * 2 + 2 * N + 6 + 3 * N + 3 * N + 4 * N * L.nch + 3 * 128 + 3  // X V m sR cm acc cterm part red acm
                      + 3 * N * 2 + 6 + 3 * N + N + N + 3 * N + 3                     // lx lv LX LV mu nu gm xterm muX
-                     + st * L.ncp + (size_t)L.C * (3 * N + 3);                        // checkpoints, segment
+                     + st * L.ncp + (size_t)L.C * (3 * N + 3)                         // checkpoints, segment
+                     + 3 * N * 3 + N + 6 + 3;                                         // tx tv tm tX da dA
       double *buf = nullptr;
       NCG_CK(cudaMalloc(&buf, total * sizeof(double)));
       double *p = buf;
@@ -312,6 +386,7 @@ int lf_run(const struct ncgpu_leapfrog_args *a, bool vjp)
       L.lx = take(3 * N); L.lv = take(3 * N); L.LX = take(3); L.LV = take(3); L.mu = take(3 * N); L.nu = take(N);
       L.gm = take(N); L.xterm = take(3 * N); L.muX = take(3);
       L.ckpt = take(st * L.ncp); L.seg = take((size_t)L.C * (3 * N + 3));
+      L.tx = take(3 * N); L.tv = take(3 * N); L.tm = take(N); L.tX = take(6); L.da = take(3 * N); L.dA = take(3);
       int status = NCGPU_OK;
       cudaError_t e = cudaSuccess;
       const double h = a->dt / 2.0, dt = a->dt;
@@ -336,8 +411,17 @@ int lf_run(const struct ncgpu_leapfrog_args *a, bool vjp)
             cudaError_t e_ = cudaGetLastError();                                      \
             if (e_ != cudaSuccess) { status = cuda_fail(e_, "launch", __FILE__, __LINE__); goto done; } \
       } while (0)
-      k_scale_R<<<nb, 256, 0, L.st>>>(L.sR, c.P.softening_parameter, L.sR, n);
+      k_scale_R<<<nb, 256, 0, L.st>>>(L.sR, c.P.par_softening_parameter, L.sR, n);
       LF_LAUNCHED();
+      if (jvp) {
+            split3(L.tx, a->tan_x0, n, L.st, &e);
+            split3(L.tv, a->tan_v0, n, L.st, &e);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(L.tm, a->tan_m, sizeof(double) * N, cudaMemcpyHostToDevice, L.st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(L.tX, 0, 6 * sizeof(double), L.st);
+            if (e != cudaSuccess) { status = cuda_fail(e, "tangent upload", __FILE__, __LINE__); goto done; }
+            k_axpy3<<<nb, 256, 0, L.st>>>(h, L.tv, L.tx, n, n, nullptr, nullptr);
+            LF_LAUNCHED();
+      }
       // half drift (src/rk4.c:873-880)
       k_axpy3<<<nb, 256, 0, L.st>>>(h, L.V, L.X, n, n, L.cm + 3, L.central ? L.cm : nullptr);
       LF_LAUNCHED();
@@ -348,7 +432,15 @@ int lf_run(const struct ncgpu_leapfrog_args *a, bool vjp)
                   if (e == cudaSuccess) e = cudaMemcpyAsync(ck + 6 * N, L.cm, 6 * sizeof(double), cudaMemcpyDeviceToDevice, L.st);
                   if (e != cudaSuccess) { status = cuda_fail(e, "checkpoint", __FILE__, __LINE__); goto done; }
             }
-            LF_TRY(lf_step(L, dt));
+            if (jvp) LF_TRY(lf_step_jvp(L, dt));
+            else LF_TRY(lf_step(L, dt));
+      }
+      if (jvp) {
+            k_xf<<<nb, 256, 0, L.st>>>(L.tx, L.tv, h, L.da, n);
+            LF_LAUNCHED();
+            join3(a->tan_x_final, L.da, n, L.st, &e);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(L.st);
+            if (e != cudaSuccess) { status = cuda_fail(e, "tangent download", __FILE__, __LINE__); goto done; }
       }
       if (a->x_final || a->v_final) {
             k_xf<<<nb, 256, 0, L.st>>>(L.X, L.V, h, L.acc, n);  // half back-drift of the output (src/rk4.c:929-936)
@@ -420,7 +512,7 @@ extern "C" int ncgpu_leapfrog(const struct ncgpu_leapfrog_args *args)
       reset_launches();
       if (!ctx().inited) return NCGPU_E_STATE;
       if (!args) return NCGPU_E_ARG;
-      return lf_run(args, false);
+      return lf_run(args, 0);
 }
 
 extern "C" int ncgpu_leapfrog_vjp(const struct ncgpu_leapfrog_args *args)
@@ -428,5 +520,13 @@ extern "C" int ncgpu_leapfrog_vjp(const struct ncgpu_leapfrog_args *args)
       reset_launches();
       if (!ctx().inited) return NCGPU_E_STATE;
       if (!args) return NCGPU_E_ARG;
-      return lf_run(args, true);
+      return lf_run(args, 1);
+}
+
+extern "C" int ncgpu_leapfrog_jvp(const struct ncgpu_leapfrog_args *args)
+{
+      reset_launches();
+      if (!ctx().inited) return NCGPU_E_STATE;
+      if (!args) return NCGPU_E_ARG;
+      return lf_run(args, 2);
 }

@@ -162,13 +162,13 @@ int kick_state()
       double cm8[8];
       NCG_TRY(state_cm_host(cm8));
       const int nslots = c.largest_id + 1;
-      if (c.P.mesh_bool && !c.force_naive)
+      if (c.P.par_mesh_bool && !c.force_naive)
             NCG_TRY(mesh_gravity_state(cm8));
       else
-            NCG_TRY(gravity_eval(state_view(), c.largest_id, cm8, c.acc, c.n_max, c.cm_acc, c.P.gravity_mode, c.s));
+            NCG_TRY(gravity_eval(state_view(), c.largest_id, cm8, c.acc, c.n_max, c.cm_acc, c.P.par_gravity_mode, c.s));
       int nb = nslots > 0 ? (nslots + 255) / 256 : 1;
       k_kick<<<nb, 256, 0, c.s>>>(c.ex, nslots, c.dt, c.acc, c.acc + c.n_max, c.acc + 2 * (size_t)c.n_max, c.vx,
-                                  c.vy, c.vz, c.cm, c.cm_acc, c.P.central_mass_bool);
+                                  c.vy, c.vz, c.cm, c.cm_acc, c.P.par_central_mass_bool);
       NCG_LAUNCHED();
       return NCGPU_OK;
 }
@@ -179,7 +179,7 @@ int drift_state()
       const int nslots = c.largest_id + 1;
       int nb = nslots > 0 ? (nslots + 255) / 256 : 1;
       k_drift<<<nb, 256, 0, c.s>>>(c.ex, nslots, c.dt, c.x, c.y, c.z, c.vx, c.vy, c.vz, c.cm,
-                                   c.P.central_mass_bool);
+                                   c.P.par_central_mass_bool);
       NCG_LAUNCHED();
       return NCGPU_OK;
 }
@@ -194,25 +194,25 @@ void ncgpu_default_params(struct ncgpu_params *p)
 {
       if (!p) return;
       memset(p, 0, sizeof *p);
-      p->G = 39.47841760435743447533796;  // src/parameters.h:131
-      p->softening_parameter = 0.;
-      p->central_mass_bool = 1;
-      p->mutual_bool = 1;
-      p->collision_bool = 1;
-      p->brute_force_bool = 1;
-      p->mesh_bool = 0;
-      p->collision_type = NCGPU_COLLISION_MERGER;
-      p->collision_parameter = 2.;
-      p->one_collision_only_bool = 0;
-      p->collision_cube_cells = 1024;
-      p->how_many_neighbours = 16.;
-      p->collision_cube_min = 80.;
-      p->switch_to_brute_force = 110;
-      p->gravity_mode = NCGPU_GRAVITY_EXACT;
-      p->near_theta = 0.25;
-      p->disruption_threshold = 1.8;     // src/parameters.h:150
-      p->high_dumping_threshold = 230.95;  // src/parameters.h:177
-      p->reduce_to_COM_bool = 1;
+      p->par_G = 39.47841760435743447533796;  // src/parameters.h:131
+      p->par_softening_parameter = 0.;
+      p->par_central_mass_bool = 1;
+      p->par_mutual_bool = 1;
+      p->par_collision_bool = 1;
+      p->par_brute_force_bool = 1;
+      p->par_mesh_bool = 0;
+      p->par_collision_type = NCGPU_COLLISION_MERGER;
+      p->par_collision_parameter = 2.;
+      p->par_one_collision_only_bool = 0;
+      p->par_collision_cube_cells = 1024;
+      p->par_how_many_neighbours = 16.;
+      p->par_collision_cube_min = 80.;
+      p->par_switch_to_brute_force = 110;
+      p->par_gravity_mode = NCGPU_GRAVITY_EXACT;
+      p->par_near_theta = 0.25;
+      p->par_disruption_threshold = 1.8;     // src/parameters.h:150
+      p->par_high_dumping_threshold = 230.95;  // src/parameters.h:177
+      p->par_reduce_to_COM_bool = 1;
 }
 
 const char *ncgpu_strerror(int s)
@@ -236,7 +236,7 @@ int ncgpu_last_launch_count(void) { return launches(); }
 int ncgpu_init(int n_max, const struct ncgpu_params *params)
 {
       if (n_max <= 0 || !params) return NCGPU_E_ARG;
-      if (params->gravity_mode < 0 || params->gravity_mode > 2) return NCGPU_E_ARG;
+      if (params->par_gravity_mode < 0 || params->par_gravity_mode > 2) return NCGPU_E_ARG;
       if (g_ctx.inited) ncgpu_finalize();
       Ctx &c = g_ctx;
       c.P = *params;
@@ -333,7 +333,7 @@ int ncgpu_last_kernel_ms(double *ms)
 int ncgpu_set_params(const struct ncgpu_params *params)
 {
       if (!g_ctx.inited) return NCGPU_E_STATE;
-      if (!params || params->gravity_mode < 0 || params->gravity_mode > 2) return NCGPU_E_ARG;
+      if (!params || params->par_gravity_mode < 0 || params->par_gravity_mode > 2) return NCGPU_E_ARG;
       g_ctx.P = *params;
       return NCGPU_OK;
 }

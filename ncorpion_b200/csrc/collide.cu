@@ -275,8 +275,8 @@ int collide_brute_state()
       int *si = c.hi + c.hit_cap / 2, *sj = c.hj + c.hit_cap / 2;  // sorted hits (upper halves)
       if (nh > c.hit_cap / 2) return NCGPU_E_CAPACITY;
       NCG_TRY(sort_hits(nh, si, sj, lid, st));
-      EvArgs E{lid, c.dt, c.P.collision_type, c.P.collision_parameter, c.P.one_collision_only_bool,
-               c.P.mesh_bool, c.ev_cap, c.n_max};
+      EvArgs E{lid, c.dt, c.P.par_collision_type, c.P.par_collision_parameter, c.P.par_one_collision_only_bool,
+               c.P.par_mesh_bool, c.ev_cap, c.n_max};
       if (E.type == NCGPU_COLLISION_FRAGMENTATION) return NCGPU_E_UNSUPPORTED;
       k_bf_events<<<1, EVT, 0, st>>>(S, si, sj, E, c.ev, c.evrec, c.dirty, c.dlist, c.err);
       NCG_LAUNCHED();

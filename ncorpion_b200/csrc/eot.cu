@@ -142,8 +142,8 @@ int eot_state(int *hm_out)
       NCG_CK(cudaMemcpyAsync(c.scal + S_HM, zero, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
       const int nb = lid >= 0 ? (lid + 256) / 256 : 1;
       int *flag = c.exs;
-      k_eot_flag<<<nb, 256, 0, st>>>(S, lid, c.cm, P.central_mass_bool, P.disruption_threshold,
-                                     P.high_dumping_threshold, flag);
+      k_eot_flag<<<nb, 256, 0, st>>>(S, lid, c.cm, P.par_central_mass_bool, P.par_disruption_threshold,
+                                     P.par_high_dumping_threshold, flag);
       NCG_LAUNCHED();
       int h[S_COUNT];
       NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
@@ -152,22 +152,22 @@ int eot_state(int *hm_out)
       if (h[S_NFLAG] > 0) {
             int nf = 0;
             NCG_TRY(compact_existing(flag, lid, &nf, st));
-            k_eot_dump<<<1, 32, 0, st>>>(S, c.cidx, nf, flag, c.cm, P.mesh_bool);
+            k_eot_dump<<<1, 32, 0, st>>>(S, c.cidx, nf, flag, c.cm, P.par_mesh_bool);
             NCG_LAUNCHED();
             NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
             NCG_CK(cudaStreamSynchronize(st));
       }
-      if (h[S_NEEDCOM] && P.reduce_to_COM_bool) {
+      if (h[S_NEEDCOM] && P.par_reduce_to_COM_bool) {
             int n = 0;
             NCG_TRY(compact_existing(c.ex, lid, &n, st));
-            k_total_momentum<<<1, 32, 0, st>>>(S, c.cidx, n, c.cm, P.central_mass_bool, c.red + 3072);
+            k_total_momentum<<<1, 32, 0, st>>>(S, c.cidx, n, c.cm, P.par_central_mass_bool, c.red + 3072);
             NCG_LAUNCHED();
-            k_sub_com<<<nb, 256, 0, st>>>(S, lid, c.red + 3072, c.cm, P.central_mass_bool);
+            k_sub_com<<<nb, 256, 0, st>>>(S, lid, c.red + 3072, c.cm, P.par_central_mass_bool);
             NCG_LAUNCHED();
             NCG_CK(cudaMemsetAsync(c.scal + S_NEEDCOM, 0, sizeof(int), st));
       }
-      if (P.mesh_bool) NCG_TRY(mesh_reset_state());  // hash table cleared (src/rk4.c:356-364)
-      if (P.collision_bool && (P.one_collision_only_bool || P.collision_type == NCGPU_COLLISION_FRAGMENTATION))
+      if (P.par_mesh_bool) NCG_TRY(mesh_reset_state());  // hash table cleared (src/rk4.c:356-364)
+      if (P.par_collision_bool && (P.par_one_collision_only_bool || P.par_collision_type == NCGPU_COLLISION_FRAGMENTATION))
             NCG_CK(cudaMemsetAsync(c.did, 0, sizeof(int) * (size_t)(lid + 1 > 0 ? lid + 1 : 1), st));
       if (hm < 9 * lid / 10) {
             int n = 0;
@@ -202,7 +202,7 @@ extern "C" int ncgpu_step_brute_force(int *how_many_moonlets)
       reset_launches();
       if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
       NCG_TRY(kick_state());
-      if (c.P.collision_bool) NCG_TRY(collide_brute_state());
+      if (c.P.par_collision_bool) NCG_TRY(collide_brute_state());
       NCG_TRY(drift_state());
       return eot_state(how_many_moonlets);
 }
@@ -216,7 +216,7 @@ extern "C" int ncgpu_step_mesh(double gam, int *how_many_moonlets, long *total_n
       if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
       if (!(gam > 0.)) return NCGPU_E_ARG;
       long tn = 0;
-      if (c.P.collision_bool) {
+      if (c.P.par_collision_bool) {
             if (c.force_naive) {
                   NCG_TRY(collide_brute_state());
             } else {
@@ -226,7 +226,7 @@ extern "C" int ncgpu_step_mesh(double gam, int *how_many_moonlets, long *total_n
             }
       }
       NCG_TRY(drift_state());
-      if (!c.P.collision_bool && !c.force_naive) {
+      if (!c.P.par_collision_bool && !c.force_naive) {
             NCG_TRY(three_largest_state(nullptr));
             NCG_TRY(mesh_pass(gam, 0));
             tn = c.total_neighbours;

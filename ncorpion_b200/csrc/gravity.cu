@@ -595,8 +595,8 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       }
       int n = 0;
       NCG_TRY(compact_existing(bv.ex, largest_id, &n, st));
-      const int central = P.central_mass_bool;
-      const double G = P.G;
+      const int central = P.par_central_mass_bool;
+      const double G = P.par_G;
       const double mu = G * cmh[6];
       if (n == 0) {
             k_set3<<<1, 1, 0, st>>>(d_cm_acc, 0., 0., 0.);
@@ -605,7 +605,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       }
       const int ntiles = (n + T - 1) / T;
       const int npad = ntiles * T;
-      const double sp = P.softening_parameter;
+      const double sp = P.par_softening_parameter;
       const bool soft = sp != 0.;
       BodyView cv = bv;
       if (mode == NCGPU_GRAVITY_EXACT) {
@@ -661,7 +661,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       // host side by the caller through near_theta's sibling field; general otherwise
       int sm = soft ? 2 : 0;
       double eps2 = 0.;
-      double theta = P.near_theta > 0. ? P.near_theta : 0.25;
+      double theta = P.par_near_theta > 0. ? P.par_near_theta : 0.25;
       dim3 grid(nchunks, ntiles);
       const float4 *s32 = (const float4 *)c.src32;
       NCG_CK(cudaEventRecord(c.kev0, st));

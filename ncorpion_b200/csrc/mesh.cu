@@ -346,7 +346,7 @@ static int mesh_alloc(int d)
             NCG_CK(cudaMalloc(&c.ckey, sizeof(int) * N));
             NCG_CK(cudaMalloc(&c.mcnt, sizeof(int) * (N + 1)));
             NCG_CK(cudaMalloc(&c.moff, sizeof(int) * (N + 2)));
-            c.pair_cap = 5L * c.n_max * (long)(c.P.how_many_neighbours > 1. ? c.P.how_many_neighbours : 16.) + 1024;
+            c.pair_cap = 5L * c.n_max * (long)(c.P.par_how_many_neighbours > 1. ? c.P.par_how_many_neighbours : 16.) + 1024;
             if (c.pair_cap > 0x7fffff00L) c.pair_cap = 0x7fffff00L;
             NCG_CK(cudaMalloc(&c.cand_k, sizeof(int) * c.pair_cap));
             NCG_CK(cudaMalloc(&c.cand_p, sizeof(int) * c.pair_cap));
@@ -394,7 +394,7 @@ int mesh_pass(double gam, int test)
 {
       Ctx &c = ctx();
       cudaStream_t st = c.s;
-      const int d = c.P.collision_cube_cells;
+      const int d = c.P.par_collision_cube_cells;
       NCG_TRY(mesh_alloc(d));
       NCG_TRY(mesh_reset_state());
       const int lid = c.largest_id;
@@ -440,8 +440,8 @@ int mesh_pass(double gam, int test)
             NCG_CK(cudaMemcpyAsync(c.keys, c.hi, sizeof(int) * (size_t)nh, cudaMemcpyDeviceToDevice, st));
             NCG_CK(cudaMemsetAsync(c.vals, 0, sizeof(int) * (size_t)nh, st));
             NCG_TRY(radix_sort_pairs(c.keys, c.vals, nh, 31, st));
-            MeshEvArgs E{lid, d, c.P.collision_type, c.P.one_collision_only_bool, c.P.mesh_bool, c.ev_cap, c.n_max,
-                         c.occ_cap, n, (long long)c.cell_cap, c.dt, c.P.collision_parameter};
+            MeshEvArgs E{lid, d, c.P.par_collision_type, c.P.par_one_collision_only_bool, c.P.par_mesh_bool, c.ev_cap, c.n_max,
+                         c.occ_cap, n, (long long)c.cell_cap, c.dt, c.P.par_collision_parameter};
             if (E.type == NCGPU_COLLISION_FRAGMENTATION) return NCGPU_E_UNSUPPORTED;
             k_mesh_events<<<1, MEV, 0, st>>>(S, c.cand_k, c.cand_p, c.cflag, c.moff, c.ckey, c.mkeys, c.mvals,
                                              c.cstart, (const int *)c.keys, nh, E, c.ev, c.evrec, c.dirty, c.occ,
@@ -455,9 +455,9 @@ int mesh_pass(double gam, int test)
             k_clear_dirty_events<<<(c.n_events + 255) / 256, 256, 0, st>>>(c.dirty, c.ev, min(c.n_events, c.ev_cap));
             NCG_LAUNCHED();
       }
-      const int merged = c.P.collision_type == NCGPU_COLLISION_MERGER ? c.n_events : 0;
+      const int merged = c.P.par_collision_type == NCGPU_COLLISION_MERGER ? c.n_events : 0;
       c.total_neighbours = (long)total - h[S_NDROP];
-      c.n_pairs = c.P.mutual_bool ? total - h[S_NDROP] - merged : 0;
+      c.n_pairs = c.P.par_mutual_bool ? total - h[S_NDROP] - merged : 0;
       c.how_many_big = h[S_NBIG];
       return NCGPU_OK;
 }

@@ -431,7 +431,7 @@ int three_largest_state(int *idx)
       int *parti = (int *)(c.red + 1792);
       k_top3_part<<<np, TB, 0, st>>>(S, lid, first3, partR, parti);
       NCG_LAUNCHED();
-      k_top3_final<<<1, 32, 0, st>>>(S, first3, partR, parti, np, c.P.mesh_bool, out);
+      k_top3_final<<<1, 32, 0, st>>>(S, first3, partR, parti, np, c.P.par_mesh_bool, out);
       NCG_LAUNCHED();
       int h[3];
       NCG_CK(cudaMemcpyAsync(h, out, sizeof h, cudaMemcpyDeviceToHost, st));
@@ -449,8 +449,8 @@ int mesh_gravity_state(const double *cm8)
       const long N = c.n_max;
       NCG_TRY(ensure_partial((size_t)12 * N));
       DevState S = dev_state();
-      MGArgs A{lid, c.P.collision_cube_cells, c.P.central_mass_bool, c.P.mutual_bool,
-               c.P.softening_parameter != 0., (long long)c.cell_cap, c.P.G, c.P.softening_parameter, c.P.G * cm8[6], cm8[0], cm8[1], cm8[2]};
+      MGArgs A{lid, c.P.par_collision_cube_cells, c.P.par_central_mass_bool, c.P.par_mutual_bool,
+               c.P.par_softening_parameter != 0., (long long)c.cell_cap, c.P.par_G, c.P.par_softening_parameter, c.P.par_G * cm8[6], cm8[0], cm8[1], cm8[2]};
       double *ax = c.acc, *ay = c.acc + N, *az = c.acc + 2 * N;
       if (lid >= 0) {
             k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.cstart, c.mesh_valid, ax,
@@ -458,7 +458,7 @@ int mesh_gravity_state(const double *cm8)
             NCG_LAUNCHED();
       }
       double *tot = c.red + 3584;
-      if (c.P.gravity_mode == NCGPU_GRAVITY_EXACT) {
+      if (c.P.par_gravity_mode == NCGPU_GRAVITY_EXACT) {
             k_mesh_chains<<<1, 384, 0, st>>>(S, A, c.partial, N, ax, ay, az, tot);
             NCG_LAUNCHED();
       } else {

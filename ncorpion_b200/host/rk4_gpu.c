@@ -1,0 +1,377 @@
+/*
+ * rk4_gpu.c - GPU drivers for NcorpiON's brute-force and mesh integrations.
+ *
+ * Drop-in replacements of integration_brute_force_SABA1 (src/rk4.c:840-954)
+ * and integration_mesh (src/rk4.c:662-837).  They are compiled against the
+ * reference's own headers (parameters.h, structure.h, rk4.h, display.h ...)
+ * and linked with its objects and libncgpu.so; main.c reaches them through
+ *     -Dintegration_brute_force_SABA1=ncgpu_integration_brute_force_SABA1
+ *     -Dintegration_mesh=ncgpu_integration_mesh
+ * on main.c's compile line only (the reference's rk4.o keeps its own copies).
+ *
+ * Bodies live on the GPU between calls.  The host keeps what the reference
+ * keeps on the host: initial conditions (populate), output files (display,
+ * readme, resume), the progress printout, the mesh size gamma (updated with
+ * the host's libm pow) and the brute-force switch.  At every output step and
+ * every step whose progress is printed the state is copied back, and the
+ * reference's own end_of_timestep runs on the host copy for its printout and
+ * gamma update; the dumping, barycentre reduction and tidy_up it would do have
+ * already been done by the device, so on the host copy they find nothing to do.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "parameters.h"
+#include "structure.h"
+#include "physics.h"
+#include "collision.h"
+#include "rk4.h"
+#include "display.h"
+#include "ncgpu.h"
+
+static void gpu_check(int status, const char *what)
+{
+      if (status != NCGPU_OK) {
+            fprintf(stderr, "Error : %s failed on the GPU: %s", what, ncgpu_strerror(status));
+            if (status == NCGPU_E_CUDA) fprintf(stderr, " (%s)", ncgpu_last_error());
+            fprintf(stderr, "\n");
+            abort();
+      }
+}
+
+/* struct ncgpu_params from the parameters.h macros */
+static void gpu_params(struct ncgpu_params *p)
+{
+      ncgpu_default_params(p);
+      p->par_G = G;
+      p->par_softening_parameter = softening_parameter;
+      p->par_central_mass_bool = central_mass_bool;
+      p->par_mutual_bool = mutual_bool;
+      p->par_collision_bool = collision_bool;
+      p->par_brute_force_bool = brute_force_bool;
+      p->par_mesh_bool = mesh_bool;
+      p->par_collision_type = elastic_collision_bool ? NCGPU_COLLISION_ELASTIC
+                        : inelastic_collision_bool ? NCGPU_COLLISION_INELASTIC
+                        : instant_merger_bool ? NCGPU_COLLISION_MERGER : NCGPU_COLLISION_FRAGMENTATION;
+      p->par_collision_parameter = collision_parameter;
+      p->par_one_collision_only_bool = one_collision_only_bool;
+#if mesh_bool
+      p->par_collision_cube_cells = collision_cube_cells;
+      p->par_how_many_neighbours = how_many_neighbours;
+      p->par_collision_cube_min = collision_cube_min;
+#endif
+      p->par_switch_to_brute_force = switch_to_brute_force;
+      p->par_gravity_mode = NCGPU_GRAVITY_EXACT;
+      p->par_disruption_threshold = disruption_threshold;
+      p->par_high_dumping_threshold = high_dumping_threshold;
+      p->par_reduce_to_COM_bool = reduce_to_COM_bool;
+}
+
+/* The GPU path covers the configurations of its hot path only. */
+static void gpu_supported(void)
+{
+      if (J2_bool || central_tides_bool || inner_fluid_disk_bool || viscoelastic_bool || pert_mass > 0. ||
+          openGL_bool) {
+            fprintf(stderr, "Error : the GPU integration does not cover J2, tides, the inner fluid disk, the "
+                            "viscoelastic body, the perturber or the 3D viewer.\n");
+            abort();
+      }
+}
+
+static void gpu_upload(struct moonlet *moonlets)
+{
+      gpu_check(ncgpu_upload((const struct ncgpu_body *)moonlets, exists, largest_id, (const struct ncgpu_body *)&CM),
+                "upload");
+}
+
+/* device state -> host arrays and the reference's globals */
+static void gpu_pull(struct moonlet *moonlets)
+{
+      int lid;
+      gpu_check(ncgpu_download((struct ncgpu_body *)moonlets, exists, &lid, (struct ncgpu_body *)&CM), "download");
+      for (int j = lid + 1; j <= largest_id && j < N_max; j++) exists[j] = 0;
+      largest_id = lid;
+}
+
+/* The collision records of the last sweep appended to collisionDatas, as
+   collision() and merger() fill them (src/physics.c:608-622, 685-704). */
+static void gpu_collision_records(double t_now)
+{
+      int n = 0;
+      gpu_check(ncgpu_get_events(NULL, NULL, 0, &n), "events");
+      if (n == 0) return;
+      struct ncgpu_event *ev = (struct ncgpu_event *)malloc(sizeof(struct ncgpu_event) * (size_t)n);
+      double *rec = (double *)malloc(sizeof(double) * 8 * (size_t)n);
+      gpu_check(ncgpu_get_events(ev, rec, n, &n), "events");
+#if write_collisions_bool
+      if (write_to_files_bool) {
+            for (int e = 0; e < n; e++) {
+                  const double *r = rec + 8 * e;
+                  double t = r[0], mA = r[1], mB = r[2], RA = r[3], RB = r[4], dV = r[5], drdv = r[6];
+                  (collisionDatas + indexCollision)->time = t_now + t;
+                  (collisionDatas + indexCollision)->m1 = mB;
+                  (collisionDatas + indexCollision)->m2 = mA;
+                  (collisionDatas + indexCollision)->R1 = RB;
+                  (collisionDatas + indexCollision)->R2 = RA;
+                  (collisionDatas + indexCollision)->DeltaV = dV;
+                  (collisionDatas + indexCollision)->impact_angle = acos(-drdv / ((RA + RB) * dV));
+                  (collisionDatas + indexCollision)->m_tilde = ev[e].type == NCGPU_COLLISION_MERGER ? mA + mB : mA;
+                  indexCollision++;
+                  if (indexCollision == 2 * output_step * N_max) {
+                        fprintf(stderr, "Error: The array collisionDatas is not large enough.\n");
+                        abort();
+                  }
+            }
+      }
+#endif
+      free(ev);
+      free(rec);
+}
+
+static int gpu_collide_brute(double t_now)
+{
+      int n = 0;
+      gpu_check(ncgpu_set_timestep(timestep), "timestep");
+      gpu_check(ncgpu_collide_brute(&n), "brute_force");
+      collision_count += n;
+      gpu_collision_records(t_now);
+      return n;
+}
+
+/* end of a step on the device, then the host's share: how_many_moonlets, the
+   brute-force switch (src/rk4.c:388-393) and, in mesh mode, gamma
+   (src/rk4.c:367-372); the reference's own end_of_timestep on a fresh host
+   copy when the step's progress is printed. */
+static void gpu_end_of_timestep(struct moonlet *moonlets, int progressed, long total_nb)
+{
+      int hm = 0;
+      gpu_check(ncgpu_end_of_timestep(&hm), "end_of_timestep");
+      if (progressed) {
+            gpu_pull(moonlets);
+#if mesh_bool
+            total_neighbours = (int)total_nb;
+#endif
+            end_of_timestep(moonlets, progressed);
+      } else {
+            how_many_moonlets = hm;
+            first_passage = 1;
+#if mesh_bool
+            if ((collision_bool || mutual_bool) && !force_naive_bool) {
+                  average_neighbours = 2.0 * ((typ)total_nb) / ((typ)how_many_moonlets);
+                  gam *= pow(how_many_neighbours / average_neighbours, 1.0 / 3.0);
+                  if (gam < gam_min) gam = gam_min;
+                  collision_cube = gam * ((typ)collision_cube_cells);
+            }
+            how_many_pairs = 0;
+            total_neighbours = 0;
+#endif
+            if (!brute_force_bool && !force_naive_bool && how_many_moonlets < switch_to_brute_force)
+                  force_naive_bool = 1;
+            else if (!brute_force_bool && force_naive_bool && how_many_moonlets > switch_to_brute_force)
+                  force_naive_bool = 0;
+      }
+      gpu_check(ncgpu_set_force_naive(force_naive_bool), "force_naive");
+      (void)total_nb;
+}
+
+static void gpu_start(struct moonlet **moonlets, struct moonlet **buffer)
+{
+      struct ncgpu_params p;
+      gpu_supported();
+      *moonlets = populate();
+      *buffer = (struct moonlet *)malloc(N_max * sizeof(struct moonlet));
+      if (*buffer == NULL) {
+            fprintf(stderr, "Error : Can't allocate buffer for array of bodies.\n");
+            abort();
+      }
+      gpu_params(&p);
+      gpu_check(ncgpu_init(N_max, &p), "init");
+      gpu_check(ncgpu_host_register(*moonlets, sizeof(struct moonlet) * (unsigned long)N_max), "host register");
+      gpu_upload(*moonlets);
+      gpu_check(ncgpu_set_timestep(timestep), "timestep");
+      gpu_check(ncgpu_set_force_naive(force_naive_bool), "force_naive");
+}
+
+static void gpu_stop(struct moonlet *moonlets, struct moonlet *buffer, bigint iter)
+{
+      if (write_to_files_bool) display(moonlets);
+      if (resume_simulation_bool) {
+            resume(moonlets);
+            resumeFile();
+      }
+      printf("progress = %.1lf %%\n", 100.0);
+      printf("total number of timestep performed : %ld\n", iter);
+      ncgpu_host_unregister(moonlets);
+      ncgpu_finalize();
+      free(moonlets);
+      free(buffer);
+}
+
+/* integration_brute_force_SABA1 (src/rk4.c:840-954) */
+void ncgpu_integration_brute_force_SABA1(typ t)
+{
+      struct moonlet *moonlets, *moonlet_buffer;
+      bigint iter = 0;
+      int progressed = 0, j;
+      typ progress = 0.0, previous_progress = 0.0;
+      gpu_start(&moonlets, &moonlet_buffer);
+      printf("progress = %.1lf %%\n", 0.0);
+      if (write_to_files_bool) {
+            readme();
+            if (central_mass_bool) CM_buffer = CM;
+            display(moonlets);
+      }
+      if (t > 0.0) {  /* half drift */
+            timestep /= 2.0;
+            if (collision_bool) gpu_collide_brute(t_init + time_elapsed);
+            gpu_check(ncgpu_set_timestep(timestep), "timestep");
+            gpu_check(ncgpu_drift(), "drift");
+            timestep *= 2.0;
+            gpu_check(ncgpu_set_timestep(timestep), "timestep");
+      }
+      while (time_elapsed < t) {
+            progressed = 0;
+            if (write_to_files_bool && iter % output_step == 0 && iter > 0) {
+                  gpu_pull(moonlets);
+                  for (j = 0; j <= largest_id; j++)
+                        if (exists[j]) moonlet_buffer[j] = moonlets[j];
+                  if (central_mass_bool) CM_buffer = CM;
+                  timestep /= -2.0;
+                  drift(moonlet_buffer, &CM_buffer);  /* half backward drift, host copy */
+                  timestep *= -2.0;
+                  display(moonlet_buffer);
+            }
+            gpu_check(ncgpu_kick(), "kick");
+            time_elapsed += .5 * timestep;
+            if (collision_bool) gpu_collide_brute(t_init + time_elapsed);
+            gpu_check(ncgpu_drift(), "drift");
+            iter++;
+            time_elapsed += .5 * timestep;
+            progress = time_elapsed / t;
+            if (progress - previous_progress > .001) {
+                  previous_progress = progress;
+                  printf("progress = %.1lf %%\n", 100. * progress);
+                  progressed = 1;
+            }
+            gpu_end_of_timestep(moonlets, progressed, 0);
+      }
+      gpu_pull(moonlets);
+      if (central_mass_bool) CM_buffer = CM;
+      if (t > 0.) {  /* half backward drift of the final output */
+            timestep /= -2.;
+            drift(moonlets, &CM_buffer);
+            timestep *= -2.;
+      }
+      gpu_stop(moonlets, moonlet_buffer, iter);
+}
+
+#if mesh_bool
+/* three largest to slots 0-2, one mesh pass; returns total_neighbours */
+static long gpu_mesh_pass(int with_collisions)
+{
+      int np = 0, ne = 0;
+      long tn = 0;
+      gpu_check(ncgpu_three_largest(NULL), "three_largest");
+      gpu_check(ncgpu_set_timestep(timestep), "timestep");
+      gpu_check(ncgpu_mesh(gam, with_collisions, &np, &ne, &tn), "mesh");
+      if (with_collisions) {
+            collision_count += ne;
+            gpu_collision_records(t_init + time_elapsed);
+      }
+      return tn;
+}
+
+/* integration_mesh (src/rk4.c:662-837) */
+void ncgpu_integration_mesh(typ t)
+{
+      struct moonlet *moonlets, *moonlet_buffer;
+      bigint iter = 0;
+      int progressed = 0, j, index;
+      typ progress = 0.0, previous_progress = 0.0;
+      long tn;
+      gpu_start(&moonlets, &moonlet_buffer);
+      printf("progress = %.1lf %%\n", 0.0);
+      if (write_to_files_bool) {
+            readme();
+            if (central_mass_bool) CM_buffer = CM;
+            display(moonlets);
+      }
+      if (t > 0.0) {  /* half kick */
+            timestep /= 2.0;
+            tn = gpu_mesh_pass(0);
+            gpu_check(ncgpu_kick(), "kick");
+            gpu_check(ncgpu_mesh_reset(), "mesh reset");
+            timestep *= 2.0;
+            gpu_check(ncgpu_set_timestep(timestep), "timestep");
+            average_neighbours = 2.0 * ((typ)tn) / ((typ)how_many_moonlets);
+            gam *= pow(how_many_neighbours / average_neighbours, 1.0 / 3.0);
+            if (gam < gam_min) gam = gam_min;
+            collision_cube = gam * ((typ)collision_cube_cells);
+            how_many_pairs = 0;
+            total_neighbours = 0;
+      }
+      while (time_elapsed < t) {
+            progressed = 0;
+            if (write_to_files_bool && iter % output_step == 0 && iter > 0) {
+                  /* half backward kick of a host copy with the reference's own code */
+                  gpu_pull(moonlets);
+                  for (j = 0; j <= largest_id; j++)
+                        if (exists[j]) moonlet_buffer[j] = moonlets[j];
+                  if (central_mass_bool) CM_buffer = CM;
+                  timestep /= -2.0;
+                  if (!force_naive_bool) {
+                        three_largest_moonlets(moonlet_buffer);
+                        three_largest_three_first(moonlet_buffer);
+                        get_neighbours_mesh(moonlet_buffer);
+                  }
+                  kick(moonlet_buffer, &CM_buffer, vector_field);
+                  timestep *= -2.0;
+                  display(moonlet_buffer);
+                  if (!force_naive_bool) {
+                        for (j = 0; j < how_many_modified; j++) {
+                              index = modified_cells[j];
+                              clear_chain(hash + index);
+                        }
+                        how_many_pairs = 0;
+                        how_many_modified = 0;
+                        total_neighbours = 0;
+                  }
+                  gpu_upload(moonlets);  /* exists[] may have changed (slots 0-2 refilled) */
+            }
+            tn = 0;
+            if (collision_bool) {
+                  if (force_naive_bool) gpu_collide_brute(t_init + time_elapsed);
+                  else tn = gpu_mesh_pass(1);
+            }
+            gpu_check(ncgpu_set_timestep(timestep), "timestep");
+            gpu_check(ncgpu_drift(), "drift");
+            time_elapsed += 0.5 * timestep;
+            if (!collision_bool && !force_naive_bool) tn = gpu_mesh_pass(0);
+            gpu_check(ncgpu_kick(), "kick");
+            iter++;
+            time_elapsed += 0.5 * timestep;
+            progress = time_elapsed / t;
+            if (progress - previous_progress > 0.001) {
+                  previous_progress = progress;
+                  printf("progress = %.1lf %%\n", 100.0 * progress);
+                  progressed = 1;
+            }
+            gpu_end_of_timestep(moonlets, progressed, tn);
+      }
+      if (central_mass_bool) CM_buffer = CM;
+      if (t > 0.0) {  /* half backward kick of the final state (the central mass kick goes to CM_buffer) */
+            gpu_pull(moonlets);
+            if (central_mass_bool) CM_buffer = CM;
+            timestep /= -2.0;
+            if (!force_naive_bool) {
+                  three_largest_moonlets(moonlets);
+                  three_largest_three_first(moonlets);
+                  get_neighbours_mesh(moonlets);
+            }
+            kick(moonlets, &CM_buffer, vector_field);
+            timestep *= -2.0;
+      }
+      gpu_stop(moonlets, moonlet_buffer, iter);
+}
+#endif

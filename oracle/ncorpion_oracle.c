@@ -28,9 +28,9 @@ void orc_vector_field(int lid, const body *b, const int *ex, const body *cm, con
                       double *acc, double *cm_acc)
 {
       int k, p;
-      const double G = P->G;
-      const double XX = P->central_mass_bool ? cm->x : 0., YY = P->central_mass_bool ? cm->y : 0.,
-                   ZZ = P->central_mass_bool ? cm->z : 0.;
+      const double G = P->par_G;
+      const double XX = P->par_central_mass_bool ? cm->x : 0., YY = P->par_central_mass_bool ? cm->y : 0.,
+                   ZZ = P->par_central_mass_bool ? cm->z : 0.;
       const double M = cm->mass;
       cm_acc[0] = cm_acc[1] = cm_acc[2] = 0.;
       for (k = 0; k <= lid; k++) {
@@ -44,7 +44,7 @@ void orc_vector_field(int lid, const body *b, const int *ex, const body *cm, con
             double r3 = rk * rk * rk;
             double mu = G * M;
             double aX, aY, aZ;
-            if (P->central_mass_bool) {            /* src/physics.c:133-146 */
+            if (P->par_central_mass_bool) {            /* src/physics.c:133-146 */
                   aX = -mu * DX / r3;
                   aY = -mu * DY / r3;
                   aZ = -mu * DZ / r3;
@@ -54,13 +54,13 @@ void orc_vector_field(int lid, const body *b, const int *ex, const body *cm, con
             } else {
                   aX = aY = aZ = 0.;
             }
-            if (P->mutual_bool) {                  /* src/physics.c:174-202 */
+            if (P->par_mutual_bool) {                  /* src/physics.c:174-202 */
                   for (p = 0; p < k; p++) {
                         if (!ex[p]) continue;
                         double mp = b[p].mass, Xp = b[p].x, Yp = b[p].y, Zp = b[p].z;
                         double Rp = b[p].radius, Rk = b[k].radius;
                         double dx = X - Xp, dy = Y - Yp, dz = Z - Zp;
-                        double soft = P->softening_parameter * (Rk + Rp);
+                        double soft = P->par_softening_parameter * (Rk + Rp);
                         double D = sqrt(dx * dx + dy * dy + dz * dz + soft * soft);
                         double D3 = D * D * D;
                         aX -= G * mp * dx / D3;
@@ -90,7 +90,7 @@ void orc_kick(int lid, body *b, const int *ex, body *cm, double dt, const struct
             b[i].vy += dt * acc[3 * i + 1];
             b[i].vz += dt * acc[3 * i + 2];
       }
-      if (P->central_mass_bool) {
+      if (P->par_central_mass_bool) {
             cm->vx += dt * cma[0];
             cm->vy += dt * cma[1];
             cm->vz += dt * cma[2];
@@ -108,7 +108,7 @@ void orc_drift(int lid, body *b, const int *ex, body *cm, double dt, const struc
             b[i].y += dt * b[i].vy;
             b[i].z += dt * b[i].vz;
       }
-      if (P->central_mass_bool) {
+      if (P->par_central_mass_bool) {
             cm->x += dt * cm->vx;
             cm->y += dt * cm->vy;
             cm->z += dt * cm->vz;
@@ -171,7 +171,7 @@ int orc_w_init(int n_max, const struct ncgpu_params *P)
       W.ex = (int *)calloc((size_t)n_max, sizeof(int));
       W.did = (int *)calloc((size_t)n_max, sizeof(int));
       W.free_idx = (int *)calloc((size_t)n_max, sizeof(int));
-      W.pair_cap = 5L * n_max * (long)P->how_many_neighbours + 64;
+      W.pair_cap = 5L * n_max * (long)P->par_how_many_neighbours + 64;
       W.pairs = (int *)malloc(sizeof(int) * 2 * (size_t)W.pair_cap);
       W.hcap = 1;
       while (W.hcap < 4L * n_max) W.hcap <<= 1;
@@ -236,7 +236,7 @@ static void lose(int a)
 {
       W.free_idx[W.n_free++] = a;
       W.ex[a] = 0;
-      if (a <= 2 && W.P.mesh_bool) W.n_free--;
+      if (a <= 2 && W.P.par_mesh_bool) W.n_free--;
 }
 
 /* closest_approach (src/collision.c:63-172); returns 1 and fills W.approach
@@ -312,7 +312,7 @@ static void merge(int a, int b)
       A->mass = m;
       A->radius = pow(3.0 * m / (4.0 * M_PI * avg), 1.0 / 3.0);
       lose(b);
-      W.did[a] = W.P.one_collision_only_bool;
+      W.did[a] = W.P.par_one_collision_only_bool;
 }
 
 /* collision_treatment (src/physics.c:1043-1091), types 0..2 */
@@ -323,10 +323,10 @@ static void treat(int a, int b, int type)
       push_event(a, b, type);
       if (!(W.ex[a] && W.ex[b])) return;
       if (type == 0 || type == 1) {
-            impulse(A, B, type == 0 ? 2.0 : W.P.collision_parameter);
-            W.did[a] = W.P.one_collision_only_bool;
-            W.did[b] = W.P.one_collision_only_bool;
-            if (W.P.mutual_bool && W.P.mesh_bool) {
+            impulse(A, B, type == 0 ? 2.0 : W.P.par_collision_parameter);
+            W.did[a] = W.P.par_one_collision_only_bool;
+            W.did[b] = W.P.par_one_collision_only_bool;
+            if (W.P.par_mutual_bool && W.P.par_mesh_bool) {
                   W.pairs[2 * W.n_pairs] = a;
                   W.pairs[2 * W.n_pairs + 1] = b;
                   W.n_pairs++;
@@ -345,7 +345,7 @@ void orc_w_brute_force(void)
             if (!W.ex[i]) continue;
             for (j = i + 1; j <= W.lid; j++) {
                   if (!W.ex[j]) continue;
-                  if (approach(i, j) && !W.did[i] && !W.did[j]) treat(i, j, W.P.collision_type);
+                  if (approach(i, j) && !W.did[i] && !W.did[j]) treat(i, j, W.P.par_collision_type);
             }
       }
 }
@@ -384,7 +384,7 @@ static void hash_clear(void)
    that pop order and inserts k into its own cell. */
 static int query_insert(int k, int *out)
 {
-      int d = W.P.collision_cube_cells;
+      int d = W.P.par_collision_cube_cells;
       long L = orc_cell_index(W.b[k].x, W.b[k].y, W.b[k].z, W.gam, d);
       if (L < 0) return 0;
       int n = 0;
@@ -435,9 +435,9 @@ void orc_w_mesh(void)
                         p = nb[q];
                         int hit = approach(p, k);
                         if (!hit || W.did[k] || W.did[p]) {
-                              if (W.P.mutual_bool) add_pair(k, p);
+                              if (W.P.par_mutual_bool) add_pair(k, p);
                         } else {
-                              treat(p, k, W.P.collision_type);
+                              treat(p, k, W.P.par_collision_type);
                         }
                         W.total_neighbours++;
                   }
@@ -449,9 +449,9 @@ void orc_w_mesh(void)
                         if (Rp < gam || (Rp >= gam && p > k)) {
                               int hit = approach(p, k);
                               if (!hit || W.did[k] || W.did[p]) {
-                                    if (W.P.mutual_bool) add_pair(k, p);
+                                    if (W.P.par_mutual_bool) add_pair(k, p);
                               } else {
-                                    treat(p, k, W.P.collision_type);
+                                    treat(p, k, W.P.par_collision_type);
                               }
                         }
                   }
@@ -542,7 +542,7 @@ static int need_to_reduce_com = 0;
 /* total_momentum (src/structure.c:1193-1227) */
 static void total_momentum(double *mom)
 {
-      const int c = W.P.central_mass_bool;
+      const int c = W.P.par_central_mass_bool;
       double X = c ? W.cm.x : 0., Y = c ? W.cm.y : 0., Z = c ? W.cm.z : 0.;
       double vX = c ? W.cm.vx : 0., vY = c ? W.cm.vy : 0., vZ = c ? W.cm.vz : 0.;
       double M = c ? W.cm.mass : 0.;
@@ -579,7 +579,7 @@ static void tidy_up(void)
 int orc_w_end_of_timestep(void)
 {
       int j, hm = 0;
-      const int c = W.P.central_mass_bool;
+      const int c = W.P.par_central_mass_bool;
       double XX = c ? W.cm.x : 0., YY = c ? W.cm.y : 0., ZZ = c ? W.cm.z : 0.;
       for (j = 0; j <= W.lid; j++) {
             if (!W.ex[j]) continue;
@@ -587,7 +587,7 @@ int orc_w_end_of_timestep(void)
             double X = B->x, Y = B->y, Z = B->z, m = B->mass;
             double DX = X - XX, DY = Y - YY, DZ = Z - ZZ;
             int losing = 0;
-            if (DX * DX + DY * DY + DZ * DZ < W.P.disruption_threshold * W.P.disruption_threshold && c) {
+            if (DX * DX + DY * DY + DZ * DZ < W.P.par_disruption_threshold * W.P.par_disruption_threshold && c) {
                   double vX = B->vx, vY = B->vy, vZ = B->vz;
                   W.cm.mass += m;
                   double M = W.cm.mass;
@@ -597,14 +597,14 @@ int orc_w_end_of_timestep(void)
                   W.cm.vx += m * vX / M; W.cm.vy += m * vY / M; W.cm.vz += m * vZ / M;
                   lose(j);
                   losing = 1;
-            } else if (DX * DX + DY * DY + DZ * DZ > W.P.high_dumping_threshold * W.P.high_dumping_threshold) {
+            } else if (DX * DX + DY * DY + DZ * DZ > W.P.par_high_dumping_threshold * W.P.par_high_dumping_threshold) {
                   lose(j);
                   losing = 1;
                   need_to_reduce_com = 1;
             }
             if (!losing) hm++;
       }
-      if (need_to_reduce_com && W.P.reduce_to_COM_bool) {
+      if (need_to_reduce_com && W.P.par_reduce_to_COM_bool) {
             double com[6];
             total_momentum(com);
             if (c) {
@@ -618,7 +618,7 @@ int orc_w_end_of_timestep(void)
             }
             need_to_reduce_com = 0;
       }
-      if (W.P.collision_bool && (W.P.one_collision_only_bool || W.P.collision_type == 3))
+      if (W.P.par_collision_bool && (W.P.par_one_collision_only_bool || W.P.par_collision_type == 3))
             for (j = 0; j <= W.lid; j++) W.did[j] = 0;
       if (hm < 9 * W.lid / 10) tidy_up();
       return hm;
@@ -633,7 +633,7 @@ void orc_w_drift(void) { orc_drift(W.lid, W.b, W.ex, &W.cm, W.dt, &W.P); }
 int orc_w_step_brute_force(void)
 {
       orc_w_kick();
-      if (W.P.collision_bool) orc_w_brute_force();
+      if (W.P.par_collision_bool) orc_w_brute_force();
       orc_w_drift();
       return orc_w_end_of_timestep();
 }
@@ -644,8 +644,8 @@ int orc_w_step_brute_force(void)
 void orc_w_vector_field_mesh(double *acc, double *cm_acc)
 {
       int k, p, j;
-      const double G = W.P.G, sp = W.P.softening_parameter;
-      const int c = W.P.central_mass_bool, mut = W.P.mutual_bool;
+      const double G = W.P.par_G, sp = W.P.par_softening_parameter;
+      const int c = W.P.par_central_mass_bool, mut = W.P.par_mutual_bool;
       const body *b = W.b;
       const int *ex = W.ex;
       double XX = c ? W.cm.x : 0., YY = c ? W.cm.y : 0., ZZ = c ? W.cm.z : 0.;
@@ -719,7 +719,7 @@ void orc_w_kick_mesh(void)
             W.b[i].vy += W.dt * acc[3 * i + 1];
             W.b[i].vz += W.dt * acc[3 * i + 2];
       }
-      if (W.P.central_mass_bool) {
+      if (W.P.par_central_mass_bool) {
             W.cm.vx += W.dt * cma[0];
             W.cm.vy += W.dt * cma[1];
             W.cm.vz += W.dt * cma[2];
@@ -734,12 +734,12 @@ long orc_w_step_mesh(void)
       int idx[3];
       long tn;
       orc_w_mesh_reset();
-      if (W.P.collision_bool) {
+      if (W.P.par_collision_bool) {
             orc_w_three_largest(idx);
             orc_w_mesh();
       }
       orc_w_drift();
-      if (!W.P.collision_bool) {
+      if (!W.P.par_collision_bool) {
             orc_w_three_largest(idx);
             orc_w_get_neighbours_mesh();
       }

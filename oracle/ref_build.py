@@ -17,7 +17,10 @@ For each profile below this script
      wrapped to log the resolution order;
    * ``oracle/_ref/<profile>/ncorpion`` = the full reference program
      (``main.c`` included), reading ``./init.txt`` and writing its output
-     files into the working directory (``pth`` = ``"./"``).
+     files into the working directory (``pth`` = ``"./"``);
+   * ``oracle/_ref/<profile>/ncorpion_gpu`` (brute-force and mesh profiles) =
+     the same program with its two integration drivers taken from
+     ``ncorpion_b200/host/rk4_gpu.c`` on ``libncgpu.so`` (the drop-in build).
 
 Only build outputs are written under ``oracle/_ref/`` (git-ignored); the
 temporary copy is deleted.  The shipped prebuilt ``src/ncorpion`` is never
@@ -157,6 +160,8 @@ def build(profile: str, src: str, verbose: bool = False) -> str:
         exe = os.path.join(dst, "ncorpion")
         subprocess.run(["gcc", *CFLAGS, "main.c", *[f"{u}.o" for u in units], "-lm", "-o", exe],
                        cwd=tmp, check=True)
+        if ov.get("brute_force_bool") == "1" or ov.get("mesh_bool") == "1":
+            build_dropin(tmp, dst, units)
         with open(os.path.join(dst, "profile.txt"), "w") as f:
             for k in sorted(ov):
                 f.write(f"{k} {ov[k]}\n")
@@ -165,6 +170,27 @@ def build(profile: str, src: str, verbose: bool = False) -> str:
         return dst
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+
+
+def build_dropin(tmp: str, dst: str, units) -> None:
+    """The reference program with its brute-force and mesh integrations
+    replaced by ncorpion_b200/host/rk4_gpu.c on libncgpu.so: main.c is
+    compiled with its two dispatch calls redirected, every other object is the
+    reference's own."""
+    root = os.path.dirname(HERE)
+    pkg = os.path.join(root, "ncorpion_b200")
+    lib = os.path.join(pkg, "libncgpu.so")
+    if not os.path.exists(lib):
+        raise RuntimeError("build libncgpu.so first (python -m ncorpion_b200.build)")
+    redirect = ["-Dintegration_brute_force_SABA1=ncgpu_integration_brute_force_SABA1",
+                "-Dintegration_mesh=ncgpu_integration_mesh"]
+    subprocess.run(["gcc", *CFLAGS, *redirect, "-c", "main.c", "-o", "main_gpu.o"], cwd=tmp, check=True)
+    subprocess.run(["gcc", *CFLAGS, "-I", tmp, "-I", os.path.join(root, "include"), "-c",
+                    os.path.join(pkg, "host", "rk4_gpu.c"), "-o", "rk4_gpu.o"], cwd=tmp, check=True)
+    rel = os.path.relpath(pkg, dst)
+    subprocess.run(["gcc", "main_gpu.o", "rk4_gpu.o", *[f"{u}.o" for u in units], "-L", pkg, "-lncgpu",
+                    f"-Wl,-rpath,$ORIGIN/{rel}", "-lm", "-o", os.path.join(dst, "ncorpion_gpu")],
+                   cwd=tmp, check=True)
 
 
 def main(argv=None) -> int:

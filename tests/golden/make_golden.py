@@ -114,6 +114,34 @@ def mesh_case(profile, n, seed, gam, dt):
     return out
 
 
+OUTPUT_FILES = ["stat.txt", "collision.txt", "mass.txt", "radius.txt", "x.txt", "y.txt", "z.txt", "vx.txt",
+                "vy.txt", "vz.txt", "readme.txt"]
+
+
+def filtered_stdout(text):
+    """The program's console output without its wall-clock timing line."""
+    return "\n".join(l for l in text.splitlines() if "integration took" not in l)
+
+
+def program_run_case(profile, bodies):
+    """The whole reference program (oracle/_ref/<profile>/ncorpion) run on
+    init.txt: digests of every output file and of the console output."""
+    import subprocess
+    import tempfile
+    d = tempfile.mkdtemp(prefix="ncref_run_")
+    disks.write_init_txt(os.path.join(d, "init.txt"), bodies)
+    exe = os.path.join(ROOT, "oracle", "_ref", profile, "ncorpion")
+    r = subprocess.run([exe], cwd=d, capture_output=True, text=True, check=True)
+    out = dict(bodies=bodies)
+    for f in OUTPUT_FILES:
+        data = open(os.path.join(d, f), "rb").read()
+        out["digest_" + f] = digest(np.frombuffer(data, np.uint8))
+    out["digest_stdout"] = digest(np.frombuffer(filtered_stdout(r.stdout).encode(), np.uint8))
+    out["collision_txt"] = np.frombuffer(open(os.path.join(d, "collision.txt"), "rb").read(), np.uint8)
+    out["stat_txt"] = np.frombuffer(open(os.path.join(d, "stat.txt"), "rb").read(), np.uint8)
+    return out
+
+
 def main():
     out = {}
     out["grav_s05_n512"] = gravity_case("bf_grav_s05", 512, 11, holes=(3, 100, 511))
@@ -127,6 +155,8 @@ def main():
     out["bf_run_merge"] = bf_run_case("bf_merge", 2000, 0, 40)
     out["mesh_merge"] = mesh_case("mesh_merge_s", 6000, 21, 0.03, 5e-4)
     out["mesh_inelastic"] = mesh_case("mesh_inelastic_s", 6000, 22, 0.03, 5e-4)
+    # the N = 2,000 collisional disk, 200 steps, output every 50 steps
+    out["program_bf_merge"] = program_run_case("bf_merge", disks.bf_collide_disk(2000, seed=0))
     for k, v in out.items():
         np.savez_compressed(os.path.join(HERE, k + ".npz"), **v)
         print("wrote", k)

@@ -5,8 +5,13 @@ Tolerances:
   forward     final positions vs the oracle's exact-FP64 integrator loop:
               max relative difference <= 1e-10 (the forward sums pairs with
               one FP64 rsqrt instead of the reference's sqrt and divisions);
-  gradients   vs FP64 central finite differences of the same forward:
-              relative error <= 1e-5 per checked coordinate.
+  x0, v0      vs FP64 central finite differences of the same forward (h = 1e-6):
+              relative error <= 1e-5 per checked coordinate;
+  m           vs the tangent-linear model (ncgpu_leapfrog_jvp, exact to
+              rounding): relative error <= 1e-8.  FP64 finite differences of
+              the masses (1e-9 .. 1e-6) drown in roundoff at h <= 1e-6 m; a
+              Richardson-extrapolated difference with steps 0.1 m and 0.05 m is
+              kept as a sanity check (<= 1e-3).
 """
 import numpy as np
 import pytest
@@ -53,7 +58,9 @@ def test_forward_matches_oracle_loop(lib_ready, port):
     assert np.abs(vf - bb[:, 3:6]).max() <= 1e-10 * np.abs(bb[:, 3:6]).max()
 
 
-def _fd_check(api, b, cm, dt, nsteps, coords, seed, h=1e-6):
+def _fd_check(api, b, cm, dt, nsteps, coords, seed, h=1e-6, richardson=False):
+    """Worst relative error of the adjoint gradient of the MSE loss over
+    `coords` random coordinates (x, v: finite differences; m: tangent model)."""
     rng = np.random.default_rng(seed)
     x0, v0, m, R = b[:, :3].copy(), b[:, 3:6].copy(), b[:, 6].copy(), b[:, 7].copy()
     xf, _ = api.leapfrog(x0, v0, m, R, cm, dt, nsteps)
@@ -65,17 +72,26 @@ def _fd_check(api, b, cm, dt, nsteps, coords, seed, h=1e-6):
     def loss_of(x0_, v0_, m_):
         return mse_loss(api.leapfrog(x0_, v0_, m_, R, cm, dt, nsteps)[0], target)
 
-    worst = 0.0
+    worst = {"x": 0.0, "v": 0.0, "m": 0.0, "m_fd": 0.0}
+    zero3 = np.zeros((n, 3))
     for q in range(coords):
         kind = q % 3
         i = int(rng.integers(n))
-        if kind == 2:  # mass: relative step
-            hm = h * m[i]
-            mp, mm = m.copy(), m.copy()
-            mp[i] += hm
-            mm[i] -= hm
-            fd = (loss_of(x0, v0, mp) - loss_of(x0, v0, mm)) / (2 * hm)
-            g = gm[i]
+        if kind == 2:
+            em = np.zeros(n)
+            em[i] = 1.0
+            tan = api.leapfrog_jvp(x0, v0, m, R, cm, dt, nsteps, zero3, zero3, em)
+            ref = float(np.sum(adj * tan))
+            worst["m"] = max(worst["m"], abs(gm[i] - ref) / abs(ref))
+            if richardson:
+                def D(rel):
+                    hm = rel * m[i]
+                    mp, mm = m.copy(), m.copy()
+                    mp[i] += hm
+                    mm[i] -= hm
+                    return (loss_of(x0, v0, mp) - loss_of(x0, v0, mm)) / (2 * hm)
+                rich = (4 * D(0.05) - D(0.1)) / 3
+                worst["m_fd"] = max(worst["m_fd"], abs(gm[i] - rich) / abs(rich))
         else:
             d = int(rng.integers(3))
             arr = x0 if kind == 0 else v0
@@ -84,18 +100,39 @@ def _fd_check(api, b, cm, dt, nsteps, coords, seed, h=1e-6):
             am[i, d] -= h
             if kind == 0:
                 fd = (loss_of(ap, v0, m) - loss_of(am, v0, m)) / (2 * h)
-                g = gx[i, d]
+                g, key = gx[i, d], "x"
             else:
                 fd = (loss_of(x0, ap, m) - loss_of(x0, am, m)) / (2 * h)
-                g = gv[i, d]
-        err = abs(g - fd) / max(abs(fd), 1e-300)
-        worst = max(worst, err)
+                g, key = gv[i, d], "v"
+            worst[key] = max(worst[key], abs(g - fd) / max(abs(fd), 1e-300))
     return worst
+
+
+def _assert_worst(w):
+    assert w["x"] <= 1e-5 and w["v"] <= 1e-5, w
+    assert w["m"] <= 1e-8, w
+    assert w["m_fd"] <= 1e-3, w
 
 
 def test_vjp_vs_finite_differences_small(lib_ready):
     b, cm = disk(200, 2)
-    assert _fd_check(lib_ready, b, cm, 1e-3, 150, 18, seed=3) <= 1e-5
+    _assert_worst(_fd_check(lib_ready, b, cm, 1e-3, 150, 18, seed=3, richardson=True))
+
+
+def test_adjoint_dot_product_identity(lib_ready):
+    """<w, J d> = <J^T w, d> for random w and random directions d."""
+    api = lib_ready
+    b, cm = disk(300, 8)
+    rng = np.random.default_rng(9)
+    n = len(b)
+    args = (b[:, :3], b[:, 3:6], b[:, 6], b[:, 7], cm, 1e-3, 120)
+    dx, dv, dm = rng.normal(size=(n, 3)), rng.normal(size=(n, 3)), rng.normal(size=n) * b[:, 6]
+    w = rng.normal(size=(n, 3))
+    jd = api.leapfrog_jvp(*args, dx, dv, dm)
+    gx, gv, gm = api.leapfrog_vjp(*args, w)
+    lhs = float(np.sum(w * jd))
+    rhs = float(np.sum(gx * dx) + np.sum(gv * dv) + np.sum(gm * dm))
+    assert abs(lhs - rhs) <= 1e-10 * abs(lhs)
 
 
 def test_vjp_checkpoint_independent(lib_ready):
@@ -130,12 +167,14 @@ def test_torch_autograd_function(lib_ready):
 def test_adjoint_disk_16384_1000_steps(lib):
     """The differentiable workload: N = 16,384 (log-uniform masses, softening
     0.5 (R_k + R_p)), 1,000 steps, dt = 1e-3, checkpoints every 32 steps;
-    MSE loss to a seeded target; 64 coordinates (x, v, m) against FP64
-    central differences with h = 1e-6."""
+    MSE loss to a seeded target; 64 coordinates: x and v against FP64 central
+    differences with h = 1e-6, m against the tangent-linear model."""
     from ncorpion_b200 import api
     api.init(16384, make_params(softening_parameter=0.5))
     try:
         b, cm = disk(16384, 0)
-        assert _fd_check(api, b, cm, 1e-3, 1000, 64, seed=11) <= 1e-5
+        w = _fd_check(api, b, cm, 1e-3, 1000, 64, seed=11)
+        print("adjoint 16384 x 1000 worst relative errors:", w)
+        _assert_worst(w)
     finally:
         api.finalize()
