@@ -317,27 +317,39 @@ __device__ __forceinline__ bool chain_live(int w, const DevState &S, const MGArg
       return w >= 9 ? A.central : (S.ex[w / 3] && A.mutual);
 }
 
+constexpr int CHB = 512;  // terms staged per warp and block
 __global__ void __launch_bounds__(384) k_mesh_chains(DevState S, MGArgs A, const double *__restrict__ terms, long N,
                                                      const double *__restrict__ ax, const double *__restrict__ ay,
                                                      const double *__restrict__ az, double *__restrict__ tot)
 {
+      __shared__ double stage[12][CHB];
       const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       double s = chain_init(w, ax, ay, az);
       if (chain_live(w, S, A)) {
             const double *t = terms + (size_t)w * N;
             const int k0 = w >= 9 ? 0 : 3;
             const int n = A.lid + 1;
-            int k = k0;
-            double v = (k + lane < n && S.ex[k + lane]) ? t[k + lane] : 0.;
-            for (; k < n; k += 32) {
-                  const int kn = k + 32 + lane;
-                  const double vn = (kn < n && S.ex[kn]) ? t[kn] : 0.;  // prefetch the next chunk
-                  double w[32];
+            double v[CHB / 32];
 #pragma unroll
-                  for (int u = 0; u < 32; u++) w[u] = __shfl_sync(0xffffffffu, v, u);  // off the add chain
+            for (int u = 0; u < CHB / 32; u++) {
+                  const int k = k0 + u * 32 + lane;
+                  v[u] = (k < n && S.ex[k]) ? t[k] : 0.;
+            }
+            for (int base = k0; base < n; base += CHB) {
 #pragma unroll
-                  for (int u = 0; u < 32; u++) s = DADD(s, w[u]);
-                  v = vn;
+                  for (int u = 0; u < CHB / 32; u++) stage[w][u * 32 + lane] = v[u];
+                  __syncwarp();
+#pragma unroll
+                  for (int u = 0; u < CHB / 32; u++) {  // next block in flight during the sums
+                        const int k = base + CHB + u * 32 + lane;
+                        v[u] = (k < n && S.ex[k]) ? t[k] : 0.;
+                  }
+                  if (lane == 0) {
+                        const int m = min(CHB, n - base);
+#pragma unroll 8
+                        for (int q = 0; q < m; q++) s = DADD(s, stage[w][q]);
+                  }
+                  __syncwarp();
             }
       }
       if (lane == 0) tot[w] = s;
