@@ -162,6 +162,90 @@ def run_reference_arm(a, ws, rank):
     return 0
 
 
+MESH_N = 1 << 20
+MESH_STEPS = 100
+MESH_DT = 5e-4
+MESH_WORKLOAD = ("mesh collision search + mesh gravity, N=1,048,576 disk (a~U[0.5,2.0], e~Rayleigh 0.01, "
+                 "i~Rayleigh 0.005), radii dN/dR~R^-3.5 over [1e-5,1e-3], 1024 cells per side, "
+                 "collision_cube_min 4.4 (mesh size >= 2 x max radius), instant mergers, dt=5e-4")
+
+
+def mesh_params(mode):
+    from ncorpion_b200 import api
+    return api.default_params(G=1.0, softening_parameter=0.0, collision_bool=1, brute_force_bool=0, mesh_bool=1,
+                              collision_type=api.COLLISION_MERGER, collision_cube_cells=1024,
+                              how_many_neighbours=16.0, collision_cube_min=4.4, gravity_mode=mode,
+                              disruption_threshold=0.1, high_dumping_threshold=100.0)
+
+
+def mesh_gamma0(n):
+    """The initial mesh size of variable_initialization (src/structure.c:515-523)
+    with sma 0.5 .. 2.0, inclination_max 0.015, how_many_neighbours 16."""
+    gam = (2.0 ** 3 - 0.5 ** 3) ** (1.0 / 3.0) * (4.0 * np.pi * 16.0 * np.sin(0.015) / (n * 81.0)) ** (1.0 / 3.0)
+    return max(gam, 4.4 / 1024)
+
+
+def bench_mesh(lib, api, torch, mode, steps, warmup):
+    """Steps/s of the mesh integrator loop on the device state, CUDA events on
+    the library stream; the half kick of integration_mesh first."""
+    from ncorpion_b200 import disks
+    b = disks.mesh_disk(MESH_N, seed=0)
+    ex = np.ones(MESH_N, np.int32)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    api.init(1100000, mesh_params(mode))
+    api.upload(b, ex, cm)
+    gmin = 4.4 / 1024
+    gam = mesh_gamma0(MESH_N)
+    api.set_timestep(MESH_DT / 2)
+    api.three_largest()
+    _, _, tn = api.mesh(gam, False)
+    api.kick()
+    api.mesh_reset()
+    api.set_timestep(MESH_DT)
+    gam = api.update_gamma(gam, tn, MESH_N, 16.0, gmin)
+    st = torch.cuda.ExternalStream(lib.ncgpu_stream())
+    for _ in range(warmup):
+        hm, tn = api.step_mesh(gam)
+        gam = api.update_gamma(gam, tn, hm, 16.0, gmin)
+    ms, events, pairs, launches = [], 0, 0, 0
+    for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        hm, tn = api.step_mesh(gam)
+        e1.record(st)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        launches += lib.ncgpu_last_launch_count()
+        events += len(api.events())
+        pairs += tn
+        gam = api.update_gamma(gam, tn, hm, 16.0, gmin)
+    api.finalize()
+    t = float(np.sum(ms)) / 1e3
+    return {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps, "steps": steps, "events": events,
+            "pairs_per_step": pairs / steps, "bodies_end": hm, "gpu_launches": launches}
+
+
+def mesh_cpu_reference(nsteps=3):
+    """The reference's mesh() + mesh gravity loop (oracle/_ref/mesh_merge_1m,
+    1 thread, 8.6 GB hash table) for a few steps of the same disk."""
+    import oracle
+    from ncorpion_b200 import disks
+    if not oracle.ref_available("mesh_merge_1m"):
+        return None
+    b = disks.mesh_disk(MESH_N, seed=0)
+    ref = oracle.Ref("mesh_merge_1m")
+    ref.set_state(b, np.ones(MESH_N, np.int32), np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0]), dt=MESH_DT,
+                  gam=mesh_gamma0(MESH_N))
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        ref.lib.orc_step_mesh()
+    dt = time.perf_counter() - t0
+    return {"value": nsteps / dt, "unit": "mesh steps/s", "cores": 1, "kind": "reference",
+            "sample": f"{nsteps} iterations of the reference's mesh loop (mesh, drift, kick, end_of_timestep) on "
+                      f"the same 1,048,576-body disk ({dt:.1f} s, 1 thread)"}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -169,6 +253,7 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mesh", action="store_true")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
     ws, rank, local = dist_info()
@@ -287,6 +372,31 @@ def main(argv=None):
         e2e_s = float(t[0])
 
     fp32_peak = api.probe_fp32_peak()
+    api.finalize()
+
+    mesh = None
+    if not a.no_mesh:
+        mesh_fast = bench_mesh(lib, api, torch, api.GRAVITY_MIXED, MESH_STEPS, 3)
+        mesh_exact = bench_mesh(lib, api, torch, api.GRAVITY_EXACT, 10, 2)
+        n_pairs = mesh_fast["pairs_per_step"]
+        # algorithmic bytes per step: 56 B/body state read + 8 B key/index + 72 B drift + 72 B kick
+        # per body; 8 B written + 16 B read per pair (search and gravity)
+        alg = MESH_N * (56 + 8 + 72 + 72) + n_pairs * (8 + 16)
+        hbm_peak = 6426.2
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                hbm_peak = json.load(f)["hbm_gbs"]
+        except Exception:
+            pass
+        ach = alg / (mesh_fast["ms_per_step"] * 1e-3) / 1e9
+        mesh = {"metric": "mesh collision steps/s at N=1M", "workload": MESH_WORKLOAD, "fast": mesh_fast,
+                "exact": mesh_exact,
+                "note": "fast: CM_acc and the three largest bodies' sums as two-level parallel sums; exact: "
+                        "sequential FP64 chains (bit-identical state); pairs[] and events are exact in both",
+                "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
+                             "algorithmic_bytes_per_step": alg, "traffic": None,
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
+                "cpu_baseline": mesh_cpu_reference() if (rank == 0 and ws == 1 and not a.no_cpu_baseline) else None}
     achieved = FLOP_PER_INTERACTION * pairs / (kms_mixed * 1e-3) / 1e12
 
     cpu = None
@@ -326,6 +436,7 @@ def main(argv=None):
                            "kernel_ms": kms_fp64t},
             "speedup_mixed_vs_fp64_exact": ms_exact / ms_mixed,
             "speedup_mixed_vs_fp64_tiled": ms_fp64t / ms_mixed,
+            "mesh": mesh,
             "accuracy": {"mutual_rel_err_max": float(rel_mut.max()),
                          "mutual_rel_err_median": float(np.median(rel_mut)),
                          "total_rel_err_max": float(rel_tot.max()),
@@ -333,7 +444,6 @@ def main(argv=None):
                          "reference": "exact FP64 kernel (bit-identical to the reference's vector_field)"},
         }
         print(json.dumps(out))
-    api.finalize()
     if ws > 1:
         torch.distributed.destroy_process_group()
     return 0

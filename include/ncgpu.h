@@ -117,6 +117,9 @@ int ncgpu_vector_field_dev(const double *d_bodies, const int *d_exists, int larg
 
 /* Number of kernel launches issued by the last API call. */
 int ncgpu_last_launch_count(void);
+/* The library's CUDA stream (a cudaStream_t), for callers that time or order
+   work against it; NULL before ncgpu_init. */
+void *ncgpu_stream(void);
 /* Device time (CUDA events on the launching stream) of the dominant kernel of
    the last gravity evaluation (the pair-sum kernel), in milliseconds. */
 int ncgpu_last_kernel_ms(double *ms);

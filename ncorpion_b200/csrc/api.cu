@@ -232,6 +232,7 @@ const char *ncgpu_strerror(int s)
 
 const char *ncgpu_last_error(void) { return g_last_error; }
 int ncgpu_last_launch_count(void) { return launches(); }
+void *ncgpu_stream(void) { return g_ctx.inited ? (void *)g_ctx.s : nullptr; }
 
 int ncgpu_init(int n_max, const struct ncgpu_params *params)
 {

@@ -177,14 +177,15 @@ __global__ void k_seq_sum3(const double *__restrict__ cterm, int n, double *__re
 
 constexpr int RB = 256;
 
+// bounding box (lo xyz, hi xyz) and radius range (min, max) of the existing bodies
 __global__ void k_bbox_part(BodyView bv, const int *__restrict__ cidx, int n, double *__restrict__ part)
 {
-      __shared__ double sh[6][RB];
-      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      __shared__ double sh[8][RB];
+      double lo[4] = {1e300, 1e300, 1e300, 1e300}, hi[4] = {-1e300, -1e300, -1e300, -1e300};
       for (int p = blockIdx.x * RB + threadIdx.x; p < n; p += gridDim.x * RB) {
             long s = (long)cidx[p] * bv.stride;
-            double v[3] = {bv.x[s], bv.y[s], bv.z[s]};
-            for (int d = 0; d < 3; d++) {
+            double v[4] = {bv.x[s], bv.y[s], bv.z[s], bv.R[s]};
+            for (int d = 0; d < 4; d++) {
                   lo[d] = fmin(lo[d], v[d]);
                   hi[d] = fmax(hi[d], v[d]);
             }
@@ -193,25 +194,30 @@ __global__ void k_bbox_part(BodyView bv, const int *__restrict__ cidx, int n, do
             sh[d][threadIdx.x] = lo[d];
             sh[3 + d][threadIdx.x] = hi[d];
       }
+      sh[6][threadIdx.x] = lo[3];
+      sh[7][threadIdx.x] = hi[3];
       __syncthreads();
       for (int o = RB / 2; o > 0; o >>= 1) {
             if (threadIdx.x < o)
-                  for (int d = 0; d < 3; d++) {
-                        sh[d][threadIdx.x] = fmin(sh[d][threadIdx.x], sh[d][threadIdx.x + o]);
-                        sh[3 + d][threadIdx.x] = fmax(sh[3 + d][threadIdx.x], sh[3 + d][threadIdx.x + o]);
+                  for (int d = 0; d < 8; d++) {
+                        const bool mx = d == 3 || d == 4 || d == 5 || d == 7;
+                        double a = sh[d][threadIdx.x], b = sh[d][threadIdx.x + o];
+                        sh[d][threadIdx.x] = mx ? fmax(a, b) : fmin(a, b);
                   }
             __syncthreads();
       }
-      if (threadIdx.x < 6) part[blockIdx.x * 6 + threadIdx.x] = sh[threadIdx.x][0];
+      if (threadIdx.x < 8) part[blockIdx.x * 8 + threadIdx.x] = sh[threadIdx.x][0];
 }
 
 __global__ void k_bbox_final(double *__restrict__ part, int nparts)
 {
       int d = threadIdx.x;
-      if (d >= 6) return;
+      if (d >= 8) return;
+      const bool mx = d == 3 || d == 4 || d == 5 || d == 7;
       double v = part[d];
-      for (int b = 1; b < nparts; b++) v = d < 3 ? fmin(v, part[b * 6 + d]) : fmax(v, part[b * 6 + d]);
-      part[d] = v;  // result in part[0..5]
+      for (int b = 1; b < nparts; b++) v = mx ? fmax(v, part[b * 8 + d]) : fmin(v, part[b * 8 + d]);
+      __syncwarp(0xffu);
+      part[d] = v;  // lo xyz, hi xyz, R min, R max in part[0..7]
 }
 
 __device__ __forceinline__ uint32_t spread3(uint32_t v)
@@ -366,6 +372,58 @@ __device__ __forceinline__ void fp64_tile(const D4 *__restrict__ tl, const doubl
       }
 }
 
+__device__ __forceinline__ float rsqrt_ftz(float x)
+{
+      float y;
+      asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+      return y;
+}
+
+// FP32 pair sums of one far tile for two targets at tile-relative positions
+// (x0..z0), (x1..z1).  SM 0: no softening; 1: uniform eps^2; 2: eps = sR_i + sR_j.
+// Runs of 32 sources are summed in FP32 and Kahan-added per tile; the tile
+// total is folded into the FP64 accumulators.
+template <int SM, bool FULL>
+__device__ __forceinline__ void far_tile(const float4 *__restrict__ tl, const float *__restrict__ tr, int cnt,
+                                         float x0, float y0, float z0, float x1, float y1, float z1, float r0f,
+                                         float r1f, float eps2f, double (&a0)[3], double (&a1)[3])
+{
+      float S0[3] = {0.f, 0.f, 0.f}, C0[3] = {0.f, 0.f, 0.f};
+      float S1[3] = {0.f, 0.f, 0.f}, C1[3] = {0.f, 0.f, 0.f};
+      const int n = FULL ? T : cnt;
+      for (int jb = 0; jb < n; jb += 32) {
+            float p0x = 0.f, p0y = 0.f, p0z = 0.f, p1x = 0.f, p1y = 0.f, p1z = 0.f;
+            const int je = FULL ? 32 : min(32, n - jb);
+#pragma unroll 8
+            for (int jj = 0; jj < je; ++jj) {
+                  const int j = jb + jj;
+                  const float4 s = tl[j];
+                  float q0 = SM == 1 ? eps2f : 0.f, q1 = SM == 1 ? eps2f : 0.f;
+                  if (SM == 2) {
+                        const float rj = tr[j];
+                        const float e0 = r0f + rj, e1 = r1f + rj;
+                        q0 = e0 * e0;
+                        q1 = e1 * e1;
+                  }
+                  const float dx0 = s.x - x0, dy0 = s.y - y0, dz0 = s.z - z0;
+                  const float dx1 = s.x - x1, dy1 = s.y - y1, dz1 = s.z - z1;
+                  q0 = fmaf(dx0, dx0, q0); q0 = fmaf(dy0, dy0, q0); q0 = fmaf(dz0, dz0, q0);
+                  q1 = fmaf(dx1, dx1, q1); q1 = fmaf(dy1, dy1, q1); q1 = fmaf(dz1, dz1, q1);
+                  const float i0 = rsqrt_ftz(q0), i1 = rsqrt_ftz(q1);
+                  const float w0 = (s.w * i0) * (i0 * i0);
+                  const float w1 = (s.w * i1) * (i1 * i1);
+                  p0x = fmaf(w0, dx0, p0x); p0y = fmaf(w0, dy0, p0y); p0z = fmaf(w0, dz0, p0z);
+                  p1x = fmaf(w1, dx1, p1x); p1y = fmaf(w1, dy1, p1y); p1z = fmaf(w1, dz1, p1z);
+            }
+            kahan_add(S0[0], C0[0], p0x); kahan_add(S0[1], C0[1], p0y); kahan_add(S0[2], C0[2], p0z);
+            kahan_add(S1[0], C1[0], p1x); kahan_add(S1[1], C1[1], p1y); kahan_add(S1[2], C1[2], p1z);
+      }
+      for (int d = 0; d < 3; d++) {
+            a0[d] += (double)S0[d] - (double)C0[d];
+            a1[d] += (double)S1[d] - (double)C1[d];
+      }
+}
+
 // One CTA = one (target block of T sorted bodies, chunk of source tiles).
 // MODE 0: mixed (FP32 far tiles + FP64 near tiles); MODE 1: all tiles FP64.
 // SOFT 0: no softening; 1: uniform epsilon^2 (all radii equal); 2: general.
@@ -374,7 +432,8 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
                                                     const float4 *__restrict__ s32, const float *__restrict__ sR32,
                                                     const double *__restrict__ box, int n, int ntiles, int tpc,
                                                     double theta, double eps2, double *__restrict__ partial,
-                                                    long npad, unsigned *__restrict__ err)
+                                                    long npad, unsigned *__restrict__ err,
+                                                    const double *__restrict__ rrange, double sp)
 {
       __shared__ float4 f4[2][T];
       __shared__ alignas(16) float fr[2][T];
@@ -393,6 +452,10 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
       const float r0f = (float)r0, r1f = (float)r1;
       const float eps2f = (float)eps2;
       const double *bi = box + ib * 6;
+      // all radii equal: eps = 2 softening R for every pair (the loads of R skip)
+      const bool uni = SOFT == 2 && rrange[0] == rrange[1];
+      const double eu = 2.0 * sp * rrange[0];
+      const float eps2u = (float)(eu * eu);
 
       double a0[3] = {0., 0., 0.}, a1[3] = {0., 0., 0.};
 
@@ -452,40 +515,15 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
                         // FP32 path, coordinates relative to the source tile's centre
                         const float x0 = (float)(m0.x - bj[0]), y0 = (float)(m0.y - bj[1]), z0 = (float)(m0.z - bj[2]);
                         const float x1 = (float)(m1.x - bj[0]), y1 = (float)(m1.y - bj[1]), z1 = (float)(m1.z - bj[2]);
-                        float S0[3] = {0.f, 0.f, 0.f}, C0[3] = {0.f, 0.f, 0.f};
-                        float S1[3] = {0.f, 0.f, 0.f}, C1[3] = {0.f, 0.f, 0.f};
                         const float4 *tl = f4[b];
                         const float *tr = fr[b];
-                        for (int jb = 0; jb < cnt; jb += 32) {
-                              const int je = min(cnt, jb + 32);
-                              float p0x = 0.f, p0y = 0.f, p0z = 0.f, p1x = 0.f, p1y = 0.f, p1z = 0.f;
-#pragma unroll 8
-                              for (int j = jb; j < je; ++j) {
-                                    const float4 s = tl[j];
-                                    float e0 = 0.f, e1 = 0.f;
-                                    if (SOFT == 2) {
-                                          const float rj = tr[j];
-                                          e0 = r0f + rj;
-                                          e1 = r1f + rj;
-                                    }
-                                    float dx0 = s.x - x0, dy0 = s.y - y0, dz0 = s.z - z0;
-                                    float dx1 = s.x - x1, dy1 = s.y - y1, dz1 = s.z - z1;
-                                    float q0 = SOFT == 1 ? eps2f : (SOFT == 2 ? e0 * e0 : 0.f);
-                                    float q1 = SOFT == 1 ? eps2f : (SOFT == 2 ? e1 * e1 : 0.f);
-                                    q0 = fmaf(dx0, dx0, q0); q0 = fmaf(dy0, dy0, q0); q0 = fmaf(dz0, dz0, q0);
-                                    q1 = fmaf(dx1, dx1, q1); q1 = fmaf(dy1, dy1, q1); q1 = fmaf(dz1, dz1, q1);
-                                    const float i0 = rsqrtf(q0), i1 = rsqrtf(q1);
-                                    const float w0 = (s.w * i0) * (i0 * i0);
-                                    const float w1 = (s.w * i1) * (i1 * i1);
-                                    p0x = fmaf(w0, dx0, p0x); p0y = fmaf(w0, dy0, p0y); p0z = fmaf(w0, dz0, p0z);
-                                    p1x = fmaf(w1, dx1, p1x); p1y = fmaf(w1, dy1, p1y); p1z = fmaf(w1, dz1, p1z);
-                              }
-                              kahan_add(S0[0], C0[0], p0x); kahan_add(S0[1], C0[1], p0y); kahan_add(S0[2], C0[2], p0z);
-                              kahan_add(S1[0], C1[0], p1x); kahan_add(S1[1], C1[1], p1y); kahan_add(S1[2], C1[2], p1z);
-                        }
-                        for (int d = 0; d < 3; d++) {
-                              a0[d] += (double)S0[d] - (double)C0[d];
-                              a1[d] += (double)S1[d] - (double)C1[d];
+                        if (cnt == T) {
+                              if (SOFT == 0) far_tile<0, true>(tl, tr, T, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
+                              else if (uni) far_tile<1, true>(tl, tr, T, x0, y0, z0, x1, y1, z1, r0f, r1f, eps2u, a0, a1);
+                              else far_tile<2, true>(tl, tr, T, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
+                        } else {
+                              if (SOFT == 0) far_tile<0, false>(tl, tr, cnt, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
+                              else far_tile<2, false>(tl, tr, cnt, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
                         }
                   }
             }
@@ -667,7 +705,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       NCG_CK(cudaEventRecord(c.kev0, st));
 #define NCG_TILED(MODE_, SOFT_)                                                                              \
       k_grav_tiled<MODE_, SOFT_><<<grid, MXB, 0, st>>>(s64, c.srcR, s32, c.srcR32, c.tilebox, n, ntiles, tpc, \
-                                                      theta, eps2, c.partial, npad, c.err)
+                                                      theta, eps2, c.partial, npad, c.err, c.red + 6, sp)
       if (mode == NCGPU_GRAVITY_MIXED) {
             if (sm == 0) NCG_TILED(0, 0); else NCG_TILED(0, 2);
       } else {
