@@ -115,6 +115,25 @@ int ncgpu_vector_field_dev(const double *d_bodies, const int *d_exists, int larg
                            const struct ncgpu_body *cm, double *d_acc, double *d_cm_acc,
                            int gravity_mode, void *stream);
 
+/* Allocation-free variant of ncgpu_vector_field_dev in the EXACT mode.  It has
+   no counterpart in the reference: it exists for callers that cannot allocate
+   device memory when they evaluate forces (a host whose device memory belongs to
+   its own pool allocator, an integration loop that forbids allocation once it
+   runs).  It needs no ncgpu_init and calls no cudaMalloc or cudaFree: its scratch
+   is a fixed file-scope device array of ncgpu_noalloc_scratch_bytes() bytes,
+   resident on every GPU that loads the library, sized for at most
+   NCGPU_NOALLOC_MAX_SLOTS body slots (largest_id + 1 larger than that returns
+   NCGPU_E_CAPACITY).  The first call on a device looks up the array's device
+   address (cudaGetSymbolAddress), so make it before any stream capture.  All
+   calls share the array: calls that overlap on the GPU race.  params supplies
+   G, softening_parameter and central_mass_bool; the other arguments are those
+   of ncgpu_vector_field_dev (stream may be NULL: the default stream). */
+#define NCGPU_NOALLOC_MAX_SLOTS 65536
+int ncgpu_vector_field_static(const double *d_bodies, const int *d_exists, int largest_id,
+                              const struct ncgpu_body *cm, const struct ncgpu_params *params,
+                              double *d_acc, double *d_cm_acc, void *stream);
+unsigned long ncgpu_noalloc_scratch_bytes(void);
+
 /* Number of kernel launches issued by the last API call. */
 int ncgpu_last_launch_count(void);
 /* The library's CUDA stream (a cudaStream_t), for callers that time or order

@@ -85,6 +85,8 @@ EXPORTS = {
     "ncgpu_vector_field_dev": (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P]),
     "ncgpu_last_launch_count": (C.c_int, []),
     "ncgpu_stream": (C.c_void_p, []),
+    "ncgpu_vector_field_static": (C.c_int, [P, P, C.c_int, P, P, P, P, P]),
+    "ncgpu_noalloc_scratch_bytes": (C.c_ulong, []),
     "ncgpu_upload": (C.c_int, [P, P, C.c_int, P]),
     "ncgpu_download": (C.c_int, [P, P, P, P]),
     "ncgpu_set_timestep": (C.c_int, [C.c_double]),

@@ -175,4 +175,13 @@ int scan_exclusive(const int *in, int *out, int n, int *sums, cudaStream_t st);
 // Returns the count through *n_host (synchronises).
 int compact_existing(const int *ex, int largest_id, int *n_host, cudaStream_t st);
 
+// Compaction of flagged slots with caller-provided scratch (no library context).
+int compact_flags_into(const int *flags, int n_slots, int *blockcnt, int *n_dev, int *out_idx, int *n_host,
+                       cudaStream_t st);
+
+// The exact gravity on caller-provided scratch (no library context).
+int gravity_exact_into(const BodyView &bv, int largest_id, const double *cmh, double G, double sp, int central,
+                       int *cidx, double *src, double *srcR, double *cterm, int *blockcnt, int *n_dev,
+                       unsigned *err, double *ax, double *ay, double *az, double *d_cm_acc, cudaStream_t st);
+
 }  // namespace ncg

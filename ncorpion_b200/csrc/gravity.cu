@@ -731,3 +731,48 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
 }
 
 }  // namespace ncg
+
+namespace ncg {
+
+// The EXACT gravity of gravity_eval on caller-provided scratch, without the
+// library context: cidx (n), src (npad double4 = 4*npad doubles), srcR (npad),
+// cterm (3n), blockcnt/n_dev for the compaction, err (1 word).  Writes ax, ay,
+// az (slots 0..largest_id, zero for empty slots) and d_cm_acc.
+int gravity_exact_into(const BodyView &bv, int largest_id, const double *cmh, double G, double sp, int central,
+                       int *cidx, double *src, double *srcR, double *cterm, int *blockcnt, int *n_dev,
+                       unsigned *err, double *ax, double *ay, double *az, double *d_cm_acc, cudaStream_t st)
+{
+      const int nslots = largest_id + 1;
+      if (nslots > 0) {
+            k_zero3<<<(nslots + 255) / 256, 256, 0, st>>>(ax, ay, az, nslots);
+            NCG_LAUNCHED();
+      }
+      int n = 0;
+      NCG_TRY(compact_flags_into(bv.ex, nslots, blockcnt, n_dev, cidx, &n, st));
+      if (n == 0 || !central) {
+            k_set3<<<1, 1, 0, st>>>(d_cm_acc, 0., 0., 0.);
+            NCG_LAUNCHED();
+            if (n == 0) return NCGPU_OK;
+      }
+      const int ntiles = (n + T - 1) / T;
+      const int npad = ntiles * T;
+      const double mu = G * cmh[6];
+      D4 *s4 = (D4 *)src;
+      k_pack_exact<<<(npad + 255) / 256, 256, 0, st>>>(bv, cidx, n, npad, G, s4, srcR);
+      NCG_LAUNCHED();
+      const int nb = (n + EXB - 1) / EXB;
+      if (sp != 0.)
+            k_grav_exact<true><<<nb, EXB, 0, st>>>(s4, srcR, cidx, n, ntiles, cmh[0], cmh[1], cmh[2], mu, sp, central,
+                                                   ax, ay, az, cterm, err);
+      else
+            k_grav_exact<false><<<nb, EXB, 0, st>>>(s4, srcR, cidx, n, ntiles, cmh[0], cmh[1], cmh[2], mu, sp,
+                                                    central, ax, ay, az, cterm, err);
+      NCG_LAUNCHED();
+      if (central) {
+            k_seq_sum3<<<1, 32, 0, st>>>(cterm, n, d_cm_acc);
+            NCG_LAUNCHED();
+      }
+      return NCGPU_OK;
+}
+
+}  // namespace ncg

@@ -242,3 +242,29 @@ int radix_sort_pairs(uint32_t *keys, int *vals, int n, int bits, cudaStream_t st
 }
 
 }  // namespace ncg
+
+namespace ncg {
+
+// Order-preserving compaction of the flagged slots 0..n_slots-1 into out_idx
+// with caller-provided scratch (blockcnt: ceil(n_slots/1024) + 1 ints, n_dev:
+// 1 int); the count is copied to *n_host (synchronises the stream).
+int compact_flags_into(const int *flags, int n_slots, int *blockcnt, int *n_dev, int *out_idx, int *n_host,
+                       cudaStream_t st)
+{
+      if (n_slots <= 0) {
+            *n_host = 0;
+            return NCGPU_OK;
+      }
+      int nb = (n_slots + CB - 1) / CB;
+      k_count_flags<<<nb, CB, 0, st>>>(flags, n_slots, blockcnt);
+      NCG_LAUNCHED();
+      k_scan_single<<<1, 1024, 0, st>>>(blockcnt, nb, n_dev);
+      NCG_LAUNCHED();
+      k_scatter_flags<<<nb, CB, 0, st>>>(flags, n_slots, blockcnt, out_idx);
+      NCG_LAUNCHED();
+      NCG_CK(cudaMemcpyAsync(n_host, n_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      return NCGPU_OK;
+}
+
+}  // namespace ncg

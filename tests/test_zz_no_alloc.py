@@ -1,0 +1,73 @@
+"""GPU: ncgpu_vector_field_static, the force evaluation for callers that
+cannot allocate device memory when they need forces (a host whose device
+memory belongs to its own pool allocator, an integration loop that forbids
+allocation once it runs).  It needs no ncgpu_init and keeps its scratch in a
+fixed device array inside libncgpu.so.
+
+Checked through the C ABI against the allocating entry point
+ncgpu_vector_field_dev in the exact mode, with that mode's tolerance
+(bit-identical accelerations and CM_acc), on two calls in a row: the first
+before the library was ever initialised in this process, the second on a
+smaller input after an init/finalize cycle, so the shared scratch still holds
+the first call's larger contents.  This file is collected last.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import make_params
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def test_static_scratch_matches_allocating_entry_point(lib):
+    import torch
+    from ncorpion_b200 import api, disks
+
+    assert 0 < lib.ncgpu_noalloc_scratch_bytes() < 64 << 20
+    cases = [(3000, 1, 0.5, 0.05), (1200, 2, 0.0, 0.1)]
+    for n, seed, soft, hole_frac in cases:
+        b = disks.gravity_disk(n, seed=seed)
+        rng = np.random.default_rng(seed)
+        ex = (rng.random(n) > hole_frac).astype(np.int32)
+        cm = np.array([1e-6, -2e-6, 0.0, 0, 0, 0, 1.0, 1.0])
+        params = make_params(softening_parameter=soft)
+        d_b = torch.from_numpy(b).cuda()
+        d_ex = torch.from_numpy(ex).cuda()
+        acc_s = torch.full((n, 3), np.nan, dtype=torch.float64, device="cuda")
+        cma_s = torch.full((3,), np.nan, dtype=torch.float64, device="cuda")
+        st = lib.ncgpu_vector_field_static(_dev(d_b), _dev(d_ex), n - 1, api.ptr(cm), C.byref(params), _dev(acc_s),
+                                           _dev(cma_s), None)
+        api.check(st, "ncgpu_vector_field_static")
+        torch.cuda.synchronize()
+
+        api.init(n, params)
+        acc_d = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+        cma_d = torch.zeros(3, dtype=torch.float64, device="cuda")
+        st = lib.ncgpu_vector_field_dev(_dev(d_b), _dev(d_ex), n - 1, api.ptr(cm), _dev(acc_d), _dev(cma_d),
+                                        api.GRAVITY_EXACT, None)
+        api.check(st, "ncgpu_vector_field_dev")
+        torch.cuda.synchronize()
+        api.finalize()
+
+        assert np.array_equal(acc_s.cpu().numpy(), acc_d.cpu().numpy())
+        assert np.array_equal(cma_s.cpu().numpy(), cma_d.cpu().numpy())
+
+
+def test_static_scratch_rejects_oversize(lib):
+    from ncorpion_b200 import api
+    import torch
+    n = 70000  # more slots than the fixed scratch holds
+    d = torch.zeros((n, 8), dtype=torch.float64, device="cuda")
+    e = torch.zeros(n, dtype=torch.int32, device="cuda")
+    out = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    cma = torch.zeros(3, dtype=torch.float64, device="cuda")
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    st = lib.ncgpu_vector_field_static(_dev(d), _dev(e), n - 1, api.ptr(cm), C.byref(make_params()), _dev(out),
+                                       _dev(cma), None)
+    assert st == api.E_CAPACITY
