@@ -114,9 +114,27 @@ def fragment_disk(n=262144, seed=0, density=3.0):
     return _assemble(rng, n, 0.9, 1.1, 0.02, 0.02, mass, rad)
 
 
-def adjoint_disk(n=16384, seed=0):
-    """Differentiable gravity-only disk (same law as ``gravity_disk``)."""
-    return gravity_disk(n, seed)
+def frag_test_disk(n=4000, seed=0, density=3.0):
+    """Crowded, hot ring for the fragmentation parity cases: a~U[0.99,1.01],
+    e,i Rayleigh 0.04, 60% of the radii U[1.5e-3,4e-3] and 40% U[1e-4,5e-4]
+    (constant density).  One collision sweep with dt = 0.02 holds impacts of
+    every outcome: merger, super-catastrophic, partial and full fragmentation."""
+    rng = np.random.default_rng(seed)
+    rad = rng.uniform(1.5e-3, 4e-3, n)
+    small = rng.random(n) < 0.4
+    rad[small] = rng.uniform(1e-4, 5e-4, int(small.sum()))
+    mass = 4.0 / 3.0 * np.pi * density * rad ** 3
+    return _assemble(rng, n, 0.99, 1.01, 0.04, 0.04, mass, rad)
+
+
+def adjoint_disk(n=16384, seed=0, radius=1e-3):
+    """Differentiable gravity-only disk: the law of ``gravity_disk`` with
+    R = 1e-3, so that the softening length 0.5 (R_k + R_p) = 1e-3 resolves
+    close encounters at dt = 1e-3.  With R = 1e-5 (the force-accuracy disk)
+    bodies of up to 1e-6 central masses bind on orbits far shorter than dt, the
+    1,000-step map is chaotic (gradient norms reach 1e22) and no finite
+    difference with h = 1e-6 is in its linear regime."""
+    return gravity_disk(n, seed, radius=radius)
 
 
 def reduce_to_com(bodies, cm=None, G=G_DEFAULT):

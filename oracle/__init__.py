@@ -104,6 +104,8 @@ class Ref:
             L.orc_three_largest.argtypes = [P]
             L.orc_mesh_counts.argtypes = [P]
         L.orc_set_free.argtypes = [C.c_int, P]
+        if hasattr(L, "orc_frag_counts"):
+            L.orc_frag_counts.argtypes = [P]
         if L.orc_init() != 0:
             raise MemoryError("reference init failed")
         self.n_max = L.orc_n_max()
@@ -131,6 +133,12 @@ class Ref:
         cma = np.zeros(3)
         self.lib.orc_vector_field(_p(acc), _p(cma))
         return acc, cma
+
+    def fragment_counts(self):
+        """(merger, super-catastrophic, partial, full) since the last reset."""
+        out = np.zeros(4, np.int32)
+        self.lib.orc_frag_counts(_p(out))
+        return out
 
     def events(self):
         n = self.lib.orc_events(None, 0)
@@ -165,6 +173,13 @@ class PortWorld:
         L.orc_w_three_largest.argtypes = [P]
         L.orc_cell_index.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int]
         L.orc_cell_index.restype = C.c_long
+        L.orc_w_step_mesh.restype = C.c_long
+        L.orc_w_end_of_timestep.restype = C.c_int
+        L.orc_w_step_brute_force.restype = C.c_int
+        L.orc_w_set_fragmentation.argtypes = [C.c_int, P, C.c_double, C.c_double, C.c_double, C.c_double,
+                                              C.c_double, C.c_double]
+        L.orc_w_fragment_counts.argtypes = [P]
+        L.orc_w_set_force_naive.argtypes = [C.c_int]
         self.n_max = n_max
         self.params = params
         if L.orc_w_init(n_max, C.byref(params)) != 0:
@@ -200,19 +215,15 @@ class PortWorld:
         self.lib.orc_w_three_largest(_p(idx))
         return idx
 
+    def set_fragmentation(self, N_tilde=15, pq=(-1, 3, -1, 1), mu=0.55, nu=0.4, C1=1.5, k=0.2,
+                          merging_threshold=0.0002, fragment_threshold=1.5e-8):
+        """The fragmentation constants (src/parameters.h:297-307); resets the
+        outcome counters."""
+        pqa = np.ascontiguousarray(pq, np.int32)
+        self.lib.orc_w_set_fragmentation(N_tilde, _p(pqa), mu, nu, C1, k, merging_threshold, fragment_threshold)
 
-def _pw_setup(L):
-    L.orc_w_step_mesh.restype = C.c_long
-    L.orc_w_end_of_timestep.restype = C.c_int
-    L.orc_w_step_brute_force.restype = C.c_int
-
-
-_orig_pw_init = PortWorld.__init__
-
-
-def _pw_init(self, n_max, params):
-    _orig_pw_init(self, n_max, params)
-    _pw_setup(self.lib)
-
-
-PortWorld.__init__ = _pw_init
+    def fragment_counts(self):
+        """(merger, super-catastrophic, partial, full) fragmentation outcomes."""
+        out = np.zeros(4, np.int32)
+        self.lib.orc_w_fragment_counts(_p(out))
+        return out

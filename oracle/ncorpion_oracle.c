@@ -120,6 +120,8 @@ void orc_drift(int lid, body *b, const int *ex, body *cm, double dt, const struc
 /* state, src/structure.c:62-115) lives in this file.                       */
 /* ======================================================================== */
 
+static int need_to_reduce_com = 0;  /* need_to_reduce_COM_bool */
+
 static struct {
       struct ncgpu_params P;
       int n_max, lid;
@@ -146,6 +148,7 @@ static struct {
       long *used_slots;
       long n_used;
       int three[3];
+      int force_naive;  /* force_naive_bool: the mesh run fell back to brute force */
 } W;
 
 static void push_event(int a, int b, int type)
@@ -204,6 +207,7 @@ void orc_w_set(int lid, const body *b, const int *ex, const body *cm, double dt,
 }
 
 void orc_w_set_timestep(double dt) { W.dt = dt; }
+void orc_w_set_force_naive(int v) { W.force_naive = v; }
 void orc_w_set_gam(double gam) { W.gam = gam; }
 
 int orc_w_get(body *b, int *ex, body *cm)
@@ -315,7 +319,9 @@ static void merge(int a, int b)
       W.did[a] = W.P.par_one_collision_only_bool;
 }
 
-/* collision_treatment (src/physics.c:1043-1091), types 0..2 */
+static void fragment(int a, int b);
+
+/* collision_treatment (src/physics.c:1043-1091) */
 static void treat(int a, int b, int type)
 {
       double m_a = W.b[a].mass, m_b = W.b[b].mass;
@@ -326,13 +332,15 @@ static void treat(int a, int b, int type)
             impulse(A, B, type == 0 ? 2.0 : W.P.par_collision_parameter);
             W.did[a] = W.P.par_one_collision_only_bool;
             W.did[b] = W.P.par_one_collision_only_bool;
-            if (W.P.par_mutual_bool && W.P.par_mesh_bool) {
+            if (W.P.par_mutual_bool && W.P.par_mesh_bool && !W.force_naive) {
                   W.pairs[2 * W.n_pairs] = a;
                   W.pairs[2 * W.n_pairs + 1] = b;
                   W.n_pairs++;
             }
       } else if (type == 2) {
             merge(A, B);
+      } else if (type == 3) {
+            fragment(A, B);
       }
       W.collision_count++;
 }
@@ -537,7 +545,6 @@ void orc_w_three_largest(int *idx)
 
 /* ---- end of timestep -------------------------------------------------- */
 
-static int need_to_reduce_com = 0;
 
 /* total_momentum (src/structure.c:1193-1227) */
 static void total_momentum(double *mom)
@@ -748,4 +755,223 @@ long orc_w_step_mesh(void)
       orc_w_end_of_timestep();
       orc_w_mesh_reset();
       return tn;
+}
+
+/* ---- fragmentation (src/physics.c:710-1040) ----------------------------- */
+
+static int frag_error = 0;  /* nonzero where the reference would abort */
+
+static struct {
+      int N_tilde, pq[4];
+      double mu, nu, C1, k, merging_threshold, fragment_threshold;
+      int merger_count, super_catastrophic_count, half_count, full_count;
+} F = {15, {-1, 3, -1, 1}, 0.55, 0.4, 1.5, 0.2, 0.0002, 1.5e-8, 0, 0, 0, 0};
+
+void orc_w_set_fragmentation(int N_tilde, const int *pq, double mu, double nu, double C1, double k,
+                             double merging_threshold, double fragment_threshold)
+{
+      F.N_tilde = N_tilde;
+      memcpy(F.pq, pq, sizeof F.pq);
+      F.mu = mu; F.nu = nu; F.C1 = C1; F.k = k;
+      F.merging_threshold = merging_threshold;
+      F.fragment_threshold = fragment_threshold;
+      F.merger_count = F.super_catastrophic_count = F.half_count = F.full_count = 0;
+      frag_error = 0;
+}
+
+void orc_w_fragment_counts(int *out)
+{
+      out[0] = F.merger_count; out[1] = F.super_catastrophic_count; out[2] = F.half_count; out[3] = F.full_count;
+}
+
+/* get_free_index (src/structure.c:849-878): 0 on success, -1 past N_max */
+static int free_index(int at_end, int *index)
+{
+      int idx;
+      if (W.n_free == 0 || at_end) {
+            W.lid += 1;
+            idx = W.lid;
+            if (idx == W.n_max) return -1;
+      } else {
+            W.n_free -= 1;
+            idx = W.free_idx[W.n_free];
+            if (idx > W.lid) W.lid = idx;
+      }
+      if (W.ex[idx]) return -2;
+      W.ex[idx] = 1;
+      *index = idx;
+      return 0;
+}
+
+int orc_w_fragment_error(void) { return frag_error; }
+
+static void fragment(int a, int b)
+{
+      const double stigma = (3. * F.mu - 1.) / (3. * F.mu);
+      body *A = W.b + a, *B = W.b + b;
+      double R_2 = A->radius, R_1 = B->radius, R = R_1 + R_2;
+      double m_2 = A->mass, m_1 = B->mass, M = m_1 + m_2;
+      double rho_1 = 3. * m_1 / (4. * M_PI * R_1 * R_1 * R_1);
+      double rho_2 = 3. * m_2 / (4. * M_PI * R_2 * R_2 * R_2);
+      double average_density = (m_1 * rho_1 + m_2 * rho_2) / M;
+      double rho_12 = rho_1 / rho_2;
+      double rho_12_3nu = pow(rho_12, 3. * F.nu);
+      double vx_a = A->vx, vy_a = A->vy, vz_a = A->vz, vx_b = B->vx, vy_b = B->vy, vz_b = B->vz;
+      double xa = W.approach[0], ya = W.approach[1], za = W.approach[2];
+      double xb = W.approach[3], yb = W.approach[4], zb = W.approach[5];
+      double dx = xa - xb, dy = ya - yb, dz = za - zb;
+      double dvx = vx_a - vx_b, dvy = vy_a - vy_b, dvz = vz_a - vz_b;
+      double dr_dot_dv = dx * dvx + dy * dvy + dz * dvz;
+      double dv_norm = sqrt(dvx * dvx + dvy * dvy + dvz * dvz);
+      double costheta = -dr_dot_dv / (R * dv_norm);
+      double costheta3mu = pow(costheta, 3. * F.mu);
+      double R_eq = pow(3. * M / (4. * M_PI * average_density), 1. / 3.);
+      double vesc = sqrt(2. * W.P.par_G * M / R_eq);
+      double K = 3. * F.k * m_1 / (4. * M_PI) / rho_12 * costheta3mu;
+      double m_check = K * (pow(F.C1 * dv_norm / vesc, 3. * F.mu) * rho_12_3nu - 1.);
+      double m_tilde = M - m_check;
+      double m_tilde_2 = m_check / (double)F.N_tilde;
+      double v_cm[3], r_cm[3], r_tilde[3], v_tilde[3];
+      double t = W.t_coll;
+      v_cm[0] = (m_2 * vx_a + m_1 * vx_b) / M; v_cm[1] = (m_2 * vy_a + m_1 * vy_b) / M; v_cm[2] = (m_2 * vz_a + m_1 * vz_b) / M;
+      r_cm[0] = (m_2 * xa + m_1 * xb) / M; r_cm[1] = (m_2 * ya + m_1 * yb) / M; r_cm[2] = (m_2 * za + m_1 * zb) / M;
+
+      if (m_check <= F.merging_threshold * M) {  /* merger */
+            merge(a, b);
+            F.merger_count++;
+            return;
+      }
+      if (m_tilde < 0.1 * M) {  /* super-catastrophic */
+            m_tilde = 0.1 * M * pow(1.0 / 0.9 * m_check / M, -1.5);
+            A->vx = v_cm[0]; A->vy = v_cm[1]; A->vz = v_cm[2];
+            A->x = r_cm[0] - t * v_cm[0]; A->y = r_cm[1] - t * v_cm[1]; A->z = r_cm[2] - t * v_cm[2];
+            A->mass = m_tilde;
+            A->radius = pow(3. * m_tilde / (4. * M_PI * average_density), 1. / 3.);
+            need_to_reduce_com = 1;
+            lose(b);
+            W.did[a] = W.P.par_one_collision_only_bool;
+            F.super_catastrophic_count++;
+            double discarded_mass = M - m_tilde;
+            if (m_tilde < F.fragment_threshold / 4.) {
+                  lose(a);
+                  discarded_mass = M;
+            }
+            if (W.P.par_central_mass_bool) W.cm.mass += discarded_mass;
+            return;
+      }
+      if (m_tilde_2 < F.fragment_threshold && m_check <= m_tilde) {  /* partial fragmentation */
+            double r_k[3], v_k[3];
+            double v_k_scalar = vesc / stigma * (m_check + K) / m_check * (1.0 - pow(K / (K + m_check), stigma));
+            if (v_k_scalar < vesc) { frag_error = 1; return; }
+            double in_front_of = v_k_scalar / R;
+            r_k[0] = -dx; r_k[1] = -dy; r_k[2] = -dz;
+            v_k[0] = in_front_of * r_k[0]; v_k[1] = in_front_of * r_k[1]; v_k[2] = in_front_of * r_k[2];
+            double R_tilde = pow(3.0 * m_tilde / (4.0 * M_PI * average_density), 1.0 / 3.0);
+            double R_check = pow(3.0 * m_check / (4.0 * M_PI * average_density), 1.0 / 3.0);
+            double R_tilde12 = R_tilde + R_check;
+            double dr_norm = sqrt(r_k[0] * r_k[0] + r_k[1] * r_k[1] + r_k[2] * r_k[2]);
+            r_k[0] *= R_tilde12 / dr_norm; r_k[1] *= R_tilde12 / dr_norm; r_k[2] *= R_tilde12 / dr_norm;
+            for (int d = 0; d < 3; d++) {
+                  r_tilde[d] = r_cm[d] - m_check / M * r_k[d];
+                  v_tilde[d] = v_cm[d] - m_check / M * v_k[d];
+            }
+            A->x = r_tilde[0] - t * v_tilde[0]; A->y = r_tilde[1] - t * v_tilde[1]; A->z = r_tilde[2] - t * v_tilde[2];
+            A->vx = v_tilde[0]; A->vy = v_tilde[1]; A->vz = v_tilde[2];
+            A->mass = m_tilde; A->radius = R_tilde;
+            B->x = r_tilde[0] + r_k[0] - t * (v_tilde[0] + v_k[0]);
+            B->y = r_tilde[1] + r_k[1] - t * (v_tilde[1] + v_k[1]);
+            B->z = r_tilde[2] + r_k[2] - t * (v_tilde[2] + v_k[2]);
+            B->vx = v_tilde[0] + v_k[0]; B->vy = v_tilde[1] + v_k[1]; B->vz = v_tilde[2] + v_k[2];
+            B->mass = m_check; B->radius = R_check;
+            if (W.P.par_mutual_bool && W.P.par_mesh_bool && !W.force_naive) add_pair(a, b);
+            W.did[a] = W.P.par_one_collision_only_bool;
+            W.did[b] = W.P.par_one_collision_only_bool;
+            F.half_count++;
+            return;
+      }
+      /* full fragmentation: the tail is N_tilde bodies on a (p, q) lattice */
+      int NT = F.N_tilde, n = 0;
+      double *r_k = (double *)malloc(sizeof(double) * 3 * (size_t)NT);
+      double *v_k = (double *)malloc(sizeof(double) * 3 * (size_t)NT);
+      int *id = (int *)malloc(sizeof(int) * (size_t)(NT + 1));
+      double dr[3], dv[3], u[3], v[3];
+      double R_tilde = pow(3.0 * m_tilde / (4.0 * M_PI * average_density), 1.0 / 3.0);
+      double R_tilde_2 = pow(3.0 * m_tilde_2 / (4.0 * M_PI * average_density), 1.0 / 3.0);
+      double R_tilde12 = R_tilde + R_tilde_2;
+      dr[0] = -dx; dr[1] = -dy; dr[2] = -dz;
+      dv[0] = -dvx; dv[1] = -dvy; dv[2] = -dvz;
+      double dr_norm = sqrt(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2]);
+      dr[0] *= R_tilde12 / dr_norm; dr[1] *= R_tilde12 / dr_norm; dr[2] *= R_tilde12 / dr_norm;
+      double dxv[3] = {dr[1] * dv[2] - dr[2] * dv[1], dr[2] * dv[0] - dr[0] * dv[2], dr[0] * dv[1] - dr[1] * dv[0]};
+      double dxv_norm = sqrt(dxv[0] * dxv[0] + dxv[1] * dxv[1] + dxv[2] * dxv[2]);
+      if (dxv_norm > 1.0e-5) {
+            v[0] = dxv[0] / dxv_norm; v[1] = dxv[1] / dxv_norm; v[2] = dxv[2] / dxv_norm;
+      } else {
+            /* maximum(|dr0|, |dr1|, |dr2|), src/structure.c:1090-1111 */
+            double f0 = fabs(dr[0]), f1 = fabs(dr[1]), f2 = fabs(dr[2]), mx;
+            int mm;
+            if (f0 >= f1) { mm = 0; mx = f0; } else { mm = 1; mx = f1; }
+            if (!(mx >= f2)) mm = 2;
+            double num;
+            if (mm == 0) {
+                  num = dr[1] + dr[2];
+                  v[1] = 1.0 / sqrt(2.0 + num * num / (dr[0] * dr[0])); v[2] = v[1]; v[0] = -v[1] * num / dr[0];
+            } else if (mm == 1) {
+                  num = dr[0] + dr[2];
+                  v[0] = 1.0 / sqrt(2.0 + num * num / (dr[1] * dr[1])); v[2] = v[0]; v[1] = -v[0] * num / dr[1];
+            } else {
+                  num = dr[0] + dr[1];
+                  v[0] = 1.0 / sqrt(2.0 + num * num / (dr[2] * dr[2])); v[1] = v[0]; v[2] = -v[0] * num / dr[2];
+            }
+      }
+      double vxd[3] = {v[1] * dr[2] - v[2] * dr[1], v[2] * dr[0] - v[0] * dr[2], v[0] * dr[1] - v[1] * dr[0]};
+      u[0] = vxd[0] / R_tilde12; u[1] = vxd[1] / R_tilde12; u[2] = vxd[2] / R_tilde12;
+      for (int p = F.pq[0]; p <= F.pq[1]; p++) {
+            for (int q = F.pq[2]; q <= F.pq[3]; q++) {
+                  double tp = ((double)(2 * p)) * R_tilde_2, tq = ((double)(2 * q)) * R_tilde_2;
+                  r_k[3 * n] = dr[0] + tp * u[0] + tq * v[0];
+                  r_k[3 * n + 1] = dr[1] + tp * u[1] + tq * v[1];
+                  r_k[3 * n + 2] = dr[2] + tp * u[2] + tq * v[2];
+                  double zk = pow(1.0 - ((double)n) * m_tilde_2 / (K + m_check), stigma);
+                  double zk1 = pow(1.0 - ((double)n + 1.) * m_tilde_2 / (K + m_check), stigma);
+                  double vks = vesc / stigma * (m_check + K) / m_tilde_2 * (zk - zk1);
+                  if (vks < vesc) frag_error = 2;
+                  double iff = vks / sqrt(1.0 + ((double)p) * ((double)p) + ((double)q) * ((double)q));
+                  v_k[3 * n] = iff * (dr[0] / R_tilde12 + ((double)p) * u[0] + ((double)q) * v[0]);
+                  v_k[3 * n + 1] = iff * (dr[1] / R_tilde12 + ((double)p) * u[1] + ((double)q) * v[1]);
+                  v_k[3 * n + 2] = iff * (dr[2] / R_tilde12 + ((double)p) * u[2] + ((double)q) * v[2]);
+                  n++;
+            }
+      }
+      double corr[6] = {0., 0., 0., 0., 0., 0.};
+      for (n = 0; n < NT; n++) {
+            corr[0] += r_k[3 * n]; corr[1] += r_k[3 * n + 1]; corr[2] += r_k[3 * n + 2];
+            corr[3] += v_k[3 * n]; corr[4] += v_k[3 * n + 1]; corr[5] += v_k[3 * n + 2];
+      }
+      for (int d = 0; d < 3; d++) {
+            r_tilde[d] = r_cm[d] - m_tilde_2 / M * corr[d];
+            v_tilde[d] = v_cm[d] - m_tilde_2 / M * corr[3 + d];
+      }
+      id[0] = a;
+      for (n = 1; n <= NT; n++)
+            if (free_index(W.P.par_mesh_bool && !W.force_naive, &id[n]) != 0) frag_error = 3;
+      if (W.P.par_mutual_bool && W.P.par_mesh_bool && !W.force_naive)
+            for (int p = 0; p <= NT; p++)
+                  for (int q = 0; q < p; q++) add_pair(id[p], id[q]);
+      lose(b);
+      for (n = 0; n <= NT; n++) W.did[id[n]] = W.P.par_one_collision_only_bool;
+      body *L0 = W.b + id[0];
+      L0->x = r_tilde[0] - t * v_tilde[0]; L0->y = r_tilde[1] - t * v_tilde[1]; L0->z = r_tilde[2] - t * v_tilde[2];
+      L0->vx = v_tilde[0]; L0->vy = v_tilde[1]; L0->vz = v_tilde[2];
+      L0->mass = m_tilde; L0->radius = R_tilde;
+      for (n = 0; n < NT; n++) {
+            body *Fk = W.b + id[n + 1];
+            Fk->x = r_tilde[0] + r_k[3 * n] - t * (v_tilde[0] + v_k[3 * n]);
+            Fk->y = r_tilde[1] + r_k[3 * n + 1] - t * (v_tilde[1] + v_k[3 * n + 1]);
+            Fk->z = r_tilde[2] + r_k[3 * n + 2] - t * (v_tilde[2] + v_k[3 * n + 2]);
+            Fk->vx = v_tilde[0] + v_k[3 * n]; Fk->vy = v_tilde[1] + v_k[3 * n + 1]; Fk->vz = v_tilde[2] + v_k[3 * n + 2];
+            Fk->mass = m_tilde_2; Fk->radius = R_tilde_2;
+      }
+      F.full_count++;
+      free(r_k); free(v_k); free(id);
 }

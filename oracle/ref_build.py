@@ -108,6 +108,15 @@ PROFILES = {
                              N_max="70000", N_0="20000", t_end="0.005", time_step="0.0005"),
     "mesh_grav_s": dict(MESH, collision_bool="0", collision_cube_cells="256", N_max="70000",
                         N_0="20000", t_end="0.005", time_step="0.0005"),
+    # fragmentation model (src/physics.c:710-1040), default constants (N_tilde 15)
+    "bf_frag": dict(BF, collision_bool="1", fragmentation_bool="1", N_max="16384", N_0="2000",
+                    t_end="0.05", time_step="0.001"),
+    "mesh_frag_s": dict(MESH, collision_bool="1", fragmentation_bool="1", collision_cube_cells="256",
+                        N_max="70000", N_0="20000", t_end="0.005", time_step="0.0005"),
+    # "up to 4 fragments": N_tilde 4 on the 2 x 2 lattice {0,1,0,1}
+    "mesh_frag4_s": dict(MESH, collision_bool="1", fragmentation_bool="1", collision_cube_cells="256",
+                         N_tilde="4", pq_min_max="{0,1,0,1}", N_max="70000", N_0="20000",
+                         t_end="0.005", time_step="0.0005"),
     # the N = 1,048,576 mesh workload: 1024 cells per side (8.6 GB hash table)
     "mesh_merge_1m": dict(MESH, collision_bool="1", instant_merger_bool="1",
                           collision_cube_cells="1024", N_max="1100000", N_0="1048576",

@@ -15,6 +15,7 @@
  *   get_neighbours_mesh    src/physics.c:1094
  *   three_largest_*        src/structure.c:914, src/structure.c:1005
  *   collision_treatment    src/physics.c:1043 (wrapped with -Wl,--wrap to log events)
+ *   fragmentation counters src/structure.h:148-151
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -141,6 +142,19 @@ void orc_set_timestep(double dt) { timestep = dt; }
 void orc_end_of_timestep(void) { end_of_timestep(B, 0); }
 
 void orc_events_reset(void) { ev_n = 0; }
+
+/* merger, super-catastrophic, partial and full fragmentation counts */
+void orc_frag_counts(int *out)
+{
+      out[0] = merger_count;
+      out[1] = super_catastrophic_count;
+      out[2] = half_fragmentation_count;
+      out[3] = full_fragmentation_count;
+}
+void orc_frag_counts_reset(void)
+{
+      merger_count = super_catastrophic_count = half_fragmentation_count = full_fragmentation_count = 0;
+}
 int orc_events(int *out, int cap)
 {
       int n = ev_n < cap ? ev_n : cap;

@@ -114,6 +114,46 @@ def mesh_case(profile, n, seed, gam, dt):
     return out
 
 
+def frag_bf_case(profile, n, seed, dt):
+    """One brute_force() sweep with the fragmentation model: events, outcome
+    counts, state (appended fragments included) and central mass."""
+    b = disks.frag_test_disk(n, seed=seed)
+    ex = np.ones(n, np.int32)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm, dt=dt)
+    ref.lib.orc_events_reset()
+    ref.lib.orc_frag_counts_reset()
+    ref.lib.orc_brute_force()
+    b2, ex2, cm2, sc = ref.get_state()
+    return dict(bodies=b, exists=ex, cm=cm, dt=np.float64(dt), events=ref.events(),
+                counts=ref.fragment_counts(), out_digest=digest(b2), out_exists_digest=digest(ex2), out_cm=cm2,
+                out_largest_id=np.int64(b2.shape[0] - 1))
+
+
+def frag_mesh_case(profile, n, seed, gam, dt, N_tilde, pq):
+    """three_largest + one mesh() call with the fragmentation model."""
+    b = disks.frag_test_disk(n, seed=seed)
+    ex = np.ones(n, np.int32)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm, dt=dt, gam=gam)
+    ref.lib.orc_events_reset()
+    ref.lib.orc_frag_counts_reset()
+    idx = np.zeros(3, np.int32)
+    ref.lib.orc_three_largest(idx.ctypes.data_as(oracle.P))
+    ref.lib.orc_mesh()
+    pairs = ref.pairs()
+    b2, ex2, cm2, sc = ref.get_state()
+    out = dict(bodies=b, exists=ex, cm=cm, dt=np.float64(dt), gam=np.float64(gam), three=idx,
+               N_tilde=np.int64(N_tilde), pq=np.array(pq, np.int32), events=ref.events(),
+               counts=ref.fragment_counts(), n_pairs=np.int64(len(pairs)), pairs_digest=digest(pairs),
+               out_digest=digest(b2), out_exists_digest=digest(ex2), out_cm=cm2,
+               out_largest_id=np.int64(b2.shape[0] - 1))
+    ref.lib.orc_mesh_reset()
+    return out
+
+
 OUTPUT_FILES = ["stat.txt", "collision.txt", "mass.txt", "radius.txt", "x.txt", "y.txt", "z.txt", "vx.txt",
                 "vy.txt", "vz.txt", "readme.txt"]
 
@@ -142,7 +182,7 @@ def program_run_case(profile, bodies):
     return out
 
 
-def main():
+def main(names=None):
     out = {}
     out["grav_s05_n512"] = gravity_case("bf_grav_s05", 512, 11, holes=(3, 100, 511))
     out["grav_s0_n64"] = gravity_case("bf_grav_s0", 64, 12, holes=(0,))
@@ -157,10 +197,16 @@ def main():
     out["mesh_inelastic"] = mesh_case("mesh_inelastic_s", 6000, 22, 0.03, 5e-4)
     # the N = 2,000 collisional disk, 200 steps, output every 50 steps
     out["program_bf_merge"] = program_run_case("bf_merge", disks.bf_collide_disk(2000, seed=0))
+    # fragmentation: every outcome in one sweep (dt = 0.02 on the crowded ring)
+    out["frag_bf"] = frag_bf_case("bf_frag", 4000, 0, 0.02)
+    out["frag_mesh15"] = frag_mesh_case("mesh_frag_s", 4000, 0, 0.01, 0.02, 15, (-1, 3, -1, 1))
+    out["frag_mesh4"] = frag_mesh_case("mesh_frag4_s", 4000, 1, 0.01, 0.02, 4, (0, 1, 0, 1))
     for k, v in out.items():
+        if names and k not in names:
+            continue
         np.savez_compressed(os.path.join(HERE, k + ".npz"), **v)
         print("wrote", k)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:] or None)

@@ -118,3 +118,43 @@ def test_port_end_of_timestep_vs_reference():
     pb, pex, pcm = w.get_state()
     assert hm == int(sc[2]) == 810
     assert np.array_equal(rb, pb) and np.array_equal(rex, pex) and np.array_equal(rcm, pcm)
+
+
+def test_port_fragmentation_sweep_matches_golden():
+    """brute_force() with the fragmentation model (src/physics.c:710-1040):
+    merger, super-catastrophic, partial and full outcomes in one sweep."""
+    g = golden("frag_bf")
+    w = oracle.PortWorld(16384, make_params(collision_bool=1, collision_type=3))
+    w.set_fragmentation()
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=float(g["dt"]))
+    w.lib.orc_w_brute_force()
+    b, ex, cm = w.get_state()
+    assert w.lib.orc_w_fragment_error() == 0
+    assert np.array_equal(w.fragment_counts(), g["counts"]) and np.all(g["counts"] > 0)
+    assert np.array_equal(w.events(), g["events"])
+    assert b.shape[0] - 1 == int(g["out_largest_id"])
+    assert np.array_equal(_digest(b), g["out_digest"]) and np.array_equal(_digest(ex), g["out_exists_digest"])
+    assert np.array_equal(cm, g["out_cm"])
+
+
+@pytest.mark.parametrize("name", ["frag_mesh15", "frag_mesh4"])
+def test_port_fragmentation_mesh_matches_golden(name):
+    """mesh() with the fragmentation model: fragments appended past the sweep's
+    largest_id, their mutual pairs in pairs[] (N_tilde 15 and the 2 x 2 lattice)."""
+    g = golden(name)
+    p = make_params(mesh_bool=1, brute_force_bool=0, collision_bool=1, collision_type=3, collision_cube_cells=256)
+    w = oracle.PortWorld(70000, p)
+    w.set_fragmentation(int(g["N_tilde"]), tuple(int(v) for v in g["pq"]))
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=float(g["dt"]), gam=float(g["gam"]))
+    assert np.array_equal(w.three_largest(), g["three"])
+    w.lib.orc_w_mesh()
+    pairs = w.pairs()
+    assert w.lib.orc_w_fragment_error() == 0
+    assert np.array_equal(w.fragment_counts(), g["counts"])
+    assert np.array_equal(w.events(), g["events"])
+    assert len(pairs) == int(g["n_pairs"]) and np.array_equal(_digest(pairs), g["pairs_digest"])
+    b, ex, cm = w.get_state()
+    assert b.shape[0] - 1 == int(g["out_largest_id"])
+    assert np.array_equal(_digest(b), g["out_digest"]) and np.array_equal(_digest(ex), g["out_exists_digest"])
+    assert np.array_equal(cm, g["out_cm"])
+    w.lib.orc_w_mesh_reset()
