@@ -40,6 +40,17 @@ WORKLOAD = ("gravity-only single-step accelerations, N=65,536 disk (a~U[0.8,1.2]
 REF_SAMPLE = 16384  # bodies per reference-arm step (bounded CPU sample)
 
 
+def max_over_ranks(values, ws, device="cpu"):
+    """Element-wise maximum of `values` over all ranks (the slowest rank's
+    time); identity on a single rank."""
+    if ws <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
 def dist_info():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -226,6 +237,62 @@ def bench_mesh(lib, api, torch, mode, steps, warmup):
             "pairs_per_step": pairs / steps, "bodies_end": hm, "gpu_launches": launches}
 
 
+FRAG_N = 262144
+FRAG_DT = 2e-4
+FRAG_STEPS = 100
+FRAG_WORKLOAD = ("collisional fragmenting disk, N_0=262,144 (a~U[0.9,1.1], e,i~Rayleigh 0.02, R~U[2e-4,5e-4], "
+                 "density 3), mesh collision search (1024 cells, collision_cube_min 4.4) with the fragmentation "
+                 "model (N_tilde 4 on the lattice {0,1,0,1}, fragments appended on the device, N_max 1,048,576), "
+                 "brute-force gravity of the stated mode over every body, dt=2e-4; a shortened run of 100 steps "
+                 "of the 10,000-step workload")
+
+
+def frag_params(mode):
+    from ncorpion_b200 import api
+    return api.default_params(G=1.0, softening_parameter=0.0, collision_bool=1, brute_force_bool=0, mesh_bool=1,
+                              collision_type=api.COLLISION_FRAGMENTATION, collision_cube_cells=1024,
+                              how_many_neighbours=16.0, collision_cube_min=4.4, gravity_mode=mode,
+                              disruption_threshold=0.1, high_dumping_threshold=100.0, N_tilde=4,
+                              pq_min_max=(C.c_int * 4)(0, 1, 0, 1), mesh_brute_gravity=1)
+
+
+def bench_fragment(lib, api, torch, mode, steps):
+    """Steps/s and energy drift of the fragmenting disk: mesh collisions with
+    fragmentation, brute-force gravity of `mode`; CUDA events on the library
+    stream around each step, energy (FP64, O(N^2)) before and after."""
+    from ncorpion_b200 import disks
+    b = disks.fragment_disk(FRAG_N, seed=0)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    b, cm = disks.reduce_to_com(b, cm)
+    api.init(1 << 20, frag_params(mode))
+    api.upload(b, np.ones(FRAG_N, np.int32), cm)
+    gmin = 4.4 / 1024
+    gam = gmin
+    api.set_timestep(FRAG_DT)
+    e0 = api.energy()
+    st = torch.cuda.ExternalStream(lib.ncgpu_stream())
+    ms, launches, hm = [], 0, FRAG_N
+    for _ in range(steps):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(st)
+        hm, tn = api.step_mesh(gam)
+        ev1.record(st)
+        ev1.synchronize()
+        ms.append(ev0.elapsed_time(ev1))
+        launches += lib.ncgpu_last_launch_count()
+        gam = api.update_gamma(gam, tn, hm, 16.0, gmin)
+    e1 = api.energy()
+    counts = api.fragment_counts()
+    api.finalize()
+    t = float(np.sum(ms)) / 1e3
+    return {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps, "steps": steps, "bodies_end": int(hm),
+            "outcomes": {"merger": int(counts[0]), "super_catastrophic": int(counts[1]), "partial": int(counts[2]),
+                         "full": int(counts[3])},
+            "energy_start": float(e0[0]), "energy_end": float(e1[0]),
+            "energy_drift_rel": float((e1[0] - e0[0]) / abs(e0[0])), "gpu_launches": launches}
+
+
 def mesh_cpu_reference(nsteps=3):
     """The reference's mesh() + mesh gravity loop (oracle/_ref/mesh_merge_1m,
     1 thread, 8.6 GB hash table) for a few steps of the same disk."""
@@ -254,6 +321,7 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mesh", action="store_true")
+    ap.add_argument("--no-frag", action="store_true")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
     ws, rank, local = dist_info()
@@ -313,12 +381,7 @@ def main(argv=None):
             torch.cuda.synchronize()
             if ws > 1:
                 torch.distributed.barrier()
-        ms = tot / steps
-        kms = float(np.mean(kern))
-        if ws > 1:
-            t = torch.tensor([ms, kms], dtype=torch.float64, device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms, kms = float(t[0]), float(t[1])
+        ms, kms = max_over_ranks([tot / steps, float(np.mean(kern))], ws, dev)
         return ms, kms, launches
 
     clock = ClockSampler(local)
@@ -355,23 +418,25 @@ def main(argv=None):
                                          api.GRAVITY_MIXED), "e2e")
         hb[:] = b
     e2e_t = []
+    lst = torch.cuda.ExternalStream(lib.ncgpu_stream())
     for _ in range(a.steps):
         hb[:] = b
         flush.zero_()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(lst)  # the library stream carries the copies in, the kernels and the copies out
         api.check(lib.ncgpu_vector_field(api.ptr(hb), api.ptr(hex_), n - 1, api.ptr(cmh), api.ptr(cma),
                                          api.GRAVITY_MIXED), "e2e")
-        e2e_t.append(time.perf_counter() - t0)
+        e1.record(lst)
+        e1.synchronize()
+        e2e_t.append(e0.elapsed_time(e1) * 1e-3)
     lib.ncgpu_host_unregister(api.ptr(hb))
     lib.ncgpu_host_unregister(api.ptr(hex_))
-    e2e_s = float(np.mean(e2e_t))
-    if ws > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t[0])
+    e2e_s = max_over_ranks([float(np.mean(e2e_t))], ws, dev)[0]
 
-    fp32_peak = api.probe_fp32_peak()
+    rates = api.probe_fp32_rates()
+    fp32_peak = max(rates["ffma_tflops"], rates["ffma2_tflops"])
     api.finalize()
 
     mesh = None
@@ -397,6 +462,15 @@ def main(argv=None):
                              "algorithmic_bytes_per_step": alg, "traffic": None,
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
                 "cpu_baseline": mesh_cpu_reference() if (rank == 0 and ws == 1 and not a.no_cpu_baseline) else None}
+    frag = None
+    if not a.no_frag:
+        fm = bench_fragment(lib, api, torch, api.GRAVITY_MIXED, FRAG_STEPS)
+        f64 = bench_fragment(lib, api, torch, api.GRAVITY_FP64, FRAG_STEPS)
+        frag = {"metric": "fragmenting-disk steps/s and energy drift", "workload": FRAG_WORKLOAD, "mixed": fm,
+                "fp64": f64,
+                "note": "no reference mode couples mesh collisions with brute-force gravity; the energy includes "
+                        "the collisions' own losses, so the mixed-minus-FP64 difference of the drift is the "
+                        "gravity precision's share"}
     achieved = FLOP_PER_INTERACTION * pairs / (kms_mixed * 1e-3) / 1e12
 
     cpu = None
@@ -423,7 +497,10 @@ def main(argv=None):
                          "frac": achieved / fp32_peak, "traffic": None,
                          "kernel": "k_grav_tiled<mixed>", "kernel_ms": kms_mixed,
                          "flop_per_interaction": FLOP_PER_INTERACTION,
-                         "peak_source": "measured FFMA-chain probe (ncgpu_probe_fp32_peak) in this run"},
+                         "peak_source": "measured in this run: best of the scalar FFMA and packed f32x2 FMA "
+                                        "dependency-chain probes (ncgpu_probe_fp32_rates)",
+                         "probes": rates,
+                         "rsqrt_bound_frac": pairs / (kms_mixed * 1e-3) / (rates["rsqrt_gops"] * 1e9)},
             "cpu_baseline": cpu,
             "e2e": {"value": ws * pairs / e2e_s, "unit": "pair-interactions/s",
                     "h2d_bytes_per_step": int(hb.nbytes + hex_.nbytes), "d2h_bytes_per_step": int(n * 24 + 24),
@@ -437,6 +514,7 @@ def main(argv=None):
             "speedup_mixed_vs_fp64_exact": ms_exact / ms_mixed,
             "speedup_mixed_vs_fp64_tiled": ms_fp64t / ms_mixed,
             "mesh": mesh,
+            "fragment": frag,
             "accuracy": {"mutual_rel_err_max": float(rel_mut.max()),
                          "mutual_rel_err_median": float(np.median(rel_mut)),
                          "total_rel_err_max": float(rel_tot.max()),

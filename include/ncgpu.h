@@ -26,6 +26,8 @@ extern "C" {
 #define NCGPU_E_STATE (-5)     /* ncgpu_init was not called / state not uploaded      */
 #define NCGPU_E_TIMEOUT (-6)   /* a bounded device-side wait gave up                  */
 #define NCGPU_E_UNSUPPORTED (-7) /* configuration outside the implemented hot path    */
+#define NCGPU_E_FRAGMENT (-8)  /* fragmentation: a fragment slower than the escape
+                                  velocity (the reference aborts, src/physics.c:818,934) */
 
 /* Gravity arithmetic modes. */
 #define NCGPU_GRAVITY_EXACT 0  /* FP64, the reference's per-body summation order and
@@ -79,10 +81,28 @@ struct ncgpu_params {
       double par_disruption_threshold;   /* disruption_threshold (dump into the CM)  */
       double par_high_dumping_threshold; /* high_dumping_threshold (dump, unbound)   */
       int par_reduce_to_COM_bool;        /* reduce_to_COM_bool                       */
+      /* fragmentation model, collision type NCGPU_COLLISION_FRAGMENTATION
+         (src/parameters.h:297-307) */
+      int par_N_tilde;                   /* N_tilde (<= NCGPU_MAX_N_TILDE)           */
+      int par_pq_min_max[4];             /* pq_min_max {p_min, p_max, q_min, q_max};
+                                            (p_max-p_min+1)(q_max-q_min+1) = N_tilde  */
+      double par_mu_parameter;           /* mu_parameter                             */
+      double par_nu_parameter;           /* nu_parameter                             */
+      double par_C1_parameter;           /* C1_parameter                             */
+      double par_k_parameter;            /* k_parameter                              */
+      double par_merging_threshold;      /* merging_threshold                        */
+      double par_fragment_threshold;     /* fragment_threshold                       */
+      /* Mesh driver only, no reference counterpart: 1 replaces the mesh gravity
+         (pairs[] + the three largest bodies) by the brute-force field of
+         par_gravity_mode over every body, keeping the mesh collision search. */
+      int par_mesh_brute_gravity;
 };
+#define NCGPU_MAX_N_TILDE 64
 
 /* Fills *p with the reference's default values for the fields above
-   (G = 39.478..., softening 0, central mass on, mutual on, ...). */
+   (fragmentation constants: N_tilde 15 on {-1,3,-1,1}, mu 0.55, nu 0.4,
+   C1 1.5, k 0.2, merging 2e-4, fragment 1.5e-8, src/parameters.h:297-307)
+   and G = 39.478..., softening 0, central mass on, mutual on, ... */
 void ncgpu_default_params(struct ncgpu_params *p);
 
 /* Allocates device state for n_max body slots (N_max, src/parameters.h:171)
@@ -152,6 +172,10 @@ int ncgpu_host_unregister(void *ptr);
    kernel (2 flops per FFMA) and returns it in *tflops; used as the roofline
    denominator of the FP32 gravity kernel. */
 int ncgpu_probe_fp32_peak(double *tflops);
+/* Diagnostic (no reference counterpart): measured FP32 rates of this GPU,
+   from independent dependency chains: scalar FFMA and packed f32x2 FMA in
+   TFLOP/s (2 flops per FMA lane), and rsqrt.approx.f32 in Gop/s. */
+int ncgpu_probe_fp32_rates(double *ffma_tflops, double *ffma2_tflops, double *rsqrt_gops);
 
 /* Diagnostic: out[i] = x[i]^(1.0/3.0), correctly rounded, as the device
    merger computes the merged radius (src/physics.c:684). */
@@ -180,6 +204,16 @@ int ncgpu_drift(void);
    *n_events receives the number of collision_treatment calls. */
 int ncgpu_collide_brute(int *n_events);
 
+/* Total energy of the device state (no reference counterpart; the reference
+   has no energy output): out[0] = E, out[1] = kinetic (bodies and central
+   body), out[2] = central-body potential, out[3] = mutual potential with the
+   force's softening sqrt(r^2 + (softening_parameter (R_k + R_p))^2).  FP64,
+   O(N^2), deterministic; for energy-drift diagnostics. */
+int ncgpu_energy(double *out);
+/* Outcomes of the fragmentation model since the last upload, in the order of
+   merger_count, super_catastrophic_count, half_fragmentation_count and
+   full_fragmentation_count (src/structure.h:148-151). */
+int ncgpu_fragment_counts(int *counts);
 /* The events of the last sweep, in resolution order: (a, b, type) as passed to
    collision_treatment, and optionally 8 doubles per event for the collision
    output file: time_until_collision, m_A, m_B, R_A, R_B (A the heavier body,

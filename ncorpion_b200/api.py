@@ -14,7 +14,7 @@ import numpy as np
 from . import LIB_PATH
 
 OK = 0
-E_ARG, E_CUDA, E_CAPACITY, E_NMAX, E_STATE, E_TIMEOUT, E_UNSUPPORTED = -1, -2, -3, -4, -5, -6, -7
+E_ARG, E_CUDA, E_CAPACITY, E_NMAX, E_STATE, E_TIMEOUT, E_UNSUPPORTED, E_FRAGMENT = -1, -2, -3, -4, -5, -6, -7, -8
 
 GRAVITY_EXACT, GRAVITY_FP64, GRAVITY_MIXED = 0, 1, 2
 GRAVITY_MODES = {"exact": GRAVITY_EXACT, "fp64": GRAVITY_FP64, "mixed": GRAVITY_MIXED}
@@ -44,6 +44,15 @@ class Params(C.Structure):
         ("disruption_threshold", C.c_double),
         ("high_dumping_threshold", C.c_double),
         ("reduce_to_COM_bool", C.c_int),
+        ("N_tilde", C.c_int),
+        ("pq_min_max", C.c_int * 4),
+        ("mu_parameter", C.c_double),
+        ("nu_parameter", C.c_double),
+        ("C1_parameter", C.c_double),
+        ("k_parameter", C.c_double),
+        ("merging_threshold", C.c_double),
+        ("fragment_threshold", C.c_double),
+        ("mesh_brute_gravity", C.c_int),
     ]
 
 
@@ -95,8 +104,11 @@ EXPORTS = {
     "ncgpu_host_register": (C.c_int, [P, C.c_ulong]),
     "ncgpu_host_unregister": (C.c_int, [P]),
     "ncgpu_probe_fp32_peak": (C.c_int, [P]),
+    "ncgpu_probe_fp32_rates": (C.c_int, [P, P, P]),
     "ncgpu_last_kernel_ms": (C.c_int, [P]),
     "ncgpu_collide_brute": (C.c_int, [P]),
+    "ncgpu_fragment_counts": (C.c_int, [P]),
+    "ncgpu_energy": (C.c_int, [P]),
     "ncgpu_probe_pow_third": (C.c_int, [P, P, C.c_int]),
     "ncgpu_get_events": (C.c_int, [P, P, C.c_int, P]),
     "ncgpu_end_of_timestep": (C.c_int, [P]),
@@ -166,6 +178,14 @@ def probe_fp32_peak() -> float:
     v = C.c_double(0.0)
     check(load().ncgpu_probe_fp32_peak(C.byref(v)), "ncgpu_probe_fp32_peak")
     return v.value
+
+
+def probe_fp32_rates() -> dict:
+    """Measured FP32 rates: scalar FFMA and packed f32x2 FMA (TFLOP/s) and
+    rsqrt.approx (Gop/s)."""
+    a, b, c = C.c_double(), C.c_double(), C.c_double()
+    check(load().ncgpu_probe_fp32_rates(C.byref(a), C.byref(b), C.byref(c)), "ncgpu_probe_fp32_rates")
+    return {"ffma_tflops": a.value, "ffma2_tflops": b.value, "rsqrt_gops": c.value}
 
 
 def last_kernel_ms() -> float:
@@ -348,4 +368,18 @@ def leapfrog_jvp(x0, v0, m, R, cm, dt, nsteps, tan_x0, tan_v0, tan_m):
                      int(nsteps), 32, None, None, None, None, None, None, tx.ctypes.data, tv.ctypes.data,
                      tm.ctypes.data, out.ctypes.data)
     check(load().ncgpu_leapfrog_jvp(C.byref(a)), "ncgpu_leapfrog_jvp")
+    return out
+
+
+def fragment_counts() -> np.ndarray:
+    """(merger, super-catastrophic, partial, full) outcomes since the upload."""
+    out = np.zeros(4, np.int32)
+    check(load().ncgpu_fragment_counts(ptr(out)), "ncgpu_fragment_counts")
+    return out
+
+
+def energy() -> np.ndarray:
+    """(E, kinetic, central potential, mutual potential) of the device state."""
+    out = np.zeros(4)
+    check(load().ncgpu_energy(ptr(out)), "ncgpu_energy")
     return out

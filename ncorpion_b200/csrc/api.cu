@@ -43,6 +43,7 @@ int check_err_word()
       if (h) NCG_CK(cudaMemsetAsync(c.err, 0, sizeof(unsigned), c.s));
       if (h & ERR_TIMEOUT) return NCGPU_E_TIMEOUT;
       if (h & ERR_NMAX) return NCGPU_E_NMAX;
+      if (h & ERR_FRAGMENT) return NCGPU_E_FRAGMENT;
       if (h & ERR_CAPACITY) return NCGPU_E_CAPACITY;
       if (h) return NCGPU_E_CUDA;
       return NCGPU_OK;
@@ -162,7 +163,7 @@ int kick_state()
       double cm8[8];
       NCG_TRY(state_cm_host(cm8));
       const int nslots = c.largest_id + 1;
-      if (c.P.par_mesh_bool && !c.force_naive)
+      if (c.P.par_mesh_bool && !c.force_naive && !c.P.par_mesh_brute_gravity)
             NCG_TRY(mesh_gravity_state(cm8));
       else
             NCG_TRY(gravity_eval(state_view(), c.largest_id, cm8, c.acc, c.n_max, c.cm_acc, c.P.par_gravity_mode, c.s));
@@ -213,6 +214,18 @@ void ncgpu_default_params(struct ncgpu_params *p)
       p->par_disruption_threshold = 1.8;     // src/parameters.h:150
       p->par_high_dumping_threshold = 230.95;  // src/parameters.h:177
       p->par_reduce_to_COM_bool = 1;
+      p->par_N_tilde = 15;  // src/parameters.h:297-307
+      p->par_pq_min_max[0] = -1;
+      p->par_pq_min_max[1] = 3;
+      p->par_pq_min_max[2] = -1;
+      p->par_pq_min_max[3] = 1;
+      p->par_mu_parameter = 0.55;
+      p->par_nu_parameter = 0.4;
+      p->par_C1_parameter = 1.5;
+      p->par_k_parameter = 0.2;
+      p->par_merging_threshold = 0.0002;
+      p->par_fragment_threshold = 1.5e-8;
+      p->par_mesh_brute_gravity = 0;
 }
 
 const char *ncgpu_strerror(int s)
@@ -226,6 +239,8 @@ const char *ncgpu_strerror(int s)
       case NCGPU_E_STATE: return "library not initialised or state not uploaded";
       case NCGPU_E_TIMEOUT: return "device-side wait timed out";
       case NCGPU_E_UNSUPPORTED: return "configuration not supported by the GPU path";
+      case NCGPU_E_FRAGMENT:
+            return "Error: In function fragmentation, the velocity of a fragment cannot be less than the escape velocity.";
       default: return "unknown status";
       }
 }
@@ -270,6 +285,13 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
             float *p = nullptr;
             A(p, 4 * npad);
             c.src32 = p;
+      }
+      {
+            int dev = 0;
+            NCG_CK(cudaGetDevice(&dev));
+            NCG_CK(cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, dev));
+            const char *e = getenv("NCGPU_GRAV_SLOTS_MULT");
+            if (e && atoi(e) > 0) c.grav_slots_mult = atoi(e);
       }
       A(c.srcR32, npad);
       A(c.tilebox, 6 * (npad / 128));

@@ -92,6 +92,7 @@ struct EvArgs {
       int mesh_bool;
       int ev_cap;
       int dcap;
+      FragArgs frag;            // fragmentation constants (type 3)
 };
 
 // collision_treatment(a, b, type) with the device state; records the event.
@@ -124,15 +125,17 @@ __device__ void d_treat(const DevState &S, int a, int b, const EvArgs &E, int *e
             S.did[b] = E.one_only;
       } else if (E.type == NCGPU_COLLISION_MERGER) {
             d_merge(S, A, B, ap, E.one_only, E.mesh_bool, rec);
-      } else {
-            atomicOr(err, ERR_INTERNAL);  // fragmentation is resolved elsewhere
       }
+      FragOut fo;
+      fo.nids = 0;
+      if (E.type == NCGPU_COLLISION_FRAGMENTATION) d_fragment(S, A, B, ap, E.frag, rec, fo, err);
       S.scal[S_CCOUNT] += 1;
-      // mark both bodies; keep the ones that still exist for re-testing
+      // mark the bodies the resolution touched (new tail fragments included);
+      // the ones that still exist are re-tested against the rest of the sweep
       int nd = S.scal[S_NDIRTY];
-      int who[2] = {A, B};
-      for (int w = 0; w < 2; w++) {
-            int k = who[w];
+      const int nw = 2 + (fo.nids > 1 ? fo.nids - 1 : 0);
+      for (int w = 0; w < nw; w++) {
+            int k = w == 0 ? A : w == 1 ? B : fo.ids[w - 1];
             if (!dirty[k]) {
                   dirty[k] = 1;
                   if (nd < E.dcap) dlist[nd++] = k;
@@ -276,8 +279,8 @@ int collide_brute_state()
       if (nh > c.hit_cap / 2) return NCGPU_E_CAPACITY;
       NCG_TRY(sort_hits(nh, si, sj, lid, st));
       EvArgs E{lid, c.dt, c.P.par_collision_type, c.P.par_collision_parameter, c.P.par_one_collision_only_bool,
-               c.P.par_mesh_bool, c.ev_cap, c.n_max};
-      if (E.type == NCGPU_COLLISION_FRAGMENTATION) return NCGPU_E_UNSUPPORTED;
+               c.P.par_mesh_bool, c.ev_cap, c.n_max, FragArgs{}};
+      if (E.type == NCGPU_COLLISION_FRAGMENTATION && !make_frag_args(c, E.frag)) return NCGPU_E_ARG;
       k_bf_events<<<1, EVT, 0, st>>>(S, si, sj, E, c.ev, c.evrec, c.dirty, c.dlist, c.err);
       NCG_LAUNCHED();
       k_clear_dirty<<<32, 256, 0, st>>>(c.dirty, c.dlist, c.scal);
@@ -288,6 +291,17 @@ int collide_brute_state()
 }  // namespace ncg
 
 using namespace ncg;
+
+extern "C" int ncgpu_fragment_counts(int *counts)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      if (!counts) return NCGPU_E_ARG;
+      NCG_CK(cudaMemcpyAsync(counts, c.scal + S_FMERGE, 4 * sizeof(int), cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaStreamSynchronize(c.s));
+      return NCGPU_OK;
+}
 
 extern "C" int ncgpu_collide_brute(int *n_events)
 {

@@ -50,12 +50,15 @@ enum : unsigned {
       ERR_NMAX = 2u,
       ERR_TIMEOUT = 4u,
       ERR_INTERNAL = 8u,
+      ERR_FRAGMENT = 16u,
 };
 
 // Scratch and state owned by the library, sized from n_max at ncgpu_init.
 struct Ctx {
       int inited = 0;
       int n_max = 0;
+      int sm_count = 148;      // multiprocessors of the current device (set by ncgpu_init)
+      int grav_slots_mult = 32; // tiled gravity: CTAs per resident CTA slot (measured best of 2..32)
       ncgpu_params P{};
       cudaStream_t s = nullptr;
 
@@ -124,6 +127,18 @@ struct Ctx {
       long pair_cap = 0;
       int *occ = nullptr;
       int occ_cap = 0;
+      // fragmentation in a mesh pass: per-event records (EVX ints: candidate
+      // position, extra-pair offset, extra-pair count, first tail fragment,
+      // largest fragment A, next full fragmentation of the same A), the tail's
+      // pairs, per-slot heads of those chains (-1), full events in order
+      int *evx = nullptr;
+      int *xpairs = nullptr;
+      long xpair_cap = 0;
+      int *xhead = nullptr;
+      int *fev = nullptr;
+      int mesh_nev = 0;            // events recorded by the last mesh pass
+      int mesh_nfev = 0;           // full fragmentations of the last mesh pass
+      int mesh_nx = 0;             // extra pairs of the last mesh pass
       int mesh_valid = 0;          // cell table populated by the last pass
       int mesh_n = 0;              // sorted entries of the last pass (largest_id + 1)
       int n_cand = 0, n_pairs = 0;
@@ -147,12 +162,21 @@ enum Scal : int {
       S_NBIG = 10,      // bodies larger than the mesh size
       S_NDROP = 11,     // candidates dropped by removals
       S_NINS = 12,      // bodies inserted in the cell table
-      S_COUNT = 16
+      S_FMERGE = 13,    // merger_count (fragmentation model outcomes, src/structure.h:148-151)
+      S_FSUPER = 14,    // super_catastrophic_count
+      S_FHALF = 15,     // half_fragmentation_count
+      S_FFULL = 16,     // full_fragmentation_count
+      S_NXPAIRS = 17,   // fragment pairs appended by a mesh pass (extra pairs)
+      S_NSKIP = 18,     // mesh event candidates that append no pair of their own
+      S_NFEV = 19,      // full fragmentations of a mesh pass
+      S_COUNT = 24
 };
 
 // Per-event record fields (doubles) kept for the collision output file
 // (collisionData, src/display.c): t_coll, m_A, m_B, R_A, R_B, DeltaV, dr.dv.
 constexpr int EVREC = 8;
+// Per-event ints of a mesh pass (see Ctx::evx).
+constexpr int EVX = 8;
 
 Ctx &ctx();
 int ensure_partial(size_t doubles);

@@ -294,19 +294,29 @@ __global__ void k_tilebox(const D4 *__restrict__ s64, int n, int ntiles, double 
       }
 }
 
-// FP32 tile-relative sources: (x - c, y - c, z - c, m) of the tile the body is in.
+// FP32 tile-relative sources, one SoA block per tile of T bodies:
+// x[T] y[T] z[T] m[T] (coordinates minus the tile's box centre).  Padding
+// sources sit at 1e18 with zero mass, so their pair terms are exactly zero.
 __global__ void k_pack32(const D4 *__restrict__ s64, const double *__restrict__ sR, const double *__restrict__ box,
-                         int n, int npad, float4 *__restrict__ s32, float *__restrict__ sR32)
+                         int n, int npad, float *__restrict__ s32, float *__restrict__ sR32)
 {
       int q = blockIdx.x * blockDim.x + threadIdx.x;
       if (q >= npad) return;
+      float *tile = s32 + (size_t)(q / T) * 4 * T;
+      const int j = q % T;
       if (q < n) {
             const double *c = box + (q / T) * 6;
             D4 s = s64[q];
-            s32[q] = make_float4((float)(s.x - c[0]), (float)(s.y - c[1]), (float)(s.z - c[2]), (float)s.w);
+            tile[j] = (float)(s.x - c[0]);
+            tile[T + j] = (float)(s.y - c[1]);
+            tile[2 * T + j] = (float)(s.z - c[2]);
+            tile[3 * T + j] = (float)s.w;
             sR32[q] = (float)sR[q];
       } else {
-            s32[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+            tile[j] = 1e18f;
+            tile[T + j] = 1e18f;
+            tile[2 * T + j] = 1e18f;
+            tile[3 * T + j] = 0.f;
             sR32[q] = 0.f;
       }
 }
@@ -379,44 +389,118 @@ __device__ __forceinline__ float rsqrt_ftz(float x)
       return y;
 }
 
-// FP32 pair sums of one far tile for two targets at tile-relative positions
-// (x0..z0), (x1..z1).  SM 0: no softening; 1: uniform eps^2; 2: eps = sR_i + sR_j.
+// Packed pairs of FP32 values (sm_100a f32x2 arithmetic: one instruction
+// operates on both halves).
+typedef unsigned long long f2;
+
+__device__ __forceinline__ f2 f2_pack(float lo, float hi)
+{
+      f2 r;
+      asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+      return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 v, float &lo, float &hi)
+{
+      asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 f2_sub(f2 a, f2 b)
+{
+      f2 r;
+      asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+      return r;
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b)
+{
+      f2 r;
+      asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+      return r;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b)
+{
+      f2 r;
+      asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+      return r;
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c)
+{
+      f2 r;
+      asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+      return r;
+}
+__device__ __forceinline__ f2 f2_rsqrt(f2 q)
+{
+      float lo, hi;
+      f2_unpack(q, lo, hi);
+      return f2_pack(rsqrt_ftz(lo), rsqrt_ftz(hi));
+}
+__device__ __forceinline__ float f2_hsum(f2 v)
+{
+      float lo, hi;
+      f2_unpack(v, lo, hi);
+      return lo + hi;
+}
+
+// One source pair against one target: adds m_j dx / (r^2 + eps^2)^(3/2) of
+// both sources into the packed partial sums P (SM 0: no softening; 1: uniform
+// eps^2 in E; 2: eps = R_target + R_source, with RT/RS the radii).
+template <int SM>
+__device__ __forceinline__ void pair_term(f2 XS, f2 YS, f2 ZS, f2 MS, f2 RS, f2 XT, f2 YT, f2 ZT, f2 RT, f2 E,
+                                          f2 &Px, f2 &Py, f2 &Pz)
+{
+      const f2 dx = f2_sub(XS, XT), dy = f2_sub(YS, YT), dz = f2_sub(ZS, ZT);
+      f2 q;
+      if (SM == 0) {
+            q = f2_mul(dx, dx);
+      } else if (SM == 1) {
+            q = f2_fma(dx, dx, E);
+      } else {
+            const f2 e = f2_add(RS, RT);
+            q = f2_fma(dx, dx, f2_mul(e, e));
+      }
+      q = f2_fma(dy, dy, q);
+      q = f2_fma(dz, dz, q);
+      const f2 i = f2_rsqrt(q);
+      const f2 w = f2_mul(f2_mul(MS, i), f2_mul(i, i));
+      Px = f2_fma(w, dx, Px);
+      Py = f2_fma(w, dy, Py);
+      Pz = f2_fma(w, dz, Pz);
+}
+
+// FP32 pair sums of one far tile (SoA x[T] y[T] z[T] m[T], radii tr[T]) for two
+// targets at tile-relative positions (x0..z0), (x1..z1).  Each 128-bit shared
+// load brings four sources of one component, processed as two f32x2 pairs.
 // Runs of 32 sources are summed in FP32 and Kahan-added per tile; the tile
 // total is folded into the FP64 accumulators.
-template <int SM, bool FULL>
-__device__ __forceinline__ void far_tile(const float4 *__restrict__ tl, const float *__restrict__ tr, int cnt,
-                                         float x0, float y0, float z0, float x1, float y1, float z1, float r0f,
-                                         float r1f, float eps2f, double (&a0)[3], double (&a1)[3])
+template <int SM>
+__device__ __forceinline__ void far_tile(const float *__restrict__ tl, const float *__restrict__ tr, float x0,
+                                         float y0, float z0, float x1, float y1, float z1, float r0f, float r1f,
+                                         float eps2f, double (&a0)[3], double (&a1)[3])
 {
+      const f2 X0 = f2_pack(x0, x0), Y0 = f2_pack(y0, y0), Z0 = f2_pack(z0, z0);
+      const f2 X1 = f2_pack(x1, x1), Y1 = f2_pack(y1, y1), Z1 = f2_pack(z1, z1);
+      const f2 R0 = f2_pack(r0f, r0f), R1 = f2_pack(r1f, r1f), E = f2_pack(eps2f, eps2f);
+      const ulonglong2 *xs = (const ulonglong2 *)tl, *ys = (const ulonglong2 *)(tl + T);
+      const ulonglong2 *zs = (const ulonglong2 *)(tl + 2 * T), *ms = (const ulonglong2 *)(tl + 3 * T);
+      const ulonglong2 *rs = (const ulonglong2 *)tr;
       float S0[3] = {0.f, 0.f, 0.f}, C0[3] = {0.f, 0.f, 0.f};
       float S1[3] = {0.f, 0.f, 0.f}, C1[3] = {0.f, 0.f, 0.f};
-      const int n = FULL ? T : cnt;
-      for (int jb = 0; jb < n; jb += 32) {
-            float p0x = 0.f, p0y = 0.f, p0z = 0.f, p1x = 0.f, p1y = 0.f, p1z = 0.f;
-            const int je = FULL ? 32 : min(32, n - jb);
-#pragma unroll 8
-            for (int jj = 0; jj < je; ++jj) {
+      for (int jb = 0; jb < T / 4; jb += 8) {
+            f2 p0x = 0ull, p0y = 0ull, p0z = 0ull, p1x = 0ull, p1y = 0ull, p1z = 0ull;
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) {
                   const int j = jb + jj;
-                  const float4 s = tl[j];
-                  float q0 = SM == 1 ? eps2f : 0.f, q1 = SM == 1 ? eps2f : 0.f;
-                  if (SM == 2) {
-                        const float rj = tr[j];
-                        const float e0 = r0f + rj, e1 = r1f + rj;
-                        q0 = e0 * e0;
-                        q1 = e1 * e1;
-                  }
-                  const float dx0 = s.x - x0, dy0 = s.y - y0, dz0 = s.z - z0;
-                  const float dx1 = s.x - x1, dy1 = s.y - y1, dz1 = s.z - z1;
-                  q0 = fmaf(dx0, dx0, q0); q0 = fmaf(dy0, dy0, q0); q0 = fmaf(dz0, dz0, q0);
-                  q1 = fmaf(dx1, dx1, q1); q1 = fmaf(dy1, dy1, q1); q1 = fmaf(dz1, dz1, q1);
-                  const float i0 = rsqrt_ftz(q0), i1 = rsqrt_ftz(q1);
-                  const float w0 = (s.w * i0) * (i0 * i0);
-                  const float w1 = (s.w * i1) * (i1 * i1);
-                  p0x = fmaf(w0, dx0, p0x); p0y = fmaf(w0, dy0, p0y); p0z = fmaf(w0, dz0, p0z);
-                  p1x = fmaf(w1, dx1, p1x); p1y = fmaf(w1, dy1, p1y); p1z = fmaf(w1, dz1, p1z);
+                  const ulonglong2 X = xs[j], Y = ys[j], Z = zs[j], M = ms[j];
+                  ulonglong2 R = make_ulonglong2(0ull, 0ull);
+                  if (SM == 2) R = rs[j];
+                  pair_term<SM>(X.x, Y.x, Z.x, M.x, R.x, X0, Y0, Z0, R0, E, p0x, p0y, p0z);
+                  pair_term<SM>(X.x, Y.x, Z.x, M.x, R.x, X1, Y1, Z1, R1, E, p1x, p1y, p1z);
+                  pair_term<SM>(X.y, Y.y, Z.y, M.y, R.y, X0, Y0, Z0, R0, E, p0x, p0y, p0z);
+                  pair_term<SM>(X.y, Y.y, Z.y, M.y, R.y, X1, Y1, Z1, R1, E, p1x, p1y, p1z);
             }
-            kahan_add(S0[0], C0[0], p0x); kahan_add(S0[1], C0[1], p0y); kahan_add(S0[2], C0[2], p0z);
-            kahan_add(S1[0], C1[0], p1x); kahan_add(S1[1], C1[1], p1y); kahan_add(S1[2], C1[2], p1z);
+            kahan_add(S0[0], C0[0], f2_hsum(p0x)); kahan_add(S0[1], C0[1], f2_hsum(p0y));
+            kahan_add(S0[2], C0[2], f2_hsum(p0z));
+            kahan_add(S1[0], C1[0], f2_hsum(p1x)); kahan_add(S1[1], C1[1], f2_hsum(p1y));
+            kahan_add(S1[2], C1[2], f2_hsum(p1z));
       }
       for (int d = 0; d < 3; d++) {
             a0[d] += (double)S0[d] - (double)C0[d];
@@ -429,13 +513,13 @@ __device__ __forceinline__ void far_tile(const float4 *__restrict__ tl, const fl
 // SOFT 0: no softening; 1: uniform epsilon^2 (all radii equal); 2: general.
 template <int MODE, int SOFT>
 __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, const double *__restrict__ sR64,
-                                                    const float4 *__restrict__ s32, const float *__restrict__ sR32,
+                                                    const float *__restrict__ s32, const float *__restrict__ sR32,
                                                     const double *__restrict__ box, int n, int ntiles, int tpc,
                                                     double theta, double eps2, double *__restrict__ partial,
                                                     long npad, unsigned *__restrict__ err,
                                                     const double *__restrict__ rrange, double sp)
 {
-      __shared__ float4 f4[2][T];
+      __shared__ alignas(16) float f4[2][4 * T];
       __shared__ alignas(16) float fr[2][T];
       __shared__ D4 d4[MODE == 1 ? 2 : 1][T];
       __shared__ alignas(16) double dr[MODE == 1 ? 2 : 1][T];
@@ -466,14 +550,14 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
       }
       __syncthreads();
       const unsigned bytes = MODE == 1 ? T * (sizeof(D4) + (SOFT == 2 ? sizeof(double) : 0))
-                                       : T * (sizeof(float4) + (SOFT == 2 ? sizeof(float) : 0));
+                                       : T * (4 * sizeof(float) + (SOFT == 2 ? sizeof(float) : 0));
       auto issue = [&](int t, int b) {
             mbar_arrive_expect(&bar[b], bytes);
             if (MODE == 1) {
                   bulk_g2s(d4[b], s64 + (size_t)t * T, T * sizeof(D4), &bar[b]);
                   if (SOFT == 2) bulk_g2s(dr[b], sR64 + (size_t)t * T, T * sizeof(double), &bar[b]);
             } else {
-                  bulk_g2s(f4[b], s32 + (size_t)t * T, T * sizeof(float4), &bar[b]);
+                  bulk_g2s(f4[b], s32 + (size_t)t * 4 * T, 4 * T * sizeof(float), &bar[b]);
                   if (SOFT == 2) bulk_g2s(fr[b], sR32 + (size_t)t * T, T * sizeof(float), &bar[b]);
             }
       };
@@ -515,16 +599,11 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
                         // FP32 path, coordinates relative to the source tile's centre
                         const float x0 = (float)(m0.x - bj[0]), y0 = (float)(m0.y - bj[1]), z0 = (float)(m0.z - bj[2]);
                         const float x1 = (float)(m1.x - bj[0]), y1 = (float)(m1.y - bj[1]), z1 = (float)(m1.z - bj[2]);
-                        const float4 *tl = f4[b];
+                        const float *tl = f4[b];
                         const float *tr = fr[b];
-                        if (cnt == T) {
-                              if (SOFT == 0) far_tile<0, true>(tl, tr, T, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
-                              else if (uni) far_tile<1, true>(tl, tr, T, x0, y0, z0, x1, y1, z1, r0f, r1f, eps2u, a0, a1);
-                              else far_tile<2, true>(tl, tr, T, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
-                        } else {
-                              if (SOFT == 0) far_tile<0, false>(tl, tr, cnt, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
-                              else far_tile<2, false>(tl, tr, cnt, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
-                        }
+                        if (SOFT == 0) far_tile<0>(tl, tr, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
+                        else if (uni) far_tile<1>(tl, tr, x0, y0, z0, x1, y1, z1, r0f, r1f, eps2u, a0, a1);
+                        else far_tile<2>(tl, tr, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
                   }
             }
             __syncthreads();
@@ -686,22 +765,32 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       k_tilebox<<<(ntiles * 32 + 255) / 256, 256, 0, st>>>(s64, n, ntiles, c.tilebox);
       NCG_LAUNCHED();
       if (mode == NCGPU_GRAVITY_MIXED) {
-            k_pack32<<<(npad + 255) / 256, 256, 0, st>>>(s64, c.srcR, c.tilebox, n, npad, (float4 *)c.src32, c.srcR32);
+            k_pack32<<<(npad + 255) / 256, 256, 0, st>>>(s64, c.srcR, c.tilebox, n, npad, (float *)c.src32, c.srcR32);
             NCG_LAUNCHED();
       }
-      // work decomposition: enough (target block, source chunk) units to fill the GPU
-      int nchunks = (4096 + ntiles - 1) / ntiles;
-      nchunks = max(1, min(nchunks, ntiles));
+      // softening: general (eps = sp (R_i + R_j)) unless sp == 0; the kernel
+      // takes its uniform-eps^2 path itself when all radii are equal
+      const int sm = soft ? 2 : 0;
+      // work decomposition: (target block, source chunk) CTAs, about
+      // grav_slots_mult per resident CTA slot, so that the last wave is short
+      // next to the whole launch (CTAs with near tiles run longer)
+      int occ = 1;
+      if (mode == NCGPU_GRAVITY_MIXED)
+            NCG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sm ? k_grav_tiled<0, 2> : k_grav_tiled<0, 0>, MXB, 0));
+      else
+            NCG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sm ? k_grav_tiled<1, 2> : k_grav_tiled<1, 0>, MXB, 0));
+      const long want = (long)max(occ, 1) * c.sm_count * c.grav_slots_mult;
+      long nch = (want + ntiles - 1) / ntiles;
+      if (nch < 1) nch = 1;
+      if (nch > ntiles) nch = ntiles;
+      int nchunks = (int)nch;
       const int tpc = (ntiles + nchunks - 1) / nchunks;
       nchunks = (ntiles + tpc - 1) / tpc;
       NCG_TRY(ensure_partial((size_t)nchunks * 3 * npad));
-      // softening: uniform epsilon when all radii are equal is detected on the
-      // host side by the caller through near_theta's sibling field; general otherwise
-      int sm = soft ? 2 : 0;
       double eps2 = 0.;
       double theta = P.par_near_theta > 0. ? P.par_near_theta : 0.25;
       dim3 grid(nchunks, ntiles);
-      const float4 *s32 = (const float4 *)c.src32;
+      const float *s32 = (const float *)c.src32;
       NCG_CK(cudaEventRecord(c.kev0, st));
 #define NCG_TILED(MODE_, SOFT_)                                                                              \
       k_grav_tiled<MODE_, SOFT_><<<grid, MXB, 0, st>>>(s64, c.srcR, s32, c.srcR32, c.tilebox, n, ntiles, tpc, \

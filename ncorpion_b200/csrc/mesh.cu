@@ -157,11 +157,23 @@ struct MeshEvArgs {
       int lid0, d, type, one_only, mesh_bool, ev_cap, dcap, occ_cap, nsorted;
       long long cell_cap;
       double dt, f_inelastic;
+      int add_pairs;            // mutual_bool: pairs[] is kept
+      long xpair_cap;
+      FragArgs frag;            // fragmentation constants (type 3)
 };
 
-// collision_treatment(p, k, type) at candidate position q (src/physics.c:1043)
+// Buffers of the fragmentation bookkeeping (see Ctx::evx).
+struct MeshFragBufs {
+      int *evx, *xpairs, *xhead, *fev;
+};
+
+// collision_treatment(p, k, type) at candidate position q (src/physics.c:1043).
+// Candidate flags: F_SWAP = pairs[] gets (p, k) here instead of (k, p)
+// (impulses; a partial fragmentation whose larger body is p); F_MERGED = no
+// pair of its own here (merger, super-catastrophic, full fragmentation: the
+// latter's tail pairs go to xpairs and are spliced in at this position).
 __device__ void d_mesh_treat(const DevState &S, int p, int k, int q, const MeshEvArgs &E, int *ev, double *evrec,
-                             unsigned char *cflag, unsigned *err, int *A_out, int *B_out)
+                             unsigned char *cflag, const MeshFragBufs &X, unsigned *err, int *A_out, int *B_out)
 {
       Approach ap;
       d_approach(S, p, k, E.dt, &ap);
@@ -169,12 +181,22 @@ __device__ void d_mesh_treat(const DevState &S, int p, int k, int q, const MeshE
       int A = m_a > m_b ? p : k, B = m_a > m_b ? k : p;
       int ne = S.scal[S_NEV];
       double *rec = nullptr;
+      int *ex_rec = nullptr;
       if (ne < E.ev_cap) {
             ev[3 * ne] = p;
             ev[3 * ne + 1] = k;
             ev[3 * ne + 2] = E.type;
             rec = evrec + (size_t)EVREC * ne;
             rec[0] = ap.t; rec[1] = S.m[A]; rec[2] = S.m[B]; rec[3] = S.R[A]; rec[4] = S.R[B];
+            ex_rec = X.evx + (size_t)EVX * ne;
+            ex_rec[0] = q;
+            ex_rec[1] = S.scal[S_NXPAIRS];
+            ex_rec[2] = 0;
+            ex_rec[3] = -1;
+            ex_rec[4] = A;
+            ex_rec[5] = -1;
+            ex_rec[6] = k;
+            ex_rec[7] = p;
       } else {
             atomicOr(err, ERR_CAPACITY);
       }
@@ -187,8 +209,48 @@ __device__ void d_mesh_treat(const DevState &S, int p, int k, int q, const MeshE
       } else if (E.type == NCGPU_COLLISION_MERGER) {
             d_merge(S, A, B, ap, E.one_only, E.mesh_bool, rec);
             cflag[q] |= F_MERGED;  // no pair appended
+            S.scal[S_NSKIP] += 1;
       } else {
-            atomicOr(err, ERR_INTERNAL);
+            FragOut fo;
+            d_fragment(S, A, B, ap, E.frag, rec, fo, err);
+            if (fo.outcome == 2) {
+                  if (A == p) cflag[q] |= F_SWAP;  // pairs[] gets (A, B)
+            } else {
+                  cflag[q] |= F_MERGED;
+                  S.scal[S_NSKIP] += 1;
+            }
+            if (fo.outcome == 3) {
+                  const int nt = fo.nids - 1;
+                  int nx = S.scal[S_NXPAIRS];
+                  const int cnt = E.add_pairs ? (nt + 1) * nt / 2 : 0;
+                  if ((long)nx + cnt > E.xpair_cap) {
+                        atomicOr(err, ERR_CAPACITY);
+                  } else {
+                        for (int a = 0; a <= nt && cnt; a++)
+                              for (int b = 0; b < a; b++) {
+                                    X.xpairs[2 * nx] = fo.ids[a];
+                                    X.xpairs[2 * nx + 1] = fo.ids[b];
+                                    nx++;
+                              }
+                        S.scal[S_NXPAIRS] = nx;
+                  }
+                  if (ex_rec) {
+                        ex_rec[2] = cnt;
+                        ex_rec[3] = fo.ids[1];  // the tail occupies fo.ids[1] .. fo.ids[1] + nt - 1
+                        int nf = S.scal[S_NFEV];
+                        X.fev[nf] = ne;
+                        S.scal[S_NFEV] = nf + 1;
+                        // chain of full fragmentations whose largest fragment is A
+                        int h = X.xhead[A];
+                        if (h < 0) {
+                              X.xhead[A] = ne;
+                        } else {
+                              int guard = 0;
+                              while (X.evx[(size_t)EVX * h + 5] >= 0 && ++guard < E.ev_cap) h = X.evx[(size_t)EVX * h + 5];
+                              X.evx[(size_t)EVX * h + 5] = ne;
+                        }
+                  }
+            }
       }
       S.scal[S_CCOUNT] += 1;
       *A_out = A;
@@ -206,7 +268,7 @@ __global__ void __launch_bounds__(MEV) k_mesh_events(DevState S, const int *__re
                                                      const int *__restrict__ vals, const int *__restrict__ cstart,
                                                      const int *__restrict__ hitpos, int nh, MeshEvArgs E, int *ev,
                                                      double *evrec, unsigned char *dirty, int *occ, int *ndrop,
-                                                     unsigned *err)
+                                                     MeshFragBufs X, unsigned *err)
 {
       __shared__ int best, hp_s, nocc, newb[2], newn, kq_s, q_s;
       if (threadIdx.x == 0) {
@@ -245,7 +307,7 @@ __global__ void __launch_bounds__(MEV) k_mesh_events(DevState S, const int *__re
             if (threadIdx.x == 0) {
                   int A, B;
                   int k = ck[q], p = cp[q];
-                  d_mesh_treat(S, p, k, q, E, ev, evrec, cflag, err, &A, &B);
+                  d_mesh_treat(S, p, k, q, E, ev, evrec, cflag, X, err, &A, &B);
                   int nn = 0;
                   if (!dirty[A]) { dirty[A] = 1; newb[nn++] = A; }
                   if (!dirty[B]) { dirty[B] = 1; newb[nn++] = B; }
@@ -285,21 +347,26 @@ __global__ void __launch_bounds__(MEV) k_mesh_events(DevState S, const int *__re
                                           else atomicOr(err, ERR_CAPACITY);
                                     } else {
                                           cflag[r] |= F_DROP;  // removed before kk's query: never pushed
-                                          atomicAdd(ndrop, 1);
                                     }
                               }
                         }
                   }
                   // a removed body does not query its own cells either
                   if (!alive && x > kq)
-                        for (int r = off[x] + threadIdx.x; r < off[x + 1]; r += MEV) {
-                              cflag[r] |= F_DROP;
-                              atomicAdd(ndrop, 1);
-                        }
+                        for (int r = off[x] + threadIdx.x; r < off[x + 1]; r += MEV) cflag[r] |= F_DROP;
             }
             cur = q;
             __syncthreads();
       }
+}
+
+// Number of dropped candidates (a candidate can be dropped by two removals).
+__global__ void k_count_dropped(const unsigned char *__restrict__ cflag, int n, int *__restrict__ ndrop)
+{
+      int q = blockIdx.x * blockDim.x + threadIdx.x;
+      int d = q < n && (cflag[q] & F_DROP) ? 1 : 0;
+      d = __syncthreads_count(d);
+      if (threadIdx.x == 0 && d) atomicAdd(ndrop, d);
 }
 
 // pairs[] = candidates without dropped / merged entries, swapped ones as (p, k)
@@ -309,18 +376,49 @@ __global__ void k_pairs_keep(const unsigned char *__restrict__ cflag, int n, int
       if (q < n) keep[q] = (cflag[q] & (F_DROP | F_MERGED)) ? 0 : 1;
 }
 
+// Extra (fragment) pairs recorded before candidate position q: the offset of
+// the first event at or after q (offsets are cumulative in event order).
+__device__ __forceinline__ int x_before(const int *__restrict__ evx, int nev, int nx, int q)
+{
+      int lo = 0, hi = nev;  // first event with position >= q
+      while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (evx[EVX * mid] < q) lo = mid + 1;
+            else hi = mid;
+      }
+      return lo < nev ? evx[EVX * lo + 1] : nx;
+}
+
 __global__ void k_pairs_emit(const int *__restrict__ ck, const int *__restrict__ cp,
                              const unsigned char *__restrict__ cflag, const int *__restrict__ pos, int n,
-                             int *__restrict__ out)
+                             const int *__restrict__ evx, int nev, int nx, int *__restrict__ out)
 {
       int q = blockIdx.x * blockDim.x + threadIdx.x;
       if (q >= n) return;
       unsigned char f = cflag[q];
       if (f & (F_DROP | F_MERGED)) return;
-      int o = pos[q];
+      int o = pos[q] + (nx > 0 ? x_before(evx, nev, nx, q) : 0);
       bool sw = f & F_SWAP;
       out[2 * o] = sw ? cp[q] : ck[q];
       out[2 * o + 1] = sw ? ck[q] : cp[q];
+}
+
+// The tail pairs of full fragmentations, spliced in at their events'
+// positions: extra pair x of event e goes to pos[q_e] + x.
+__global__ void k_pairs_extra(const int *__restrict__ xpairs, int nx, const int *__restrict__ evx, int nev,
+                              const int *__restrict__ pos, int *__restrict__ out)
+{
+      int x = blockIdx.x * blockDim.x + threadIdx.x;
+      if (x >= nx) return;
+      int lo = 0, hi = nev - 1;  // last event with offset <= x
+      while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (evx[EVX * mid + 1] <= x) lo = mid;
+            else hi = mid - 1;
+      }
+      const int o = pos[evx[EVX * lo]] + x;
+      out[2 * o] = xpairs[2 * x];
+      out[2 * o + 1] = xpairs[2 * x + 1];
 }
 
 }  // namespace
@@ -355,6 +453,12 @@ static int mesh_alloc(int d)
             NCG_CK(cudaMalloc(&c.msums, sizeof(int) * (c.pair_cap / 1024 + 2)));
             c.occ_cap = 64 * c.n_max + 4096;
             NCG_CK(cudaMalloc(&c.occ, sizeof(int) * (size_t)c.occ_cap));
+            NCG_CK(cudaMalloc(&c.evx, sizeof(int) * EVX * (size_t)c.ev_cap));
+            c.xpair_cap = 4L * c.n_max + 4096;
+            NCG_CK(cudaMalloc(&c.xpairs, sizeof(int) * 2 * (size_t)c.xpair_cap));
+            NCG_CK(cudaMalloc(&c.xhead, sizeof(int) * N));
+            NCG_CK(cudaMemsetAsync(c.xhead, 0xff, sizeof(int) * N, c.s));
+            NCG_CK(cudaMalloc(&c.fev, sizeof(int) * (size_t)c.ev_cap));
       }
       return NCGPU_OK;
 }
@@ -363,9 +467,15 @@ void mesh_free()
 {
       Ctx &c = ctx();
       void *ptrs[] = {c.cstart, c.mkeys, c.mvals, c.ckey, c.mcnt, c.moff, c.cand_k, c.cand_p, c.cflag, c.cpos,
-                      c.occ, c.msums};
+                      c.occ, c.msums, c.evx, c.xpairs, c.xhead, c.fev};
       for (void *p : ptrs)
             if (p) cudaFree(p);
+}
+
+__global__ void k_clear_xhead(const int *__restrict__ evx, int nev, int *__restrict__ xhead)
+{
+      int e = blockIdx.x * blockDim.x + threadIdx.x;
+      if (e < nev) xhead[evx[EVX * e + 4]] = -1;
 }
 
 int mesh_reset_state()
@@ -375,7 +485,12 @@ int mesh_reset_state()
             k_cell_clear<<<(c.mesh_n + 255) / 256, 256, 0, c.s>>>(c.mkeys, c.mesh_n, c.cstart);
             NCG_LAUNCHED();
       }
+      if (c.mesh_nfev > 0) {
+            k_clear_xhead<<<(c.mesh_nev + 255) / 256, 256, 0, c.s>>>(c.evx, c.mesh_nev, c.xhead);
+            NCG_LAUNCHED();
+      }
       c.mesh_valid = 0;
+      c.mesh_nev = c.mesh_nfev = c.mesh_nx = 0;
       return NCGPU_OK;
 }
 
@@ -402,6 +517,7 @@ int mesh_pass(double gam, int test)
       int zero[S_COUNT] = {0};
       NCG_CK(cudaMemcpyAsync(c.scal + S_NHITS, zero, 2 * sizeof(int), cudaMemcpyHostToDevice, st));  // NHITS, NEV
       NCG_CK(cudaMemcpyAsync(c.scal + S_NBIG, zero, 3 * sizeof(int), cudaMemcpyHostToDevice, st));   // NBIG, NDROP, NINS
+      NCG_CK(cudaMemcpyAsync(c.scal + S_NXPAIRS, zero, 3 * sizeof(int), cudaMemcpyHostToDevice, st));  // NXPAIRS, NSKIP, NFEV
       c.n_cand = c.n_pairs = 0;
       c.total_neighbours = 0;
       c.how_many_small = c.how_many_big = 0;
@@ -441,11 +557,15 @@ int mesh_pass(double gam, int test)
             NCG_CK(cudaMemsetAsync(c.vals, 0, sizeof(int) * (size_t)nh, st));
             NCG_TRY(radix_sort_pairs(c.keys, c.vals, nh, 31, st));
             MeshEvArgs E{lid, d, c.P.par_collision_type, c.P.par_one_collision_only_bool, c.P.par_mesh_bool, c.ev_cap, c.n_max,
-                         c.occ_cap, n, (long long)c.cell_cap, c.dt, c.P.par_collision_parameter};
-            if (E.type == NCGPU_COLLISION_FRAGMENTATION) return NCGPU_E_UNSUPPORTED;
+                         c.occ_cap, n, (long long)c.cell_cap, c.dt, c.P.par_collision_parameter,
+                         c.P.par_mutual_bool, c.xpair_cap, FragArgs{}};
+            if (E.type == NCGPU_COLLISION_FRAGMENTATION && !make_frag_args(c, E.frag)) return NCGPU_E_ARG;
+            MeshFragBufs X{c.evx, c.xpairs, c.xhead, c.fev};
             k_mesh_events<<<1, MEV, 0, st>>>(S, c.cand_k, c.cand_p, c.cflag, c.moff, c.ckey, c.mkeys, c.mvals,
                                              c.cstart, (const int *)c.keys, nh, E, c.ev, c.evrec, c.dirty, c.occ,
-                                             c.scal + S_NDROP, c.err);
+                                             c.scal + S_NDROP, X, c.err);
+            NCG_LAUNCHED();
+            k_count_dropped<<<(total + 255) / 256, 256, 0, st>>>(c.cflag, total, c.scal + S_NDROP);
             NCG_LAUNCHED();
       }
       NCG_TRY(sync_scalars());
@@ -455,9 +575,11 @@ int mesh_pass(double gam, int test)
             k_clear_dirty_events<<<(c.n_events + 255) / 256, 256, 0, st>>>(c.dirty, c.ev, min(c.n_events, c.ev_cap));
             NCG_LAUNCHED();
       }
-      const int merged = c.P.par_collision_type == NCGPU_COLLISION_MERGER ? c.n_events : 0;
+      c.mesh_nev = min(c.n_events, c.ev_cap);
+      c.mesh_nfev = h[S_NFEV];
+      c.mesh_nx = h[S_NXPAIRS];
       c.total_neighbours = (long)total - h[S_NDROP];
-      c.n_pairs = c.P.par_mutual_bool ? total - h[S_NDROP] - merged : 0;
+      c.n_pairs = c.P.par_mutual_bool ? total - h[S_NDROP] - h[S_NSKIP] + h[S_NXPAIRS] : 0;
       c.how_many_big = h[S_NBIG];
       return NCGPU_OK;
 }
@@ -495,8 +617,12 @@ extern "C" int ncgpu_get_pairs(struct ncgpu_pair *out, int cap, int *n)
       NCG_TRY(scan_exclusive(c.cpos, c.cpos, nc, c.msums, st));  // in place
       int *dst = nullptr;
       NCG_CK(cudaMalloc(&dst, sizeof(int) * 2 * (size_t)c.n_pairs));
-      k_pairs_emit<<<nb, 256, 0, st>>>(c.cand_k, c.cand_p, c.cflag, c.cpos, nc, dst);
+      k_pairs_emit<<<nb, 256, 0, st>>>(c.cand_k, c.cand_p, c.cflag, c.cpos, nc, c.evx, c.mesh_nev, c.mesh_nx, dst);
       NCG_LAUNCHED();
+      if (c.mesh_nx > 0) {
+            k_pairs_extra<<<(c.mesh_nx + 255) / 256, 256, 0, st>>>(c.xpairs, c.mesh_nx, c.evx, c.mesh_nev, c.cpos, dst);
+            NCG_LAUNCHED();
+      }
       const int k = c.n_pairs < cap ? c.n_pairs : cap;
       cudaError_t e = cudaMemcpyAsync(out, dst, sizeof(int) * 2 * (size_t)k, cudaMemcpyDeviceToHost, st);
       if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -223,7 +223,26 @@ struct MGArgs {
       int lid, d, central, mutual, soft;
       long long cell_cap;
       double G, sp, mu, cmx, cmy, cmz;
+      int lid0;                 // largest_id of the mesh pass (slots in the cell table)
+      int nt;                   // N_tilde
+      int nfev;                 // full fragmentations of the pass
+      const int *evx, *fev, *xhead;
 };
+
+// The tail fragments of full fragmentation e (EVX record): slots
+// fid0 .. fid0 + nt - 1.  Adds, in pairs[] order, the terms of the largest
+// fragment A and of the tail (except `self`) to body b.
+__device__ __forceinline__ void tail_terms(const DevState &S, const MGArgs &A, int e, int self, int b,
+                                           double &ax, double &ay, double &az)
+{
+      const int *r = A.evx + (size_t)EVX * e;
+      const int fid0 = r[3], big = r[4];
+      if (big != self && big > 2 && S.ex[big]) pair_add(S, b, big, A.G, A.sp, A.soft, ax, ay, az);
+      for (int n = 0; n < A.nt; n++) {
+            const int f = fid0 + n;
+            if (f != self && f > 2 && S.ex[f]) pair_add(S, b, f, A.G, A.sp, A.soft, ax, ay, az);
+      }
+}
 
 // Accelerations of bodies 3..lid (bodies 0..2 are finished by k_mesh_big3);
 // terms for bodies 0..2 and CM_acc go to `terms` (12 blocks of n_max).
@@ -262,8 +281,26 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                   terms[(3 * i + 2) * N + b] = t[2];
             }
       }
-      const int L = have_cells ? ckey[b] : -1;
+      if (A.mutual && have_cells && b > A.lid0) {
+            // a tail fragment created by the pass: its pairs are those of its
+            // fragmentation (the largest fragment, then the other tail bodies)
+            int lo = 0, hi = A.nfev - 1;  // last full fragmentation with fid0 <= b
+            while (lo < hi) {
+                  int mid = (lo + hi + 1) >> 1;
+                  if (A.evx[(size_t)EVX * A.fev[mid] + 3] <= b) lo = mid;
+                  else hi = mid - 1;
+            }
+            if (A.nfev > 0) {
+                  const int e = A.fev[lo];
+                  const int fid0 = A.evx[(size_t)EVX * e + 3];
+                  if (b >= fid0 && b < fid0 + A.nt) tail_terms(S, A, e, b, b, a_x, a_y, a_z);
+            }
+      }
+      const int L = (have_cells && b <= A.lid0) ? ckey[b] : -1;
       if (A.mutual && L >= 0) {
+            // full fragmentations whose largest fragment is b: their tail pairs
+            // follow the event's own candidate in b's sequence
+            int xe = A.xhead ? A.xhead[b] : -1;
             // own pops: cells 26..0, lower indices ascending
             int cur[27];
             for (int l = 26; l >= 0; --l) {
@@ -277,6 +314,10 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                         int p = vals[q];
                         if (p >= b) break;
                         if (p > 2 && S.ex[p]) pair_add(S, b, p, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                        while (xe >= 0 && A.evx[(size_t)EVX * xe + 6] == b && A.evx[(size_t)EVX * xe + 7] == p) {
+                              tail_terms(S, A, xe, b, b, a_x, a_y, a_z);
+                              xe = A.evx[(size_t)EVX * xe + 5];
+                        }
                   }
                   cur[l] = (keys[q] == (uint32_t)cell) ? q : -1;  // first higher index, if any
             }
@@ -291,10 +332,15 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                   }
                   if (bl < 0) break;
                   if (best > 2 && best != b && S.ex[best]) pair_add(S, b, best, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                  while (xe >= 0 && A.evx[(size_t)EVX * xe + 6] == best && A.evx[(size_t)EVX * xe + 7] == b) {
+                        tail_terms(S, A, xe, b, b, a_x, a_y, a_z);
+                        xe = A.evx[(size_t)EVX * xe + 5];
+                  }
                   long long cell = L + g_noff(bl, A.d);
                   int q = cur[bl] + 1;
                   cur[bl] = (keys[q] == (uint32_t)cell) ? q : -1;
             }
+            for (; xe >= 0; xe = A.evx[(size_t)EVX * xe + 5]) tail_terms(S, A, xe, b, b, a_x, a_y, a_z);
       }
       ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
 }
@@ -462,7 +508,10 @@ int mesh_gravity_state(const double *cm8)
       NCG_TRY(ensure_partial((size_t)12 * N));
       DevState S = dev_state();
       MGArgs A{lid, c.P.par_collision_cube_cells, c.P.par_central_mass_bool, c.P.par_mutual_bool,
-               c.P.par_softening_parameter != 0., (long long)c.cell_cap, c.P.par_G, c.P.par_softening_parameter, c.P.par_G * cm8[6], cm8[0], cm8[1], cm8[2]};
+               c.P.par_softening_parameter != 0., (long long)c.cell_cap, c.P.par_G, c.P.par_softening_parameter,
+               c.P.par_G * cm8[6], cm8[0], cm8[1], cm8[2],
+               c.mesh_valid ? c.mesh_n - 1 : -1, c.P.par_N_tilde, c.mesh_nfev, c.evx, c.fev,
+               c.mesh_nfev > 0 ? c.xhead : nullptr};
       double *ax = c.acc, *ay = c.acc + N, *az = c.acc + 2 * N;
       if (lid >= 0) {
             k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.cstart, c.mesh_valid, ax,

@@ -7,7 +7,10 @@
 //   collision (impulse)   src/physics.c:545-625
 //   merger                src/physics.c:628-708
 //   collision_treatment   src/physics.c:1043-1091
+//   fragmentation         src/physics.c:710-1040
 //   lose_moonlet          src/structure.c:1077-1087
+//   get_free_index        src/structure.c:849-878
+//   cross_product         src/structure.c:1066-1074
 #pragma once
 #include "common.cuh"
 
@@ -152,6 +155,321 @@ __device__ __forceinline__ void d_merge(const DevState &S, int a, int b, const A
             double xa = ap.p[0], ya = ap.p[1], za = ap.p[2], xb = ap.p[3], yb = ap.p[4], zb = ap.p[5];
             rec[6] = DADD(DADD(DMUL(DSUB(xa, xb), dvx), DMUL(DSUB(ya, yb), dvy)), DMUL(DSUB(za, zb), dvz));
       }
+}
+
+// get_free_index(at_end): a freed slot (the top of the free stack) or a new
+// slot past largest_id; -1 (with ERR_NMAX) when that would reach N_max.
+__device__ __forceinline__ int d_free_index(const DevState &S, int at_end, int n_max, unsigned *err)
+{
+      int idx;
+      int nf = S.scal[S_NFREE];
+      if (nf == 0 || at_end) {
+            idx = S.scal[S_LID] + 1;
+            if (idx >= n_max) {
+                  atomicOr(err, ERR_NMAX);
+                  return -1;
+            }
+            S.scal[S_LID] = idx;
+      } else {
+            nf -= 1;
+            S.scal[S_NFREE] = nf;
+            idx = S.free_idx[nf];
+            if (idx > S.scal[S_LID]) S.scal[S_LID] = idx;
+      }
+      if (S.ex[idx]) {  // the reference aborts: "This index is not free"
+            atomicOr(err, ERR_INTERNAL);
+            return -1;
+      }
+      S.ex[idx] = 1;
+      return idx;
+}
+
+// Constants of the fragmentation model and the driver switches it reads.
+struct FragArgs {
+      int N_tilde;
+      int pq[4];
+      double mu, nu, C1, k, merging_threshold, fragment_threshold, G;
+      int central_mass_bool;
+      int at_end;       // mesh_bool && !force_naive_bool: fragments go past largest_id
+      int mesh_bool;    // lose_moonlet's rule for slots 0-2
+      int one_only;     // one_collision_only_bool
+      int n_max;
+      double *cm;       // device central body (x, y, z, vx, vy, vz, mass, radius)
+};
+
+// Outcome of one fragmentation: 0 merger, 1 super-catastrophic, 2 partial
+// (ids = a, b: the pair (a, b) enters pairs[] in mesh mode), 3 full (ids =
+// id[0..N_tilde]: a, then the tail fragments in creation order).
+struct FragOut {
+      int outcome;
+      int nids;
+      int ids[NCGPU_MAX_N_TILDE + 1];
+};
+
+__device__ __forceinline__ void d_cross(double u1, double u2, double u3, double v1, double v2, double v3, double *w)
+{
+      w[0] = DSUB(DMUL(u2, v3), DMUL(u3, v2));
+      w[1] = DSUB(DMUL(u3, v1), DMUL(u1, v3));
+      w[2] = DSUB(DMUL(u1, v2), DMUL(u2, v1));
+}
+
+// One tail fragment's offsets (r_k, v_k) relative to the largest fragment, at
+// lattice point (p, q) with running index n (the body of the reference's
+// (p, q) loop).  Returns false when its speed is below the escape velocity.
+__device__ __forceinline__ bool d_tail(int n, int p, int q, const double *dr, const double *u, const double *v,
+                                       double R_tilde_2, double R_tilde12, double m_tilde_2, double K,
+                                       double m_check, double stigma, double vesc, double *rk, double *vk)
+{
+      const double tp = DMUL((double)(2 * p), R_tilde_2), tq = DMUL((double)(2 * q), R_tilde_2);
+      for (int d = 0; d < 3; d++) rk[d] = DADD(DADD(dr[d], DMUL(tp, u[d])), DMUL(tq, v[d]));
+      const double Km = DADD(K, m_check);
+      const double zk = pow(DSUB(1.0, DDIV(DMUL((double)n, m_tilde_2), Km)), stigma);
+      const double zk1 = pow(DSUB(1.0, DDIV(DMUL(DADD((double)n, 1.), m_tilde_2), Km)), stigma);
+      const double vks = DMUL(DDIV(DMUL(DDIV(vesc, stigma), DADD(m_check, K)), m_tilde_2), DSUB(zk, zk1));
+      const double pp = (double)p, qq = (double)q;
+      const double iff = DDIV(vks, __dsqrt_rn(DADD(DADD(1.0, DMUL(pp, pp)), DMUL(qq, qq))));
+      for (int d = 0; d < 3; d++)
+            vk[d] = DMUL(iff, DADD(DADD(DDIV(dr[d], R_tilde12), DMUL(pp, u[d])), DMUL(qq, v[d])));
+      return !(vks < vesc);
+}
+
+// fragmentation(a, b): a is the heavier body (the target), b the impactor.
+// General powers use CUDA's pow (the reference uses libm's); the cube roots
+// use pow_one_third.  rec (if given) receives DeltaV, dr.dv and m_tilde.
+__device__ inline void d_fragment(const DevState &S, int a, int b, const Approach &ap, const FragArgs &F, double *rec,
+                           FragOut &out, unsigned *err)
+{
+      const double FOUR_PI = 4. * 3.14159265358979323846;
+      const double stigma = DDIV(DSUB(DMUL(3., F.mu), 1.), DMUL(3., F.mu));
+      const double R_2 = S.R[a], R_1 = S.R[b], R = DADD(R_1, R_2);
+      const double m_2 = S.m[a], m_1 = S.m[b], M = DADD(m_1, m_2);
+      const double rho_1 = DDIV(DMUL(3., m_1), DMUL(DMUL(DMUL(FOUR_PI, R_1), R_1), R_1));
+      const double rho_2 = DDIV(DMUL(3., m_2), DMUL(DMUL(DMUL(FOUR_PI, R_2), R_2), R_2));
+      const double avg = DDIV(DADD(DMUL(m_1, rho_1), DMUL(m_2, rho_2)), M);
+      const double rho_12 = DDIV(rho_1, rho_2);
+      const double rho_12_3nu = pow(rho_12, DMUL(3., F.nu));
+      const double vx_a = S.vx[a], vy_a = S.vy[a], vz_a = S.vz[a];
+      const double vx_b = S.vx[b], vy_b = S.vy[b], vz_b = S.vz[b];
+      const double xa = ap.p[0], ya = ap.p[1], za = ap.p[2], xb = ap.p[3], yb = ap.p[4], zb = ap.p[5];
+      const double dx = DSUB(xa, xb), dy = DSUB(ya, yb), dz = DSUB(za, zb);
+      const double dvx = DSUB(vx_a, vx_b), dvy = DSUB(vy_a, vy_b), dvz = DSUB(vz_a, vz_b);
+      const double dr_dot_dv = DADD(DADD(DMUL(dx, dvx), DMUL(dy, dvy)), DMUL(dz, dvz));
+      const double dv_norm = __dsqrt_rn(DADD(DADD(DMUL(dvx, dvx), DMUL(dvy, dvy)), DMUL(dvz, dvz)));
+      const double costheta = DDIV(-dr_dot_dv, DMUL(R, dv_norm));
+      const double costheta3mu = pow(costheta, DMUL(3., F.mu));
+      const double R_eq = pow_one_third(DDIV(DMUL(3., M), DMUL(FOUR_PI, avg)));
+      const double vesc = __dsqrt_rn(DDIV(DMUL(DMUL(2., F.G), M), R_eq));
+      const double K = DMUL(DDIV(DDIV(DMUL(DMUL(3., F.k), m_1), FOUR_PI), rho_12), costheta3mu);
+      const double m_check =
+          DMUL(K, DSUB(DMUL(pow(DDIV(DMUL(F.C1, dv_norm), vesc), DMUL(3., F.mu)), rho_12_3nu), 1.));
+      double m_tilde = DSUB(M, m_check);
+      const double m_tilde_2 = DDIV(m_check, (double)F.N_tilde);
+      const double t = ap.t;
+      double v_cm[3], r_cm[3];
+      v_cm[0] = DDIV(DADD(DMUL(m_2, vx_a), DMUL(m_1, vx_b)), M);
+      v_cm[1] = DDIV(DADD(DMUL(m_2, vy_a), DMUL(m_1, vy_b)), M);
+      v_cm[2] = DDIV(DADD(DMUL(m_2, vz_a), DMUL(m_1, vz_b)), M);
+      r_cm[0] = DDIV(DADD(DMUL(m_2, xa), DMUL(m_1, xb)), M);
+      r_cm[1] = DDIV(DADD(DMUL(m_2, ya), DMUL(m_1, yb)), M);
+      r_cm[2] = DDIV(DADD(DMUL(m_2, za), DMUL(m_1, zb)), M);
+      if (rec) {
+            rec[5] = dv_norm;
+            rec[6] = dr_dot_dv;
+            rec[7] = m_tilde;
+      }
+      out.nids = 0;
+
+      if (m_check <= DMUL(F.merging_threshold, M)) {  // merger
+            d_merge(S, a, b, ap, F.one_only, F.mesh_bool, nullptr);
+            S.scal[S_FMERGE] += 1;
+            out.outcome = 0;
+            return;
+      }
+      if (m_tilde < DMUL(0.1, M)) {  // super-catastrophic: only the largest fragment stays
+            m_tilde = DMUL(DMUL(0.1, M), pow(DDIV(DMUL(DDIV(1.0, 0.9), m_check), M), -1.5));
+            S.vx[a] = v_cm[0]; S.vy[a] = v_cm[1]; S.vz[a] = v_cm[2];
+            S.x[a] = DSUB(r_cm[0], DMUL(t, v_cm[0]));
+            S.y[a] = DSUB(r_cm[1], DMUL(t, v_cm[1]));
+            S.z[a] = DSUB(r_cm[2], DMUL(t, v_cm[2]));
+            S.m[a] = m_tilde;
+            S.R[a] = pow_one_third(DDIV(DMUL(3., m_tilde), DMUL(FOUR_PI, avg)));
+            S.scal[S_NEEDCOM] = 1;
+            d_lose(S, b, F.mesh_bool);
+            S.did[a] = F.one_only;
+            S.scal[S_FSUPER] += 1;
+            double discarded = DSUB(M, m_tilde);
+            if (m_tilde < DDIV(F.fragment_threshold, 4.)) {
+                  d_lose(S, a, F.mesh_bool);
+                  discarded = M;
+            }
+            if (F.central_mass_bool) F.cm[6] = DADD(F.cm[6], discarded);
+            if (rec) rec[7] = m_tilde;
+            out.outcome = 1;
+            return;
+      }
+      if (m_tilde_2 < F.fragment_threshold && m_check <= m_tilde) {  // partial: the tail is one body
+            const double vks = DMUL(DDIV(DMUL(DDIV(vesc, stigma), DADD(m_check, K)), m_check),
+                                    DSUB(1.0, pow(DDIV(K, DADD(K, m_check)), stigma)));
+            if (vks < vesc) {
+                  atomicOr(err, ERR_FRAGMENT);
+                  out.outcome = -1;
+                  return;
+            }
+            const double in_front_of = DDIV(vks, R);
+            double rk[3] = {-dx, -dy, -dz};
+            double vk[3];
+            for (int d = 0; d < 3; d++) vk[d] = DMUL(in_front_of, rk[d]);
+            const double R_tilde = pow_one_third(DDIV(DMUL(3.0, m_tilde), DMUL(FOUR_PI, avg)));
+            const double R_check = pow_one_third(DDIV(DMUL(3.0, m_check), DMUL(FOUR_PI, avg)));
+            const double R_tilde12 = DADD(R_tilde, R_check);
+            const double dr_norm = __dsqrt_rn(DADD(DADD(DMUL(rk[0], rk[0]), DMUL(rk[1], rk[1])), DMUL(rk[2], rk[2])));
+            const double sc = DDIV(R_tilde12, dr_norm);
+            for (int d = 0; d < 3; d++) rk[d] = DMUL(rk[d], sc);
+            const double f = DDIV(m_check, M);
+            double rt[3], vt[3];
+            for (int d = 0; d < 3; d++) {
+                  rt[d] = DSUB(r_cm[d], DMUL(f, rk[d]));
+                  vt[d] = DSUB(v_cm[d], DMUL(f, vk[d]));
+            }
+            S.x[a] = DSUB(rt[0], DMUL(t, vt[0]));
+            S.y[a] = DSUB(rt[1], DMUL(t, vt[1]));
+            S.z[a] = DSUB(rt[2], DMUL(t, vt[2]));
+            S.vx[a] = vt[0]; S.vy[a] = vt[1]; S.vz[a] = vt[2];
+            S.m[a] = m_tilde;
+            S.R[a] = R_tilde;
+            S.x[b] = DSUB(DADD(rt[0], rk[0]), DMUL(t, DADD(vt[0], vk[0])));
+            S.y[b] = DSUB(DADD(rt[1], rk[1]), DMUL(t, DADD(vt[1], vk[1])));
+            S.z[b] = DSUB(DADD(rt[2], rk[2]), DMUL(t, DADD(vt[2], vk[2])));
+            S.vx[b] = DADD(vt[0], vk[0]); S.vy[b] = DADD(vt[1], vk[1]); S.vz[b] = DADD(vt[2], vk[2]);
+            S.m[b] = m_check;
+            S.R[b] = R_check;
+            S.did[a] = F.one_only;
+            S.did[b] = F.one_only;
+            S.scal[S_FHALF] += 1;
+            out.outcome = 2;
+            out.nids = 2;
+            out.ids[0] = a;
+            out.ids[1] = b;
+            return;
+      }
+      // full fragmentation: N_tilde tail fragments on the (p, q) lattice
+      const double R_tilde = pow_one_third(DDIV(DMUL(3.0, m_tilde), DMUL(FOUR_PI, avg)));
+      const double R_tilde_2 = pow_one_third(DDIV(DMUL(3.0, m_tilde_2), DMUL(FOUR_PI, avg)));
+      const double R_tilde12 = DADD(R_tilde, R_tilde_2);
+      double dr[3] = {-dx, -dy, -dz};
+      const double dv[3] = {-dvx, -dvy, -dvz};
+      const double dr_norm = __dsqrt_rn(DADD(DADD(DMUL(dr[0], dr[0]), DMUL(dr[1], dr[1])), DMUL(dr[2], dr[2])));
+      const double sc = DDIV(R_tilde12, dr_norm);
+      for (int d = 0; d < 3; d++) dr[d] = DMUL(dr[d], sc);
+      double dxv[3], u[3], v[3];
+      d_cross(dr[0], dr[1], dr[2], dv[0], dv[1], dv[2], dxv);
+      const double dxv_norm =
+          __dsqrt_rn(DADD(DADD(DMUL(dxv[0], dxv[0]), DMUL(dxv[1], dxv[1])), DMUL(dxv[2], dxv[2])));
+      if (dxv_norm > 1.0e-5) {  // oblique impact
+            for (int d = 0; d < 3; d++) v[d] = DDIV(dxv[d], dxv_norm);
+      } else {  // nearly frontal: any unit vector orthogonal to dr (maximum(), src/structure.c:1090)
+            const double f0 = fabs(dr[0]), f1 = fabs(dr[1]), f2 = fabs(dr[2]);
+            int mm = f0 >= f1 ? 0 : 1;
+            const double mx = f0 >= f1 ? f0 : f1;
+            if (!(mx >= f2)) mm = 2;
+            const int i0 = mm, i1 = mm == 0 ? 1 : 0, i2 = mm == 2 ? 1 : 2;
+            const double num = DADD(dr[i1], dr[i2]);
+            const double w = DDIV(1.0, __dsqrt_rn(DADD(2.0, DDIV(DMUL(num, num), DMUL(dr[i0], dr[i0])))));
+            v[i1] = w;
+            v[i2] = w;
+            v[i0] = DDIV(DMUL(-w, num), dr[i0]);
+      }
+      double vxd[3];
+      d_cross(v[0], v[1], v[2], dr[0], dr[1], dr[2], vxd);
+      for (int d = 0; d < 3; d++) u[d] = DDIV(vxd[d], R_tilde12);
+      // momentum correction: sums of the tail offsets in lattice order
+      double corr[6] = {0., 0., 0., 0., 0., 0.};
+      {
+            int n = 0;
+            bool ok = true;
+            for (int p = F.pq[0]; p <= F.pq[1]; p++)
+                  for (int q = F.pq[2]; q <= F.pq[3]; q++) {
+                        double rk[3], vk[3];
+                        ok &= d_tail(n, p, q, dr, u, v, R_tilde_2, R_tilde12, m_tilde_2, K, m_check, stigma, vesc,
+                                     rk, vk);
+                        for (int d = 0; d < 3; d++) {
+                              corr[d] = DADD(corr[d], rk[d]);
+                              corr[3 + d] = DADD(corr[3 + d], vk[d]);
+                        }
+                        n++;
+                  }
+            if (!ok) {
+                  atomicOr(err, ERR_FRAGMENT);
+                  out.outcome = -1;
+                  return;
+            }
+      }
+      const double f = DDIV(m_tilde_2, M);
+      double rt[3], vt[3];
+      for (int d = 0; d < 3; d++) {
+            rt[d] = DSUB(r_cm[d], DMUL(f, corr[d]));
+            vt[d] = DSUB(v_cm[d], DMUL(f, corr[3 + d]));
+      }
+      out.ids[0] = a;
+      for (int n = 1; n <= F.N_tilde; n++) {
+            const int id = d_free_index(S, F.at_end, F.n_max, err);
+            if (id < 0) {
+                  out.outcome = -1;
+                  return;
+            }
+            out.ids[n] = id;
+      }
+      out.nids = F.N_tilde + 1;
+      d_lose(S, b, F.mesh_bool);
+      for (int n = 0; n <= F.N_tilde; n++) S.did[out.ids[n]] = F.one_only;
+      S.x[a] = DSUB(rt[0], DMUL(t, vt[0]));
+      S.y[a] = DSUB(rt[1], DMUL(t, vt[1]));
+      S.z[a] = DSUB(rt[2], DMUL(t, vt[2]));
+      S.vx[a] = vt[0]; S.vy[a] = vt[1]; S.vz[a] = vt[2];
+      S.m[a] = m_tilde;
+      S.R[a] = R_tilde;
+      int n = 0;
+      for (int p = F.pq[0]; p <= F.pq[1]; p++)
+            for (int q = F.pq[2]; q <= F.pq[3]; q++) {
+                  double rk[3], vk[3];
+                  d_tail(n, p, q, dr, u, v, R_tilde_2, R_tilde12, m_tilde_2, K, m_check, stigma, vesc, rk, vk);
+                  const int id = out.ids[n + 1];
+                  S.x[id] = DSUB(DADD(rt[0], rk[0]), DMUL(t, DADD(vt[0], vk[0])));
+                  S.y[id] = DSUB(DADD(rt[1], rk[1]), DMUL(t, DADD(vt[1], vk[1])));
+                  S.z[id] = DSUB(DADD(rt[2], rk[2]), DMUL(t, DADD(vt[2], vk[2])));
+                  S.vx[id] = DADD(vt[0], vk[0]);
+                  S.vy[id] = DADD(vt[1], vk[1]);
+                  S.vz[id] = DADD(vt[2], vk[2]);
+                  S.m[id] = m_tilde_2;
+                  S.R[id] = R_tilde_2;
+                  n++;
+            }
+      S.scal[S_FFULL] += 1;
+      out.outcome = 3;
+}
+
+// FragArgs from the library parameters; false when N_tilde and the lattice
+// do not agree (N_tilde = (p_max - p_min + 1)(q_max - q_min + 1), src/parameters.h:307-309).
+inline bool make_frag_args(const Ctx &c, FragArgs &F)
+{
+      const ncgpu_params &P = c.P;
+      F.N_tilde = P.par_N_tilde;
+      for (int j = 0; j < 4; j++) F.pq[j] = P.par_pq_min_max[j];
+      F.mu = P.par_mu_parameter;
+      F.nu = P.par_nu_parameter;
+      F.C1 = P.par_C1_parameter;
+      F.k = P.par_k_parameter;
+      F.merging_threshold = P.par_merging_threshold;
+      F.fragment_threshold = P.par_fragment_threshold;
+      F.G = P.par_G;
+      F.central_mass_bool = P.par_central_mass_bool;
+      F.at_end = P.par_mesh_bool && !c.force_naive;
+      F.mesh_bool = P.par_mesh_bool;
+      F.one_only = P.par_one_collision_only_bool;
+      F.n_max = c.n_max;
+      F.cm = c.cm;
+      const long np = (long)F.pq[1] - F.pq[0] + 1, nq = (long)F.pq[3] - F.pq[2] + 1;
+      return F.N_tilde >= 1 && F.N_tilde <= NCGPU_MAX_N_TILDE && np > 0 && nq > 0 && np * nq == F.N_tilde;
 }
 
 }  // namespace ncg

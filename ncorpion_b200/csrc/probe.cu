@@ -1,6 +1,7 @@
-// Diagnostic FP32 throughput probe: independent FFMA chains, enough warps per
-// SM to saturate the FP32 pipe.  Its measured rate is the denominator used
-// for the FP32 gravity kernel's roofline fraction.
+// Diagnostic FP32 throughput probes: independent FFMA chains (scalar and the
+// sm_100a packed f32x2 form) and independent rsqrt.approx chains, with enough
+// warps per SM to saturate each pipe.  The measured rates are the denominators
+// of the FP32 gravity kernel's roofline fractions.
 #include "common.cuh"
 
 namespace ncg {
@@ -21,10 +22,103 @@ __global__ void __launch_bounds__(256) k_ffma_probe(float *out, float a, float b
       if (s == 123.456f) out[0] = s;  // keeps the chains live
 }
 
+__global__ void __launch_bounds__(256) k_ffma2_probe(float *out, float a, float b)
+{
+      unsigned long long A, B, r[8];
+      asm("mov.b64 %0, {%1, %1};" : "=l"(A) : "f"(a));
+      asm("mov.b64 %0, {%1, %1};" : "=l"(B) : "f"(b));
+      for (int k = 0; k < 8; k++) {
+            const float lo = threadIdx.x * 1e-7f + k, hi = lo + 0.5f;
+            asm("mov.b64 %0, {%1, %2};" : "=l"(r[k]) : "f"(lo), "f"(hi));
+      }
+#pragma unroll 4
+      for (int i = 0; i < PROBE_ITERS; i++) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) asm volatile("fma.rn.f32x2 %0, %0, %1, %2;" : "+l"(r[k]) : "l"(A), "l"(B));
+      }
+      float s = 0.f;
+      for (int k = 0; k < 8; k++) {
+            float lo, hi;
+            asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(r[k]));
+            s += lo + hi;
+      }
+      if (s == 123.456f) out[0] = s;
+}
+
+__global__ void __launch_bounds__(256) k_rsqrt_probe(float *out, float b)
+{
+      float r[8];
+      for (int k = 0; k < 8; k++) r[k] = 1.f + threadIdx.x * 1e-7f + k;
+#pragma unroll 4
+      for (int i = 0; i < PROBE_ITERS; i++) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                  float y;
+                  asm volatile("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(r[k]));
+                  r[k] = y + b;  // stays near 1: alternates around the fixed point
+            }
+      }
+      float s = 0.f;
+      for (int k = 0; k < 8; k++) s += r[k];
+      if (s == 123.456f) out[0] = s;
+}
+
 }  // namespace
 }  // namespace ncg
 
 using namespace ncg;
+
+namespace {
+// Best-of-5 duration (ms) of one probe launch over sms*8 blocks of 256 threads.
+template <typename L>
+int best_ms(L launch, float *best)
+{
+      cudaEvent_t e0, e1;
+      NCG_CK(cudaEventCreate(&e0));
+      NCG_CK(cudaEventCreate(&e1));
+      launch();  // warm-up
+      NCG_LAUNCHED();
+      *best = 1e30f;
+      for (int rep = 0; rep < 5; rep++) {
+            NCG_CK(cudaEventRecord(e0));
+            launch();
+            NCG_LAUNCHED();
+            NCG_CK(cudaEventRecord(e1));
+            NCG_CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            NCG_CK(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < *best) *best = ms;
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return NCGPU_OK;
+}
+}  // namespace
+
+extern "C" int ncgpu_probe_fp32_rates(double *ffma_tflops, double *ffma2_tflops, double *rsqrt_gops)
+{
+      if (!ffma_tflops || !ffma2_tflops || !rsqrt_gops) return NCGPU_E_ARG;
+      int dev = 0, sms = 0;
+      NCG_CK(cudaGetDevice(&dev));
+      NCG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+      float *out = nullptr;
+      NCG_CK(cudaMalloc(&out, sizeof(float)));
+      const int blocks = sms * 8;
+      const double lanes = (double)blocks * 256.0 * 8.0 * PROBE_ITERS;
+      float ms = 0.f;
+      int st = best_ms([&] { k_ffma_probe<<<blocks, 256>>>(out, 0.9999f, 1e-6f); }, &ms);
+      if (st == NCGPU_OK) {
+            *ffma_tflops = 2.0 * lanes / (ms * 1e-3) / 1e12;
+            st = best_ms([&] { k_ffma2_probe<<<blocks, 256>>>(out, 0.9999f, 1e-6f); }, &ms);
+      }
+      if (st == NCGPU_OK) {
+            *ffma2_tflops = 4.0 * lanes / (ms * 1e-3) / 1e12;
+            st = best_ms([&] { k_rsqrt_probe<<<blocks, 256>>>(out, 0.5f); }, &ms);
+      }
+      if (st == NCGPU_OK) *rsqrt_gops = lanes / (ms * 1e-3) / 1e9;
+      cudaFree(out);
+      return st;
+}
 
 extern "C" int ncgpu_probe_fp32_peak(double *tflops)
 {

@@ -127,10 +127,10 @@ def frag_test_disk(n=4000, seed=0, density=3.0):
     return _assemble(rng, n, 0.99, 1.01, 0.04, 0.04, mass, rad)
 
 
-def adjoint_disk(n=16384, seed=0, radius=1e-3):
+def adjoint_disk(n=16384, seed=0, radius=1e-2):
     """Differentiable gravity-only disk: the law of ``gravity_disk`` with
-    R = 1e-3, so that the softening length 0.5 (R_k + R_p) = 1e-3 resolves
-    close encounters at dt = 1e-3.  With R = 1e-5 (the force-accuracy disk)
+    R = 1e-2, so that the softening length 0.5 (R_k + R_p) = 1e-2 (about the
+    mean spacing) keeps every encounter smooth at dt = 1e-3.  With R = 1e-5 (the force-accuracy disk)
     bodies of up to 1e-6 central masses bind on orbits far shorter than dt, the
     1,000-step map is chaotic (gradient norms reach 1e22) and no finite
     difference with h = 1e-6 is in its linear regime."""

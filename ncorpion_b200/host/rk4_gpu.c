@@ -66,6 +66,17 @@ static void gpu_params(struct ncgpu_params *p)
       p->par_disruption_threshold = disruption_threshold;
       p->par_high_dumping_threshold = high_dumping_threshold;
       p->par_reduce_to_COM_bool = reduce_to_COM_bool;
+      {
+            int pq[4] = pq_min_max;
+            p->par_N_tilde = N_tilde;
+            for (int j = 0; j < 4; j++) p->par_pq_min_max[j] = pq[j];
+      }
+      p->par_mu_parameter = mu_parameter;
+      p->par_nu_parameter = nu_parameter;
+      p->par_C1_parameter = C1_parameter;
+      p->par_k_parameter = k_parameter;
+      p->par_merging_threshold = merging_threshold;
+      p->par_fragment_threshold = fragment_threshold;
 }
 
 /* The GPU path covers the configurations of its hot path only. */
@@ -116,7 +127,9 @@ static void gpu_collision_records(double t_now)
                   (collisionDatas + indexCollision)->R2 = RA;
                   (collisionDatas + indexCollision)->DeltaV = dV;
                   (collisionDatas + indexCollision)->impact_angle = acos(-drdv / ((RA + RB) * dV));
-                  (collisionDatas + indexCollision)->m_tilde = ev[e].type == NCGPU_COLLISION_MERGER ? mA + mB : mA;
+                  (collisionDatas + indexCollision)->m_tilde = ev[e].type == NCGPU_COLLISION_MERGER         ? mA + mB
+                                                               : ev[e].type == NCGPU_COLLISION_FRAGMENTATION ? r[7]
+                                                                                                             : mA;
                   indexCollision++;
                   if (indexCollision == 2 * output_step * N_max) {
                         fprintf(stderr, "Error: The array collisionDatas is not large enough.\n");
@@ -149,6 +162,14 @@ static void gpu_end_of_timestep(struct moonlet *moonlets, int progressed, long t
       gpu_check(ncgpu_end_of_timestep(&hm), "end_of_timestep");
       if (progressed) {
             gpu_pull(moonlets);
+            if (fragmentation_bool) {  /* the outcome shares of the progress printout (src/rk4.c:244-247) */
+                  int fc[4];
+                  gpu_check(ncgpu_fragment_counts(fc), "fragment counts");
+                  merger_count = fc[0];
+                  super_catastrophic_count = fc[1];
+                  half_fragmentation_count = fc[2];
+                  full_fragmentation_count = fc[3];
+            }
 #if mesh_bool
             total_neighbours = (int)total_nb;
 #endif

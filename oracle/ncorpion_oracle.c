@@ -204,6 +204,7 @@ void orc_w_set(int lid, const body *b, const int *ex, const body *cm, double dt,
       W.n_pairs = 0;
       W.total_neighbours = 0;
       W.collision_count = 0;
+      need_to_reduce_com = 0;
 }
 
 void orc_w_set_timestep(double dt) { W.dt = dt; }

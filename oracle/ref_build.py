@@ -181,6 +181,22 @@ def build(profile: str, src: str, verbose: bool = False) -> str:
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def stale(profile: str) -> bool:
+    """True when the profile is missing, or its drop-in program predates the
+    C ABI header or the drop-in driver it was compiled from."""
+    dst = os.path.join(OUT, profile)
+    if not os.path.exists(os.path.join(dst, "libref.so")):
+        return True
+    ov = PROFILES[profile]
+    if ov.get("brute_force_bool") == "1" or ov.get("mesh_bool") == "1":
+        exe = os.path.join(dst, "ncorpion_gpu")
+        root = os.path.dirname(HERE)
+        deps = [os.path.join(root, "include", "ncgpu.h"), os.path.join(root, "ncorpion_b200", "host", "rk4_gpu.c")]
+        if not os.path.exists(exe) or any(os.path.getmtime(d) > os.path.getmtime(exe) for d in deps):
+            return True
+    return False
+
+
 def build_dropin(tmp: str, dst: str, units) -> None:
     """The reference program with its brute-force and mesh integrations
     replaced by ncorpion_b200/host/rk4_gpu.c on libncgpu.so: main.c is

@@ -55,6 +55,18 @@ def make_params(**kw):
     p.disruption_threshold = 0.1
     p.high_dumping_threshold = 100.0
     p.reduce_to_COM_bool = 1
+    p.N_tilde = 15
+    p.pq_min_max[:] = [-1, 3, -1, 1]
+    p.mu_parameter = 0.55
+    p.nu_parameter = 0.4
+    p.C1_parameter = 1.5
+    p.k_parameter = 0.2
+    p.merging_threshold = 0.0002
+    p.fragment_threshold = 1.5e-8
+    p.mesh_brute_gravity = 0
     for k, v in kw.items():
+        if k == "pq_min_max":
+            p.pq_min_max[:] = list(v)
+            continue
         setattr(p, k, v)
     return p

@@ -166,16 +166,40 @@ def test_torch_autograd_function(lib_ready):
 
 
 def test_adjoint_disk_16384_1000_steps(lib):
-    """The differentiable workload: N = 16,384 (log-uniform masses, softening
-    0.5 (R_k + R_p)), 1,000 steps, dt = 1e-3, checkpoints every 32 steps;
-    MSE loss to a seeded target; 64 coordinates: x and v against FP64 central
-    differences with h = 1e-6, m against the tangent-linear model."""
+    """The differentiable workload: N = 16,384 (log-uniform masses, R = 1e-2,
+    softening 0.5 (R_k + R_p)), 1,000 steps, dt = 1e-3, checkpoints every 32
+    steps; MSE loss to a seeded target; 64 coordinates: x and v against FP64
+    central differences with h = 1e-6, m against the tangent-linear model."""
+    from ncorpion_b200 import api, disks
+    api.init(16384, make_params(softening_parameter=0.5))
+    try:
+        b, cm = disks.reduce_to_com(disks.adjoint_disk(16384, 0), np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0]))
+        w = _fd_check(api, b, cm, 1e-3, 1000, 64, seed=11)
+        print("adjoint 16384 x 1000 worst relative errors:", w)
+        _assert_worst(w)
+    finally:
+        api.finalize()
+
+
+def test_adjoint_chaotic_disk_dot_product(lib):
+    """On the R = 1e-5 disk the 1,000-step map is chaotic (finite differences
+    leave the linear regime), but the adjoint must still be the exact
+    transpose of the tangent-linear model along the same trajectory:
+    <w, J d> = <J^T w, d> for seeded w, d, to 1e-8 relative."""
     from ncorpion_b200 import api
     api.init(16384, make_params(softening_parameter=0.5))
     try:
         b, cm = disk(16384, 0)
-        w = _fd_check(api, b, cm, 1e-3, 1000, 64, seed=11)
-        print("adjoint 16384 x 1000 worst relative errors:", w)
-        _assert_worst(w)
+        n = len(b)
+        rng = np.random.default_rng(21)
+        args = (b[:, :3], b[:, 3:6], b[:, 6], b[:, 7], cm, 1e-3, 1000)
+        dx, dv, dm = rng.normal(size=(n, 3)), rng.normal(size=(n, 3)), rng.normal(size=n) * b[:, 6]
+        w = rng.normal(size=(n, 3))
+        jd = api.leapfrog_jvp(*args, dx, dv, dm)
+        gx, gv, gm = api.leapfrog_vjp(*args, w)
+        lhs = float(np.sum(w * jd))
+        rhs = float(np.sum(gx * dx) + np.sum(gv * dv) + np.sum(gm * dm))
+        print("chaotic disk <w, J d> =", lhs, " <J^T w, d> =", rhs)
+        assert np.isfinite(lhs) and abs(lhs - rhs) <= 1e-8 * abs(lhs)
     finally:
         api.finalize()
