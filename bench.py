@@ -181,39 +181,40 @@ MESH_WORKLOAD = ("mesh collision search + mesh gravity, N=1,048,576 disk (a~U[0.
                  "collision_cube_min 4.4 (mesh size >= 2 x max radius), instant mergers, dt=5e-4")
 
 
-def mesh_params(mode):
+def mesh_params(mode, cells=1024):
     from ncorpion_b200 import api
     return api.default_params(G=1.0, softening_parameter=0.0, collision_bool=1, brute_force_bool=0, mesh_bool=1,
-                              collision_type=api.COLLISION_MERGER, collision_cube_cells=1024,
+                              collision_type=api.COLLISION_MERGER, collision_cube_cells=cells,
                               how_many_neighbours=16.0, collision_cube_min=4.4, gravity_mode=mode,
                               disruption_threshold=0.1, high_dumping_threshold=100.0)
 
 
-def mesh_gamma0(n):
+def mesh_gamma0(n, cells=1024):
     """The initial mesh size of variable_initialization (src/structure.c:515-523)
     with sma 0.5 .. 2.0, inclination_max 0.015, how_many_neighbours 16."""
     gam = (2.0 ** 3 - 0.5 ** 3) ** (1.0 / 3.0) * (4.0 * np.pi * 16.0 * np.sin(0.015) / (n * 81.0)) ** (1.0 / 3.0)
-    return max(gam, 4.4 / 1024)
+    return max(gam, 4.4 / cells)
 
 
-def bench_mesh(lib, api, torch, mode, steps, warmup):
+def bench_mesh(lib, api, torch, mode, steps, warmup, n_bodies=None, cells=1024):
     """Steps/s of the mesh integrator loop on the device state, CUDA events on
     the library stream; the half kick of integration_mesh first."""
     from ncorpion_b200 import disks
-    b = disks.mesh_disk(MESH_N, seed=0)
-    ex = np.ones(MESH_N, np.int32)
+    n_bodies = n_bodies or MESH_N
+    b = disks.mesh_disk(n_bodies, seed=0)
+    ex = np.ones(n_bodies, np.int32)
     cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
-    api.init(1100000, mesh_params(mode))
+    api.init(n_bodies + n_bodies // 20, mesh_params(mode, cells))
     api.upload(b, ex, cm)
-    gmin = 4.4 / 1024
-    gam = mesh_gamma0(MESH_N)
+    gmin = 4.4 / cells
+    gam = mesh_gamma0(n_bodies, cells)
     api.set_timestep(MESH_DT / 2)
     api.three_largest()
     _, _, tn = api.mesh(gam, False)
     api.kick()
     api.mesh_reset()
     api.set_timestep(MESH_DT)
-    gam = api.update_gamma(gam, tn, MESH_N, 16.0, gmin)
+    gam = api.update_gamma(gam, tn, n_bodies, 16.0, gmin)
     st = torch.cuda.ExternalStream(lib.ncgpu_stream())
     for _ in range(warmup):
         hm, tn = api.step_mesh(gam)
@@ -322,6 +323,9 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mesh", action="store_true")
     ap.add_argument("--no-frag", action="store_true")
+    ap.add_argument("--mesh-n", type=int, default=MESH_N, help="mesh workload bodies (smaller cases for profiling)")
+    ap.add_argument("--mesh-cells", type=int, default=1024)
+    ap.add_argument("--mesh-steps", type=int, default=MESH_STEPS)
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
     ws, rank, local = dist_info()
@@ -388,8 +392,8 @@ def main(argv=None):
     clock.start()
     ms_mixed, kms_mixed, launches = timed(api.GRAVITY_MIXED, a.steps, a.warmup)
     clocks = clock.stop()
-    ms_fp64t, kms_fp64t, _ = timed(api.GRAVITY_FP64, max(2, a.steps // 3), 1)
-    ms_exact, kms_exact, _ = timed(api.GRAVITY_EXACT, 2, 1)
+    ms_fp64t, kms_fp64t, _ = timed(api.GRAVITY_FP64, max(3, a.steps // 3), 3)
+    ms_exact, kms_exact, _ = timed(api.GRAVITY_EXACT, 3, 3)
 
     # accuracy of the mixed kernel against the exact FP64 result
     def accel(mode, central):
@@ -441,12 +445,13 @@ def main(argv=None):
 
     mesh = None
     if not a.no_mesh:
-        mesh_fast = bench_mesh(lib, api, torch, api.GRAVITY_MIXED, MESH_STEPS, 3)
-        mesh_exact = bench_mesh(lib, api, torch, api.GRAVITY_EXACT, 10, 2)
+        mesh_fast = bench_mesh(lib, api, torch, api.GRAVITY_MIXED, a.mesh_steps, 3, a.mesh_n, a.mesh_cells)
+        mesh_exact = bench_mesh(lib, api, torch, api.GRAVITY_EXACT, min(10, a.mesh_steps), 3, a.mesh_n,
+                                a.mesh_cells)
         n_pairs = mesh_fast["pairs_per_step"]
         # algorithmic bytes per step: 56 B/body state read + 8 B key/index + 72 B drift + 72 B kick
         # per body; 8 B written + 16 B read per pair (search and gravity)
-        alg = MESH_N * (56 + 8 + 72 + 72) + n_pairs * (8 + 16)
+        alg = a.mesh_n * (56 + 8 + 72 + 72) + n_pairs * (8 + 16)
         hbm_peak = 6426.2
         try:
             with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -454,14 +459,17 @@ def main(argv=None):
         except Exception:
             pass
         ach = alg / (mesh_fast["ms_per_step"] * 1e-3) / 1e9
-        mesh = {"metric": "mesh collision steps/s at N=1M", "workload": MESH_WORKLOAD, "fast": mesh_fast,
+        wl = MESH_WORKLOAD if (a.mesh_n, a.mesh_cells) == (MESH_N, 1024) else \
+            f"{MESH_WORKLOAD} -- reduced to N={a.mesh_n}, {a.mesh_cells} cells per side"
+        mesh = {"metric": f"mesh collision steps/s at N={a.mesh_n}", "workload": wl, "fast": mesh_fast,
                 "exact": mesh_exact,
                 "note": "fast: CM_acc and the three largest bodies' sums as two-level parallel sums; exact: "
                         "sequential FP64 chains (bit-identical state); pairs[] and events are exact in both",
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
                              "algorithmic_bytes_per_step": alg, "traffic": None,
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
-                "cpu_baseline": mesh_cpu_reference() if (rank == 0 and ws == 1 and not a.no_cpu_baseline) else None}
+                "cpu_baseline": mesh_cpu_reference() if (rank == 0 and ws == 1 and not a.no_cpu_baseline
+                                                         and a.mesh_n == MESH_N) else None}
     frag = None
     if not a.no_frag:
         fm = bench_fragment(lib, api, torch, api.GRAVITY_MIXED, FRAG_STEPS)

@@ -5,6 +5,7 @@
 // sequential momentum sums of total_momentum, src/structure.c:1193-1227) run
 // in slot order on one thread per sum, so results match the reference bit for
 // bit; the O(N) scans around them are parallel.
+#include <algorithm>
 #include "common.cuh"
 #include "physics.cuh"
 
@@ -70,24 +71,93 @@ __global__ void k_eot_dump(const DevState S, const int *__restrict__ list, int n
 }
 
 // total_momentum: lane d < 6 sums component d, lane 6 the mass, in slot order.
-__global__ void k_total_momentum(const DevState S, const int *__restrict__ list, int n, const double *__restrict__ cm,
-                                 int central, double *__restrict__ com)
+// total_momentum's terms in slot order: m_j x_j, m_j y_j, ... m_j vz_j and
+// m_j (7 arrays of n), so the sums below read them coalesced.
+__global__ void k_momentum_terms(const DevState S, const int *__restrict__ list, int n, double *__restrict__ terms)
 {
-      __shared__ double M_s;
-      int d = threadIdx.x;
-      double M = central ? cm[6] : 0.;
-      double s = 0.;
-      if (d < 6) s = DMUL(M, central ? cm[d] : 0.);
-      const double *f = d == 0 ? S.x : d == 1 ? S.y : d == 2 ? S.z : d == 3 ? S.vx : d == 4 ? S.vy : S.vz;
-      for (int q = 0; q < n; q++) {
-            int j = list[q];
-            double m = S.m[j];
-            if (d < 6) s = DADD(s, DMUL(m, f[j]));
-            else if (d == 6) M = DADD(M, m);
+      int q = blockIdx.x * blockDim.x + threadIdx.x;
+      if (q >= n) return;
+      int j = list[q];
+      double m = S.m[j];
+      terms[q] = DMUL(m, S.x[j]);
+      terms[(size_t)n + q] = DMUL(m, S.y[j]);
+      terms[2 * (size_t)n + q] = DMUL(m, S.z[j]);
+      terms[3 * (size_t)n + q] = DMUL(m, S.vx[j]);
+      terms[4 * (size_t)n + q] = DMUL(m, S.vy[j]);
+      terms[5 * (size_t)n + q] = DMUL(m, S.vz[j]);
+      terms[6 * (size_t)n + q] = m;
+}
+
+// The central body's share, which starts every sum (src/structure.c:1202-1210).
+__device__ __forceinline__ double momentum_init(int d, const double *cm, int central)
+{
+      const double M = central ? cm[6] : 0.;
+      return d == 6 ? M : DMUL(M, central ? cm[d] : 0.);
+}
+
+// total_momentum (src/structure.c:1193-1227) in the reference's order: one
+// warp per component sums its n terms sequentially (FP64, no reassociation);
+// the warp stages CHM terms at a time in shared memory with coalesced loads so
+// the dependent adds do not wait on global memory.
+constexpr int CHM = 512;
+__global__ void __launch_bounds__(224) k_momentum_chains(const double *__restrict__ terms, int n,
+                                                         const double *__restrict__ cm, int central,
+                                                         double *__restrict__ com)
+{
+      __shared__ double buf[7][CHM];
+      __shared__ double tot[7];
+      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const double *t = terms + (size_t)w * n;
+      double s = momentum_init(w, cm, central);
+      for (int base = 0; base < n; base += CHM) {
+            const int cnt = min(CHM, n - base);
+            for (int i = lane; i < cnt; i += 32) buf[w][i] = t[base + i];
+            __syncwarp();
+            if (lane == 0)
+                  for (int i = 0; i < cnt; i++) s = DADD(s, buf[w][i]);
+            __syncwarp();
       }
-      if (d == 6) M_s = M;
+      if (lane == 0) tot[w] = s;
       __syncthreads();
-      if (d < 6) com[d] = DDIV(s, M_s);
+      if (threadIdx.x < 6) com[threadIdx.x] = DDIV(tot[threadIdx.x], tot[6]);
+}
+
+// The same sums as a deterministic two-level parallel reduction (non-exact
+// gravity modes): block b adds a fixed slice, the fold adds the slices in order.
+constexpr int MPB = 256;
+__global__ void __launch_bounds__(MPB) k_momentum_part(const double *__restrict__ terms, int n,
+                                                       double *__restrict__ part)
+{
+      __shared__ double sh[7][MPB / 32];
+      double s[7] = {0., 0., 0., 0., 0., 0., 0.};
+      for (int q = blockIdx.x * MPB + threadIdx.x; q < n; q += gridDim.x * MPB)
+            for (int d = 0; d < 7; d++) s[d] += terms[(size_t)d * n + q];
+      const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+      for (int d = 0; d < 7; d++) {
+            double v = s[d];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) sh[d][wp] = v;
+      }
+      __syncthreads();
+      if (threadIdx.x < 7) {
+            double v = 0.;
+            for (int q = 0; q < MPB / 32; q++) v += sh[threadIdx.x][q];
+            part[blockIdx.x * 7 + threadIdx.x] = v;
+      }
+}
+
+__global__ void k_momentum_fold(const double *__restrict__ part, int nparts, const double *__restrict__ cm,
+                                int central, double *__restrict__ com)
+{
+      __shared__ double tot[7];
+      const int d = threadIdx.x;
+      if (d < 7) {
+            double s = 0.;
+            for (int b = 0; b < nparts; b++) s += part[7 * b + d];
+            tot[d] = momentum_init(d, cm, central) + s;
+      }
+      __syncthreads();
+      if (d < 6) com[d] = tot[d] / tot[6];
 }
 
 __global__ void k_sub_com(const DevState S, int lid, const double *__restrict__ com, double *cm, int central)
@@ -160,9 +230,28 @@ int eot_state(int *hm_out)
       if (h[S_NEEDCOM] && P.par_reduce_to_COM_bool) {
             int n = 0;
             NCG_TRY(compact_existing(c.ex, lid, &n, st));
-            k_total_momentum<<<1, 32, 0, st>>>(S, c.cidx, n, c.cm, P.par_central_mass_bool, c.red + 3072);
-            NCG_LAUNCHED();
-            k_sub_com<<<nb, 256, 0, st>>>(S, lid, c.red + 3072, c.cm, P.par_central_mass_bool);
+            double *com = c.red + 3072;
+            if (n > 0) {
+                  NCG_TRY(ensure_partial((size_t)7 * n + 7 * 148));
+                  double *terms = c.partial;
+                  k_momentum_terms<<<(n + 255) / 256, 256, 0, st>>>(S, c.cidx, n, terms);
+                  NCG_LAUNCHED();
+                  if (P.par_gravity_mode == NCGPU_GRAVITY_EXACT) {
+                        k_momentum_chains<<<1, 224, 0, st>>>(terms, n, c.cm, P.par_central_mass_bool, com);
+                        NCG_LAUNCHED();
+                  } else {
+                        const int np = std::min(148, (n + MPB - 1) / MPB);
+                        double *part = terms + (size_t)7 * n;
+                        k_momentum_part<<<np, MPB, 0, st>>>(terms, n, part);
+                        NCG_LAUNCHED();
+                        k_momentum_fold<<<1, 32, 0, st>>>(part, np, c.cm, P.par_central_mass_bool, com);
+                        NCG_LAUNCHED();
+                  }
+            } else {
+                  k_momentum_fold<<<1, 32, 0, st>>>(c.red + 3584, 0, c.cm, P.par_central_mass_bool, com);
+                  NCG_LAUNCHED();
+            }
+            k_sub_com<<<nb, 256, 0, st>>>(S, lid, com, c.cm, P.par_central_mass_bool);
             NCG_LAUNCHED();
             NCG_CK(cudaMemsetAsync(c.scal + S_NEEDCOM, 0, sizeof(int), st));
       }

@@ -90,8 +90,11 @@ __global__ void k_mesh_count(const int *__restrict__ ckey, const uint32_t *__res
                              const int *__restrict__ vals, const int *__restrict__ cstart, int lid, int d,
                              long long cap, int *__restrict__ cnt)
 {
-      int k = blockIdx.x * blockDim.x + threadIdx.x;
-      if (k > lid) return;
+      // threads walk the bodies in cell order (vals = bodies sorted by cell), so
+      // the threads of a warp share cells and partners
+      const int t = blockIdx.x * blockDim.x + threadIdx.x;
+      if (t > lid) return;
+      const int k = vals[t];
       int L = ckey[k];
       int c = 0;
       if (L >= 0) {
@@ -116,8 +119,9 @@ __global__ void k_mesh_write(DevState S, const int *__restrict__ ckey, const uin
                              int *__restrict__ ck, int *__restrict__ cp, unsigned char *__restrict__ cflag,
                              int *__restrict__ hitpos, int hit_cap, int *__restrict__ nhits, unsigned *err)
 {
-      int k = blockIdx.x * blockDim.x + threadIdx.x;
-      if (k > lid) return;
+      const int t = blockIdx.x * blockDim.x + threadIdx.x;  // cell order, as k_mesh_count
+      if (t > lid) return;
+      const int k = vals[t];
       int L = ckey[k];
       if (L < 0) return;
       int pos = off[k];

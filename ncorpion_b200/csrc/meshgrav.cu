@@ -251,8 +251,12 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                             double *__restrict__ ax, double *__restrict__ ay, double *__restrict__ az,
                             double *__restrict__ terms, long N)
 {
-      int b = blockIdx.x * blockDim.x + threadIdx.x;
-      if (b > A.lid || !S.ex[b]) return;
+      // bodies of the cell table in cell order (neighbouring threads share cells
+      // and partners), then the bodies appended after the pass
+      const int t = blockIdx.x * blockDim.x + threadIdx.x;
+      if (t > A.lid) return;
+      const int b = (have_cells && t <= A.lid0) ? vals[t] : t;
+      if (!S.ex[b]) return;
       double a_x = 0., a_y = 0., a_z = 0.;
       if (A.central) {
             double DX = DSUB(S.x[b], A.cmx), DY = DSUB(S.y[b], A.cmy), DZ = DSUB(S.z[b], A.cmz);
