@@ -139,6 +139,11 @@ struct Ctx {
       int mesh_nev = 0;            // events recorded by the last mesh pass
       int mesh_nfev = 0;           // full fragmentations of the last mesh pass
       int mesh_nx = 0;             // extra pairs of the last mesh pass
+      // visits of bodies larger than the mesh size in the last mesh pass:
+      // (body, first candidate, end) in visit order
+      int *vis = nullptr;
+      int vis_host[3 * 1024];
+      int mesh_nvis = 0;
       int mesh_valid = 0;          // cell table populated by the last pass
       int mesh_n = 0;              // sorted entries of the last pass (largest_id + 1)
       int n_cand = 0, n_pairs = 0;
@@ -177,6 +182,8 @@ enum Scal : int {
 constexpr int EVREC = 8;
 // Per-event ints of a mesh pass (see Ctx::evx).
 constexpr int EVX = 8;
+// Visits of bodies larger than the mesh size recorded per mesh pass.
+constexpr int MAX_VISITS = 1024;
 
 Ctx &ctx();
 int ensure_partial(size_t doubles);

@@ -85,17 +85,19 @@ __global__ void k_cell_clear(const uint32_t *__restrict__ keys, int n, int *__re
       if (key != NOKEY && (q == 0 || keys[q - 1] != key)) cstart[key] = -1;
 }
 
-// number of candidates of body k: bodies of lower index in its 27 cells
-__global__ void k_mesh_count(const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
-                             const int *__restrict__ vals, const int *__restrict__ cstart, int lid, int d,
-                             long long cap, int *__restrict__ cnt)
+// number of candidates of body k (lo <= k < hi): existing bodies of lower
+// index in its 27 cells; 0 outside [lo, hi)
+__global__ void k_mesh_count(const int *__restrict__ ex, const int *__restrict__ ckey,
+                             const uint32_t *__restrict__ keys, const int *__restrict__ vals,
+                             const int *__restrict__ cstart, int lid, int lo, int hi, int d, long long cap,
+                             int *__restrict__ cnt)
 {
       // threads walk the bodies in cell order (vals = bodies sorted by cell), so
       // the threads of a warp share cells and partners
       const int t = blockIdx.x * blockDim.x + threadIdx.x;
       if (t > lid) return;
       const int k = vals[t];
-      int L = ckey[k];
+      int L = (k >= lo && k < hi) ? ckey[k] : -1;
       int c = 0;
       if (L >= 0) {
             for (int l = 26; l >= 0; --l) {
@@ -104,8 +106,9 @@ __global__ void k_mesh_count(const int *__restrict__ ckey, const uint32_t *__res
                   int s = cstart[cell];
                   if (s < 0) continue;
                   for (int q = s; keys[q] == (uint32_t)cell; ++q) {
-                        if (vals[q] >= k) break;
-                        c++;
+                        const int p = vals[q];
+                        if (p >= k) break;
+                        if (ex[p]) c++;  // a body removed earlier in the pass is not pushed
                   }
             }
       }
@@ -115,13 +118,14 @@ __global__ void k_mesh_count(const int *__restrict__ ckey, const uint32_t *__res
 // candidates of body k in pop order; hit flag from the entry-state predicate
 __global__ void k_mesh_write(DevState S, const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
                              const int *__restrict__ vals, const int *__restrict__ cstart,
-                             const int *__restrict__ off, int lid, int d, long long cap, double dt, int test,
-                             int *__restrict__ ck, int *__restrict__ cp, unsigned char *__restrict__ cflag,
+                             const int *__restrict__ off, int lid, int lo, int hi, int d, long long cap, double dt,
+                             int test, int *__restrict__ ck, int *__restrict__ cp, unsigned char *__restrict__ cflag,
                              int *__restrict__ hitpos, int hit_cap, int *__restrict__ nhits, unsigned *err)
 {
       const int t = blockIdx.x * blockDim.x + threadIdx.x;  // cell order, as k_mesh_count
       if (t > lid) return;
       const int k = vals[t];
+      if (k < lo || k >= hi) return;
       int L = ckey[k];
       if (L < 0) return;
       int pos = off[k];
@@ -134,6 +138,7 @@ __global__ void k_mesh_write(DevState S, const int *__restrict__ ckey, const uin
             for (int q = s; keys[q] == (uint32_t)cell; ++q) {
                   int p = vals[q];
                   if (p >= k) break;
+                  if (!S.ex[p]) continue;
                   ck[pos] = k;
                   cp[pos] = p;
                   unsigned char f = 0;
@@ -164,6 +169,7 @@ struct MeshEvArgs {
       int add_pairs;            // mutual_bool: pairs[] is kept
       long xpair_cap;
       FragArgs frag;            // fragmentation constants (type 3)
+      int seg_hi;               // querying bodies of this replay: below seg_hi (candidate lists exist)
 };
 
 // Buffers of the fragmentation bookkeeping (see Ctx::evx).
@@ -312,9 +318,20 @@ __global__ void __launch_bounds__(MEV) k_mesh_events(DevState S, const int *__re
                   int A, B;
                   int k = ck[q], p = cp[q];
                   d_mesh_treat(S, p, k, q, E, ev, evrec, cflag, X, err, &A, &B);
+                  // dirty: 1 = modified (its later occurrences are re-tested), 2 = removed
+                  // (its later occurrences are dropped).  A body already modified by an
+                  // earlier event and removed by this one is processed again.
                   int nn = 0;
-                  if (!dirty[A]) { dirty[A] = 1; newb[nn++] = A; }
-                  if (!dirty[B]) { dirty[B] = 1; newb[nn++] = B; }
+                  const int who[2] = {A, B};
+                  for (int w = 0; w < 2; w++) {
+                        const int x = who[w];
+                        if (w == 1 && x == A) break;
+                        const unsigned char want = S.ex[x] ? 1 : 2;
+                        if (dirty[x] < want) {
+                              dirty[x] = want;
+                              newb[nn++] = x;
+                        }
+                  }
                   newn = nn;
                   kq_s = k;
                   q_s = q;
@@ -342,7 +359,7 @@ __global__ void __launch_bounds__(MEV) k_mesh_events(DevState S, const int *__re
                         if (s < 0) continue;
                         for (int qq = s + (threadIdx.x & 31); qq < E.nsorted && keys[qq] == (uint32_t)cell; qq += 32) {
                               int kk = vals[qq];
-                              if (kk <= kq) continue;
+                              if (kk <= kq || kk >= E.seg_hi) continue;
                               for (int r = off[kk]; r < off[kk + 1]; ++r) {
                                     if (cp[r] != x) continue;
                                     if (alive) {
@@ -356,7 +373,7 @@ __global__ void __launch_bounds__(MEV) k_mesh_events(DevState S, const int *__re
                         }
                   }
                   // a removed body does not query its own cells either
-                  if (!alive && x > kq)
+                  if (!alive && x > kq && x < E.seg_hi)
                         for (int r = off[x] + threadIdx.x; r < off[x + 1]; r += MEV) cflag[r] |= F_DROP;
             }
             cur = q;
@@ -371,6 +388,123 @@ __global__ void k_count_dropped(const unsigned char *__restrict__ cflag, int n, 
       int d = q < n && (cflag[q] & F_DROP) ? 1 : 0;
       d = __syncthreads_count(d);
       if (threadIdx.x == 0 && d) atomicAdd(ndrop, d);
+}
+
+// ---- bodies larger than the mesh size (src/collision.c:380-410) ----------
+
+// The smallest slot k in [lo, lid] holding a body larger than the mesh size.
+__global__ void k_next_big(const DevState S, int lo, int lid, double gam, int *__restrict__ out)
+{
+      int k = lo + blockIdx.x * blockDim.x + threadIdx.x;
+      if (k <= lid && S.ex[k] && S.R[k] > gam) atomicMin(out, k);
+}
+
+// Cell keys for a pass resumed at slot lo: bodies below lo keep the cell they
+// were inserted in; the others get the cell of their current position (or
+// none: removed, larger than the mesh size, outside the cube).
+__global__ void k_mesh_rekey(const DevState S, int lo, int lid, double gam, double half, int d,
+                             uint32_t *__restrict__ keys, int *__restrict__ vals, int *__restrict__ ckey)
+{
+      int k = blockIdx.x * blockDim.x + threadIdx.x;
+      if (k > lid) return;
+      long long L;
+      if (k < lo) {
+            L = ckey[k];
+      } else {
+            L = -1;
+            if (S.ex[k] && S.R[k] <= gam) L = d_cell(S.x[k], S.y[k], S.z[k], gam, half, d);
+            ckey[k] = (int)L;
+      }
+      keys[k] = L >= 0 ? (uint32_t)L : NOKEY;
+      vals[k] = k;
+}
+
+__global__ void k_add_base(int *__restrict__ off, int n, int base)
+{
+      int k = blockIdx.x * blockDim.x + threadIdx.x;
+      if (k <= n) off[k] += base;
+}
+
+// The big-body branch of mesh() for body e at its turn, one CTA: every
+// existing p != e with R_p < gam, or p > e, in ascending p up to the live
+// largest_id (tail fragments made meanwhile are visited too), becomes the
+// candidate (e, p) at positions base, base + 1, ...; collisions are resolved
+// one at a time in p order against the current state.  *count gets the number
+// of candidates written.
+constexpr int BVT = 1024;
+__global__ void __launch_bounds__(BVT) k_big_visit(DevState S, int e, double gam, int base, long cap, MeshEvArgs E,
+                                                   int *__restrict__ ck, int *__restrict__ cp,
+                                                   unsigned char *__restrict__ cflag, int *ev, double *evrec,
+                                                   MeshFragBufs X, int *__restrict__ count, unsigned *err)
+{
+      __shared__ int ws[BVT / 32];
+      __shared__ int s_lid, s_pos, s_first;
+      const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+      if (t == 0) s_pos = base;
+      int p0 = 0;
+      for (int iter = 0;; ++iter) {
+            if (iter > (1 << 24)) {
+                  if (t == 0) atomicOr(err, ERR_TIMEOUT);
+                  break;
+            }
+            __syncthreads();
+            if (t == 0) s_lid = S.scal[S_LID];
+            __syncthreads();
+            const int lid = s_lid;
+            if (p0 > lid) break;
+            const int p = p0 + t;
+            const bool qual = p <= lid && S.ex[p] && p != e && (S.R[p] < gam || p > e);
+            // exclusive rank of this candidate within the chunk
+            const unsigned bal = __ballot_sync(0xffffffffu, qual);
+            int rank = __popc(bal & ((1u << lane) - 1u));
+            if (lane == 0) ws[w] = __popc(bal);
+            __syncthreads();
+            if (w == 0) {
+                  int v = ws[lane];
+                  for (int o = 1; o < 32; o <<= 1) {
+                        int u = __shfl_up_sync(0xffffffffu, v, o);
+                        if (lane >= o) v += u;
+                  }
+                  ws[lane] = v;  // inclusive
+            }
+            __syncthreads();
+            rank += w > 0 ? ws[w - 1] : 0;
+            const int chunk = ws[BVT / 32 - 1];
+            const long q = (long)s_pos + rank;
+            if (qual) {
+                  if (q < cap) {
+                        ck[q] = e;
+                        cp[q] = p;
+                        cflag[q] = 0;
+                  } else {
+                        atomicOr(err, ERR_CAPACITY);
+                  }
+            }
+            // collisions in p order: the first hit is resolved, the rest re-tested
+            int from = p0;
+            for (int r = 0; r <= BVT; ++r) {
+                  const bool hit = qual && p >= from && q < cap && !S.did[e] && !S.did[p] &&
+                                   d_approach(S, p, e, E.dt, nullptr);
+                  if (t == 0) s_first = 0x7fffffff;
+                  __syncthreads();
+                  if (hit) atomicMin(&s_first, p);
+                  __syncthreads();
+                  const int ph = s_first;
+                  if (ph == 0x7fffffff) break;
+                  if (p == ph) {
+                        int A, B;
+                        d_mesh_treat(S, p, e, (int)q, E, ev, evrec, cflag, X, err, &A, &B);
+                  }
+                  __syncthreads();
+                  from = ph + 1;
+            }
+            __syncthreads();
+            if (t == 0) s_pos += chunk;
+            // bodies appended past this chunk's largest_id are visited next
+            p0 = min(p0 + BVT, lid + 1);
+      }
+      __syncthreads();
+      if (t == 0) *count = s_pos - base;
 }
 
 // pairs[] = candidates without dropped / merged entries, swapped ones as (p, k)
@@ -463,6 +597,7 @@ static int mesh_alloc(int d)
             NCG_CK(cudaMalloc(&c.xhead, sizeof(int) * N));
             NCG_CK(cudaMemsetAsync(c.xhead, 0xff, sizeof(int) * N, c.s));
             NCG_CK(cudaMalloc(&c.fev, sizeof(int) * (size_t)c.ev_cap));
+            NCG_CK(cudaMalloc(&c.vis, sizeof(int) * 3 * (size_t)MAX_VISITS));
       }
       return NCGPU_OK;
 }
@@ -471,7 +606,7 @@ void mesh_free()
 {
       Ctx &c = ctx();
       void *ptrs[] = {c.cstart, c.mkeys, c.mvals, c.ckey, c.mcnt, c.moff, c.cand_k, c.cand_p, c.cflag, c.cpos,
-                      c.occ, c.msums, c.evx, c.xpairs, c.xhead, c.fev};
+                      c.occ, c.msums, c.evx, c.xpairs, c.xhead, c.fev, c.vis};
       for (void *p : ptrs)
             if (p) cudaFree(p);
 }
@@ -494,7 +629,7 @@ int mesh_reset_state()
             NCG_LAUNCHED();
       }
       c.mesh_valid = 0;
-      c.mesh_nev = c.mesh_nfev = c.mesh_nx = 0;
+      c.mesh_nev = c.mesh_nfev = c.mesh_nx = c.mesh_nvis = 0;
       return NCGPU_OK;
 }
 
@@ -507,8 +642,85 @@ __global__ void k_clear_dirty_events(unsigned char *dirty, const int *ev, int n)
       }
 }
 
+// Candidates of the bodies k in [lo, hi) (pop order, positions from base),
+// their hits against the current state and, with collisions, the ordered
+// event replay over them.  *tot = candidates written.
+static int mesh_segment(const DevState &S, int lid, int lo, int hi, long base, int test, const MeshEvArgs &E0,
+                        int *tot)
+{
+      Ctx &c = ctx();
+      cudaStream_t st = c.s;
+      const int n = lid + 1;
+      const int nb = (n + 255) / 256;
+      const int d = c.P.par_collision_cube_cells;
+      k_mesh_count<<<nb, 256, 0, st>>>(c.ex, c.ckey, c.mkeys, c.mvals, c.cstart, lid, lo, hi, d,
+                                       (long long)c.cell_cap, c.mcnt);
+      NCG_LAUNCHED();
+      NCG_TRY(scan_exclusive(c.mcnt, c.moff, n, c.cnt, st));
+      if (base > 0) {
+            k_add_base<<<(n + 256) / 256, 256, 0, st>>>(c.moff, n, (int)base);
+            NCG_LAUNCHED();
+      }
+      int end = 0;
+      NCG_CK(cudaMemcpyAsync(&end, c.moff + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaMemsetAsync(c.scal + S_NHITS, 0, sizeof(int), st));
+      NCG_CK(cudaStreamSynchronize(st));
+      const long total = (long)end - base;
+      if ((long)end > c.pair_cap) return NCGPU_E_CAPACITY;
+      *tot = (int)total;
+      if (total == 0) return NCGPU_OK;
+      k_mesh_write<<<nb, 256, 0, st>>>(S, c.ckey, c.mkeys, c.mvals, c.cstart, c.moff, lid, lo, hi, d,
+                                       (long long)c.cell_cap, c.dt, test, c.cand_k, c.cand_p, c.cflag, c.hi, c.hit_cap,
+                                       c.scal + S_NHITS, c.err);
+      NCG_LAUNCHED();
+      int nh = 0;
+      NCG_CK(cudaMemcpyAsync(&nh, c.scal + S_NHITS, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      if (nh > c.hit_cap) return NCGPU_E_CAPACITY;
+      if (nh > 0) {
+            NCG_CK(cudaMemcpyAsync(c.keys, c.hi, sizeof(int) * (size_t)nh, cudaMemcpyDeviceToDevice, st));
+            NCG_CK(cudaMemsetAsync(c.vals, 0, sizeof(int) * (size_t)nh, st));
+            NCG_TRY(radix_sort_pairs(c.keys, c.vals, nh, 31, st));
+            MeshEvArgs E = E0;
+            E.seg_hi = hi;
+            MeshFragBufs X{c.evx, c.xpairs, c.xhead, c.fev};
+            k_mesh_events<<<1, MEV, 0, st>>>(S, c.cand_k, c.cand_p, c.cflag, c.moff, c.ckey, c.mkeys, c.mvals,
+                                             c.cstart, (const int *)c.keys, nh, E, c.ev, c.evrec, c.dirty, c.occ,
+                                             c.scal + S_NDROP, X, c.err);
+            NCG_LAUNCHED();
+            k_count_dropped<<<(int)((total + 255) / 256), 256, 0, st>>>(c.cflag + base, (int)total,
+                                                                       c.scal + S_NDROP);
+            NCG_LAUNCHED();
+      }
+      return NCGPU_OK;
+}
+
+// Cell table of the bodies' insertion cells (ckey -> sorted keys, heads).
+static int mesh_table(int n)
+{
+      Ctx &c = ctx();
+      cudaStream_t st = c.s;
+      NCG_TRY(radix_sort_pairs(c.mkeys, c.mvals, n, 32, st));
+      NCG_CK(cudaMemsetAsync(c.mkeys + n, 0xff, sizeof(uint32_t), st));
+      k_cell_heads<<<(n + 255) / 256, 256, 0, st>>>(c.mkeys, n, c.cstart, c.scal + S_NINS);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
+
+static int read_scal(int idx, int *out)
+{
+      Ctx &c = ctx();
+      NCG_CK(cudaMemcpyAsync(out, c.scal + idx, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaStreamSynchronize(c.s));
+      return NCGPU_OK;
+}
+
 // One mesh pass.  test = 1: mesh() (small bodies, predicate and resolution);
-// test = 0: get_neighbours_mesh() (every body, no predicate).
+// test = 0: get_neighbours_mesh() (every body, no predicate).  With bodies
+// larger than the mesh size the pass runs as segments of small bodies (the
+// parallel candidate machinery) separated by the big bodies' visits (one CTA
+// each); a visit that resolved collisions re-keys the bodies after it, whose
+// positions and radii at their turn may have changed.
 int mesh_pass(double gam, int test)
 {
       Ctx &c = ctx();
@@ -525,66 +737,104 @@ int mesh_pass(double gam, int test)
       c.n_cand = c.n_pairs = 0;
       c.total_neighbours = 0;
       c.how_many_small = c.how_many_big = 0;
+      c.mesh_nvis = 0;
       if (n <= 0) return sync_scalars();
       DevState S = dev_state();
       const double half = gam * (double)d / 2.0;
       const int nb = (n + 255) / 256;
       k_mesh_keys<<<nb, 256, 0, st>>>(S, lid, gam, half, d, !test, c.mkeys, c.mvals, c.ckey, c.scal + S_NBIG);
       NCG_LAUNCHED();
-      NCG_TRY(radix_sort_pairs(c.mkeys, c.mvals, n, 32, st));
-      NCG_CK(cudaMemsetAsync(c.mkeys + n, 0xff, sizeof(uint32_t), st));
-      k_cell_heads<<<nb, 256, 0, st>>>(c.mkeys, n, c.cstart, c.scal + S_NINS);
-      NCG_LAUNCHED();
+      NCG_TRY(mesh_table(n));
       c.mesh_valid = 1;
       c.mesh_n = n;
-      k_mesh_count<<<nb, 256, 0, st>>>(c.ckey, c.mkeys, c.mvals, c.cstart, lid, d, (long long)c.cell_cap, c.mcnt);
-      NCG_LAUNCHED();
-      NCG_TRY(scan_exclusive(c.mcnt, c.moff, n, c.cnt, st));
-      int h[S_COUNT];
-      int total = 0;
-      NCG_CK(cudaMemcpyAsync(&total, c.moff + n, sizeof(int), cudaMemcpyDeviceToHost, st));
-      NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
-      NCG_CK(cudaStreamSynchronize(st));
-      if (test && h[S_NBIG] > 0) return NCGPU_E_UNSUPPORTED;  // bodies larger than the mesh size
-      if ((long)total > c.pair_cap) return NCGPU_E_CAPACITY;
-      c.n_cand = total;
-      k_mesh_write<<<nb, 256, 0, st>>>(S, c.ckey, c.mkeys, c.mvals, c.cstart, c.moff, lid, d, (long long)c.cell_cap,
-                                       c.dt, test, c.cand_k,
-                                       c.cand_p, c.cflag, c.hi, c.hit_cap, c.scal + S_NHITS, c.err);
-      NCG_LAUNCHED();
-      int nh = 0;
-      NCG_CK(cudaMemcpyAsync(&nh, c.scal + S_NHITS, sizeof(int), cudaMemcpyDeviceToHost, st));
-      NCG_CK(cudaStreamSynchronize(st));
-      if (nh > c.hit_cap) return NCGPU_E_CAPACITY;
-      if (nh > 0) {
-            NCG_CK(cudaMemcpyAsync(c.keys, c.hi, sizeof(int) * (size_t)nh, cudaMemcpyDeviceToDevice, st));
-            NCG_CK(cudaMemsetAsync(c.vals, 0, sizeof(int) * (size_t)nh, st));
-            NCG_TRY(radix_sort_pairs(c.keys, c.vals, nh, 31, st));
-            MeshEvArgs E{lid, d, c.P.par_collision_type, c.P.par_one_collision_only_bool, c.P.par_mesh_bool, c.ev_cap, c.n_max,
-                         c.occ_cap, n, (long long)c.cell_cap, c.dt, c.P.par_collision_parameter,
-                         c.P.par_mutual_bool, c.xpair_cap, FragArgs{}};
-            if (E.type == NCGPU_COLLISION_FRAGMENTATION && !make_frag_args(c, E.frag)) return NCGPU_E_ARG;
-            MeshFragBufs X{c.evx, c.xpairs, c.xhead, c.fev};
-            k_mesh_events<<<1, MEV, 0, st>>>(S, c.cand_k, c.cand_p, c.cflag, c.moff, c.ckey, c.mkeys, c.mvals,
-                                             c.cstart, (const int *)c.keys, nh, E, c.ev, c.evrec, c.dirty, c.occ,
-                                             c.scal + S_NDROP, X, c.err);
-            NCG_LAUNCHED();
-            k_count_dropped<<<(total + 255) / 256, 256, 0, st>>>(c.cflag, total, c.scal + S_NDROP);
-            NCG_LAUNCHED();
+      int nbig = 0;
+      NCG_TRY(read_scal(S_NBIG, &nbig));
+      MeshEvArgs E{lid, d, c.P.par_collision_type, c.P.par_one_collision_only_bool, c.P.par_mesh_bool, c.ev_cap,
+                   c.n_max, c.occ_cap, n, (long long)c.cell_cap, c.dt, c.P.par_collision_parameter,
+                   c.P.par_mutual_bool, c.xpair_cap, FragArgs{}, lid + 1};
+      if (test && E.type == NCGPU_COLLISION_FRAGMENTATION && !make_frag_args(c, E.frag)) return NCGPU_E_ARG;
+      long base = 0, small_total = 0;
+      int ev_clean = 0;  // events whose dirty marks are cleared
+      auto clear_dirty = [&](int nev) -> int {
+            const int hi = min(nev, c.ev_cap);
+            if (hi > ev_clean) {
+                  k_clear_dirty_events<<<(hi - ev_clean + 255) / 256, 256, 0, st>>>(c.dirty, c.ev + 3 * (size_t)ev_clean,
+                                                                                  hi - ev_clean);
+                  NCG_LAUNCHED();
+                  ev_clean = hi;
+            }
+            return NCGPU_OK;
+      };
+      if (!test || nbig == 0) {
+            int tot = 0;
+            NCG_TRY(mesh_segment(S, lid, 0, lid + 1, 0, test, E, &tot));
+            base = small_total = tot;
+      } else {
+            int s = 0;
+            bool rekey = false;
+            for (;;) {
+                  int e = 0x7fffffff;
+                  NCG_CK(cudaMemcpyAsync(c.n_dev, &e, sizeof(int), cudaMemcpyHostToDevice, st));
+                  k_next_big<<<(lid - s + 256) / 256, 256, 0, st>>>(S, s, lid, gam, c.n_dev);
+                  NCG_LAUNCHED();
+                  NCG_CK(cudaMemcpyAsync(&e, c.n_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+                  NCG_CK(cudaStreamSynchronize(st));
+                  const int hi = e == 0x7fffffff ? lid + 1 : e;
+                  if (hi > s) {
+                        if (rekey) {
+                              k_cell_clear<<<nb, 256, 0, st>>>(c.mkeys, n, c.cstart);
+                              NCG_LAUNCHED();
+                              k_mesh_rekey<<<nb, 256, 0, st>>>(S, s, lid, gam, half, d, c.mkeys, c.mvals, c.ckey);
+                              NCG_LAUNCHED();
+                              NCG_TRY(mesh_table(n));
+                              rekey = false;
+                        }
+                        int tot = 0;
+                        NCG_TRY(mesh_segment(S, lid, s, hi, base, test, E, &tot));
+                        base += tot;
+                        small_total += tot;
+                        int nev = 0;
+                        NCG_TRY(read_scal(S_NEV, &nev));
+                        NCG_TRY(clear_dirty(nev));
+                  }
+                  if (e == 0x7fffffff) break;
+                  int nev0 = 0, nev1 = 0, cnt = 0;
+                  NCG_TRY(read_scal(S_NEV, &nev0));
+                  MeshFragBufs X{c.evx, c.xpairs, c.xhead, c.fev};
+                  k_big_visit<<<1, BVT, 0, st>>>(S, e, gam, (int)base, c.pair_cap, E, c.cand_k, c.cand_p, c.cflag,
+                                                 c.ev, c.evrec, X, c.n_dev, c.err);
+                  NCG_LAUNCHED();
+                  NCG_CK(cudaMemcpyAsync(&cnt, c.n_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+                  NCG_TRY(read_scal(S_NEV, &nev1));
+                  if (c.mesh_nvis < MAX_VISITS) {
+                        c.vis_host[3 * c.mesh_nvis] = e;
+                        c.vis_host[3 * c.mesh_nvis + 1] = (int)base;
+                        c.vis_host[3 * c.mesh_nvis + 2] = (int)base + cnt;
+                  }
+                  c.mesh_nvis++;
+                  base += cnt;
+                  if (base > c.pair_cap) return NCGPU_E_CAPACITY;
+                  rekey = rekey || nev1 > nev0;
+                  s = e + 1;
+                  if (s > lid) break;
+            }
+            if (c.mesh_nvis > MAX_VISITS) return NCGPU_E_CAPACITY;
+            if (c.mesh_nvis > 0)
+                  NCG_CK(cudaMemcpyAsync(c.vis, c.vis_host, sizeof(int) * 3 * (size_t)c.mesh_nvis,
+                                         cudaMemcpyHostToDevice, st));
       }
+      int h[S_COUNT];
       NCG_TRY(sync_scalars());
       NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
       NCG_CK(cudaStreamSynchronize(st));
-      if (c.n_events > 0) {
-            k_clear_dirty_events<<<(c.n_events + 255) / 256, 256, 0, st>>>(c.dirty, c.ev, min(c.n_events, c.ev_cap));
-            NCG_LAUNCHED();
-      }
+      NCG_TRY(clear_dirty(c.n_events));
+      c.n_cand = (int)base;
       c.mesh_nev = min(c.n_events, c.ev_cap);
       c.mesh_nfev = h[S_NFEV];
       c.mesh_nx = h[S_NXPAIRS];
-      c.total_neighbours = (long)total - h[S_NDROP];
-      c.n_pairs = c.P.par_mutual_bool ? total - h[S_NDROP] - h[S_NSKIP] + h[S_NXPAIRS] : 0;
-      c.how_many_big = h[S_NBIG];
+      c.total_neighbours = small_total - h[S_NDROP];
+      c.n_pairs = c.P.par_mutual_bool ? (int)(base - h[S_NDROP] - h[S_NSKIP] + h[S_NXPAIRS]) : 0;
+      c.how_many_big = test ? c.mesh_nvis : 0;
       return NCGPU_OK;
 }
 

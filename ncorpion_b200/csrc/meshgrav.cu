@@ -227,7 +227,23 @@ struct MGArgs {
       int nt;                   // N_tilde
       int nfev;                 // full fragmentations of the pass
       const int *evx, *fev, *xhead;
+      int nvis;                 // visits of bodies larger than the mesh size
+      const int *vis;           // (body, first, end) candidate positions, in visit order
+      const int *cp;            // candidate partners (a visit's list ascends)
 };
+
+// Whether b is in the candidate list cp[lo, hi) (ascending).
+__device__ __forceinline__ bool in_list(const int *__restrict__ cp, int lo, int hi, int b)
+{
+      while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            const int v = cp[mid];
+            if (v < b) lo = mid + 1;
+            else if (v > b) hi = mid;
+            else return true;
+      }
+      return false;
+}
 
 // The tail fragments of full fragmentation e (EVX record): slots
 // fid0 .. fid0 + nt - 1.  Adds, in pairs[] order, the terms of the largest
@@ -301,49 +317,73 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
             }
       }
       const int L = (have_cells && b <= A.lid0) ? ckey[b] : -1;
-      if (A.mutual && L >= 0) {
+      if (A.mutual && have_cells) {
             // full fragmentations whose largest fragment is b: their tail pairs
-            // follow the event's own candidate in b's sequence
+            // follow the event's own candidate (k, p) in b's sequence
             int xe = A.xhead ? A.xhead[b] : -1;
-            // own pops: cells 26..0, lower indices ascending
-            int cur[27];
-            for (int l = 26; l >= 0; --l) {
-                  long long cell = L + g_noff(l, A.d);
-                  cur[l] = -1;
-                  if (cell < 0 || cell >= A.cell_cap) continue;
-                  int s = cstart[cell];
-                  if (s < 0) continue;
-                  int q = s;
-                  for (; keys[q] == (uint32_t)cell; ++q) {
-                        int p = vals[q];
-                        if (p >= b) break;
-                        if (p > 2 && S.ex[p]) pair_add(S, b, p, A.G, A.sp, A.soft, a_x, a_y, a_z);
-                        while (xe >= 0 && A.evx[(size_t)EVX * xe + 6] == b && A.evx[(size_t)EVX * xe + 7] == p) {
-                              tail_terms(S, A, xe, b, b, a_x, a_y, a_z);
-                              xe = A.evx[(size_t)EVX * xe + 5];
-                        }
-                  }
-                  cur[l] = (keys[q] == (uint32_t)cell) ? q : -1;  // first higher index, if any
-            }
-            // later bodies that found b, ascending index: 27-way merge
-            for (;;) {
-                  int best = 0x7fffffff, bl = -1;
-                  for (int l = 0; l < 27; ++l) {
-                        int q = cur[l];
-                        if (q < 0) continue;
-                        int v = vals[q];
-                        if (v < best) { best = v; bl = l; }
-                  }
-                  if (bl < 0) break;
-                  if (best > 2 && best != b && S.ex[best]) pair_add(S, b, best, A.G, A.sp, A.soft, a_x, a_y, a_z);
-                  while (xe >= 0 && A.evx[(size_t)EVX * xe + 6] == best && A.evx[(size_t)EVX * xe + 7] == b) {
+            auto anchor = [&](int k, int p) {
+                  while (xe >= 0 && A.evx[(size_t)EVX * xe + 6] == k && A.evx[(size_t)EVX * xe + 7] == p) {
                         tail_terms(S, A, xe, b, b, a_x, a_y, a_z);
                         xe = A.evx[(size_t)EVX * xe + 5];
                   }
-                  long long cell = L + g_noff(bl, A.d);
-                  int q = cur[bl] + 1;
-                  cur[bl] = (keys[q] == (uint32_t)cell) ? q : -1;
+            };
+            // a big body's visit that listed b (pairs[] holds (e, b) at e's turn)
+            auto visit_term = [&](int v) {
+                  const int e = A.vis[3 * v];
+                  if (!in_list(A.cp, A.vis[3 * v + 1], A.vis[3 * v + 2], b)) return;
+                  if (e > 2 && S.ex[e]) pair_add(S, b, e, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                  anchor(e, b);
+            };
+            // visits of big bodies before b
+            int vi = 0;
+            for (; vi < A.nvis && A.vis[3 * vi] < b; ++vi) visit_term(vi);
+            // b's own visit (b larger than the mesh size) replaces its pops
+            if (vi < A.nvis && A.vis[3 * vi] == b) {
+                  for (int r = A.vis[3 * vi + 1]; r < A.vis[3 * vi + 2]; ++r) {
+                        const int p = A.cp[r];
+                        if (p > 2 && S.ex[p]) pair_add(S, b, p, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                        anchor(b, p);
+                  }
+                  ++vi;
             }
+            if (L >= 0) {
+                  // own pops: cells 26..0, lower indices ascending
+                  int cur[27];
+                  for (int l = 26; l >= 0; --l) {
+                        long long cell = L + g_noff(l, A.d);
+                        cur[l] = -1;
+                        if (cell < 0 || cell >= A.cell_cap) continue;
+                        int s = cstart[cell];
+                        if (s < 0) continue;
+                        int q = s;
+                        for (; keys[q] == (uint32_t)cell; ++q) {
+                              int p = vals[q];
+                              if (p >= b) break;
+                              if (p > 2 && S.ex[p]) pair_add(S, b, p, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                              anchor(b, p);
+                        }
+                        cur[l] = (keys[q] == (uint32_t)cell) ? q : -1;  // first higher index, if any
+                  }
+                  // later bodies that found b, ascending index: 27-way merge, with
+                  // the later big bodies' visits in index order
+                  for (;;) {
+                        int best = 0x7fffffff, bl = -1;
+                        for (int l = 0; l < 27; ++l) {
+                              int q = cur[l];
+                              if (q < 0) continue;
+                              int v = vals[q];
+                              if (v < best) { best = v; bl = l; }
+                        }
+                        for (; vi < A.nvis && A.vis[3 * vi] < best; ++vi) visit_term(vi);
+                        if (bl < 0) break;
+                        if (best > 2 && best != b && S.ex[best]) pair_add(S, b, best, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                        anchor(best, b);
+                        long long cell = L + g_noff(bl, A.d);
+                        int q = cur[bl] + 1;
+                        cur[bl] = (keys[q] == (uint32_t)cell) ? q : -1;
+                  }
+            }
+            for (; vi < A.nvis; ++vi) visit_term(vi);
             for (; xe >= 0; xe = A.evx[(size_t)EVX * xe + 5]) tail_terms(S, A, xe, b, b, a_x, a_y, a_z);
       }
       ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
@@ -515,7 +555,7 @@ int mesh_gravity_state(const double *cm8)
                c.P.par_softening_parameter != 0., (long long)c.cell_cap, c.P.par_G, c.P.par_softening_parameter,
                c.P.par_G * cm8[6], cm8[0], cm8[1], cm8[2],
                c.mesh_valid ? c.mesh_n - 1 : -1, c.P.par_N_tilde, c.mesh_nfev, c.evx, c.fev,
-               c.mesh_nfev > 0 ? c.xhead : nullptr};
+               c.mesh_nfev > 0 ? c.xhead : nullptr, c.mesh_valid ? c.mesh_nvis : 0, c.vis, c.cand_p};
       double *ax = c.acc, *ay = c.acc + N, *az = c.acc + 2 * N;
       if (lid >= 0) {
             k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.cstart, c.mesh_valid, ax,

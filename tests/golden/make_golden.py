@@ -154,6 +154,44 @@ def frag_mesh_case(profile, n, seed, gam, dt, N_tilde, pq):
     return out
 
 
+def big_disk(n, seed):
+    """Mesh disk with six bodies larger than the mesh size (two at slots 1, 2,
+    the others anywhere) among radii U[2e-3, 6e-3], 2% holes."""
+    rng = np.random.default_rng(seed)
+    b = disks.mesh_disk(n, seed=seed)
+    b[:, 7] = rng.uniform(2e-3, 6e-3, n)
+    big = rng.choice(n, 6, replace=False)
+    big[:2] = [1, 2]
+    b[big, 7] = rng.uniform(0.012, 0.03, len(big))
+    b[:, 6] = 4.0 / 3.0 * np.pi * 3.0 * b[:, 7] ** 3
+    ex = np.ones(n, np.int32)
+    ex[rng.choice(n, n // 50, replace=False)] = 0
+    ex[big] = 1
+    return b, ex
+
+
+def mesh_big_case(profile, n, seed, gam, dt):
+    """three_largest + one mesh() call with bodies larger than the mesh size
+    (the big-body branch, src/collision.c:380-410)."""
+    b, ex = big_disk(n, seed)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm, dt=dt, gam=gam)
+    ref.lib.orc_events_reset()
+    ref.lib.orc_frag_counts_reset()
+    idx = np.zeros(3, np.int32)
+    ref.lib.orc_three_largest(idx.ctypes.data_as(oracle.P))
+    ref.lib.orc_mesh()
+    pairs = ref.pairs()
+    b2, ex2, cm2, sc = ref.get_state()
+    out = dict(bodies=b, exists=ex, cm=cm, dt=np.float64(dt), gam=np.float64(gam), three=idx,
+               events=ref.events(), counts=ref.fragment_counts(), n_pairs=np.int64(len(pairs)),
+               pairs_digest=digest(pairs), total_neighbours=np.int64(ref.lib.orc_total_neighbours()),
+               out_digest=digest(b2), out_exists_digest=digest(ex2), out_largest_id=np.int64(b2.shape[0] - 1))
+    ref.lib.orc_mesh_reset()
+    return out
+
+
 OUTPUT_FILES = ["stat.txt", "collision.txt", "mass.txt", "radius.txt", "x.txt", "y.txt", "z.txt", "vx.txt",
                 "vy.txt", "vz.txt", "readme.txt"]
 
@@ -201,6 +239,10 @@ def main(names=None):
     out["frag_bf"] = frag_bf_case("bf_frag", 4000, 0, 0.02)
     out["frag_mesh15"] = frag_mesh_case("mesh_frag_s", 4000, 0, 0.01, 0.02, 15, (-1, 3, -1, 1))
     out["frag_mesh4"] = frag_mesh_case("mesh_frag4_s", 4000, 1, 0.01, 0.02, 4, (0, 1, 0, 1))
+    # bodies larger than the mesh size, three of them past slot 2
+    out["mesh_big_merge"] = mesh_big_case("mesh_merge_s", 10000, 100, 0.01, 5e-3)
+    out["mesh_big_inelastic"] = mesh_big_case("mesh_inelastic_s", 10000, 101, 0.01, 5e-3)
+    out["mesh_big_frag"] = mesh_big_case("mesh_frag_s", 10000, 102, 0.01, 5e-3)
     for k, v in out.items():
         if names and k not in names:
             continue

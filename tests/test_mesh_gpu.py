@@ -172,13 +172,74 @@ def test_mesh_steps_with_gamma_updates(gpu):
     assert np.array_equal(cmg, cm_ref)
 
 
-def test_big_bodies_rejected(gpu):
+@pytest.mark.parametrize("name,ctype", [("mesh_big_merge", 2), ("mesh_big_inelastic", 1), ("mesh_big_frag", 3)])
+def test_mesh_pass_big_bodies(gpu, name, ctype):
+    """Bodies larger than the mesh size (src/collision.c:380-410), three of
+    them past slot 2: their visits list every smaller body and every later big
+    one, collisions with them are resolved at their turn, and the bodies after
+    a visit are queried from their state at their own turn.  The fixtures also
+    hold bodies that collide twice in one pass (merged into, then merged away).
+    Then the kick: mesh gravity over pairs[] with the big bodies' pairs."""
+    g = golden(name)
+    p = mesh_params(ctype)
+    api = gpu(16384, p)
+    api.upload(g["bodies"], g["exists"], g["cm"])
+    api.set_timestep(float(g["dt"]))
+    assert np.array_equal(api.three_largest(), g["three"])
+    n_pairs, n_ev, tn = api.mesh(float(g["gam"]), True)
+    assert np.array_equal(api.events(), g["events"])
+    pairs = api.pairs()
+    assert n_pairs == int(g["n_pairs"]) == len(pairs)
+    assert np.array_equal(_digest(pairs), g["pairs_digest"])
+    assert tn == int(g["total_neighbours"])
+    b, ex, cm = api.download(16384)
+    assert b.shape[0] - 1 == int(g["out_largest_id"])
+    w = oracle.PortWorld(16384, p)
+    if ctype == 3:
+        w.set_fragmentation()
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=float(g["dt"]), gam=float(g["gam"]))
+    w.three_largest()
+    w.lib.orc_w_mesh()
+    b_ref, ex_ref, _ = w.get_state()
+    assert np.array_equal(_digest(b_ref), g["out_digest"])
+    live = ex_ref == 1
+    if ctype == 3:
+        assert np.array_equal(ex, ex_ref)
+        np.testing.assert_allclose(b[live], b_ref[live], rtol=1e-11, atol=0)
+    else:
+        assert_state_equal(b, ex, b_ref, ex_ref)
+    api.kick()
+    w.lib.orc_w_kick_mesh()
+    b1, _, _ = api.download(16384)
+    r1, _, _ = w.get_state()
+    if ctype == 3:
+        np.testing.assert_allclose(b1[live][:, 3:6], r1[live][:, 3:6], rtol=1e-10, atol=0)
+    else:
+        assert np.array_equal(b1[live][:, 3:6], r1[live][:, 3:6])
+
+
+def test_mesh_steps_big_bodies(gpu):
+    """Four iterations of the mesh loop (mergers) with bodies larger than the
+    mesh size, gamma updated on the host."""
     from ncorpion_b200 import api as A
-    b, ex = collisional_disk(1000, seed=3, holes=False)
-    b[10, 7] = 0.5  # larger than the mesh size
-    api = gpu(2048, mesh_params(2))
-    api.upload(b, ex, np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0]))
+    g = golden("mesh_big_merge")
+    p = mesh_params(2)
+    api = gpu(16384, p)
+    api.upload(g["bodies"], g["exists"], g["cm"])
     api.set_timestep(5e-4)
-    with pytest.raises(A.NcgpuError) as e:
-        api.mesh(0.03, True)
-    assert e.value.status == A.E_UNSUPPORTED
+    w = oracle.PortWorld(16384, p)
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=5e-4, gam=0.01)
+    gam_g = gam_w = 0.01
+    gmin = 4.4 / 256
+    for _ in range(4):
+        hm, tn = api.step_mesh(gam_g)
+        gam_g = A.update_gamma(gam_g, tn, hm, 16.0, gmin)
+        w.lib.orc_w_set_gam(C.c_double(gam_w))
+        tn_w = w.lib.orc_w_step_mesh()
+        hm_w = int(w.get_state()[1].sum())
+        gam_w = A.update_gamma(gam_w, tn_w, hm_w, 16.0, gmin)
+        assert (hm, tn) == (hm_w, tn_w)
+    bg, exg, cmg = api.download(16384)
+    b_ref, ex_ref, cm_ref = w.get_state()
+    assert_state_equal(bg, exg, b_ref, ex_ref)
+    assert np.array_equal(cmg, cm_ref)

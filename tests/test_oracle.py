@@ -158,3 +158,24 @@ def test_port_fragmentation_mesh_matches_golden(name):
     assert np.array_equal(_digest(b), g["out_digest"]) and np.array_equal(_digest(ex), g["out_exists_digest"])
     assert np.array_equal(cm, g["out_cm"])
     w.lib.orc_w_mesh_reset()
+
+
+@pytest.mark.parametrize("name,ctype", [("mesh_big_merge", 2), ("mesh_big_inelastic", 1), ("mesh_big_frag", 3)])
+def test_port_mesh_big_bodies_matches_golden(name, ctype):
+    """The big-body branch of mesh() (src/collision.c:380-410)."""
+    g = golden(name)
+    p = make_params(mesh_bool=1, brute_force_bool=0, collision_bool=1, collision_type=ctype,
+                    collision_parameter=1.5, collision_cube_cells=256)
+    w = oracle.PortWorld(16384, p)
+    if ctype == 3:
+        w.set_fragmentation()
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=float(g["dt"]), gam=float(g["gam"]))
+    assert np.array_equal(w.three_largest(), g["three"])
+    w.lib.orc_w_mesh()
+    pairs = w.pairs()
+    assert len(pairs) == int(g["n_pairs"]) and np.array_equal(_digest(pairs), g["pairs_digest"])
+    assert w.lib.orc_w_total_neighbours() == int(g["total_neighbours"])
+    assert np.array_equal(w.events(), g["events"])
+    b, ex, cm = w.get_state()
+    assert np.array_equal(_digest(b), g["out_digest"]) and np.array_equal(_digest(ex), g["out_exists_digest"])
+    w.lib.orc_w_mesh_reset()
