@@ -34,6 +34,9 @@ sys.path.insert(0, ROOT)
 N_BODIES = 65536
 SOFTENING = 0.5
 FLOP_PER_INTERACTION = 20  # 3 sub, 3 FMA (r^2+eps^2), rsqrt (2), 3 mul, 3 FMA accumulate
+# DRAM bytes (read + write) of one k_grav_tiled<mixed> launch at N=65,536, from one ncu capture of
+# this script's gravity workload (profiles/k_grav_tiled_mixed_n65536.txt): 4.0 MB read + 62.2 MB written.
+MIXED_DRAM_BYTES = 66.24e6
 METRIC = "Pair-interactions/s mixed vs FP64 (rel err<1e-6); mesh collision steps/s at N=1M"
 WORKLOAD = ("gravity-only single-step accelerations, N=65,536 disk (a~U[0.8,1.2], e~Rayleigh 0.01, "
             "i~Rayleigh 0.005), masses log-uniform [1e-9,1e-6], R=1e-5, softening 0.5*(R_k+R_p)")
@@ -502,7 +505,9 @@ def main(argv=None):
                        "l2": "flushed between timed steps (256 MiB write outside the events)",
                        "parallelism": "replicas" if ws > 1 else "single GPU"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-                         "frac": achieved / fp32_peak, "traffic": None,
+                         "frac": achieved / fp32_peak, "traffic": MIXED_DRAM_BYTES,
+                         "traffic_note": "bytes per launch from ncu (dram__bytes_read.sum + dram__bytes_write.sum); "
+                                         "algorithmic input 2.6 MB, the rest is the per-chunk partial sums",
                          "kernel": "k_grav_tiled<mixed>", "kernel_ms": kms_mixed,
                          "flop_per_interaction": FLOP_PER_INTERACTION,
                          "peak_source": "measured in this run: best of the scalar FFMA and packed f32x2 FMA "

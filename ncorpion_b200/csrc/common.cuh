@@ -126,6 +126,7 @@ struct Ctx {
       int *msums = nullptr;        // scan scratch for candidate-sized scans
       long pair_cap = 0;
       int *occ = nullptr;
+      void *mrec = nullptr;        // cell-ordered body records of a mesh pass (64 B each, n_max)
       int occ_cap = 0;
       // fragmentation in a mesh pass: per-event records (EVX ints: candidate
       // position, extra-pair offset, extra-pair count, first tail fragment,

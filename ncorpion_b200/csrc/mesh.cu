@@ -87,7 +87,21 @@ __global__ void k_cell_clear(const uint32_t *__restrict__ keys, int n, int *__re
 
 // number of candidates of body k (lo <= k < hi): existing bodies of lower
 // index in its 27 cells; 0 outside [lo, hi)
-__global__ void k_mesh_count(const int *__restrict__ ex, const int *__restrict__ ckey,
+// Cell-ordered copy of the fields the pass reads: record q is body vals[q].
+__global__ void k_mesh_records(const DevState S, const int *__restrict__ vals, int n, MRec *__restrict__ rec)
+{
+      int q = blockIdx.x * blockDim.x + threadIdx.x;
+      if (q >= n) return;
+      const int b = vals[q];
+      MRec r;
+      r.x = S.x[b]; r.y = S.y[b]; r.z = S.z[b]; r.R = S.R[b];
+      r.vx = S.vx[b]; r.vy = S.vy[b]; r.vz = S.vz[b];
+      r.ex = S.ex[b];
+      r.did = S.did[b];
+      rec[q] = r;
+}
+
+__global__ void k_mesh_count(const MRec *__restrict__ rec, const int *__restrict__ ckey,
                              const uint32_t *__restrict__ keys, const int *__restrict__ vals,
                              const int *__restrict__ cstart, int lid, int lo, int hi, int d, long long cap,
                              int *__restrict__ cnt)
@@ -108,7 +122,7 @@ __global__ void k_mesh_count(const int *__restrict__ ex, const int *__restrict__
                   for (int q = s; keys[q] == (uint32_t)cell; ++q) {
                         const int p = vals[q];
                         if (p >= k) break;
-                        if (ex[p]) c++;  // a body removed earlier in the pass is not pushed
+                        if (rec[q].ex) c++;  // a body removed earlier in the pass is not pushed
                   }
             }
       }
@@ -116,7 +130,8 @@ __global__ void k_mesh_count(const int *__restrict__ ex, const int *__restrict__
 }
 
 // candidates of body k in pop order; hit flag from the entry-state predicate
-__global__ void k_mesh_write(DevState S, const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
+__global__ void k_mesh_write(const MRec *__restrict__ rec, const int *__restrict__ ckey,
+                             const uint32_t *__restrict__ keys,
                              const int *__restrict__ vals, const int *__restrict__ cstart,
                              const int *__restrict__ off, int lid, int lo, int hi, int d, long long cap, double dt,
                              int test, int *__restrict__ ck, int *__restrict__ cp, unsigned char *__restrict__ cflag,
@@ -129,7 +144,8 @@ __global__ void k_mesh_write(DevState S, const int *__restrict__ ckey, const uin
       int L = ckey[k];
       if (L < 0) return;
       int pos = off[k];
-      const bool dk = test && S.did[k];
+      const MRec rk = rec[t];
+      const bool dk = test && rk.did;
       for (int l = 26; l >= 0; --l) {
             long long cell = L + d_noff(l, d);
             if (cell < 0 || cell >= cap) continue;
@@ -138,11 +154,12 @@ __global__ void k_mesh_write(DevState S, const int *__restrict__ ckey, const uin
             for (int q = s; keys[q] == (uint32_t)cell; ++q) {
                   int p = vals[q];
                   if (p >= k) break;
-                  if (!S.ex[p]) continue;
+                  const MRec rp = rec[q];
+                  if (!rp.ex) continue;
                   ck[pos] = k;
                   cp[pos] = p;
                   unsigned char f = 0;
-                  if (test && !dk && !S.did[p] && d_approach(S, p, k, dt, nullptr)) {
+                  if (test && !dk && !rp.did && d_contact_rec(rp, rk, dt)) {  // closest_approach(p, k)
                         f = 1;
                         int h = atomicAdd(nhits, 1);
                         if (h < hit_cap) hitpos[h] = pos;
@@ -598,6 +615,7 @@ static int mesh_alloc(int d)
             NCG_CK(cudaMemsetAsync(c.xhead, 0xff, sizeof(int) * N, c.s));
             NCG_CK(cudaMalloc(&c.fev, sizeof(int) * (size_t)c.ev_cap));
             NCG_CK(cudaMalloc(&c.vis, sizeof(int) * 3 * (size_t)MAX_VISITS));
+            NCG_CK(cudaMalloc(&c.mrec, sizeof(MRec) * N));
       }
       return NCGPU_OK;
 }
@@ -606,7 +624,7 @@ void mesh_free()
 {
       Ctx &c = ctx();
       void *ptrs[] = {c.cstart, c.mkeys, c.mvals, c.ckey, c.mcnt, c.moff, c.cand_k, c.cand_p, c.cflag, c.cpos,
-                      c.occ, c.msums, c.evx, c.xpairs, c.xhead, c.fev, c.vis};
+                      c.occ, c.msums, c.evx, c.xpairs, c.xhead, c.fev, c.vis, c.mrec};
       for (void *p : ptrs)
             if (p) cudaFree(p);
 }
@@ -653,7 +671,10 @@ static int mesh_segment(const DevState &S, int lid, int lo, int hi, long base, i
       const int n = lid + 1;
       const int nb = (n + 255) / 256;
       const int d = c.P.par_collision_cube_cells;
-      k_mesh_count<<<nb, 256, 0, st>>>(c.ex, c.ckey, c.mkeys, c.mvals, c.cstart, lid, lo, hi, d,
+      MRec *rec = (MRec *)c.mrec;
+      k_mesh_records<<<nb, 256, 0, st>>>(S, c.mvals, n, rec);
+      NCG_LAUNCHED();
+      k_mesh_count<<<nb, 256, 0, st>>>(rec, c.ckey, c.mkeys, c.mvals, c.cstart, lid, lo, hi, d,
                                        (long long)c.cell_cap, c.mcnt);
       NCG_LAUNCHED();
       NCG_TRY(scan_exclusive(c.mcnt, c.moff, n, c.cnt, st));
@@ -669,7 +690,7 @@ static int mesh_segment(const DevState &S, int lid, int lo, int hi, long base, i
       if ((long)end > c.pair_cap) return NCGPU_E_CAPACITY;
       *tot = (int)total;
       if (total == 0) return NCGPU_OK;
-      k_mesh_write<<<nb, 256, 0, st>>>(S, c.ckey, c.mkeys, c.mvals, c.cstart, c.moff, lid, lo, hi, d,
+      k_mesh_write<<<nb, 256, 0, st>>>(rec, c.ckey, c.mkeys, c.mvals, c.cstart, c.moff, lid, lo, hi, d,
                                        (long long)c.cell_cap, c.dt, test, c.cand_k, c.cand_p, c.cflag, c.hi, c.hit_cap,
                                        c.scal + S_NHITS, c.err);
       NCG_LAUNCHED();

@@ -201,6 +201,44 @@ __device__ __forceinline__ void pair_add(const DevState &S, int b, int o, double
       az = DADD(az, DDIV(DMUL(g, dz), D3));
 }
 
+// A body's gravity fields in a cell-ordered copy (64 bytes), read by the walk
+// instead of gathering each field from the state arrays.
+struct GRec {
+      double x, y, z, m, R, pad0, pad1;
+      int ex, pad2;
+};
+
+__global__ void k_grav_records(const DevState S, const int *__restrict__ vals, int n, GRec *__restrict__ rec)
+{
+      int q = blockIdx.x * blockDim.x + threadIdx.x;
+      if (q >= n) return;
+      const int b = vals[q];
+      GRec r;
+      r.x = S.x[b]; r.y = S.y[b]; r.z = S.z[b]; r.m = S.m[b]; r.R = S.R[b];
+      r.pad0 = r.pad1 = 0.;
+      r.ex = S.ex[b];
+      r.pad2 = 0;
+      rec[q] = r;
+}
+
+// pair_add with the partner's fields from its record (same operations)
+__device__ __forceinline__ void pair_add_rec(double xb, double yb, double zb, double Rb, const GRec &o, double G,
+                                             double sp, bool soft, double &ax, double &ay, double &az)
+{
+      double dx = DSUB(o.x, xb), dy = DSUB(o.y, yb), dz = DSUB(o.z, zb);
+      double r2 = DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz));
+      if (soft) {
+            double s = DMUL(sp, DADD(Rb, o.R));
+            r2 = DADD(r2, DMUL(s, s));
+      }
+      double D = __dsqrt_rn(r2);
+      double D3 = DMUL(DMUL(D, D), D);
+      double g = DMUL(G, o.m);
+      ax = DADD(ax, DDIV(DMUL(g, dx), D3));
+      ay = DADD(ay, DDIV(DMUL(g, dy), D3));
+      az = DADD(az, DDIV(DMUL(g, dz), D3));
+}
+
 // The term body b adds to body i (0..2) in the k > 2 loop: G*mk*DX/D3 with
 // DX = X_b - X_i (src/physics.c:216-257).
 __device__ __forceinline__ void big_term(const DevState &S, int b, int i, double G, double sp, bool soft, double *t)
@@ -264,8 +302,8 @@ __device__ __forceinline__ void tail_terms(const DevState &S, const MGArgs &A, i
 // terms for bodies 0..2 and CM_acc go to `terms` (12 blocks of n_max).
 __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
                             const int *__restrict__ vals, const int *__restrict__ cstart, int have_cells,
-                            double *__restrict__ ax, double *__restrict__ ay, double *__restrict__ az,
-                            double *__restrict__ terms, long N)
+                            const GRec *__restrict__ grec, double *__restrict__ ax, double *__restrict__ ay,
+                            double *__restrict__ az, double *__restrict__ terms, long N)
 {
       // bodies of the cell table in cell order (neighbouring threads share cells
       // and partners), then the bodies appended after the pass
@@ -347,6 +385,7 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                   ++vi;
             }
             if (L >= 0) {
+                  const double xb = S.x[b], yb = S.y[b], zb = S.z[b], Rb = S.R[b];
                   // own pops: cells 26..0, lower indices ascending
                   int cur[27];
                   for (int l = 26; l >= 0; --l) {
@@ -359,7 +398,7 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                         for (; keys[q] == (uint32_t)cell; ++q) {
                               int p = vals[q];
                               if (p >= b) break;
-                              if (p > 2 && S.ex[p]) pair_add(S, b, p, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                              if (p > 2 && grec[q].ex) pair_add_rec(xb, yb, zb, Rb, grec[q], A.G, A.sp, A.soft, a_x, a_y, a_z);
                               anchor(b, p);
                         }
                         cur[l] = (keys[q] == (uint32_t)cell) ? q : -1;  // first higher index, if any
@@ -376,7 +415,9 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                         }
                         for (; vi < A.nvis && A.vis[3 * vi] < best; ++vi) visit_term(vi);
                         if (bl < 0) break;
-                        if (best > 2 && best != b && S.ex[best]) pair_add(S, b, best, A.G, A.sp, A.soft, a_x, a_y, a_z);
+                        const int qb = cur[bl];
+                        if (best > 2 && best != b && grec[qb].ex)
+                              pair_add_rec(xb, yb, zb, Rb, grec[qb], A.G, A.sp, A.soft, a_x, a_y, a_z);
                         anchor(best, b);
                         long long cell = L + g_noff(bl, A.d);
                         int q = cur[bl] + 1;
@@ -558,8 +599,13 @@ int mesh_gravity_state(const double *cm8)
                c.mesh_nfev > 0 ? c.xhead : nullptr, c.mesh_valid ? c.mesh_nvis : 0, c.vis, c.cand_p};
       double *ax = c.acc, *ay = c.acc + N, *az = c.acc + 2 * N;
       if (lid >= 0) {
-            k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.cstart, c.mesh_valid, ax,
-                                                          ay, az, c.partial, N);
+            GRec *grec = (GRec *)c.mrec;
+            if (c.mesh_valid) {
+                  k_grav_records<<<(c.mesh_n + 255) / 256, 256, 0, st>>>(S, c.mvals, c.mesh_n, grec);
+                  NCG_LAUNCHED();
+            }
+            k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.cstart, c.mesh_valid, grec,
+                                                          ax, ay, az, c.partial, N);
             NCG_LAUNCHED();
       }
       double *tot = c.red + 3584;

@@ -31,15 +31,12 @@ struct Approach {
       double p[6];    // approach[]: heavier body's position first
 };
 
-// closest_approach(a, b): 1 when a and b collide within dt.
-__device__ __forceinline__ bool d_approach(const DevState &S, int a, int b, double dt, Approach *ap)
+// The collision test of closest_approach on the two bodies' values: true
+// when they collide within dt, with *t the time of contact (src/collision.c:101-160).
+__device__ __forceinline__ bool d_contact(double xa, double ya, double za, double vx_a, double vy_a, double vz_a,
+                                          double R_a, double xb, double yb, double zb, double vx_b, double vy_b,
+                                          double vz_b, double R_b, double dt, double *t_out)
 {
-      if (!(S.ex[a] && S.ex[b])) return false;
-      double R_a = S.R[a], R_b = S.R[b];
-      double vx_a = S.vx[a], vy_a = S.vy[a], vz_a = S.vz[a];
-      double vx_b = S.vx[b], vy_b = S.vy[b], vz_b = S.vz[b];
-      double xa = S.x[a], ya = S.y[a], za = S.z[a];
-      double xb = S.x[b], yb = S.y[b], zb = S.z[b];
       double dx = DSUB(xa, xb), dy = DSUB(ya, yb), dz = DSUB(za, zb);
       double dvx = DSUB(vx_a, vx_b), dvy = DSUB(vy_a, vy_b), dvz = DSUB(vz_a, vz_b);
       double dr_dot_dv = DADD(DADD(DMUL(dx, dvx), DMUL(dy, dvy)), DMUL(dz, dvz));
@@ -51,6 +48,20 @@ __device__ __forceinline__ bool d_approach(const DevState &S, int a, int b, doub
       if (disc <= 0.0) return false;
       double t = DDIV(-DADD(dr_dot_dv, __dsqrt_rn(disc)), dv2);
       if (t > dt) return false;
+      *t_out = t;
+      return true;
+}
+
+// closest_approach(a, b): 1 when a and b collide within dt.
+__device__ __forceinline__ bool d_approach(const DevState &S, int a, int b, double dt, Approach *ap)
+{
+      if (!(S.ex[a] && S.ex[b])) return false;
+      double vx_a = S.vx[a], vy_a = S.vy[a], vz_a = S.vz[a];
+      double vx_b = S.vx[b], vy_b = S.vy[b], vz_b = S.vz[b];
+      double xa = S.x[a], ya = S.y[a], za = S.z[a];
+      double xb = S.x[b], yb = S.y[b], zb = S.z[b];
+      double t;
+      if (!d_contact(xa, ya, za, vx_a, vy_a, vz_a, S.R[a], xb, yb, zb, vx_b, vy_b, vz_b, S.R[b], dt, &t)) return false;
       if (ap) {
             ap->t = t;
             xa = DADD(xa, DMUL(t, vx_a)); ya = DADD(ya, DMUL(t, vy_a)); za = DADD(za, DMUL(t, vz_a));
@@ -62,6 +73,19 @@ __device__ __forceinline__ bool d_approach(const DevState &S, int a, int b, doub
             }
       }
       return true;
+}
+
+// One body's fields in a cell-ordered copy (64 bytes): the mesh pass reads
+// partners from it instead of gathering each field from the state arrays.
+struct MRec {
+      double x, y, z, R, vx, vy, vz;
+      int ex, did;
+};
+
+__device__ __forceinline__ bool d_contact_rec(const MRec &a, const MRec &b, double dt)
+{
+      double t;
+      return a.ex && b.ex && d_contact(a.x, a.y, a.z, a.vx, a.vy, a.vz, a.R, b.x, b.y, b.z, b.vx, b.vy, b.vz, b.R, dt, &t);
 }
 
 // x^(1/3.) with the double exponent y = 1.0/3.0, correctly rounded.

@@ -117,6 +117,10 @@ PROFILES = {
     "mesh_frag4_s": dict(MESH, collision_bool="1", fragmentation_bool="1", collision_cube_cells="256",
                          N_tilde="4", pq_min_max="{0,1,0,1}", N_max="70000", N_0="20000",
                          t_end="0.005", time_step="0.0005"),
+    # whole-program run of the mesh driver: 20,000 bodies, 100 steps, outputs every 25 steps
+    "mesh_prog": dict(MESH, collision_bool="1", instant_merger_bool="1", collision_cube_cells="256",
+                      N_max="30000", N_0="20000", t_end="0.05", time_step="0.0005", output_step="25",
+                      write_to_files_bool="1", write_cartesian_bool="1", write_collisions_bool="1"),
     # the N = 1,048,576 mesh workload: 1024 cells per side (8.6 GB hash table)
     "mesh_merge_1m": dict(MESH, collision_bool="1", instant_merger_bool="1",
                           collision_cube_cells="1024", N_max="1100000", N_0="1048576",

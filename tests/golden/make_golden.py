@@ -235,6 +235,8 @@ def main(names=None):
     out["mesh_inelastic"] = mesh_case("mesh_inelastic_s", 6000, 22, 0.03, 5e-4)
     # the N = 2,000 collisional disk, 200 steps, output every 50 steps
     out["program_bf_merge"] = program_run_case("bf_merge", disks.bf_collide_disk(2000, seed=0))
+    # the mesh driver: 20,000 bodies with four larger than the mesh size, 100 steps
+    out["program_mesh_merge"] = program_run_case("mesh_prog", big_disk(20000, 7)[0])
     # fragmentation: every outcome in one sweep (dt = 0.02 on the crowded ring)
     out["frag_bf"] = frag_bf_case("bf_frag", 4000, 0, 0.02)
     out["frag_mesh15"] = frag_mesh_case("mesh_frag_s", 4000, 0, 0.01, 0.02, 15, (-1, 3, -1, 1))

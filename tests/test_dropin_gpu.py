@@ -1,8 +1,14 @@
-"""GPU: the drop-in build.  The reference program with its brute-force
-integration taken from ncorpion_b200/host/rk4_gpu.c on libncgpu.so
-(oracle/_ref/bf_merge/ncorpion_gpu, see oracle/ref_build.py) runs the
-N = 2,000 collisional disk for 200 steps (instant mergers, outputs every 50
-steps); every output file (positions, velocities, masses, radii, stat.txt,
+"""GPU: the drop-in build.  The reference program with its integration
+drivers taken from ncorpion_b200/host/rk4_gpu.c on libncgpu.so
+(oracle/_ref/<profile>/ncorpion_gpu, see oracle/ref_build.py):
+
+- brute force (bf_merge): the N = 2,000 collisional disk for 200 steps
+  (instant mergers, outputs every 50 steps);
+- mesh (mesh_prog): a 20,000-body disk with bodies larger than the mesh size,
+  100 steps (mesh search with mergers, mesh gravity, adaptive mesh size,
+  outputs every 25 steps).
+
+Every output file (positions, velocities, masses, radii, stat.txt,
 collision.txt, readme.txt) and the console output must be byte-identical to
 the reference program's own run (golden digests).
 """
@@ -17,7 +23,7 @@ from conftest import ROOT, golden
 
 pytestmark = pytest.mark.gpu
 
-EXE = os.path.join(ROOT, "oracle", "_ref", "bf_merge", "ncorpion_gpu")
+PROGRAMS = [("bf_merge", "program_bf_merge"), ("mesh_prog", "program_mesh_merge")]
 
 
 def _digest(b):
@@ -25,16 +31,19 @@ def _digest(b):
     return np.frombuffer(hashlib.sha256(b).digest(), np.uint8)
 
 
-@pytest.mark.skipif(not os.path.exists(EXE), reason="drop-in build not present (needs the reference sources)")
-def test_dropin_program_matches_reference_outputs(lib):
+@pytest.mark.parametrize("profile,fixture", PROGRAMS)
+def test_dropin_program_matches_reference_outputs(lib, profile, fixture):
+    exe = os.path.join(ROOT, "oracle", "_ref", profile, "ncorpion_gpu")
+    if not os.path.exists(exe):
+        pytest.skip("drop-in build not present (needs the reference sources)")
     import sys
     sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
     from make_golden import OUTPUT_FILES, filtered_stdout
     from ncorpion_b200 import disks
-    g = golden("program_bf_merge")
+    g = golden(fixture)
     d = tempfile.mkdtemp(prefix="ncgpu_dropin_")
     disks.write_init_txt(os.path.join(d, "init.txt"), g["bodies"])
-    r = subprocess.run([EXE], cwd=d, capture_output=True, text=True, timeout=600)
+    r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     bad = []
     for f in OUTPUT_FILES:
