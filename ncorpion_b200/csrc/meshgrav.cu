@@ -122,6 +122,21 @@ __device__ void move_body(const DevState &S, int dst, int src)
 __global__ void k_top3_final(const DevState S, const int *__restrict__ first3, const double *__restrict__ partR,
                              const int *__restrict__ parti, int nparts, int mesh_bool, int *__restrict__ out)
 {
+      // later bodies' top three: the block partials folded by the warp (the order
+      // (radius desc, slot asc) is total, so any folding order gives the same three)
+      Top3 rest;
+      for (int q = 0; q < 3; q++) { rest.R[q] = 0.; rest.i[q] = -1; }
+      for (int b = threadIdx.x; b < nparts; b += 32)
+            for (int q = 0; q < 3; q++) t3_insert(rest, partR[3 * b + q], parti[3 * b + q]);
+      for (int o = 16; o > 0; o >>= 1) {
+            double oR[3];
+            int oi[3];
+            for (int q = 0; q < 3; q++) {
+                  oR[q] = __shfl_down_sync(0xffffffffu, rest.R[q], o);
+                  oi[q] = __shfl_down_sync(0xffffffffu, rest.i[q], o);
+            }
+            for (int q = 0; q < 3; q++) t3_insert(rest, oR[q], oi[q]);
+      }
       if (threadIdx.x != 0) return;
       int e0 = first3[0], e1 = first3[1], e2 = first3[2];
       int t[3] = {-1, -1, -1};
@@ -140,10 +155,6 @@ __global__ void k_top3_final(const DevState S, const int *__restrict__ first3, c
             else { t[2] = t[1]; t[1] = t[0]; t[0] = e2; R = R2; R2 = R1; R1 = R0; R0 = R; }
       }
       // later bodies, strictly-larger insertion in (radius desc, slot asc) order
-      Top3 rest;
-      for (int q = 0; q < 3; q++) { rest.R[q] = 0.; rest.i[q] = -1; }
-      for (int b = 0; b < nparts; b++)
-            for (int q = 0; q < 3; q++) t3_insert(rest, partR[3 * b + q], parti[3 * b + q]);
       for (int q = 0; q < 3; q++) {
             int j = rest.i[q];
             if (j < 0 || e2 < 0) continue;
@@ -329,14 +340,26 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
             return;
       }
       if (A.mutual) {
+            const double xb = S.x[b], yb = S.y[b], zb = S.z[b], Rb = S.R[b], mb = S.m[b];
             for (int i = 0; i < 3; i++) {
                   if (!S.ex[i]) continue;
-                  pair_add(S, b, i, A.G, A.sp, A.soft, a_x, a_y, a_z);
-                  double t[3];
-                  big_term(S, b, i, A.G, A.sp, A.soft, t);
-                  terms[(3 * i) * N + b] = t[0];
-                  terms[(3 * i + 1) * N + b] = t[1];
-                  terms[(3 * i + 2) * N + b] = t[2];
+                  // pair_add(b, i) and big_term(b, i) share D^3 (the squared
+                  // differences and the softening are the same numbers)
+                  double dx = DSUB(S.x[i], xb), dy = DSUB(S.y[i], yb), dz = DSUB(S.z[i], zb);
+                  double r2 = DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz));
+                  if (A.soft) {
+                        double sft = DMUL(A.sp, DADD(Rb, S.R[i]));
+                        r2 = DADD(r2, DMUL(sft, sft));
+                  }
+                  const double D = __dsqrt_rn(r2);
+                  const double D3 = DMUL(DMUL(D, D), D);
+                  const double gi = DMUL(A.G, S.m[i]), gb = DMUL(A.G, mb);
+                  a_x = DADD(a_x, DDIV(DMUL(gi, dx), D3));
+                  a_y = DADD(a_y, DDIV(DMUL(gi, dy), D3));
+                  a_z = DADD(a_z, DDIV(DMUL(gi, dz), D3));
+                  terms[(3 * i) * N + b] = DDIV(DMUL(gb, DSUB(xb, S.x[i])), D3);
+                  terms[(3 * i + 1) * N + b] = DDIV(DMUL(gb, DSUB(yb, S.y[i])), D3);
+                  terms[(3 * i + 2) * N + b] = DDIV(DMUL(gb, DSUB(zb, S.z[i])), D3);
             }
       }
       if (A.mutual && have_cells && b > A.lid0) {
