@@ -297,6 +297,80 @@ def bench_fragment(lib, api, torch, mode, steps):
             "energy_drift_rel": float((e1[0] - e0[0]) / abs(e0[0])), "gpu_launches": launches}
 
 
+BF_N, BF_STEPS, BF_DT = 2000, 200, 1e-3
+ADJ_N, ADJ_STEPS = 16384, 100
+
+
+def bench_bf_collide(lib, api, torch, cpu_ref):
+    """C1: brute-force gravity (exact FP64) + brute-force collision search with
+    instant mergers on the N=2,000 disk, 200 integrator steps on the device;
+    beside it the reference's own loop (oracle/_ref/bf_merge) for the same steps."""
+    from ncorpion_b200 import disks
+    b = disks.bf_collide_disk(BF_N, seed=0)
+    ex = np.ones(BF_N, np.int32)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    p = api.default_params(G=1.0, softening_parameter=0.0, collision_bool=1, brute_force_bool=1, mesh_bool=0,
+                           collision_type=api.COLLISION_MERGER, gravity_mode=api.GRAVITY_EXACT,
+                           disruption_threshold=0.1, high_dumping_threshold=100.0)
+    api.init(4096, p)
+    api.upload(b, ex, cm)
+    api.set_timestep(BF_DT)
+    for _ in range(3):
+        api.step_brute_force()
+    api.upload(b, ex, cm)
+    st = torch.cuda.ExternalStream(lib.ncgpu_stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(BF_STEPS):
+        hm = api.step_brute_force()
+    e1.record(st)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    api.finalize()
+    out = {"metric": "brute-force collisional steps/s at N=2,000", "steps_per_s": BF_STEPS / t,
+           "ms_per_step": 1e3 * t / BF_STEPS, "bodies_end": int(hm),
+           "workload": "N=2,000 disk (a~U[0.8,1.2], e~Rayleigh 0.01, i~Rayleigh 0.005), equal masses (1e-3 in "
+                       "all), R=2e-3, instant mergers, exact FP64 gravity, dt=1e-3, 200 steps", "cpu_baseline": None}
+    if cpu_ref:
+        import oracle
+        if oracle.ref_available("bf_merge"):
+            ref = oracle.Ref("bf_merge")
+            ref.set_state(b, ex, cm, dt=BF_DT)
+            t0 = time.perf_counter()
+            for _ in range(BF_STEPS):
+                ref.lib.orc_step_brute_force()
+            dt = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": BF_STEPS / dt, "unit": "steps/s", "cores": 1, "kind": "reference",
+                                   "sample": f"the same 200 steps, reference loop (gcc -O2), {dt:.1f} s, 1 thread"}
+    return out
+
+
+def bench_adjoint(lib, api, torch):
+    """C4: forward + adjoint of the differentiable leapfrog (ncgpu_leapfrog_vjp:
+    forward with checkpoints every 32 steps, then the reverse sweep with
+    recomputation) at N=16,384 for 100 steps; CUDA events on the library stream."""
+    from ncorpion_b200 import disks
+    b, cm = disks.reduce_to_com(disks.adjoint_disk(ADJ_N, 0), np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0]))
+    api.init(ADJ_N, api.default_params(G=1.0, softening_parameter=0.5, collision_bool=0))
+    adj = np.random.default_rng(0).normal(size=(ADJ_N, 3))
+    args = (b[:, :3], b[:, 3:6], b[:, 6], b[:, 7], cm, 1e-3, ADJ_STEPS, adj)
+    api.leapfrog_vjp(*args)
+    st = torch.cuda.ExternalStream(lib.ncgpu_stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    api.leapfrog_vjp(*args)
+    e1.record(st)
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / 1e3
+    api.finalize()
+    return {"metric": "forward+adjoint leapfrog steps/s at N=16,384", "steps_per_s": ADJ_STEPS / t,
+            "ms_per_step": 1e3 * t / ADJ_STEPS, "checkpoint": 32,
+            "workload": "gravity-only disk, N=16,384, log-uniform masses, R=1e-2, softening 0.5 (R_k+R_p), dt=1e-3, "
+                        "100 steps: forward with checkpoints, reverse sweep with recomputation (FP64)"}
+
+
 def mesh_cpu_reference(nsteps=3):
     """The reference's mesh() + mesh gravity loop (oracle/_ref/mesh_merge_1m,
     1 thread, 8.6 GB hash table) for a few steps of the same disk."""
@@ -326,6 +400,8 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mesh", action="store_true")
     ap.add_argument("--no-frag", action="store_true")
+    ap.add_argument("--no-bf", action="store_true", help="skip the N=2,000 brute-force collisional section")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint section")
     ap.add_argument("--mesh-n", type=int, default=MESH_N, help="mesh workload bodies (smaller cases for profiling)")
     ap.add_argument("--mesh-cells", type=int, default=1024)
     ap.add_argument("--mesh-steps", type=int, default=MESH_STEPS)
@@ -473,6 +549,8 @@ def main(argv=None):
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
                 "cpu_baseline": mesh_cpu_reference() if (rank == 0 and ws == 1 and not a.no_cpu_baseline
                                                          and a.mesh_n == MESH_N) else None}
+    bf = None if a.no_bf else bench_bf_collide(lib, api, torch, rank == 0 and ws == 1 and not a.no_cpu_baseline)
+    adjoint = None if a.no_adjoint else bench_adjoint(lib, api, torch)
     frag = None
     if not a.no_frag:
         fm = bench_fragment(lib, api, torch, api.GRAVITY_MIXED, FRAG_STEPS)
@@ -528,6 +606,8 @@ def main(argv=None):
             "speedup_mixed_vs_fp64_tiled": ms_fp64t / ms_mixed,
             "mesh": mesh,
             "fragment": frag,
+            "brute_force_collisional": bf,
+            "adjoint": adjoint,
             "accuracy": {"mutual_rel_err_max": float(rel_mut.max()),
                          "mutual_rel_err_median": float(np.median(rel_mut)),
                          "total_rel_err_max": float(rel_tot.max()),
