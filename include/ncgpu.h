@@ -176,6 +176,12 @@ int ncgpu_probe_fp32_peak(double *tflops);
    from independent dependency chains: scalar FFMA and packed f32x2 FMA in
    TFLOP/s (2 flops per FMA lane), and rsqrt.approx.f32 in Gop/s. */
 int ncgpu_probe_fp32_rates(double *ffma_tflops, double *ffma2_tflops, double *rsqrt_gops);
+/* Diagnostic (no reference counterpart): a kernel waits on a barrier that
+   nothing completes, giving up after `probes` failed probes (1 .. 2^20, the
+   library's limit for every device wait), as every bounded wait here does.
+   Returns NCGPU_E_TIMEOUT with the cycles one failed probe took; the library
+   stays usable.  Tests the timeout path without hanging a GPU. */
+int ncgpu_probe_wait_timeout(int probes, double *cycles_per_probe);
 
 /* Diagnostic: out[i] = x[i]^(1.0/3.0), correctly rounded, as the device
    merger computes the merged radius (src/physics.c:684). */

@@ -105,6 +105,7 @@ EXPORTS = {
     "ncgpu_host_unregister": (C.c_int, [P]),
     "ncgpu_probe_fp32_peak": (C.c_int, [P]),
     "ncgpu_probe_fp32_rates": (C.c_int, [P, P, P]),
+    "ncgpu_probe_wait_timeout": (C.c_int, [C.c_int, P]),
     "ncgpu_last_kernel_ms": (C.c_int, [P]),
     "ncgpu_collide_brute": (C.c_int, [P]),
     "ncgpu_fragment_counts": (C.c_int, [P]),

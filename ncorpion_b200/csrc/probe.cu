@@ -3,6 +3,7 @@
 // warps per SM to saturate each pipe.  The measured rates are the denominators
 // of the FP32 gravity kernel's roofline fractions.
 #include "common.cuh"
+#include "bulk.cuh"
 
 namespace ncg {
 namespace {
@@ -61,6 +62,23 @@ __global__ void __launch_bounds__(256) k_rsqrt_probe(float *out, float b)
       float s = 0.f;
       for (int k = 0; k < 8; k++) s += r[k];
       if (s == 123.456f) out[0] = s;
+}
+
+// One thread waits on an mbarrier that nothing will complete, for at most
+// `probes` failed try_waits (the primitive of every bounded wait here), then
+// records the timeout in the error word as the real kernels do, with the
+// cycles the wait took.
+__global__ void k_timeout_probe(int probes, unsigned *err, long long *cycles)
+{
+      __shared__ uint64_t bar;
+      if (threadIdx.x != 0) return;
+      mbar_init(&bar, 1);
+      mbar_fence_init();
+      const long long t0 = clock64();
+      bool ok = false;
+      for (int it = 0; it < probes && !ok; ++it) ok = mbar_try_wait(&bar, 0);
+      *cycles = clock64() - t0;
+      if (!ok) atomicOr(err, ERR_TIMEOUT);
 }
 
 }  // namespace
@@ -151,4 +169,20 @@ extern "C" int ncgpu_probe_fp32_peak(double *tflops)
       double flops = 2.0 * 8.0 * PROBE_ITERS * (double)blocks * 256.0;
       *tflops = flops / (best * 1e-3) / 1e12;
       return NCGPU_OK;
+}
+
+extern "C" int ncgpu_probe_wait_timeout(int probes, double *cycles_per_probe)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited) return NCGPU_E_STATE;
+      if (probes < 1 || probes > WAIT_LIMIT || !cycles_per_probe) return NCGPU_E_ARG;
+      long long *cyc = (long long *)c.n_dev;  // 8 spare bytes of the library's scratch ints
+      k_timeout_probe<<<1, 32, 0, c.s>>>(probes, c.err, cyc);
+      NCG_LAUNCHED();
+      long long h = 0;
+      NCG_CK(cudaMemcpyAsync(&h, cyc, sizeof h, cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaStreamSynchronize(c.s));
+      *cycles_per_probe = (double)h / probes;
+      return check_err_word();
 }
