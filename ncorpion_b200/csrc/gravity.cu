@@ -537,9 +537,10 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
       const float eps2f = (float)eps2;
       const double *bi = box + ib * 6;
       // all radii equal: eps = 2 softening R for every pair (the loads of R skip)
+      // (SOFT 1: the host found all radii equal and passes eps^2 = (2 sp R)^2)
       const bool uni = SOFT == 2 && rrange[0] == rrange[1];
       const double eu = 2.0 * sp * rrange[0];
-      const float eps2u = (float)(eu * eu);
+      const float eps2u = SOFT == 1 ? (float)eps2 : (float)(eu * eu);
 
       double a0[3] = {0., 0., 0.}, a1[3] = {0., 0., 0.};
 
@@ -602,7 +603,7 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
                         const float *tl = f4[b];
                         const float *tr = fr[b];
                         if (SOFT == 0) far_tile<0>(tl, tr, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
-                        else if (uni) far_tile<1>(tl, tr, x0, y0, z0, x1, y1, z1, r0f, r1f, eps2u, a0, a1);
+                        else if (SOFT == 1 || uni) far_tile<1>(tl, tr, x0, y0, z0, x1, y1, z1, r0f, r1f, eps2u, a0, a1);
                         else far_tile<2>(tl, tr, x0, y0, z0, x1, y1, z1, r0f, r1f, 0.f, a0, a1);
                   }
             }
@@ -788,6 +789,19 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       nchunks = (ntiles + tpc - 1) / tpc;
       NCG_TRY(ensure_partial((size_t)nchunks * 3 * npad));
       double eps2 = 0.;
+      int soft_kind = sm;
+      if (sm == 2) {
+            // all radii equal (the bounding-box pass found R_min == R_max): the
+            // uniform-epsilon instance, with fewer registers
+            double rr[2];
+            NCG_CK(cudaMemcpyAsync(rr, c.red + 6, sizeof rr, cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaStreamSynchronize(st));
+            if (rr[0] == rr[1]) {
+                  const double eu = 2.0 * sp * rr[0];
+                  eps2 = eu * eu;
+                  soft_kind = 1;
+            }
+      }
       double theta = P.par_near_theta > 0. ? P.par_near_theta : 0.25;
       dim3 grid(nchunks, ntiles);
       const float *s32 = (const float *)c.src32;
@@ -796,9 +810,9 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       k_grav_tiled<MODE_, SOFT_><<<grid, MXB, 0, st>>>(s64, c.srcR, s32, c.srcR32, c.tilebox, n, ntiles, tpc, \
                                                       theta, eps2, c.partial, npad, c.err, c.red + 6, sp)
       if (mode == NCGPU_GRAVITY_MIXED) {
-            if (sm == 0) NCG_TILED(0, 0); else NCG_TILED(0, 2);
+            if (soft_kind == 0) NCG_TILED(0, 0); else if (soft_kind == 1) NCG_TILED(0, 1); else NCG_TILED(0, 2);
       } else {
-            if (sm == 0) NCG_TILED(1, 0); else NCG_TILED(1, 2);
+            if (soft_kind == 0) NCG_TILED(1, 0); else if (soft_kind == 1) NCG_TILED(1, 1); else NCG_TILED(1, 2);
       }
 #undef NCG_TILED
       NCG_LAUNCHED();
