@@ -77,7 +77,7 @@ struct ncgpu_params {
       int par_gravity_mode;              /* NCGPU_GRAVITY_*                          */
       double par_near_theta;             /* MIXED: tile pairs whose boxes are closer
                                         than near_theta x the larger box diagonal
-                                        are summed in FP64 (default 0.25 if <= 0) */
+                                        are summed in FP64 (default 0.15 if <= 0) */
       double par_disruption_threshold;   /* disruption_threshold (dump into the CM)  */
       double par_high_dumping_threshold; /* high_dumping_threshold (dump, unbound)   */
       int par_reduce_to_COM_bool;        /* reduce_to_COM_bool                       */

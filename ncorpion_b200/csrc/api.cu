@@ -210,7 +210,7 @@ void ncgpu_default_params(struct ncgpu_params *p)
       p->par_collision_cube_min = 80.;
       p->par_switch_to_brute_force = 110;
       p->par_gravity_mode = NCGPU_GRAVITY_EXACT;
-      p->par_near_theta = 0.25;
+      p->par_near_theta = 0.15;
       p->par_disruption_threshold = 1.8;     // src/parameters.h:150
       p->par_high_dumping_threshold = 230.95;  // src/parameters.h:177
       p->par_reduce_to_COM_bool = 1;

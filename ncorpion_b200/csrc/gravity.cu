@@ -802,7 +802,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
                   soft_kind = 1;
             }
       }
-      double theta = P.par_near_theta > 0. ? P.par_near_theta : 0.25;
+      double theta = P.par_near_theta > 0. ? P.par_near_theta : 0.15;
       dim3 grid(nchunks, ntiles);
       const float *s32 = (const float *)c.src32;
       NCG_CK(cudaEventRecord(c.kev0, st));
