@@ -321,7 +321,12 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
       const int t = blockIdx.x * blockDim.x + threadIdx.x;
       if (t > A.lid) return;
       const int b = (have_cells && t <= A.lid0) ? vals[t] : t;
-      if (!S.ex[b]) return;
+      if (!S.ex[b]) {
+            // an empty slot adds +0.0 to every chain (they then read all terms
+            // without looking at exists[])
+            for (int w = 0; w < 12; w++) terms[(size_t)w * N + b] = 0.;
+            return;
+      }
       double a_x = 0., a_y = 0., a_z = 0.;
       if (A.central) {
             double DX = DSUB(S.x[b], A.cmx), DY = DSUB(S.y[b], A.cmy), DZ = DSUB(S.z[b], A.cmz);
@@ -487,7 +492,7 @@ __global__ void __launch_bounds__(384) k_mesh_chains(DevState S, MGArgs A, const
 #pragma unroll
             for (int u = 0; u < CHB / 32; u++) {
                   const int k = k0 + u * 32 + lane;
-                  v[u] = (k < n && S.ex[k]) ? t[k] : 0.;
+                  v[u] = k < n ? t[k] : 0.;
             }
             for (int base = k0; base < n; base += CHB) {
 #pragma unroll
@@ -496,7 +501,7 @@ __global__ void __launch_bounds__(384) k_mesh_chains(DevState S, MGArgs A, const
 #pragma unroll
                   for (int u = 0; u < CHB / 32; u++) {  // next block in flight during the sums
                         const int k = base + CHB + u * 32 + lane;
-                        v[u] = (k < n && S.ex[k]) ? t[k] : 0.;
+                        v[u] = k < n ? t[k] : 0.;
                   }
                   if (lane == 0) {
                         const int m = min(CHB, n - base);
