@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(384) k_mesh_chains(DevState S, MGArgs A, const
                                                      const double *__restrict__ ax, const double *__restrict__ ay,
                                                      const double *__restrict__ az, double *__restrict__ tot)
 {
-      __shared__ double stage[12][CHB];
+      __shared__ __align__(16) double stage[12][CHB];
       const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       double s = chain_init(w, ax, ay, az);
       if (chain_live(w, S, A)) {
@@ -505,8 +505,17 @@ __global__ void __launch_bounds__(384) k_mesh_chains(DevState S, MGArgs A, const
                   }
                   if (lane == 0) {
                         const int m = min(CHB, n - base);
-#pragma unroll 8
-                        for (int q = 0; q < m; q++) s = DADD(s, stage[w][q]);
+                        if (m == CHB) {  // full block: fixed trip count, two terms per shared load
+                              const double2 *st2 = reinterpret_cast<const double2 *>(stage[w]);
+#pragma unroll 16
+                              for (int q = 0; q < CHB / 2; q++) {
+                                    const double2 pr = st2[q];
+                                    s = DADD(s, pr.x);
+                                    s = DADD(s, pr.y);
+                              }
+                        } else {
+                              for (int q = 0; q < m; q++) s = DADD(s, stage[w][q]);
+                        }
                   }
                   __syncwarp();
             }
