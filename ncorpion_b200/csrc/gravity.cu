@@ -155,22 +155,49 @@ __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, 
 
 // CM_acc += G*mk*DX/r3 in slot order (src/physics.c:137-139): one thread per
 // component, sequential, so the FP64 result matches the reference bit for bit.
-__global__ void k_seq_sum3(const double *__restrict__ cterm, int n, double *__restrict__ out)
+// Sequential FP64 sums of the 3 arrays cterm[c*n .. c*n + n), in index order
+// (CM_acc of the exact mode).  One warp per array: the warp stages CHS terms at
+// a time in shared memory with coalesced loads, the next block loading while
+// lane 0 adds, so the dependent adds do not wait on global memory.
+constexpr int CHS = 512;
+__global__ void __launch_bounds__(96) k_seq_sum3(const double *__restrict__ cterm, int n, double *__restrict__ out)
 {
-      int c = threadIdx.x;
-      if (c >= 3) return;
-      const double *t = cterm + (size_t)c * n;
+      __shared__ __align__(16) double stage[3][CHS];
+      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const double *t = cterm + (size_t)w * n;
       double s = 0.;
-      int i = 0;
-      for (; i + 4 <= n; i += 4) {
-            double t0 = t[i], t1 = t[i + 1], t2 = t[i + 2], t3 = t[i + 3];
-            s = __dadd_rn(s, t0);
-            s = __dadd_rn(s, t1);
-            s = __dadd_rn(s, t2);
-            s = __dadd_rn(s, t3);
+      double v[CHS / 32];
+#pragma unroll
+      for (int u = 0; u < CHS / 32; u++) {
+            const int k = u * 32 + lane;
+            v[u] = k < n ? t[k] : 0.;
       }
-      for (; i < n; ++i) s = __dadd_rn(s, t[i]);
-      out[c] = s;
+      for (int base = 0; base < n; base += CHS) {
+#pragma unroll
+            for (int u = 0; u < CHS / 32; u++) stage[w][u * 32 + lane] = v[u];
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < CHS / 32; u++) {
+                  const int k = base + CHS + u * 32 + lane;
+                  v[u] = k < n ? t[k] : 0.;
+            }
+            if (lane == 0) {
+                  const int m = min(CHS, n - base);
+                  if (m == CHS) {
+                        const double2 *st2 = reinterpret_cast<const double2 *>(stage[w]);
+#pragma unroll 16
+                        for (int q = 0; q < CHS / 2; q++) {
+                              const double2 pr = st2[q];
+                              s = __dadd_rn(s, pr.x);
+                              s = __dadd_rn(s, pr.y);
+                        }
+                  } else {
+                        for (int q = 0; q < m; q++) s = __dadd_rn(s, stage[w][q]);
+                  }
+            }
+            __syncwarp();
+      }
+      if (lane == 0) out[w] = s;
 }
 
 // ------------------------------------------------------------ tiled modes --
@@ -742,7 +769,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
             NCG_CK(cudaEventRecord(c.kev1, st));
             c.kev_valid = 1;
             if (central) {
-                  k_seq_sum3<<<1, 32, 0, st>>>(c.cmterm, n, d_cm_acc);
+                  k_seq_sum3<<<1, 96, 0, st>>>(c.cmterm, n, d_cm_acc);
             } else {
                   k_set3<<<1, 1, 0, st>>>(d_cm_acc, 0., 0., 0.);
             }
@@ -872,7 +899,7 @@ int gravity_exact_into(const BodyView &bv, int largest_id, const double *cmh, do
                                                     central, ax, ay, az, cterm, err);
       NCG_LAUNCHED();
       if (central) {
-            k_seq_sum3<<<1, 32, 0, st>>>(cterm, n, d_cm_acc);
+            k_seq_sum3<<<1, 96, 0, st>>>(cterm, n, d_cm_acc);
             NCG_LAUNCHED();
       }
       return NCGPU_OK;
