@@ -96,6 +96,17 @@ struct ncgpu_params {
          (pairs[] + the three largest bodies) by the brute-force field of
          par_gravity_mode over every body, keeping the mesh collision search. */
       int par_mesh_brute_gravity;
+      /* the central body's symmetrical equatorial bulge (src/physics.c:149-160),
+         which needs the central mass.  par_J2 is parameters.h's J2_value: a
+         nonzero value is the J2; 0 selects the fluid-body
+         J2 = 0.5*SideralOmega*SideralOmega*R_unit^3/(G*M), re-evaluated from the
+         current central mass M at every force evaluation (src/structure.c:507,
+         src/rk4.c:459-463; M only changes in end_of_timestep).
+         par_sideral_omega is SideralOmega = 2*pi/Tearth. */
+      int par_J2_bool;
+      double par_J2;
+      double par_R_unit;
+      double par_sideral_omega;
 };
 #define NCGPU_MAX_N_TILDE 64
 

@@ -53,6 +53,10 @@ class Params(C.Structure):
         ("merging_threshold", C.c_double),
         ("fragment_threshold", C.c_double),
         ("mesh_brute_gravity", C.c_int),
+        ("J2_bool", C.c_int),
+        ("J2", C.c_double),
+        ("R_unit", C.c_double),
+        ("sideral_omega", C.c_double),
     ]
 
 

@@ -355,6 +355,7 @@ int lf_run(const struct ncgpu_leapfrog_args *a, int mode)
       Ctx &c = ctx();
       const int n = a->n;
       if (n <= 0 || !a->x0 || !a->v0 || !a->m || !a->R || !a->cm || a->nsteps < 0) return NCGPU_E_ARG;
+      if (c.P.par_J2_bool) return NCGPU_E_UNSUPPORTED;  // the J2 term has no derivative kernels
       if (vjp && (!a->adj_x_final || !a->grad_x0 || !a->grad_v0 || !a->grad_m)) return NCGPU_E_ARG;
       if (jvp && (!a->tan_x0 || !a->tan_v0 || !a->tan_m || !a->tan_x_final)) return NCGPU_E_ARG;
       LF L{};

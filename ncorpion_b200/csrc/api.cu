@@ -226,6 +226,10 @@ void ncgpu_default_params(struct ncgpu_params *p)
       p->par_merging_threshold = 0.0002;
       p->par_fragment_threshold = 1.5e-8;
       p->par_mesh_brute_gravity = 0;
+      p->par_J2_bool = 0;
+      p->par_J2 = 0.;
+      p->par_R_unit = 1.;
+      p->par_sideral_omega = 2. * 3.14159265358979323846 / 3.556721809;  /* Tearth's default */
 }
 
 const char *ncgpu_strerror(int s)
@@ -249,10 +253,19 @@ const char *ncgpu_last_error(void) { return g_last_error; }
 int ncgpu_last_launch_count(void) { return launches(); }
 void *ncgpu_stream(void) { return g_ctx.inited ? (void *)g_ctx.s : nullptr; }
 
+// Parameter checks of the reference's own (src/structure.c:1278, 1407-1410)
+// that concern the device path, plus the gravity mode's range.
+static bool params_ok(const struct ncgpu_params *p)
+{
+      if (!p || p->par_gravity_mode < 0 || p->par_gravity_mode > 2) return false;
+      if (p->par_J2_bool != 0 && p->par_J2_bool != 1) return false;
+      if (p->par_J2_bool && !p->par_central_mass_bool) return false;
+      return true;
+}
+
 int ncgpu_init(int n_max, const struct ncgpu_params *params)
 {
-      if (n_max <= 0 || !params) return NCGPU_E_ARG;
-      if (params->par_gravity_mode < 0 || params->par_gravity_mode > 2) return NCGPU_E_ARG;
+      if (n_max <= 0 || !params_ok(params)) return NCGPU_E_ARG;
       if (g_ctx.inited) ncgpu_finalize();
       Ctx &c = g_ctx;
       c.P = *params;
@@ -271,7 +284,7 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
       A(c.ex, N); A(c.exs, N);
       A(c.cm, 8); A(c.cm_acc, 3);
       A(c.acc, 3 * N);
-      A(c.cmterm, 3 * N);
+      A(c.cmterm, 6 * N);
       A(c.cidx, N);
       A(c.cnt, (std::max(N, (size_t)1 << 20) + 1023) / 1024 + 2);
       A(c.n_dev, 8);
@@ -356,7 +369,7 @@ int ncgpu_last_kernel_ms(double *ms)
 int ncgpu_set_params(const struct ncgpu_params *params)
 {
       if (!g_ctx.inited) return NCGPU_E_STATE;
-      if (!params || params->par_gravity_mode < 0 || params->par_gravity_mode > 2) return NCGPU_E_ARG;
+      if (!params_ok(params)) return NCGPU_E_ARG;
       g_ctx.P = *params;
       return NCGPU_OK;
 }

@@ -44,6 +44,45 @@ struct BodyView {
       const int *ex;
 };
 
+// The J2 term of a force evaluation (src/physics.c:149-160): off, or on with
+// R_unit, the J2 in force and the central mass M.
+struct J2Arg {
+      int on;
+      double R, J2, M;
+};
+
+// J2_value when it is nonzero, else the fluid-body J2 of the current central
+// mass M, the expression of src/structure.c:507 and src/rk4.c:462 in its order.
+inline J2Arg j2_arg(const ncgpu_params &P, double M)
+{
+      J2Arg j{P.par_J2_bool && P.par_central_mass_bool, P.par_R_unit, P.par_J2, M};
+      if (j.on && P.par_J2 == 0.)
+            j.J2 = 0.5 * P.par_sideral_omega * P.par_sideral_omega * P.par_R_unit * P.par_R_unit * P.par_R_unit /
+                   (P.par_G * M);
+      return j;
+}
+
+// Adds body k's J2 term to its acceleration a[] and returns CM_acc's share in
+// c[], every operation the reference's in its order with IEEE rounding:
+//   r2 = rk*rk, r5 = r3*r2, K = mu*R*R*J2/r5, q = 7.5/r2*DZ*DZ
+//   a += K*(-1.5*DX + q*DX), K*(-1.5*DY + q*DY), K*(-4.5*DZ + q*DZ)
+//   c  = K*(1.5*DX - q*DX)*mk/M, ... (4.5 for z)
+__device__ __forceinline__ void d_j2(const J2Arg &j, double mu, double DX, double DY, double DZ, double rk,
+                                     double r3, double mk, double &ax, double &ay, double &az, double *c)
+{
+      const double r2 = __dmul_rn(rk, rk);
+      const double r5 = __dmul_rn(r3, r2);
+      const double K = __ddiv_rn(__dmul_rn(__dmul_rn(__dmul_rn(mu, j.R), j.R), j.J2), r5);
+      const double q = __dmul_rn(__dmul_rn(__ddiv_rn(7.5, r2), DZ), DZ);
+      const double qx = __dmul_rn(q, DX), qy = __dmul_rn(q, DY), qz = __dmul_rn(q, DZ);
+      ax = __dadd_rn(ax, __dmul_rn(K, __dadd_rn(__dmul_rn(-1.5, DX), qx)));
+      ay = __dadd_rn(ay, __dmul_rn(K, __dadd_rn(__dmul_rn(-1.5, DY), qy)));
+      az = __dadd_rn(az, __dmul_rn(K, __dadd_rn(__dmul_rn(-4.5, DZ), qz)));
+      c[0] = __ddiv_rn(__dmul_rn(__dmul_rn(K, __dsub_rn(__dmul_rn(1.5, DX), qx)), mk), j.M);
+      c[1] = __ddiv_rn(__dmul_rn(__dmul_rn(K, __dsub_rn(__dmul_rn(1.5, DY), qy)), mk), j.M);
+      c[2] = __ddiv_rn(__dmul_rn(__dmul_rn(K, __dsub_rn(__dmul_rn(4.5, DZ), qz)), mk), j.M);
+}
+
 // Device error word bits (set by kernels instead of trapping).
 enum : unsigned {
       ERR_CAPACITY = 1u,
@@ -76,7 +115,7 @@ struct Ctx {
 
       // gravity scratch
       double *acc = nullptr;       // 3 * n_max (x block, y block, z block)
-      double *cmterm = nullptr;    // 3 * n_max
+      double *cmterm = nullptr;    // 6 * n_max (CM_acc terms; two per body with J2)
       double *partial = nullptr;   // gravity partial sums (chunks x 3 x n_max)
       size_t partial_cap = 0;      // doubles
       int *cidx = nullptr;         // compacted existing slot ids
@@ -213,7 +252,8 @@ int compact_flags_into(const int *flags, int n_slots, int *blockcnt, int *n_dev,
 
 // The exact gravity on caller-provided scratch (no library context).
 int gravity_exact_into(const BodyView &bv, int largest_id, const double *cmh, double G, double sp, int central,
-                       int *cidx, double *src, double *srcR, double *cterm, int *blockcnt, int *n_dev,
-                       unsigned *err, double *ax, double *ay, double *az, double *d_cm_acc, cudaStream_t st);
+                       const J2Arg &j2, int *cidx, double *src, double *srcR, double *cterm, int *blockcnt,
+                       int *n_dev, unsigned *err, double *ax, double *ay, double *az, double *d_cm_acc,
+                       cudaStream_t st);
 
 }  // namespace ncg

@@ -4,6 +4,7 @@
 //
 //   E = sum_k m_k |v_k|^2 / 2 + M |V|^2 / 2                  (kinetic)
 //     - sum_k G M m_k / |r_k - R|                            (central body)
+//     + sum_k m_k G M R_u^2 J2 (3 dz^2 - r^2) / (2 r^5)       (J2, r = r_k - R)
 //     - sum_{k<p} G m_k m_p / sqrt(|r_k - r_p|^2 + eps^2)    (mutual)
 //
 // with eps = softening_parameter (R_k + R_p), the softening of the force
@@ -13,13 +14,14 @@
 #include "common.cuh"
 
 namespace ncg {
+int state_cm_host(double *cm8);
 namespace {
 
 constexpr int EB = 256;
 
 __global__ void __launch_bounds__(EB) k_energy_part(BodyView bv, const int *__restrict__ cidx, int n,
                                                     const double *__restrict__ cm, double G, double sp, int central,
-                                                    int mutual, double *__restrict__ part)
+                                                    int mutual, J2Arg j2, double *__restrict__ part)
 {
       __shared__ double sx[EB], sy[EB], sz[EB], sm[EB], sr[EB];
       __shared__ double red[3][EB];
@@ -35,7 +37,10 @@ __global__ void __launch_bounds__(EB) k_energy_part(BodyView bv, const int *__re
             kin = 0.5 * m * (vx * vx + vy * vy + vz * vz);
             if (central) {
                   const double dx = x - cm[0], dy = y - cm[1], dz = z - cm[2];
-                  pc = -G * cm[6] * m / sqrt(dx * dx + dy * dy + dz * dz);
+                  const double r2 = dx * dx + dy * dy + dz * dz, r = sqrt(r2);
+                  pc = -G * cm[6] * m / r;
+                  if (j2.on)  // the potential whose gradient is the force of src/physics.c:149-160
+                        pc += m * G * cm[6] * j2.R * j2.R * j2.J2 * (3. * dz * dz - r2) / (2. * r2 * r2 * r);
             }
       }
       for (int t0 = 0; mutual && t0 < n; t0 += EB) {
@@ -104,9 +109,12 @@ extern "C" int ncgpu_energy(double *energy)
       const int nb = n > 0 ? (n + EB - 1) / EB : 0;
       NCG_TRY(ensure_partial((size_t)3 * (nb > 0 ? nb : 1) + 4));
       BodyView bv{c.x, c.y, c.z, c.vx, c.vy, c.vz, c.m, c.R, 1, c.ex};
+      double cmh[8] = {0., 0., 0., 0., 0., 0., 1., 0.};  // the J2 in force needs the central mass
+      if (c.P.par_J2_bool) NCG_TRY(state_cm_host(cmh));
       if (nb > 0) {
             k_energy_part<<<nb, EB, 0, st>>>(bv, c.cidx, n, c.cm, c.P.par_G, c.P.par_softening_parameter,
-                                             c.P.par_central_mass_bool, c.P.par_mutual_bool, c.partial);
+                                             c.P.par_central_mass_bool, c.P.par_mutual_bool, j2_arg(c.P, cmh[6]),
+                                             c.partial);
             NCG_LAUNCHED();
       }
       double *out = c.partial + 3 * (size_t)nb;

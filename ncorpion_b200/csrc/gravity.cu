@@ -64,9 +64,9 @@ template <bool SOFT>
 __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, const double *__restrict__ srcR,
                                                     const int *__restrict__ cidx, int n, int ntiles,
                                                     double cmx, double cmy, double cmz, double mu, double sp,
-                                                    int central, double *__restrict__ ax, double *__restrict__ ay,
-                                                    double *__restrict__ az, double *__restrict__ cterm,
-                                                    unsigned *__restrict__ err)
+                                                    int central, J2Arg j2, BodyView bv, double *__restrict__ ax,
+                                                    double *__restrict__ ay, double *__restrict__ az,
+                                                    double *__restrict__ cterm, unsigned *__restrict__ err)
 {
       __shared__ D4 tile[2][T];
       __shared__ alignas(16) double tR[2][T];
@@ -87,9 +87,20 @@ __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, 
             a_x = __ddiv_rn(__dmul_rn(-mu, DX), r3);
             a_y = __ddiv_rn(__dmul_rn(-mu, DY), r3);
             a_z = __ddiv_rn(__dmul_rn(-mu, DZ), r3);
-            cterm[p] = __ddiv_rn(__dmul_rn(me.w, DX), r3);       // G*mk*DX/r3
-            cterm[n + p] = __ddiv_rn(__dmul_rn(me.w, DY), r3);
-            cterm[2 * n + p] = __ddiv_rn(__dmul_rn(me.w, DZ), r3);
+            // CM_acc terms: G*mk*DX/r3, then (with J2) the J2 share, so that
+            // cterm's sequential sum adds them in the reference's order
+            const int f = j2.on ? 2 : 1;
+            const size_t nf = (size_t)f * n;
+            cterm[f * p] = __ddiv_rn(__dmul_rn(me.w, DX), r3);
+            cterm[nf + f * p] = __ddiv_rn(__dmul_rn(me.w, DY), r3);
+            cterm[2 * nf + f * p] = __ddiv_rn(__dmul_rn(me.w, DZ), r3);
+            if (j2.on) {  // src/physics.c:149-160
+                  double cj[3];
+                  d_j2(j2, mu, DX, DY, DZ, rk, r3, bv.m[(long)cidx[p] * bv.stride], a_x, a_y, a_z, cj);
+                  cterm[2 * p + 1] = cj[0];
+                  cterm[nf + 2 * p + 1] = cj[1];
+                  cterm[2 * nf + 2 * p + 1] = cj[2];
+            }
       }
 
       if (tid == 0) {
@@ -653,7 +664,7 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
 // term and scatter back to slot order; per-body CM_acc terms for the reduction.
 __global__ void k_grav_final(const double *__restrict__ partial, int nchunks, long npad, const D4 *__restrict__ s64,
                              const int *__restrict__ slots, int n, double cmx, double cmy, double cmz, double mu,
-                             double G, int central, double *__restrict__ ax, double *__restrict__ ay,
+                             double G, int central, J2Arg j2, double *__restrict__ ax, double *__restrict__ ay,
                              double *__restrict__ az, double *__restrict__ cterm)
 {
       int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -671,9 +682,11 @@ __global__ void k_grav_final(const double *__restrict__ partial, int nchunks, lo
             a[1] += -mu * DY / r3;
             a[2] += -mu * DZ / r3;
             double gm = G * s.w;
-            cterm[q] = gm * DX / r3;
-            cterm[n + q] = gm * DY / r3;
-            cterm[2 * n + q] = gm * DZ / r3;
+            double cj[3] = {0., 0., 0.};
+            if (j2.on) d_j2(j2, mu, DX, DY, DZ, rk, r3, s.w, a[0], a[1], a[2], cj);
+            cterm[q] = gm * DX / r3 + cj[0];
+            cterm[n + q] = gm * DY / r3 + cj[1];
+            cterm[2 * n + q] = gm * DZ / r3 + cj[2];
       }
       int slot = slots[q];
       ax[slot] = a[0];
@@ -753,6 +766,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       const double sp = P.par_softening_parameter;
       const bool soft = sp != 0.;
       BodyView cv = bv;
+      const J2Arg j2 = j2_arg(P, cmh[6]);
       if (mode == NCGPU_GRAVITY_EXACT) {
             D4 *src = (D4 *)c.src64;
             k_pack_exact<<<(npad + 255) / 256, 256, 0, st>>>(cv, c.cidx, n, npad, G, src, c.srcR);
@@ -761,15 +775,15 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
             NCG_CK(cudaEventRecord(c.kev0, st));
             if (soft)
                   k_grav_exact<true><<<nb, EXB, 0, st>>>(src, c.srcR, c.cidx, n, ntiles, cmh[0], cmh[1], cmh[2], mu,
-                                                         sp, central, ax, ay, az, c.cmterm, c.err);
+                                                         sp, central, j2, cv, ax, ay, az, c.cmterm, c.err);
             else
                   k_grav_exact<false><<<nb, EXB, 0, st>>>(src, c.srcR, c.cidx, n, ntiles, cmh[0], cmh[1], cmh[2],
-                                                          mu, sp, central, ax, ay, az, c.cmterm, c.err);
+                                                          mu, sp, central, j2, cv, ax, ay, az, c.cmterm, c.err);
             NCG_LAUNCHED();
             NCG_CK(cudaEventRecord(c.kev1, st));
             c.kev_valid = 1;
             if (central) {
-                  k_seq_sum3<<<1, 96, 0, st>>>(c.cmterm, n, d_cm_acc);
+                  k_seq_sum3<<<1, 96, 0, st>>>(c.cmterm, j2.on ? 2 * n : n, d_cm_acc);
             } else {
                   k_set3<<<1, 1, 0, st>>>(d_cm_acc, 0., 0., 0.);
             }
@@ -846,7 +860,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       NCG_CK(cudaEventRecord(c.kev1, st));
       c.kev_valid = 1;
       k_grav_final<<<(n + 255) / 256, 256, 0, st>>>(c.partial, nchunks, npad, s64, c.vals, n, cmh[0], cmh[1], cmh[2],
-                                                    mu, G, central, ax, ay, az, c.cmterm);
+                                                    mu, G, central, j2, ax, ay, az, c.cmterm);
       NCG_LAUNCHED();
       if (central) {
             const int np = min(128, (n + RB - 1) / RB);
@@ -866,11 +880,12 @@ namespace ncg {
 
 // The EXACT gravity of gravity_eval on caller-provided scratch, without the
 // library context: cidx (n), src (npad double4 = 4*npad doubles), srcR (npad),
-// cterm (3n), blockcnt/n_dev for the compaction, err (1 word).  Writes ax, ay,
+// cterm (3n, 6n with J2), blockcnt/n_dev for the compaction, err (1 word).  Writes ax, ay,
 // az (slots 0..largest_id, zero for empty slots) and d_cm_acc.
 int gravity_exact_into(const BodyView &bv, int largest_id, const double *cmh, double G, double sp, int central,
-                       int *cidx, double *src, double *srcR, double *cterm, int *blockcnt, int *n_dev,
-                       unsigned *err, double *ax, double *ay, double *az, double *d_cm_acc, cudaStream_t st)
+                       const J2Arg &j2, int *cidx, double *src, double *srcR, double *cterm, int *blockcnt,
+                       int *n_dev, unsigned *err, double *ax, double *ay, double *az, double *d_cm_acc,
+                       cudaStream_t st)
 {
       const int nslots = largest_id + 1;
       if (nslots > 0) {
@@ -893,13 +908,13 @@ int gravity_exact_into(const BodyView &bv, int largest_id, const double *cmh, do
       const int nb = (n + EXB - 1) / EXB;
       if (sp != 0.)
             k_grav_exact<true><<<nb, EXB, 0, st>>>(s4, srcR, cidx, n, ntiles, cmh[0], cmh[1], cmh[2], mu, sp, central,
-                                                   ax, ay, az, cterm, err);
+                                                   j2, bv, ax, ay, az, cterm, err);
       else
             k_grav_exact<false><<<nb, EXB, 0, st>>>(s4, srcR, cidx, n, ntiles, cmh[0], cmh[1], cmh[2], mu, sp,
-                                                    central, ax, ay, az, cterm, err);
+                                                    central, j2, bv, ax, ay, az, cterm, err);
       NCG_LAUNCHED();
       if (central) {
-            k_seq_sum3<<<1, 96, 0, st>>>(cterm, n, d_cm_acc);
+            k_seq_sum3<<<1, 96, 0, st>>>(cterm, j2.on ? 2 * n : n, d_cm_acc);
             NCG_LAUNCHED();
       }
       return NCGPU_OK;

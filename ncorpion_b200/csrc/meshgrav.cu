@@ -279,7 +279,15 @@ struct MGArgs {
       int nvis;                 // visits of bodies larger than the mesh size
       const int *vis;           // (body, first, end) candidate positions, in visit order
       const int *cp;            // candidate partners (a visit's list ascends)
+      J2Arg j2;                 // the central body's J2 term
 };
+
+// CM_acc's chain c (0..2) in `terms`: after the 9 chains of bodies 0..2, one
+// term per slot, or two (central, J2) with J2, in the reference's order.
+__device__ __forceinline__ double *cm_chain(double *terms, const MGArgs &A, long N, int c)
+{
+      return terms + 9 * N + (size_t)c * (A.j2.on ? 2 : 1) * N;
+}
 
 // Whether b is in the candidate list cp[lo, hi) (ascending).
 __device__ __forceinline__ bool in_list(const int *__restrict__ cp, int lo, int hi, int b)
@@ -310,7 +318,8 @@ __device__ __forceinline__ void tail_terms(const DevState &S, const MGArgs &A, i
 }
 
 // Accelerations of bodies 3..lid (bodies 0..2 are finished by k_mesh_big3);
-// terms for bodies 0..2 and CM_acc go to `terms` (12 blocks of n_max).
+// terms for bodies 0..2 and CM_acc go to `terms` (12 blocks of n_max, the
+// CM_acc ones doubled with J2).
 __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
                             const int *__restrict__ vals, const int *__restrict__ cstart, int have_cells,
                             const GRec *__restrict__ grec, double *__restrict__ ax, double *__restrict__ ay,
@@ -321,10 +330,13 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
       const int t = blockIdx.x * blockDim.x + threadIdx.x;
       if (t > A.lid) return;
       const int b = (have_cells && t <= A.lid0) ? vals[t] : t;
+      const int f = A.j2.on ? 2 : 1;
       if (!S.ex[b]) {
             // an empty slot adds +0.0 to every chain (they then read all terms
             // without looking at exists[])
-            for (int w = 0; w < 12; w++) terms[(size_t)w * N + b] = 0.;
+            for (int w = 0; w < 9; w++) terms[(size_t)w * N + b] = 0.;
+            for (int c = 0; c < 3; c++)
+                  for (int u = 0; u < f; u++) cm_chain(terms, A, N, c)[f * b + u] = 0.;
             return;
       }
       double a_x = 0., a_y = 0., a_z = 0.;
@@ -336,9 +348,14 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
             a_y = DDIV(DMUL(-A.mu, DY), r3);
             a_z = DDIV(DMUL(-A.mu, DZ), r3);
             double g = DMUL(A.G, S.m[b]);
-            terms[9 * N + b] = DDIV(DMUL(g, DX), r3);
-            terms[10 * N + b] = DDIV(DMUL(g, DY), r3);
-            terms[11 * N + b] = DDIV(DMUL(g, DZ), r3);
+            cm_chain(terms, A, N, 0)[f * b] = DDIV(DMUL(g, DX), r3);
+            cm_chain(terms, A, N, 1)[f * b] = DDIV(DMUL(g, DY), r3);
+            cm_chain(terms, A, N, 2)[f * b] = DDIV(DMUL(g, DZ), r3);
+            if (A.j2.on) {  // src/physics.c:149-160
+                  double cj[3];
+                  d_j2(A.j2, A.mu, DX, DY, DZ, rk, r3, S.m[b], a_x, a_y, a_z, cj);
+                  for (int c = 0; c < 3; c++) cm_chain(terms, A, N, c)[2 * b + 1] = cj[c];
+            }
       }
       if (b <= 2) {  // bodies 0..2: central term only here
             ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
@@ -485,9 +502,9 @@ __global__ void __launch_bounds__(384) k_mesh_chains(DevState S, MGArgs A, const
       const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       double s = chain_init(w, ax, ay, az);
       if (chain_live(w, S, A)) {
-            const double *t = terms + (size_t)w * N;
+            const double *t = w >= 9 ? cm_chain(const_cast<double *>(terms), A, N, w - 9) : terms + (size_t)w * N;
             const int k0 = w >= 9 ? 0 : 3;
-            const int n = A.lid + 1;
+            const int n = w >= 9 ? (A.j2.on ? 2 : 1) * (A.lid + 1) : A.lid + 1;
             double v[CHB / 32];
 #pragma unroll
             for (int u = 0; u < CHB / 32; u++) {
@@ -532,10 +549,15 @@ __global__ void k_mesh_chains_part(DevState S, MGArgs A, const double *__restric
       double s[12];
       for (int w = 0; w < 12; w++) s[w] = 0.;
       const int n = A.lid + 1;
+      const int f = A.j2.on ? 2 : 1;
       for (int k = blockIdx.x * RB12 + threadIdx.x; k < n; k += gridDim.x * RB12) {
             if (!S.ex[k]) continue;
-            for (int w = 0; w < 12; w++)
-                  if (k >= (w >= 9 ? 0 : 3)) s[w] += terms[(size_t)w * N + k];
+            for (int w = 0; w < 9; w++)
+                  if (k >= 3) s[w] += terms[(size_t)w * N + k];
+            for (int c = 0; c < 3; c++) {
+                  const double *t = cm_chain(const_cast<double *>(terms), A, N, c) + (size_t)f * k;
+                  s[9 + c] += f == 2 ? t[0] + t[1] : t[0];
+            }
       }
       const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
       for (int w = 0; w < 12; w++) {
@@ -627,13 +649,14 @@ int mesh_gravity_state(const double *cm8)
       cudaStream_t st = c.s;
       const int lid = c.largest_id;
       const long N = c.n_max;
-      NCG_TRY(ensure_partial((size_t)12 * N));
+      const J2Arg j2 = j2_arg(c.P, cm8[6]);
+      NCG_TRY(ensure_partial((size_t)(j2.on ? 15 : 12) * N));
       DevState S = dev_state();
       MGArgs A{lid, c.P.par_collision_cube_cells, c.P.par_central_mass_bool, c.P.par_mutual_bool,
                c.P.par_softening_parameter != 0., (long long)c.cell_cap, c.P.par_G, c.P.par_softening_parameter,
                c.P.par_G * cm8[6], cm8[0], cm8[1], cm8[2],
                c.mesh_valid ? c.mesh_n - 1 : -1, c.P.par_N_tilde, c.mesh_nfev, c.evx, c.fev,
-               c.mesh_nfev > 0 ? c.xhead : nullptr, c.mesh_valid ? c.mesh_nvis : 0, c.vis, c.cand_p};
+               c.mesh_nfev > 0 ? c.xhead : nullptr, c.mesh_valid ? c.mesh_nvis : 0, c.vis, c.cand_p, j2};
       double *ax = c.acc, *ay = c.acc + N, *az = c.acc + 2 * N;
       if (lid >= 0) {
             GRec *grec = (GRec *)c.mrec;

@@ -30,8 +30,8 @@ constexpr size_t NBLK = (size_t)NOALLOC_MAX_SLOTS / 1024 + 2;
 // layout (doubles first, 256-byte aligned blocks)
 constexpr size_t OFF_SRC = 0;                                   // 4 * NPAD doubles
 constexpr size_t OFF_SRCR = OFF_SRC + 4 * NPAD * 8;             // NPAD doubles
-constexpr size_t OFF_CTERM = OFF_SRCR + NPAD * 8;               // 3 * NPAD doubles
-constexpr size_t OFF_ACC = OFF_CTERM + 3 * NPAD * 8;            // 3 * NPAD doubles
+constexpr size_t OFF_CTERM = OFF_SRCR + NPAD * 8;               // 6 * NPAD doubles (two per body with J2)
+constexpr size_t OFF_ACC = OFF_CTERM + 6 * NPAD * 8;            // 3 * NPAD doubles
 constexpr size_t OFF_CIDX = OFF_ACC + 3 * NPAD * 8;             // NPAD ints
 constexpr size_t OFF_BLK = OFF_CIDX + NPAD * 4;                 // NBLK ints
 constexpr size_t OFF_MISC = (OFF_BLK + NBLK * 4 + 255) / 256 * 256;  // n_dev, err
@@ -84,8 +84,10 @@ extern "C" int ncgpu_vector_field_static(const double *d_bodies, const int *d_ex
       BodyView bv{d_bodies, d_bodies + 1, d_bodies + 2, d_bodies + 3, d_bodies + 4, d_bodies + 5,
                   d_bodies + 6, d_bodies + 7, 8, d_exists};
       const long bs = largest_id + 1;
+      if (params->par_J2_bool && !params->par_central_mass_bool) return NCGPU_E_ARG;
       NCG_TRY(gravity_exact_into(bv, largest_id, (const double *)cm, params->par_G, params->par_softening_parameter,
-                                 params->par_central_mass_bool, cidx, src, srcR, cterm, blk, n_dev, err, acc,
+                                 params->par_central_mass_bool, j2_arg(*params, cm->mass), cidx, src, srcR, cterm,
+                                 blk, n_dev, err, acc,
                                  acc + NPAD, acc + 2 * NPAD, d_cm_acc, st));
       if (bs > 0) {
             for (int d = 0; d < 3; d++)

@@ -77,14 +77,17 @@ static void gpu_params(struct ncgpu_params *p)
       p->par_k_parameter = k_parameter;
       p->par_merging_threshold = merging_threshold;
       p->par_fragment_threshold = fragment_threshold;
+      p->par_J2_bool = J2_bool;
+      p->par_J2 = J2_value;
+      p->par_R_unit = R_unit;
+      p->par_sideral_omega = SideralOmega;
 }
 
 /* The GPU path covers the configurations of its hot path only. */
 static void gpu_supported(void)
 {
-      if (J2_bool || central_tides_bool || inner_fluid_disk_bool || viscoelastic_bool || pert_mass > 0. ||
-          openGL_bool) {
-            fprintf(stderr, "Error : the GPU integration does not cover J2, tides, the inner fluid disk, the "
+      if (central_tides_bool || inner_fluid_disk_bool || viscoelastic_bool || pert_mass > 0. || openGL_bool) {
+            fprintf(stderr, "Error : the GPU integration does not cover tides, the inner fluid disk, the "
                             "viscoelastic body, the perturber or the 3D viewer.\n");
             abort();
       }
@@ -103,6 +106,9 @@ static void gpu_pull(struct moonlet *moonlets)
       gpu_check(ncgpu_download((struct ncgpu_body *)moonlets, exists, &lid, (struct ncgpu_body *)&CM), "download");
       for (int j = lid + 1; j <= largest_id && j < N_max; j++) exists[j] = 0;
       largest_id = lid;
+      /* the host's J2 for its own kicks: the fluid-body J2 follows the central
+         mass, which only the device's end_of_timestep changes (src/rk4.c:459-463) */
+      if (J2_bool && J2_value == 0.) J2 = 0.5 * SideralOmega * SideralOmega * R_unit * R_unit * R_unit / (G * CM.mass);
 }
 
 /* The collision records of the last sweep appended to collisionDatas, as

@@ -22,8 +22,29 @@
 
 typedef struct ncgpu_body body;
 
-/* vector_field, brute-force branch + central mass (src/physics.c:63-266 with
-   mesh_bool = 0, J2/tides/perturber off).  acc: 3 doubles per slot. */
+/* The J2 contribution of the central body's bulge to body k and to CM_acc
+   (src/physics.c:149-160), in the reference's operation order. */
+static void j2_terms(const struct ncgpu_params *P, double mu, double M, double DX, double DY, double DZ, double rk,
+                     double r3, double mk, double *aX, double *aY, double *aZ, double *cm_acc)
+{
+      /* J2_value, or the fluid-body J2 of the current central mass
+         (src/structure.c:507, src/rk4.c:459-463) */
+      double J2 = P->par_J2 != 0. ? P->par_J2
+                                  : 0.5 * P->par_sideral_omega * P->par_sideral_omega * P->par_R_unit * P->par_R_unit *
+                                            P->par_R_unit / (P->par_G * M);
+      double r2 = rk * rk;
+      double r5 = r3 * r2;
+      double K = mu * P->par_R_unit * P->par_R_unit * J2 / r5;
+      *aX += K * (-1.5 * DX + 7.5 / r2 * DZ * DZ * DX);
+      *aY += K * (-1.5 * DY + 7.5 / r2 * DZ * DZ * DY);
+      *aZ += K * (-4.5 * DZ + 7.5 / r2 * DZ * DZ * DZ);
+      cm_acc[0] += K * (1.5 * DX - 7.5 / r2 * DZ * DZ * DX) * mk / M;
+      cm_acc[1] += K * (1.5 * DY - 7.5 / r2 * DZ * DZ * DY) * mk / M;
+      cm_acc[2] += K * (4.5 * DZ - 7.5 / r2 * DZ * DZ * DZ) * mk / M;
+}
+
+/* vector_field, brute-force branch + central mass and J2 (src/physics.c:63-266
+   with mesh_bool = 0, tides/perturber off).  acc: 3 doubles per slot. */
 void orc_vector_field(int lid, const body *b, const int *ex, const body *cm, const struct ncgpu_params *P,
                       double *acc, double *cm_acc)
 {
@@ -54,6 +75,7 @@ void orc_vector_field(int lid, const body *b, const int *ex, const body *cm, con
             } else {
                   aX = aY = aZ = 0.;
             }
+            if (P->par_J2_bool) j2_terms(P, mu, M, DX, DY, DZ, rk, r3, mk, &aX, &aY, &aZ, cm_acc);
             if (P->par_mutual_bool) {                  /* src/physics.c:174-202 */
                   for (p = 0; p < k; p++) {
                         if (!ex[p]) continue;
@@ -674,6 +696,7 @@ void orc_w_vector_field_mesh(double *acc, double *cm_acc)
                   aX = -mu * DX / r3; aY = -mu * DY / r3; aZ = -mu * DZ / r3;
                   cm_acc[0] += G * mk * DX / r3; cm_acc[1] += G * mk * DY / r3; cm_acc[2] += G * mk * DZ / r3;
             }
+            if (W.P.par_J2_bool) j2_terms(&W.P, mu, M, DX, DY, DZ, rk, r3, mk, &aX, &aY, &aZ, cm_acc);
             if (mut && k > 2) {
                   double Rk = b[k].radius, soft, D, D3;
                   double Xi[3] = {X0, X1, X2}, Yi[3] = {Y0, Y1, Y2}, Zi[3] = {Z0, Z1, Z2}, mi[3] = {m0, m1, m2},

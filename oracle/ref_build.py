@@ -121,6 +121,24 @@ PROFILES = {
     "mesh_prog": dict(MESH, collision_bool="1", instant_merger_bool="1", collision_cube_cells="256",
                       N_max="30000", N_0="20000", t_end="0.05", time_step="0.0005", output_step="25",
                       write_to_files_bool="1", write_cartesian_bool="1", write_collisions_bool="1"),
+    # the central body's J2 (src/physics.c:149-160): a constant J2_value, and
+    # the fluid-body J2 (J2_value 0) that follows the central mass, with a
+    # sideral period Tearth = 25 (J2 = 0.0316 for M = 1)
+    "bf_grav_j2": dict(BF, collision_bool="0", softening_parameter="0.5", J2_bool="1", J2_value="0.0125",
+                       N_max="70000", N_0="2000", t_end="0.01", time_step="0.001"),
+    "bf_grav_j2f": dict(BF, collision_bool="0", J2_bool="1", J2_value="0.", Tearth="25.", N_max="70000",
+                        N_0="2000", t_end="0.01", time_step="0.001"),
+    "mesh_grav_j2f": dict(MESH, collision_bool="0", J2_bool="1", J2_value="0.", Tearth="25.",
+                          collision_cube_cells="256", N_max="70000", N_0="20000", t_end="0.005",
+                          time_step="0.0005"),
+    # whole-program runs with J2: the brute-force and mesh drivers
+    "bf_merge_j2": dict(BF, collision_bool="1", instant_merger_bool="1", J2_bool="1", J2_value="0.", Tearth="25.",
+                        N_max="4096", N_0="2000", t_end="0.2", time_step="0.001", output_step="50",
+                        write_to_files_bool="1", write_cartesian_bool="1", write_collisions_bool="1"),
+    "mesh_prog_j2": dict(MESH, collision_bool="1", instant_merger_bool="1", J2_bool="1", J2_value="0.", Tearth="25.",
+                         collision_cube_cells="256", N_max="30000", N_0="20000", t_end="0.05",
+                         time_step="0.0005", output_step="25", write_to_files_bool="1",
+                         write_cartesian_bool="1", write_collisions_bool="1"),
     # the N = 1,048,576 mesh workload: 1024 cells per side (8.6 GB hash table)
     "mesh_merge_1m": dict(MESH, collision_bool="1", instant_merger_bool="1",
                           collision_cube_cells="1024", N_max="1100000", N_0="1048576",

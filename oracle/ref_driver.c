@@ -78,6 +78,11 @@ void orc_set_state(int lid, const double *bodies, const int *ex, const double *c
       how_many_moonlets = 0;
       for (j = 0; j <= lid; j++) how_many_moonlets += ex[j] ? 1 : 0;
       need_to_reduce_COM_bool = 0;
+#if J2_bool
+      /* the J2 in force for this central mass, as variable_initialization
+         sets it (src/structure.c:507) */
+      J2 = J2_value == 0. ? 0.5 * SideralOmega * SideralOmega * R_unit * R_unit * R_unit / (G * CM.mass) : J2_value;
+#endif
 #if mesh_bool
       gam = g;
       collision_cube = gam * ((typ)collision_cube_cells);

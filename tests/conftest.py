@@ -1,3 +1,4 @@
+import math
 import os
 import sys
 
@@ -64,6 +65,10 @@ def make_params(**kw):
     p.merging_threshold = 0.0002
     p.fragment_threshold = 1.5e-8
     p.mesh_brute_gravity = 0
+    p.J2_bool = 0
+    p.J2 = 0.0
+    p.R_unit = 1.0
+    p.sideral_omega = 2.0 * math.pi / 3.556721809
     for k, v in kw.items():
         if k == "pq_min_max":
             p.pq_min_max[:] = list(v)

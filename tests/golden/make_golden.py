@@ -192,6 +192,50 @@ def mesh_big_case(profile, n, seed, gam, dt):
     return out
 
 
+def j2_gravity_case(profile, n, seed, mass, holes):
+    """One vector_field with the J2 term; the central mass `mass` sets the
+    fluid-body J2 when the profile's J2_value is 0."""
+    b = disks.gravity_disk(n, seed=seed)
+    ex = np.ones(n, np.int32)
+    ex[list(holes)] = 0
+    cm = cm_state(seed)
+    cm[6] = mass
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm)
+    acc, cma = ref.vector_field()
+    return dict(bodies=b, exists=ex, cm=cm, acc=acc, cm_acc=cma)
+
+
+def j2_mesh_steps_case(profile, n, seed, nsteps, gam, dt):
+    """nsteps of the mesh integrator loop without collisions (mesh gravity
+    with the fluid-body J2), four bodies placed inside the disruption
+    threshold so that the central mass, and with it J2, changes.  The gamma
+    the reference reaches after each step is stored for the replay."""
+    rng = np.random.default_rng(seed)
+    b = disks.mesh_disk(n, seed=seed)
+    b[:, 7] = rng.uniform(2e-3, 6e-3, n)
+    b[:, 6] = 4.0 / 3.0 * np.pi * 3.0 * b[:, 7] ** 3
+    idx = rng.choice(n, 4, replace=False)
+    ang = rng.uniform(0, 2 * np.pi, 4)
+    b[idx, 0] = 0.05 * np.cos(ang)
+    b[idx, 1] = 0.05 * np.sin(ang)
+    b[idx, 2] = 0.001
+    ex = np.ones(n, np.int32)
+    ex[rng.choice(n, n // 50, replace=False)] = 0
+    ex[idx] = 1
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm, dt=dt, gam=gam)
+    gams = []
+    for _ in range(nsteps):
+        ref.lib.orc_step_mesh()
+        gams.append(ref.get_state()[3][1])
+    b2, ex2, cm2, sc = ref.get_state()
+    return dict(bodies=b, exists=ex, cm=cm, dt=np.float64(dt), gam=np.float64(gam), nsteps=np.int64(nsteps),
+                gams=np.array(gams), out_digest=digest(b2), out_exists_digest=digest(ex2), out_cm=cm2,
+                out_largest_id=np.int64(b2.shape[0] - 1))
+
+
 OUTPUT_FILES = ["stat.txt", "collision.txt", "mass.txt", "radius.txt", "x.txt", "y.txt", "z.txt", "vx.txt",
                 "vy.txt", "vz.txt", "readme.txt"]
 
@@ -201,16 +245,18 @@ def filtered_stdout(text):
     return "\n".join(l for l in text.splitlines() if "integration took" not in l)
 
 
-def program_run_case(profile, bodies):
+def program_run_case(profile, bodies, bodies_from=None):
     """The whole reference program (oracle/_ref/<profile>/ncorpion) run on
-    init.txt: digests of every output file and of the console output."""
+    init.txt: digests of every output file and of the console output.  With
+    bodies_from, the fixture names the fixture that holds the same bodies
+    instead of storing them again."""
     import subprocess
     import tempfile
     d = tempfile.mkdtemp(prefix="ncref_run_")
     disks.write_init_txt(os.path.join(d, "init.txt"), bodies)
     exe = os.path.join(ROOT, "oracle", "_ref", profile, "ncorpion")
     r = subprocess.run([exe], cwd=d, capture_output=True, text=True, check=True)
-    out = dict(bodies=bodies)
+    out = dict(bodies=bodies) if bodies_from is None else dict(bodies_from=np.array(bodies_from))
     for f in OUTPUT_FILES:
         data = open(os.path.join(d, f), "rb").read()
         out["digest_" + f] = digest(np.frombuffer(data, np.uint8))
@@ -222,33 +268,41 @@ def program_run_case(profile, bodies):
 
 def main(names=None):
     out = {}
-    out["grav_s05_n512"] = gravity_case("bf_grav_s05", 512, 11, holes=(3, 100, 511))
-    out["grav_s0_n64"] = gravity_case("bf_grav_s0", 64, 12, holes=(0,))
-    out["grav_s0_n2"] = gravity_case("bf_grav_s0", 2, 13)
-    out["grav_s05_n3"] = gravity_case("bf_grav_s05", 3, 14)
-    out["steps_s0_n256"] = step_case("bf_grav_s0", 256, 15, 5, 1e-3, lambda n, s: disks.gravity_disk(n, s))
-    out["bf_sweep_merge"] = bf_sweep_case("bf_merge", 2000, 0)
-    out["bf_sweep_elastic"] = bf_sweep_case("bf_elastic", 2000, 0)
-    out["bf_sweep_inelastic"] = bf_sweep_case("bf_inelastic", 2000, 0)
-    out["bf_run_merge"] = bf_run_case("bf_merge", 2000, 0, 40)
-    out["mesh_merge"] = mesh_case("mesh_merge_s", 6000, 21, 0.03, 5e-4)
-    out["mesh_inelastic"] = mesh_case("mesh_inelastic_s", 6000, 22, 0.03, 5e-4)
+    out["grav_s05_n512"] = lambda: gravity_case("bf_grav_s05", 512, 11, holes=(3, 100, 511))
+    out["grav_s0_n64"] = lambda: gravity_case("bf_grav_s0", 64, 12, holes=(0,))
+    out["grav_s0_n2"] = lambda: gravity_case("bf_grav_s0", 2, 13)
+    out["grav_s05_n3"] = lambda: gravity_case("bf_grav_s05", 3, 14)
+    out["steps_s0_n256"] = lambda: step_case("bf_grav_s0", 256, 15, 5, 1e-3, lambda n, s: disks.gravity_disk(n, s))
+    out["bf_sweep_merge"] = lambda: bf_sweep_case("bf_merge", 2000, 0)
+    out["bf_sweep_elastic"] = lambda: bf_sweep_case("bf_elastic", 2000, 0)
+    out["bf_sweep_inelastic"] = lambda: bf_sweep_case("bf_inelastic", 2000, 0)
+    out["bf_run_merge"] = lambda: bf_run_case("bf_merge", 2000, 0, 40)
+    out["mesh_merge"] = lambda: mesh_case("mesh_merge_s", 6000, 21, 0.03, 5e-4)
+    out["mesh_inelastic"] = lambda: mesh_case("mesh_inelastic_s", 6000, 22, 0.03, 5e-4)
     # the N = 2,000 collisional disk, 200 steps, output every 50 steps
-    out["program_bf_merge"] = program_run_case("bf_merge", disks.bf_collide_disk(2000, seed=0))
+    out["program_bf_merge"] = lambda: program_run_case("bf_merge", disks.bf_collide_disk(2000, seed=0))
     # the mesh driver: 20,000 bodies with four larger than the mesh size, 100 steps
-    out["program_mesh_merge"] = program_run_case("mesh_prog", big_disk(20000, 7)[0])
+    out["program_mesh_merge"] = lambda: program_run_case("mesh_prog", big_disk(20000, 7)[0])
     # fragmentation: every outcome in one sweep (dt = 0.02 on the crowded ring)
-    out["frag_bf"] = frag_bf_case("bf_frag", 4000, 0, 0.02)
-    out["frag_mesh15"] = frag_mesh_case("mesh_frag_s", 4000, 0, 0.01, 0.02, 15, (-1, 3, -1, 1))
-    out["frag_mesh4"] = frag_mesh_case("mesh_frag4_s", 4000, 1, 0.01, 0.02, 4, (0, 1, 0, 1))
+    out["frag_bf"] = lambda: frag_bf_case("bf_frag", 4000, 0, 0.02)
+    out["frag_mesh15"] = lambda: frag_mesh_case("mesh_frag_s", 4000, 0, 0.01, 0.02, 15, (-1, 3, -1, 1))
+    out["frag_mesh4"] = lambda: frag_mesh_case("mesh_frag4_s", 4000, 1, 0.01, 0.02, 4, (0, 1, 0, 1))
     # bodies larger than the mesh size, three of them past slot 2
-    out["mesh_big_merge"] = mesh_big_case("mesh_merge_s", 10000, 100, 0.01, 5e-3)
-    out["mesh_big_inelastic"] = mesh_big_case("mesh_inelastic_s", 10000, 101, 0.01, 5e-3)
-    out["mesh_big_frag"] = mesh_big_case("mesh_frag_s", 10000, 102, 0.01, 5e-3)
-    for k, v in out.items():
+    out["mesh_big_merge"] = lambda: mesh_big_case("mesh_merge_s", 10000, 100, 0.01, 5e-3)
+    out["mesh_big_inelastic"] = lambda: mesh_big_case("mesh_inelastic_s", 10000, 101, 0.01, 5e-3)
+    out["mesh_big_frag"] = lambda: mesh_big_case("mesh_frag_s", 10000, 102, 0.01, 5e-3)
+    # the central body's J2: constant (softening 0.5) and fluid-body (M = 1.3)
+    out["grav_j2_n512"] = lambda: j2_gravity_case("bf_grav_j2", 512, 31, 1.0, (3, 100, 511))
+    out["grav_j2f_n300"] = lambda: j2_gravity_case("bf_grav_j2f", 300, 32, 1.3, (0, 7))
+    out["mesh_j2f_steps"] = lambda: j2_mesh_steps_case("mesh_grav_j2f", 6000, 33, 4, 0.03, 5e-4)
+    # whole-program runs of both drivers with the fluid-body J2
+    out["program_bf_merge_j2"] = lambda: program_run_case("bf_merge_j2", disks.bf_collide_disk(2000, seed=0))
+    out["program_mesh_merge_j2"] = lambda: program_run_case("mesh_prog_j2", big_disk(20000, 7)[0],
+                                                                bodies_from="program_mesh_merge")
+    for k, make in out.items():
         if names and k not in names:
             continue
-        np.savez_compressed(os.path.join(HERE, k + ".npz"), **v)
+        np.savez_compressed(os.path.join(HERE, k + ".npz"), **make())
         print("wrote", k)
 
 

@@ -6,7 +6,9 @@ drivers taken from ncorpion_b200/host/rk4_gpu.c on libncgpu.so
   (instant mergers, outputs every 50 steps);
 - mesh (mesh_prog): a 20,000-body disk with bodies larger than the mesh size,
   100 steps (mesh search with mergers, mesh gravity, adaptive mesh size,
-  outputs every 25 steps).
+  outputs every 25 steps);
+- both again with the central body's fluid-body J2 (bf_merge_j2,
+  mesh_prog_j2: J2_value 0, Tearth 25).
 
 Every output file (positions, velocities, masses, radii, stat.txt,
 collision.txt, readme.txt) and the console output must be byte-identical to
@@ -23,7 +25,8 @@ from conftest import ROOT, golden
 
 pytestmark = pytest.mark.gpu
 
-PROGRAMS = [("bf_merge", "program_bf_merge"), ("mesh_prog", "program_mesh_merge")]
+PROGRAMS = [("bf_merge", "program_bf_merge"), ("mesh_prog", "program_mesh_merge"),
+            ("bf_merge_j2", "program_bf_merge_j2"), ("mesh_prog_j2", "program_mesh_merge_j2")]
 
 
 def _digest(b):
@@ -42,7 +45,8 @@ def test_dropin_program_matches_reference_outputs(lib, profile, fixture):
     from ncorpion_b200 import disks
     g = golden(fixture)
     d = tempfile.mkdtemp(prefix="ncgpu_dropin_")
-    disks.write_init_txt(os.path.join(d, "init.txt"), g["bodies"])
+    bodies = golden(str(g["bodies_from"]))["bodies"] if "bodies_from" in g else g["bodies"]
+    disks.write_init_txt(os.path.join(d, "init.txt"), bodies)
     r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     bad = []

@@ -179,3 +179,66 @@ def test_port_mesh_big_bodies_matches_golden(name, ctype):
     b, ex, cm = w.get_state()
     assert np.array_equal(_digest(b), g["out_digest"]) and np.array_equal(_digest(ex), g["out_exists_digest"])
     w.lib.orc_w_mesh_reset()
+
+
+# ---- the central body's J2 (src/physics.c:149-160) --------------------------
+
+TEARTH_J2F = 25.0  # the sideral period of the fluid-body J2 profiles
+
+
+def j2_params(name, **kw):
+    """Port parameters of the J2 fixtures: a constant J2 (softening 0.5), or
+    the fluid-body J2 (J2_value 0) of a central body with Tearth = 25."""
+    if name == "grav_j2_n512":
+        return make_params(softening_parameter=0.5, J2_bool=1, J2=0.0125, **kw)
+    return make_params(J2_bool=1, J2=0.0, sideral_omega=2.0 * np.pi / TEARTH_J2F, **kw)
+
+
+@pytest.mark.parametrize("name", ["grav_j2_n512", "grav_j2f_n300"])
+def test_port_vector_field_j2_matches_golden(port, name):
+    """Brute-force vector_field with the J2 term: accelerations and CM_acc,
+    whose two terms per body (central, then J2) are added in that order."""
+    g = golden(name)
+    acc, cma = port.vector_field(g["bodies"], g["exists"], g["cm"], j2_params(name))
+    assert np.array_equal(acc, g["acc"])
+    assert np.array_equal(cma, g["cm_acc"])
+    # the term is there: without it the accelerations differ
+    acc0, _ = port.vector_field(g["bodies"], g["exists"], g["cm"], make_params(softening_parameter=0.5))
+    assert not np.array_equal(acc0, g["acc"])
+
+
+def test_port_mesh_steps_j2_matches_golden():
+    """Four iterations of the mesh loop (mesh gravity, no collisions) with the
+    fluid-body J2, bodies falling into the central mass on the way, so that J2
+    follows the new mass (src/rk4.c:459-463)."""
+    from ncorpion_b200 import api as A
+    import ctypes as C
+    g = golden("mesh_j2f_steps")
+    p = j2_params("mesh_j2f_steps", mesh_bool=1, brute_force_bool=0, collision_cube_cells=256)
+    w = oracle.PortWorld(16384, p)
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=float(g["dt"]), gam=float(g["gam"]))
+    gam = float(g["gam"])
+    for s in range(int(g["nsteps"])):
+        w.lib.orc_w_set_gam(C.c_double(gam))
+        tn = w.lib.orc_w_step_mesh()
+        gam = A.update_gamma(gam, tn, int(w.get_state()[1].sum()), 16.0, 4.4 / 256)
+        assert gam == g["gams"][s]
+    b, ex, cm = w.get_state()
+    assert np.array_equal(_digest(b), g["out_digest"]) and np.array_equal(_digest(ex), g["out_exists_digest"])
+    assert np.array_equal(cm, g["out_cm"])
+    assert cm[6] > g["cm"][6], "no body fell into the central mass"
+
+
+@pytest.mark.skipif(not oracle.ref_available("bf_grav_j2f"), reason="reference not compiled here")
+def test_port_vs_reference_j2_random_holes(port):
+    from ncorpion_b200 import disks
+    rng = np.random.default_rng(8)
+    for n in (4, 129, 700):
+        b = disks.gravity_disk(n, seed=int(rng.integers(1 << 30)))
+        ex = (rng.random(n) > 0.1).astype(np.int32)
+        cm = np.array([1e-5, -1e-5, 2e-6, 0, 0, 0, float(rng.uniform(0.8, 1.5)), 1.0])
+        ref = oracle.Ref("bf_grav_j2f")
+        ref.set_state(b, ex, cm)
+        a_ref, c_ref = ref.vector_field()
+        a, c = port.vector_field(b, ex, cm, j2_params("bf_grav_j2f"))
+        assert np.array_equal(a, a_ref) and np.array_equal(c, c_ref)

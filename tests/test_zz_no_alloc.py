@@ -30,13 +30,15 @@ def test_static_scratch_matches_allocating_entry_point(lib):
     from ncorpion_b200 import api, disks
 
     assert 0 < lib.ncgpu_noalloc_scratch_bytes() < 64 << 20
-    cases = [(3000, 1, 0.5, 0.05), (1200, 2, 0.0, 0.1)]
-    for n, seed, soft, hole_frac in cases:
+    # the third case carries the fluid-body J2 (two CM_acc terms per body)
+    cases = [(3000, 1, 0.5, 0.05, {}), (1200, 2, 0.0, 0.1, {}),
+             (2000, 3, 0.5, 0.05, dict(J2_bool=1, J2=0.0, sideral_omega=2.0 * np.pi / 25.0))]
+    for n, seed, soft, hole_frac, extra in cases:
         b = disks.gravity_disk(n, seed=seed)
         rng = np.random.default_rng(seed)
         ex = (rng.random(n) > hole_frac).astype(np.int32)
         cm = np.array([1e-6, -2e-6, 0.0, 0, 0, 0, 1.0, 1.0])
-        params = make_params(softening_parameter=soft)
+        params = make_params(softening_parameter=soft, **extra)
         d_b = torch.from_numpy(b).cuda()
         d_ex = torch.from_numpy(ex).cuda()
         acc_s = torch.full((n, 3), np.nan, dtype=torch.float64, device="cuda")
