@@ -107,6 +107,15 @@ struct ncgpu_params {
       double par_J2;
       double par_R_unit;
       double par_sideral_omega;
+      /* tides raised on the central body, constant time lag model (tides,
+         src/physics.c:496-542, called from kick, src/rk4.c:88-90): k2, Delta_t
+         and dimensionless_moi (src/parameters.h:143-145).  Tides change the
+         central body's sideral rotation, which is then device state
+         (ncgpu_get_sideral_omega).  Needs the central mass. */
+      int par_central_tides_bool;
+      double par_k2;
+      double par_Delta_t;
+      double par_dimensionless_moi;
 };
 #define NCGPU_MAX_N_TILDE 64
 
@@ -227,6 +236,13 @@ int ncgpu_collide_brute(int *n_events);
    force's softening sqrt(r^2 + (softening_parameter (R_k + R_p))^2).  FP64,
    O(N^2), deterministic; for energy-drift diagnostics. */
 int ncgpu_energy(double *out);
+/* The central body's sideral rotation SideralOmega (src/structure.c:110), part
+   of the device state: ncgpu_init sets it to par_sideral_omega, the tides of
+   every kick change it (src/physics.c:539), and the fluid-body J2 of the
+   state-based kicks is evaluated from it.  The stateless vector_field entry
+   points use par_sideral_omega. */
+int ncgpu_get_sideral_omega(double *omega);
+int ncgpu_set_sideral_omega(double omega);
 /* Outcomes of the fragmentation model since the last upload, in the order of
    merger_count, super_catastrophic_count, half_fragmentation_count and
    full_fragmentation_count (src/structure.h:148-151). */

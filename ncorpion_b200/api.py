@@ -57,6 +57,10 @@ class Params(C.Structure):
         ("J2", C.c_double),
         ("R_unit", C.c_double),
         ("sideral_omega", C.c_double),
+        ("central_tides_bool", C.c_int),
+        ("k2", C.c_double),
+        ("Delta_t", C.c_double),
+        ("dimensionless_moi", C.c_double),
     ]
 
 
@@ -114,6 +118,8 @@ EXPORTS = {
     "ncgpu_collide_brute": (C.c_int, [P]),
     "ncgpu_fragment_counts": (C.c_int, [P]),
     "ncgpu_energy": (C.c_int, [P]),
+    "ncgpu_get_sideral_omega": (C.c_int, [P]),
+    "ncgpu_set_sideral_omega": (C.c_int, [C.c_double]),
     "ncgpu_probe_pow_third": (C.c_int, [P, P, C.c_int]),
     "ncgpu_get_events": (C.c_int, [P, P, C.c_int, P]),
     "ncgpu_end_of_timestep": (C.c_int, [P]),
@@ -381,6 +387,17 @@ def fragment_counts() -> np.ndarray:
     out = np.zeros(4, np.int32)
     check(load().ncgpu_fragment_counts(ptr(out)), "ncgpu_fragment_counts")
     return out
+
+
+def get_sideral_omega() -> float:
+    """The central body's sideral rotation of the device state."""
+    w = C.c_double(0.0)
+    check(load().ncgpu_get_sideral_omega(C.byref(w)), "ncgpu_get_sideral_omega")
+    return w.value
+
+
+def set_sideral_omega(omega: float):
+    check(load().ncgpu_set_sideral_omega(float(omega)), "ncgpu_set_sideral_omega")
 
 
 def energy() -> np.ndarray:

@@ -147,26 +147,44 @@ BodyView state_view()
       return v;
 }
 
-int state_cm_host(double *cm8)
+int state_cm_host(double *cm9)
 {
       Ctx &c = ctx();
-      NCG_CK(cudaMemcpyAsync(cm8, c.cm, 8 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaMemcpyAsync(cm9, c.cm, 9 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
       NCG_CK(cudaStreamSynchronize(c.s));
       return NCGPU_OK;
 }
 
-int mesh_gravity_state(const double *cm8);
+// The J2 in force for the state's kicks: J2_value, or the fluid-body J2 of the
+// state's central mass and rotation at this moment, which is when the
+// reference sets it (upload = variable_initialization, src/structure.c:507;
+// end of a step, src/rk4.c:459-463).  Kicks between two updates use it even if
+// the rotation changes meanwhile.
+int refresh_j2()
+{
+      Ctx &c = ctx();
+      if (!c.P.par_J2_bool) return NCGPU_OK;
+      double cm9[9];
+      NCG_TRY(state_cm_host(cm9));
+      c.j2 = j2_value(c.P, cm9[6], cm9[8]);
+      return NCGPU_OK;
+}
+
+int mesh_gravity_state(const double *cm8, const J2Arg &j2);
 
 int kick_state()
 {
       Ctx &c = ctx();
-      double cm8[8];
-      NCG_TRY(state_cm_host(cm8));
+      double cm9[9];
+      NCG_TRY(state_cm_host(cm9));
       const int nslots = c.largest_id + 1;
+      const J2Arg j2 = j2_arg(c.P, cm9[6], c.j2);
       if (c.P.par_mesh_bool && !c.force_naive && !c.P.par_mesh_brute_gravity)
-            NCG_TRY(mesh_gravity_state(cm8));
+            NCG_TRY(mesh_gravity_state(cm9, j2));
       else
-            NCG_TRY(gravity_eval(state_view(), c.largest_id, cm8, c.acc, c.n_max, c.cm_acc, c.P.par_gravity_mode, c.s));
+            NCG_TRY(gravity_eval(state_view(), c.largest_id, cm9, j2, c.acc, c.n_max, c.cm_acc, c.P.par_gravity_mode,
+                                 c.s));
+      if (c.P.par_central_tides_bool && c.P.par_central_mass_bool) NCG_TRY(tides_state(c.acc, c.n_max, c.cm_acc));
       int nb = nslots > 0 ? (nslots + 255) / 256 : 1;
       k_kick<<<nb, 256, 0, c.s>>>(c.ex, nslots, c.dt, c.acc, c.acc + c.n_max, c.acc + 2 * (size_t)c.n_max, c.vx,
                                   c.vy, c.vz, c.cm, c.cm_acc, c.P.par_central_mass_bool);
@@ -230,6 +248,10 @@ void ncgpu_default_params(struct ncgpu_params *p)
       p->par_J2 = 0.;
       p->par_R_unit = 1.;
       p->par_sideral_omega = 2. * 3.14159265358979323846 / 3.556721809;  /* Tearth's default */
+      p->par_central_tides_bool = 0;
+      p->par_k2 = 1.5;                  /* src/parameters.h:143-145 */
+      p->par_Delta_t = 0.0015807;
+      p->par_dimensionless_moi = 0.3307;
 }
 
 const char *ncgpu_strerror(int s)
@@ -259,7 +281,8 @@ static bool params_ok(const struct ncgpu_params *p)
 {
       if (!p || p->par_gravity_mode < 0 || p->par_gravity_mode > 2) return false;
       if (p->par_J2_bool != 0 && p->par_J2_bool != 1) return false;
-      if (p->par_J2_bool && !p->par_central_mass_bool) return false;
+      if (p->par_central_tides_bool != 0 && p->par_central_tides_bool != 1) return false;
+      if ((p->par_J2_bool || p->par_central_tides_bool) && !p->par_central_mass_bool) return false;
       return true;
 }
 
@@ -282,7 +305,7 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
       } while (0)
       A(c.x, N); A(c.y, N); A(c.z, N); A(c.vx, N); A(c.vy, N); A(c.vz, N); A(c.m, N); A(c.R, N);
       A(c.ex, N); A(c.exs, N);
-      A(c.cm, 8); A(c.cm_acc, 3);
+      A(c.cm, 16); A(c.cm_acc, 3);
       A(c.acc, 3 * N);
       A(c.cmterm, 6 * N);
       A(c.cidx, N);
@@ -345,8 +368,9 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
       cudaMemsetAsync(c.did, 0, N * sizeof(int), c.s);
       cudaMemsetAsync(c.dirty, 0, N, c.s);
       cudaMemsetAsync(c.scal, 0, S_COUNT * sizeof(int), c.s);
-      double cm0[8] = {0., 0., 0., 0., 0., 0., 1., 1.};
+      double cm0[16] = {0., 0., 0., 0., 0., 0., 1., 1., params->par_sideral_omega};
       cudaMemcpyAsync(c.cm, cm0, sizeof cm0, cudaMemcpyHostToDevice, c.s);
+      c.j2 = j2_value(*params, 1., params->par_sideral_omega);
       if (cudaStreamSynchronize(c.s) != cudaSuccess) {
             free_all();
             return NCGPU_E_CUDA;
@@ -371,6 +395,7 @@ int ncgpu_set_params(const struct ncgpu_params *params)
       if (!g_ctx.inited) return NCGPU_E_STATE;
       if (!params_ok(params)) return NCGPU_E_ARG;
       g_ctx.P = *params;
+      if (g_ctx.uploaded) return refresh_j2();
       return NCGPU_OK;
 }
 
@@ -409,7 +434,8 @@ int ncgpu_vector_field_dev(const double *d_bodies, const int *d_exists, int larg
       // d_acc is 3 consecutive blocks of (largest_id + 1) doubles
       long bs = largest_id + 1;
       // gravity_eval writes ax, ay, az blocks; repack to xyz triples
-      NCG_TRY(gravity_eval(bv, largest_id, (const double *)cm, c.acc, c.n_max, d_cm_acc, gravity_mode, st));
+      const J2Arg j2 = j2_arg(c.P, cm->mass, j2_value(c.P, cm->mass, c.P.par_sideral_omega));
+      NCG_TRY(gravity_eval(bv, largest_id, (const double *)cm, j2, c.acc, c.n_max, d_cm_acc, gravity_mode, st));
       if (bs > 0) {
             // interleave into d_acc[3*k + d]
             NCG_CK(cudaMemcpy2DAsync(d_acc, 3 * sizeof(double), c.acc, sizeof(double), sizeof(double), bs,
@@ -437,7 +463,8 @@ int ncgpu_vector_field(struct ncgpu_body *bodies, const int *exists, int largest
             NCG_CK(cudaMemcpyAsync(c.exs, exists, sizeof(int) * (size_t)ns, cudaMemcpyHostToDevice, st));
       }
       BodyView bv{c.aos, c.aos + 1, c.aos + 2, c.aos + 3, c.aos + 4, c.aos + 5, c.aos + 6, c.aos + 7, 8, c.exs};
-      NCG_TRY(gravity_eval(bv, largest_id, (const double *)cm, c.acc, c.n_max, c.cm_acc, gravity_mode, st));
+      const J2Arg j2 = j2_arg(c.P, cm->mass, j2_value(c.P, cm->mass, c.P.par_sideral_omega));
+      NCG_TRY(gravity_eval(bv, largest_id, (const double *)cm, j2, c.acc, c.n_max, c.cm_acc, gravity_mode, st));
       double *h = c.pinned;
       if (ns > 0) {
             NCG_CK(cudaMemcpyAsync(h, c.acc, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
@@ -486,7 +513,7 @@ int ncgpu_upload(const struct ncgpu_body *bodies, const int *exists, int largest
       c.n_events = 0;
       c.collision_count = 0;
       c.uploaded = 1;
-      return NCGPU_OK;
+      return refresh_j2();
 }
 
 int ncgpu_download(struct ncgpu_body *bodies, int *exists, int *largest_id, struct ncgpu_body *cm)
@@ -507,6 +534,25 @@ int ncgpu_download(struct ncgpu_body *bodies, int *exists, int *largest_id, stru
       NCG_CK(cudaStreamSynchronize(st));
       *largest_id = c.largest_id;
       return check_err_word();
+}
+
+int ncgpu_get_sideral_omega(double *omega)
+{
+      Ctx &c = g_ctx;
+      if (!c.inited) return NCGPU_E_STATE;
+      if (!omega) return NCGPU_E_ARG;
+      NCG_CK(cudaMemcpyAsync(omega, c.cm + 8, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaStreamSynchronize(c.s));
+      return NCGPU_OK;
+}
+
+int ncgpu_set_sideral_omega(double omega)
+{
+      Ctx &c = g_ctx;
+      if (!c.inited) return NCGPU_E_STATE;
+      NCG_CK(cudaMemcpyAsync(c.cm + 8, &omega, sizeof(double), cudaMemcpyHostToDevice, c.s));
+      NCG_CK(cudaStreamSynchronize(c.s));
+      return NCGPU_OK;
 }
 
 int ncgpu_set_timestep(double dt)

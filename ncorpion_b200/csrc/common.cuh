@@ -51,15 +51,19 @@ struct J2Arg {
       double R, J2, M;
 };
 
-// J2_value when it is nonzero, else the fluid-body J2 of the current central
-// mass M, the expression of src/structure.c:507 and src/rk4.c:462 in its order.
-inline J2Arg j2_arg(const ncgpu_params &P, double M)
+// J2_value when it is nonzero, else the fluid-body J2 of central mass M and
+// sideral rotation omega, the expression of src/structure.c:507 and
+// src/rk4.c:462 in its order.
+inline double j2_value(const ncgpu_params &P, double M, double omega)
 {
-      J2Arg j{P.par_J2_bool && P.par_central_mass_bool, P.par_R_unit, P.par_J2, M};
-      if (j.on && P.par_J2 == 0.)
-            j.J2 = 0.5 * P.par_sideral_omega * P.par_sideral_omega * P.par_R_unit * P.par_R_unit * P.par_R_unit /
-                   (P.par_G * M);
-      return j;
+      if (P.par_J2 != 0.) return P.par_J2;
+      return 0.5 * omega * omega * P.par_R_unit * P.par_R_unit * P.par_R_unit / (P.par_G * M);
+}
+
+// The J2 term of a force evaluation with the J2 value j2 (central mass M).
+inline J2Arg j2_arg(const ncgpu_params &P, double M, double j2)
+{
+      return J2Arg{P.par_J2_bool && P.par_central_mass_bool, P.par_R_unit, j2, M};
 }
 
 // Adds body k's J2 term to its acceleration a[] and returns CM_acc's share in
@@ -109,7 +113,8 @@ struct Ctx {
       int *exs = nullptr;          // scratch exists flags for stateless calls
       int largest_id = -1;
       int uploaded = 0;
-      double *cm = nullptr;        // 8 doubles: central mass record
+      double *cm = nullptr;        // 16 doubles: central mass record (8), SideralOmega at [8]
+      double j2 = 0.;              // the J2 in force for the state's kicks (set at upload and end of step)
       double *cm_acc = nullptr;    // 3 doubles
       double dt = 0.0;
 
@@ -232,8 +237,23 @@ int check_err_word();        // syncs the stream, reads and clears the device er
 // Gravity driver (gravity.cu).  Reads bodies through `bv` for slots
 // 0..largest_id, writes acc (3 blocks of n_max: ax, ay, az, zero for empty
 // slots) and cm_acc (3 doubles, device).
-int gravity_eval(const BodyView &bv, int largest_id, const double *cm_host8, double *d_acc,
+int gravity_eval(const BodyView &bv, int largest_id, const double *cm_host8, const J2Arg &j2, double *d_acc,
                  long acc_stride_block, double *d_cm_acc, int mode, cudaStream_t st);
+
+// Sequential FP64 sums, in index order, of the 3 arrays terms[c*n .. c*n + n),
+// starting from init[c] (0 when init is null); out may alias init.
+int seq_sum3(const double *terms, int n, const double *init, double *out, cudaStream_t st);
+
+// tides (src/physics.c:496-542) on the device state after the vector field
+// (tides.cu): acc blocks of n_max and the device CM_acc receive the tidal
+// terms, SideralOmega (cm[8]) changes body by body.
+int tides_state(double *d_acc, long acc_stride_block, double *d_cm_acc);
+
+// The central mass record and SideralOmega of the device state (9 doubles).
+int state_cm_host(double *cm9);
+
+// Re-evaluates the J2 in force (ctx().j2) from the device state.
+int refresh_j2();
 
 // LSD radix sort of (key, value) pairs, stable; keys use `bits` low bits.
 // Result ends in (keys, vals) buffers passed in (ping-pong through ctx scratch).

@@ -14,7 +14,6 @@
 #include "common.cuh"
 
 namespace ncg {
-int state_cm_host(double *cm8);
 namespace {
 
 constexpr int EB = 256;
@@ -109,11 +108,11 @@ extern "C" int ncgpu_energy(double *energy)
       const int nb = n > 0 ? (n + EB - 1) / EB : 0;
       NCG_TRY(ensure_partial((size_t)3 * (nb > 0 ? nb : 1) + 4));
       BodyView bv{c.x, c.y, c.z, c.vx, c.vy, c.vz, c.m, c.R, 1, c.ex};
-      double cmh[8] = {0., 0., 0., 0., 0., 0., 1., 0.};  // the J2 in force needs the central mass
+      double cmh[9] = {0., 0., 0., 0., 0., 0., 1., 0., 0.};  // the J2 term needs the central mass
       if (c.P.par_J2_bool) NCG_TRY(state_cm_host(cmh));
       if (nb > 0) {
             k_energy_part<<<nb, EB, 0, st>>>(bv, c.cidx, n, c.cm, c.P.par_G, c.P.par_softening_parameter,
-                                             c.P.par_central_mass_bool, c.P.par_mutual_bool, j2_arg(c.P, cmh[6]),
+                                             c.P.par_central_mass_bool, c.P.par_mutual_bool, j2_arg(c.P, cmh[6], c.j2),
                                              c.partial);
             NCG_LAUNCHED();
       }

@@ -269,6 +269,7 @@ int eot_state(int *hm_out)
             NCG_LAUNCHED();
       }
       NCG_TRY(sync_scalars());
+      if (P.par_J2_bool && P.par_J2 == 0.) NCG_TRY(refresh_j2());  // src/rk4.c:459-463
       if (hm_out) *hm_out = hm;
       return NCGPU_OK;
 }

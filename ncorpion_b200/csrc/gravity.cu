@@ -171,12 +171,13 @@ __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, 
 // a time in shared memory with coalesced loads, the next block loading while
 // lane 0 adds, so the dependent adds do not wait on global memory.
 constexpr int CHS = 512;
-__global__ void __launch_bounds__(96) k_seq_sum3(const double *__restrict__ cterm, int n, double *__restrict__ out)
+__global__ void __launch_bounds__(96) k_seq_sum3(const double *__restrict__ cterm, int n, const double *init,
+                                                 double *out)
 {
       __shared__ __align__(16) double stage[3][CHS];
       const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       const double *t = cterm + (size_t)w * n;
-      double s = 0.;
+      double s = init ? init[w] : 0.;
       double v[CHS / 32];
 #pragma unroll
       for (int u = 0; u < CHS / 32; u++) {
@@ -739,7 +740,14 @@ __global__ void k_set3(double *__restrict__ out, double a, double b, double c)
 
 }  // namespace
 
-int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *d_acc, long bs,
+int seq_sum3(const double *terms, int n, const double *init, double *out, cudaStream_t st)
+{
+      k_seq_sum3<<<1, 96, 0, st>>>(terms, n, init, out);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
+
+int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2Arg &j2, double *d_acc, long bs,
                  double *d_cm_acc, int mode, cudaStream_t st)
 {
       Ctx &c = ctx();
@@ -766,7 +774,6 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
       const double sp = P.par_softening_parameter;
       const bool soft = sp != 0.;
       BodyView cv = bv;
-      const J2Arg j2 = j2_arg(P, cmh[6]);
       if (mode == NCGPU_GRAVITY_EXACT) {
             D4 *src = (D4 *)c.src64;
             k_pack_exact<<<(npad + 255) / 256, 256, 0, st>>>(cv, c.cidx, n, npad, G, src, c.srcR);
@@ -783,7 +790,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, double *
             NCG_CK(cudaEventRecord(c.kev1, st));
             c.kev_valid = 1;
             if (central) {
-                  k_seq_sum3<<<1, 96, 0, st>>>(c.cmterm, j2.on ? 2 * n : n, d_cm_acc);
+                  k_seq_sum3<<<1, 96, 0, st>>>(c.cmterm, j2.on ? 2 * n : n, nullptr, d_cm_acc);
             } else {
                   k_set3<<<1, 1, 0, st>>>(d_cm_acc, 0., 0., 0.);
             }
@@ -914,7 +921,7 @@ int gravity_exact_into(const BodyView &bv, int largest_id, const double *cmh, do
                                                     central, j2, bv, ax, ay, az, cterm, err);
       NCG_LAUNCHED();
       if (central) {
-            k_seq_sum3<<<1, 96, 0, st>>>(cterm, j2.on ? 2 * n : n, d_cm_acc);
+            k_seq_sum3<<<1, 96, 0, st>>>(cterm, j2.on ? 2 * n : n, nullptr, d_cm_acc);
             NCG_LAUNCHED();
       }
       return NCGPU_OK;

@@ -643,13 +643,12 @@ int three_largest_state(int *idx)
 }
 
 // vector_field in mesh mode on the device state; acc blocks + cm_acc.
-int mesh_gravity_state(const double *cm8)
+int mesh_gravity_state(const double *cm8, const J2Arg &j2)
 {
       Ctx &c = ctx();
       cudaStream_t st = c.s;
       const int lid = c.largest_id;
       const long N = c.n_max;
-      const J2Arg j2 = j2_arg(c.P, cm8[6]);
       NCG_TRY(ensure_partial((size_t)(j2.on ? 15 : 12) * N));
       DevState S = dev_state();
       MGArgs A{lid, c.P.par_collision_cube_cells, c.P.par_central_mass_bool, c.P.par_mutual_bool,

@@ -86,7 +86,7 @@ extern "C" int ncgpu_vector_field_static(const double *d_bodies, const int *d_ex
       const long bs = largest_id + 1;
       if (params->par_J2_bool && !params->par_central_mass_bool) return NCGPU_E_ARG;
       NCG_TRY(gravity_exact_into(bv, largest_id, (const double *)cm, params->par_G, params->par_softening_parameter,
-                                 params->par_central_mass_bool, j2_arg(*params, cm->mass), cidx, src, srcR, cterm,
+                                 params->par_central_mass_bool, j2_arg(*params, cm->mass, j2_value(*params, cm->mass, params->par_sideral_omega)), cidx, src, srcR, cterm,
                                  blk, n_dev, err, acc,
                                  acc + NPAD, acc + 2 * NPAD, d_cm_acc, st));
       if (bs > 0) {

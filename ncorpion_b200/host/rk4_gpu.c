@@ -81,14 +81,18 @@ static void gpu_params(struct ncgpu_params *p)
       p->par_J2 = J2_value;
       p->par_R_unit = R_unit;
       p->par_sideral_omega = SideralOmega;
+      p->par_central_tides_bool = central_tides_bool;
+      p->par_k2 = k2;
+      p->par_Delta_t = Delta_t;
+      p->par_dimensionless_moi = dimensionless_moi;
 }
 
 /* The GPU path covers the configurations of its hot path only. */
 static void gpu_supported(void)
 {
-      if (central_tides_bool || inner_fluid_disk_bool || viscoelastic_bool || pert_mass > 0. || openGL_bool) {
-            fprintf(stderr, "Error : the GPU integration does not cover tides, the inner fluid disk, the "
-                            "viscoelastic body, the perturber or the 3D viewer.\n");
+      if (inner_fluid_disk_bool || viscoelastic_bool || pert_mass > 0. || openGL_bool) {
+            fprintf(stderr, "Error : the GPU integration does not cover the inner fluid disk, the viscoelastic "
+                            "body, the perturber or the 3D viewer.\n");
             abort();
       }
 }
@@ -106,8 +110,11 @@ static void gpu_pull(struct moonlet *moonlets)
       gpu_check(ncgpu_download((struct ncgpu_body *)moonlets, exists, &lid, (struct ncgpu_body *)&CM), "download");
       for (int j = lid + 1; j <= largest_id && j < N_max; j++) exists[j] = 0;
       largest_id = lid;
-      /* the host's J2 for its own kicks: the fluid-body J2 follows the central
-         mass, which only the device's end_of_timestep changes (src/rk4.c:459-463) */
+      /* the central body's rotation, which the device's tides change, and the
+         host's J2 for its own kicks: the fluid-body J2 of the state at the
+         last end of step (src/rk4.c:459-463); neither the rotation nor the
+         central mass has changed since */
+      if (central_tides_bool) gpu_check(ncgpu_get_sideral_omega(&SideralOmega), "sideral rotation");
       if (J2_bool && J2_value == 0.) J2 = 0.5 * SideralOmega * SideralOmega * R_unit * R_unit * R_unit / (G * CM.mass);
 }
 
@@ -365,6 +372,11 @@ void ncgpu_integration_mesh(typ t)
                         total_neighbours = 0;
                   }
                   gpu_upload(moonlets);  /* exists[] may have changed (slots 0-2 refilled) */
+                  /* the host kick's tides changed the rotation, and the integration
+                     goes on with it (the J2 in force stays the one of the last end
+                     of step, which the upload took from the device's rotation) */
+                  if (central_tides_bool)
+                        gpu_check(ncgpu_set_sideral_omega(SideralOmega), "sideral rotation");
             }
             tn = 0;
             if (collision_bool) {

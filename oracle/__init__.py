@@ -54,6 +54,7 @@ class Port:
         return acc, cma
 
     def kick(self, bodies, exists, cm, dt, params):
+        """One kick; with tides, params.sideral_omega is updated in place."""
         b = np.ascontiguousarray(bodies, np.float64).copy()
         cmv = np.ascontiguousarray(cm, np.float64).copy()
         ex = np.ascontiguousarray(exists, np.int32)
@@ -94,6 +95,8 @@ class Ref:
         L.orc_get_state.restype = C.c_int
         L.orc_vector_field.argtypes = [P, P]
         L.orc_set_timestep.argtypes = [C.c_double]
+        L.orc_get_sideral_omega.restype = C.c_double
+        L.orc_set_sideral_omega.argtypes = [C.c_double]
         L.orc_events.argtypes = [P, C.c_int]
         L.orc_events.restype = C.c_int
         L.orc_n_max.restype = C.c_int
@@ -180,6 +183,8 @@ class PortWorld:
                                               C.c_double, C.c_double]
         L.orc_w_fragment_counts.argtypes = [P]
         L.orc_w_set_force_naive.argtypes = [C.c_int]
+        L.orc_w_get_sideral_omega.restype = C.c_double
+        L.orc_w_set_sideral_omega.argtypes = [C.c_double]
         self.n_max = n_max
         self.params = params
         if L.orc_w_init(n_max, C.byref(params)) != 0:

@@ -99,13 +99,56 @@ void orc_vector_field(int lid, const body *b, const int *ex, const body *cm, con
       }
 }
 
-/* kick (src/rk4.c:68-106): F on a copy, then v += timestep * a. */
-void orc_kick(int lid, body *b, const int *ex, body *cm, double dt, const struct ncgpu_params *P)
+/* tides (src/physics.c:496-542), constant time lag tides raised on the central
+   body, as kick calls them after the vector field (src/rk4.c:88-90).  b is the
+   state before the kick, acc (3 per slot) and cm_acc hold the vector field's
+   accelerations and receive the tidal terms; the central body's rotation
+   P->par_sideral_omega changes body by body in slot order, and the next body's
+   terms use the changed value. */
+static void port_tides(int lid, const body *b, const int *ex, const body *cm, double dt, struct ncgpu_params *P,
+                       double *acc, double *cm_acc)
+{
+      const double R_unit = P->par_R_unit, Dt = P->par_Delta_t;
+      double R5 = R_unit * R_unit * R_unit * R_unit * R_unit;
+      double A = 3. * P->par_k2 * P->par_G * R5;
+      double M = cm->mass;
+      double CMaccX = cm_acc[0], CMaccY = cm_acc[1], CMaccZ = cm_acc[2];
+      for (int j = 0; j <= lid; j++) {
+            if (!ex[j]) continue;
+            double X = b[j].x - cm->x, Y = b[j].y - cm->y, Z = b[j].z - cm->z;
+            double vX = b[j].vx - cm->vx + 0.5 * dt * (acc[3 * j] - CMaccX);
+            double vY = b[j].vy - cm->vy + 0.5 * dt * (acc[3 * j + 1] - CMaccY);
+            double vZ = b[j].vz - cm->vz + 0.5 * dt * (acc[3 * j + 2] - CMaccZ);
+            double m = b[j].mass;
+            double r2 = X * X + Y * Y + Z * Z;
+            double r10 = r2 * r2 * r2 * r2 * r2;
+            double rv = X * vX + Y * vY + Z * vZ;
+            double r_x_OmX = Y * P->par_sideral_omega;
+            double r_x_OmY = -X * P->par_sideral_omega;
+            double K = A * m / r10;
+            double S = 1. / (1. + m / M);
+            double aX = S * K * (r2 * X + Dt * (2. * rv * X + r2 * (vX + r_x_OmX)));
+            double aY = S * K * (r2 * Y + Dt * (2. * rv * Y + r2 * (vY + r_x_OmY)));
+            double aZ = S * K * (r2 * Z + Dt * (2. * rv * Z + r2 * vZ));
+            acc[3 * j] -= aX;
+            acc[3 * j + 1] -= aY;
+            acc[3 * j + 2] -= aZ;
+            cm_acc[0] += aX * m / M;
+            cm_acc[1] += aY * m / M;
+            cm_acc[2] += aZ * m / M;
+            P->par_sideral_omega += dt * m / (P->par_dimensionless_moi * M * R_unit * R_unit) * (X * aY - Y * aX) / S;
+      }
+}
+
+/* kick (src/rk4.c:68-106): F on a copy, tides, then v += timestep * a.  With
+   tides, P->par_sideral_omega is updated. */
+void orc_kick(int lid, body *b, const int *ex, body *cm, double dt, struct ncgpu_params *P)
 {
       int i;
       double *acc = (double *)malloc(sizeof(double) * 3 * (size_t)(lid + 1 > 0 ? lid + 1 : 1));
       double cma[3];
       orc_vector_field(lid, b, ex, cm, P, acc, cma);
+      if (P->par_central_tides_bool) port_tides(lid, b, ex, cm, dt, P, acc, cma);
       for (i = 0; i <= lid; i++) {
             if (!ex[i]) continue;
             b[i].vx += dt * acc[3 * i];
@@ -656,6 +699,9 @@ int orc_w_end_of_timestep(void)
 
 /* the world's kick / drift (src/rk4.c:68-127) */
 void orc_w_kick(void) { orc_kick(W.lid, W.b, W.ex, &W.cm, W.dt, &W.P); }
+/* the world's central-body rotation SideralOmega (changed by tides) */
+double orc_w_get_sideral_omega(void) { return W.P.par_sideral_omega; }
+void orc_w_set_sideral_omega(double w) { W.P.par_sideral_omega = w; }
 void orc_w_drift(void) { orc_drift(W.lid, W.b, W.ex, &W.cm, W.dt, &W.P); }
 
 /* one iteration of integration_brute_force_SABA1's loop (src/rk4.c:906-921):
@@ -744,6 +790,7 @@ void orc_w_kick_mesh(void)
       double *acc = (double *)malloc(sizeof(double) * 3 * (size_t)(W.lid + 1 > 0 ? W.lid + 1 : 1));
       double cma[3];
       orc_w_vector_field_mesh(acc, cma);
+      if (W.P.par_central_tides_bool) port_tides(W.lid, W.b, W.ex, &W.cm, W.dt, &W.P, acc, cma);
       for (i = 0; i <= W.lid; i++) {
             if (!W.ex[i]) continue;
             W.b[i].vx += W.dt * acc[3 * i];

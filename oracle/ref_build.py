@@ -139,6 +139,25 @@ PROFILES = {
                          collision_cube_cells="256", N_max="30000", N_0="20000", t_end="0.05",
                          time_step="0.0005", output_step="25", write_to_files_bool="1",
                          write_cartesian_bool="1", write_collisions_bool="1"),
+    # tides raised on the central body (src/physics.c:496-542) with a long time
+    # lag (Delta_t = 1) so that every body changes SideralOmega; alone, and with
+    # the fluid-body J2 that follows the changing rotation
+    "bf_tides": dict(BF, collision_bool="0", softening_parameter="0.5", central_tides_bool="1", Delta_t="1.0",
+                     N_max="70000", N_0="2000", t_end="0.01", time_step="0.001"),
+    "bf_tides_j2f": dict(BF, collision_bool="0", central_tides_bool="1", Delta_t="1.0", J2_bool="1",
+                         J2_value="0.", Tearth="25.", N_max="70000", N_0="2000", t_end="0.01", time_step="0.001"),
+    "mesh_tides_j2f": dict(MESH, collision_bool="0", central_tides_bool="1", Delta_t="1.0", J2_bool="1",
+                           J2_value="0.", Tearth="25.", collision_cube_cells="256", N_max="70000", N_0="20000",
+                           t_end="0.005", time_step="0.0005"),
+    # whole-program runs with tides and the fluid-body J2: both drivers
+    "bf_merge_tides": dict(BF, collision_bool="1", instant_merger_bool="1", central_tides_bool="1", Delta_t="1.0",
+                           J2_bool="1", J2_value="0.", Tearth="25.", N_max="4096", N_0="2000", t_end="0.2",
+                           time_step="0.001", output_step="50", write_to_files_bool="1",
+                           write_cartesian_bool="1", write_collisions_bool="1"),
+    "mesh_prog_tides": dict(MESH, collision_bool="1", instant_merger_bool="1", central_tides_bool="1",
+                            Delta_t="1.0", J2_bool="1", J2_value="0.", Tearth="25.", collision_cube_cells="256",
+                            N_max="30000", N_0="20000", t_end="0.05", time_step="0.0005", output_step="25",
+                            write_to_files_bool="1", write_cartesian_bool="1", write_collisions_bool="1"),
     # the N = 1,048,576 mesh workload: 1024 cells per side (8.6 GB hash table)
     "mesh_merge_1m": dict(MESH, collision_bool="1", instant_merger_bool="1",
                           collision_cube_cells="1024", N_max="1100000", N_0="1048576",
@@ -204,10 +223,12 @@ def build(profile: str, src: str, verbose: bool = False) -> str:
 
 
 def stale(profile: str) -> bool:
-    """True when the profile is missing, or its drop-in program predates the
-    C ABI header or the drop-in driver it was compiled from."""
+    """True when the profile is missing, its library predates ref_driver.c, or
+    its drop-in program predates the C ABI header or the drop-in driver it was
+    compiled from."""
     dst = os.path.join(OUT, profile)
-    if not os.path.exists(os.path.join(dst, "libref.so")):
+    lib = os.path.join(dst, "libref.so")
+    if not os.path.exists(lib) or os.path.getmtime(os.path.join(HERE, "ref_driver.c")) > os.path.getmtime(lib):
         return True
     ov = PROFILES[profile]
     if ov.get("brute_force_bool") == "1" or ov.get("mesh_bool") == "1":

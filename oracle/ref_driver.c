@@ -78,9 +78,10 @@ void orc_set_state(int lid, const double *bodies, const int *ex, const double *c
       how_many_moonlets = 0;
       for (j = 0; j <= lid; j++) how_many_moonlets += ex[j] ? 1 : 0;
       need_to_reduce_COM_bool = 0;
+      /* the central body's rotation and the J2 in force for this central
+         mass, as variable_initialization sets them (src/structure.c:506-507) */
+      SideralOmega = 2. * M_PI / Tearth;
 #if J2_bool
-      /* the J2 in force for this central mass, as variable_initialization
-         sets it (src/structure.c:507) */
       J2 = J2_value == 0. ? 0.5 * SideralOmega * SideralOmega * R_unit * R_unit * R_unit / (G * CM.mass) : J2_value;
 #endif
 #if mesh_bool
@@ -144,6 +145,8 @@ void orc_vector_field(double *acc, double *cm_acc)
 void orc_kick(void) { kick(B, &CM, vector_field); }
 void orc_drift(void) { drift(B, &CM); }
 void orc_set_timestep(double dt) { timestep = dt; }
+double orc_get_sideral_omega(void) { return SideralOmega; }
+void orc_set_sideral_omega(double w) { SideralOmega = w; }
 void orc_end_of_timestep(void) { end_of_timestep(B, 0); }
 
 void orc_events_reset(void) { ev_n = 0; }

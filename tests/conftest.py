@@ -69,6 +69,10 @@ def make_params(**kw):
     p.J2 = 0.0
     p.R_unit = 1.0
     p.sideral_omega = 2.0 * math.pi / 3.556721809
+    p.central_tides_bool = 0
+    p.k2 = 1.5
+    p.Delta_t = 0.0015807
+    p.dimensionless_moi = 0.3307
     for k, v in kw.items():
         if k == "pq_min_max":
             p.pq_min_max[:] = list(v)

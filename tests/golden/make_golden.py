@@ -236,6 +236,47 @@ def j2_mesh_steps_case(profile, n, seed, nsteps, gam, dt):
                 out_largest_id=np.int64(b2.shape[0] - 1))
 
 
+def tides_bf_case(profile, n, seed, nsteps, dt):
+    """nsteps of the brute-force loop (no collisions) with tides raised on the
+    central body: the final state and SideralOmega after every step."""
+    b = disks.gravity_disk(n, seed=seed)
+    ex = np.ones(n, np.int32)
+    ex[[3, n // 2]] = 0
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm, dt=dt)
+    omegas = [ref.lib.orc_get_sideral_omega()]
+    for _ in range(nsteps):
+        ref.lib.orc_step_brute_force()
+        omegas.append(ref.lib.orc_get_sideral_omega())
+    b2, ex2, cm2, sc = ref.get_state()
+    return dict(bodies=b, exists=ex, cm=cm, dt=np.float64(dt), nsteps=np.int64(nsteps), omegas=np.array(omegas),
+                out_bodies=b2, out_exists=ex2, out_cm=cm2)
+
+
+def tides_mesh_case(profile, n, seed, nsteps, gam, dt):
+    """nsteps of the mesh loop (no collisions) with tides and the fluid-body
+    J2: gamma and SideralOmega after every step, the final state."""
+    rng = np.random.default_rng(seed)
+    b = disks.mesh_disk(n, seed=seed)
+    b[:, 7] = rng.uniform(2e-3, 6e-3, n)
+    b[:, 6] = 4.0 / 3.0 * np.pi * 3.0 * b[:, 7] ** 3
+    ex = np.ones(n, np.int32)
+    ex[rng.choice(n, n // 50, replace=False)] = 0
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm, dt=dt, gam=gam)
+    gams, omegas = [], [ref.lib.orc_get_sideral_omega()]
+    for _ in range(nsteps):
+        ref.lib.orc_step_mesh()
+        gams.append(ref.get_state()[3][1])
+        omegas.append(ref.lib.orc_get_sideral_omega())
+    b2, ex2, cm2, sc = ref.get_state()
+    return dict(bodies=b, exists=ex, cm=cm, dt=np.float64(dt), gam=np.float64(gam), nsteps=np.int64(nsteps),
+                gams=np.array(gams), omegas=np.array(omegas), out_digest=digest(b2), out_exists_digest=digest(ex2),
+                out_cm=cm2, out_largest_id=np.int64(b2.shape[0] - 1))
+
+
 OUTPUT_FILES = ["stat.txt", "collision.txt", "mass.txt", "radius.txt", "x.txt", "y.txt", "z.txt", "vx.txt",
                 "vy.txt", "vz.txt", "readme.txt"]
 
@@ -296,9 +337,19 @@ def main(names=None):
     out["grav_j2f_n300"] = lambda: j2_gravity_case("bf_grav_j2f", 300, 32, 1.3, (0, 7))
     out["mesh_j2f_steps"] = lambda: j2_mesh_steps_case("mesh_grav_j2f", 6000, 33, 4, 0.03, 5e-4)
     # whole-program runs of both drivers with the fluid-body J2
-    out["program_bf_merge_j2"] = lambda: program_run_case("bf_merge_j2", disks.bf_collide_disk(2000, seed=0))
+    out["program_bf_merge_j2"] = lambda: program_run_case("bf_merge_j2", disks.bf_collide_disk(2000, seed=0),
+                                                          bodies_from="program_bf_merge")
     out["program_mesh_merge_j2"] = lambda: program_run_case("mesh_prog_j2", big_disk(20000, 7)[0],
                                                                 bodies_from="program_mesh_merge")
+    # tides raised on the central body (Delta_t = 1): alone, with the fluid-body
+    # J2, in the mesh loop, and whole-program runs of both drivers
+    out["tides_bf_steps"] = lambda: tides_bf_case("bf_tides", 512, 41, 6, 1e-3)
+    out["tides_j2f_bf_steps"] = lambda: tides_bf_case("bf_tides_j2f", 512, 42, 6, 1e-3)
+    out["tides_mesh_steps"] = lambda: tides_mesh_case("mesh_tides_j2f", 6000, 43, 4, 0.03, 5e-4)
+    out["program_bf_merge_tides"] = lambda: program_run_case("bf_merge_tides", disks.bf_collide_disk(2000, seed=0),
+                                                             bodies_from="program_bf_merge")
+    out["program_mesh_merge_tides"] = lambda: program_run_case("mesh_prog_tides", big_disk(20000, 7)[0],
+                                                               bodies_from="program_mesh_merge")
     for k, make in out.items():
         if names and k not in names:
             continue

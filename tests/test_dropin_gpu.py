@@ -8,7 +8,9 @@ drivers taken from ncorpion_b200/host/rk4_gpu.c on libncgpu.so
   100 steps (mesh search with mergers, mesh gravity, adaptive mesh size,
   outputs every 25 steps);
 - both again with the central body's fluid-body J2 (bf_merge_j2,
-  mesh_prog_j2: J2_value 0, Tearth 25).
+  mesh_prog_j2: J2_value 0, Tearth 25), and with tides raised on the central
+  body besides (bf_merge_tides, mesh_prog_tides: Delta_t 1), whose rotation
+  the output files print.
 
 Every output file (positions, velocities, masses, radii, stat.txt,
 collision.txt, readme.txt) and the console output must be byte-identical to
@@ -26,7 +28,8 @@ from conftest import ROOT, golden
 pytestmark = pytest.mark.gpu
 
 PROGRAMS = [("bf_merge", "program_bf_merge"), ("mesh_prog", "program_mesh_merge"),
-            ("bf_merge_j2", "program_bf_merge_j2"), ("mesh_prog_j2", "program_mesh_merge_j2")]
+            ("bf_merge_j2", "program_bf_merge_j2"), ("mesh_prog_j2", "program_mesh_merge_j2"),
+            ("bf_merge_tides", "program_bf_merge_tides"), ("mesh_prog_tides", "program_mesh_merge_tides")]
 
 
 def _digest(b):

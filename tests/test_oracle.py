@@ -242,3 +242,50 @@ def test_port_vs_reference_j2_random_holes(port):
         a_ref, c_ref = ref.vector_field()
         a, c = port.vector_field(b, ex, cm, j2_params("bf_grav_j2f"))
         assert np.array_equal(a, a_ref) and np.array_equal(c, c_ref)
+
+
+# ---- tides raised on the central body (src/physics.c:496-542) --------------
+
+TIDES = dict(central_tides_bool=1, Delta_t=1.0)
+
+
+@pytest.mark.parametrize("name", ["tides_bf_steps", "tides_j2f_bf_steps"])
+def test_port_tides_bf_steps_match_golden(name):
+    """Six iterations of the brute-force loop with tides (and, in the second
+    fixture, the fluid-body J2 that follows the changing rotation):
+    SideralOmega after every step and the final state."""
+    g = golden(name)
+    if name == "tides_bf_steps":
+        p = make_params(softening_parameter=0.5, **TIDES)
+    else:
+        p = make_params(J2_bool=1, J2=0.0, sideral_omega=2.0 * np.pi / TEARTH_J2F, **TIDES)
+    w = oracle.PortWorld(4096, p)
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=float(g["dt"]))
+    assert w.lib.orc_w_get_sideral_omega() == g["omegas"][0]
+    for s in range(int(g["nsteps"])):
+        w.lib.orc_w_step_brute_force()
+        assert w.lib.orc_w_get_sideral_omega() == g["omegas"][s + 1]
+    b, ex, cm = w.get_state()
+    assert np.array_equal(b, g["out_bodies"]) and np.array_equal(ex, g["out_exists"])
+    assert np.array_equal(cm, g["out_cm"])
+    assert len(set(g["omegas"].tolist())) == len(g["omegas"]), "the rotation did not change"
+
+
+def test_port_tides_mesh_steps_match_golden():
+    from ncorpion_b200 import api as A
+    import ctypes as C
+    g = golden("tides_mesh_steps")
+    p = make_params(J2_bool=1, J2=0.0, sideral_omega=2.0 * np.pi / TEARTH_J2F, mesh_bool=1, brute_force_bool=0,
+                    collision_cube_cells=256, **TIDES)
+    w = oracle.PortWorld(16384, p)
+    w.set_state(g["bodies"], g["exists"], g["cm"], dt=float(g["dt"]), gam=float(g["gam"]))
+    gam = float(g["gam"])
+    for s in range(int(g["nsteps"])):
+        w.lib.orc_w_set_gam(C.c_double(gam))
+        tn = w.lib.orc_w_step_mesh()
+        gam = A.update_gamma(gam, tn, int(w.get_state()[1].sum()), 16.0, 4.4 / 256)
+        assert gam == g["gams"][s]
+        assert w.lib.orc_w_get_sideral_omega() == g["omegas"][s + 1]
+    b, ex, cm = w.get_state()
+    assert np.array_equal(_digest(b), g["out_digest"]) and np.array_equal(_digest(ex), g["out_exists_digest"])
+    assert np.array_equal(cm, g["out_cm"])
