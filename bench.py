@@ -12,8 +12,13 @@ measured against the exact FP64 result.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Under torchrun each rank evaluates its own copy of the workload (replicas,
-weak scaling); times are the max over ranks.
+Under torchrun the gravity headline is split over the ranks (strong scaling):
+each rank evaluates the field of its part of the targets
+(ncgpu_vector_field_part) and one NCCL all-reduce per step assembles the
+whole field on every rank (ncorpion_b200/shard.py); ``value`` is the job's
+pair-interactions/s.  The secondary sections (mesh, fragmenting disk,
+collisional disk, adjoint) run as one replica per rank.  Times are the max
+over ranks.
 """
 from __future__ import annotations
 
@@ -440,10 +445,14 @@ def main(argv=None):
     sp = C.c_void_p(stream.cuda_stream)
 
     def step(mode):
-        st = lib.ncgpu_vector_field_dev(C.c_void_p(d_b.data_ptr()), C.c_void_p(d_ex.data_ptr()), n - 1,
-                                        api.ptr(cmh), C.c_void_p(d_acc.data_ptr()), C.c_void_p(d_cma.data_ptr()),
-                                        mode, sp)
-        api.check(st, "ncgpu_vector_field_dev")
+        # this rank's part of the targets, then (N > 1) the all-reduce that
+        # assembles the field on every rank, ordered on `stream`
+        st = lib.ncgpu_vector_field_part(C.c_void_p(d_b.data_ptr()), C.c_void_p(d_ex.data_ptr()), n - 1,
+                                         api.ptr(cmh), rank, ws, C.c_void_p(d_acc.data_ptr()),
+                                         C.c_void_p(d_cma.data_ptr()), mode, sp)
+        api.check(st, "ncgpu_vector_field_part")
+        if ws > 1:
+            torch.distributed.all_reduce(d_acc)
 
     def timed(mode, steps, warmup):
         with torch.cuda.stream(stream):
@@ -493,30 +502,47 @@ def main(argv=None):
     rel_tot = np.linalg.norm(a_mx_tot - a_ex_tot, axis=1) / np.linalg.norm(a_ex_tot, axis=1)
     api.set_params(params(api.GRAVITY_MIXED))
 
-    # end to end through the host-buffer C ABI call (pinned host memory)
+    # end to end with host buffers (pinned host memory): one GPU, the C ABI's
+    # host-buffer call; N GPUs, the sharded field (copies in, this rank's part,
+    # all-reduce, copies out)
     hb = b.copy()
     hex_ = ex.copy()
     api.check(lib.ncgpu_host_register(api.ptr(hb), hb.nbytes), "register")
     api.check(lib.ncgpu_host_register(api.ptr(hex_), hex_.nbytes), "register")
     cma = np.zeros(3)
+    hacc = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    hb_t, hex_t = torch.from_numpy(hb), torch.from_numpy(hex_)
+
+    def e2e_step():
+        if ws == 1:
+            api.check(lib.ncgpu_vector_field(api.ptr(hb), api.ptr(hex_), n - 1, api.ptr(cmh), api.ptr(cma),
+                                             api.GRAVITY_MIXED), "e2e")
+            return
+        with torch.cuda.stream(stream):
+            d_b.copy_(hb_t, non_blocking=True)
+            d_ex.copy_(hex_t, non_blocking=True)
+            step(api.GRAVITY_MIXED)
+            hacc.copy_(d_acc, non_blocking=True)
+
     for _ in range(2):
-        api.check(lib.ncgpu_vector_field(api.ptr(hb), api.ptr(hex_), n - 1, api.ptr(cmh), api.ptr(cma),
-                                         api.GRAVITY_MIXED), "e2e")
+        e2e_step()
+        torch.cuda.synchronize()
         hb[:] = b
     e2e_t = []
-    lst = torch.cuda.ExternalStream(lib.ncgpu_stream())
+    # the library stream carries the copies in, the kernels and the copies out (one GPU); `stream` (N GPUs)
+    lst = torch.cuda.ExternalStream(lib.ncgpu_stream()) if ws == 1 else stream
     for _ in range(a.steps):
         hb[:] = b
         flush.zero_()
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(lst)  # the library stream carries the copies in, the kernels and the copies out
-        api.check(lib.ncgpu_vector_field(api.ptr(hb), api.ptr(hex_), n - 1, api.ptr(cmh), api.ptr(cma),
-                                         api.GRAVITY_MIXED), "e2e")
+        e0.record(lst)
+        e2e_step()
         e1.record(lst)
         e1.synchronize()
         e2e_t.append(e0.elapsed_time(e1) * 1e-3)
+    torch.cuda.synchronize()
     lib.ncgpu_host_unregister(api.ptr(hb))
     lib.ncgpu_host_unregister(api.ptr(hex_))
     e2e_s = max_over_ranks([float(np.mean(e2e_t))], ws, dev)[0]
@@ -566,7 +592,8 @@ def main(argv=None):
                 "note": "no reference mode couples mesh collisions with brute-force gravity; the energy includes "
                         "the collisions' own losses, so the mixed-minus-FP64 difference of the drift is the "
                         "gravity precision's share"}
-    achieved = FLOP_PER_INTERACTION * pairs / (kms_mixed * 1e-3) / 1e12
+    # one launch (one GPU) processes its part of the interactions
+    achieved = FLOP_PER_INTERACTION * (pairs / ws) / (kms_mixed * 1e-3) / 1e12
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
@@ -580,14 +607,15 @@ def main(argv=None):
                    "sample": f"unavailable: {e}"}
 
     if rank == 0:
-        value = ws * pairs / (ms_mixed * 1e-3)
+        value = pairs / (ms_mixed * 1e-3)  # the whole job's field, split over the ranks
         out = {
             "metric": METRIC, "value": value, "unit": "pair-interactions/s", "n_gpus": ws, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+            "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32 pair terms, f64 state/accumulation", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n": N_BODIES, "gravity_mode": "mixed",
                        "l2": "flushed between timed steps (256 MiB write outside the events)",
-                       "parallelism": "replicas" if ws > 1 else "single GPU"},
+                       "parallelism": (f"targets split over {ws} GPUs, one NCCL all-reduce of the field per step; "
+                                       "secondary sections one replica per GPU") if ws > 1 else "single GPU"},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak, "traffic": MIXED_DRAM_BYTES,
                          "traffic_note": "bytes per launch from ncu (dram__bytes_read.sum + dram__bytes_write.sum); "
@@ -597,16 +625,16 @@ def main(argv=None):
                          "peak_source": "measured in this run: best of the scalar FFMA and packed f32x2 FMA "
                                         "dependency-chain probes (ncgpu_probe_fp32_rates)",
                          "probes": rates,
-                         "rsqrt_bound_frac": pairs / (kms_mixed * 1e-3) / (rates["rsqrt_gops"] * 1e9)},
+                         "rsqrt_bound_frac": (pairs / ws) / (kms_mixed * 1e-3) / (rates["rsqrt_gops"] * 1e9)},
             "cpu_baseline": cpu,
-            "e2e": {"value": ws * pairs / e2e_s, "unit": "pair-interactions/s",
+            "e2e": {"value": pairs / e2e_s, "unit": "pair-interactions/s",
                     "h2d_bytes_per_step": int(hb.nbytes + hex_.nbytes), "d2h_bytes_per_step": int(n * 24 + 24),
                     "ms_per_step": e2e_s * 1e3},
             "gpu_launches": launches,
             "clocks": clocks,
-            "fp64_exact": {"value": ws * pairs / (ms_exact * 1e-3), "ms_per_step": ms_exact,
+            "fp64_exact": {"value": pairs / (ms_exact * 1e-3), "ms_per_step": ms_exact,
                            "kernel_ms": kms_exact},
-            "fp64_tiled": {"value": ws * pairs / (ms_fp64t * 1e-3), "ms_per_step": ms_fp64t,
+            "fp64_tiled": {"value": pairs / (ms_fp64t * 1e-3), "ms_per_step": ms_fp64t,
                            "kernel_ms": kms_fp64t},
             "speedup_mixed_vs_fp64_exact": ms_exact / ms_mixed,
             "speedup_mixed_vs_fp64_tiled": ms_fp64t / ms_mixed,

@@ -155,6 +155,20 @@ int ncgpu_vector_field_dev(const double *d_bodies, const int *d_exists, int larg
                            const struct ncgpu_body *cm, double *d_acc, double *d_cm_acc,
                            int gravity_mode, void *stream);
 
+/* One part of the same field, for runs that split the targets over several
+   GPUs (one process per GPU; the parts exchange through an all-reduce sum):
+   only the targets of part `part` of `nparts` get their acceleration -- the
+   part-th slice of the existing bodies in slot order (exact mode), or of the
+   Morton-ordered 128-body target blocks (FP64 / mixed) -- and every other row
+   of d_acc receives -0.0 (+0.0 for empty slots from part 0), the identity of
+   the sum, so that the element-wise sum of the parts' d_acc is the full field
+   bit for bit.  d_cm_acc receives the full CM_acc in every part.
+   ncgpu_vector_field_dev is part 0 of 1.  (No reference counterpart: the
+   reference is single-threaded; the sum of the parts is vector_field's.) */
+int ncgpu_vector_field_part(const double *d_bodies, const int *d_exists, int largest_id,
+                            const struct ncgpu_body *cm, int part, int nparts, double *d_acc,
+                            double *d_cm_acc, int gravity_mode, void *stream);
+
 /* Allocation-free variant of ncgpu_vector_field_dev in the EXACT mode.  It has
    no counterpart in the reference: it exists for callers that cannot allocate
    device memory when they evaluate forces (a host whose device memory belongs to

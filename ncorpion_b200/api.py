@@ -100,6 +100,7 @@ EXPORTS = {
     "ncgpu_last_error": (C.c_char_p, []),
     "ncgpu_vector_field": (C.c_int, [P, P, C.c_int, P, P, C.c_int]),
     "ncgpu_vector_field_dev": (C.c_int, [P, P, C.c_int, P, P, P, C.c_int, P]),
+    "ncgpu_vector_field_part": (C.c_int, [P, P, C.c_int, P, C.c_int, C.c_int, P, P, C.c_int, P]),
     "ncgpu_last_launch_count": (C.c_int, []),
     "ncgpu_stream": (C.c_void_p, []),
     "ncgpu_vector_field_static": (C.c_int, [P, P, C.c_int, P, P, P, P, P]),

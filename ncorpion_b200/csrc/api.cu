@@ -423,10 +423,18 @@ int ncgpu_vector_field_dev(const double *d_bodies, const int *d_exists, int larg
                            const struct ncgpu_body *cm, double *d_acc, double *d_cm_acc, int gravity_mode,
                            void *stream)
 {
+      return ncgpu_vector_field_part(d_bodies, d_exists, largest_id, cm, 0, 1, d_acc, d_cm_acc, gravity_mode, stream);
+}
+
+int ncgpu_vector_field_part(const double *d_bodies, const int *d_exists, int largest_id,
+                            const struct ncgpu_body *cm, int part, int nparts, double *d_acc, double *d_cm_acc,
+                            int gravity_mode, void *stream)
+{
       Ctx &c = g_ctx;
       reset_launches();
       if (!c.inited) return NCGPU_E_STATE;
       if (!d_bodies || !d_exists || !cm || !d_acc || !d_cm_acc) return NCGPU_E_ARG;
+      if (nparts < 1 || part < 0 || part >= nparts) return NCGPU_E_ARG;
       if (largest_id < -1 || largest_id >= c.n_max) return NCGPU_E_ARG;
       cudaStream_t st = stream ? (cudaStream_t)stream : c.s;
       BodyView bv{d_bodies, d_bodies + 1, d_bodies + 2, d_bodies + 3, d_bodies + 4, d_bodies + 5,
@@ -435,7 +443,8 @@ int ncgpu_vector_field_dev(const double *d_bodies, const int *d_exists, int larg
       long bs = largest_id + 1;
       // gravity_eval writes ax, ay, az blocks; repack to xyz triples
       const J2Arg j2 = j2_arg(c.P, cm->mass, j2_value(c.P, cm->mass, c.P.par_sideral_omega));
-      NCG_TRY(gravity_eval(bv, largest_id, (const double *)cm, j2, c.acc, c.n_max, d_cm_acc, gravity_mode, st));
+      NCG_TRY(gravity_eval(bv, largest_id, (const double *)cm, j2, c.acc, c.n_max, d_cm_acc, gravity_mode, st, part,
+                           nparts));
       if (bs > 0) {
             // interleave into d_acc[3*k + d]
             NCG_CK(cudaMemcpy2DAsync(d_acc, 3 * sizeof(double), c.acc, sizeof(double), sizeof(double), bs,

@@ -237,8 +237,13 @@ int check_err_word();        // syncs the stream, reads and clears the device er
 // Gravity driver (gravity.cu).  Reads bodies through `bv` for slots
 // 0..largest_id, writes acc (3 blocks of n_max: ax, ay, az, zero for empty
 // slots) and cm_acc (3 doubles, device).
+// With nparts > 1 only the targets of part `part` get their acceleration (the
+// compacted order's part-th slice in the exact mode, the part-th slice of the
+// Morton-ordered target blocks in the tiled modes); every other row gets -0.0
+// (+0.0 for empty slots from part 0), so that the sum over the parts is the
+// full field, bit for bit.  CM_acc is the full one in every part.
 int gravity_eval(const BodyView &bv, int largest_id, const double *cm_host8, const J2Arg &j2, double *d_acc,
-                 long acc_stride_block, double *d_cm_acc, int mode, cudaStream_t st);
+                 long acc_stride_block, double *d_cm_acc, int mode, cudaStream_t st, int part = 0, int nparts = 1);
 
 // Sequential FP64 sums, in index order, of the 3 arrays terms[c*n .. c*n + n),
 // starting from init[c] (0 when init is null); out may alias init.

@@ -64,9 +64,10 @@ template <bool SOFT>
 __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, const double *__restrict__ srcR,
                                                     const int *__restrict__ cidx, int n, int ntiles,
                                                     double cmx, double cmy, double cmz, double mu, double sp,
-                                                    int central, J2Arg j2, BodyView bv, double *__restrict__ ax,
-                                                    double *__restrict__ ay, double *__restrict__ az,
-                                                    double *__restrict__ cterm, unsigned *__restrict__ err)
+                                                    int central, J2Arg j2, BodyView bv, int p_lo, int p_hi,
+                                                    double *__restrict__ ax, double *__restrict__ ay,
+                                                    double *__restrict__ az, double *__restrict__ cterm,
+                                                    unsigned *__restrict__ err)
 {
       __shared__ D4 tile[2][T];
       __shared__ alignas(16) double tR[2][T];
@@ -102,6 +103,18 @@ __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, 
                   cterm[2 * nf + 2 * p + 1] = cj[2];
             }
       }
+      // targets of this part: [p_lo, p_hi) of the compacted order; the others
+      // get -0.0, the identity of the sum that combines the parts
+      const bool own = active && p >= p_lo && p < p_hi;
+      if (!__syncthreads_or(own)) {
+            if (active) {
+                  const int slot = cidx[p];
+                  ax[slot] = -0.0;
+                  ay[slot] = -0.0;
+                  az[slot] = -0.0;
+            }
+            return;
+      }
 
       if (tid == 0) {
             mbar_init(&bar[0], 1);
@@ -133,7 +146,7 @@ __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, 
                   }
                   return;
             }
-            if (active) {
+            if (own) {
                   const int jbase = t * T;
                   const int cnt = min(T, n - jbase);
                   for (int jj = 0; jj < cnt; ++jj) {
@@ -158,9 +171,9 @@ __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, 
       }
       if (active) {
             int slot = cidx[p];
-            ax[slot] = a_x;
-            ay[slot] = a_y;
-            az[slot] = a_z;
+            ax[slot] = own ? a_x : -0.0;
+            ay[slot] = own ? a_y : -0.0;
+            az[slot] = own ? a_z : -0.0;
       }
 }
 
@@ -556,7 +569,7 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
                                                     const double *__restrict__ box, int n, int ntiles, int tpc,
                                                     double theta, double eps2, double *__restrict__ partial,
                                                     long npad, unsigned *__restrict__ err,
-                                                    const double *__restrict__ rrange, double sp)
+                                                    const double *__restrict__ rrange, double sp, int ib_lo)
 {
       __shared__ alignas(16) float f4[2][4 * T];
       __shared__ alignas(16) float fr[2][T];
@@ -565,7 +578,7 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
       __shared__ uint64_t bar[2];
 
       const int tid = threadIdx.x;
-      const int ib = blockIdx.y;
+      const int ib = blockIdx.y + ib_lo;  // target block (the part's blocks start at ib_lo)
       const int t0 = blockIdx.x * tpc;
       const int t1 = min(ntiles, t0 + tpc);
       const int q0 = ib * T + tid, q1 = q0 + MXB;
@@ -665,13 +678,14 @@ __global__ void __launch_bounds__(MXB) k_grav_tiled(const D4 *__restrict__ s64, 
 // term and scatter back to slot order; per-body CM_acc terms for the reduction.
 __global__ void k_grav_final(const double *__restrict__ partial, int nchunks, long npad, const D4 *__restrict__ s64,
                              const int *__restrict__ slots, int n, double cmx, double cmy, double cmz, double mu,
-                             double G, int central, J2Arg j2, double *__restrict__ ax, double *__restrict__ ay,
-                             double *__restrict__ az, double *__restrict__ cterm)
+                             double G, int central, J2Arg j2, int q_lo, int q_hi, double *__restrict__ ax,
+                             double *__restrict__ ay, double *__restrict__ az, double *__restrict__ cterm)
 {
       int q = blockIdx.x * blockDim.x + threadIdx.x;
       if (q >= n) return;
+      const bool own = q >= q_lo && q < q_hi;  // this part's targets (sorted order)
       double m[3] = {0., 0., 0.};
-      for (int c = 0; c < nchunks; c++)
+      for (int c = 0; own && c < nchunks; c++)
             for (int d = 0; d < 3; d++) m[d] += partial[(size_t)c * 3 * npad + d * npad + q];
       D4 s = s64[q];
       double a[3] = {G * m[0], G * m[1], G * m[2]};
@@ -690,9 +704,9 @@ __global__ void k_grav_final(const double *__restrict__ partial, int nchunks, lo
             cterm[2 * n + q] = gm * DZ / r3 + cj[2];
       }
       int slot = slots[q];
-      ax[slot] = a[0];
-      ay[slot] = a[1];
-      az[slot] = a[2];
+      ax[slot] = own ? a[0] : -0.0;
+      ay[slot] = own ? a[1] : -0.0;
+      az[slot] = own ? a[2] : -0.0;
 }
 
 // Deterministic two-level sum of 3 component arrays of length n.
@@ -721,13 +735,13 @@ __global__ void k_sum3_final(const double *__restrict__ part, int nparts, double
       out[d] = s;
 }
 
-__global__ void k_zero3(double *__restrict__ ax, double *__restrict__ ay, double *__restrict__ az, int n)
+__global__ void k_fill3(double *__restrict__ ax, double *__restrict__ ay, double *__restrict__ az, int n, double v)
 {
       int i = blockIdx.x * blockDim.x + threadIdx.x;
       if (i < n) {
-            ax[i] = 0.;
-            ay[i] = 0.;
-            az[i] = 0.;
+            ax[i] = v;
+            ay[i] = v;
+            az[i] = v;
       }
 }
 
@@ -748,15 +762,17 @@ int seq_sum3(const double *terms, int n, const double *init, double *out, cudaSt
 }
 
 int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2Arg &j2, double *d_acc, long bs,
-                 double *d_cm_acc, int mode, cudaStream_t st)
+                 double *d_cm_acc, int mode, cudaStream_t st, int part, int nparts)
 {
       Ctx &c = ctx();
       const ncgpu_params &P = c.P;
       if (largest_id + 1 > c.n_max) return NCGPU_E_ARG;
+      if (nparts < 1 || part < 0 || part >= nparts) return NCGPU_E_ARG;
       const int nslots = largest_id + 1;
       double *ax = d_acc, *ay = d_acc + bs, *az = d_acc + 2 * bs;
       if (nslots > 0) {
-            k_zero3<<<(nslots + 255) / 256, 256, 0, st>>>(ax, ay, az, nslots);
+            // empty slots: +0.0 from part 0, -0.0 (the identity of the parts' sum) from the others
+            k_fill3<<<(nslots + 255) / 256, 256, 0, st>>>(ax, ay, az, nslots, part == 0 ? 0. : -0.);
             NCG_LAUNCHED();
       }
       int n = 0;
@@ -779,13 +795,16 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
             k_pack_exact<<<(npad + 255) / 256, 256, 0, st>>>(cv, c.cidx, n, npad, G, src, c.srcR);
             NCG_LAUNCHED();
             int nb = (n + EXB - 1) / EXB;
+            const int p_lo = (int)((long)n * part / nparts), p_hi = (int)((long)n * (part + 1) / nparts);
             NCG_CK(cudaEventRecord(c.kev0, st));
             if (soft)
                   k_grav_exact<true><<<nb, EXB, 0, st>>>(src, c.srcR, c.cidx, n, ntiles, cmh[0], cmh[1], cmh[2], mu,
-                                                         sp, central, j2, cv, ax, ay, az, c.cmterm, c.err);
+                                                         sp, central, j2, cv, p_lo, p_hi, ax, ay, az, c.cmterm,
+                                                         c.err);
             else
                   k_grav_exact<false><<<nb, EXB, 0, st>>>(src, c.srcR, c.cidx, n, ntiles, cmh[0], cmh[1], cmh[2],
-                                                          mu, sp, central, j2, cv, ax, ay, az, c.cmterm, c.err);
+                                                          mu, sp, central, j2, cv, p_lo, p_hi, ax, ay, az, c.cmterm,
+                                                          c.err);
             NCG_LAUNCHED();
             NCG_CK(cudaEventRecord(c.kev1, st));
             c.kev_valid = 1;
@@ -828,8 +847,11 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
             NCG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sm ? k_grav_tiled<0, 2> : k_grav_tiled<0, 0>, MXB, 0));
       else
             NCG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sm ? k_grav_tiled<1, 2> : k_grav_tiled<1, 0>, MXB, 0));
+      // this part's target blocks
+      const int ib_lo = (int)((long)ntiles * part / nparts), ib_hi = (int)((long)ntiles * (part + 1) / nparts);
+      const int nblk = ib_hi - ib_lo;
       const long want = (long)max(occ, 1) * c.sm_count * c.grav_slots_mult;
-      long nch = (want + ntiles - 1) / ntiles;
+      long nch = (want + max(nblk, 1) - 1) / max(nblk, 1);
       if (nch < 1) nch = 1;
       if (nch > ntiles) nch = ntiles;
       int nchunks = (int)nch;
@@ -851,23 +873,26 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
             }
       }
       double theta = P.par_near_theta > 0. ? P.par_near_theta : 0.15;
-      dim3 grid(nchunks, ntiles);
+      dim3 grid(nchunks, nblk);
       const float *s32 = (const float *)c.src32;
       NCG_CK(cudaEventRecord(c.kev0, st));
 #define NCG_TILED(MODE_, SOFT_)                                                                              \
       k_grav_tiled<MODE_, SOFT_><<<grid, MXB, 0, st>>>(s64, c.srcR, s32, c.srcR32, c.tilebox, n, ntiles, tpc, \
-                                                      theta, eps2, c.partial, npad, c.err, c.red + 6, sp)
-      if (mode == NCGPU_GRAVITY_MIXED) {
-            if (soft_kind == 0) NCG_TILED(0, 0); else if (soft_kind == 1) NCG_TILED(0, 1); else NCG_TILED(0, 2);
-      } else {
-            if (soft_kind == 0) NCG_TILED(1, 0); else if (soft_kind == 1) NCG_TILED(1, 1); else NCG_TILED(1, 2);
+                                                      theta, eps2, c.partial, npad, c.err, c.red + 6, sp, ib_lo)
+      if (nblk > 0) {  // (a part without target blocks has only the central terms below)
+            if (mode == NCGPU_GRAVITY_MIXED) {
+                  if (soft_kind == 0) NCG_TILED(0, 0); else if (soft_kind == 1) NCG_TILED(0, 1); else NCG_TILED(0, 2);
+            } else {
+                  if (soft_kind == 0) NCG_TILED(1, 0); else if (soft_kind == 1) NCG_TILED(1, 1); else NCG_TILED(1, 2);
+            }
+            NCG_LAUNCHED();
       }
 #undef NCG_TILED
-      NCG_LAUNCHED();
       NCG_CK(cudaEventRecord(c.kev1, st));
       c.kev_valid = 1;
       k_grav_final<<<(n + 255) / 256, 256, 0, st>>>(c.partial, nchunks, npad, s64, c.vals, n, cmh[0], cmh[1], cmh[2],
-                                                    mu, G, central, j2, ax, ay, az, c.cmterm);
+                                                    mu, G, central, j2, ib_lo * T, min(n, ib_hi * T), ax, ay, az,
+                                                    c.cmterm);
       NCG_LAUNCHED();
       if (central) {
             const int np = min(128, (n + RB - 1) / RB);
@@ -896,7 +921,7 @@ int gravity_exact_into(const BodyView &bv, int largest_id, const double *cmh, do
 {
       const int nslots = largest_id + 1;
       if (nslots > 0) {
-            k_zero3<<<(nslots + 255) / 256, 256, 0, st>>>(ax, ay, az, nslots);
+            k_fill3<<<(nslots + 255) / 256, 256, 0, st>>>(ax, ay, az, nslots, 0.);
             NCG_LAUNCHED();
       }
       int n = 0;
@@ -915,10 +940,10 @@ int gravity_exact_into(const BodyView &bv, int largest_id, const double *cmh, do
       const int nb = (n + EXB - 1) / EXB;
       if (sp != 0.)
             k_grav_exact<true><<<nb, EXB, 0, st>>>(s4, srcR, cidx, n, ntiles, cmh[0], cmh[1], cmh[2], mu, sp, central,
-                                                   j2, bv, ax, ay, az, cterm, err);
+                                                   j2, bv, 0, n, ax, ay, az, cterm, err);
       else
             k_grav_exact<false><<<nb, EXB, 0, st>>>(s4, srcR, cidx, n, ntiles, cmh[0], cmh[1], cmh[2], mu, sp,
-                                                    central, j2, bv, ax, ay, az, cterm, err);
+                                                    central, j2, bv, 0, n, ax, ay, az, cterm, err);
       NCG_LAUNCHED();
       if (central) {
             k_seq_sum3<<<1, 96, 0, st>>>(cterm, j2.on ? 2 * n : n, nullptr, d_cm_acc);
