@@ -192,12 +192,12 @@ MESH_WORKLOAD = ("mesh collision search + mesh gravity, N=1,048,576 disk (a~U[0.
                  "collision_cube_min 4.4 (mesh size >= 2 x max radius), instant mergers, dt=5e-4")
 
 
-def mesh_params(mode, cells=1024):
+def mesh_params(mode, cells=1024, **extra):
     from ncorpion_b200 import api
     return api.default_params(G=1.0, softening_parameter=0.0, collision_bool=1, brute_force_bool=0, mesh_bool=1,
                               collision_type=api.COLLISION_MERGER, collision_cube_cells=cells,
                               how_many_neighbours=16.0, collision_cube_min=4.4, gravity_mode=mode,
-                              disruption_threshold=0.1, high_dumping_threshold=100.0)
+                              disruption_threshold=0.1, high_dumping_threshold=100.0, **extra)
 
 
 def mesh_gamma0(n, cells=1024):
@@ -207,15 +207,16 @@ def mesh_gamma0(n, cells=1024):
     return max(gam, 4.4 / cells)
 
 
-def bench_mesh(lib, api, torch, mode, steps, warmup, n_bodies=None, cells=1024):
+def bench_mesh(lib, api, torch, mode, steps, warmup, n_bodies=None, cells=1024, **extra):
     """Steps/s of the mesh integrator loop on the device state, CUDA events on
-    the library stream; the half kick of integration_mesh first."""
+    the library stream; the half kick of integration_mesh first.  `extra`:
+    further parameters (the central body's J2 and tides)."""
     from ncorpion_b200 import disks
     n_bodies = n_bodies or MESH_N
     b = disks.mesh_disk(n_bodies, seed=0)
     ex = np.ones(n_bodies, np.int32)
     cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
-    api.init(n_bodies + n_bodies // 20, mesh_params(mode, cells))
+    api.init(n_bodies + n_bodies // 20, mesh_params(mode, cells, **extra))
     api.upload(b, ex, cm)
     gmin = 4.4 / cells
     gam = mesh_gamma0(n_bodies, cells)
@@ -247,6 +248,31 @@ def bench_mesh(lib, api, torch, mode, steps, warmup, n_bodies=None, cells=1024):
     t = float(np.sum(ms)) / 1e3
     return {"steps_per_s": steps / t, "ms_per_step": 1e3 * t / steps, "steps": steps, "events": events,
             "pairs_per_step": pairs / steps, "bodies_end": hm, "gpu_launches": launches}
+
+
+CENTRAL_N = 262144
+CENTRAL_WORKLOAD = ("mesh steps (fast mode) of the N=262,144 mesh disk, 512 cells per side, alone, with the "
+                    "fluid-body J2 (J2_value 0, Tearth 25), and with tides raised on the central body besides "
+                    "(k2 1.5, Delta_t 1e-3, dimensionless_moi 0.3307)")
+
+
+def bench_central(lib, api, torch, steps=20):
+    """The central body's J2 and tides in the mesh loop: their cost per step,
+    and the sequential SideralOmega recurrence of the tides per body."""
+    j2 = dict(J2_bool=1, J2=0.0, sideral_omega=2.0 * np.pi / 25.0)
+    tides = dict(central_tides_bool=1, k2=1.5, Delta_t=1e-3, dimensionless_moi=0.3307)
+    runs = {"plain": bench_mesh(lib, api, torch, api.GRAVITY_MIXED, steps, 3, CENTRAL_N, 512),
+            "j2": bench_mesh(lib, api, torch, api.GRAVITY_MIXED, steps, 3, CENTRAL_N, 512, **j2),
+            "j2_tides": bench_mesh(lib, api, torch, api.GRAVITY_MIXED, steps, 3, CENTRAL_N, 512, **j2, **tides)}
+    out = {"metric": "mesh steps/s with the central body's J2 and tides", "workload": CENTRAL_WORKLOAD}
+    for k, v in runs.items():
+        out[k] = {"steps_per_s": v["steps_per_s"], "ms_per_step": v["ms_per_step"]}
+    tides_ms = runs["j2_tides"]["ms_per_step"] - runs["j2"]["ms_per_step"]
+    out["tides_ms_per_kick"] = tides_ms
+    out["tides_ns_per_body"] = tides_ms * 1e6 / CENTRAL_N
+    out["note"] = ("the tides' SideralOmega recurrence is sequential (one warp: 11 dependent FP64 operations and "
+                   "a division per body); J2 adds O(N) work to the kick")
+    return out
 
 
 FRAG_N = 262144
@@ -410,6 +436,7 @@ def main(argv=None):
     ap.add_argument("--no-frag", action="store_true")
     ap.add_argument("--no-bf", action="store_true", help="skip the N=2,000 brute-force collisional section")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint section")
+    ap.add_argument("--no-central", action="store_true", help="skip the J2 / tides section")
     ap.add_argument("--mesh-n", type=int, default=MESH_N, help="mesh workload bodies (smaller cases for profiling)")
     ap.add_argument("--mesh-cells", type=int, default=1024)
     ap.add_argument("--mesh-steps", type=int, default=MESH_STEPS)
@@ -583,6 +610,7 @@ def main(argv=None):
                                                          and a.mesh_n == MESH_N) else None}
     bf = None if a.no_bf else bench_bf_collide(lib, api, torch, rank == 0 and ws == 1 and not a.no_cpu_baseline)
     adjoint = None if a.no_adjoint else bench_adjoint(lib, api, torch)
+    central = None if a.no_central else bench_central(lib, api, torch)
     frag = None
     if not a.no_frag:
         fm = bench_fragment(lib, api, torch, api.GRAVITY_MIXED, FRAG_STEPS)
@@ -642,6 +670,7 @@ def main(argv=None):
             "fragment": frag,
             "brute_force_collisional": bf,
             "adjoint": adjoint,
+            "central_body": central,
             "accuracy": {"mutual_rel_err_max": float(rel_mut.max()),
                          "mutual_rel_err_median": float(np.median(rel_mut)),
                          "total_rel_err_max": float(rel_tot.max()),

@@ -220,6 +220,9 @@ int ncgpu_probe_wait_timeout(int probes, double *cycles_per_probe);
 /* Diagnostic: out[i] = x[i]^(1.0/3.0), correctly rounded, as the device
    merger computes the merged radius (src/physics.c:684). */
 int ncgpu_probe_pow_third(const double *x, double *out, int n);
+/* a[i] / b[i] with the correctly rounded division of the tides' recurrence
+   (reciprocal and two residual corrections), for tests.  Host buffers. */
+int ncgpu_probe_div(const double *a, const double *b, double *out, int n);
 
 /* ---- device-resident integrator state ------------------------------------ */
 

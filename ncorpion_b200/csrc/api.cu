@@ -101,6 +101,17 @@ __global__ void k_soa_to_aos(double *__restrict__ aos, int n, const double *x, c
       b[6] = m[i]; b[7] = R[i];
 }
 
+// (ax, ay, az) blocks -> xyz triples out[3k + d]
+__global__ void k_interleave3(const double *__restrict__ ax, const double *__restrict__ ay,
+                              const double *__restrict__ az, long n, double *__restrict__ out)
+{
+      const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+      if (k >= n) return;
+      out[3 * k] = ax[k];
+      out[3 * k + 1] = ay[k];
+      out[3 * k + 2] = az[k];
+}
+
 // kick, src/rk4.c:96-105: v += timestep * a for existing bodies, then the
 // central mass with CM_acc.  Explicit _rn operations: no FMA contraction.
 __global__ void k_kick(const int *__restrict__ ex, int n, double dt, const double *__restrict__ ax,
@@ -445,14 +456,10 @@ int ncgpu_vector_field_part(const double *d_bodies, const int *d_exists, int lar
       const J2Arg j2 = j2_arg(c.P, cm->mass, j2_value(c.P, cm->mass, c.P.par_sideral_omega));
       NCG_TRY(gravity_eval(bv, largest_id, (const double *)cm, j2, c.acc, c.n_max, d_cm_acc, gravity_mode, st, part,
                            nparts));
-      if (bs > 0) {
-            // interleave into d_acc[3*k + d]
-            NCG_CK(cudaMemcpy2DAsync(d_acc, 3 * sizeof(double), c.acc, sizeof(double), sizeof(double), bs,
-                                     cudaMemcpyDeviceToDevice, st));
-            NCG_CK(cudaMemcpy2DAsync(d_acc + 1, 3 * sizeof(double), c.acc + c.n_max, sizeof(double),
-                                     sizeof(double), bs, cudaMemcpyDeviceToDevice, st));
-            NCG_CK(cudaMemcpy2DAsync(d_acc + 2, 3 * sizeof(double), c.acc + 2 * (size_t)c.n_max, sizeof(double),
-                                     sizeof(double), bs, cudaMemcpyDeviceToDevice, st));
+      if (bs > 0) {  // interleave into d_acc[3*k + d]
+            k_interleave3<<<(int)((bs + 255) / 256), 256, 0, st>>>(c.acc, c.acc + c.n_max, c.acc + 2 * (size_t)c.n_max,
+                                                                  bs, d_acc);
+            NCG_LAUNCHED();
       }
       return NCGPU_OK;
 }

@@ -87,6 +87,69 @@ __device__ __forceinline__ void d_j2(const J2Arg &j, double mu, double DX, doubl
       c[2] = __ddiv_rn(__dmul_rn(__dmul_rn(K, __dsub_rn(__dmul_rn(4.5, DZ), qz)), mk), j.M);
 }
 
+// x / b correctly rounded (round to nearest even) from y = RN(1/b), with
+// Markstein's residual correction (P. Markstein, IBM J. Res. Dev. 34 (1990)
+// 111-119; J.-M. Muller et al., Handbook of Floating-Point Arithmetic, ch. 4)
+// applied twice: r = x - b q is exact when q is within an ulp of x/b, and then
+// RN(q + r y) = RN(x/b); the first correction brings RN(x y) within that ulp.
+// Valid for finite nonzero b with the quotient and residuals in the normal
+// range; a zero x gives x * y, a zero with the quotient's sign.  A short
+// dependent chain (one multiply, four FMAs) for the latency-bound recurrences
+// that need the quotient; the reciprocal is computed off the chain.
+__device__ __forceinline__ double div_by_recip(double x, double b, double y)
+{
+      if (x == 0.) return __dmul_rn(x, y);
+      double q = __dmul_rn(x, y);
+      double r = __fma_rn(-q, b, x);
+      q = __fma_rn(r, y, q);
+      r = __fma_rn(-q, b, x);
+      return __fma_rn(r, y, q);
+}
+
+// Sequential FP64 sum s + t[0] + t[1] + ... + t[n-1], in that order with IEEE
+// rounding, by one warp (the result is lane 0's): the lanes stage CHN terms at
+// a time in shared memory (`stage`, CHN doubles, 16-byte aligned) with
+// coalesced loads, the next block in flight while lane 0 adds, two terms per
+// shared load.  Launched as one warp per CTA, so that every chain has an SM's
+// FP64 pipe to itself.
+constexpr int CHN = 512;
+__device__ __forceinline__ double warp_chain_sum(const double *__restrict__ t, long n, double s, double *stage)
+{
+      const int lane = threadIdx.x & 31;
+      double v[CHN / 32];
+#pragma unroll
+      for (int u = 0; u < CHN / 32; u++) {
+            const long k = (long)u * 32 + lane;
+            v[u] = k < n ? t[k] : 0.;
+      }
+      for (long base = 0; base < n; base += CHN) {
+#pragma unroll
+            for (int u = 0; u < CHN / 32; u++) stage[u * 32 + lane] = v[u];
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < CHN / 32; u++) {  // the next block, in flight during the sums
+                  const long k = base + CHN + (long)u * 32 + lane;
+                  v[u] = k < n ? t[k] : 0.;
+            }
+            if (lane == 0) {
+                  const long m = n - base < CHN ? n - base : CHN;
+                  if (m == CHN) {  // full block: fixed trip count
+                        const double2 *st2 = reinterpret_cast<const double2 *>(stage);
+#pragma unroll 16
+                        for (int q = 0; q < CHN / 2; q++) {
+                              const double2 pr = st2[q];
+                              s = __dadd_rn(s, pr.x);
+                              s = __dadd_rn(s, pr.y);
+                        }
+                  } else {
+                        for (int q = 0; q < m; q++) s = __dadd_rn(s, stage[q]);
+                  }
+            }
+            __syncwarp();
+      }
+      return s;
+}
+
 // Device error word bits (set by kernels instead of trapping).
 enum : unsigned {
       ERR_CAPACITY = 1u,
@@ -248,6 +311,9 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cm_host8, con
 // Sequential FP64 sums, in index order, of the 3 arrays terms[c*n .. c*n + n),
 // starting from init[c] (0 when init is null); out may alias init.
 int seq_sum3(const double *terms, int n, const double *init, double *out, cudaStream_t st);
+// The same sums as a deterministic two-level parallel reduction (non-exact
+// gravity modes), added to init[c] at the end.
+int par_sum3(const double *terms, int n, const double *init, double *out, cudaStream_t st);
 
 // tides (src/physics.c:496-542) on the device state after the vector field
 // (tides.cu): acc blocks of n_max and the device CM_acc receive the tidal
@@ -270,6 +336,9 @@ int scan_exclusive(const int *in, int *out, int n, int *sums, cudaStream_t st);
 // Stream compaction of existing slots 0..largest_id into ctx().cidx (ascending).
 // Returns the count through *n_host (synchronises).
 int compact_existing(const int *ex, int largest_id, int *n_host, cudaStream_t st);
+// The same compaction without the synchronisation: the count stays in
+// ctx().n_dev[0].
+int compact_existing_dev(const int *ex, int largest_id, cudaStream_t st);
 
 // Compaction of flagged slots with caller-provided scratch (no library context).
 int compact_flags_into(const int *flags, int n_slots, int *blockcnt, int *n_dev, int *out_idx, int *n_host,

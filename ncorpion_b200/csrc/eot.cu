@@ -96,29 +96,20 @@ __device__ __forceinline__ double momentum_init(int d, const double *cm, int cen
 }
 
 // total_momentum (src/structure.c:1193-1227) in the reference's order: one
-// warp per component sums its n terms sequentially (FP64, no reassociation);
-// the warp stages CHM terms at a time in shared memory with coalesced loads so
-// the dependent adds do not wait on global memory.
-constexpr int CHM = 512;
-__global__ void __launch_bounds__(224) k_momentum_chains(const double *__restrict__ terms, int n,
-                                                         const double *__restrict__ cm, int central,
-                                                         double *__restrict__ com)
+// CTA (one warp) per component sums its n terms sequentially (FP64, no
+// reassociation, warp_chain_sum) into tot[0..6]; k_momentum_div divides.
+__global__ void __launch_bounds__(32) k_momentum_chains(const double *__restrict__ terms, int n,
+                                                        const double *__restrict__ cm, int central,
+                                                        double *__restrict__ tot)
 {
-      __shared__ double buf[7][CHM];
-      __shared__ double tot[7];
-      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-      const double *t = terms + (size_t)w * n;
-      double s = momentum_init(w, cm, central);
-      for (int base = 0; base < n; base += CHM) {
-            const int cnt = min(CHM, n - base);
-            for (int i = lane; i < cnt; i += 32) buf[w][i] = t[base + i];
-            __syncwarp();
-            if (lane == 0)
-                  for (int i = 0; i < cnt; i++) s = DADD(s, buf[w][i]);
-            __syncwarp();
-      }
-      if (lane == 0) tot[w] = s;
-      __syncthreads();
+      __shared__ __align__(16) double stage[CHN];
+      const int w = blockIdx.x;
+      const double s = warp_chain_sum(terms + (size_t)w * n, n, momentum_init(w, cm, central), stage);
+      if (threadIdx.x == 0) tot[w] = s;
+}
+
+__global__ void k_momentum_div(const double *__restrict__ tot, double *__restrict__ com)
+{
       if (threadIdx.x < 6) com[threadIdx.x] = DDIV(tot[threadIdx.x], tot[6]);
 }
 
@@ -237,7 +228,9 @@ int eot_state(int *hm_out)
                   k_momentum_terms<<<(n + 255) / 256, 256, 0, st>>>(S, c.cidx, n, terms);
                   NCG_LAUNCHED();
                   if (P.par_gravity_mode == NCGPU_GRAVITY_EXACT) {
-                        k_momentum_chains<<<1, 224, 0, st>>>(terms, n, c.cm, P.par_central_mass_bool, com);
+                        k_momentum_chains<<<7, 32, 0, st>>>(terms, n, c.cm, P.par_central_mass_bool, com + 8);
+                        NCG_LAUNCHED();
+                        k_momentum_div<<<1, 32, 0, st>>>(com + 8, com);
                         NCG_LAUNCHED();
                   } else {
                         const int np = std::min(148, (n + MPB - 1) / MPB);

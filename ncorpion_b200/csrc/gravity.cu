@@ -177,52 +177,17 @@ __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, 
       }
 }
 
-// CM_acc += G*mk*DX/r3 in slot order (src/physics.c:137-139): one thread per
-// component, sequential, so the FP64 result matches the reference bit for bit.
-// Sequential FP64 sums of the 3 arrays cterm[c*n .. c*n + n), in index order
-// (CM_acc of the exact mode).  One warp per array: the warp stages CHS terms at
-// a time in shared memory with coalesced loads, the next block loading while
-// lane 0 adds, so the dependent adds do not wait on global memory.
-constexpr int CHS = 512;
-__global__ void __launch_bounds__(96) k_seq_sum3(const double *__restrict__ cterm, int n, const double *init,
+// CM_acc += G*mk*DX/r3 in slot order (src/physics.c:137-139): sequential FP64
+// sums of the 3 arrays cterm[c*n .. c*n + n), in index order, from init[c] (0
+// without init), one CTA (one warp) per component, so the result matches the
+// reference bit for bit.  out may alias init.
+__global__ void __launch_bounds__(32) k_seq_sum3(const double *__restrict__ cterm, int n, const double *init,
                                                  double *out)
 {
-      __shared__ __align__(16) double stage[3][CHS];
-      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-      const double *t = cterm + (size_t)w * n;
-      double s = init ? init[w] : 0.;
-      double v[CHS / 32];
-#pragma unroll
-      for (int u = 0; u < CHS / 32; u++) {
-            const int k = u * 32 + lane;
-            v[u] = k < n ? t[k] : 0.;
-      }
-      for (int base = 0; base < n; base += CHS) {
-#pragma unroll
-            for (int u = 0; u < CHS / 32; u++) stage[w][u * 32 + lane] = v[u];
-            __syncwarp();
-#pragma unroll
-            for (int u = 0; u < CHS / 32; u++) {
-                  const int k = base + CHS + u * 32 + lane;
-                  v[u] = k < n ? t[k] : 0.;
-            }
-            if (lane == 0) {
-                  const int m = min(CHS, n - base);
-                  if (m == CHS) {
-                        const double2 *st2 = reinterpret_cast<const double2 *>(stage[w]);
-#pragma unroll 16
-                        for (int q = 0; q < CHS / 2; q++) {
-                              const double2 pr = st2[q];
-                              s = __dadd_rn(s, pr.x);
-                              s = __dadd_rn(s, pr.y);
-                        }
-                  } else {
-                        for (int q = 0; q < m; q++) s = __dadd_rn(s, stage[w][q]);
-                  }
-            }
-            __syncwarp();
-      }
-      if (lane == 0) out[w] = s;
+      __shared__ __align__(16) double stage[CHN];
+      const int w = blockIdx.x;
+      const double s = warp_chain_sum(cterm + (size_t)w * n, n, init ? init[w] : 0., stage);
+      if (threadIdx.x == 0) out[w] = s;
 }
 
 // ------------------------------------------------------------ tiled modes --
@@ -230,9 +195,11 @@ __global__ void __launch_bounds__(96) k_seq_sum3(const double *__restrict__ cter
 constexpr int RB = 256;
 
 // bounding box (lo xyz, hi xyz) and radius range (min, max) of the existing bodies
-__global__ void k_bbox_part(BodyView bv, const int *__restrict__ cidx, int n, double *__restrict__ part)
+__global__ void k_bbox_part(BodyView bv, const int *__restrict__ cidx, const int *__restrict__ n_dev,
+                            double *__restrict__ part)
 {
       __shared__ double sh[8][RB];
+      const int n = *n_dev;
       double lo[4] = {1e300, 1e300, 1e300, 1e300}, hi[4] = {-1e300, -1e300, -1e300, -1e300};
       for (int p = blockIdx.x * RB + threadIdx.x; p < n; p += gridDim.x * RB) {
             long s = (long)cidx[p] * bv.stride;
@@ -261,15 +228,26 @@ __global__ void k_bbox_part(BodyView bv, const int *__restrict__ cidx, int n, do
       if (threadIdx.x < 8) part[blockIdx.x * 8 + threadIdx.x] = sh[threadIdx.x][0];
 }
 
-__global__ void k_bbox_final(double *__restrict__ part, int nparts)
+// Folds the (at most 256) block partials: lo xyz, hi xyz, R min, R max in part[0..7].
+__global__ void __launch_bounds__(256) k_bbox_final(double *__restrict__ part, int nparts)
 {
-      int d = threadIdx.x;
-      if (d >= 8) return;
-      const bool mx = d == 3 || d == 4 || d == 5 || d == 7;
-      double v = part[d];
-      for (int b = 1; b < nparts; b++) v = mx ? fmax(v, part[b * 8 + d]) : fmin(v, part[b * 8 + d]);
-      __syncwarp(0xffu);
-      part[d] = v;  // lo xyz, hi xyz, R min, R max in part[0..7]
+      __shared__ double sh[8][256];
+      const int t = threadIdx.x;
+      for (int d = 0; d < 8; d++) {
+            const bool mx = d == 3 || d == 4 || d == 5 || d == 7;
+            sh[d][t] = t < nparts ? part[t * 8 + d] : (mx ? -1e300 : 1e300);
+      }
+      __syncthreads();
+      for (int o = 128; o > 0; o >>= 1) {
+            if (t < o)
+                  for (int d = 0; d < 8; d++) {
+                        const bool mx = d == 3 || d == 4 || d == 5 || d == 7;
+                        const double a = sh[d][t], b = sh[d][t + o];
+                        sh[d][t] = mx ? fmax(a, b) : fmin(a, b);
+                  }
+            __syncthreads();
+      }
+      if (t < 8) part[t] = sh[t][0];
 }
 
 __device__ __forceinline__ uint32_t spread3(uint32_t v)
@@ -726,13 +704,16 @@ __global__ void k_sum3_part(const double *__restrict__ v, int n, double *__restr
       if (threadIdx.x < 3) part[blockIdx.x * 3 + threadIdx.x] = sh[threadIdx.x][0];
 }
 
-__global__ void k_sum3_final(const double *__restrict__ part, int nparts, double *__restrict__ out)
+// One warp per component, a fixed-shape (deterministic) fold of the partials,
+// plus init[d] when given (out may alias init).
+__global__ void k_sum3_final(const double *__restrict__ part, int nparts, const double *init, double *out)
 {
-      int d = threadIdx.x;
+      const int d = threadIdx.x >> 5, lane = threadIdx.x & 31;
       if (d >= 3) return;
       double s = 0.;
-      for (int b = 0; b < nparts; b++) s += part[b * 3 + d];
-      out[d] = s;
+      for (int b = lane; b < nparts; b += 32) s += part[b * 3 + d];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) out[d] = init ? init[d] + s : s;
 }
 
 __global__ void k_fill3(double *__restrict__ ax, double *__restrict__ ay, double *__restrict__ az, int n, double v)
@@ -754,9 +735,20 @@ __global__ void k_set3(double *__restrict__ out, double a, double b, double c)
 
 }  // namespace
 
+int par_sum3(const double *terms, int n, const double *init, double *out, cudaStream_t st)
+{
+      Ctx &c = ctx();
+      const int np = min(128, max(1, (n + RB - 1) / RB));
+      k_sum3_part<<<np, RB, 0, st>>>(terms, n, c.red + 2048);
+      NCG_LAUNCHED();
+      k_sum3_final<<<1, 96, 0, st>>>(c.red + 2048, np, init, out);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
+
 int seq_sum3(const double *terms, int n, const double *init, double *out, cudaStream_t st)
 {
-      k_seq_sum3<<<1, 96, 0, st>>>(terms, n, init, out);
+      k_seq_sum3<<<3, 32, 0, st>>>(terms, n, init, out);
       NCG_LAUNCHED();
       return NCGPU_OK;
 }
@@ -776,7 +768,22 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
             NCG_LAUNCHED();
       }
       int n = 0;
-      NCG_TRY(compact_existing(bv.ex, largest_id, &n, st));
+      const bool tiled = mode == NCGPU_GRAVITY_FP64 || mode == NCGPU_GRAVITY_MIXED;
+      double rr[2] = {0., 0.};  // radius range of the existing bodies (tiled modes)
+      if (!tiled) {
+            NCG_TRY(compact_existing(bv.ex, largest_id, &n, st));
+      } else if (nslots > 0) {
+            // compaction, bounding box and radius range behind one synchronisation
+            NCG_TRY(compact_existing_dev(bv.ex, largest_id, st));
+            const int nbb = min(256, (nslots + RB - 1) / RB);
+            k_bbox_part<<<nbb, RB, 0, st>>>(bv, c.cidx, c.n_dev, c.red);
+            NCG_LAUNCHED();
+            k_bbox_final<<<1, 256, 0, st>>>(c.red, nbb);
+            NCG_LAUNCHED();
+            NCG_CK(cudaMemcpyAsync(&n, c.n_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaMemcpyAsync(rr, c.red + 6, sizeof rr, cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaStreamSynchronize(st));
+      }
       const int central = P.par_central_mass_bool;
       const double G = P.par_G;
       const double mu = G * cmh[6];
@@ -809,7 +816,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
             NCG_CK(cudaEventRecord(c.kev1, st));
             c.kev_valid = 1;
             if (central) {
-                  k_seq_sum3<<<1, 96, 0, st>>>(c.cmterm, j2.on ? 2 * n : n, nullptr, d_cm_acc);
+                  k_seq_sum3<<<3, 32, 0, st>>>(c.cmterm, j2.on ? 2 * n : n, nullptr, d_cm_acc);
             } else {
                   k_set3<<<1, 1, 0, st>>>(d_cm_acc, 0., 0., 0.);
             }
@@ -818,12 +825,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
       }
       if (mode != NCGPU_GRAVITY_FP64 && mode != NCGPU_GRAVITY_MIXED) return NCGPU_E_ARG;
 
-      // Morton ordering of the existing bodies
-      const int nbb = min(256, (n + RB - 1) / RB);
-      k_bbox_part<<<nbb, RB, 0, st>>>(cv, c.cidx, n, c.red);
-      NCG_LAUNCHED();
-      k_bbox_final<<<1, 32, 0, st>>>(c.red, nbb);
-      NCG_LAUNCHED();
+      // Morton ordering of the existing bodies (bounding box from above)
       k_morton<<<(n + 255) / 256, 256, 0, st>>>(cv, c.cidx, n, c.red, c.keys, c.vals);
       NCG_LAUNCHED();
       NCG_TRY(radix_sort_pairs(c.keys, c.vals, n, 30, st));
@@ -863,9 +865,6 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
       if (sm == 2) {
             // all radii equal (the bounding-box pass found R_min == R_max): the
             // uniform-epsilon instance, with fewer registers
-            double rr[2];
-            NCG_CK(cudaMemcpyAsync(rr, c.red + 6, sizeof rr, cudaMemcpyDeviceToHost, st));
-            NCG_CK(cudaStreamSynchronize(st));
             if (rr[0] == rr[1]) {
                   const double eu = 2.0 * sp * rr[0];
                   eps2 = eu * eu;
@@ -898,7 +897,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
             const int np = min(128, (n + RB - 1) / RB);
             k_sum3_part<<<np, RB, 0, st>>>(c.cmterm, n, c.red + 2048);
             NCG_LAUNCHED();
-            k_sum3_final<<<1, 32, 0, st>>>(c.red + 2048, np, d_cm_acc);
+            k_sum3_final<<<1, 96, 0, st>>>(c.red + 2048, np, nullptr, d_cm_acc);
       } else {
             k_set3<<<1, 1, 0, st>>>(d_cm_acc, 0., 0., 0.);
       }
@@ -946,7 +945,7 @@ int gravity_exact_into(const BodyView &bv, int largest_id, const double *cmh, do
                                                     central, j2, bv, 0, n, ax, ay, az, cterm, err);
       NCG_LAUNCHED();
       if (central) {
-            k_seq_sum3<<<1, 96, 0, st>>>(cterm, j2.on ? 2 * n : n, nullptr, d_cm_acc);
+            k_seq_sum3<<<3, 32, 0, st>>>(cterm, j2.on ? 2 * n : n, nullptr, d_cm_acc);
             NCG_LAUNCHED();
       }
       return NCGPU_OK;

@@ -476,8 +476,8 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
 }
 
 // Bodies 0..2 and CM_acc.  Chain w (0..8: body w/3, component w%3; 9..11:
-// CM_acc components) sums its terms in slot order.  exact: one warp per chain,
-// coalesced loads of 32 terms handed to the chain through shuffles, so the
+// CM_acc components) sums its terms in slot order.  exact: one CTA (one warp)
+// per chain staging the terms through shared memory (warp_chain_sum), so the
 // FP64 sum is the reference's sequential one (a body that does not exist adds
 // +0.0, which leaves any sum other than -0.0 unchanged).  Body i's chain starts
 // from its central term, CM_acc from 0.
@@ -493,51 +493,21 @@ __device__ __forceinline__ bool chain_live(int w, const DevState &S, const MGArg
       return w >= 9 ? A.central : (S.ex[w / 3] && A.mutual);
 }
 
-constexpr int CHB = 512;  // terms staged per warp and block
-__global__ void __launch_bounds__(384) k_mesh_chains(DevState S, MGArgs A, const double *__restrict__ terms, long N,
-                                                     const double *__restrict__ ax, const double *__restrict__ ay,
-                                                     const double *__restrict__ az, double *__restrict__ tot)
+__global__ void __launch_bounds__(32) k_mesh_chains(DevState S, MGArgs A, const double *__restrict__ terms, long N,
+                                                    const double *__restrict__ ax, const double *__restrict__ ay,
+                                                    const double *__restrict__ az, double *__restrict__ tot)
 {
-      __shared__ __align__(16) double stage[12][CHB];
-      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      __shared__ __align__(16) double stage[CHN];
+      const int w = blockIdx.x;  // one chain per CTA
       double s = chain_init(w, ax, ay, az);
       if (chain_live(w, S, A)) {
-            const double *t = w >= 9 ? cm_chain(const_cast<double *>(terms), A, N, w - 9) : terms + (size_t)w * N;
             const int k0 = w >= 9 ? 0 : 3;
-            const int n = w >= 9 ? (A.j2.on ? 2 : 1) * (A.lid + 1) : A.lid + 1;
-            double v[CHB / 32];
-#pragma unroll
-            for (int u = 0; u < CHB / 32; u++) {
-                  const int k = k0 + u * 32 + lane;
-                  v[u] = k < n ? t[k] : 0.;
-            }
-            for (int base = k0; base < n; base += CHB) {
-#pragma unroll
-                  for (int u = 0; u < CHB / 32; u++) stage[w][u * 32 + lane] = v[u];
-                  __syncwarp();
-#pragma unroll
-                  for (int u = 0; u < CHB / 32; u++) {  // next block in flight during the sums
-                        const int k = base + CHB + u * 32 + lane;
-                        v[u] = k < n ? t[k] : 0.;
-                  }
-                  if (lane == 0) {
-                        const int m = min(CHB, n - base);
-                        if (m == CHB) {  // full block: fixed trip count, two terms per shared load
-                              const double2 *st2 = reinterpret_cast<const double2 *>(stage[w]);
-#pragma unroll 16
-                              for (int q = 0; q < CHB / 2; q++) {
-                                    const double2 pr = st2[q];
-                                    s = DADD(s, pr.x);
-                                    s = DADD(s, pr.y);
-                              }
-                        } else {
-                              for (int q = 0; q < m; q++) s = DADD(s, stage[w][q]);
-                        }
-                  }
-                  __syncwarp();
-            }
+            const double *t =
+                w >= 9 ? cm_chain(const_cast<double *>(terms), A, N, w - 9) : terms + (size_t)w * N + k0;
+            const long n = w >= 9 ? (long)(A.j2.on ? 2 : 1) * (A.lid + 1) : (long)A.lid + 1 - k0;
+            s = warp_chain_sum(t, n > 0 ? n : 0, s, stage);
       }
-      if (lane == 0) tot[w] = s;
+      if (threadIdx.x == 0) tot[w] = s;
 }
 
 // Non-exact modes: deterministic two-level sums of the same 12 chains.
@@ -573,15 +543,17 @@ __global__ void k_mesh_chains_part(DevState S, MGArgs A, const double *__restric
       }
 }
 
+// One warp per chain: a fixed-shape (deterministic) fold of the block partials.
 __global__ void k_mesh_chains_fold(DevState S, MGArgs A, const double *__restrict__ part, int nparts,
                                    const double *__restrict__ ax, const double *__restrict__ ay,
                                    const double *__restrict__ az, double *__restrict__ tot)
 {
-      const int w = threadIdx.x;
+      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       if (w >= 12) return;
       double s = 0.;
-      for (int b = 0; b < nparts; b++) s += part[12 * b + w];
-      tot[w] = chain_live(w, S, A) ? chain_init(w, ax, ay, az) + s : chain_init(w, ax, ay, az);
+      for (int b = lane; b < nparts; b += 32) s += part[12 * b + w];
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) tot[w] = chain_live(w, S, A) ? chain_init(w, ax, ay, az) + s : chain_init(w, ax, ay, az);
 }
 
 // CM_acc and bodies 0..2: chain totals, then the (0,1), (0,2), (1,2) pairs
@@ -649,7 +621,8 @@ int mesh_gravity_state(const double *cm8, const J2Arg &j2)
       cudaStream_t st = c.s;
       const int lid = c.largest_id;
       const long N = c.n_max;
-      NCG_TRY(ensure_partial((size_t)(j2.on ? 15 : 12) * N));
+      constexpr int MAXP = 1184;  // block partials of the parallel chain sums (8 per SM)
+      NCG_TRY(ensure_partial((size_t)(j2.on ? 15 : 12) * N + 12 * MAXP));
       DevState S = dev_state();
       MGArgs A{lid, c.P.par_collision_cube_cells, c.P.par_central_mass_bool, c.P.par_mutual_bool,
                c.P.par_softening_parameter != 0., (long long)c.cell_cap, c.P.par_G, c.P.par_softening_parameter,
@@ -669,14 +642,14 @@ int mesh_gravity_state(const double *cm8, const J2Arg &j2)
       }
       double *tot = c.red + 3584;
       if (c.P.par_gravity_mode == NCGPU_GRAVITY_EXACT) {
-            k_mesh_chains<<<1, 384, 0, st>>>(S, A, c.partial, N, ax, ay, az, tot);
+            k_mesh_chains<<<12, 32, 0, st>>>(S, A, c.partial, N, ax, ay, az, tot);
             NCG_LAUNCHED();
       } else {
-            const int np = std::min(148, std::max(1, (lid + RB12) / RB12));
-            double *part = c.red + 1024;  // up to 148 x 12 doubles
+            const int np = std::min(MAXP, std::max(1, (lid + RB12) / RB12));
+            double *part = c.partial + (size_t)(j2.on ? 15 : 12) * N;  // after the terms
             k_mesh_chains_part<<<np, RB12, 0, st>>>(S, A, c.partial, N, part);
             NCG_LAUNCHED();
-            k_mesh_chains_fold<<<1, 32, 0, st>>>(S, A, part, np, ax, ay, az, tot);
+            k_mesh_chains_fold<<<1, 384, 0, st>>>(S, A, part, np, ax, ay, az, tot);
             NCG_LAUNCHED();
       }
       k_mesh_big3<<<1, 32, 0, st>>>(S, A, tot, ax, ay, az, c.cm_acc);

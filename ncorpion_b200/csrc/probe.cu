@@ -186,3 +186,30 @@ extern "C" int ncgpu_probe_wait_timeout(int probes, double *cycles_per_probe)
       *cycles_per_probe = (double)h / probes;
       return check_err_word();
 }
+
+namespace ncg {
+namespace {
+__global__ void k_div_probe(const double *__restrict__ a, const double *__restrict__ b, double *__restrict__ out,
+                            int n)
+{
+      const int i = blockIdx.x * blockDim.x + threadIdx.x;
+      if (i < n) out[i] = div_by_recip(a[i], b[i], __drcp_rn(b[i]));
+}
+}  // namespace
+}  // namespace ncg
+
+// out[i] = a[i] / b[i] through div_by_recip (the quotient of the tides'
+// recurrence), for tests against correctly rounded division.  Host buffers.
+extern "C" int ncgpu_probe_div(const double *a, const double *b, double *out, int n)
+{
+      if (!a || !b || !out || n <= 0) return NCGPU_E_ARG;
+      double *d = nullptr;
+      NCG_CK(cudaMalloc(&d, 3 * sizeof(double) * (size_t)n));
+      NCG_CK(cudaMemcpy(d, a, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice));
+      NCG_CK(cudaMemcpy(d + n, b, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice));
+      k_div_probe<<<(n + 255) / 256, 256>>>(d, d + n, d + 2 * (size_t)n, n);
+      NCG_LAUNCHED();
+      NCG_CK(cudaMemcpy(out, d + 2 * (size_t)n, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost));
+      NCG_CK(cudaFree(d));
+      return NCGPU_OK;
+}

@@ -193,6 +193,24 @@ int scan_exclusive(const int *in, int *out, int n, int *sums, cudaStream_t st)
       return NCGPU_OK;
 }
 
+int compact_existing_dev(const int *ex, int largest_id, cudaStream_t st)
+{
+      Ctx &c = ctx();
+      int n = largest_id + 1;
+      if (n <= 0) {
+            NCG_CK(cudaMemsetAsync(c.n_dev, 0, sizeof(int), st));
+            return NCGPU_OK;
+      }
+      int nb = (n + CB - 1) / CB;
+      k_count_flags<<<nb, CB, 0, st>>>(ex, n, c.cnt);
+      NCG_LAUNCHED();
+      k_scan_single<<<1, 1024, 0, st>>>(c.cnt, nb, c.n_dev);
+      NCG_LAUNCHED();
+      k_scatter_flags<<<nb, CB, 0, st>>>(ex, n, c.cnt, c.cidx);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
+
 int compact_existing(const int *ex, int largest_id, int *n_host, cudaStream_t st)
 {
       Ctx &c = ctx();

@@ -10,14 +10,21 @@
 // subtracts a from the body's acceleration, adds a m / M to CM_acc and then
 //   SideralOmega += timestep m / (moi M R^2) (X a_y - Y a_x) / S,
 // and the next body's r x Omega uses the new SideralOmega.  That recurrence is
-// sequential, so the work is split in three:
+// sequential, but a body's increment is usually far below half an ulp of
+// SideralOmega, so that the sum leaves it unchanged.  The work is split in three:
 //   k_tides_prep   one thread per body: everything that does not depend on
-//                  SideralOmega (the z component entirely), as 12 doubles a body;
-//   k_tides_chain  one warp: lane 0 runs the recurrence over the bodies in slot
-//                  order (11 dependent FP64 operations and a division a body)
-//                  while the warp stages the next records through shared memory;
+//                  SideralOmega (the z component entirely), as 13 doubles a body,
+//                  and then, speculatively, the body's step with the rotation the
+//                  kick starts from; the first body whose step would change the
+//                  rotation is recorded (every step before it used the right
+//                  value, so its results are final);
+//   k_tides_chain  one warp, from that body on (nothing when no body changes
+//                  the rotation): lane 0 runs the recurrence in slot order (11
+//                  dependent FP64 operations and a division a body) while the
+//                  warp stages the next records through shared memory;
 //   k_tides_apply  one thread per body: the accelerations and CM_acc terms,
-//                  then CM_acc's sequential sums from the vector field's value.
+//                  then CM_acc's sums from the vector field's value (sequential
+//                  in the exact gravity mode, a parallel reduction otherwise).
 // Every operation is the reference's, in its order, with IEEE rounding.
 #include "common.cuh"
 #include "physics.cuh"
@@ -29,14 +36,26 @@ DevState dev_state();
 
 namespace {
 
-constexpr int TREC = 12;  // doubles per record
-// record: X, Y, vX, vY, r2, r2*X, r2*Y, (2 rv)*X, (2 rv)*Y, S*K, timestep m/(moi M R R), S
-enum { RX, RY, RVX, RVY, RR2, RR2X, RR2Y, RTX, RTY, RSK, RCQ, RS };
+constexpr int TREC = 13;  // doubles per record
+// record: X, Y, vX, vY, r2, r2*X, r2*Y, (2 rv)*X, (2 rv)*Y, S*K, timestep m/(moi M R R), S, 1/S
+enum { RX, RY, RVX, RVY, RR2, RR2X, RR2Y, RTX, RTY, RSK, RCQ, RS, RYS };
+
+// One body's step of the recurrence: its (a_x, a_y) with rotation W, and the
+// rotation after it (src/physics.c:523-539).
+__device__ __forceinline__ double tide_step(const double *r, double W, double Dt, double &aX, double &aY)
+{
+      const double oX = DMUL(r[RY], W);   // r_x_OmX =  Y*SideralOmega
+      const double oY = DMUL(-r[RX], W);  // r_x_OmY = -X*SideralOmega
+      aX = DMUL(r[RSK], DADD(r[RR2X], DMUL(Dt, DADD(r[RTX], DMUL(r[RR2], DADD(r[RVX], oX))))));
+      aY = DMUL(r[RSK], DADD(r[RR2Y], DMUL(Dt, DADD(r[RTY], DMUL(r[RR2], DADD(r[RVY], oY))))));
+      return DADD(W, div_by_recip(DMUL(r[RCQ], DSUB(DMUL(r[RX], aY), DMUL(r[RY], aX))), r[RS], r[RYS]));
+}
 
 __global__ void k_tides_prep(DevState S, const int *__restrict__ cidx, int n, const double *__restrict__ cm,
                              const double *__restrict__ cm_acc, const double *__restrict__ ax,
                              const double *__restrict__ ay, double *__restrict__ az, double dt, double A, double Dt,
-                             double moi, double R, double *__restrict__ rec, double *__restrict__ terms)
+                             double moi, double R, double *__restrict__ rec, double *__restrict__ terms,
+                             double *__restrict__ aout, int *__restrict__ first)
 {
       const int q = blockIdx.x * blockDim.x + threadIdx.x;
       if (q >= n) return;
@@ -72,28 +91,39 @@ __global__ void k_tides_prep(DevState S, const int *__restrict__ cidx, int n, co
       r[RSK] = SK;
       r[RCQ] = DDIV(DMUL(dt, m), DMUL(DMUL(DMUL(moi, M), R), R));
       r[RS] = Sf;
+      r[RYS] = __drcp_rn(Sf);
+      // the step with the rotation the kick starts from: final for every body
+      // before the first one whose step changes the rotation
+      const double W0 = cm[8];
+      double aX, aY;
+      if (tide_step(r, W0, Dt, aX, aY) != W0) atomicMin(first, q);
+      aout[2 * (size_t)q] = aX;
+      aout[2 * (size_t)q + 1] = aY;
 }
 
 constexpr int TBK = 64;                 // records staged per block
 constexpr int TPER = TBK * TREC / 32;   // doubles each lane stages per block
 
-// The SideralOmega recurrence in slot order (one warp); writes (a_x, a_y) of
-// every body to aout and the final SideralOmega to cm[8].
+// The SideralOmega recurrence in slot order (one warp) from the first body
+// whose step changes the rotation (none: nothing to do); writes (a_x, a_y) of
+// those bodies to aout and the final SideralOmega to cm[8].
 __global__ void __launch_bounds__(32) k_tides_chain(const double *__restrict__ rec, int n, double Dt, double *cm,
-                                                    double *__restrict__ aout)
+                                                    double *__restrict__ aout, const int *__restrict__ first)
 {
       __shared__ __align__(16) double st[TBK * TREC];
       __shared__ double ob[2 * TBK];
       const int lane = threadIdx.x;
+      const int q0 = *first;
+      if (q0 >= n) return;
       const long total = (long)n * TREC;
       double v[TPER];
 #pragma unroll
       for (int u = 0; u < TPER; u++) {
-            const long i = (long)u * 32 + lane;
+            const long i = (long)q0 * TREC + (long)u * 32 + lane;
             v[u] = i < total ? rec[i] : 0.;
       }
       double W = cm[8];
-      for (int base = 0; base < n; base += TBK) {
+      for (int base = q0; base < n; base += TBK) {
 #pragma unroll
             for (int u = 0; u < TPER; u++) st[u * 32 + lane] = v[u];
             __syncwarp();
@@ -105,14 +135,8 @@ __global__ void __launch_bounds__(32) k_tides_chain(const double *__restrict__ r
             const int cnt = min(TBK, n - base);
             if (lane == 0) {
                   for (int q = 0; q < cnt; q++) {
-                        const double *r = st + q * TREC;
-                        const double oX = DMUL(r[RY], W);   // r_x_OmX =  Y*SideralOmega
-                        const double oY = DMUL(-r[RX], W);  // r_x_OmY = -X*SideralOmega
-                        const double aX =
-                            DMUL(r[RSK], DADD(r[RR2X], DMUL(Dt, DADD(r[RTX], DMUL(r[RR2], DADD(r[RVX], oX))))));
-                        const double aY =
-                            DMUL(r[RSK], DADD(r[RR2Y], DMUL(Dt, DADD(r[RTY], DMUL(r[RR2], DADD(r[RVY], oY))))));
-                        W = DADD(W, DDIV(DMUL(r[RCQ], DSUB(DMUL(r[RX], aY), DMUL(r[RY], aX))), r[RS]));
+                        double aX, aY;
+                        W = tide_step(st + q * TREC, W, Dt, aX, aY);
                         ob[2 * q] = aX;
                         ob[2 * q + 1] = aY;
                   }
@@ -149,8 +173,10 @@ int tides_state(double *d_acc, long bs, double *d_cm_acc)
       int n = 0;
       NCG_TRY(compact_existing(c.ex, c.largest_id, &n, st));
       if (n == 0) return NCGPU_OK;
-      NCG_TRY(ensure_partial((size_t)(TREC + 2 + 3) * n));
+      NCG_TRY(ensure_partial((size_t)(TREC + 2 + 3) * n + 1));
       double *rec = c.partial, *aout = rec + (size_t)TREC * n, *terms = aout + 2 * (size_t)n;
+      int *first = (int *)(terms + 3 * (size_t)n);  // first body whose step changes the rotation
+      NCG_CK(cudaMemsetAsync(first, 0x7f, sizeof(int), st));
       const double R = P.par_R_unit;
       const double R5 = R * R * R * R * R;
       const double A = 3. * P.par_k2 * P.par_G * R5;  // src/physics.c:505-506
@@ -158,13 +184,15 @@ int tides_state(double *d_acc, long bs, double *d_cm_acc)
       DevState S = dev_state();
       const int nb = (n + 255) / 256;
       k_tides_prep<<<nb, 256, 0, st>>>(S, c.cidx, n, c.cm, d_cm_acc, ax, ay, az, c.dt, A, P.par_Delta_t,
-                                       P.par_dimensionless_moi, R, rec, terms);
+                                       P.par_dimensionless_moi, R, rec, terms, aout, first);
       NCG_LAUNCHED();
-      k_tides_chain<<<1, 32, 0, st>>>(rec, n, P.par_Delta_t, c.cm, aout);
+      k_tides_chain<<<1, 32, 0, st>>>(rec, n, P.par_Delta_t, c.cm, aout, first);
       NCG_LAUNCHED();
       k_tides_apply<<<nb, 256, 0, st>>>(S, c.cidx, n, c.cm, aout, ax, ay, terms);
       NCG_LAUNCHED();
-      return seq_sum3(terms, n, d_cm_acc, d_cm_acc, st);  // CM_acc += a m / M in slot order
+      // CM_acc += a m / M: in slot order (exact mode), or a parallel sum
+      if (P.par_gravity_mode == NCGPU_GRAVITY_EXACT) return seq_sum3(terms, n, d_cm_acc, d_cm_acc, st);
+      return par_sum3(terms, n, d_cm_acc, d_cm_acc, st);
 }
 
 }  // namespace ncg

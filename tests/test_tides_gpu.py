@@ -126,3 +126,23 @@ def test_tides_need_central_mass(lib):
         A.init(64, make_params(central_mass_bool=0, **TIDES))
     assert e.value.status == A.E_ARG
     A.finalize()
+
+
+def test_tides_division_is_correctly_rounded(lib):
+    """The recurrence's quotient (reciprocal + two residual corrections,
+    Markstein) against correctly rounded division, bit for bit: random
+    quotients, divisors in S's range (0.5, 1] and beyond, quotients next to
+    exactly representable ones, zeros of both signs."""
+    from ncorpion_b200 import api
+    rng = np.random.default_rng(12)
+    n = 1 << 21
+    a = rng.standard_normal(n) * np.exp2(rng.integers(-60, 60, n).astype(np.float64))
+    b = np.where(np.arange(n) % 2 == 0, rng.uniform(0.5, 1.0, n), rng.uniform(1e-3, 1e3, n))
+    near = np.arange(n) % 4 == 3  # a = b * q0 one or two ulps off: quotients next to q0
+    q0 = rng.uniform(-1, 1, n) * np.exp2(rng.integers(-30, 30, n).astype(np.float64))
+    step = np.where(np.arange(near.sum()) % 2 == 0, np.inf, -np.inf)
+    a[near] = np.nextafter(np.nextafter(b[near] * q0[near], step), step)
+    a[:4] = [0.0, -0.0, 1.0, -3.0]
+    out = np.empty(n)
+    api.check(lib.ncgpu_probe_div(api.ptr(a), api.ptr(b), api.ptr(out), n), "ncgpu_probe_div")
+    assert np.array_equal(out.view(np.int64), (a / b).view(np.int64))
