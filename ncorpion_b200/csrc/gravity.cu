@@ -10,7 +10,8 @@
 //        in the reference's order and rounding (explicit _rn intrinsics, no FMA
 //        contraction), so accelerations are bit-identical to vector_field:
 //          a_i = central_i ; for j ascending, j != i:
-//          a_i += ((G*m_j) * (x_j - x_i)) / (D*D*D),
+//          a_i += ((G*m_j) * (x_j - x_i)) / (D*D*D),   (the three quotients by
+//          D^3 correctly rounded from one correctly rounded reciprocal)
 //          D = sqrt(((dx*dx + dy*dy) + dz*dz) + (s*(R_i+R_j))^2)
 //        (the reference subtracts ((G*m_j)*(x_i-x_j))/D^3 for j < i, which is
 //        the same IEEE value).  CM_acc is summed sequentially in slot order.
@@ -85,16 +86,17 @@ __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, 
             double DX = __dsub_rn(me.x, cmx), DY = __dsub_rn(me.y, cmy), DZ = __dsub_rn(me.z, cmz);
             double rk = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(DX, DX), __dmul_rn(DY, DY)), __dmul_rn(DZ, DZ)));
             double r3 = __dmul_rn(__dmul_rn(rk, rk), rk);
-            a_x = __ddiv_rn(__dmul_rn(-mu, DX), r3);
-            a_y = __ddiv_rn(__dmul_rn(-mu, DY), r3);
-            a_z = __ddiv_rn(__dmul_rn(-mu, DZ), r3);
+            const double y3 = __drcp_rn(r3);  // the six quotients by r3 share RN(1/r3)
+            a_x = div_by_recip(__dmul_rn(-mu, DX), r3, y3);
+            a_y = div_by_recip(__dmul_rn(-mu, DY), r3, y3);
+            a_z = div_by_recip(__dmul_rn(-mu, DZ), r3, y3);
             // CM_acc terms: G*mk*DX/r3, then (with J2) the J2 share, so that
             // cterm's sequential sum adds them in the reference's order
             const int f = j2.on ? 2 : 1;
             const size_t nf = (size_t)f * n;
-            cterm[f * p] = __ddiv_rn(__dmul_rn(me.w, DX), r3);
-            cterm[nf + f * p] = __ddiv_rn(__dmul_rn(me.w, DY), r3);
-            cterm[2 * nf + f * p] = __ddiv_rn(__dmul_rn(me.w, DZ), r3);
+            cterm[f * p] = div_by_recip(__dmul_rn(me.w, DX), r3, y3);
+            cterm[nf + f * p] = div_by_recip(__dmul_rn(me.w, DY), r3, y3);
+            cterm[2 * nf + f * p] = div_by_recip(__dmul_rn(me.w, DZ), r3, y3);
             if (j2.on) {  // src/physics.c:149-160
                   double cj[3];
                   d_j2(j2, mu, DX, DY, DZ, rk, r3, bv.m[(long)cidx[p] * bv.stride], a_x, a_y, a_z, cj);
@@ -162,9 +164,10 @@ __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, 
                         }
                         double D = __dsqrt_rn(r2);
                         double D3 = __dmul_rn(__dmul_rn(D, D), D);
-                        a_x = __dadd_rn(a_x, __ddiv_rn(__dmul_rn(s.w, dx), D3));
-                        a_y = __dadd_rn(a_y, __ddiv_rn(__dmul_rn(s.w, dy), D3));
-                        a_z = __dadd_rn(a_z, __ddiv_rn(__dmul_rn(s.w, dz), D3));
+                        const double y = __drcp_rn(D3);  // the three quotients by D3 share RN(1/D3)
+                        a_x = __dadd_rn(a_x, div_by_recip(__dmul_rn(s.w, dx), D3, y));
+                        a_y = __dadd_rn(a_y, div_by_recip(__dmul_rn(s.w, dy), D3, y));
+                        a_z = __dadd_rn(a_z, div_by_recip(__dmul_rn(s.w, dz), D3, y));
                   }
             }
             __syncthreads();

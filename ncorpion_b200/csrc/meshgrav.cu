@@ -207,9 +207,10 @@ __device__ __forceinline__ void pair_add(const DevState &S, int b, int o, double
       double D = __dsqrt_rn(r2);
       double D3 = DMUL(DMUL(D, D), D);
       double g = DMUL(G, S.m[o]);
-      ax = DADD(ax, DDIV(DMUL(g, dx), D3));
-      ay = DADD(ay, DDIV(DMUL(g, dy), D3));
-      az = DADD(az, DDIV(DMUL(g, dz), D3));
+      const double y = __drcp_rn(D3);  // the three quotients by D3 share RN(1/D3)
+      ax = DADD(ax, div_by_recip(DMUL(g, dx), D3, y));
+      ay = DADD(ay, div_by_recip(DMUL(g, dy), D3, y));
+      az = DADD(az, div_by_recip(DMUL(g, dz), D3, y));
 }
 
 // A body's gravity fields in a cell-ordered copy (64 bytes), read by the walk
@@ -245,9 +246,10 @@ __device__ __forceinline__ void pair_add_rec(double xb, double yb, double zb, do
       double D = __dsqrt_rn(r2);
       double D3 = DMUL(DMUL(D, D), D);
       double g = DMUL(G, o.m);
-      ax = DADD(ax, DDIV(DMUL(g, dx), D3));
-      ay = DADD(ay, DDIV(DMUL(g, dy), D3));
-      az = DADD(az, DDIV(DMUL(g, dz), D3));
+      const double y = __drcp_rn(D3);
+      ax = DADD(ax, div_by_recip(DMUL(g, dx), D3, y));
+      ay = DADD(ay, div_by_recip(DMUL(g, dy), D3, y));
+      az = DADD(az, div_by_recip(DMUL(g, dz), D3, y));
 }
 
 // The term body b adds to body i (0..2) in the k > 2 loop: G*mk*DX/D3 with
@@ -263,9 +265,10 @@ __device__ __forceinline__ void big_term(const DevState &S, int b, int i, double
       double D = __dsqrt_rn(r2);
       double D3 = DMUL(DMUL(D, D), D);
       double g = DMUL(G, S.m[b]);
-      t[0] = DDIV(DMUL(g, dx), D3);
-      t[1] = DDIV(DMUL(g, dy), D3);
-      t[2] = DDIV(DMUL(g, dz), D3);
+      const double y = __drcp_rn(D3);
+      t[0] = div_by_recip(DMUL(g, dx), D3, y);
+      t[1] = div_by_recip(DMUL(g, dy), D3, y);
+      t[2] = div_by_recip(DMUL(g, dz), D3, y);
 }
 
 struct MGArgs {
@@ -344,13 +347,14 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
             double DX = DSUB(S.x[b], A.cmx), DY = DSUB(S.y[b], A.cmy), DZ = DSUB(S.z[b], A.cmz);
             double rk = __dsqrt_rn(DADD(DADD(DMUL(DX, DX), DMUL(DY, DY)), DMUL(DZ, DZ)));
             double r3 = DMUL(DMUL(rk, rk), rk);
-            a_x = DDIV(DMUL(-A.mu, DX), r3);
-            a_y = DDIV(DMUL(-A.mu, DY), r3);
-            a_z = DDIV(DMUL(-A.mu, DZ), r3);
+            const double y3 = __drcp_rn(r3);  // the six quotients by r3 share RN(1/r3)
+            a_x = div_by_recip(DMUL(-A.mu, DX), r3, y3);
+            a_y = div_by_recip(DMUL(-A.mu, DY), r3, y3);
+            a_z = div_by_recip(DMUL(-A.mu, DZ), r3, y3);
             double g = DMUL(A.G, S.m[b]);
-            cm_chain(terms, A, N, 0)[f * b] = DDIV(DMUL(g, DX), r3);
-            cm_chain(terms, A, N, 1)[f * b] = DDIV(DMUL(g, DY), r3);
-            cm_chain(terms, A, N, 2)[f * b] = DDIV(DMUL(g, DZ), r3);
+            cm_chain(terms, A, N, 0)[f * b] = div_by_recip(DMUL(g, DX), r3, y3);
+            cm_chain(terms, A, N, 1)[f * b] = div_by_recip(DMUL(g, DY), r3, y3);
+            cm_chain(terms, A, N, 2)[f * b] = div_by_recip(DMUL(g, DZ), r3, y3);
             if (A.j2.on) {  // src/physics.c:149-160
                   double cj[3];
                   d_j2(A.j2, A.mu, DX, DY, DZ, rk, r3, S.m[b], a_x, a_y, a_z, cj);
@@ -376,12 +380,13 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                   const double D = __dsqrt_rn(r2);
                   const double D3 = DMUL(DMUL(D, D), D);
                   const double gi = DMUL(A.G, S.m[i]), gb = DMUL(A.G, mb);
-                  a_x = DADD(a_x, DDIV(DMUL(gi, dx), D3));
-                  a_y = DADD(a_y, DDIV(DMUL(gi, dy), D3));
-                  a_z = DADD(a_z, DDIV(DMUL(gi, dz), D3));
-                  terms[(3 * i) * N + b] = DDIV(DMUL(gb, DSUB(xb, S.x[i])), D3);
-                  terms[(3 * i + 1) * N + b] = DDIV(DMUL(gb, DSUB(yb, S.y[i])), D3);
-                  terms[(3 * i + 2) * N + b] = DDIV(DMUL(gb, DSUB(zb, S.z[i])), D3);
+                  const double y = __drcp_rn(D3);
+                  a_x = DADD(a_x, div_by_recip(DMUL(gi, dx), D3, y));
+                  a_y = DADD(a_y, div_by_recip(DMUL(gi, dy), D3, y));
+                  a_z = DADD(a_z, div_by_recip(DMUL(gi, dz), D3, y));
+                  terms[(3 * i) * N + b] = div_by_recip(DMUL(gb, DSUB(xb, S.x[i])), D3, y);
+                  terms[(3 * i + 1) * N + b] = div_by_recip(DMUL(gb, DSUB(yb, S.y[i])), D3, y);
+                  terms[(3 * i + 2) * N + b] = div_by_recip(DMUL(gb, DSUB(zb, S.z[i])), D3, y);
             }
       }
       if (A.mutual && have_cells && b > A.lid0) {
