@@ -40,11 +40,11 @@ N_BODIES = 65536
 SOFTENING = 0.5
 FLOP_PER_INTERACTION = 20  # 3 sub, 3 FMA (r^2+eps^2), rsqrt (2), 3 mul, 3 FMA accumulate
 # DRAM bytes (read + write) of one k_grav_tiled<mixed> launch at N=65,536, from one ncu capture of
-# this script's gravity workload (profiles/k_grav_tiled_mixed_n65536.txt): 4.0 MB read + 62.2 MB written.
-MIXED_DRAM_BYTES = 66.24e6
+# this script's gravity workload (profiles/k_grav_tiled_mixed_n65536.txt): 3.35 MB read + 58.09 MB written.
+MIXED_DRAM_BYTES = 61.45e6
 # DRAM bytes of one mesh step's two main kernels (k_mesh_write + k_mesh_grav) captured at N=262,144
-# (profiles/k_mesh_write_grav_n262144.txt: 43.4 MB + 95.3 MB), scaled by the bodies to N=1,048,576.
-MESH_DRAM_BYTES_262K = 138.7e6
+# (profiles/k_mesh_write_grav_n262144.txt: 44.1 MB + 101.2 MB), scaled by the bodies to N=1,048,576.
+MESH_DRAM_BYTES_262K = 145.3e6
 METRIC = "Pair-interactions/s mixed vs FP64 (rel err<1e-6); mesh collision steps/s at N=1M"
 WORKLOAD = ("gravity-only single-step accelerations, N=65,536 disk (a~U[0.8,1.2], e~Rayleigh 0.01, "
             "i~Rayleigh 0.005), masses log-uniform [1e-9,1e-6], R=1e-5, softening 0.5*(R_k+R_p)")
