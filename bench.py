@@ -172,7 +172,7 @@ def run_reference_arm(a, ws, rank):
     t = float(np.mean(times))
     v = REF_SAMPLE * (REF_SAMPLE - 1) / t
     out = {"metric": METRIC, "value": v, "unit": "pair-interactions/s", "n_gpus": a.gpus, "steps": a.steps,
-           "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+           "warmup": a.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "strong",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
            "config": {"workload": WORKLOAD, "n": N_BODIES, "sample_bodies": REF_SAMPLE,
                       "parallelism": "single thread (the reference has no threading)"},

@@ -260,6 +260,34 @@ int ncgpu_energy(double *out);
    points use par_sideral_omega. */
 int ncgpu_get_sideral_omega(double *omega);
 int ncgpu_set_sideral_omega(double omega);
+/* Output staging (display(), src/display.c:239-451, at the drivers' output
+   steps).  ncgpu_snapshot_begin copies the bodies' fields and the central body
+   and makes the copy the state: until ncgpu_snapshot_end every entry point
+   (drift, kick, three_largest, mesh, the two calls below) works on the copy,
+   while exists[], the free slots and largest_id stay shared with the original,
+   as the reference's globals are shared between its body array and the copy it
+   prints (src/rk4.c:740-757, 881-890).  ncgpu_snapshot_end makes the original
+   the state again; SideralOmega keeps the copy's value (one global in the
+   reference). */
+int ncgpu_snapshot_begin(void);
+int ncgpu_snapshot_end(void);
+/* The cartesian files' text of this output for the current state (display()
+   with write_cartesian_bool): x, y, z, vx, vy, vz (the central body first when
+   par_central_mass_bool), mass, radius, each value as "%.14lf " (the exact
+   decimal of the double rounded to 14 digits, ties to even, as glibc prints it)
+   over the existing bodies in slot order.  The 8 files' texts are concatenated
+   in `text` (no newlines; display() ends each line with one) and lens[8]
+   receives their byte counts.  cap >= ncgpu_format_cartesian_cap() always
+   suffices.  NCGPU_E_UNSUPPORTED when a value exceeds 1.7e24 in magnitude
+   (the caller prints that output itself). */
+int ncgpu_format_cartesian(char *text, unsigned long cap, unsigned long *lens);
+unsigned long ncgpu_format_cartesian_cap(void);
+/* display()'s statistics of the current state (src/display.c:303-379):
+   stats[0] the total mass of the bodies summed in slot order, stats[1..2] and
+   idx[0..1] the masses M1, M2 and slots of the two most massive bodies as its
+   loop picks them (0 when absent), two[0..1] those slots' records, cm the
+   central body. */
+int ncgpu_output_stats(double *stats, int *idx, struct ncgpu_body *cm, struct ncgpu_body *two);
 /* Outcomes of the fragmentation model since the last upload, in the order of
    merger_count, super_catastrophic_count, half_fragmentation_count and
    full_fragmentation_count (src/structure.h:148-151). */

@@ -120,6 +120,11 @@ EXPORTS = {
     "ncgpu_fragment_counts": (C.c_int, [P]),
     "ncgpu_energy": (C.c_int, [P]),
     "ncgpu_get_sideral_omega": (C.c_int, [P]),
+    "ncgpu_snapshot_begin": (C.c_int, []),
+    "ncgpu_snapshot_end": (C.c_int, []),
+    "ncgpu_format_cartesian": (C.c_int, [P, C.c_ulong, P]),
+    "ncgpu_format_cartesian_cap": (C.c_ulong, []),
+    "ncgpu_output_stats": (C.c_int, [P, P, P, P]),
     "ncgpu_set_sideral_omega": (C.c_int, [C.c_double]),
     "ncgpu_probe_pow_third": (C.c_int, [P, P, C.c_int]),
     "ncgpu_probe_div": (C.c_int, [P, P, P, C.c_int]),
@@ -389,6 +394,41 @@ def fragment_counts() -> np.ndarray:
     out = np.zeros(4, np.int32)
     check(load().ncgpu_fragment_counts(ptr(out)), "ncgpu_fragment_counts")
     return out
+
+
+def snapshot_begin():
+    check(load().ncgpu_snapshot_begin(), "ncgpu_snapshot_begin")
+
+
+def snapshot_end():
+    check(load().ncgpu_snapshot_end(), "ncgpu_snapshot_end")
+
+
+def format_cartesian() -> list:
+    """The 8 cartesian files' texts (x y z vx vy vz mass radius) of the state,
+    as display() writes them, without the newlines."""
+    lib = load()
+    cap = lib.ncgpu_format_cartesian_cap()
+    buf = C.create_string_buffer(cap)
+    lens = (C.c_ulong * 8)()
+    check(lib.ncgpu_format_cartesian(buf, cap, lens), "ncgpu_format_cartesian")
+    raw = buf.raw
+    out, pos = [], 0
+    for f in range(8):
+        out.append(raw[pos:pos + lens[f]].decode())
+        pos += lens[f]
+    return out
+
+
+def output_stats():
+    """(stats (total_mass, M1, M2), (i1, i2), cm (8), two bodies (2 x 8)) as display() computes them."""
+    lib = load()
+    stats = np.zeros(3)
+    idx = np.zeros(2, np.int32)
+    cm = np.zeros(8)
+    two = np.zeros((2, 8))
+    check(lib.ncgpu_output_stats(ptr(stats), ptr(idx), ptr(cm), ptr(two)), "ncgpu_output_stats")
+    return stats, idx, cm, two
 
 
 def get_sideral_omega() -> float:

@@ -178,6 +178,14 @@ struct Ctx {
       int uploaded = 0;
       double *cm = nullptr;        // 16 doubles: central mass record (8), SideralOmega at [8]
       double j2 = 0.;              // the J2 in force for the state's kicks (set at upload and end of step)
+      // output staging (output.cu): snapshot body fields and central body, the
+      // formatter's slots / packed text / lengths
+      double *snap[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+      double *snap_cm = nullptr;
+      int snap_active = 0;
+      char *fmt_slots = nullptr, *fmt_text = nullptr;
+      int *fmt_len = nullptr;
+      size_t fmt_cap = 0;
       double *cm_acc = nullptr;    // 3 doubles
       double dt = 0.0;
 

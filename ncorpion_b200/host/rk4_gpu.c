@@ -10,13 +10,16 @@
  * on main.c's compile line only (the reference's rk4.o keeps its own copies).
  *
  * Bodies live on the GPU between calls.  The host keeps what the reference
- * keeps on the host: initial conditions (populate), output files (display,
- * readme, resume), the progress printout, the mesh size gamma (updated with
- * the host's libm pow) and the brute-force switch.  At every output step and
- * every step whose progress is printed the state is copied back, and the
- * reference's own end_of_timestep runs on the host copy for its printout and
- * gamma update; the dumping, barycentre reduction and tidy_up it would do have
- * already been done by the device, so on the host copy they find nothing to do.
+ * keeps on the host: initial conditions (populate), the output files (readme,
+ * resume, the first and last display), the progress printout, the mesh size
+ * gamma (updated with the host's libm pow) and the brute-force switch.  At an
+ * output step the half backward drift or kick of the printed copy runs on a
+ * device snapshot and the cartesian files' text is formatted on the device
+ * (gpu_display_device); stat.txt's line is printed here.  At every step whose
+ * progress is printed the state is copied back, and the reference's own
+ * end_of_timestep runs on the host copy for its printout and gamma update; the
+ * dumping, barycentre reduction and tidy_up it would do have already been done
+ * by the device, so on the host copy they find nothing to do.
  */
 #include <math.h>
 #include <stdio.h>
@@ -118,6 +121,17 @@ static void gpu_pull(struct moonlet *moonlets)
       if (J2_bool && J2_value == 0.) J2 = 0.5 * SideralOmega * SideralOmega * R_unit * R_unit * R_unit / (G * CM.mass);
 }
 
+/* the output step's copy (device snapshot) -> buffer, the shared globals and
+   CM_buffer, for an output the host prints itself */
+static void gpu_snapshot_pull(struct moonlet *buffer)
+{
+      int lid;
+      gpu_check(ncgpu_download((struct ncgpu_body *)buffer, exists, &lid, (struct ncgpu_body *)&CM_buffer), "download");
+      for (int j = lid + 1; j <= largest_id && j < N_max; j++) exists[j] = 0;
+      largest_id = lid;
+      if (central_tides_bool) gpu_check(ncgpu_get_sideral_omega(&SideralOmega), "sideral rotation");
+}
+
 /* The collision records of the last sweep appended to collisionDatas, as
    collision() and merger() fill them (src/physics.c:608-622, 685-704). */
 static void gpu_collision_records(double t_now)
@@ -153,6 +167,97 @@ static void gpu_collision_records(double t_now)
 #endif
       free(ev);
       free(rec);
+}
+
+/* display() (src/display.c:239-451) of the device state -- the output step's
+   copy -- for the cartesian files: their text comes formatted from the device
+   (ncgpu_format_cartesian), stat.txt's line is printed here from the device's
+   statistics with the reference's own cart2ell, and collision.txt from the
+   host's records, every line as display() prints it.  CM_buffer receives the
+   copy's central body.  Returns 0 (nothing written) when the host must print
+   this output itself: elliptic elements, or a value beyond the device
+   formatter's range. */
+static int gpu_display_device(void)
+{
+      static char *text = NULL;
+      static unsigned long cap = 0;
+      if (!write_cartesian_bool || write_elliptic_bool) return 0;
+      if (cap < ncgpu_format_cartesian_cap()) {
+            free(text);
+            cap = ncgpu_format_cartesian_cap();
+            text = (char *)malloc(cap);
+            if (text == NULL) {
+                  fprintf(stderr, "Error : Can't allocate the output text buffer.\n");
+                  abort();
+            }
+      }
+      unsigned long lens[8];
+      int st = ncgpu_format_cartesian(text, cap, lens);
+      if (st == NCGPU_E_UNSUPPORTED) return 0;
+      gpu_check(st, "output text");
+      double stats[3];
+      int idx[2];
+      struct moonlet two[2];
+      gpu_check(ncgpu_output_stats(stats, idx, (struct ncgpu_body *)&CM_buffer, (struct ncgpu_body *)two), "output stats");
+      if (central_tides_bool || (J2_bool && J2_value == 0.)) gpu_check(ncgpu_get_sideral_omega(&SideralOmega), "sideral rotation");
+
+      int collision = collision_bool && write_collisions_bool ? 1 : 0;
+      FILE *filestat = *files;
+      FILE *out[8];  /* in the device's order: x y z vx vy vz mass radius */
+      for (int f = 0; f < 6; f++) out[f] = *(files + 3 + collision + f);
+      out[6] = *(files + 1 + collision);
+      out[7] = *(files + 2 + collision);
+      unsigned long pos = 0;
+      for (int f = 0; f < 8; f++) {
+            fwrite(text + pos, 1, lens[f], out[f]);
+            pos += lens[f];
+      }
+
+      typ total_mass = stats[0], M1 = stats[1], M2 = stats[2];
+      typ mu, R1, R2, a1, a2, l1, l2, K1, K2, H1, H2, Q1, Q2, P1, P2, inner_fluid_disk_mass;
+      typ alkhqp[6];
+      mu = central_mass_bool ? CM_buffer.mass : M_unit;  mu += inner_fluid_disk_bool ? fluid_disk_Sigma*M_PI*(Rout*Rout - R_unit*R_unit) : 0.;  mu *= G;
+      if (how_many_moonlets == 0){
+            M1 = 0.; M2 = 0.; R1 = 0.; R2 = 0.; a1 = 0.; a2 = 0.; l1 = 0.; l2 = 0.; K1 = 0.; K2 = 0.; H1 = 0.; H2 = 0.; Q1 = 0.; Q2 = 0.; P1 = 0.; P2 = 0.;
+      }
+      else if (how_many_moonlets == 1){
+            M2 = 0.; R2 = 0.; a2 = 0.; l2 = 0.; K2 = 0.; H2 = 0.; Q2 = 0.; P2 = 0.;
+            R1 = two[0].radius;
+            cart2ell(two, 0, alkhqp, mu + G*M1);
+            a1 = *alkhqp; l1 = alkhqp[1]; K1 = alkhqp[2]; H1 = alkhqp[3]; Q1 = alkhqp[4]; P1 = alkhqp[5];
+      }
+      else{
+            R1 = two[0].radius;  R2 = two[1].radius;
+            cart2ell(two, 0, alkhqp, mu + G*M1);
+            a1 = *alkhqp; l1 = alkhqp[1]; K1 = alkhqp[2]; H1 = alkhqp[3]; Q1 = alkhqp[4]; P1 = alkhqp[5];
+            cart2ell(two, 1, alkhqp, mu + G*M2);
+            a2 = *alkhqp; l2 = alkhqp[1]; K2 = alkhqp[2]; H2 = alkhqp[3]; Q2 = alkhqp[4]; P2 = alkhqp[5];
+      }
+      fprintf(filestat, "%.14lf %d %d", time_elapsed + t_init, how_many_moonlets, collision_count);
+      if (central_mass_bool) fprintf(filestat, " %.14lf", CM_buffer.mass);
+      else fprintf(filestat, " %.1lf",  0.);
+      fprintf(filestat, " %.14lf", total_mass);
+      if (inner_fluid_disk_bool){
+            inner_fluid_disk_mass = fluid_disk_Sigma*M_PI*(Rout*Rout - R_unit*R_unit);
+            fprintf(filestat, " %.14lf %.14lf", inner_fluid_disk_mass, Rout);
+      }
+      else fprintf(filestat, " %.1lf %.1lf",  0., 0.);
+      if (central_tides_bool || (J2_bool && J2_value == 0.)) fprintf(filestat, " %.14lf", SideralOmega);
+      else fprintf(filestat, " %.1lf", 0.);
+      fprintf(filestat, " %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf",
+      M1, M2, R1, R2, a1, a2, l1, l2, K1, K2, H1, H2, Q1, Q2, P1, P2);
+      fprintf(filestat, "\n");
+      for (int f = 0; f < 8; f++) fprintf(out[f], "\n");
+      if (collision){
+            FILE *filecol = *(files + 1);
+            for (int p = 0; p < indexCollision; p ++){
+                  struct collisionData *cd = collisionDatas + p;
+                  fprintf(filecol, "%.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf\n", cd->time, cd->m1, cd->m2,
+                          cd->R1, cd->R2, cd->DeltaV, cd->impact_angle, cd->m_tilde);
+            }
+            indexCollision = 0;
+      }
+      return 1;
 }
 
 static int gpu_collide_brute(double t_now)
@@ -267,14 +372,16 @@ void ncgpu_integration_brute_force_SABA1(typ t)
       while (time_elapsed < t) {
             progressed = 0;
             if (write_to_files_bool && iter % output_step == 0 && iter > 0) {
-                  gpu_pull(moonlets);
-                  for (j = 0; j <= largest_id; j++)
-                        if (exists[j]) moonlet_buffer[j] = moonlets[j];
-                  if (central_mass_bool) CM_buffer = CM;
-                  timestep /= -2.0;
-                  drift(moonlet_buffer, &CM_buffer);  /* half backward drift, host copy */
-                  timestep *= -2.0;
-                  display(moonlet_buffer);
+                  /* the half backward drift of a copy, printed (src/rk4.c:881-890), on the device */
+                  gpu_check(ncgpu_snapshot_begin(), "snapshot");
+                  gpu_check(ncgpu_set_timestep(timestep / -2.0), "timestep");
+                  gpu_check(ncgpu_drift(), "drift");
+                  if (!gpu_display_device()) {
+                        gpu_snapshot_pull(moonlet_buffer);
+                        display(moonlet_buffer);
+                  }
+                  gpu_check(ncgpu_snapshot_end(), "snapshot");
+                  gpu_check(ncgpu_set_timestep(timestep), "timestep");
             }
             gpu_check(ncgpu_kick(), "kick");
             time_elapsed += .5 * timestep;
@@ -348,35 +455,30 @@ void ncgpu_integration_mesh(typ t)
       while (time_elapsed < t) {
             progressed = 0;
             if (write_to_files_bool && iter % output_step == 0 && iter > 0) {
-                  /* half backward kick of a host copy with the reference's own code */
-                  gpu_pull(moonlets);
-                  for (j = 0; j <= largest_id; j++)
-                        if (exists[j]) moonlet_buffer[j] = moonlets[j];
-                  if (central_mass_bool) CM_buffer = CM;
-                  timestep /= -2.0;
+                  /* the half backward kick of a copy, printed (src/rk4.c:740-757), on the
+                     device: the copy shares exists[], the free slots and SideralOmega
+                     with the bodies, as the reference's globals do */
+                  gpu_check(ncgpu_snapshot_begin(), "snapshot");
+                  gpu_check(ncgpu_set_timestep(timestep / -2.0), "timestep");
                   if (!force_naive_bool) {
-                        three_largest_moonlets(moonlet_buffer);
-                        three_largest_three_first(moonlet_buffer);
-                        get_neighbours_mesh(moonlet_buffer);
+                        int np = 0, ne = 0;
+                        long tn0 = 0;
+                        gpu_check(ncgpu_three_largest(NULL), "three_largest");
+                        gpu_check(ncgpu_mesh(gam, 0, &np, &ne, &tn0), "mesh");  /* get_neighbours_mesh */
                   }
-                  kick(moonlet_buffer, &CM_buffer, vector_field);
-                  timestep *= -2.0;
-                  display(moonlet_buffer);
+                  gpu_check(ncgpu_kick(), "kick");
+                  if (!gpu_display_device()) {
+                        gpu_snapshot_pull(moonlet_buffer);
+                        display(moonlet_buffer);
+                  }
+                  gpu_check(ncgpu_snapshot_end(), "snapshot");
                   if (!force_naive_bool) {
-                        for (j = 0; j < how_many_modified; j++) {
-                              index = modified_cells[j];
-                              clear_chain(hash + index);
-                        }
+                        gpu_check(ncgpu_mesh_reset(), "mesh reset");
                         how_many_pairs = 0;
                         how_many_modified = 0;
                         total_neighbours = 0;
                   }
-                  gpu_upload(moonlets);  /* exists[] may have changed (slots 0-2 refilled) */
-                  /* the host kick's tides changed the rotation, and the integration
-                     goes on with it (the J2 in force stays the one of the last end
-                     of step, which the upload took from the device's rotation) */
-                  if (central_tides_bool)
-                        gpu_check(ncgpu_set_sideral_omega(SideralOmega), "sideral rotation");
+                  gpu_check(ncgpu_set_timestep(timestep), "timestep");
             }
             tn = 0;
             if (collision_bool) {
