@@ -250,6 +250,84 @@ def bench_mesh(lib, api, torch, mode, steps, warmup, n_bodies=None, cells=1024, 
             "pairs_per_step": pairs / steps, "bodies_end": hm, "gpu_launches": launches}
 
 
+def bench_output(lib, api, torch, reps=5, cpu=True):
+    """An output step of the mesh driver at N=1,048,576, as the drop-in runs it:
+    snapshot, half backward kick of the copy (three largest, neighbours, mesh
+    gravity), the cartesian files' text formatted on the device and copied to
+    the host, display()'s statistics, snapshot end.  Host wall clock (every call
+    synchronises).  Beside it, the reference's own formatting: fprintf of
+    "%.14lf " for the same number of values on one host core."""
+    import time
+    from ncorpion_b200 import disks
+    n = MESH_N
+    b = disks.mesh_disk(n, seed=0)
+    ex = np.ones(n, np.int32)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0])
+    api.init(n + n // 20, mesh_params(api.GRAVITY_MIXED))
+    api.upload(b, ex, cm)
+    gmin = 4.4 / 1024
+    gam = mesh_gamma0(n)
+    api.set_timestep(MESH_DT)
+    for _ in range(3):
+        hm, tn = api.step_mesh(gam)
+        gam = api.update_gamma(gam, tn, hm, 16.0, gmin)
+
+    cap = lib.ncgpu_format_cartesian_cap()
+    text = np.empty(cap, np.uint8)  # the caller's persistent host buffer, as the drop-in keeps one (pinned)
+    api.check(lib.ncgpu_host_register(api.ptr(text), text.nbytes), "register")
+    lens = (C.c_ulong * 8)()
+    stats, idx, cmo, two = np.zeros(3), np.zeros(2, np.int32), np.zeros(8), np.zeros((2, 8))
+
+    def one():
+        api.snapshot_begin()
+        api.set_timestep(MESH_DT / -2.0)
+        api.three_largest()
+        api.mesh(gam, False)
+        api.kick()
+        api.check(lib.ncgpu_format_cartesian(api.ptr(text), cap, lens), "ncgpu_format_cartesian")
+        api.check(lib.ncgpu_output_stats(api.ptr(stats), api.ptr(idx), api.ptr(cmo), api.ptr(two)), "stats")
+        api.snapshot_end()
+        api.mesh_reset()
+        api.set_timestep(MESH_DT)
+
+    one()
+    times = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t0)
+    lib.ncgpu_host_unregister(api.ptr(text))
+    api.finalize()
+    text_bytes = int(sum(lens))
+    nvals = int(np.count_nonzero(text[:text_bytes] == ord(" ")))
+    ms = 1e3 * float(np.median(times))
+    out = {"metric": "output step of the mesh driver at N=1,048,576 (cartesian files)", "ms": ms, "values": nvals,
+           "text_bytes": text_bytes, "values_per_s": nvals / (ms * 1e-3),
+           "note": "snapshot, half backward kick (three largest, neighbours, mesh gravity), device formatting, "
+                   "statistics, the text copied into a host buffer through the C ABI; host wall clock, median of "
+                   "%d" % reps}
+    if cpu:
+        try:
+            import tempfile
+            import oracle
+            import ctypes as Cc
+            port = Cc.CDLL(oracle.build_port())
+            port.orc_fprintf_values.restype = Cc.c_long
+            port.orc_fprintf_values.argtypes = [Cc.c_void_p, Cc.c_long, Cc.c_char_p]
+            vals = np.ascontiguousarray(b[:, :8].T.reshape(-1)[: nvals], dtype=np.float64)
+            d = tempfile.mkdtemp(prefix="ncgpu_out_")
+            t0 = time.perf_counter()
+            port.orc_fprintf_values(vals.ctypes.data, len(vals), os.path.join(d, "values.txt").encode())
+            dt = time.perf_counter() - t0
+            out["cpu_baseline"] = {"value": dt * 1e3, "unit": "ms", "cores": 1, "kind": "port",
+                                   "sample": f'fprintf "%.14lf " of {len(vals)} values (display()\'s formatting '
+                                             "alone, without the host copy's backward kick), one core"}
+        except Exception as e:  # noqa: BLE001
+            out["cpu_baseline"] = {"value": None, "unit": "ms", "cores": 1, "kind": "port", "sample": f"unavailable: {e}"}
+    return out
+
+
 CENTRAL_N = 262144
 CENTRAL_WORKLOAD = ("mesh steps (fast mode) of the N=262,144 mesh disk, 512 cells per side, alone, with the "
                     "fluid-body J2 (J2_value 0, Tearth 25), and with tides raised on the central body besides "
@@ -437,6 +515,7 @@ def main(argv=None):
     ap.add_argument("--no-bf", action="store_true", help="skip the N=2,000 brute-force collisional section")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint section")
     ap.add_argument("--no-central", action="store_true", help="skip the J2 / tides section")
+    ap.add_argument("--no-output", action="store_true", help="skip the output-step section")
     ap.add_argument("--mesh-n", type=int, default=MESH_N, help="mesh workload bodies (smaller cases for profiling)")
     ap.add_argument("--mesh-cells", type=int, default=1024)
     ap.add_argument("--mesh-steps", type=int, default=MESH_STEPS)
@@ -611,6 +690,7 @@ def main(argv=None):
     bf = None if a.no_bf else bench_bf_collide(lib, api, torch, rank == 0 and ws == 1 and not a.no_cpu_baseline)
     adjoint = None if a.no_adjoint else bench_adjoint(lib, api, torch)
     central = None if a.no_central else bench_central(lib, api, torch)
+    output = None if a.no_output else bench_output(lib, api, torch, cpu=(rank == 0 and ws == 1 and not a.no_cpu_baseline))
     frag = None
     if not a.no_frag:
         fm = bench_fragment(lib, api, torch, api.GRAVITY_MIXED, FRAG_STEPS)
@@ -671,6 +751,7 @@ def main(argv=None):
             "brute_force_collisional": bf,
             "adjoint": adjoint,
             "central_body": central,
+            "output_step": output,
             "accuracy": {"mutual_rel_err_max": float(rel_mut.max()),
                          "mutual_rel_err_median": float(np.median(rel_mut)),
                          "total_rel_err_max": float(rel_tot.max()),

@@ -182,14 +182,18 @@ static int gpu_display_device(void)
       static char *text = NULL;
       static unsigned long cap = 0;
       if (!write_cartesian_bool || write_elliptic_bool) return 0;
-      if (cap < ncgpu_format_cartesian_cap()) {
-            free(text);
+      if (cap < ncgpu_format_cartesian_cap()) {  /* one pinned buffer for the whole run */
+            if (text) {
+                  ncgpu_host_unregister(text);
+                  free(text);
+            }
             cap = ncgpu_format_cartesian_cap();
             text = (char *)malloc(cap);
             if (text == NULL) {
                   fprintf(stderr, "Error : Can't allocate the output text buffer.\n");
                   abort();
             }
+            gpu_check(ncgpu_host_register(text, cap), "host register");
       }
       unsigned long lens[8];
       int st = ncgpu_format_cartesian(text, cap, lens);

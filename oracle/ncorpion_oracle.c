@@ -16,6 +16,7 @@
  * radius (src/structure.h:74-84); exists[] one int per slot.
  */
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #include "../include/ncgpu.h"
@@ -1045,4 +1046,20 @@ static void fragment(int a, int b)
       }
       F.full_count++;
       free(r_k); free(v_k); free(id);
+}
+
+/* ---- output text (src/display.c:321-349) --------------------------------- */
+
+/* display()'s per-value output, fprintf(file, "%.14lf ", v), for the n values
+   of v into the file at `path`, then one newline: the CPU baseline of the
+   device formatter.  Returns the bytes written, or -1. */
+long orc_fprintf_values(const double *v, long n, const char *path)
+{
+      FILE *f = fopen(path, "w");
+      if (!f) return -1;
+      for (long i = 0; i < n; i++) fprintf(f, "%.14lf ", v[i]);
+      fprintf(f, "\n");
+      long bytes = ftell(f);
+      fclose(f);
+      return bytes;
 }
