@@ -259,6 +259,12 @@ int ncgpu_energy(double *out);
    state-based kicks is evaluated from it.  The stateless vector_field entry
    points use par_sideral_omega. */
 int ncgpu_get_sideral_omega(double *omega);
+/* The J2 in force for the state's kicks (J2_value, or the fluid-body J2 of the
+   last upload or end of step, src/rk4.c:459-463) and, in j2_before (may be
+   NULL), the one before the last end of step's update -- the value
+   end_of_timestep's printout still sees (src/rk4.c:225-333 precede the
+   update).  0 without J2. */
+int ncgpu_get_j2(double *j2, double *j2_before);
 int ncgpu_set_sideral_omega(double omega);
 /* Output staging (display(), src/display.c:239-451, at the drivers' output
    steps).  ncgpu_snapshot_begin copies the bodies' fields and the central body
@@ -288,6 +294,15 @@ unsigned long ncgpu_format_cartesian_cap(void);
    loop picks them (0 when absent), two[0..1] those slots' records, cm the
    central body. */
 int ncgpu_output_stats(double *stats, int *idx, struct ncgpu_body *cm, struct ncgpu_body *two);
+/* The barycentre end_of_timestep prints at a progress step (src/rk4.c:202-222,
+   333): zeros right after an ncgpu_end_of_timestep that reduced the barycentre
+   (the reference zeroes the vector it subtracted), otherwise the state's
+   total_momentum (src/structure.c:1193-1227), exact sums in slot order. */
+int ncgpu_total_momentum(double *com);
+/* largest_id of the device state, and (before_tidy, may be NULL) its value at
+   the start of the last ncgpu_end_of_timestep, before tidy_up -- the one
+   end_of_timestep prints (src/rk4.c:235-240). */
+int ncgpu_get_largest_id(int *largest_id, int *before_tidy);
 /* Outcomes of the fragmentation model since the last upload, in the order of
    merger_count, super_catastrophic_count, half_fragmentation_count and
    full_fragmentation_count (src/structure.h:148-151). */

@@ -120,6 +120,9 @@ EXPORTS = {
     "ncgpu_fragment_counts": (C.c_int, [P]),
     "ncgpu_energy": (C.c_int, [P]),
     "ncgpu_get_sideral_omega": (C.c_int, [P]),
+    "ncgpu_get_j2": (C.c_int, [P, P]),
+    "ncgpu_total_momentum": (C.c_int, [P]),
+    "ncgpu_get_largest_id": (C.c_int, [P, P]),
     "ncgpu_snapshot_begin": (C.c_int, []),
     "ncgpu_snapshot_end": (C.c_int, []),
     "ncgpu_format_cartesian": (C.c_int, [P, C.c_ulong, P]),

@@ -179,6 +179,7 @@ int refresh_j2()
       if (!c.P.par_J2_bool) return NCGPU_OK;
       double cm9[9];
       NCG_TRY(state_cm_host(cm9));
+      c.j2_prev = c.j2;
       c.j2 = j2_value(c.P, cm9[6], cm9[8]);
       return NCGPU_OK;
 }
@@ -188,6 +189,7 @@ int mesh_gravity_state(const double *cm8, const J2Arg &j2);
 int kick_state()
 {
       Ctx &c = ctx();
+      c.com_reduced = 0;
       double cm9[9];
       NCG_TRY(state_cm_host(cm9));
       const int nslots = c.largest_id + 1;
@@ -208,6 +210,7 @@ int kick_state()
 int drift_state()
 {
       Ctx &c = ctx();
+      c.com_reduced = 0;
       const int nslots = c.largest_id + 1;
       int nb = nslots > 0 ? (nslots + 255) / 256 : 1;
       k_drift<<<nb, 256, 0, c.s>>>(c.ex, nslots, c.dt, c.x, c.y, c.z, c.vx, c.vy, c.vz, c.cm,
@@ -531,7 +534,10 @@ int ncgpu_upload(const struct ncgpu_body *bodies, const int *exists, int largest
       c.n_events = 0;
       c.collision_count = 0;
       c.uploaded = 1;
-      return refresh_j2();
+      c.com_reduced = 0;
+      NCG_TRY(refresh_j2());
+      c.j2_prev = c.j2;
+      return NCGPU_OK;
 }
 
 int ncgpu_download(struct ncgpu_body *bodies, int *exists, int *largest_id, struct ncgpu_body *cm)
@@ -552,6 +558,16 @@ int ncgpu_download(struct ncgpu_body *bodies, int *exists, int *largest_id, stru
       NCG_CK(cudaStreamSynchronize(st));
       *largest_id = c.largest_id;
       return check_err_word();
+}
+
+int ncgpu_get_j2(double *j2, double *j2_before)
+{
+      Ctx &c = g_ctx;
+      if (!c.inited) return NCGPU_E_STATE;
+      if (!j2) return NCGPU_E_ARG;
+      *j2 = c.P.par_J2_bool ? c.j2 : 0.;
+      if (j2_before) *j2_before = c.P.par_J2_bool ? c.j2_prev : 0.;
+      return NCGPU_OK;
 }
 
 int ncgpu_get_sideral_omega(double *omega)

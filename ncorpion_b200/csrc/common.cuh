@@ -178,6 +178,9 @@ struct Ctx {
       int uploaded = 0;
       double *cm = nullptr;        // 16 doubles: central mass record (8), SideralOmega at [8]
       double j2 = 0.;              // the J2 in force for the state's kicks (set at upload and end of step)
+      double j2_prev = 0.;         // the J2 in force before the last end of step's update
+      int com_reduced = 0;         // the last end of step reduced the barycentre
+      int eot_lid = -1;            // largest_id at the start of the last end of step
       // output staging (output.cu): snapshot body fields and central body, the
       // formatter's slots / packed text / lengths
       double *snap[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};

@@ -192,12 +192,49 @@ __global__ void k_tidy_scatter(const DevState S, int n, int lid, const double *_
 
 }  // namespace
 
+// total_momentum (src/structure.c:1193-1227) of the state into com[0..5]
+// (device; com[8..14] scratch): the position and velocity of the barycentre,
+// sequential FP64 sums in slot order (exact) or a parallel reduction.
+int total_momentum_dev(bool exact, double *com)
+{
+      Ctx &c = ctx();
+      cudaStream_t st = c.s;
+      const ncgpu_params &P = c.P;
+      DevState S = dev_state();
+      int n = 0;
+      NCG_TRY(compact_existing(c.ex, c.largest_id, &n, st));
+      if (n > 0) {
+            NCG_TRY(ensure_partial((size_t)7 * n + 7 * 148));
+            double *terms = c.partial;
+            k_momentum_terms<<<(n + 255) / 256, 256, 0, st>>>(S, c.cidx, n, terms);
+            NCG_LAUNCHED();
+            if (exact) {
+                  k_momentum_chains<<<7, 32, 0, st>>>(terms, n, c.cm, P.par_central_mass_bool, com + 8);
+                  NCG_LAUNCHED();
+                  k_momentum_div<<<1, 32, 0, st>>>(com + 8, com);
+                  NCG_LAUNCHED();
+            } else {
+                  const int np = std::min(148, (n + MPB - 1) / MPB);
+                  double *part = terms + (size_t)7 * n;
+                  k_momentum_part<<<np, MPB, 0, st>>>(terms, n, part);
+                  NCG_LAUNCHED();
+                  k_momentum_fold<<<1, 32, 0, st>>>(part, np, c.cm, P.par_central_mass_bool, com);
+                  NCG_LAUNCHED();
+            }
+      } else {
+            k_momentum_fold<<<1, 32, 0, st>>>(c.red + 3584, 0, c.cm, P.par_central_mass_bool, com);
+            NCG_LAUNCHED();
+      }
+      return NCGPU_OK;
+}
+
 int eot_state(int *hm_out)
 {
       Ctx &c = ctx();
       cudaStream_t st = c.s;
       const ncgpu_params &P = c.P;
       const int lid = c.largest_id;
+      c.eot_lid = lid;  // largest_id before tidy_up, which end_of_timestep prints
       DevState S = dev_state();
       int zero[2] = {0, 0};
       NCG_CK(cudaMemcpyAsync(c.scal + S_HM, zero, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -218,32 +255,11 @@ int eot_state(int *hm_out)
             NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
             NCG_CK(cudaStreamSynchronize(st));
       }
+      c.com_reduced = 0;
       if (h[S_NEEDCOM] && P.par_reduce_to_COM_bool) {
-            int n = 0;
-            NCG_TRY(compact_existing(c.ex, lid, &n, st));
             double *com = c.red + 3072;
-            if (n > 0) {
-                  NCG_TRY(ensure_partial((size_t)7 * n + 7 * 148));
-                  double *terms = c.partial;
-                  k_momentum_terms<<<(n + 255) / 256, 256, 0, st>>>(S, c.cidx, n, terms);
-                  NCG_LAUNCHED();
-                  if (P.par_gravity_mode == NCGPU_GRAVITY_EXACT) {
-                        k_momentum_chains<<<7, 32, 0, st>>>(terms, n, c.cm, P.par_central_mass_bool, com + 8);
-                        NCG_LAUNCHED();
-                        k_momentum_div<<<1, 32, 0, st>>>(com + 8, com);
-                        NCG_LAUNCHED();
-                  } else {
-                        const int np = std::min(148, (n + MPB - 1) / MPB);
-                        double *part = terms + (size_t)7 * n;
-                        k_momentum_part<<<np, MPB, 0, st>>>(terms, n, part);
-                        NCG_LAUNCHED();
-                        k_momentum_fold<<<1, 32, 0, st>>>(part, np, c.cm, P.par_central_mass_bool, com);
-                        NCG_LAUNCHED();
-                  }
-            } else {
-                  k_momentum_fold<<<1, 32, 0, st>>>(c.red + 3584, 0, c.cm, P.par_central_mass_bool, com);
-                  NCG_LAUNCHED();
-            }
+            NCG_TRY(total_momentum_dev(P.par_gravity_mode == NCGPU_GRAVITY_EXACT, com));
+            c.com_reduced = 1;
             k_sub_com<<<nb, 256, 0, st>>>(S, lid, com, c.cm, P.par_central_mass_bool);
             NCG_LAUNCHED();
             NCG_CK(cudaMemsetAsync(c.scal + S_NEEDCOM, 0, sizeof(int), st));
@@ -270,6 +286,36 @@ int eot_state(int *hm_out)
 }  // namespace ncg
 
 using namespace ncg;
+
+// end_of_timestep's barycentre printout (src/rk4.c:202-222, 333): zeros right
+// after an end of step that reduced the barycentre, else the state's
+// total_momentum now (exact sums).
+extern "C" int ncgpu_total_momentum(double *com)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      if (!com) return NCGPU_E_ARG;
+      if (c.com_reduced) {  // end_of_timestep zeroes the vector it subtracted (src/rk4.c:219)
+            for (int d = 0; d < 6; d++) com[d] = 0.;
+            return NCGPU_OK;
+      }
+      double *d = c.red + 3072;
+      NCG_TRY(total_momentum_dev(true, d));
+      NCG_CK(cudaMemcpyAsync(com, d, 6 * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaStreamSynchronize(c.s));
+      return NCGPU_OK;
+}
+
+extern "C" int ncgpu_get_largest_id(int *largest_id, int *before_tidy)
+{
+      Ctx &c = ctx();
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      if (!largest_id) return NCGPU_E_ARG;
+      *largest_id = c.largest_id;
+      if (before_tidy) *before_tidy = c.eot_lid;
+      return NCGPU_OK;
+}
 
 extern "C" int ncgpu_end_of_timestep(int *how_many_moonlets)
 {

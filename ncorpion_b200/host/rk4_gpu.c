@@ -15,11 +15,10 @@
  * gamma (updated with the host's libm pow) and the brute-force switch.  At an
  * output step the half backward drift or kick of the printed copy runs on a
  * device snapshot and the cartesian files' text is formatted on the device
- * (gpu_display_device); stat.txt's line is printed here.  At every step whose
- * progress is printed the state is copied back, and the reference's own
- * end_of_timestep runs on the host copy for its printout and gamma update; the
- * dumping, barycentre reduction and tidy_up it would do have already been done
- * by the device, so on the host copy they find nothing to do.
+ * (gpu_display_device); stat.txt's line is printed here.  A step whose
+ * progress is printed prints end_of_timestep's lines from the device's
+ * statistics (gpu_progress_printout); the state comes back to the host only
+ * for the last output and where the host's own code needs it.
  */
 #include <math.h>
 #include <stdio.h>
@@ -204,6 +203,7 @@ static int gpu_display_device(void)
       struct moonlet two[2];
       gpu_check(ncgpu_output_stats(stats, idx, (struct ncgpu_body *)&CM_buffer, (struct ncgpu_body *)two), "output stats");
       if (central_tides_bool || (J2_bool && J2_value == 0.)) gpu_check(ncgpu_get_sideral_omega(&SideralOmega), "sideral rotation");
+      if (J2_bool) gpu_check(ncgpu_get_j2(&J2, NULL), "J2");  /* cart2ell reads it (src/structure.c:205-207) */
 
       int collision = collision_bool && write_collisions_bool ? 1 : 0;
       FILE *filestat = *files;
@@ -274,48 +274,137 @@ static int gpu_collide_brute(double t_now)
       return n;
 }
 
-/* end of a step on the device, then the host's share: how_many_moonlets, the
-   brute-force switch (src/rk4.c:388-393) and, in mesh mode, gamma
-   (src/rk4.c:367-372); the reference's own end_of_timestep on a fresh host
-   copy when the step's progress is printed. */
+/* end_of_timestep's printout at a progress step (src/rk4.c:225-333) from the
+   device's statistics (total mass, the two most massive bodies, the
+   barycentre, largest_id before tidy_up), the host's counters and the
+   reference's own cart2ell, instead of a copy of the whole state; CM and
+   CM_buffer as the reference leaves them. */
+static void gpu_progress_printout(void)
+{
+      typ stats[3], com[6], alkhqp[6];
+      int idx[2], lid = 0, lid_printed = 0;
+      struct moonlet two[2];
+      gpu_check(ncgpu_output_stats(stats, idx, (struct ncgpu_body *)&CM, (struct ncgpu_body *)two), "stats");
+      gpu_check(ncgpu_total_momentum(com), "total_momentum");
+      gpu_check(ncgpu_get_largest_id(&lid, &lid_printed), "largest_id");
+      if (central_tides_bool || (J2_bool && J2_value == 0.))
+            gpu_check(ncgpu_get_sideral_omega(&SideralOmega), "sideral rotation");
+      if (J2_bool) {  /* the printout precedes end_of_timestep's J2 update (src/rk4.c:459-463) */
+            typ j2_now = 0.;
+            gpu_check(ncgpu_get_j2(&j2_now, &J2), "J2");
+      }
+      if (fragmentation_bool) {  /* the outcome shares (src/rk4.c:244-247) */
+            int fc[4];
+            gpu_check(ncgpu_fragment_counts(fc), "fragment counts");
+            merger_count = fc[0];
+            super_catastrophic_count = fc[1];
+            half_fragmentation_count = fc[2];
+            full_fragmentation_count = fc[3];
+      }
+      typ total_mass = stats[0], M1 = stats[1], M2 = stats[2];
+      typ R1, R2, a1, a2, e1, e2, I1, I2, l1, l2, o1, o2, O1, O2;
+      if (central_mass_bool){
+            CM_buffer = CM;
+            CM_buffer.x -= .5*timestep*CM_buffer.vx;  CM_buffer.y -= .5*timestep*CM_buffer.vy;  CM_buffer.z -= .5*timestep*CM_buffer.vz;
+      }
+      if (collision_bool){
+            printf("                  N = %d  |  Collisions = %d  |  t = %.13lf   (largest id in the body array = %d)\n",
+            how_many_moonlets, collision_count, t_init + time_elapsed, lid_printed);
+      }
+      else{
+            printf("                  N = %d  |  t = %.13lf   (largest id in the body array = %d)\n", how_many_moonlets, t_init + time_elapsed, lid_printed);
+      }
+      if (collision_bool && fragmentation_bool && collision_count != 0){
+            typ cll = (typ) collision_count;
+            typ mrg = 100.*((typ) merger_count)/cll;
+            typ spc = 100.*((typ) super_catastrophic_count)/cll;
+            typ hfr = 100.*((typ) half_fragmentation_count)/cll;
+            typ ffr = 100.*((typ) full_fragmentation_count)/cll;
+            printf("                  Merger = %.2lf %% | Super-catastrophic = %.2lf %% | Partially fragmented = %.2lf %% | Fully fragmented = %.2lf %%\n",
+            mrg, spc, hfr, ffr);
+      }
+      if (central_mass_bool){
+            printf("                  Central mass = %.8lf,  Bodies mass = %.8lf\n", CM.mass, total_mass);
+      }
+      else{
+            printf("                  Bodies total mass = %.8lf\n", total_mass);
+      }
+      typ mu = central_mass_bool ? CM.mass : M_unit;  mu *= G;
+      if (how_many_moonlets > 1){
+            typ vp1, vp2;
+            struct moonlet mlt1 = {two[0].x, two[0].y, two[0].z, two[0].vx, two[0].vy, two[0].vz, 0., 0.};
+            struct moonlet mlt2 = {two[1].x, two[1].y, two[1].z, two[1].vx, two[1].vy, two[1].vz, 0., 0.};
+            mlt1.x -= .5*timestep*mlt1.vx;  mlt1.y -= .5*timestep*mlt1.vy;  mlt1.z -= .5*timestep*mlt1.vz;
+            mlt2.x -= .5*timestep*mlt2.vx;  mlt2.y -= .5*timestep*mlt2.vy;  mlt2.z -= .5*timestep*mlt2.vz;
+            R1  = two[0].radius;  R2 = two[1].radius;
+            cart2ell(&mlt1, 0, alkhqp, mu + G*M1);
+            a1  = *alkhqp; e1 = sqrt(alkhqp[2]*alkhqp[2] + alkhqp[3]*alkhqp[3]); I1 = 360.*asin(sqrt(alkhqp[4]*alkhqp[4] + alkhqp[5]*alkhqp[5]))/M_PI;
+            vp1 = 180.*atan2(alkhqp[3], alkhqp[2])/M_PI;
+            l1  = 180.*alkhqp[1]/M_PI - vp1; O1 = 180.*atan2(alkhqp[5], alkhqp[4])/M_PI; o1 = vp1 - O1;
+            cart2ell(&mlt2, 0, alkhqp, mu + G*M2);
+            a2  = *alkhqp; e2 = sqrt(alkhqp[2]*alkhqp[2] + alkhqp[3]*alkhqp[3]); I2 = 360.*asin(sqrt(alkhqp[4]*alkhqp[4] + alkhqp[5]*alkhqp[5]))/M_PI;
+            vp2 = 180.*atan2(alkhqp[3], alkhqp[2])/M_PI;
+            l2  = 180.*alkhqp[1]/M_PI - vp2; O2 = 180.*atan2(alkhqp[5], alkhqp[4])/M_PI; o2 = vp2 - O2;
+            printf("                  Most massive : (m, R; a, e, i; M, o, O) = (%.7lf, %.4lf; %.3lf, %.3lf, %.3lf°; %.2lf°, %.2lf°, %.2lf°)\n",
+            M1, R1, a1, e1, I1, l1, o1, O1);
+            printf("                  Second most  : (m, R; a, e, i; M, o, O) = (%.7lf, %.4lf; %.3lf, %.3lf, %.3lf°; %.2lf°, %.2lf°, %.2lf°)\n",
+            M2, R2, a2, e2, I2, l2, o2, O2);
+      }
+      else if (how_many_moonlets == 1){
+            typ vp1;
+            struct moonlet mlt1 = {two[0].x, two[0].y, two[0].z, two[0].vx, two[0].vy, two[0].vz, 0., 0.};
+            mlt1.x -= .5*timestep*mlt1.vx;  mlt1.y -= .5*timestep*mlt1.vy;  mlt1.z -= .5*timestep*mlt1.vz;
+            R1  = two[0].radius;
+            cart2ell(&mlt1, 0, alkhqp, mu + G*M1);
+            a1  = *alkhqp; e1 = sqrt(alkhqp[2]*alkhqp[2] + alkhqp[3]*alkhqp[3]); I1 = 360.*asin(sqrt(alkhqp[4]*alkhqp[4] + alkhqp[5]*alkhqp[5]))/M_PI;
+            vp1 = 180.*atan2(alkhqp[3], alkhqp[2])/M_PI;
+            l1  = 180.*alkhqp[1]/M_PI - vp1; O1 = 180.*atan2(alkhqp[5], alkhqp[4])/M_PI; o1 = vp1 - O1;
+            printf("                  Most massive : (m, R; a, e, i; M, o, O) = (%.7lf, %.4lf; %.3lf, %.3lf, %.3lf°; %.2lf°, %.2lf°, %.2lf°)\n",
+            M1, R1, a1, e1, I1, l1, o1, O1);
+      }
+      if (central_tides_bool){
+            printf("                  Sideral rotation = %.13lf\n", SideralOmega);
+      }
+      printf("                  COM = (%.9lf, %.9lf,  %.9lf,  %.9lf,  %.9lf,  %.9lf)\n", com[0], com[1], com[2], com[3], com[4], com[5]);
+      largest_id = lid;
+}
+
+/* end of a step on the device, then the host's share of end_of_timestep
+   (src/rk4.c:130-473): how_many_moonlets, at a progress step the printout,
+   in mesh mode gamma (src/rk4.c:356-381) and the brute-force switch
+   (src/rk4.c:384-389).  The fluid-body J2 the device keeps itself; the host's
+   copy is refreshed when the host needs it (gpu_pull). */
 static void gpu_end_of_timestep(struct moonlet *moonlets, int progressed, long total_nb)
 {
       int hm = 0;
       gpu_check(ncgpu_end_of_timestep(&hm), "end_of_timestep");
-      if (progressed) {
-            gpu_pull(moonlets);
-            if (fragmentation_bool) {  /* the outcome shares of the progress printout (src/rk4.c:244-247) */
-                  int fc[4];
-                  gpu_check(ncgpu_fragment_counts(fc), "fragment counts");
-                  merger_count = fc[0];
-                  super_catastrophic_count = fc[1];
-                  half_fragmentation_count = fc[2];
-                  full_fragmentation_count = fc[3];
-            }
+      how_many_moonlets = hm;
+      first_passage = 1;
+      if (progressed) gpu_progress_printout();
 #if mesh_bool
-            total_neighbours = (int)total_nb;
-#endif
-            end_of_timestep(moonlets, progressed);
-      } else {
-            how_many_moonlets = hm;
-            first_passage = 1;
-#if mesh_bool
-            if ((collision_bool || mutual_bool) && !force_naive_bool) {
-                  average_neighbours = 2.0 * ((typ)total_nb) / ((typ)how_many_moonlets);
-                  gam *= pow(how_many_neighbours / average_neighbours, 1.0 / 3.0);
-                  if (gam < gam_min) gam = gam_min;
-                  collision_cube = gam * ((typ)collision_cube_cells);
-            }
+      if ((collision_bool || mutual_bool) && !force_naive_bool) {
             how_many_pairs = 0;
+            average_neighbours = 2.0 * ((typ)total_nb) / ((typ)how_many_moonlets);
+            gam *= pow(how_many_neighbours / average_neighbours, 1.0 / 3.0);
+            if (gam < gam_min) gam = gam_min;
+            collision_cube = gam * ((typ)collision_cube_cells);
+            if (progressed) {
+                  printf("                  average number of neighbours = %.3lf\n", average_neighbours);
+                  printf("                  gamma = %.6lf\n", gam);
+            }
+            how_many_modified = 0;
+            how_many_big = 0;
+            how_many_small = 0;
             total_neighbours = 0;
-#endif
-            if (!brute_force_bool && !force_naive_bool && how_many_moonlets < switch_to_brute_force)
-                  force_naive_bool = 1;
-            else if (!brute_force_bool && force_naive_bool && how_many_moonlets > switch_to_brute_force)
-                  force_naive_bool = 0;
       }
+#endif
+      if (!brute_force_bool && !force_naive_bool && how_many_moonlets < switch_to_brute_force)
+            force_naive_bool = 1;
+      else if (!brute_force_bool && force_naive_bool && how_many_moonlets > switch_to_brute_force)
+            force_naive_bool = 0;
+      if (J2_bool) gpu_check(ncgpu_get_j2(&J2, NULL), "J2");  /* after end_of_timestep's update */
+      (void)moonlets;  /* the host copy is refreshed only where the host uses it (gpu_pull) */
       gpu_check(ncgpu_set_force_naive(force_naive_bool), "force_naive");
-      (void)total_nb;
 }
 
 static void gpu_start(struct moonlet **moonlets, struct moonlet **buffer)
