@@ -328,6 +328,61 @@ def bench_output(lib, api, torch, reps=5, cpu=True):
     return out
 
 
+def bench_programs():
+    """The whole reference program and its drop-in build on the same init.txt,
+    host wall clock: the brute-force driver on the N=2,000 collisional disk
+    (200 steps, outputs every 50), the mesh driver on a 20,000-body disk with
+    bodies larger than the mesh size (100 steps, outputs every 25) and on
+    200,000 bodies of the mesh workload's disk (20 steps, outputs every 10).
+    Output files and console output of the two are byte-identical (tests).
+    Needs the programs built from the reference sources (oracle/_ref)."""
+    import shutil
+    import tempfile
+    import time
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from ncorpion_b200 import disks
+    out = {"metric": "whole-program wall time, reference program vs drop-in build"}
+    cases = [("bf_merge", "collisional disk N=2,000, brute-force driver, 200 steps",
+              lambda: disks.bf_collide_disk(2000, seed=0)),
+             ("mesh_prog", "20,000-body disk (four bodies larger than the mesh size), mesh driver, 100 steps",
+              None),
+             ("mesh_prog_200k", "200,000-body disk of the mesh workload (radii dN/dR~R^-3.5 over [1e-5,1e-3]), "
+              "mesh driver, 20 steps, outputs every 10", lambda: disks.mesh_disk(200000, seed=0))]
+    for prof, what, make in cases:
+        ref = os.path.join(ROOT, "oracle", "_ref", prof, "ncorpion")
+        gpu = os.path.join(ROOT, "oracle", "_ref", prof, "ncorpion_gpu")
+        if not (os.path.exists(ref) and os.path.exists(gpu)):
+            out[prof] = {"unavailable": "programs not built (oracle/ref_build.py needs the reference sources)"}
+            continue
+        if make is None:
+            from make_golden import big_disk
+            bodies = big_disk(20000, 7)[0]
+        else:
+            bodies = make()
+        res = {"workload": what}
+        for name, exe in (("reference", ref), ("dropin", gpu)):
+            walls, integ = [], []
+            for _ in range(2):  # the better of two runs
+                d = tempfile.mkdtemp(prefix="ncgpu_prog_")
+                disks.write_init_txt(os.path.join(d, "init.txt"), bodies)
+                t0 = time.perf_counter()
+                r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=900)
+                walls.append(time.perf_counter() - t0)
+                res[name + "_rc"] = r.returncode
+                # main()'s own timing of the integration (src/main.c): "The integration took X seconds"
+                for line in r.stdout.splitlines():
+                    if "integration took" in line:
+                        integ.append(float(line.split("took")[1].split()[0]))
+                shutil.rmtree(d, ignore_errors=True)
+            res[name + "_s"] = min(walls)
+            res[name + "_integration_s"] = min(integ) if integ else None
+        res["speedup"] = res["reference_s"] / res["dropin_s"]
+        if res["reference_integration_s"] and res["dropin_integration_s"]:
+            res["speedup_integration"] = res["reference_integration_s"] / res["dropin_integration_s"]
+        out[prof] = res
+    return out
+
+
 CENTRAL_N = 262144
 CENTRAL_WORKLOAD = ("mesh steps (fast mode) of the N=262,144 mesh disk, 512 cells per side, alone, with the "
                     "fluid-body J2 (J2_value 0, Tearth 25), and with tides raised on the central body besides "
@@ -516,6 +571,7 @@ def main(argv=None):
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward+adjoint section")
     ap.add_argument("--no-central", action="store_true", help="skip the J2 / tides section")
     ap.add_argument("--no-output", action="store_true", help="skip the output-step section")
+    ap.add_argument("--no-programs", action="store_true", help="skip the whole-program section")
     ap.add_argument("--mesh-n", type=int, default=MESH_N, help="mesh workload bodies (smaller cases for profiling)")
     ap.add_argument("--mesh-cells", type=int, default=1024)
     ap.add_argument("--mesh-steps", type=int, default=MESH_STEPS)
@@ -691,6 +747,7 @@ def main(argv=None):
     adjoint = None if a.no_adjoint else bench_adjoint(lib, api, torch)
     central = None if a.no_central else bench_central(lib, api, torch)
     output = None if a.no_output else bench_output(lib, api, torch, cpu=(rank == 0 and ws == 1 and not a.no_cpu_baseline))
+    programs = bench_programs() if (rank == 0 and ws == 1 and not a.no_programs and not a.no_cpu_baseline) else None
     frag = None
     if not a.no_frag:
         fm = bench_fragment(lib, api, torch, api.GRAVITY_MIXED, FRAG_STEPS)
@@ -752,6 +809,7 @@ def main(argv=None):
             "adjoint": adjoint,
             "central_body": central,
             "output_step": output,
+            "programs": programs,
             "accuracy": {"mutual_rel_err_max": float(rel_mut.max()),
                          "mutual_rel_err_median": float(np.median(rel_mut)),
                          "total_rel_err_max": float(rel_tot.max()),

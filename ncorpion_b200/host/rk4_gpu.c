@@ -425,9 +425,23 @@ static void gpu_start(struct moonlet **moonlets, struct moonlet **buffer)
       gpu_check(ncgpu_set_force_naive(force_naive_bool), "force_naive");
 }
 
-static void gpu_stop(struct moonlet *moonlets, struct moonlet *buffer, bigint iter)
+/* The last output without a state copy (write_to_files_bool, no resume
+   files): the final half backward drift or kick already ran on a device
+   snapshot, which is printed here.  Returns 0 when the host must print it. */
+static int gpu_final_display_device(struct moonlet *buffer)
 {
-      if (write_to_files_bool) display(moonlets);
+      int done = gpu_display_device();
+      if (!done) {
+            gpu_snapshot_pull(buffer);
+            display(buffer);
+      }
+      gpu_check(ncgpu_snapshot_end(), "snapshot");
+      return 1;
+}
+
+static void gpu_stop(struct moonlet *moonlets, struct moonlet *buffer, bigint iter, int displayed)
+{
+      if (write_to_files_bool && !displayed) display(moonlets);
       if (resume_simulation_bool) {
             resume(moonlets);
             resumeFile();
@@ -452,7 +466,7 @@ void ncgpu_integration_brute_force_SABA1(typ t)
       if (write_to_files_bool) {
             readme();
             if (central_mass_bool) CM_buffer = CM;
-            display(moonlets);
+            if (!gpu_display_device()) display(moonlets);  /* the uploaded state, formatted on the device */
       }
       if (t > 0.0) {  /* half drift */
             timestep /= 2.0;
@@ -490,6 +504,15 @@ void ncgpu_integration_brute_force_SABA1(typ t)
             }
             gpu_end_of_timestep(moonlets, progressed, 0);
       }
+      if (write_to_files_bool && !resume_simulation_bool) {  /* the last output from a device snapshot */
+            gpu_check(ncgpu_snapshot_begin(), "snapshot");
+            if (t > 0.) {  /* half backward drift of the final output */
+                  gpu_check(ncgpu_set_timestep(timestep / -2.), "timestep");
+                  gpu_check(ncgpu_drift(), "drift");
+            }
+            gpu_stop(moonlets, moonlet_buffer, iter, gpu_final_display_device(moonlet_buffer));
+            return;
+      }
       gpu_pull(moonlets);
       if (central_mass_bool) CM_buffer = CM;
       if (t > 0.) {  /* half backward drift of the final output */
@@ -497,7 +520,7 @@ void ncgpu_integration_brute_force_SABA1(typ t)
             drift(moonlets, &CM_buffer);
             timestep *= -2.;
       }
-      gpu_stop(moonlets, moonlet_buffer, iter);
+      gpu_stop(moonlets, moonlet_buffer, iter, 0);
 }
 
 #if mesh_bool
@@ -529,7 +552,7 @@ void ncgpu_integration_mesh(typ t)
       if (write_to_files_bool) {
             readme();
             if (central_mass_bool) CM_buffer = CM;
-            display(moonlets);
+            if (!gpu_display_device()) display(moonlets);  /* the uploaded state, formatted on the device */
       }
       if (t > 0.0) {  /* half kick */
             timestep /= 2.0;
@@ -593,6 +616,21 @@ void ncgpu_integration_mesh(typ t)
             }
             gpu_end_of_timestep(moonlets, progressed, tn);
       }
+      if (write_to_files_bool && !resume_simulation_bool) {  /* the last output from a device snapshot */
+            gpu_check(ncgpu_snapshot_begin(), "snapshot");
+            if (t > 0.0) {  /* half backward kick of the final state */
+                  gpu_check(ncgpu_set_timestep(timestep / -2.0), "timestep");
+                  if (!force_naive_bool) {
+                        int np = 0, ne = 0;
+                        long tn0 = 0;
+                        gpu_check(ncgpu_three_largest(NULL), "three_largest");
+                        gpu_check(ncgpu_mesh(gam, 0, &np, &ne, &tn0), "mesh");
+                  }
+                  gpu_check(ncgpu_kick(), "kick");
+            }
+            gpu_stop(moonlets, moonlet_buffer, iter, gpu_final_display_device(moonlet_buffer));
+            return;
+      }
       if (central_mass_bool) CM_buffer = CM;
       if (t > 0.0) {  /* half backward kick of the final state (the central mass kick goes to CM_buffer) */
             gpu_pull(moonlets);
@@ -606,6 +644,6 @@ void ncgpu_integration_mesh(typ t)
             kick(moonlets, &CM_buffer, vector_field);
             timestep *= -2.0;
       }
-      gpu_stop(moonlets, moonlet_buffer, iter);
+      gpu_stop(moonlets, moonlet_buffer, iter, 0);
 }
 #endif

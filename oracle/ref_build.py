@@ -158,6 +158,11 @@ PROFILES = {
                             Delta_t="1.0", J2_bool="1", J2_value="0.", Tearth="25.", collision_cube_cells="256",
                             N_max="30000", N_0="20000", t_end="0.05", time_step="0.0005", output_step="25",
                             write_to_files_bool="1", write_cartesian_bool="1", write_collisions_bool="1"),
+    # a larger run of the mesh driver (bench: whole-program wall time): 200,000
+    # bodies of the mesh workload's disk, 20 steps, outputs every 10
+    "mesh_prog_200k": dict(MESH, collision_bool="1", instant_merger_bool="1", collision_cube_cells="1024",
+                           N_max="250000", N_0="200000", t_end="0.01", time_step="0.0005", output_step="10",
+                           write_to_files_bool="1", write_cartesian_bool="1", write_collisions_bool="1"),
     # the N = 1,048,576 mesh workload: 1024 cells per side (8.6 GB hash table)
     "mesh_merge_1m": dict(MESH, collision_bool="1", instant_merger_bool="1",
                           collision_cube_cells="1024", N_max="1100000", N_0="1048576",

@@ -286,18 +286,26 @@ def filtered_stdout(text):
     return "\n".join(l for l in text.splitlines() if "integration took" not in l)
 
 
-def program_run_case(profile, bodies, bodies_from=None):
+def program_run_case(profile, bodies, bodies_from=None, disk=None):
     """The whole reference program (oracle/_ref/<profile>/ncorpion) run on
     init.txt: digests of every output file and of the console output.  With
     bodies_from, the fixture names the fixture that holds the same bodies
-    instead of storing them again."""
+    instead of storing them again; with disk = (generator, n, seed), a large
+    input is stored as the recipe of ncorpion_b200.disks plus the digest of
+    its init.txt (the test regenerates it and checks the digest first)."""
     import subprocess
     import tempfile
     d = tempfile.mkdtemp(prefix="ncref_run_")
     disks.write_init_txt(os.path.join(d, "init.txt"), bodies)
     exe = os.path.join(ROOT, "oracle", "_ref", profile, "ncorpion")
     r = subprocess.run([exe], cwd=d, capture_output=True, text=True, check=True)
-    out = dict(bodies=bodies) if bodies_from is None else dict(bodies_from=np.array(bodies_from))
+    if disk is not None:
+        out = dict(disk_generator=np.array(disk[0]), disk_n=np.int64(disk[1]), disk_seed=np.int64(disk[2]),
+                   digest_init=digest(np.frombuffer(open(os.path.join(d, "init.txt"), "rb").read(), np.uint8)))
+    elif bodies_from is not None:
+        out = dict(bodies_from=np.array(bodies_from))
+    else:
+        out = dict(bodies=bodies)
     for f in OUTPUT_FILES:
         data = open(os.path.join(d, f), "rb").read()
         out["digest_" + f] = digest(np.frombuffer(data, np.uint8))
@@ -350,6 +358,9 @@ def main(names=None):
                                                              bodies_from="program_bf_merge")
     out["program_mesh_merge_tides"] = lambda: program_run_case("mesh_prog_tides", big_disk(20000, 7)[0],
                                                                bodies_from="program_mesh_merge")
+    # the mesh driver on 200,000 bodies of the mesh workload's disk, 20 steps
+    out["program_mesh_merge_200k"] = lambda: program_run_case("mesh_prog_200k", disks.mesh_disk(200000, seed=0),
+                                                              disk=("mesh_disk", 200000, 0))
     for k, make in out.items():
         if names and k not in names:
             continue

@@ -7,6 +7,9 @@ drivers taken from ncorpion_b200/host/rk4_gpu.c on libncgpu.so
 - mesh (mesh_prog): a 20,000-body disk with bodies larger than the mesh size,
   100 steps (mesh search with mergers, mesh gravity, adaptive mesh size,
   outputs every 25 steps);
+- the mesh driver on 200,000 bodies of the mesh workload's disk, 20 steps
+  (mesh_prog_200k; the input is regenerated from its recipe and checked
+  against its digest);
 - both again with the central body's fluid-body J2 (bf_merge_j2,
   mesh_prog_j2: J2_value 0, Tearth 25), and with tides raised on the central
   body besides (bf_merge_tides, mesh_prog_tides: Delta_t 1), whose rotation
@@ -29,7 +32,8 @@ pytestmark = pytest.mark.gpu
 
 PROGRAMS = [("bf_merge", "program_bf_merge"), ("mesh_prog", "program_mesh_merge"),
             ("bf_merge_j2", "program_bf_merge_j2"), ("mesh_prog_j2", "program_mesh_merge_j2"),
-            ("bf_merge_tides", "program_bf_merge_tides"), ("mesh_prog_tides", "program_mesh_merge_tides")]
+            ("bf_merge_tides", "program_bf_merge_tides"), ("mesh_prog_tides", "program_mesh_merge_tides"),
+            ("mesh_prog_200k", "program_mesh_merge_200k")]
 
 
 def _digest(b):
@@ -48,8 +52,14 @@ def test_dropin_program_matches_reference_outputs(lib, profile, fixture):
     from ncorpion_b200 import disks
     g = golden(fixture)
     d = tempfile.mkdtemp(prefix="ncgpu_dropin_")
-    bodies = golden(str(g["bodies_from"]))["bodies"] if "bodies_from" in g else g["bodies"]
+    if "disk_generator" in g:  # a large input stored as its recipe
+        bodies = getattr(disks, str(g["disk_generator"]))(int(g["disk_n"]), seed=int(g["disk_seed"]))
+    else:
+        bodies = golden(str(g["bodies_from"]))["bodies"] if "bodies_from" in g else g["bodies"]
     disks.write_init_txt(os.path.join(d, "init.txt"), bodies)
+    if "digest_init" in g:
+        init = open(os.path.join(d, "init.txt"), "rb").read()
+        assert np.array_equal(_digest(init), g["digest_init"]), "the regenerated input differs from the fixture's"
     r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     bad = []
