@@ -572,6 +572,9 @@ def main(argv=None):
     ap.add_argument("--no-central", action="store_true", help="skip the J2 / tides section")
     ap.add_argument("--no-output", action="store_true", help="skip the output-step section")
     ap.add_argument("--no-programs", action="store_true", help="skip the whole-program section")
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="collectives between the ranks (gloo: several ranks may share one GPU, e.g. to test the "
+                         "multi-rank path on a one-GPU machine)")
     ap.add_argument("--mesh-n", type=int, default=MESH_N, help="mesh workload bodies (smaller cases for profiling)")
     ap.add_argument("--mesh-cells", type=int, default=1024)
     ap.add_argument("--mesh-steps", type=int, default=MESH_STEPS)
@@ -582,11 +585,13 @@ def main(argv=None):
         return run_reference_arm(a, ws, rank)
 
     import torch
+    if a.dist_backend == "gloo" and local >= torch.cuda.device_count():
+        local = local % torch.cuda.device_count()  # ranks sharing a GPU (gloo only)
     torch.cuda.set_device(local)
     if ws > 1:
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist.init_process_group(a.dist_backend, timeout=timedelta(seconds=120))
     from ncorpion_b200 import api, build
     if not os.path.exists(api.LIB_PATH):
         build.build()

@@ -111,3 +111,31 @@ def test_part_arguments_checked(lib):
             assert st == api.E_ARG
     finally:
         api.finalize()
+
+
+def test_bench_two_ranks_share_one_gpu():
+    """bench.py's multi-rank path (the gravity headline split over the ranks,
+    one all-reduce per step) with two ranks on one GPU over gloo: it runs to
+    the end and reports the whole field's accuracy unchanged.  (NCCL needs one
+    GPU per rank; the collective here goes through the host.)"""
+    import json
+    import os
+    import socket
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", str(port), os.path.join(root, "bench.py"), "--gpus", "2", "--steps", "3",
+           "--warmup", "3", "--dist-backend", "gloo", "--no-mesh", "--no-frag", "--no-bf", "--no-adjoint",
+           "--no-central", "--no-output", "--no-cpu-baseline"]
+    r = subprocess.run(cmd, cwd=root, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout[-2000:]
+    out = json.loads(lines[0])
+    assert out["n_gpus"] == 2 and out["scaling"] == "strong"
+    assert out["accuracy"]["mutual_rel_err_max"] < 1e-6
+    assert out["accuracy"]["total_rel_err_max"] < 1e-8
