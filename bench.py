@@ -40,8 +40,9 @@ N_BODIES = 65536
 SOFTENING = 0.5
 FLOP_PER_INTERACTION = 20  # 3 sub, 3 FMA (r^2+eps^2), rsqrt (2), 3 mul, 3 FMA accumulate
 # DRAM bytes (read + write) of one k_grav_tiled<mixed> launch at N=65,536, from one ncu capture of
-# this script's gravity workload (profiles/k_grav_tiled_mixed_n65536.txt): 3.35 MB read + 58.09 MB written.
-MIXED_DRAM_BYTES = 61.45e6
+# this script's gravity workload (profiles/k_grav_tiled_mixed_n65536.txt): 3.21 MB read + 103.57 MB written
+# (the written bytes are the per-chunk partial sums: 103 source chunks x 3 x 65,536 doubles).
+MIXED_DRAM_BYTES = 106.78e6
 # DRAM bytes of one mesh step's two main kernels (k_mesh_write + k_mesh_grav) captured at N=262,144
 # (profiles/k_mesh_write_grav_n262144.txt: 44.1 MB + 101.2 MB), scaled by the bodies to N=1,048,576.
 MESH_DRAM_BYTES_262K = 145.3e6
