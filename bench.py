@@ -799,7 +799,9 @@ def main(argv=None):
                          "rsqrt_bound_frac": (pairs / ws) / (kms_mixed * 1e-3) / (rates["rsqrt_gops"] * 1e9)},
             "cpu_baseline": cpu,
             "e2e": {"value": pairs / e2e_s, "unit": "pair-interactions/s",
-                    "h2d_bytes_per_step": int(hb.nbytes + hex_.nbytes), "d2h_bytes_per_step": int(n * 24 + 24),
+                    "h2d_bytes_per_step": int(hb.nbytes + hex_.nbytes),
+                    # one GPU: the records come back whole (64 B each) + CM_acc; N GPUs: the field (24 B each)
+                    "d2h_bytes_per_step": int(n * 64 + 24) if ws == 1 else int(n * 24),
                     "ms_per_step": e2e_s * 1e3},
             "gpu_launches": launches,
             "clocks": clocks,

@@ -143,7 +143,9 @@ const char *ncgpu_last_error(void);
    acceleration of body k into bodies[k].vx, vy, vz (the reference stores
    accelerations in the velocity fields, src/physics.c:264-266) and the central
    mass back-reaction into cm_acc[3] (CM_acc, src/physics.c:137-139).  Host
-   buffers; copies in and out on the library stream. */
+   buffers; copies in and out on the library stream.  The records come back
+   whole in one copy: every byte other than those velocity fields is the
+   caller's own (on an error status the velocity fields may be overwritten). */
 int ncgpu_vector_field(struct ncgpu_body *bodies, const int *exists, int largest_id,
                        const struct ncgpu_body *cm, double *cm_acc, int gravity_mode);
 

@@ -92,6 +92,19 @@ __global__ void k_aos_to_soa(const double *__restrict__ aos, int n, double *x, d
       m[i] = b[6]; R[i] = b[7];
 }
 
+// The accelerations of the existing bodies into the velocity fields of the
+// device copy of the caller's records (the other fields keep the bytes the
+// caller sent), so that one contiguous copy returns them.
+__global__ void k_acc_into_aos(double *__restrict__ aos, const int *__restrict__ ex, int n,
+                               const double *__restrict__ ax, const double *__restrict__ ay,
+                               const double *__restrict__ az)
+{
+      int i = blockIdx.x * blockDim.x + threadIdx.x;
+      if (i >= n || !ex[i]) return;
+      double *b = aos + 8 * (size_t)i;
+      b[3] = ax[i]; b[4] = ay[i]; b[5] = az[i];
+}
+
 __global__ void k_soa_to_aos(double *__restrict__ aos, int n, const double *x, const double *y, const double *z,
                              const double *vx, const double *vy, const double *vz, const double *m, const double *R)
 {
@@ -486,25 +499,21 @@ int ncgpu_vector_field(struct ncgpu_body *bodies, const int *exists, int largest
       BodyView bv{c.aos, c.aos + 1, c.aos + 2, c.aos + 3, c.aos + 4, c.aos + 5, c.aos + 6, c.aos + 7, 8, c.exs};
       const J2Arg j2 = j2_arg(c.P, cm->mass, j2_value(c.P, cm->mass, c.P.par_sideral_omega));
       NCG_TRY(gravity_eval(bv, largest_id, (const double *)cm, j2, c.acc, c.n_max, c.cm_acc, gravity_mode, st));
-      double *h = c.pinned;
+      // the records come back whole: the velocity fields of the existing bodies
+      // carry their accelerations, every other byte is the caller's own
       if (ns > 0) {
-            NCG_CK(cudaMemcpyAsync(h, c.acc, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
-            NCG_CK(cudaMemcpyAsync(h + ns, c.acc + c.n_max, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
-            NCG_CK(cudaMemcpyAsync(h + 2 * ns, c.acc + 2 * (size_t)c.n_max, sizeof(double) * ns,
-                                   cudaMemcpyDeviceToHost, st));
+            k_acc_into_aos<<<(ns + 255) / 256, 256, 0, st>>>(c.aos, c.exs, ns, c.acc, c.acc + c.n_max,
+                                                            c.acc + 2 * (size_t)c.n_max);
+            NCG_LAUNCHED();
+            NCG_CK(cudaMemcpyAsync(bodies, c.aos, sizeof(struct ncgpu_body) * (size_t)ns, cudaMemcpyDeviceToHost, st));
       }
-      NCG_CK(cudaMemcpyAsync(h + 3 * ns, c.cm_acc, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      double *h = c.pinned;
+      NCG_CK(cudaMemcpyAsync(h, c.cm_acc, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
       NCG_CK(cudaStreamSynchronize(st));
       NCG_TRY(check_err_word());
-      for (int k = 0; k < ns; k++) {
-            if (!exists[k]) continue;
-            bodies[k].vx = h[k];
-            bodies[k].vy = h[ns + k];
-            bodies[k].vz = h[2 * ns + k];
-      }
-      cm_acc[0] = h[3 * ns];
-      cm_acc[1] = h[3 * ns + 1];
-      cm_acc[2] = h[3 * ns + 2];
+      cm_acc[0] = h[0];
+      cm_acc[1] = h[1];
+      cm_acc[2] = h[2];
       return NCGPU_OK;
 }
 

@@ -120,3 +120,35 @@ def test_state_errors(gpu):
     with pytest.raises(A.NcgpuError) as e:
         api.vector_field(b, np.ones(32, np.int32), None)
     assert e.value.status == A.E_ARG
+
+
+def test_host_call_writes_only_the_velocity_fields_of_existing_bodies(gpu, port):
+    """ncgpu_vector_field returns the caller's records whole: the existing
+    bodies' vx, vy, vz hold their accelerations (bit-identical to the
+    oracle's vector_field in the exact mode); every other byte, the holes'
+    velocity fields (signed zeros and NaN payloads here) included, is the
+    caller's own."""
+    import ctypes as C
+    from ncorpion_b200 import disks
+    n = 700
+    b = disks.gravity_disk(n, seed=21)
+    rng = np.random.default_rng(21)
+    ex = (rng.random(n) > 0.2).astype(np.int32)
+    holes = np.flatnonzero(ex == 0)
+    bits = b.view(np.int64)
+    bits[holes[0::3], 3] = np.int64(0x7FF8DEADBEEF0001)   # NaN with a payload
+    bits[holes[1::3], 4] = np.int64(-0x8000000000000000)  # -0.0
+    b[holes[2::3], 5] = -1.5e300
+    before = b.copy()
+    cm = np.array([1e-7, -2e-7, 0, 0, 0, 0, 1.0, 1.0])
+    api = gpu(1024, softening_parameter=0.5)
+    lib = api.load()
+    cma = np.zeros(3)
+    api.check(lib.ncgpu_vector_field(api.ptr(b), api.ptr(ex), n - 1, api.ptr(cm), api.ptr(cma), api.GRAVITY_EXACT),
+              "ncgpu_vector_field")
+    a_ref, c_ref = port.vector_field(before, ex, cm, make_params(softening_parameter=0.5))
+    live = ex == 1
+    assert np.array_equal(b[:, [0, 1, 2, 6, 7]].view(np.int64), before[:, [0, 1, 2, 6, 7]].view(np.int64))
+    assert np.array_equal(b[~live].view(np.int64), before[~live].view(np.int64))
+    assert np.array_equal(b[live, 3:6].view(np.int64), a_ref[live].view(np.int64))
+    assert np.array_equal(cma, c_ref)
