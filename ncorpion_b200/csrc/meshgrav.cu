@@ -332,9 +332,19 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
       // and partners), then the bodies appended after the pass
       const int t = blockIdx.x * blockDim.x + threadIdx.x;
       if (t > A.lid) return;
-      const int b = (have_cells && t <= A.lid0) ? vals[t] : t;
+      const bool incell = have_cells && t <= A.lid0;
+      const int b = incell ? vals[t] : t;
       const int f = A.j2.on ? 2 : 1;
-      if (!S.ex[b]) {
+      // this body's fields, loaded once: from its cell-ordered record (one
+      // contiguous 64-byte read; the same values as the state arrays)
+      GRec me;
+      if (incell) {
+            me = grec[t];
+      } else {
+            me.x = S.x[b]; me.y = S.y[b]; me.z = S.z[b]; me.m = S.m[b]; me.R = S.R[b];
+            me.ex = S.ex[b];
+      }
+      if (!me.ex) {
             // an empty slot adds +0.0 to every chain (they then read all terms
             // without looking at exists[])
             for (int w = 0; w < 9; w++) terms[(size_t)w * N + b] = 0.;
@@ -344,20 +354,20 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
       }
       double a_x = 0., a_y = 0., a_z = 0.;
       if (A.central) {
-            double DX = DSUB(S.x[b], A.cmx), DY = DSUB(S.y[b], A.cmy), DZ = DSUB(S.z[b], A.cmz);
+            double DX = DSUB(me.x, A.cmx), DY = DSUB(me.y, A.cmy), DZ = DSUB(me.z, A.cmz);
             double rk = __dsqrt_rn(DADD(DADD(DMUL(DX, DX), DMUL(DY, DY)), DMUL(DZ, DZ)));
             double r3 = DMUL(DMUL(rk, rk), rk);
             const double y3 = __drcp_rn(r3);  // the six quotients by r3 share RN(1/r3)
             a_x = div_by_recip(DMUL(-A.mu, DX), r3, y3);
             a_y = div_by_recip(DMUL(-A.mu, DY), r3, y3);
             a_z = div_by_recip(DMUL(-A.mu, DZ), r3, y3);
-            double g = DMUL(A.G, S.m[b]);
+            double g = DMUL(A.G, me.m);
             cm_chain(terms, A, N, 0)[f * b] = div_by_recip(DMUL(g, DX), r3, y3);
             cm_chain(terms, A, N, 1)[f * b] = div_by_recip(DMUL(g, DY), r3, y3);
             cm_chain(terms, A, N, 2)[f * b] = div_by_recip(DMUL(g, DZ), r3, y3);
             if (A.j2.on) {  // src/physics.c:149-160
                   double cj[3];
-                  d_j2(A.j2, A.mu, DX, DY, DZ, rk, r3, S.m[b], a_x, a_y, a_z, cj);
+                  d_j2(A.j2, A.mu, DX, DY, DZ, rk, r3, me.m, a_x, a_y, a_z, cj);
                   for (int c = 0; c < 3; c++) cm_chain(terms, A, N, c)[2 * b + 1] = cj[c];
             }
       }
@@ -366,7 +376,7 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
             return;
       }
       if (A.mutual) {
-            const double xb = S.x[b], yb = S.y[b], zb = S.z[b], Rb = S.R[b], mb = S.m[b];
+            const double xb = me.x, yb = me.y, zb = me.z, Rb = me.R, mb = me.m;
             for (int i = 0; i < 3; i++) {
                   if (!S.ex[i]) continue;
                   // pair_add(b, i) and big_term(b, i) share D^3 (the squared
@@ -435,7 +445,7 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                   ++vi;
             }
             if (L >= 0) {
-                  const double xb = S.x[b], yb = S.y[b], zb = S.z[b], Rb = S.R[b];
+                  const double xb = me.x, yb = me.y, zb = me.z, Rb = me.R;
                   // own pops: cells 26..0, lower indices ascending
                   int cur[27];
                   for (int l = 26; l >= 0; --l) {
