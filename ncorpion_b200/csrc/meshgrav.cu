@@ -283,6 +283,8 @@ struct MGArgs {
       const int *vis;           // (body, first, end) candidate positions, in visit order
       const int *cp;            // candidate partners (a visit's list ascends)
       J2Arg j2;                 // the central body's J2 term
+      int cellterms;            // terms of bodies 0..2 and CM_acc at the walk's (cell-order)
+                                // position, for the parallel sums; else at the slot (exact chains)
 };
 
 // CM_acc's chain c (0..2) in `terms`: after the 9 chains of bodies 0..2, one
@@ -334,6 +336,7 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
       if (t > A.lid) return;
       const bool incell = have_cells && t <= A.lid0;
       const int b = incell ? vals[t] : t;
+      const long ti = A.cellterms ? t : b;  // where this body's terms go (coalesced in cell order)
       const int f = A.j2.on ? 2 : 1;
       // this body's fields, loaded once: from its cell-ordered record (one
       // contiguous 64-byte read; the same values as the state arrays)
@@ -347,9 +350,9 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
       if (!me.ex) {
             // an empty slot adds +0.0 to every chain (they then read all terms
             // without looking at exists[])
-            for (int w = 0; w < 9; w++) terms[(size_t)w * N + b] = 0.;
+            for (int w = 0; w < 9; w++) terms[(size_t)w * N + ti] = 0.;
             for (int c = 0; c < 3; c++)
-                  for (int u = 0; u < f; u++) cm_chain(terms, A, N, c)[f * b + u] = 0.;
+                  for (int u = 0; u < f; u++) cm_chain(terms, A, N, c)[f * ti + u] = 0.;
             return;
       }
       double a_x = 0., a_y = 0., a_z = 0.;
@@ -362,17 +365,19 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
             a_y = div_by_recip(DMUL(-A.mu, DY), r3, y3);
             a_z = div_by_recip(DMUL(-A.mu, DZ), r3, y3);
             double g = DMUL(A.G, me.m);
-            cm_chain(terms, A, N, 0)[f * b] = div_by_recip(DMUL(g, DX), r3, y3);
-            cm_chain(terms, A, N, 1)[f * b] = div_by_recip(DMUL(g, DY), r3, y3);
-            cm_chain(terms, A, N, 2)[f * b] = div_by_recip(DMUL(g, DZ), r3, y3);
+            cm_chain(terms, A, N, 0)[f * ti] = div_by_recip(DMUL(g, DX), r3, y3);
+            cm_chain(terms, A, N, 1)[f * ti] = div_by_recip(DMUL(g, DY), r3, y3);
+            cm_chain(terms, A, N, 2)[f * ti] = div_by_recip(DMUL(g, DZ), r3, y3);
             if (A.j2.on) {  // src/physics.c:149-160
                   double cj[3];
                   d_j2(A.j2, A.mu, DX, DY, DZ, rk, r3, me.m, a_x, a_y, a_z, cj);
-                  for (int c = 0; c < 3; c++) cm_chain(terms, A, N, c)[2 * b + 1] = cj[c];
+                  for (int c = 0; c < 3; c++) cm_chain(terms, A, N, c)[2 * ti + 1] = cj[c];
             }
       }
       if (b <= 2) {  // bodies 0..2: central term only here
             ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
+            if (A.cellterms)  // (the parallel sums read every position)
+                  for (int w = 0; w < 9; w++) terms[(size_t)w * N + ti] = 0.;
             return;
       }
       if (A.mutual) {
@@ -394,9 +399,9 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                   a_x = DADD(a_x, div_by_recip(DMUL(gi, dx), D3, y));
                   a_y = DADD(a_y, div_by_recip(DMUL(gi, dy), D3, y));
                   a_z = DADD(a_z, div_by_recip(DMUL(gi, dz), D3, y));
-                  terms[(3 * i) * N + b] = div_by_recip(DMUL(gb, DSUB(xb, S.x[i])), D3, y);
-                  terms[(3 * i + 1) * N + b] = div_by_recip(DMUL(gb, DSUB(yb, S.y[i])), D3, y);
-                  terms[(3 * i + 2) * N + b] = div_by_recip(DMUL(gb, DSUB(zb, S.z[i])), D3, y);
+                  terms[(3 * i) * N + ti] = div_by_recip(DMUL(gb, DSUB(xb, S.x[i])), D3, y);
+                  terms[(3 * i + 1) * N + ti] = div_by_recip(DMUL(gb, DSUB(yb, S.y[i])), D3, y);
+                  terms[(3 * i + 2) * N + ti] = div_by_recip(DMUL(gb, DSUB(zb, S.z[i])), D3, y);
             }
       }
       if (A.mutual && have_cells && b > A.lid0) {
@@ -536,9 +541,13 @@ __global__ void k_mesh_chains_part(DevState S, MGArgs A, const double *__restric
       const int n = A.lid + 1;
       const int f = A.j2.on ? 2 : 1;
       for (int k = blockIdx.x * RB12 + threadIdx.x; k < n; k += gridDim.x * RB12) {
-            if (!S.ex[k]) continue;
-            for (int w = 0; w < 9; w++)
-                  if (k >= 3) s[w] += terms[(size_t)w * N + k];
+            if (A.cellterms) {  // cell order: every position holds its terms (zeros for empty slots and bodies 0..2)
+                  for (int w = 0; w < 9; w++) s[w] += terms[(size_t)w * N + k];
+            } else {
+                  if (!S.ex[k]) continue;
+                  for (int w = 0; w < 9; w++)
+                        if (k >= 3) s[w] += terms[(size_t)w * N + k];
+            }
             for (int c = 0; c < 3; c++) {
                   const double *t = cm_chain(const_cast<double *>(terms), A, N, c) + (size_t)f * k;
                   s[9 + c] += f == 2 ? t[0] + t[1] : t[0];
@@ -643,7 +652,8 @@ int mesh_gravity_state(const double *cm8, const J2Arg &j2)
                c.P.par_softening_parameter != 0., (long long)c.cell_cap, c.P.par_G, c.P.par_softening_parameter,
                c.P.par_G * cm8[6], cm8[0], cm8[1], cm8[2],
                c.mesh_valid ? c.mesh_n - 1 : -1, c.P.par_N_tilde, c.mesh_nfev, c.evx, c.fev,
-               c.mesh_nfev > 0 ? c.xhead : nullptr, c.mesh_valid ? c.mesh_nvis : 0, c.vis, c.cand_p, j2};
+               c.mesh_nfev > 0 ? c.xhead : nullptr, c.mesh_valid ? c.mesh_nvis : 0, c.vis, c.cand_p, j2,
+               c.P.par_gravity_mode != NCGPU_GRAVITY_EXACT};
       double *ax = c.acc, *ay = c.acc + N, *az = c.acc + 2 * N;
       if (lid >= 0) {
             GRec *grec = (GRec *)c.mrec;
