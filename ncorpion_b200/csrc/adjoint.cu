@@ -335,7 +335,8 @@ void join3(double *dst, const double *src, int n, cudaStream_t st, cudaError_t *
                                    cudaMemcpyDeviceToHost, st);
 }
 
-__global__ void k_scale_R(const double *__restrict__ R, double sp, double *__restrict__ sR, int n)
+// sR = sp * R, element by element (in place when sR == R)
+__global__ void k_scale_R(const double *R, double sp, double *sR, int n)
 {
       int k = blockIdx.x * blockDim.x + threadIdx.x;
       if (k < n) sR[k] = sp * R[k];

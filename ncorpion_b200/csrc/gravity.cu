@@ -558,7 +558,6 @@ __global__ void __launch_bounds__(MXB, 12) k_grav_tiled(const D4 *__restrict__ s
       const D4 m0 = s64[v0 ? q0 : 0], m1 = s64[v1 ? q1 : 0];
       const double r0 = sR64[v0 ? q0 : 0], r1 = sR64[v1 ? q1 : 0];
       const float r0f = (float)r0, r1f = (float)r1;
-      const float eps2f = (float)eps2;
       const double *bi = box + ib * 6;
       // all radii equal: eps = 2 softening R for every pair (the loads of R skip)
       // (SOFT 1: the host found all radii equal and passes eps^2 = (2 sp R)^2)

@@ -252,25 +252,6 @@ __device__ __forceinline__ void pair_add_rec(double xb, double yb, double zb, do
       az = DADD(az, div_by_recip(DMUL(g, dz), D3, y));
 }
 
-// The term body b adds to body i (0..2) in the k > 2 loop: G*mk*DX/D3 with
-// DX = X_b - X_i (src/physics.c:216-257).
-__device__ __forceinline__ void big_term(const DevState &S, int b, int i, double G, double sp, bool soft, double *t)
-{
-      double dx = DSUB(S.x[b], S.x[i]), dy = DSUB(S.y[b], S.y[i]), dz = DSUB(S.z[b], S.z[i]);
-      double r2 = DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz));
-      if (soft) {
-            double s = DMUL(sp, DADD(S.R[b], S.R[i]));
-            r2 = DADD(r2, DMUL(s, s));
-      }
-      double D = __dsqrt_rn(r2);
-      double D3 = DMUL(DMUL(D, D), D);
-      double g = DMUL(G, S.m[b]);
-      const double y = __drcp_rn(D3);
-      t[0] = div_by_recip(DMUL(g, dx), D3, y);
-      t[1] = div_by_recip(DMUL(g, dy), D3, y);
-      t[2] = div_by_recip(DMUL(g, dz), D3, y);
-}
-
 struct MGArgs {
       int lid, d, central, mutual, soft;
       long long cell_cap;
@@ -384,8 +365,9 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
             const double xb = me.x, yb = me.y, zb = me.z, Rb = me.R, mb = me.m;
             for (int i = 0; i < 3; i++) {
                   if (!S.ex[i]) continue;
-                  // pair_add(b, i) and big_term(b, i) share D^3 (the squared
-                  // differences and the softening are the same numbers)
+                  // body b's term from i and i's term from b (G*m_b*(X_b - X_i)/D^3,
+                  // src/physics.c:216-257) share D^3: the squared differences and
+                  // the softening are the same numbers
                   double dx = DSUB(S.x[i], xb), dy = DSUB(S.y[i], yb), dz = DSUB(S.z[i], zb);
                   double r2 = DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz));
                   if (A.soft) {
