@@ -71,7 +71,10 @@ def dist_info():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 50 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms.  start()
+    returns once the first sample has arrived and stop() waits for one more,
+    so that samples bracket a timed region shorter than nvidia-smi's start-up
+    (each wait bounded)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -91,6 +94,13 @@ class ClockSampler:
             self.t.start()
         except FileNotFoundError:
             self.proc = None
+            return
+        self._wait_for(1, 5.0)
+
+    def _wait_for(self, n, limit_s):
+        t0 = time.monotonic()
+        while len(self.lines) < n and self.proc.poll() is None and time.monotonic() - t0 < limit_s:
+            time.sleep(0.005)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -99,6 +109,7 @@ class ClockSampler:
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self._wait_for(len(self.lines) + 1, 1.0)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
