@@ -215,8 +215,8 @@ def mesh_params(mode, cells=1024, **extra):
 def mesh_gamma0(n, cells=1024):
     """The initial mesh size of variable_initialization (src/structure.c:515-523)
     with sma 0.5 .. 2.0, inclination_max 0.015, how_many_neighbours 16."""
-    gam = (2.0 ** 3 - 0.5 ** 3) ** (1.0 / 3.0) * (4.0 * np.pi * 16.0 * np.sin(0.015) / (n * 81.0)) ** (1.0 / 3.0)
-    return max(gam, 4.4 / cells)
+    from ncorpion_b200 import api
+    return api.initial_gamma(n, cells, 0.5, 2.0, 0.015, 16.0, 4.4)
 
 
 def bench_mesh(lib, api, torch, mode, steps, warmup, n_bodies=None, cells=1024, **extra):

@@ -152,7 +152,10 @@ int ncgpu_vector_field(struct ncgpu_body *bodies, const int *exists, int largest
 /* Same computation on device-resident buffers: d_bodies holds 8 doubles per
    slot (struct moonlet layout), d_exists one int per slot, d_acc receives
    3 doubles per slot (zero for empty slots), d_cm_acc 3 doubles.  cm points to
-   host memory.  stream is a cudaStream_t (NULL = the library stream). */
+   host memory.  stream is a cudaStream_t (NULL = the library stream).  The
+   call is asynchronous on that stream: a device wait that gave up (or another
+   device-side error) is reported by ncgpu_check_error, or by the next call
+   that waits for the library stream. */
 int ncgpu_vector_field_dev(const double *d_bodies, const int *d_exists, int largest_id,
                            const struct ncgpu_body *cm, double *d_acc, double *d_cm_acc,
                            int gravity_mode, void *stream);
@@ -171,19 +174,35 @@ int ncgpu_vector_field_part(const double *d_bodies, const int *d_exists, int lar
                             const struct ncgpu_body *cm, int part, int nparts, double *d_acc,
                             double *d_cm_acc, int gravity_mode, void *stream);
 
+/* Waits for `stream` (NULL = the library stream) and for the library stream,
+   then returns and clears the status that device kernels recorded since the
+   last check: NCGPU_E_TIMEOUT for a bounded device wait that gave up,
+   NCGPU_E_CAPACITY / NCGPU_E_NMAX for a device-side overflow, NCGPU_OK when
+   nothing was recorded.  (No reference counterpart: the reference has no
+   asynchronous calls.) */
+int ncgpu_check_error(void *stream);
+
 /* Allocation-free variant of ncgpu_vector_field_dev in the EXACT mode.  It has
    no counterpart in the reference: it exists for callers that cannot allocate
    device memory when they evaluate forces (a host whose device memory belongs to
    its own pool allocator, an integration loop that forbids allocation once it
    runs).  It needs no ncgpu_init and calls no cudaMalloc or cudaFree: its scratch
    is a fixed file-scope device array of ncgpu_noalloc_scratch_bytes() bytes,
-   resident on every GPU that loads the library, sized for at most
+   held by every GPU that the library's device code is loaded on, sized for at most
    NCGPU_NOALLOC_MAX_SLOTS body slots (largest_id + 1 larger than that returns
-   NCGPU_E_CAPACITY).  The first call on a device looks up the array's device
-   address (cudaGetSymbolAddress), so make it before any stream capture.  All
-   calls share the array: calls that overlap on the GPU race.  params supplies
-   G, softening_parameter and central_mass_bool; the other arguments are those
-   of ncgpu_vector_field_dev (stream may be NULL: the default stream). */
+   NCGPU_E_CAPACITY).  CUDA loads device code lazily by default, so the array
+   and the kernels reach a device at the first call on it: that call is the
+   set-up (it loads them and looks up the array's device address with
+   cudaGetSymbolAddress).  Make one call on each device before the host's pool
+   allocator takes the device's memory and before any stream capture, or run
+   with CUDA_MODULE_LOADING=EAGER; after cudaDeviceReset do not call it again.
+   All calls share the array and it keeps the last call's contents: calls that
+   overlap on the GPU race.  params supplies G, softening_parameter,
+   central_mass_bool and the central body's J2 (par_J2_bool, par_J2, par_R_unit,
+   par_sideral_omega for the fluid-body J2 when par_J2 is 0; J2 without a
+   central mass returns NCGPU_E_ARG); the other arguments are those of
+   ncgpu_vector_field_dev (stream may be NULL: the default stream).  The call
+   waits for its stream and returns NCGPU_E_TIMEOUT if a device wait gave up. */
 #define NCGPU_NOALLOC_MAX_SLOTS 65536
 int ncgpu_vector_field_static(const double *d_bodies, const int *d_exists, int largest_id,
                               const struct ncgpu_body *cm, const struct ncgpu_params *params,

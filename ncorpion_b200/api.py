@@ -104,6 +104,7 @@ EXPORTS = {
     "ncgpu_last_launch_count": (C.c_int, []),
     "ncgpu_stream": (C.c_void_p, []),
     "ncgpu_vector_field_static": (C.c_int, [P, P, C.c_int, P, P, P, P, P]),
+    "ncgpu_check_error": (C.c_int, [P]),
     "ncgpu_noalloc_scratch_bytes": (C.c_ulong, []),
     "ncgpu_upload": (C.c_int, [P, P, C.c_int, P]),
     "ncgpu_download": (C.c_int, [P, P, P, P]),
@@ -333,6 +334,15 @@ def step_mesh(gam: float):
     hm, tn = C.c_int(0), C.c_long(0)
     check(load().ncgpu_step_mesh(float(gam), C.byref(hm), C.byref(tn)), "ncgpu_step_mesh")
     return hm.value, tn.value
+
+
+def initial_gamma(n_0, cells, sma_min, sma_max, inclination_max, how_many_neighbours, cube_min):
+    """Initial mesh size of variable_initialization (src/structure.c:515-523,
+    host side, libm pow), clamped below at cube_min / cells."""
+    gam = (sma_max ** 3 - sma_min ** 3) ** (1.0 / 3.0) * \
+        (4.0 * np.pi * how_many_neighbours * np.sin(inclination_max) / (float(n_0) * 81.0)) ** (1.0 / 3.0)
+    gam_min = cube_min / float(cells)
+    return gam_min if gam < gam_min else gam
 
 
 def update_gamma(gam, total_neighbours, how_many_moonlets, how_many_neighbours, gam_min):

@@ -482,6 +482,14 @@ int ncgpu_vector_field_part(const double *d_bodies, const int *d_exists, int lar
       return NCGPU_OK;
 }
 
+int ncgpu_check_error(void *stream)
+{
+      Ctx &c = g_ctx;
+      if (!c.inited) return NCGPU_E_STATE;
+      if (stream) NCG_CK(cudaStreamSynchronize((cudaStream_t)stream));
+      return check_err_word();
+}
+
 int ncgpu_vector_field(struct ncgpu_body *bodies, const int *exists, int largest_id, const struct ncgpu_body *cm,
                        double *cm_acc, int gravity_mode)
 {

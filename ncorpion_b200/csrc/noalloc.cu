@@ -8,16 +8,23 @@
 // ncgpu_init, allocates nothing (no cudaMalloc, cudaFree or allocating library
 // call), and keeps its scratch in the fixed file-scope device array below.
 //
-// The array is part of the library image: every GPU that loads libncgpu.so
-// holds NOALLOC_SCRATCH_BYTES of it until the process exits.  Host code cannot
-// use the array's name as a device address (on the host it is only a
-// stand-in); the first call on each device resolves the real address with
-// cudaGetSymbolAddress, with that device current, and caches it.  That first
-// call should therefore come before any stream capture.  All calls share the
-// one array and it keeps the last call's contents: what must start at zero is
-// cleared at every call, and calls that overlap on the GPU (other streams,
-// other host threads) race on it.
+// The array belongs to the library's device code: every GPU that loads that
+// code holds NOALLOC_SCRATCH_BYTES of it until the process exits.  CUDA loads
+// device code lazily by default (CUDA_MODULE_LOADING=LAZY), so the array and
+// the kernels reach a device at the first call on that device, not when the
+// library is opened.  The first call on each device is therefore the set-up:
+// with that device current it loads the code and the array, and resolves the
+// array's device address with cudaGetSymbolAddress (host code cannot use the
+// array's name as a device address: on the host it is only a stand-in).  Make
+// that first call before the host's pool allocator takes the device's memory
+// and before any stream capture, or run with CUDA_MODULE_LOADING=EAGER.  The
+// address is cached per device under a lock; cudaDeviceReset invalidates it,
+// so a process that resets a device must not call this entry point again.
+// All calls share the one array and it keeps the last call's contents: what
+// must start at zero is cleared at every call, and calls that overlap on the
+// GPU (other streams, other host threads) race on it.
 #include <string.h>
+#include <mutex>
 #include "common.cuh"
 
 namespace ncg {
@@ -41,13 +48,16 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH
 
 constexpr int MAX_DEVICES = 64;
 static unsigned char *g_scratch_addr[MAX_DEVICES];
+static std::mutex g_scratch_lock;
 
-// The device address of g_noalloc_scratch on the current device (resolved once).
+// The device address of g_noalloc_scratch on the current device, resolved at
+// the first call on that device and cached (a failed lookup is retried).
 int scratch_address(unsigned char **out)
 {
       int dev = 0;
       NCG_CK(cudaGetDevice(&dev));
       if (dev < 0 || dev >= MAX_DEVICES) return NCGPU_E_UNSUPPORTED;
+      std::lock_guard<std::mutex> hold(g_scratch_lock);
       if (!g_scratch_addr[dev]) {
             void *p = nullptr;
             NCG_CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));

@@ -26,7 +26,8 @@ Only build outputs are written under ``oracle/_ref/`` (git-ignored); the
 temporary copy is deleted.  The shipped prebuilt ``src/ncorpion`` is never
 copied, read or run.
 
-Usage: ``python oracle/ref_build.py [--src DIR] [profile ...]``
+Usage: ``python oracle/ref_build.py [--src DIR] [profile ...]`` (``DIR`` defaults to
+``$NCORPION_REF_SRC``).
 """
 from __future__ import annotations
 
@@ -41,7 +42,9 @@ import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-DEFAULT_SRC = "/root/reference/src"
+# the reference's src/ directory: --src, else $NCORPION_REF_SRC, else where this
+# build machine mounts the reference
+DEFAULT_SRC = os.environ.get("NCORPION_REF_SRC", "/root/reference/src")
 
 COMMON = {
     "write_to_files_bool": "0",

@@ -52,7 +52,7 @@ def make_params(**kw):
     p.collision_cube_min = 80.0
     p.switch_to_brute_force = 110
     p.gravity_mode = 0
-    p.near_theta = 0.25
+    p.near_theta = 0.15
     p.disruption_threshold = 0.1
     p.high_dumping_threshold = 100.0
     p.reduce_to_COM_bool = 1
