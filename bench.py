@@ -751,7 +751,8 @@ def main(argv=None):
         mesh = {"metric": f"mesh collision steps/s at N={a.mesh_n}", "workload": wl, "fast": mesh_fast,
                 "exact": mesh_exact,
                 "note": "fast: CM_acc and the three largest bodies' sums as two-level parallel sums; exact: "
-                        "sequential FP64 chains (bit-identical state); pairs[] and events are exact in both",
+                        "sequential FP64 chains (bit-identical state); the pass's pairs[], events and the exact "
+                        "mode's state are checked against the reference at this size by tests/test_mesh_1m_gpu.py",
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
                              "algorithmic_bytes_per_step": alg,
                              "traffic": MESH_DRAM_BYTES_262K * a.mesh_n / 262144,
@@ -790,8 +791,21 @@ def main(argv=None):
 
     if rank == 0:
         value = pairs / (ms_mixed * 1e-3)  # the whole job's field, split over the ranks
+        # the metric's second half, compact and early in the line (the full mesh record is further down)
+        mesh_headline = None
+        if mesh is not None:
+            mcpu = mesh.get("cpu_baseline") or {}
+            mesh_headline = {"n": a.mesh_n, "cells": a.mesh_cells,
+                             "fast_steps_per_s": mesh["fast"]["steps_per_s"],
+                             "fast_ms_per_step": mesh["fast"]["ms_per_step"],
+                             "exact_steps_per_s": mesh["exact"]["steps_per_s"],
+                             "exact_ms_per_step": mesh["exact"]["ms_per_step"],
+                             "hbm_frac_fast": mesh["roofline"]["frac"],
+                             "reference_cpu_steps_per_s": mcpu.get("value"),
+                             "pairs_bit_exact_vs_reference": "tests/test_mesh_1m_gpu.py"}
         out = {
-            "metric": METRIC, "value": value, "unit": "pair-interactions/s", "n_gpus": ws, "steps": a.steps,
+            "metric": METRIC, "value": value, "unit": "pair-interactions/s", "mesh_headline": mesh_headline,
+            "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32 pair terms, f64 state/accumulation", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n": N_BODIES, "gravity_mode": "mixed",

@@ -303,40 +303,26 @@ __device__ __forceinline__ void tail_terms(const DevState &S, const MGArgs &A, i
       }
 }
 
-// Accelerations of bodies 3..lid (bodies 0..2 are finished by k_mesh_big3);
-// terms for bodies 0..2 and CM_acc go to `terms` (12 blocks of n_max, the
-// CM_acc ones doubled with J2).
-__global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
-                            const int *__restrict__ vals, const int *__restrict__ cstart, int have_cells,
-                            const GRec *__restrict__ grec, double *__restrict__ ax, double *__restrict__ ay,
-                            double *__restrict__ az, double *__restrict__ terms, long N)
+// A body's terms that do not come from pairs[]: the central mass (its
+// acceleration and, with J2, the J2 share; CM_acc's terms) and the three
+// largest bodies 0..2 (b's acceleration from them, their terms from b), with
+// the reference's operations.  Writes the per-body terms at ti; returns false
+// when the body has nothing more to add (empty slot, or one of bodies 0..2).
+__device__ __forceinline__ bool body_prologue(const DevState &S, const MGArgs &A, const GRec &me, int b, long ti,
+                                              double *__restrict__ terms, long N, double *__restrict__ ax,
+                                              double *__restrict__ ay, double *__restrict__ az, double &a_x,
+                                              double &a_y, double &a_z)
 {
-      // bodies of the cell table in cell order (neighbouring threads share cells
-      // and partners), then the bodies appended after the pass
-      const int t = blockIdx.x * blockDim.x + threadIdx.x;
-      if (t > A.lid) return;
-      const bool incell = have_cells && t <= A.lid0;
-      const int b = incell ? vals[t] : t;
-      const long ti = A.cellterms ? t : b;  // where this body's terms go (coalesced in cell order)
       const int f = A.j2.on ? 2 : 1;
-      // this body's fields, loaded once: from its cell-ordered record (one
-      // contiguous 64-byte read; the same values as the state arrays)
-      GRec me;
-      if (incell) {
-            me = grec[t];
-      } else {
-            me.x = S.x[b]; me.y = S.y[b]; me.z = S.z[b]; me.m = S.m[b]; me.R = S.R[b];
-            me.ex = S.ex[b];
-      }
+      a_x = a_y = a_z = 0.;
       if (!me.ex) {
             // an empty slot adds +0.0 to every chain (they then read all terms
             // without looking at exists[])
             for (int w = 0; w < 9; w++) terms[(size_t)w * N + ti] = 0.;
             for (int c = 0; c < 3; c++)
                   for (int u = 0; u < f; u++) cm_chain(terms, A, N, c)[f * ti + u] = 0.;
-            return;
+            return false;
       }
-      double a_x = 0., a_y = 0., a_z = 0.;
       if (A.central) {
             double DX = DSUB(me.x, A.cmx), DY = DSUB(me.y, A.cmy), DZ = DSUB(me.z, A.cmz);
             double rk = __dsqrt_rn(DADD(DADD(DMUL(DX, DX), DMUL(DY, DY)), DMUL(DZ, DZ)));
@@ -359,7 +345,7 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
             ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
             if (A.cellterms)  // (the parallel sums read every position)
                   for (int w = 0; w < 9; w++) terms[(size_t)w * N + ti] = 0.;
-            return;
+            return false;
       }
       if (A.mutual) {
             const double xb = me.x, yb = me.y, zb = me.z, Rb = me.R, mb = me.m;
@@ -386,6 +372,36 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                   terms[(3 * i + 2) * N + ti] = div_by_recip(DMUL(gb, DSUB(zb, S.z[i])), D3, y);
             }
       }
+      return true;
+}
+
+// Accelerations of bodies 3..lid (bodies 0..2 are finished by k_mesh_big3);
+// terms for bodies 0..2 and CM_acc go to `terms` (12 blocks of n_max, the
+// CM_acc ones doubled with J2).  Every body's pair terms are added in pairs[]
+// order (the exact mode's kernel).
+__global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
+                            const int *__restrict__ vals, const int *__restrict__ cstart, int have_cells,
+                            const GRec *__restrict__ grec, double *__restrict__ ax, double *__restrict__ ay,
+                            double *__restrict__ az, double *__restrict__ terms, long N)
+{
+      // bodies of the cell table in cell order (neighbouring threads share cells
+      // and partners), then the bodies appended after the pass
+      const int t = blockIdx.x * blockDim.x + threadIdx.x;
+      if (t > A.lid) return;
+      const bool incell = have_cells && t <= A.lid0;
+      const int b = incell ? vals[t] : t;
+      const long ti = A.cellterms ? t : b;  // where this body's terms go (coalesced in cell order)
+      // this body's fields, loaded once: from its cell-ordered record (one
+      // contiguous 64-byte read; the same values as the state arrays)
+      GRec me;
+      if (incell) {
+            me = grec[t];
+      } else {
+            me.x = S.x[b]; me.y = S.y[b]; me.z = S.z[b]; me.m = S.m[b]; me.R = S.R[b];
+            me.ex = S.ex[b];
+      }
+      double a_x, a_y, a_z;
+      if (!body_prologue(S, A, me, b, ti, terms, N, ax, ay, az, a_x, a_y, a_z)) return;
       if (A.mutual && have_cells && b > A.lid0) {
             // a tail fragment created by the pass: its pairs are those of its
             // fragmentation (the largest fragment, then the other tail bodies)
@@ -475,6 +491,126 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
             for (; xe >= 0; xe = A.evx[(size_t)EVX * xe + 5]) tail_terms(S, A, xe, b, b, a_x, a_y, a_z);
       }
       ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
+}
+
+// The fast modes' mesh gravity, for passes without bodies larger than the
+// mesh size and without fragments appended: a body's pairs[] partners are then
+// exactly the existing bodies p > 2, p != b, in the 27 cells around its own
+// (the cell relation is symmetric, the reference's index aliasing included),
+// and the sum over them is taken in any fixed order.  The warp's bodies queue
+// their partners (record positions, per lane in shared memory) while they walk
+// their cells; then the warp evaluates the queued pair terms 32 at a time,
+// every lane busy whatever the lengths of the bodies' lists, and each body adds
+// its own terms in its queue's order (deterministic).  The pair term is the
+// exact mode's (the same FP64 operations); only the order of the sum differs.
+constexpr int FGW = 8;   // warps per block
+constexpr int FGQ = 32;  // queued partners per lane and round
+
+__device__ __forceinline__ void term_rec(double xb, double yb, double zb, double Rb, const GRec &o, const MGArgs &A,
+                                         double &tx, double &ty, double &tz)
+{
+      double dx = DSUB(o.x, xb), dy = DSUB(o.y, yb), dz = DSUB(o.z, zb);
+      double r2 = DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz));
+      if (A.soft) {
+            double s = DMUL(A.sp, DADD(Rb, o.R));
+            r2 = DADD(r2, DMUL(s, s));
+      }
+      double D = __dsqrt_rn(r2);
+      double D3 = DMUL(DMUL(D, D), D);
+      double g = DMUL(A.G, o.m);
+      const double y = __drcp_rn(D3);
+      tx = div_by_recip(DMUL(g, dx), D3, y);
+      ty = div_by_recip(DMUL(g, dy), D3, y);
+      tz = div_by_recip(DMUL(g, dz), D3, y);
+}
+
+__global__ void __launch_bounds__(FGW * 32) k_mesh_grav_fast(DevState S, MGArgs A, const uint32_t *__restrict__ keys,
+                                                            const int *__restrict__ vals,
+                                                            const int *__restrict__ cstart,
+                                                            const GRec *__restrict__ grec, double *__restrict__ ax,
+                                                            double *__restrict__ ay, double *__restrict__ az,
+                                                            double *__restrict__ terms, long N)
+{
+      __shared__ int qb[FGW][32 * FGQ];
+      __shared__ double tb[FGW][3][32];
+      __shared__ double ob[FGW][4][32];
+      __shared__ int pre[FGW][33];
+      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      const int t = blockIdx.x * blockDim.x + threadIdx.x;  // cell order
+      const bool act = t <= A.lid;
+      const int b = act ? vals[t] : 0;
+      GRec me;
+      me.x = me.y = me.z = me.m = me.R = 0.;
+      me.ex = 0;
+      if (act) me = grec[t];
+      double a_x = 0., a_y = 0., a_z = 0.;
+      bool walk = act && body_prologue(S, A, me, b, t, terms, N, ax, ay, az, a_x, a_y, a_z) && A.mutual;
+      const uint32_t L = act ? keys[t] : 0xffffffffu;
+      walk = walk && L != 0xffffffffu;  // outside the collision cube: no pairs
+      ob[w][0][lane] = me.x;
+      ob[w][1][lane] = me.y;
+      ob[w][2][lane] = me.z;
+      ob[w][3][lane] = me.R;
+      int skip = 0;
+      bool more = walk;
+      while (__any_sync(0xffffffffu, more)) {
+            int cnt = 0;
+            if (more) {
+                  int idx = 0;
+                  for (int l = 0; l < 27; ++l) {
+                        const long long cell = (long long)L + g_noff(l, A.d);
+                        if (cell < 0 || cell >= A.cell_cap) continue;
+                        const int s0 = cstart[cell];
+                        if (s0 < 0) continue;
+                        for (int q = s0; keys[q] == (uint32_t)cell; ++q) {
+                              if (q == t) continue;
+                              if (vals[q] <= 2 || !grec[q].ex) continue;
+                              if (idx >= skip && idx < skip + FGQ) qb[w][lane * FGQ + idx - skip] = q;
+                              ++idx;
+                        }
+                  }
+                  cnt = min(idx - skip, FGQ);
+                  more = idx > skip + FGQ;
+            }
+            int incl = cnt;
+            for (int o = 1; o < 32; o <<= 1) {
+                  const int u = __shfl_up_sync(0xffffffffu, incl, o);
+                  if (lane >= o) incl += u;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            const int mine = incl - cnt;
+            pre[w][lane] = mine;
+            __syncwarp();
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                  const int fi = f0 + lane;
+                  if (fi < total) {
+                        int lo = 0, hi = 31;  // the last lane whose items start at or before fi
+                        while (lo < hi) {
+                              const int mid = (lo + hi + 1) >> 1;
+                              if (pre[w][mid] <= fi) lo = mid;
+                              else hi = mid - 1;
+                        }
+                        const int q = qb[w][lo * FGQ + fi - pre[w][lo]];
+                        double tx, ty, tz;
+                        term_rec(ob[w][0][lo], ob[w][1][lo], ob[w][2][lo], ob[w][3][lo], grec[q], A, tx, ty, tz);
+                        tb[w][0][lane] = tx;
+                        tb[w][1][lane] = ty;
+                        tb[w][2][lane] = tz;
+                  }
+                  __syncwarp();
+                  const int i0 = max(mine, f0), i1 = min(mine + cnt, f0 + 32);
+                  for (int i = i0; i < i1; ++i) {
+                        a_x = DADD(a_x, tb[w][0][i - f0]);
+                        a_y = DADD(a_y, tb[w][1][i - f0]);
+                        a_z = DADD(a_z, tb[w][2][i - f0]);
+                  }
+                  __syncwarp();
+            }
+            skip += FGQ;
+      }
+      if (walk || (act && me.ex && b > 2)) {
+            ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
+      }
 }
 
 // Bodies 0..2 and CM_acc.  Chain w (0..8: body w/3, component w%3; 9..11:
@@ -643,8 +779,15 @@ int mesh_gravity_state(const double *cm8, const J2Arg &j2)
                   k_grav_records<<<(c.mesh_n + 255) / 256, 256, 0, st>>>(S, c.mvals, c.mesh_n, grec);
                   NCG_LAUNCHED();
             }
-            k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.cstart, c.mesh_valid, grec,
-                                                          ax, ay, az, c.partial, N);
+            // the fast modes' order-free kernel where a body's pairs are exactly its
+            // 27-cell neighbours (no big bodies' visits, no fragments appended)
+            const bool fast = A.cellterms && c.mesh_valid && A.nvis == 0 && A.nfev == 0 && lid == A.lid0;
+            if (fast)
+                  k_mesh_grav_fast<<<(lid + FGW * 32) / (FGW * 32), FGW * 32, 0, st>>>(S, A, c.mkeys, c.mvals, c.cstart,
+                                                                                     grec, ax, ay, az, c.partial, N);
+            else
+                  k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.cstart, c.mesh_valid,
+                                                                grec, ax, ay, az, c.partial, N);
             NCG_LAUNCHED();
       }
       double *tot = c.red + 3584;
