@@ -197,18 +197,21 @@ int refresh_j2()
       return NCGPU_OK;
 }
 
-int mesh_gravity_state(const double *cm8, const J2Arg &j2);
+int mesh_gravity_state(const J2Arg &j2);
 
 int kick_state()
 {
       Ctx &c = ctx();
       c.com_reduced = 0;
-      double cm9[9];
-      NCG_TRY(state_cm_host(cm9));
       const int nslots = c.largest_id + 1;
+      const bool mesh_grav = c.P.par_mesh_bool && !c.force_naive && !c.P.par_mesh_brute_gravity;
+      // the central mass's state on the host: for the brute-force gravity's
+      // arguments and the J2 term; mesh gravity reads it from device memory
+      double cm9[9] = {0.};
+      if (!mesh_grav || c.P.par_J2_bool) NCG_TRY(state_cm_host(cm9));
       const J2Arg j2 = j2_arg(c.P, cm9[6], c.j2);
-      if (c.P.par_mesh_bool && !c.force_naive && !c.P.par_mesh_brute_gravity)
-            NCG_TRY(mesh_gravity_state(cm9, j2));
+      if (mesh_grav)
+            NCG_TRY(mesh_gravity_state(j2));
       else
             NCG_TRY(gravity_eval(state_view(), c.largest_id, cm9, j2, c.acc, c.n_max, c.cm_acc, c.P.par_gravity_mode,
                                  c.s));

@@ -241,16 +241,21 @@ static int sort_hits(int n, int *out_i, int *out_j, int lid, cudaStream_t st)
 }
 
 // Reads back the scalars a sweep changed and the device error word.
-int sync_scalars()
+int sync_scalars() { int h[S_COUNT]; return sync_scalars_h(h); }
+
+// sync_scalars, also handing the device scalars to the caller (h: S_COUNT ints)
+int sync_scalars_h(int *h)
 {
       Ctx &c = ctx();
-      int h[S_COUNT];
-      NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, c.s));
+      unsigned e = 0;  // the device scalars and the error word behind one synchronisation
+      NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof(int) * S_COUNT, cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaMemcpyAsync(&e, c.err, sizeof e, cudaMemcpyDeviceToHost, c.s));
       NCG_CK(cudaStreamSynchronize(c.s));
       c.largest_id = h[S_LID];
       c.n_events = h[S_NEV];
       c.collision_count = h[S_CCOUNT];
-      return check_err_word();
+      if (!e) return NCGPU_OK;
+      return check_err_word();  // reads, clears and maps the recorded error
 }
 
 int collide_brute_state()

@@ -106,6 +106,39 @@ __device__ __forceinline__ double div_by_recip(double x, double b, double y)
       return __fma_rn(r, y, q);
 }
 
+// The 27 neighbour cells of a cell L (linear index i + j d + k d^2) as 9 rows
+// of three consecutive indices (x - 1, x, x + 1): row r (0..8) is centred on
+// L + (r % 3 - 1) d + (r / 3 - 1) d^2, so the cell slots l = 26..0 of the
+// reference's pop order are the rows r = 8..0, each from x + 1 down to x - 1.
+__device__ __forceinline__ long long d_row(long long L, int r, int d, long long dd)
+{
+      return L + (r % 3 - 1) * (long long)d + (r / 3 - 1) * dd;
+}
+
+// The [first, end) ranges of the cells mid - 1, mid, mid + 1 in the cell table
+// ({-1, -1} for an empty cell or one outside [0, cap)); three independent loads.
+__device__ __forceinline__ void row_cells(const int2 *__restrict__ crange, long long mid, long long cap, int2 (&cr)[3])
+{
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+            const long long c = mid - 1 + x;
+            cr[x] = (c >= 0 && c < cap) ? crange[c] : make_int2(-1, -1);
+      }
+}
+
+// The row's cells are consecutive keys, hence one contiguous range [s, e) of
+// the cell-sorted bodies; false when all three are empty.
+__device__ __forceinline__ bool row_range(const int2 *__restrict__ crange, long long mid, long long cap, int *s, int *e)
+{
+      int2 cr[3];
+      row_cells(crange, mid, cap, cr);
+      const int s0 = cr[0].x >= 0 ? cr[0].x : cr[1].x >= 0 ? cr[1].x : cr[2].x;
+      if (s0 < 0) return false;
+      *s = s0;
+      *e = cr[2].y >= 0 ? cr[2].y : cr[1].y >= 0 ? cr[1].y : cr[0].y;
+      return true;
+}
+
 // Sequential FP64 sum s + t[0] + t[1] + ... + t[n-1], in that order with IEEE
 // rounding, by one warp (the result is lane 0's): the lanes stage CHN terms at
 // a time in shared memory (`stage`, CHN doubles, 16-byte aligned) with
@@ -231,7 +264,7 @@ struct Ctx {
       int collision_count = 0;     // collision_count (host copy)
 
       // mesh search (allocated on the first mesh pass)
-      int *cstart = nullptr;       // dense cell -> first sorted position (-1 empty)
+      int2 *crange = nullptr;      // dense cell -> [first, end) of its bodies in the sorted keys ({-1, -1} empty)
       size_t cell_cap = 0;
       int mesh_d = 0;
       uint32_t *mkeys = nullptr;   // cell index per sorted body (n + 1, sentinel)
@@ -307,6 +340,7 @@ constexpr int MAX_VISITS = 1024;
 Ctx &ctx();
 int ensure_partial(size_t doubles);
 int check_err_word();        // syncs the stream, reads and clears the device error word
+int sync_scalars_h(int *h);  // device scalars into c.* and h[S_COUNT], error word checked (one sync)
 
 // Gravity driver (gravity.cu).  Reads bodies through `bv` for slots
 // 0..largest_id, writes acc (3 blocks of n_max: ax, ay, az, zero for empty

@@ -244,9 +244,13 @@ int eot_state(int *hm_out)
                                      P.par_high_dumping_threshold, flag);
       NCG_LAUNCHED();
       int h[S_COUNT];
+      unsigned e = 0;  // the step's device errors come back with the counts
       NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaMemcpyAsync(&e, c.err, sizeof e, cudaMemcpyDeviceToHost, st));
       NCG_CK(cudaStreamSynchronize(st));
+      if (e) NCG_TRY(check_err_word());
       const int hm = h[S_HM];
+      const bool changed = h[S_NFLAG] > 0 || hm < 9 * lid / 10;  // dumping or tidy_up change the scalars
       if (h[S_NFLAG] > 0) {
             int nf = 0;
             NCG_TRY(compact_existing(flag, lid, &nf, st));
@@ -277,7 +281,7 @@ int eot_state(int *hm_out)
             k_tidy_scatter<<<nb, 256, 0, st>>>(S, n, lid, c.aos, c.n_max);
             NCG_LAUNCHED();
       }
-      NCG_TRY(sync_scalars());
+      if (changed) NCG_TRY(sync_scalars());
       if (P.par_J2_bool && P.par_J2 == 0.) NCG_TRY(refresh_j2());  // src/rk4.c:459-463
       if (hm_out) *hm_out = hm;
       return NCGPU_OK;

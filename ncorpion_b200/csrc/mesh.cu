@@ -63,7 +63,7 @@ __global__ void k_mesh_keys(DevState S, int lid, double gam, double half, int d,
       vals[k] = k;
 }
 
-__global__ void k_cell_heads(const uint32_t *__restrict__ keys, int n, int *__restrict__ cstart,
+__global__ void k_cell_heads(const uint32_t *__restrict__ keys, int n, int2 *__restrict__ crange,
                              int *__restrict__ n_ins)
 {
       int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -73,16 +73,17 @@ __global__ void k_cell_heads(const uint32_t *__restrict__ keys, int n, int *__re
             if (q == 0 || keys[q - 1] != NOKEY) *n_ins = q;
             return;
       }
-      if (q == 0 || keys[q - 1] != key) cstart[key] = q;
+      if (q == 0 || keys[q - 1] != key) crange[key].x = q;
+      if (keys[q + 1] != key) crange[key].y = q + 1;  // (keys[n] is the NOKEY sentinel)
       if (q == n - 1) *n_ins = n;
 }
 
-__global__ void k_cell_clear(const uint32_t *__restrict__ keys, int n, int *__restrict__ cstart)
+__global__ void k_cell_clear(const uint32_t *__restrict__ keys, int n, int2 *__restrict__ crange)
 {
       int q = blockIdx.x * blockDim.x + threadIdx.x;
       if (q >= n) return;
       uint32_t key = keys[q];
-      if (key != NOKEY && (q == 0 || keys[q - 1] != key)) cstart[key] = -1;
+      if (key != NOKEY && (q == 0 || keys[q - 1] != key)) crange[key] = make_int2(-1, -1);
 }
 
 // number of candidates of body k (lo <= k < hi): existing bodies of lower
@@ -101,10 +102,14 @@ __global__ void k_mesh_records(const DevState S, const int *__restrict__ vals, i
       rec[q] = r;
 }
 
+// The 27 neighbour cells as 9 rows of three consecutive linear indices
+// (x - 1, x, x + 1): row r (0..8) has dy = r % 3 - 1, dz = r / 3 - 1, so the
+// cell slots l = 26..0 of the pop order are the rows r = 8..0, each from x + 1
+// down to x - 1.
+
 __global__ void k_mesh_count(const MRec *__restrict__ rec, const int *__restrict__ ckey,
-                             const uint32_t *__restrict__ keys, const int *__restrict__ vals,
-                             const int *__restrict__ cstart, int lid, int lo, int hi, int d, long long cap,
-                             int *__restrict__ cnt)
+                             const int *__restrict__ vals, const int2 *__restrict__ crange, int lid, int lo, int hi,
+                             int d, long long cap, int *__restrict__ cnt)
 {
       // threads walk the bodies in cell order (vals = bodies sorted by cell), so
       // the threads of a warp share cells and partners
@@ -114,16 +119,15 @@ __global__ void k_mesh_count(const MRec *__restrict__ rec, const int *__restrict
       int L = (k >= lo && k < hi) ? ckey[k] : -1;
       int c = 0;
       if (L >= 0) {
-            for (int l = 26; l >= 0; --l) {
-                  long long cell = L + d_noff(l, d);
-                  if (cell < 0 || cell >= cap) continue;  // i = 0 after rounding at -cube/2
-                  int s = cstart[cell];
-                  if (s < 0) continue;
-                  for (int q = s; keys[q] == (uint32_t)cell; ++q) {
-                        const int p = vals[q];
-                        if (p >= k) break;
-                        if (rec[q].ex) c++;  // a body removed earlier in the pass is not pushed
-                  }
+            const long long dd = (long long)d * d;
+            // a row's three cells are one contiguous range of the sorted bodies
+#pragma unroll 1
+            for (int r = 0; r < 9; ++r) {
+                  const long long mid = d_row(L, r, d, dd);
+                  int s, e;
+                  if (!row_range(crange, mid, cap, &s, &e)) continue;
+                  for (int q = s; q < e; ++q)
+                        if (vals[q] < k && rec[q].ex) c++;  // a body removed earlier in the pass is not pushed
             }
       }
       cnt[k] = c;
@@ -131,11 +135,11 @@ __global__ void k_mesh_count(const MRec *__restrict__ rec, const int *__restrict
 
 // candidates of body k in pop order; hit flag from the entry-state predicate
 __global__ void k_mesh_write(const MRec *__restrict__ rec, const int *__restrict__ ckey,
-                             const uint32_t *__restrict__ keys,
-                             const int *__restrict__ vals, const int *__restrict__ cstart,
+                             const int *__restrict__ vals, const int2 *__restrict__ crange,
                              const int *__restrict__ off, int lid, int lo, int hi, int d, long long cap, double dt,
                              int test, int *__restrict__ ck, int *__restrict__ cp, unsigned char *__restrict__ cflag,
-                             int *__restrict__ hitpos, int hit_cap, int *__restrict__ nhits, unsigned *err)
+                             int *__restrict__ hitpos, int hit_cap, int *__restrict__ nhits, long pair_cap,
+                             unsigned *err)
 {
       const int t = blockIdx.x * blockDim.x + threadIdx.x;  // cell order, as k_mesh_count
       if (t > lid) return;
@@ -144,29 +148,37 @@ __global__ void k_mesh_write(const MRec *__restrict__ rec, const int *__restrict
       int L = ckey[k];
       if (L < 0) return;
       int pos = off[k];
-      const MRec rk = rec[t];
+      const MRec rk = load_mrec(rec, t);
       const bool dk = test && rk.did;
-      for (int l = 26; l >= 0; --l) {
-            long long cell = L + d_noff(l, d);
-            if (cell < 0 || cell >= cap) continue;
-            int s = cstart[cell];
-            if (s < 0) continue;
-            for (int q = s; keys[q] == (uint32_t)cell; ++q) {
-                  int p = vals[q];
-                  if (p >= k) break;
-                  const MRec rp = rec[q];
-                  if (!rp.ex) continue;
-                  ck[pos] = k;
-                  cp[pos] = p;
-                  unsigned char f = 0;
-                  if (test && !dk && !rp.did && d_contact_rec(rp, rk, dt)) {  // closest_approach(p, k)
-                        f = 1;
-                        int h = atomicAdd(nhits, 1);
-                        if (h < hit_cap) hitpos[h] = pos;
-                        else atomicOr(err, ERR_CAPACITY);
+      const long long dd = (long long)d * d;
+#pragma unroll 1
+      for (int r = 8; r >= 0; --r) {
+            const long long mid = d_row(L, r, d, dd);
+            int2 cr[3];
+            row_cells(crange, mid, cap, cr);
+#pragma unroll
+            for (int x = 2; x >= 0; --x) {  // cells mid + 1, mid, mid - 1
+                  for (int q = cr[x].x; q < cr[x].y; ++q) {
+                        int p = vals[q];
+                        if (p >= k) break;
+                        const MRec rp = load_mrec(rec, q);
+                        if (!rp.ex) continue;
+                        if (pos >= pair_cap) {
+                              atomicOr(err, ERR_CAPACITY);
+                              return;
+                        }
+                        ck[pos] = k;
+                        cp[pos] = p;
+                        unsigned char f = 0;
+                        if (test && !dk && !rp.did && d_contact_rec(rp, rk, dt)) {  // closest_approach(p, k)
+                              f = 1;
+                              int h = atomicAdd(nhits, 1);
+                              if (h < hit_cap) hitpos[h] = pos;
+                              else atomicOr(err, ERR_CAPACITY);
+                        }
+                        cflag[pos] = f;
+                        ++pos;
                   }
-                  cflag[pos] = f;
-                  ++pos;
             }
       }
 }
@@ -292,7 +304,7 @@ __device__ void d_mesh_treat(const DevState &S, int p, int k, int q, const MeshE
 __global__ void __launch_bounds__(MEV) k_mesh_events(DevState S, const int *__restrict__ ck, const int *__restrict__ cp,
                                                      unsigned char *cflag, const int *__restrict__ off,
                                                      const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
-                                                     const int *__restrict__ vals, const int *__restrict__ cstart,
+                                                     const int *__restrict__ vals, const int2 *__restrict__ crange,
                                                      const int *__restrict__ hitpos, int nh, MeshEvArgs E, int *ev,
                                                      double *evrec, unsigned char *dirty, int *occ, int *ndrop,
                                                      MeshFragBufs X, unsigned *err)
@@ -372,7 +384,7 @@ __global__ void __launch_bounds__(MEV) k_mesh_events(DevState S, const int *__re
                   for (int l = threadIdx.x >> 5; l < 27; l += MEV / 32) {
                         long long cell = Lx + d_noff(l, E.d);
                         if (cell < 0 || cell >= E.cell_cap) continue;
-                        int s = cstart[cell];
+                        int s = crange[cell].x;
                         if (s < 0) continue;
                         for (int qq = s + (threadIdx.x & 31); qq < E.nsorted && keys[qq] == (uint32_t)cell; qq += 32) {
                               int kk = vals[qq];
@@ -585,12 +597,12 @@ static int mesh_alloc(int d)
 {
       Ctx &c = ctx();
       if (d < 4 || d % 2 || d > 1200) return NCGPU_E_UNSUPPORTED;  // int cell index up to ~1.7e9
-      if (c.cstart && c.mesh_d == d) return NCGPU_OK;
-      if (c.cstart) cudaFree(c.cstart);
+      if (c.crange && c.mesh_d == d) return NCGPU_OK;
+      if (c.crange) cudaFree(c.crange);
       size_t dd = (size_t)d;
       c.cell_cap = (dd + 3) * (1 + dd + dd * dd);
-      NCG_CK(cudaMalloc(&c.cstart, sizeof(int) * c.cell_cap));
-      NCG_CK(cudaMemsetAsync(c.cstart, 0xff, sizeof(int) * c.cell_cap, c.s));
+      NCG_CK(cudaMalloc(&c.crange, sizeof(int2) * c.cell_cap));
+      NCG_CK(cudaMemsetAsync(c.crange, 0xff, sizeof(int2) * c.cell_cap, c.s));
       c.mesh_d = d;
       if (!c.mkeys) {
             size_t N = (size_t)c.n_max;
@@ -623,7 +635,7 @@ static int mesh_alloc(int d)
 void mesh_free()
 {
       Ctx &c = ctx();
-      void *ptrs[] = {c.cstart, c.mkeys, c.mvals, c.ckey, c.mcnt, c.moff, c.cand_k, c.cand_p, c.cflag, c.cpos,
+      void *ptrs[] = {c.crange, c.mkeys, c.mvals, c.ckey, c.mcnt, c.moff, c.cand_k, c.cand_p, c.cflag, c.cpos,
                       c.occ, c.msums, c.evx, c.xpairs, c.xhead, c.fev, c.vis, c.mrec};
       for (void *p : ptrs)
             if (p) cudaFree(p);
@@ -639,7 +651,7 @@ int mesh_reset_state()
 {
       Ctx &c = ctx();
       if (c.mesh_valid && c.mesh_n > 0) {
-            k_cell_clear<<<(c.mesh_n + 255) / 256, 256, 0, c.s>>>(c.mkeys, c.mesh_n, c.cstart);
+            k_cell_clear<<<(c.mesh_n + 255) / 256, 256, 0, c.s>>>(c.mkeys, c.mesh_n, c.crange);
             NCG_LAUNCHED();
       }
       if (c.mesh_nfev > 0) {
@@ -660,11 +672,9 @@ __global__ void k_clear_dirty_events(unsigned char *dirty, const int *ev, int n)
       }
 }
 
-// Candidates of the bodies k in [lo, hi) (pop order, positions from base),
-// their hits against the current state and, with collisions, the ordered
-// event replay over them.  *tot = candidates written.
-static int mesh_segment(const DevState &S, int lid, int lo, int hi, long base, int test, const MeshEvArgs &E0,
-                        int *tot)
+// Candidates of the bodies k in [lo, hi) (pop order, positions from base) and
+// their hits against the current state: the kernels, without waiting.
+static int mesh_segment_launch(const DevState &S, int lid, int lo, int hi, long base, int test)
 {
       Ctx &c = ctx();
       cudaStream_t st = c.s;
@@ -674,7 +684,7 @@ static int mesh_segment(const DevState &S, int lid, int lo, int hi, long base, i
       MRec *rec = (MRec *)c.mrec;
       k_mesh_records<<<nb, 256, 0, st>>>(S, c.mvals, n, rec);
       NCG_LAUNCHED();
-      k_mesh_count<<<nb, 256, 0, st>>>(rec, c.ckey, c.mkeys, c.mvals, c.cstart, lid, lo, hi, d,
+      k_mesh_count<<<nb, 256, 0, st>>>(rec, c.ckey, c.mvals, c.crange, lid, lo, hi, d,
                                        (long long)c.cell_cap, c.mcnt);
       NCG_LAUNCHED();
       NCG_TRY(scan_exclusive(c.mcnt, c.moff, n, c.cnt, st));
@@ -682,21 +692,27 @@ static int mesh_segment(const DevState &S, int lid, int lo, int hi, long base, i
             k_add_base<<<(n + 256) / 256, 256, 0, st>>>(c.moff, n, (int)base);
             NCG_LAUNCHED();
       }
-      int end = 0;
-      NCG_CK(cudaMemcpyAsync(&end, c.moff + n, sizeof(int), cudaMemcpyDeviceToHost, st));
       NCG_CK(cudaMemsetAsync(c.scal + S_NHITS, 0, sizeof(int), st));
-      NCG_CK(cudaStreamSynchronize(st));
+      // (positions at or past pair_cap are not written: the kernel records the
+      // overflow and the host returns NCGPU_E_CAPACITY)
+      k_mesh_write<<<nb, 256, 0, st>>>(rec, c.ckey, c.mvals, c.crange, c.moff, lid, lo, hi, d,
+                                       (long long)c.cell_cap, c.dt, test, c.cand_k, c.cand_p, c.cflag, c.hi, c.hit_cap,
+                                       c.scal + S_NHITS, c.pair_cap, c.err);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
+
+// After mesh_segment_launch and a synchronisation that brought back the
+// candidates' end and the hits' count: with hits, the ordered event replay.
+// *tot = candidates written.
+static int mesh_segment_finish(const DevState &S, int lid, int hi, long base, int end, int nh, const MeshEvArgs &E0,
+                               int *tot)
+{
+      Ctx &c = ctx();
+      cudaStream_t st = c.s;
       const long total = (long)end - base;
       if ((long)end > c.pair_cap) return NCGPU_E_CAPACITY;
       *tot = (int)total;
-      if (total == 0) return NCGPU_OK;
-      k_mesh_write<<<nb, 256, 0, st>>>(rec, c.ckey, c.mkeys, c.mvals, c.cstart, c.moff, lid, lo, hi, d,
-                                       (long long)c.cell_cap, c.dt, test, c.cand_k, c.cand_p, c.cflag, c.hi, c.hit_cap,
-                                       c.scal + S_NHITS, c.err);
-      NCG_LAUNCHED();
-      int nh = 0;
-      NCG_CK(cudaMemcpyAsync(&nh, c.scal + S_NHITS, sizeof(int), cudaMemcpyDeviceToHost, st));
-      NCG_CK(cudaStreamSynchronize(st));
       if (nh > c.hit_cap) return NCGPU_E_CAPACITY;
       if (nh > 0) {
             NCG_CK(cudaMemcpyAsync(c.keys, c.hi, sizeof(int) * (size_t)nh, cudaMemcpyDeviceToDevice, st));
@@ -706,7 +722,7 @@ static int mesh_segment(const DevState &S, int lid, int lo, int hi, long base, i
             E.seg_hi = hi;
             MeshFragBufs X{c.evx, c.xpairs, c.xhead, c.fev};
             k_mesh_events<<<1, MEV, 0, st>>>(S, c.cand_k, c.cand_p, c.cflag, c.moff, c.ckey, c.mkeys, c.mvals,
-                                             c.cstart, (const int *)c.keys, nh, E, c.ev, c.evrec, c.dirty, c.occ,
+                                             c.crange, (const int *)c.keys, nh, E, c.ev, c.evrec, c.dirty, c.occ,
                                              c.scal + S_NDROP, X, c.err);
             NCG_LAUNCHED();
             k_count_dropped<<<(int)((total + 255) / 256), 256, 0, st>>>(c.cflag + base, (int)total,
@@ -716,6 +732,19 @@ static int mesh_segment(const DevState &S, int lid, int lo, int hi, long base, i
       return NCGPU_OK;
 }
 
+// Both halves with one synchronisation between them.
+static int mesh_segment(const DevState &S, int lid, int lo, int hi, long base, int test, const MeshEvArgs &E0,
+                        int *tot)
+{
+      Ctx &c = ctx();
+      NCG_TRY(mesh_segment_launch(S, lid, lo, hi, base, test));
+      int h2[2] = {0, 0};  // candidates' end, hits
+      NCG_CK(cudaMemcpyAsync(&h2[0], c.moff + lid + 1, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaMemcpyAsync(&h2[1], c.scal + S_NHITS, sizeof(int), cudaMemcpyDeviceToHost, c.s));
+      NCG_CK(cudaStreamSynchronize(c.s));
+      return mesh_segment_finish(S, lid, hi, base, h2[0], h2[1], E0, tot);
+}
+
 // Cell table of the bodies' insertion cells (ckey -> sorted keys, heads).
 static int mesh_table(int n)
 {
@@ -723,7 +752,7 @@ static int mesh_table(int n)
       cudaStream_t st = c.s;
       NCG_TRY(radix_sort_pairs(c.mkeys, c.mvals, n, 32, st));
       NCG_CK(cudaMemsetAsync(c.mkeys + n, 0xff, sizeof(uint32_t), st));
-      k_cell_heads<<<(n + 255) / 256, 256, 0, st>>>(c.mkeys, n, c.cstart, c.scal + S_NINS);
+      k_cell_heads<<<(n + 255) / 256, 256, 0, st>>>(c.mkeys, n, c.crange, c.scal + S_NINS);
       NCG_LAUNCHED();
       return NCGPU_OK;
 }
@@ -768,8 +797,17 @@ int mesh_pass(double gam, int test)
       NCG_TRY(mesh_table(n));
       c.mesh_valid = 1;
       c.mesh_n = n;
-      int nbig = 0;
-      NCG_TRY(read_scal(S_NBIG, &nbig));
+      // the pass as one segment of every body, its candidates launched before
+      // the count of bodies larger than the mesh size comes back (with the
+      // candidates' end and the hits, one synchronisation); with such bodies
+      // the segmented pass below starts over
+      NCG_TRY(mesh_segment_launch(S, lid, 0, lid + 1, 0, test));
+      int h3[3] = {0, 0, 0};  // bodies larger than the mesh size, candidates' end, hits
+      NCG_CK(cudaMemcpyAsync(&h3[0], c.scal + S_NBIG, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaMemcpyAsync(&h3[1], c.moff + n, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaMemcpyAsync(&h3[2], c.scal + S_NHITS, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      const int nbig = h3[0];
       MeshEvArgs E{lid, d, c.P.par_collision_type, c.P.par_one_collision_only_bool, c.P.par_mesh_bool, c.ev_cap,
                    c.n_max, c.occ_cap, n, (long long)c.cell_cap, c.dt, c.P.par_collision_parameter,
                    c.P.par_mutual_bool, c.xpair_cap, FragArgs{}, lid + 1};
@@ -788,7 +826,7 @@ int mesh_pass(double gam, int test)
       };
       if (!test || nbig == 0) {
             int tot = 0;
-            NCG_TRY(mesh_segment(S, lid, 0, lid + 1, 0, test, E, &tot));
+            NCG_TRY(mesh_segment_finish(S, lid, lid + 1, 0, h3[1], h3[2], E, &tot));
             base = small_total = tot;
       } else {
             int s = 0;
@@ -803,7 +841,7 @@ int mesh_pass(double gam, int test)
                   const int hi = e == 0x7fffffff ? lid + 1 : e;
                   if (hi > s) {
                         if (rekey) {
-                              k_cell_clear<<<nb, 256, 0, st>>>(c.mkeys, n, c.cstart);
+                              k_cell_clear<<<nb, 256, 0, st>>>(c.mkeys, n, c.crange);
                               NCG_LAUNCHED();
                               k_mesh_rekey<<<nb, 256, 0, st>>>(S, s, lid, gam, half, d, c.mkeys, c.mvals, c.ckey);
                               NCG_LAUNCHED();
@@ -845,9 +883,7 @@ int mesh_pass(double gam, int test)
                                          cudaMemcpyHostToDevice, st));
       }
       int h[S_COUNT];
-      NCG_TRY(sync_scalars());
-      NCG_CK(cudaMemcpyAsync(h, c.scal, sizeof h, cudaMemcpyDeviceToHost, st));
-      NCG_CK(cudaStreamSynchronize(st));
+      NCG_TRY(sync_scalars_h(h));
       NCG_TRY(clear_dirty(c.n_events));
       c.n_cand = (int)base;
       c.mesh_nev = min(c.n_events, c.ev_cap);

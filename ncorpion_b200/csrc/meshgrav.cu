@@ -215,9 +215,10 @@ __device__ __forceinline__ void pair_add(const DevState &S, int b, int o, double
 
 // A body's gravity fields in a cell-ordered copy (64 bytes), read by the walk
 // instead of gathering each field from the state arrays.
-struct GRec {
-      double x, y, z, m, R, pad0, pad1;
-      int ex, pad2;
+struct __align__(16) GRec {
+      double x, y, z, mp;  // mp: the mass of a pairs[] partner (existing, not one of bodies 0..2), else 0
+      double m, R, pad0;
+      int ex, partner;
 };
 
 __global__ void k_grav_records(const DevState S, const int *__restrict__ vals, int n, GRec *__restrict__ rec)
@@ -227,9 +228,10 @@ __global__ void k_grav_records(const DevState S, const int *__restrict__ vals, i
       const int b = vals[q];
       GRec r;
       r.x = S.x[b]; r.y = S.y[b]; r.z = S.z[b]; r.m = S.m[b]; r.R = S.R[b];
-      r.pad0 = r.pad1 = 0.;
+      r.pad0 = 0.;
       r.ex = S.ex[b];
-      r.pad2 = 0;
+      r.partner = (b > 2 && r.ex) ? 1 : 0;
+      r.mp = r.partner ? r.m : 0.;
       rec[q] = r;
 }
 
@@ -255,7 +257,8 @@ __device__ __forceinline__ void pair_add_rec(double xb, double yb, double zb, do
 struct MGArgs {
       int lid, d, central, mutual, soft;
       long long cell_cap;
-      double G, sp, mu, cmx, cmy, cmz;
+      double G, sp;
+      const double *cm;         // the central mass's record (device): x, y, z at 0..2, mass at 6
       int lid0;                 // largest_id of the mesh pass (slots in the cell table)
       int nt;                   // N_tilde
       int nfev;                 // full fragmentations of the pass
@@ -324,20 +327,21 @@ __device__ __forceinline__ bool body_prologue(const DevState &S, const MGArgs &A
             return false;
       }
       if (A.central) {
-            double DX = DSUB(me.x, A.cmx), DY = DSUB(me.y, A.cmy), DZ = DSUB(me.z, A.cmz);
+            const double mu = DMUL(A.G, A.cm[6]);
+            double DX = DSUB(me.x, A.cm[0]), DY = DSUB(me.y, A.cm[1]), DZ = DSUB(me.z, A.cm[2]);
             double rk = __dsqrt_rn(DADD(DADD(DMUL(DX, DX), DMUL(DY, DY)), DMUL(DZ, DZ)));
             double r3 = DMUL(DMUL(rk, rk), rk);
             const double y3 = __drcp_rn(r3);  // the six quotients by r3 share RN(1/r3)
-            a_x = div_by_recip(DMUL(-A.mu, DX), r3, y3);
-            a_y = div_by_recip(DMUL(-A.mu, DY), r3, y3);
-            a_z = div_by_recip(DMUL(-A.mu, DZ), r3, y3);
+            a_x = div_by_recip(DMUL(-mu, DX), r3, y3);
+            a_y = div_by_recip(DMUL(-mu, DY), r3, y3);
+            a_z = div_by_recip(DMUL(-mu, DZ), r3, y3);
             double g = DMUL(A.G, me.m);
             cm_chain(terms, A, N, 0)[f * ti] = div_by_recip(DMUL(g, DX), r3, y3);
             cm_chain(terms, A, N, 1)[f * ti] = div_by_recip(DMUL(g, DY), r3, y3);
             cm_chain(terms, A, N, 2)[f * ti] = div_by_recip(DMUL(g, DZ), r3, y3);
             if (A.j2.on) {  // src/physics.c:149-160
                   double cj[3];
-                  d_j2(A.j2, A.mu, DX, DY, DZ, rk, r3, me.m, a_x, a_y, a_z, cj);
+                  d_j2(A.j2, mu, DX, DY, DZ, rk, r3, me.m, a_x, a_y, a_z, cj);
                   for (int c = 0; c < 3; c++) cm_chain(terms, A, N, c)[2 * ti + 1] = cj[c];
             }
       }
@@ -380,7 +384,7 @@ __device__ __forceinline__ bool body_prologue(const DevState &S, const MGArgs &A
 // CM_acc ones doubled with J2).  Every body's pair terms are added in pairs[]
 // order (the exact mode's kernel).
 __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, const uint32_t *__restrict__ keys,
-                            const int *__restrict__ vals, const int *__restrict__ cstart, int have_cells,
+                            const int *__restrict__ vals, const int2 *__restrict__ crange, int have_cells,
                             const GRec *__restrict__ grec, double *__restrict__ ax, double *__restrict__ ay,
                             double *__restrict__ az, double *__restrict__ terms, long N)
 {
@@ -455,7 +459,7 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
                         long long cell = L + g_noff(l, A.d);
                         cur[l] = -1;
                         if (cell < 0 || cell >= A.cell_cap) continue;
-                        int s = cstart[cell];
+                        int s = crange[cell].x;
                         if (s < 0) continue;
                         int q = s;
                         for (; keys[q] == (uint32_t)cell; ++q) {
@@ -497,46 +501,53 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
 // mesh size and without fragments appended: a body's pairs[] partners are then
 // exactly the existing bodies p > 2, p != b, in the 27 cells around its own
 // (the cell relation is symmetric, the reference's index aliasing included),
-// and the sum over them is taken in any fixed order.  The warp's bodies queue
-// their partners (record positions, per lane in shared memory) while they walk
-// their cells; then the warp evaluates the queued pair terms 32 at a time,
-// every lane busy whatever the lengths of the bodies' lists, and each body adds
-// its own terms in its queue's order (deterministic).  The pair term is the
-// exact mode's (the same FP64 operations); only the order of the sum differs.
-constexpr int FGW = 8;   // warps per block
+// and the sum over them is taken in any fixed order.  The three cells of a row
+// (x - 1, x, x + 1) are consecutive linear indices, hence one contiguous range
+// of the cell-sorted bodies: a body walks 9 ranges.  The warp's bodies queue
+// their partners (record positions, per lane in shared memory) during the
+// walk; then the warp evaluates the queued pair terms 32 at a time, every lane
+// busy whatever the lengths of the bodies' lists, and each body adds its own
+// terms in its queue's order (deterministic).  The pair term is FP64 with one
+// reciprocal square root (G m dx / D^3 = G m dx (1/D)^3); against the exact
+// mode, only its rounding and the order of the sum differ.
+constexpr int FGW = 4;   // warps per block
 constexpr int FGQ = 32;  // queued partners per lane and round
 
-__device__ __forceinline__ void term_rec(double xb, double yb, double zb, double Rb, const GRec &o, const MGArgs &A,
-                                         double &tx, double &ty, double &tz)
+// The partner's record (position q) against a body at (xb, yb, zb) of radius
+// Rb: the partner's x, y, z and partner mass come in two 16-byte loads of its
+// record's first 32 bytes (a zero mass for bodies that add no term).
+__device__ __forceinline__ void term_fast(double xb, double yb, double zb, double Rb, const GRec *__restrict__ grec,
+                                          int q, const MGArgs &A, double &tx, double &ty, double &tz)
 {
-      double dx = DSUB(o.x, xb), dy = DSUB(o.y, yb), dz = DSUB(o.z, zb);
-      double r2 = DADD(DADD(DMUL(dx, dx), DMUL(dy, dy)), DMUL(dz, dz));
+      const double2 *r = reinterpret_cast<const double2 *>(grec + q);
+      const double2 xy = r[0], zm = r[1];
+      const double dx = xy.x - xb, dy = xy.y - yb, dz = zm.x - zb;
+      double r2 = dx * dx + dy * dy + dz * dz;
       if (A.soft) {
-            double s = DMUL(A.sp, DADD(Rb, o.R));
-            r2 = DADD(r2, DMUL(s, s));
+            const double s = A.sp * (Rb + grec[q].R);
+            r2 += s * s;
       }
-      double D = __dsqrt_rn(r2);
-      double D3 = DMUL(DMUL(D, D), D);
-      double g = DMUL(A.G, o.m);
-      const double y = __drcp_rn(D3);
-      tx = div_by_recip(DMUL(g, dx), D3, y);
-      ty = div_by_recip(DMUL(g, dy), D3, y);
-      tz = div_by_recip(DMUL(g, dz), D3, y);
+      const double ri = rsqrt(r2);
+      const double w = A.G * zm.y * (ri * ri * ri);
+      tx = w * dx;
+      ty = w * dy;
+      tz = w * dz;
 }
 
-__global__ void __launch_bounds__(FGW * 32) k_mesh_grav_fast(DevState S, MGArgs A, const uint32_t *__restrict__ keys,
-                                                            const int *__restrict__ vals,
-                                                            const int *__restrict__ cstart,
-                                                            const GRec *__restrict__ grec, double *__restrict__ ax,
-                                                            double *__restrict__ ay, double *__restrict__ az,
-                                                            double *__restrict__ terms, long N)
+__global__ void __launch_bounds__(FGW * 32, 8) k_mesh_grav_fast(DevState S, MGArgs A, const uint32_t *__restrict__ keys,
+                                                               const int *__restrict__ vals,
+                                                               const int2 *__restrict__ crange,
+                                                               const GRec *__restrict__ grec, double *__restrict__ ax,
+                                                               double *__restrict__ ay, double *__restrict__ az,
+                                                               double *__restrict__ terms, long N)
 {
       __shared__ int qb[FGW][32 * FGQ];
+      __shared__ unsigned char owner[FGW][32 * FGQ];
       __shared__ double tb[FGW][3][32];
-      __shared__ double ob[FGW][4][32];
-      __shared__ int pre[FGW][33];
+      __shared__ int pre[FGW][32];
       const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       const int t = blockIdx.x * blockDim.x + threadIdx.x;  // cell order
+      const int t0 = t - lane;                               // the warp's first record
       const bool act = t <= A.lid;
       const int b = act ? vals[t] : 0;
       GRec me;
@@ -547,24 +558,19 @@ __global__ void __launch_bounds__(FGW * 32) k_mesh_grav_fast(DevState S, MGArgs 
       bool walk = act && body_prologue(S, A, me, b, t, terms, N, ax, ay, az, a_x, a_y, a_z) && A.mutual;
       const uint32_t L = act ? keys[t] : 0xffffffffu;
       walk = walk && L != 0xffffffffu;  // outside the collision cube: no pairs
-      ob[w][0][lane] = me.x;
-      ob[w][1][lane] = me.y;
-      ob[w][2][lane] = me.z;
-      ob[w][3][lane] = me.R;
+      const long long dd = (long long)A.d * A.d;
       int skip = 0;
       bool more = walk;
       while (__any_sync(0xffffffffu, more)) {
             int cnt = 0;
             if (more) {
                   int idx = 0;
-                  for (int l = 0; l < 27; ++l) {
-                        const long long cell = (long long)L + g_noff(l, A.d);
-                        if (cell < 0 || cell >= A.cell_cap) continue;
-                        const int s0 = cstart[cell];
-                        if (s0 < 0) continue;
-                        for (int q = s0; keys[q] == (uint32_t)cell; ++q) {
-                              if (q == t) continue;
-                              if (vals[q] <= 2 || !grec[q].ex) continue;
+#pragma unroll 1
+                  for (int r = 0; r < 9; ++r) {
+                        int s0, e0;
+                        if (!row_range(crange, d_row(L, r, A.d, dd), A.cell_cap, &s0, &e0)) continue;
+                        for (int q = s0; q < e0; ++q) {
+                              if (q == t) continue;  // (bodies 0..2 and removed ones add zero terms)
                               if (idx >= skip && idx < skip + FGQ) qb[w][lane * FGQ + idx - skip] = q;
                               ++idx;
                         }
@@ -580,19 +586,17 @@ __global__ void __launch_bounds__(FGW * 32) k_mesh_grav_fast(DevState S, MGArgs 
             const int total = __shfl_sync(0xffffffffu, incl, 31);
             const int mine = incl - cnt;
             pre[w][lane] = mine;
+            for (int j = 0; j < cnt; ++j) owner[w][mine + j] = (unsigned char)lane;
             __syncwarp();
             for (int f0 = 0; f0 < total; f0 += 32) {
                   const int fi = f0 + lane;
                   if (fi < total) {
-                        int lo = 0, hi = 31;  // the last lane whose items start at or before fi
-                        while (lo < hi) {
-                              const int mid = (lo + hi + 1) >> 1;
-                              if (pre[w][mid] <= fi) lo = mid;
-                              else hi = mid - 1;
-                        }
-                        const int q = qb[w][lo * FGQ + fi - pre[w][lo]];
+                        const int o = owner[w][fi];
+                        const int q = qb[w][o * FGQ + fi - pre[w][o]];
+                        const double2 *ow = reinterpret_cast<const double2 *>(grec + t0 + o);
+                        const double2 oxy = ow[0], oz = ow[1];
                         double tx, ty, tz;
-                        term_rec(ob[w][0][lo], ob[w][1][lo], ob[w][2][lo], ob[w][3][lo], grec[q], A, tx, ty, tz);
+                        term_fast(oxy.x, oxy.y, oz.x, A.soft ? grec[t0 + o].R : 0., grec, q, A, tx, ty, tz);
                         tb[w][0][lane] = tx;
                         tb[w][1][lane] = ty;
                         tb[w][2][lane] = tz;
@@ -600,9 +604,9 @@ __global__ void __launch_bounds__(FGW * 32) k_mesh_grav_fast(DevState S, MGArgs 
                   __syncwarp();
                   const int i0 = max(mine, f0), i1 = min(mine + cnt, f0 + 32);
                   for (int i = i0; i < i1; ++i) {
-                        a_x = DADD(a_x, tb[w][0][i - f0]);
-                        a_y = DADD(a_y, tb[w][1][i - f0]);
-                        a_z = DADD(a_z, tb[w][2][i - f0]);
+                        a_x += tb[w][0][i - f0];
+                        a_y += tb[w][1][i - f0];
+                        a_z += tb[w][2][i - f0];
                   }
                   __syncwarp();
             }
@@ -749,15 +753,15 @@ int three_largest_state(int *idx)
       NCG_LAUNCHED();
       k_top3_final<<<1, 32, 0, st>>>(S, first3, partR, parti, np, c.P.par_mesh_bool, out);
       NCG_LAUNCHED();
-      int h[3];
-      NCG_CK(cudaMemcpyAsync(h, out, sizeof h, cudaMemcpyDeviceToHost, st));
-      NCG_CK(cudaStreamSynchronize(st));
-      if (idx) { idx[0] = h[0]; idx[1] = h[1]; idx[2] = h[2]; }
+      if (idx) {  // (the loop itself needs no indices on the host)
+            NCG_CK(cudaMemcpyAsync(idx, out, 3 * sizeof(int), cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaStreamSynchronize(st));
+      }
       return NCGPU_OK;
 }
 
 // vector_field in mesh mode on the device state; acc blocks + cm_acc.
-int mesh_gravity_state(const double *cm8, const J2Arg &j2)
+int mesh_gravity_state(const J2Arg &j2)
 {
       Ctx &c = ctx();
       cudaStream_t st = c.s;
@@ -768,7 +772,7 @@ int mesh_gravity_state(const double *cm8, const J2Arg &j2)
       DevState S = dev_state();
       MGArgs A{lid, c.P.par_collision_cube_cells, c.P.par_central_mass_bool, c.P.par_mutual_bool,
                c.P.par_softening_parameter != 0., (long long)c.cell_cap, c.P.par_G, c.P.par_softening_parameter,
-               c.P.par_G * cm8[6], cm8[0], cm8[1], cm8[2],
+               c.cm,
                c.mesh_valid ? c.mesh_n - 1 : -1, c.P.par_N_tilde, c.mesh_nfev, c.evx, c.fev,
                c.mesh_nfev > 0 ? c.xhead : nullptr, c.mesh_valid ? c.mesh_nvis : 0, c.vis, c.cand_p, j2,
                c.P.par_gravity_mode != NCGPU_GRAVITY_EXACT};
@@ -783,10 +787,10 @@ int mesh_gravity_state(const double *cm8, const J2Arg &j2)
             // 27-cell neighbours (no big bodies' visits, no fragments appended)
             const bool fast = A.cellterms && c.mesh_valid && A.nvis == 0 && A.nfev == 0 && lid == A.lid0;
             if (fast)
-                  k_mesh_grav_fast<<<(lid + FGW * 32) / (FGW * 32), FGW * 32, 0, st>>>(S, A, c.mkeys, c.mvals, c.cstart,
+                  k_mesh_grav_fast<<<(lid + FGW * 32) / (FGW * 32), FGW * 32, 0, st>>>(S, A, c.mkeys, c.mvals, c.crange,
                                                                                      grec, ax, ay, az, c.partial, N);
             else
-                  k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.cstart, c.mesh_valid,
+                  k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.crange, c.mesh_valid,
                                                                 grec, ax, ay, az, c.partial, N);
             NCG_LAUNCHED();
       }

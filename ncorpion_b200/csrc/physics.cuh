@@ -77,10 +77,24 @@ __device__ __forceinline__ bool d_approach(const DevState &S, int a, int b, doub
 
 // One body's fields in a cell-ordered copy (64 bytes): the mesh pass reads
 // partners from it instead of gathering each field from the state arrays.
-struct MRec {
+struct __align__(16) MRec {
       double x, y, z, R, vx, vy, vz;
       int ex, did;
 };
+
+// A record in four 16-byte loads.
+__device__ __forceinline__ MRec load_mrec(const MRec *__restrict__ rec, long q)
+{
+      const double2 *p = reinterpret_cast<const double2 *>(rec + q);
+      const double2 a = p[0], b = p[1], c = p[2];
+      const int4 d = reinterpret_cast<const int4 *>(rec + q)[3];
+      MRec r;
+      r.x = a.x; r.y = a.y; r.z = b.x; r.R = b.y; r.vx = c.x; r.vy = c.y;
+      r.vz = __longlong_as_double(((long long)(unsigned)d.y << 32) | (unsigned)d.x);
+      r.ex = d.z;
+      r.did = d.w;
+      return r;
+}
 
 __device__ __forceinline__ bool d_contact_rec(const MRec &a, const MRec &b, double dt)
 {

@@ -513,12 +513,16 @@ void ncgpu_integration_brute_force_SABA1(typ t)
             gpu_stop(moonlets, moonlet_buffer, iter, gpu_final_display_device(moonlet_buffer));
             return;
       }
+      /* the final state (CM is the state's), then its half backward drift on a
+         device copy: the bodies and CM_buffer come from the copy */
       gpu_pull(moonlets);
       if (central_mass_bool) CM_buffer = CM;
-      if (t > 0.) {  /* half backward drift of the final output */
-            timestep /= -2.;
-            drift(moonlets, &CM_buffer);
-            timestep *= -2.;
+      if (t > 0.) {
+            gpu_check(ncgpu_snapshot_begin(), "snapshot");
+            gpu_check(ncgpu_set_timestep(timestep / -2.), "timestep");
+            gpu_check(ncgpu_drift(), "drift");
+            gpu_snapshot_pull(moonlets);
+            gpu_check(ncgpu_snapshot_end(), "snapshot");
       }
       gpu_stop(moonlets, moonlet_buffer, iter, 0);
 }
@@ -631,18 +635,23 @@ void ncgpu_integration_mesh(typ t)
             gpu_stop(moonlets, moonlet_buffer, iter, gpu_final_display_device(moonlet_buffer));
             return;
       }
+      /* the final state (CM is the state's), then its half backward kick on a
+         device copy: the three largest bodies' reordering, the neighbours and
+         the gravity of the copy, whose bodies and CM_buffer the host gets */
+      gpu_pull(moonlets);
       if (central_mass_bool) CM_buffer = CM;
-      if (t > 0.0) {  /* half backward kick of the final state (the central mass kick goes to CM_buffer) */
-            gpu_pull(moonlets);
-            if (central_mass_bool) CM_buffer = CM;
-            timestep /= -2.0;
+      if (t > 0.0) {
+            gpu_check(ncgpu_snapshot_begin(), "snapshot");
+            gpu_check(ncgpu_set_timestep(timestep / -2.0), "timestep");
             if (!force_naive_bool) {
-                  three_largest_moonlets(moonlets);
-                  three_largest_three_first(moonlets);
-                  get_neighbours_mesh(moonlets);
+                  int np = 0, ne = 0;
+                  long tn0 = 0;
+                  gpu_check(ncgpu_three_largest(NULL), "three_largest");
+                  gpu_check(ncgpu_mesh(gam, 0, &np, &ne, &tn0), "mesh");
             }
-            kick(moonlets, &CM_buffer, vector_field);
-            timestep *= -2.0;
+            gpu_check(ncgpu_kick(), "kick");
+            gpu_snapshot_pull(moonlets);
+            gpu_check(ncgpu_snapshot_end(), "snapshot");
       }
       gpu_stop(moonlets, moonlet_buffer, iter, 0);
 }

@@ -166,6 +166,17 @@ PROFILES = {
     "mesh_prog_200k": dict(MESH, collision_bool="1", instant_merger_bool="1", collision_cube_cells="1024",
                            N_max="250000", N_0="200000", t_end="0.01", time_step="0.0005", output_step="10",
                            write_to_files_bool="1", write_cartesian_bool="1", write_collisions_bool="1"),
+    # whole-program runs without output files, resuming files at the end (init.txt,
+    # resume.txt): the final half backward drift / kick of both drivers; the mesh
+    # driver also below switch_to_brute_force from the start (force_naive_bool)
+    "bf_merge_resume": dict(BF, collision_bool="1", instant_merger_bool="1", N_max="4096", N_0="2000",
+                            t_end="0.2", time_step="0.001", resume_simulation_bool="1"),
+    "mesh_prog_resume": dict(MESH, collision_bool="1", instant_merger_bool="1", collision_cube_cells="256",
+                             N_max="30000", N_0="20000", t_end="0.05", time_step="0.0005",
+                             resume_simulation_bool="1"),
+    "mesh_naive_resume": dict(MESH, collision_bool="1", instant_merger_bool="1", collision_cube_cells="256",
+                              switch_to_brute_force="5000", N_max="4096", N_0="2000", t_end="0.05",
+                              time_step="0.001", resume_simulation_bool="1"),
     # the N = 1,048,576 mesh workload: 1024 cells per side (8.6 GB hash table)
     "mesh_merge_1m": dict(MESH, collision_bool="1", instant_merger_bool="1",
                           collision_cube_cells="1024", N_max="1100000", N_0="1048576",

@@ -315,6 +315,27 @@ def program_run_case(profile, bodies, bodies_from=None, disk=None):
     return out
 
 
+RESUME_FILES = ["init.txt", "resume.txt"]
+
+
+def program_resume_case(profile, bodies, bodies_from):
+    """The whole reference program run without output files and with
+    resume_simulation_bool: digests of the files it writes at the end (the
+    final state in init.txt, resume.txt) and of the console output."""
+    import subprocess
+    import tempfile
+    d = tempfile.mkdtemp(prefix="ncref_run_")
+    disks.write_init_txt(os.path.join(d, "init.txt"), bodies)
+    exe = os.path.join(ROOT, "oracle", "_ref", profile, "ncorpion")
+    r = subprocess.run([exe], cwd=d, capture_output=True, text=True, check=True)
+    out = dict(bodies_from=np.array(bodies_from))
+    for f in RESUME_FILES:
+        data = open(os.path.join(d, f), "rb").read()
+        out["digest_" + f] = digest(np.frombuffer(data, np.uint8))
+    out["digest_stdout"] = digest(np.frombuffer(filtered_stdout(r.stdout).encode(), np.uint8))
+    return out
+
+
 def main(names=None):
     out = {}
     out["grav_s05_n512"] = lambda: gravity_case("bf_grav_s05", 512, 11, holes=(3, 100, 511))
@@ -361,6 +382,15 @@ def main(names=None):
     # the mesh driver on 200,000 bodies of the mesh workload's disk, 20 steps
     out["program_mesh_merge_200k"] = lambda: program_run_case("mesh_prog_200k", disks.mesh_disk(200000, seed=0),
                                                               disk=("mesh_disk", 200000, 0))
+    # both drivers without output files, with the resuming files at the end; the
+    # mesh driver also in its brute-force regime (below switch_to_brute_force)
+    out["program_bf_merge_resume"] = lambda: program_resume_case("bf_merge_resume", disks.bf_collide_disk(2000, seed=0),
+                                                                 "program_bf_merge")
+    out["program_mesh_merge_resume"] = lambda: program_resume_case("mesh_prog_resume", big_disk(20000, 7)[0],
+                                                                   "program_mesh_merge")
+    out["program_mesh_naive_resume"] = lambda: program_resume_case("mesh_naive_resume",
+                                                                   disks.bf_collide_disk(2000, seed=0),
+                                                                   "program_bf_merge")
     for k, make in out.items():
         if names and k not in names:
             continue

@@ -69,3 +69,33 @@ def test_dropin_program_matches_reference_outputs(lib, profile, fixture):
             bad.append(f)
     assert not bad, f"output files differ from the reference run: {bad}"
     assert np.array_equal(_digest(filtered_stdout(r.stdout).encode()), g["digest_stdout"])
+
+
+RESUMING = [("bf_merge_resume", "program_bf_merge_resume"), ("mesh_prog_resume", "program_mesh_merge_resume"),
+            ("mesh_naive_resume", "program_mesh_naive_resume")]
+
+
+@pytest.mark.parametrize("profile,fixture", RESUMING)
+def test_dropin_program_without_outputs_resumes_like_reference(lib, profile, fixture):
+    """Both drivers with write_to_files_bool 0 and resume_simulation_bool 1:
+    the final half backward drift (brute force) or kick (mesh; in the third
+    case below switch_to_brute_force, so brute-force gravity and collisions)
+    runs on a device copy of the state, and the resuming files the program
+    writes at the end (the final state in init.txt, resume.txt) and the console
+    output are byte-identical to the reference program's."""
+    exe = os.path.join(ROOT, "oracle", "_ref", profile, "ncorpion_gpu")
+    if not os.path.exists(exe):
+        pytest.skip("drop-in build not present (needs the reference sources)")
+    import sys
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_golden import RESUME_FILES, filtered_stdout
+    from ncorpion_b200 import disks
+    g = golden(fixture)
+    d = tempfile.mkdtemp(prefix="ncgpu_dropin_")
+    disks.write_init_txt(os.path.join(d, "init.txt"), golden(str(g["bodies_from"]))["bodies"])
+    r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    for f in RESUME_FILES:
+        data = open(os.path.join(d, f), "rb").read()
+        assert np.array_equal(_digest(data), g["digest_" + f]), f
+    assert np.array_equal(_digest(filtered_stdout(r.stdout).encode()), g["digest_stdout"])
