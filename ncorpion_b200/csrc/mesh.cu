@@ -133,53 +133,122 @@ __global__ void k_mesh_count(const MRec *__restrict__ rec, const int *__restrict
       cnt[k] = c;
 }
 
-// candidates of body k in pop order; hit flag from the entry-state predicate
-__global__ void k_mesh_write(const MRec *__restrict__ rec, const int *__restrict__ ckey,
-                             const int *__restrict__ vals, const int2 *__restrict__ crange,
-                             const int *__restrict__ off, int lid, int lo, int hi, int d, long long cap, double dt,
-                             int test, int *__restrict__ ck, int *__restrict__ cp, unsigned char *__restrict__ cflag,
-                             int *__restrict__ hitpos, int hit_cap, int *__restrict__ nhits, long pair_cap,
-                             unsigned *err)
+// Candidates of body k in pop order; hit flag from the entry-state predicate.
+//
+// The warp's 32 bodies (consecutive in cell order) share the work: each lane
+// queues the positions of every body in its 27 cells, in pop order (rows 8..0,
+// cells x + 1 .. x - 1, each cell's bodies in ascending index), into shared
+// memory; then the warp takes the queued entries 32 at a time, each lane one
+// entry whatever list it belongs to.  An entry is a candidate when its body p
+// has a lower index than the list's owner k and exists; its position is the
+// owner's offset plus the number of the owner's candidates before it (a ballot
+// over the round, plus a running count per owner), so the lists come out in
+// the reference's order.  The candidates of one list are written by adjacent
+// lanes (coalesced stores) and the FP64 predicates run with every lane busy.
+// A lane whose queue is full walks again in the next round, queueing the
+// entries after those already taken.
+constexpr int MWW = 4;   // warps per block
+constexpr int MWQ = 48;  // queued entries per lane and round
+
+__global__ void __launch_bounds__(MWW * 32) k_mesh_write(const MRec *__restrict__ rec, const int *__restrict__ ckey,
+                                                        const int *__restrict__ vals, const int2 *__restrict__ crange,
+                                                        const int *__restrict__ off, int lid, int lo, int hi, int d,
+                                                        long long cap, double dt, int test, int *__restrict__ ck,
+                                                        int *__restrict__ cp, unsigned char *__restrict__ cflag,
+                                                        int *__restrict__ hitpos, int hit_cap, int *__restrict__ nhits,
+                                                        long pair_cap, unsigned *err)
 {
+      __shared__ int qb[MWW][32 * MWQ];
+      __shared__ unsigned char owner[MWW][32 * MWQ];
+      __shared__ int pre[MWW][32], run[MWW][32], okk[MWW][32], opos[MWW][32];
+      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       const int t = blockIdx.x * blockDim.x + threadIdx.x;  // cell order, as k_mesh_count
-      if (t > lid) return;
-      const int k = vals[t];
-      if (k < lo || k >= hi) return;
-      int L = ckey[k];
-      if (L < 0) return;
-      int pos = off[k];
-      const MRec rk = load_mrec(rec, t);
-      const bool dk = test && rk.did;
+      const int t0 = t - lane;
+      int k = -1, L = -1;
+      if (t <= lid) {
+            k = vals[t];
+            if (k >= lo && k < hi) L = ckey[k];
+      }
+      bool dk = false;
+      if (L >= 0) {
+            dk = test && rec[t].did;
+            opos[w][lane] = off[k];
+      }
+      okk[w][lane] = (L >= 0 ? k : -1) | (dk ? 0x80000000 : 0);
+      run[w][lane] = 0;
       const long long dd = (long long)d * d;
+      int skip = 0;
+      bool more = L >= 0;
+      while (__any_sync(0xffffffffu, more)) {
+            int cnt = 0;
+            if (more) {
+                  int idx = 0;
 #pragma unroll 1
-      for (int r = 8; r >= 0; --r) {
-            const long long mid = d_row(L, r, d, dd);
-            int2 cr[3];
-            row_cells(crange, mid, cap, cr);
+                  for (int r = 8; r >= 0; --r) {
+                        int2 cr[3];
+                        row_cells(crange, d_row(L, r, d, dd), cap, cr);
 #pragma unroll
-            for (int x = 2; x >= 0; --x) {  // cells mid + 1, mid, mid - 1
-                  for (int q = cr[x].x; q < cr[x].y; ++q) {
-                        int p = vals[q];
-                        if (p >= k) break;
-                        const MRec rp = load_mrec(rec, q);
-                        if (!rp.ex) continue;
+                        for (int x = 2; x >= 0; --x) {  // cells mid + 1, mid, mid - 1
+                              const int a = max(cr[x].x, cr[x].x + skip - idx), b = min(cr[x].y, cr[x].x + skip + MWQ - idx);
+                              for (int q = a; q < b; ++q) qb[w][lane * MWQ + idx + (q - cr[x].x) - skip] = q;
+                              if (cr[x].x >= 0) idx += cr[x].y - cr[x].x;
+                        }
+                  }
+                  cnt = min(max(idx - skip, 0), MWQ);
+                  more = idx > skip + MWQ;
+            }
+            int incl = cnt;
+            for (int o = 1; o < 32; o <<= 1) {
+                  const int u = __shfl_up_sync(0xffffffffu, incl, o);
+                  if (lane >= o) incl += u;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            const int mine = incl - cnt;
+            pre[w][lane] = mine;
+            for (int j = 0; j < cnt; ++j) owner[w][mine + j] = (unsigned char)lane;
+            __syncwarp();
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                  const int fi = f0 + lane;
+                  int o = -1, q = 0, p = 0, kk = -1;
+                  bool cand = false;
+                  if (fi < total) {
+                        o = owner[w][fi];
+                        q = qb[w][o * MWQ + fi - pre[w][o]];
+                        kk = okk[w][o] & 0x7fffffff;
+                        p = vals[q];
+                        cand = p < kk && rec[q].ex;  // a body removed earlier in the pass is not pushed
+                  }
+                  const unsigned m = __ballot_sync(0xffffffffu, cand);
+                  // this entry's list starts at lane a of the round (the lists are contiguous, in lane order)
+                  const int a = o >= 0 ? max(pre[w][o] - f0, 0) : 0;
+                  const unsigned below = (1u << lane) - 1u, from_a = ~((1u << a) - 1u);
+                  const int nb = o >= 0 ? run[w][o] + __popc(m & below & from_a) : 0;
+                  const int on = __shfl_down_sync(0xffffffffu, o, 1);
+                  __syncwarp();
+                  if (o >= 0 && (lane == 31 || on != o))  // the list's last entry in this round: its running count
+                        run[w][o] += __popc(m & from_a & (lane == 31 ? 0xffffffffu : ((2u << lane) - 1u)));
+                  if (cand) {
+                        const long pos = (long)opos[w][o] + nb;
                         if (pos >= pair_cap) {
                               atomicOr(err, ERR_CAPACITY);
-                              return;
+                        } else {
+                              ck[pos] = kk;
+                              cp[pos] = p;
+                              unsigned char f = 0;
+                              const MRec rp = load_mrec(rec, q);
+                              if (test && !(okk[w][o] & 0x80000000) && !rp.did &&
+                                  d_contact_rec(rp, load_mrec(rec, t0 + o), dt)) {  // closest_approach(p, k)
+                                    f = 1;
+                                    int h = atomicAdd(nhits, 1);
+                                    if (h < hit_cap) hitpos[h] = (int)pos;
+                                    else atomicOr(err, ERR_CAPACITY);
+                              }
+                              cflag[pos] = f;
                         }
-                        ck[pos] = k;
-                        cp[pos] = p;
-                        unsigned char f = 0;
-                        if (test && !dk && !rp.did && d_contact_rec(rp, rk, dt)) {  // closest_approach(p, k)
-                              f = 1;
-                              int h = atomicAdd(nhits, 1);
-                              if (h < hit_cap) hitpos[h] = pos;
-                              else atomicOr(err, ERR_CAPACITY);
-                        }
-                        cflag[pos] = f;
-                        ++pos;
                   }
+                  __syncwarp();
             }
+            skip += MWQ;
       }
 }
 
@@ -695,7 +764,7 @@ static int mesh_segment_launch(const DevState &S, int lid, int lo, int hi, long 
       NCG_CK(cudaMemsetAsync(c.scal + S_NHITS, 0, sizeof(int), st));
       // (positions at or past pair_cap are not written: the kernel records the
       // overflow and the host returns NCGPU_E_CAPACITY)
-      k_mesh_write<<<nb, 256, 0, st>>>(rec, c.ckey, c.mvals, c.crange, c.moff, lid, lo, hi, d,
+      k_mesh_write<<<(n + MWW * 32 - 1) / (MWW * 32), MWW * 32, 0, st>>>(rec, c.ckey, c.mvals, c.crange, c.moff, lid, lo, hi, d,
                                        (long long)c.cell_cap, c.dt, test, c.cand_k, c.cand_p, c.cflag, c.hi, c.hit_cap,
                                        c.scal + S_NHITS, c.pair_cap, c.err);
       NCG_LAUNCHED();

@@ -332,8 +332,20 @@ def program_resume_case(profile, bodies, bodies_from):
     for f in RESUME_FILES:
         data = open(os.path.join(d, f), "rb").read()
         out["digest_" + f] = digest(np.frombuffer(data, np.uint8))
+    cols, radii = split_radius_column(open(os.path.join(d, "init.txt")).read())
+    out["digest_init_without_radius"] = digest(np.frombuffer(cols.encode(), np.uint8))
+    out["init_radius"] = radii
     out["digest_stdout"] = digest(np.frombuffer(filtered_stdout(r.stdout).encode(), np.uint8))
     return out
+
+
+def split_radius_column(text):
+    """init.txt as written by resume(): the text of its first seven columns and
+    the eighth (the radius) parsed as doubles."""
+    lines = text.splitlines()
+    cols = "\n".join(" ".join(l.split()[:7]) for l in lines)
+    radii = np.array([float(l.split()[7]) for l in lines])
+    return cols, radii
 
 
 def main(names=None):
