@@ -148,7 +148,7 @@ __global__ void k_mesh_count(const MRec *__restrict__ rec, const int *__restrict
 // A lane whose queue is full walks again in the next round, queueing the
 // entries after those already taken.
 constexpr int MWW = 4;   // warps per block
-constexpr int MWQ = 48;  // queued entries per lane and round
+constexpr int MWQ = 32;  // queued entries per lane and round
 
 __global__ void __launch_bounds__(MWW * 32) k_mesh_write(const MRec *__restrict__ rec, const int *__restrict__ ckey,
                                                         const int *__restrict__ vals, const int2 *__restrict__ crange,
@@ -161,9 +161,9 @@ __global__ void __launch_bounds__(MWW * 32) k_mesh_write(const MRec *__restrict_
       __shared__ int qb[MWW][32 * MWQ];
       __shared__ unsigned char owner[MWW][32 * MWQ];
       __shared__ int pre[MWW][32], run[MWW][32], okk[MWW][32], opos[MWW][32];
+      __shared__ MRec orec[MWW][32];  // the lists' owners' records
       const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       const int t = blockIdx.x * blockDim.x + threadIdx.x;  // cell order, as k_mesh_count
-      const int t0 = t - lane;
       int k = -1, L = -1;
       if (t <= lid) {
             k = vals[t];
@@ -171,7 +171,9 @@ __global__ void __launch_bounds__(MWW * 32) k_mesh_write(const MRec *__restrict_
       }
       bool dk = false;
       if (L >= 0) {
-            dk = test && rec[t].did;
+            const MRec rk = load_mrec(rec, t);
+            orec[w][lane] = rk;
+            dk = test && rk.did;
             opos[w][lane] = off[k];
       }
       okk[w][lane] = (L >= 0 ? k : -1) | (dk ? 0x80000000 : 0);
@@ -237,7 +239,7 @@ __global__ void __launch_bounds__(MWW * 32) k_mesh_write(const MRec *__restrict_
                               unsigned char f = 0;
                               const MRec rp = load_mrec(rec, q);
                               if (test && !(okk[w][o] & 0x80000000) && !rp.did &&
-                                  d_contact_rec(rp, load_mrec(rec, t0 + o), dt)) {  // closest_approach(p, k)
+                                  d_contact_rec(rp, orec[w][o], dt)) {  // closest_approach(p, k)
                                     f = 1;
                                     int h = atomicAdd(nhits, 1);
                                     if (h < hit_cap) hitpos[h] = (int)pos;
