@@ -590,6 +590,8 @@ def main(argv=None):
     ap.add_argument("--mesh-n", type=int, default=MESH_N, help="mesh workload bodies (smaller cases for profiling)")
     ap.add_argument("--mesh-cells", type=int, default=1024)
     ap.add_argument("--mesh-steps", type=int, default=MESH_STEPS)
+    ap.add_argument("--mesh-only", action="store_true",
+                    help="profiling aid: only the mesh section (fast mode), its own JSON line")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
     ws, rank, local = dist_info()
@@ -608,6 +610,18 @@ def main(argv=None):
     if not os.path.exists(api.LIB_PATH):
         build.build()
     lib = api.load()
+
+    if a.mesh_only:
+        r = bench_mesh(lib, api, torch, api.GRAVITY_MIXED, a.mesh_steps, a.warmup, a.mesh_n, a.mesh_cells)
+        if rank == 0:
+            print(json.dumps({"metric": f"mesh collision steps/s at N={a.mesh_n} (fast mode)",
+                              "value": r["steps_per_s"], "unit": "steps/s", "n_gpus": ws, "steps": a.mesh_steps,
+                              "warmup": a.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+                              "config": {"workload": MESH_WORKLOAD, "n": a.mesh_n, "cells": a.mesh_cells},
+                              "mesh": r}))
+        if ws > 1:
+            torch.distributed.destroy_process_group()
+        return 0
 
     b, ex, cm = make_workload()
     n = N_BODIES
