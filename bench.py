@@ -477,7 +477,7 @@ def bench_fragment(lib, api, torch, mode, steps):
 
 
 BF_N, BF_STEPS, BF_DT = 2000, 200, 1e-3
-ADJ_N, ADJ_STEPS = 16384, 100
+ADJ_N, ADJ_STEPS = 16384, 1000
 
 
 def bench_bf_collide(lib, api, torch, cpu_ref):
@@ -528,26 +528,33 @@ def bench_bf_collide(lib, api, torch, cpu_ref):
 def bench_adjoint(lib, api, torch):
     """C4: forward + adjoint of the differentiable leapfrog (ncgpu_leapfrog_vjp:
     forward with checkpoints every 32 steps, then the reverse sweep with
-    recomputation) at N=16,384 for 100 steps; CUDA events on the library stream."""
+    recomputation) at N=16,384 for the workload's 1,000 steps, in the MIXED
+    mode (FP32 pair terms for far tile pairs) and the FP64 mode; CUDA events on
+    the library stream."""
     from ncorpion_b200 import disks
     b, cm = disks.reduce_to_com(disks.adjoint_disk(ADJ_N, 0), np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0]))
-    api.init(ADJ_N, api.default_params(G=1.0, softening_parameter=0.5, collision_bool=0))
     adj = np.random.default_rng(0).normal(size=(ADJ_N, 3))
     args = (b[:, :3], b[:, 3:6], b[:, 6], b[:, 7], cm, 1e-3, ADJ_STEPS, adj)
-    api.leapfrog_vjp(*args)
-    st = torch.cuda.ExternalStream(lib.ncgpu_stream())
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    api.leapfrog_vjp(*args)
-    e1.record(st)
-    e1.synchronize()
-    t = e0.elapsed_time(e1) / 1e3
-    api.finalize()
-    return {"metric": "forward+adjoint leapfrog steps/s at N=16,384", "steps_per_s": ADJ_STEPS / t,
-            "ms_per_step": 1e3 * t / ADJ_STEPS, "checkpoint": 32,
-            "workload": "gravity-only disk, N=16,384, log-uniform masses, R=1e-2, softening 0.5 (R_k+R_p), dt=1e-3, "
-                        "100 steps: forward with checkpoints, reverse sweep with recomputation (FP64)"}
+    out = {"metric": "forward+adjoint leapfrog steps/s at N=16,384", "checkpoint": 32, "steps": ADJ_STEPS,
+           "workload": "gravity-only disk, N=16,384, log-uniform masses, R=1e-2, softening 0.5 (R_k+R_p), dt=1e-3, "
+                       f"{ADJ_STEPS} steps: forward with checkpoints, reverse sweep with recomputation"}
+    for name, mode in (("mixed", api.GRAVITY_MIXED), ("fp64", api.GRAVITY_EXACT)):
+        api.init(ADJ_N, api.default_params(G=1.0, softening_parameter=0.5, collision_bool=0, gravity_mode=mode))
+        short = args[:6] + (10,) + args[7:]
+        api.leapfrog_vjp(*short)  # warm-up
+        st = torch.cuda.ExternalStream(lib.ncgpu_stream())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        api.leapfrog_vjp(*args)
+        e1.record(st)
+        e1.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        api.finalize()
+        out[name] = {"steps_per_s": ADJ_STEPS / t, "ms_per_step": 1e3 * t / ADJ_STEPS}
+    out["steps_per_s"] = out["mixed"]["steps_per_s"]
+    out["ms_per_step"] = out["mixed"]["ms_per_step"]
+    return out
 
 
 def mesh_cpu_reference(nsteps=3):

@@ -15,7 +15,16 @@
 //   (da/dX)^T ...          = sum_k G J_k (M lambda_k - m_k Lambda)
 //   (da/dm)^T ...     |_k  = -sum_j G (lambda_j . r) / D^3 + G Lambda . s_k / |s_k|^3
 // Pair sums are FP64 with one rsqrt per pair, tiled through shared memory with
-// (target block, source chunk) work units reduced in a fixed order.
+// (target block, source chunk) work units reduced in a fixed order.  In the
+// MIXED gravity mode the bodies are taken in the Morton order of their initial
+// positions (a permutation done on the host at the call's boundary), every
+// evaluation computes the 128-body tiles' boxes, and only the tile pairs whose
+// boxes are near (near_theta x the larger diagonal, and each tile with itself)
+// are summed in FP64; the others in FP32 on coordinates relative to the source
+// tile's centre, the FP32 sums of every 64 sources folded into FP64 -- the
+// force kernel's scheme applied to the force, its VJP and its JVP.
+#include <algorithm>
+#include <vector>
 #include "common.cuh"
 
 namespace ncg {
@@ -84,6 +93,223 @@ __global__ void __launch_bounds__(AT) k_pairs(Src s, int n, int tpc, double *__r
                         const double c = 3.0 * rw * i5;
                         o0 += wx * i3 - rx * c; o1 += wy * i3 - ry * c; o2 += wz * i3 - rz * c;
                         o3 -= (slx[q] * rx + sly[q] * ry + slz[q] * rz) * i3;
+                  }
+            }
+      }
+      if (act) {
+            double *p = part + (size_t)blockIdx.x * (OP == 1 ? 4 : 3) * stride;
+            p[k] = o0; p[stride + k] = o1; p[2 * stride + k] = o2;
+            if (OP == 1) p[3 * stride + k] = o3;
+      }
+}
+
+// One warp per tile: centre and half extents of its bodies' box.
+__global__ void k_adj_tilebox(const double *__restrict__ pos, int n, int ntiles, double *__restrict__ box)
+{
+      const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+      if (warp >= ntiles) return;
+      const int base = warp * AT, cnt = min(AT, n - base);
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (int j = lane; j < cnt; j += 32)
+            for (int d = 0; d < 3; d++) {
+                  const double v = pos[(size_t)d * n + base + j];
+                  lo[d] = fmin(lo[d], v);
+                  hi[d] = fmax(hi[d], v);
+            }
+      for (int o = 16; o > 0; o >>= 1)
+            for (int d = 0; d < 3; d++) {
+                  lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                  hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+            }
+      if (lane < 3) {
+            box[warp * 6 + lane] = 0.5 * (lo[lane] + hi[lane]);
+            box[warp * 6 + 3 + lane] = 0.5 * (hi[lane] - lo[lane]);
+      }
+}
+
+// k_pairs in the MIXED mode: FP64 for near tile pairs (the same pair terms),
+// FP32 relative to the source tile's centre for the others, with packed f32x2
+// arithmetic (two sources per instruction) for the force and its VJP.  (Two
+// targets a thread measured slower: 1.56 against 1.15 ms per forward+adjoint
+// step at N = 16,384, from 128 registers a thread and the serial FP64 near
+// tiles.)
+template <int OP, bool SOFT>
+__global__ void __launch_bounds__(AT) k_pairs_mx(Src s, int n, int tpc, const double *__restrict__ box, double theta,
+                                                 double *__restrict__ part, long stride)
+{
+      __shared__ double sx[AT], sy[AT], sz[AT], sm[AT], sr[AT], slx[AT], sly[AT], slz[AT], sdm[AT];
+      __shared__ __align__(16) float fx[AT], fy[AT], fz[AT], fm[AT], fr[AT], flx[AT], fly[AT], flz[AT], fdm[AT];
+      const int ib = blockIdx.y;
+      const int k = ib * AT + threadIdx.x;
+      const bool act = k < n;
+      const int kk = act ? k : 0;
+      const double xk = s.x[kk], yk = s.y[kk], zk = s.z[kk], mk = s.m[kk], rk = SOFT ? s.sR[kk] : 0.;
+      double lxk = 0., lyk = 0., lzk = 0.;
+      if (OP >= 1) { lxk = s.lx[kk]; lyk = s.ly[kk]; lzk = s.lz[kk]; }
+      const float mkf = (float)mk, rkf = (float)rk, lxkf = (float)lxk, lykf = (float)lyk, lzkf = (float)lzk;
+      double o0 = 0., o1 = 0., o2 = 0., o3 = 0.;
+      const int ntiles = (n + AT - 1) / AT;
+      const int t0 = blockIdx.x * tpc, t1 = min(ntiles, t0 + tpc);
+      const double *bi = box + 6 * ib;
+      for (int t = t0; t < t1; ++t) {
+            const int j = t * AT + threadIdx.x;
+            const double *bj = box + 6 * t;
+            const bool near = t == ib || tiles_near(bi, bj, theta);
+            __syncthreads();
+            if (j >= n && !near) {  // padding of the far path: far away, massless, no adjoint
+                  fx[threadIdx.x] = fy[threadIdx.x] = fz[threadIdx.x] = 1e18f;
+                  fm[threadIdx.x] = fr[threadIdx.x] = flx[threadIdx.x] = fly[threadIdx.x] = flz[threadIdx.x] = 0.f;
+                  fdm[threadIdx.x] = 0.f;
+            }
+            if (j < n) {
+                  if (near) {
+                        sx[threadIdx.x] = s.x[j]; sy[threadIdx.x] = s.y[j]; sz[threadIdx.x] = s.z[j];
+                        sm[threadIdx.x] = s.m[j];
+                        if (SOFT) sr[threadIdx.x] = s.sR[j];
+                        if (OP >= 1) { slx[threadIdx.x] = s.lx[j]; sly[threadIdx.x] = s.ly[j]; slz[threadIdx.x] = s.lz[j]; }
+                        if (OP == 2) sdm[threadIdx.x] = s.dm[j];
+                  } else {
+                        fx[threadIdx.x] = (float)(s.x[j] - bj[0]);
+                        fy[threadIdx.x] = (float)(s.y[j] - bj[1]);
+                        fz[threadIdx.x] = (float)(s.z[j] - bj[2]);
+                        fm[threadIdx.x] = (float)s.m[j];
+                        if (SOFT) fr[threadIdx.x] = (float)s.sR[j];
+                        if (OP >= 1) {
+                              flx[threadIdx.x] = (float)s.lx[j]; fly[threadIdx.x] = (float)s.ly[j];
+                              flz[threadIdx.x] = (float)s.lz[j];
+                        }
+                        if (OP == 2) fdm[threadIdx.x] = (float)s.dm[j];
+                  }
+            }
+            __syncthreads();
+            const int cnt = min(AT, n - t * AT);
+            if (near) {
+                  for (int q = 0; q < cnt; ++q) {
+                        if (t * AT + q == k) continue;
+                        const double rx = sx[q] - xk, ry = sy[q] - yk, rz = sz[q] - zk;
+                        double d2 = 0.;
+                        if (SOFT) { const double e = rk + sr[q]; d2 = e * e; }
+                        d2 = fma(rx, rx, fma(ry, ry, fma(rz, rz, d2)));
+                        const double ri = rsqrt(d2);
+                        const double i3 = ri * ri * ri;
+                        if (OP == 0) {
+                              const double w = sm[q] * i3;
+                              o0 = fma(w, rx, o0); o1 = fma(w, ry, o1); o2 = fma(w, rz, o2);
+                        } else if (OP == 2) {
+                              const double i5 = i3 * ri * ri;
+                              const double dx = slx[q] - lxk, dy = sly[q] - lyk, dz = slz[q] - lzk;
+                              const double rd = rx * dx + ry * dy + rz * dz;
+                              const double mj = sm[q], c = 3.0 * rd * i5 * mj, g = sdm[q] * i3;
+                              o0 += g * rx + mj * i3 * dx - rx * c;
+                              o1 += g * ry + mj * i3 * dy - ry * c;
+                              o2 += g * rz + mj * i3 * dz - rz * c;
+                        } else {
+                              const double i5 = i3 * ri * ri;
+                              const double mj = sm[q];
+                              const double wx = mk * slx[q] - mj * lxk, wy = mk * sly[q] - mj * lyk, wz = mk * slz[q] - mj * lzk;
+                              const double rw = rx * wx + ry * wy + rz * wz;
+                              const double c = 3.0 * rw * i5;
+                              o0 += wx * i3 - rx * c; o1 += wy * i3 - ry * c; o2 += wz * i3 - rz * c;
+                              o3 -= (slx[q] * rx + sly[q] * ry + slz[q] * rz) * i3;
+                        }
+                  }
+            } else if (OP == 0) {
+                  // packed f32x2: two sources per instruction; FP32 runs of 64 sources
+                  const float xr = (float)(xk - bj[0]), yr = (float)(yk - bj[1]), zr = (float)(zk - bj[2]);
+                  const f2 XT = f2_pack(xr, xr), YT = f2_pack(yr, yr), ZT = f2_pack(zr, zr), RT = f2_pack(rkf, rkf);
+                  const int ce = (cnt + 1) & ~1;
+                  for (int q0 = 0; q0 < ce; q0 += 64) {
+                        f2 P0 = 0ull, P1 = 0ull, P2 = 0ull;
+                        const int qe = min(ce, q0 + 64);
+#pragma unroll 4
+                        for (int q = q0; q < qe; q += 2) {
+                              const f2 dx = f2_sub(*(const f2 *)&fx[q], XT), dy = f2_sub(*(const f2 *)&fy[q], YT);
+                              const f2 dz = f2_sub(*(const f2 *)&fz[q], ZT);
+                              f2 d2;
+                              if (SOFT) {
+                                    const f2 e = f2_add(*(const f2 *)&fr[q], RT);
+                                    d2 = f2_fma(dx, dx, f2_mul(e, e));
+                              } else {
+                                    d2 = f2_mul(dx, dx);
+                              }
+                              d2 = f2_fma(dy, dy, d2);
+                              d2 = f2_fma(dz, dz, d2);
+                              const f2 i = f2_rsqrt(d2);
+                              const f2 w = f2_mul(f2_mul(*(const f2 *)&fm[q], i), f2_mul(i, i));
+                              P0 = f2_fma(w, dx, P0);
+                              P1 = f2_fma(w, dy, P1);
+                              P2 = f2_fma(w, dz, P2);
+                        }
+                        float lo, hi;
+                        f2_unpack(P0, lo, hi); o0 += (double)lo + (double)hi;
+                        f2_unpack(P1, lo, hi); o1 += (double)lo + (double)hi;
+                        f2_unpack(P2, lo, hi); o2 += (double)lo + (double)hi;
+                  }
+            } else if (OP == 1) {
+                  // the VJP's pair terms, packed as OP 0
+                  const float xr = (float)(xk - bj[0]), yr = (float)(yk - bj[1]), zr = (float)(zk - bj[2]);
+                  const f2 XT = f2_pack(xr, xr), YT = f2_pack(yr, yr), ZT = f2_pack(zr, zr), RT = f2_pack(rkf, rkf);
+                  const f2 MK = f2_pack(mkf, mkf), NLX = f2_pack(-lxkf, -lxkf), NLY = f2_pack(-lykf, -lykf),
+                           NLZ = f2_pack(-lzkf, -lzkf), NEG3 = f2_pack(-3.f, -3.f);
+                  const int ce = (cnt + 1) & ~1;
+                  for (int q0 = 0; q0 < ce; q0 += 64) {
+                        f2 P0 = 0ull, P1 = 0ull, P2 = 0ull, P3 = 0ull;
+                        const int qe = min(ce, q0 + 64);
+#pragma unroll 2
+                        for (int q = q0; q < qe; q += 2) {
+                              const f2 rx = f2_sub(*(const f2 *)&fx[q], XT), ry = f2_sub(*(const f2 *)&fy[q], YT);
+                              const f2 rz = f2_sub(*(const f2 *)&fz[q], ZT);
+                              f2 d2;
+                              if (SOFT) {
+                                    const f2 e = f2_add(*(const f2 *)&fr[q], RT);
+                                    d2 = f2_fma(rx, rx, f2_mul(e, e));
+                              } else {
+                                    d2 = f2_mul(rx, rx);
+                              }
+                              d2 = f2_fma(ry, ry, d2);
+                              d2 = f2_fma(rz, rz, d2);
+                              const f2 ri = f2_rsqrt(d2);
+                              const f2 r2i = f2_mul(ri, ri);
+                              const f2 i3 = f2_mul(r2i, ri), i5 = f2_mul(i3, r2i);
+                              const f2 mj = *(const f2 *)&fm[q];
+                              const f2 LX = *(const f2 *)&flx[q], LY = *(const f2 *)&fly[q], LZ = *(const f2 *)&flz[q];
+                              // w = m_k lambda_j - m_j lambda_k
+                              const f2 wx = f2_fma(mj, NLX, f2_mul(MK, LX)), wy = f2_fma(mj, NLY, f2_mul(MK, LY));
+                              const f2 wz = f2_fma(mj, NLZ, f2_mul(MK, LZ));
+                              const f2 rw = f2_fma(rz, wz, f2_fma(ry, wy, f2_mul(rx, wx)));
+                              const f2 nc = f2_mul(f2_mul(NEG3, rw), i5);  // -3 (r . w) / D^5
+                              P0 = f2_fma(wx, i3, f2_fma(rx, nc, P0));
+                              P1 = f2_fma(wy, i3, f2_fma(ry, nc, P1));
+                              P2 = f2_fma(wz, i3, f2_fma(rz, nc, P2));
+                              const f2 lr = f2_fma(LZ, rz, f2_fma(LY, ry, f2_mul(LX, rx)));
+                              P3 = f2_sub(P3, f2_mul(lr, i3));
+                        }
+                        float lo, hi;
+                        f2_unpack(P0, lo, hi); o0 += (double)lo + (double)hi;
+                        f2_unpack(P1, lo, hi); o1 += (double)lo + (double)hi;
+                        f2_unpack(P2, lo, hi); o2 += (double)lo + (double)hi;
+                        f2_unpack(P3, lo, hi); o3 += (double)lo + (double)hi;
+                  }
+            } else {  // OP 2 (the JVP), scalar FP32
+                  const float xr = (float)(xk - bj[0]), yr = (float)(yk - bj[1]), zr = (float)(zk - bj[2]);
+                  for (int q0 = 0; q0 < cnt; q0 += 64) {  // FP32 runs of 64 sources
+                        float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+                        const int qe = min(cnt, q0 + 64);
+                        for (int q = q0; q < qe; ++q) {
+                              const float rx = fx[q] - xr, ry = fy[q] - yr, rz = fz[q] - zr;
+                              float d2 = 0.f;
+                              if (SOFT) { const float e = rkf + fr[q]; d2 = e * e; }
+                              d2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, d2)));
+                              const float ri = rsqrtf(d2);
+                              const float i3 = ri * ri * ri, i5 = i3 * ri * ri;
+                              const float dx = flx[q] - lxkf, dy = fly[q] - lykf, dz = flz[q] - lzkf;
+                              const float rd = rx * dx + ry * dy + rz * dz;
+                              const float mj = fm[q], c = 3.f * rd * i5 * mj, g = fdm[q] * i3;
+                              p0 += g * rx + mj * i3 * dx - rx * c;
+                              p1 += g * ry + mj * i3 * dy - ry * c;
+                              p2 += g * rz + mj * i3 * dz - rz * c;
+                        }
+                        o0 += (double)p0; o1 += (double)p1; o2 += (double)p2;
                   }
             }
       }
@@ -236,17 +462,35 @@ struct LF {
       double *ckpt, *seg;
       double *tx, *tv, *tm, *tX, *da, *dA;  // tangents (JVP)
       int C, ncp;
+      bool mixed;                  // MIXED gravity mode: k_pairs_mx with tile boxes
+      double theta, *box;
       cudaStream_t st;
 };
+
+// the pair sums of OP over positions pos (tile boxes first in the mixed mode)
+template <int OP>
+int lf_pairs(LF &L, const Src &s, const double *pos)
+{
+      const int n = L.n;
+      dim3 grid(L.nch, L.ntiles);
+      if (L.mixed) {
+            k_adj_tilebox<<<(L.ntiles * 32 + 255) / 256, 256, 0, L.st>>>(pos, n, L.ntiles, L.box);
+            NCG_LAUNCHED();
+            if (L.soft) k_pairs_mx<OP, true><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.box, L.theta, L.part, n);
+            else k_pairs_mx<OP, false><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.box, L.theta, L.part, n);
+      } else {
+            if (L.soft) k_pairs<OP, true><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
+            else k_pairs<OP, false><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
+      }
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
 
 int lf_force(LF &L, const double *pos, const double *cmpos)
 {
       const int n = L.n;
       Src s{pos, pos + n, pos + 2 * n, L.m, L.sR, nullptr, nullptr, nullptr};
-      dim3 grid(L.nch, L.ntiles);
-      if (L.soft) k_pairs<0, true><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
-      else k_pairs<0, false><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
-      NCG_LAUNCHED();
+      NCG_TRY(lf_pairs<0>(L, s, pos));
       k_force_final<<<(n + 255) / 256, 256, 0, L.st>>>(L.part, L.nch, n, s, n, cmpos, L.G, L.M, L.central, L.acc,
                                                        L.acc + n, L.acc + 2 * n, L.cterm);
       NCG_LAUNCHED();
@@ -275,10 +519,7 @@ int lf_vjp(LF &L, const double *pos, const double *cmpos)
 {
       const int n = L.n;
       Src s{pos, pos + n, pos + 2 * n, L.m, L.sR, L.lv, L.lv + n, L.lv + 2 * n};
-      dim3 grid(L.nch, L.ntiles);
-      if (L.soft) k_pairs<1, true><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
-      else k_pairs<1, false><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
-      NCG_LAUNCHED();
+      NCG_TRY(lf_pairs<1>(L, s, pos));
       k_vjp_final<<<(n + 255) / 256, 256, 0, L.st>>>(L.part, L.nch, n, s, n, cmpos, L.LV, L.G, L.M, L.central, L.mu,
                                                      L.mu + n, L.mu + 2 * n, L.nu, L.xterm);
       NCG_LAUNCHED();
@@ -297,10 +538,7 @@ int lf_step_jvp(LF &L, double dt)
       const int n = L.n, nb = (n + 255) / 256;
       NCG_TRY(lf_force(L, L.X, L.cm));
       Src s{L.X, L.X + n, L.X + 2 * n, L.m, L.sR, L.tx, L.tx + n, L.tx + 2 * n, L.tm};
-      dim3 grid(L.nch, L.ntiles);
-      if (L.soft) k_pairs<2, true><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
-      else k_pairs<2, false><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
-      NCG_LAUNCHED();
+      NCG_TRY(lf_pairs<2>(L, s, L.X));
       k_jvp_final<<<nb, 256, 0, L.st>>>(L.part, L.nch, n, s, n, L.cm, L.tX, L.G, L.M, L.central, L.da, L.da + n,
                                         L.da + 2 * n, L.xterm);
       NCG_LAUNCHED();
@@ -350,7 +588,7 @@ __global__ void k_xf(const double *__restrict__ X, const double *__restrict__ V,
             for (int d = 0; d < 3; d++) out[(size_t)d * n + k] = X[(size_t)d * n + k] - h * V[(size_t)d * n + k];
 }
 
-int lf_run(const struct ncgpu_leapfrog_args *a, int mode)
+int lf_core(const struct ncgpu_leapfrog_args *a, int mode, bool mixed)
 {
       const bool vjp = mode == 1, jvp = mode == 2;
       Ctx &c = ctx();
@@ -367,17 +605,29 @@ int lf_run(const struct ncgpu_leapfrog_args *a, int mode)
       L.central = c.P.par_central_mass_bool != 0;
       L.soft = c.P.par_softening_parameter != 0.;
       L.ntiles = (n + AT - 1) / AT;
-      L.nch = std::max(1, std::min(L.ntiles, (2048 + L.ntiles - 1) / L.ntiles));
+      if (mixed) {
+            // (target tile, source chunk) work units: about 8 per resident CTA
+            // slot, so that the last wave is short
+            int occ = 1;
+            NCG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pairs_mx<1, true>, AT, 0));
+            const long want = 8L * std::max(occ, 1) * c.sm_count;
+            L.nch = (int)std::max(1L, std::min((long)L.ntiles, (want + L.ntiles - 1) / L.ntiles));
+      } else {
+            L.nch = std::max(1, std::min(L.ntiles, (2048 + L.ntiles - 1) / L.ntiles));
+      }
       L.tpc = (L.ntiles + L.nch - 1) / L.nch;
       L.nch = (L.ntiles + L.tpc - 1) / L.tpc;
       L.np = std::min(128, (n + SB - 1) / SB);
+      L.mixed = mixed;
+      L.theta = c.P.par_near_theta > 0. ? c.P.par_near_theta : 0.15;
       L.C = a->checkpoint > 0 ? a->checkpoint : 32;
       L.ncp = (a->nsteps + L.C - 1) / L.C + 1;
       const size_t N = (size_t)n, st = 6 * N + 6;
       size_t total = 3 * N * 2 + 2 * N + 6 + 3 * N + 3 * N + 4 * N * L.nch + 3 * 128 + 3  // X V m sR cm acc cterm part red acm
                      + 3 * N * 2 + 6 + 3 * N + N + N + 3 * N + 3                     // lx lv LX LV mu nu gm xterm muX
                      + st * L.ncp + (size_t)L.C * (3 * N + 3)                         // checkpoints, segment
-                     + 3 * N * 3 + N + 6 + 3;                                         // tx tv tm tX da dA
+                     + 3 * N * 3 + N + 6 + 3                                          // tx tv tm tX da dA
+                     + 6 * (size_t)L.ntiles;                                          // tile boxes
       double *buf = nullptr;
       NCG_CK(cudaMalloc(&buf, total * sizeof(double)));
       double *p = buf;
@@ -389,6 +639,7 @@ int lf_run(const struct ncgpu_leapfrog_args *a, int mode)
       L.gm = take(N); L.xterm = take(3 * N); L.muX = take(3);
       L.ckpt = take(st * L.ncp); L.seg = take((size_t)L.C * (3 * N + 3));
       L.tx = take(3 * N); L.tv = take(3 * N); L.tm = take(N); L.tX = take(6); L.da = take(3 * N); L.dA = take(3);
+      L.box = take(6 * (size_t)L.ntiles);
       int status = NCGPU_OK;
       cudaError_t e = cudaSuccess;
       const double h = a->dt / 2.0, dt = a->dt;
@@ -502,6 +753,85 @@ done:
       cudaStreamSynchronize(L.st);
       cudaFree(buf);
       return status;
+}
+
+// Morton order (30-bit keys from one cubic quantisation of the bounding box)
+// of n positions given as 3n AoS doubles: perm[i] = the body at position i.
+void morton_order(const double *x, int n, std::vector<int> &perm)
+{
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+      for (int k = 0; k < n; k++)
+            for (int d = 0; d < 3; d++) {
+                  lo[d] = std::min(lo[d], x[3 * k + d]);
+                  hi[d] = std::max(hi[d], x[3 * k + d]);
+            }
+      const double ext = std::max(std::max(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]);
+      std::vector<uint32_t> key(n);
+      for (int k = 0; k < n; k++) {
+            uint32_t q[3];
+            for (int d = 0; d < 3; d++) {
+                  const double f = ext > 0. ? (x[3 * k + d] - lo[d]) / ext : 0.;
+                  q[d] = (uint32_t)std::min(std::max((int)(f * 1023.999), 0), 1023);
+            }
+            uint32_t m = 0;
+            for (int b = 9; b >= 0; b--)
+                  for (int d = 2; d >= 0; d--) m = (m << 1) | ((q[d] >> b) & 1u);
+            key[k] = m;
+      }
+      perm.resize(n);
+      for (int k = 0; k < n; k++) perm[k] = k;
+      std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return key[a] < key[b]; });
+}
+
+// The MIXED mode runs on the bodies in Morton order of their initial
+// positions: the inputs are permuted here, the outputs restored to the
+// caller's order.
+int lf_run(const struct ncgpu_leapfrog_args *a, int mode)
+{
+      Ctx &c = ctx();
+      if (c.P.par_gravity_mode != NCGPU_GRAVITY_MIXED) return lf_core(a, mode, false);
+      const int n = a->n;
+      if (n <= 0 || !a->x0 || !a->v0 || !a->m || !a->R || !a->cm || a->nsteps < 0) return NCGPU_E_ARG;
+      std::vector<int> perm;
+      morton_order(a->x0, n, perm);
+      const size_t N = (size_t)n;
+      auto gather3 = [&](const double *src, std::vector<double> &dst) {
+            dst.resize(3 * N);
+            for (size_t i = 0; i < N; i++)
+                  for (int d = 0; d < 3; d++) dst[3 * i + d] = src[3 * (size_t)perm[i] + d];
+      };
+      auto gather1 = [&](const double *src, std::vector<double> &dst) {
+            dst.resize(N);
+            for (size_t i = 0; i < N; i++) dst[i] = src[perm[i]];
+      };
+      std::vector<double> x0, v0, m, R, adj, tx0, tv0, tm, xf, vf, gx, gv, gm, txf;
+      gather3(a->x0, x0); gather3(a->v0, v0); gather1(a->m, m); gather1(a->R, R);
+      struct ncgpu_leapfrog_args b = *a;
+      b.x0 = x0.data(); b.v0 = v0.data(); b.m = m.data(); b.R = R.data();
+      if (a->adj_x_final) { gather3(a->adj_x_final, adj); b.adj_x_final = adj.data(); }
+      if (a->tan_x0) { gather3(a->tan_x0, tx0); b.tan_x0 = tx0.data(); }
+      if (a->tan_v0) { gather3(a->tan_v0, tv0); b.tan_v0 = tv0.data(); }
+      if (a->tan_m) { gather1(a->tan_m, tm); b.tan_m = tm.data(); }
+      if (a->x_final) { xf.resize(3 * N); b.x_final = xf.data(); }
+      if (a->v_final) { vf.resize(3 * N); b.v_final = vf.data(); }
+      if (a->grad_x0) { gx.resize(3 * N); b.grad_x0 = gx.data(); }
+      if (a->grad_v0) { gv.resize(3 * N); b.grad_v0 = gv.data(); }
+      if (a->grad_m) { gm.resize(N); b.grad_m = gm.data(); }
+      if (a->tan_x_final) { txf.resize(3 * N); b.tan_x_final = txf.data(); }
+      const int st = lf_core(&b, mode, true);
+      if (st != NCGPU_OK) return st;
+      auto scatter3 = [&](const std::vector<double> &src, double *dst) {
+            for (size_t i = 0; i < N; i++)
+                  for (int d = 0; d < 3; d++) dst[3 * (size_t)perm[i] + d] = src[3 * i + d];
+      };
+      if (a->x_final) scatter3(xf, a->x_final);
+      if (a->v_final) scatter3(vf, a->v_final);
+      if (a->grad_x0) scatter3(gx, a->grad_x0);
+      if (a->grad_v0) scatter3(gv, a->grad_v0);
+      if (a->grad_m)
+            for (size_t i = 0; i < N; i++) a->grad_m[perm[i]] = gm[i];
+      if (a->tan_x_final) scatter3(txf, a->tan_x_final);
+      return NCGPU_OK;
 }
 
 }  // namespace

@@ -106,6 +106,75 @@ __device__ __forceinline__ double div_by_recip(double x, double b, double y)
       return __fma_rn(r, y, q);
 }
 
+// FP32 reciprocal square root (MUFU, flush-to-zero) and sm_100a's packed
+// f32x2 arithmetic (one instruction on both halves of a 64-bit register pair).
+__device__ __forceinline__ float rsqrt_ftz(float x)
+{
+      float y;
+      asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+      return y;
+}
+
+// Packed pairs of FP32 values (sm_100a f32x2 arithmetic: one instruction
+// operates on both halves).
+typedef unsigned long long f2;
+
+__device__ __forceinline__ f2 f2_pack(float lo, float hi)
+{
+      f2 r;
+      asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+      return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 v, float &lo, float &hi)
+{
+      asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 f2_sub(f2 a, f2 b)
+{
+      f2 r;
+      asm("sub.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+      return r;
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b)
+{
+      f2 r;
+      asm("add.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+      return r;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b)
+{
+      f2 r;
+      asm("mul.rn.ftz.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+      return r;
+}
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c)
+{
+      f2 r;
+      asm("fma.rn.ftz.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+      return r;
+}
+__device__ __forceinline__ f2 f2_rsqrt(f2 q)
+{
+      float lo, hi;
+      f2_unpack(q, lo, hi);
+      return f2_pack(rsqrt_ftz(lo), rsqrt_ftz(hi));
+}
+
+// Two tiles' boxes (centre xyz, half extents xyz) are near when the gap
+// between them is below theta times the larger full diagonal.
+__device__ __forceinline__ bool tiles_near(const double *__restrict__ bi, const double *__restrict__ bj, double theta)
+{
+      double g2 = 0., di = 0., dj = 0.;
+      for (int d = 0; d < 3; d++) {
+            double gap = fabs(bi[d] - bj[d]) - bi[3 + d] - bj[3 + d];
+            if (gap > 0.) g2 += gap * gap;
+            di += bi[3 + d] * bi[3 + d];
+            dj += bj[3 + d] * bj[3 + d];
+      }
+      double dmax2 = 4. * fmax(di, dj);  // squared full diagonal
+      return g2 < theta * theta * dmax2;
+}
+
 // The 27 neighbour cells of a cell L (linear index i + j d + k d^2) as 9 rows
 // of three consecutive indices (x - 1, x, x + 1): row r (0..8) is centred on
 // L + (r % 3 - 1) d + (r / 3 - 1) d^2, so the cell slots l = 26..0 of the

@@ -203,3 +203,84 @@ def test_adjoint_chaotic_disk_dot_product(lib):
         assert np.isfinite(lhs) and abs(lhs - rhs) <= 1e-8 * abs(lhs)
     finally:
         api.finalize()
+
+
+def test_mixed_adjoint_disk_16384_1000_steps(lib):
+    """The differentiable workload in the MIXED gravity mode (FP32 pair terms
+    on tile-relative coordinates for far tile pairs, FP64 for near ones, FP64
+    state): its gradients against the FP64 ones -- x and v against FP64
+    central finite differences (h = 1e-6) of the FP64 forward, m against the
+    FP64 tangent-linear model -- within 1e-5 relative on 64 coordinates of
+    the 16,384-body, 1,000-step run."""
+    from ncorpion_b200 import api, disks
+    p64 = make_params(softening_parameter=0.5)
+    pmx = make_params(softening_parameter=0.5, gravity_mode=api.GRAVITY_MIXED)
+    api.init(16384, p64)
+    try:
+        b, cm = disks.reduce_to_com(disks.adjoint_disk(16384, 0), np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0]))
+        dt, nsteps, n = 1e-3, 1000, len(b)
+        rng = np.random.default_rng(11)
+        x0, v0, m, R = b[:, :3].copy(), b[:, 3:6].copy(), b[:, 6].copy(), b[:, 7].copy()
+        xf, _ = api.leapfrog(x0, v0, m, R, cm, dt, nsteps)
+        api.set_params(pmx)
+        xf_mx, _ = api.leapfrog(x0, v0, m, R, cm, dt, nsteps)
+        print("mixed vs FP64 forward, max |dx| / max |x|:", np.abs(xf_mx - xf).max() / np.abs(xf).max())
+        target = xf + rng.normal(0, 1e-4, xf.shape)
+        adj = 2.0 * (xf - target) / n
+        gx, gv, gm = api.leapfrog_vjp(x0, v0, m, R, cm, dt, nsteps, adj)
+        api.set_params(p64)
+
+        def loss_of(x0_, v0_):
+            return mse_loss(api.leapfrog(x0_, v0_, m, R, cm, dt, nsteps)[0], target)
+
+        worst = {"x": 0.0, "v": 0.0, "m": 0.0}
+        zero3 = np.zeros((n, 3))
+        h = 1e-6
+        for q in range(64):
+            kind = q % 3
+            i = int(rng.integers(n))
+            if kind == 2:
+                em = np.zeros(n)
+                em[i] = 1.0
+                ref = float(np.sum(adj * api.leapfrog_jvp(x0, v0, m, R, cm, dt, nsteps, zero3, zero3, em)))
+                worst["m"] = max(worst["m"], abs(gm[i] - ref) / abs(ref))
+                continue
+            d = int(rng.integers(3))
+            arr = x0 if kind == 0 else v0
+            ap, am = arr.copy(), arr.copy()
+            ap[i, d] += h
+            am[i, d] -= h
+            if kind == 0:
+                fd = (loss_of(ap, v0) - loss_of(am, v0)) / (2 * h)
+                g, key = gx[i, d], "x"
+            else:
+                fd = (loss_of(x0, ap) - loss_of(x0, am)) / (2 * h)
+                g, key = gv[i, d], "v"
+            worst[key] = max(worst[key], abs(g - fd) / max(abs(fd), 1e-300))
+        print("mixed adjoint 16384 x 1000 worst relative errors vs FP64:", worst)
+        assert worst["x"] <= 1e-5 and worst["v"] <= 1e-5 and worst["m"] <= 1e-5, worst
+    finally:
+        api.finalize()
+
+
+def test_mixed_adjoint_is_the_transpose_of_its_tangent(lib):
+    """In the MIXED mode too the VJP and the JVP are transposes of each other
+    along the same trajectory (dot-product identity, 1e-6 relative: both carry
+    FP32 pair terms)."""
+    from ncorpion_b200 import api
+    api.init(1024, make_params(softening_parameter=0.5, gravity_mode=api.GRAVITY_MIXED))
+    try:
+        b, cm = disk(1000, 8)
+        rng = np.random.default_rng(9)
+        n = len(b)
+        args = (b[:, :3], b[:, 3:6], b[:, 6], b[:, 7], cm, 1e-3, 120)
+        dx, dv, dm = rng.normal(size=(n, 3)), rng.normal(size=(n, 3)), rng.normal(size=n) * b[:, 6]
+        w = rng.normal(size=(n, 3))
+        jd = api.leapfrog_jvp(*args, dx, dv, dm)
+        gx, gv, gm = api.leapfrog_vjp(*args, w)
+        lhs = float(np.sum(w * jd))
+        rhs = float(np.sum(gx * dx) + np.sum(gv * dv) + np.sum(gm * dm))
+        print("mixed <w, J d> =", lhs, " <J^T w, d> =", rhs)
+        assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
+    finally:
+        api.finalize()
