@@ -253,6 +253,13 @@ __global__ void __launch_bounds__(256) k_bbox_final(double *__restrict__ part, i
       if (t < 8) part[t] = sh[t][0];
 }
 
+// part[8] = the count of existing bodies (as a double, beside the radius range
+// at part[6..7], so that one copy brings back both)
+__global__ void k_count_beside(const int *__restrict__ n_dev, double *__restrict__ part)
+{
+      part[8] = (double)*n_dev;
+}
+
 __device__ __forceinline__ uint32_t spread3(uint32_t v)
 {
       v &= 0x3ffu;
@@ -263,11 +270,18 @@ __device__ __forceinline__ uint32_t spread3(uint32_t v)
       return v;
 }
 
-__global__ void k_morton(BodyView bv, const int *__restrict__ cidx, int n, const double *__restrict__ box,
-                         uint32_t *__restrict__ keys, int *__restrict__ vals)
+// (n: the existing bodies, from device memory; entries n .. nub - 1 get the
+// largest key, so that they sort after every body)
+__global__ void k_morton(BodyView bv, const int *__restrict__ cidx, const int *__restrict__ n_dev, int nub,
+                         const double *__restrict__ box, uint32_t *__restrict__ keys, int *__restrict__ vals)
 {
       int p = blockIdx.x * blockDim.x + threadIdx.x;
-      if (p >= n) return;
+      if (p >= nub) return;
+      if (p >= *n_dev) {
+            keys[p] = 0xffffffffu;
+            vals[p] = -1;
+            return;
+      }
       int slot = cidx[p];
       long s = (long)slot * bv.stride;
       double v[3] = {bv.x[s], bv.y[s], bv.z[s]};
@@ -284,76 +298,72 @@ __global__ void k_morton(BodyView bv, const int *__restrict__ cidx, int n, const
       vals[p] = slot;
 }
 
-// Sorted FP64 sources: (x, y, z, m) and softening*R, padded with zeros.
-__global__ void k_gather_sorted(BodyView bv, const int *__restrict__ slots, int n, int npad, double sp,
-                                D4 *__restrict__ s64, double *__restrict__ sR)
-{
-      int q = blockIdx.x * blockDim.x + threadIdx.x;
-      if (q >= npad) return;
-      if (q < n) {
-            long s = (long)slots[q] * bv.stride;
-            s64[q] = D4{bv.x[s], bv.y[s], bv.z[s], bv.m[s]};
-            sR[q] = sp * bv.R[s];
-      } else {
-            s64[q] = D4{0., 0., 0., 0.};
-            sR[q] = 0.;
-      }
-}
 
-// One warp per tile: centre and half extents of the tile's bounding box.
-__global__ void k_tilebox(const D4 *__restrict__ s64, int n, int ntiles, double *__restrict__ box)
-{
-      int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-      int lane = threadIdx.x & 31;
-      if (warp >= ntiles) return;
-      int base = warp * T, cnt = min(T, n - base);
-      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-      for (int j = lane; j < cnt; j += 32) {
-            D4 s = s64[base + j];
-            lo[0] = fmin(lo[0], s.x); hi[0] = fmax(hi[0], s.x);
-            lo[1] = fmin(lo[1], s.y); hi[1] = fmax(hi[1], s.y);
-            lo[2] = fmin(lo[2], s.z); hi[2] = fmax(hi[2], s.z);
-      }
-      for (int o = 16; o > 0; o >>= 1)
-            for (int d = 0; d < 3; d++) {
-                  lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
-                  hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
-            }
-      if (lane < 3) {
-            double l = lane == 0 ? lo[0] : lane == 1 ? lo[1] : lo[2];
-            double h = lane == 0 ? hi[0] : lane == 1 ? hi[1] : hi[2];
-            box[warp * 6 + lane] = 0.5 * (l + h);
-            box[warp * 6 + 3 + lane] = 0.5 * (h - l);
-      }
-}
 
 // FP32 tile-relative sources, one SoA block per tile of T bodies:
 // x[T] y[T] z[T] m[T] (coordinates minus the tile's box centre).  Padding
 // sources sit at 1e18 with zero mass, so their pair terms are exactly zero.
-__global__ void k_pack32(const D4 *__restrict__ s64, const double *__restrict__ sR, const double *__restrict__ box,
-                         int n, int npad, float *__restrict__ s32, float *__restrict__ sR32)
+//
+// One warp per tile, in one launch: the tile's bodies gathered in sorted order
+// as FP64 sources (x, y, z, m) and softening * R (zero padding), the centre and
+// half extents of its box, and with `mixed` the FP32 tile-relative copy.
+__global__ void k_tile_prep(BodyView bv, const int *__restrict__ slots, const int *__restrict__ n_dev, int ntiles,
+                            double sp, int mixed, D4 *__restrict__ s64, double *__restrict__ sR,
+                            double *__restrict__ box, float *__restrict__ s32, float *__restrict__ sR32)
 {
-      int q = blockIdx.x * blockDim.x + threadIdx.x;
-      if (q >= npad) return;
-      float *tile = s32 + (size_t)(q / T) * 4 * T;
-      const int j = q % T;
-      if (q < n) {
-            const double *c = box + (q / T) * 6;
-            D4 s = s64[q];
-            tile[j] = (float)(s.x - c[0]);
-            tile[T + j] = (float)(s.y - c[1]);
-            tile[2 * T + j] = (float)(s.z - c[2]);
-            tile[3 * T + j] = (float)s.w;
-            sR32[q] = (float)sR[q];
-      } else {
-            tile[j] = 1e18f;
-            tile[T + j] = 1e18f;
-            tile[2 * T + j] = 1e18f;
-            tile[3 * T + j] = 0.f;
-            sR32[q] = 0.f;
+      const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+      if (warp >= ntiles) return;
+      const int n = *n_dev, base = warp * T;
+      D4 d[T / 32];
+      double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+#pragma unroll
+      for (int u = 0; u < T / 32; u++) {
+            const int q = base + lane + 32 * u;
+            if (q < n) {
+                  const long s = (long)slots[q] * bv.stride;
+                  d[u] = D4{bv.x[s], bv.y[s], bv.z[s], bv.m[s]};
+                  const double r = sp * bv.R[s];
+                  s64[q] = d[u];
+                  sR[q] = r;
+                  if (mixed) sR32[q] = (float)r;
+                  lo[0] = fmin(lo[0], d[u].x); hi[0] = fmax(hi[0], d[u].x);
+                  lo[1] = fmin(lo[1], d[u].y); hi[1] = fmax(hi[1], d[u].y);
+                  lo[2] = fmin(lo[2], d[u].z); hi[2] = fmax(hi[2], d[u].z);
+            } else {
+                  d[u] = D4{0., 0., 0., 0.};
+                  s64[q] = d[u];
+                  sR[q] = 0.;
+                  if (mixed) sR32[q] = 0.f;
+            }
+      }
+      for (int o = 16; o > 0; o >>= 1)
+            for (int k = 0; k < 3; k++) {
+                  lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+                  hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+            }
+      const double c[3] = {0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2])};
+      if (lane < 3) {
+            box[warp * 6 + lane] = c[lane];
+            box[warp * 6 + 3 + lane] = 0.5 * (hi[lane] - lo[lane]);
+      }
+      if (!mixed) return;
+      float *tile = s32 + (size_t)warp * 4 * T;
+#pragma unroll
+      for (int u = 0; u < T / 32; u++) {
+            const int j = lane + 32 * u;
+            if (base + j < n) {
+                  tile[j] = (float)(d[u].x - c[0]);
+                  tile[T + j] = (float)(d[u].y - c[1]);
+                  tile[2 * T + j] = (float)(d[u].z - c[2]);
+                  tile[3 * T + j] = (float)d[u].w;
+            } else {
+                  tile[j] = 1e18f;
+                  tile[T + j] = 1e18f;
+                  tile[2 * T + j] = 1e18f;
+                  tile[3 * T + j] = 0.f;
+            }
       }
 }
-
 
 // FP64 pair sum of one tile against this thread's two targets.
 template <int SOFT>
@@ -704,16 +714,32 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
       if (!tiled) {
             NCG_TRY(compact_existing(bv.ex, largest_id, &n, st));
       } else if (nslots > 0) {
-            // compaction, bounding box and radius range behind one synchronisation
+            // compaction, bounding box, Morton order and the tile data sized for
+            // every slot, the count of existing bodies read in the kernels; the
+            // count and the radius range come back to the host (for the pair
+            // kernel's grid and instance) while the GPU sorts and packs
             NCG_TRY(compact_existing_dev(bv.ex, largest_id, st));
             const int nbb = min(256, (nslots + RB - 1) / RB);
             k_bbox_part<<<nbb, RB, 0, st>>>(bv, c.cidx, c.n_dev, c.red);
             NCG_LAUNCHED();
             k_bbox_final<<<1, 256, 0, st>>>(c.red, nbb);
             NCG_LAUNCHED();
-            NCG_CK(cudaMemcpyAsync(&n, c.n_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
-            NCG_CK(cudaMemcpyAsync(rr, c.red + 6, sizeof rr, cudaMemcpyDeviceToHost, st));
+            const int ntub = (nslots + T - 1) / T;
+            k_morton<<<(nslots + 255) / 256, 256, 0, st>>>(bv, c.cidx, c.n_dev, nslots, c.red, c.keys, c.vals);
+            NCG_LAUNCHED();
+            NCG_TRY(radix_sort_pairs(c.keys, c.vals, nslots, 30, st));
+            k_tile_prep<<<(ntub * 32 + 255) / 256, 256, 0, st>>>(bv, c.vals, c.n_dev, ntub, P.par_softening_parameter,
+                                                                 mode == NCGPU_GRAVITY_MIXED, (D4 *)c.src64, c.srcR,
+                                                                 c.tilebox, (float *)c.src32, c.srcR32);
+            NCG_LAUNCHED();
+            k_count_beside<<<1, 1, 0, st>>>(c.n_dev, c.red);
+            NCG_LAUNCHED();
+            double h3[3];  // radius range and count: one copy
+            NCG_CK(cudaMemcpyAsync(h3, c.red + 6, sizeof h3, cudaMemcpyDeviceToHost, st));
             NCG_CK(cudaStreamSynchronize(st));
+            rr[0] = h3[0];
+            rr[1] = h3[1];
+            n = (int)h3[2];
       }
       const int central = P.par_central_mass_bool;
       const double G = P.par_G;
@@ -756,19 +782,8 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
       }
       if (mode != NCGPU_GRAVITY_FP64 && mode != NCGPU_GRAVITY_MIXED) return NCGPU_E_ARG;
 
-      // Morton ordering of the existing bodies (bounding box from above)
-      k_morton<<<(n + 255) / 256, 256, 0, st>>>(cv, c.cidx, n, c.red, c.keys, c.vals);
-      NCG_LAUNCHED();
-      NCG_TRY(radix_sort_pairs(c.keys, c.vals, n, 30, st));
+      // (the Morton order and the tile data were made above, before the count came back)
       D4 *s64 = (D4 *)c.src64;
-      k_gather_sorted<<<(npad + 255) / 256, 256, 0, st>>>(cv, c.vals, n, npad, sp, s64, c.srcR);
-      NCG_LAUNCHED();
-      k_tilebox<<<(ntiles * 32 + 255) / 256, 256, 0, st>>>(s64, n, ntiles, c.tilebox);
-      NCG_LAUNCHED();
-      if (mode == NCGPU_GRAVITY_MIXED) {
-            k_pack32<<<(npad + 255) / 256, 256, 0, st>>>(s64, c.srcR, c.tilebox, n, npad, (float *)c.src32, c.srcR32);
-            NCG_LAUNCHED();
-      }
       // softening: general (eps = sp (R_i + R_j)) unless sp == 0; the kernel
       // takes its uniform-eps^2 path itself when all radii are equal
       const int sm = soft ? 2 : 0;

@@ -139,6 +139,74 @@ __global__ void k_radix_scatter(const uint32_t *__restrict__ kin, const int *__r
       }
 }
 
+// k_radix_scatter for a few blocks (n up to 64 RB keys): each block finds its
+// digits' global offsets from the unscanned histograms itself (the totals of
+// every digit over all blocks, scanned across the block's 256 threads, plus the
+// counts of the blocks before it), which saves the histogram scan's launches.
+__global__ void k_radix_scatter_inline(const uint32_t *__restrict__ kin, const int *__restrict__ vin,
+                                       uint32_t *__restrict__ kout, int *__restrict__ vout, int n, int shift,
+                                       const int *__restrict__ hist, int nblocks)
+{
+      __shared__ int run[RADIX];
+      __shared__ int gofs[RADIX];
+      __shared__ int wc[RT / 32][RADIX];
+      __shared__ int wsum[RT / 32];
+      int t = threadIdx.x, lane = t & 31, w = t >> 5;
+      int tot = 0, pre = 0;
+      for (int b = 0; b < nblocks; b++) {
+            const int v = hist[t * nblocks + b];
+            tot += v;
+            if (b < (int)blockIdx.x) pre += v;
+      }
+      int x = tot;  // exclusive scan of the digit totals over the 256 digits
+      for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += u;
+      }
+      if (lane == 31) wsum[w] = x;
+      __syncthreads();
+      int before = 0;
+      for (int q = 0; q < w; q++) before += wsum[q];
+      gofs[t] = before + x - tot + pre;
+      run[t] = 0;
+      int base = blockIdx.x * RB;
+      for (int r = 0; r < RK; r++) {
+            for (int q = 0; q < RT / 32; q++) wc[q][t] = 0;
+            __syncthreads();
+            int i = base + r * RT + t;
+            uint32_t key = 0;
+            int val = 0;
+            int d = RADIX;  // sentinel: no key
+            if (i < n) {
+                  key = kin[i];
+                  val = vin[i];
+                  d = (key >> shift) & 0xffu;
+            }
+            unsigned peers = __match_any_sync(0xffffffffu, d);
+            int rk = __popc(peers & ((1u << lane) - 1u));
+            int leader = __ffs(peers) - 1;
+            if (lane == leader && d < RADIX) wc[w][d] = __popc(peers);
+            __syncthreads();
+            {
+                  int acc = run[t];
+#pragma unroll
+                  for (int q = 0; q < RT / 32; q++) {
+                        int c = wc[q][t];
+                        wc[q][t] = acc;
+                        acc += c;
+                  }
+                  run[t] = acc;
+            }
+            __syncthreads();
+            if (d < RADIX) {
+                  int dst = gofs[d] + wc[w][d] + rk;
+                  kout[dst] = key;
+                  vout[dst] = val;
+            }
+            __syncthreads();
+      }
+}
+
 // Exclusive scan of one 1024-element block; block total to sums[b].
 __global__ void k_block_scan(const int *__restrict__ in, int n, int *__restrict__ out, int *__restrict__ sums)
 {
@@ -246,9 +314,14 @@ int radix_sort_pairs(uint32_t *keys, int *vals, int n, int bits, cudaStream_t st
             int shift = 8 * p;
             k_radix_hist<<<nb, RT, 0, st>>>(ka, n, shift, c.hist, nb);
             NCG_LAUNCHED();
-            NCG_TRY(scan_exclusive(c.hist, c.hist, (int)need, c.cnt, st));
-            k_radix_scatter<<<nb, RT, 0, st>>>(ka, va, kb, vb, n, shift, c.hist, nb);
-            NCG_LAUNCHED();
+            if (nb <= 64) {  // two launches a pass: the scatter scans the histograms itself
+                  k_radix_scatter_inline<<<nb, RT, 0, st>>>(ka, va, kb, vb, n, shift, c.hist, nb);
+                  NCG_LAUNCHED();
+            } else {
+                  NCG_TRY(scan_exclusive(c.hist, c.hist, (int)need, c.cnt, st));
+                  k_radix_scatter<<<nb, RT, 0, st>>>(ka, va, kb, vb, n, shift, c.hist, nb);
+                  NCG_LAUNCHED();
+            }
             uint32_t *tk = ka; ka = kb; kb = tk;
             int *tv = va; va = vb; vb = tv;
       }
