@@ -40,12 +40,12 @@ N_BODIES = 65536
 SOFTENING = 0.5
 FLOP_PER_INTERACTION = 20  # 3 sub, 3 FMA (r^2+eps^2), rsqrt (2), 3 mul, 3 FMA accumulate
 # DRAM bytes (read + write) of one k_grav_tiled<mixed> launch at N=65,536, from one ncu capture of
-# this script's gravity workload (profiles/k_grav_tiled_mixed_n65536.txt): 3.21 MB read + 103.57 MB written
+# this script's gravity workload (profiles/k_grav_tiled_mixed_n65536.txt): 3.77 MB read + 105.56 MB written
 # (the written bytes are the per-chunk partial sums: 103 source chunks x 3 x 65,536 doubles).
-MIXED_DRAM_BYTES = 106.78e6
-# DRAM bytes of one mesh step's two main kernels (k_mesh_write + k_mesh_grav) captured at N=262,144
-# (profiles/k_mesh_write_grav_n262144.txt: 44.0 MB + 29.6 MB), scaled by the bodies to N=1,048,576.
-MESH_DRAM_BYTES_262K = 73.6e6
+MIXED_DRAM_BYTES = 109.33e6
+# DRAM bytes of one mesh step's two main kernels (k_mesh_write + k_mesh_grav_fast) captured at N=262,144
+# (profiles/mesh_step_kernels_n262144.txt: 34.1 MB + 29.3 MB), scaled by the bodies to N=1,048,576.
+MESH_DRAM_BYTES_262K = 63.4e6
 METRIC = "Pair-interactions/s mixed vs FP64 (rel err<1e-6); mesh collision steps/s at N=1M"
 WORKLOAD = ("gravity-only single-step accelerations, N=65,536 disk (a~U[0.8,1.2], e~Rayleigh 0.01, "
             "i~Rayleigh 0.005), masses log-uniform [1e-9,1e-6], R=1e-5, softening 0.5*(R_k+R_p)")
@@ -777,7 +777,7 @@ def main(argv=None):
                 "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
                              "algorithmic_bytes_per_step": alg,
                              "traffic": MESH_DRAM_BYTES_262K * a.mesh_n / 262144,
-                             "traffic_note": "k_mesh_write + k_mesh_grav DRAM bytes from an ncu capture at N=262,144, "
+                             "traffic_note": "k_mesh_write + k_mesh_grav_fast DRAM bytes from an ncu capture at N=262,144, "
                                              "scaled by the body count",
                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
                 "cpu_baseline": mesh_cpu_reference() if (rank == 0 and ws == 1 and not a.no_cpu_baseline
