@@ -557,6 +557,35 @@ def bench_adjoint(lib, api, torch):
     return out
 
 
+# Algorithmic bytes per body of the mesh step's O(N) kernels (reads + writes of the arrays each one must touch):
+# kick / drift: exists 4 + acceleration or position 24 + velocity 24 read, 24 written; the records: the cell
+# order 4 + the fields gathered (7 doubles + exists + did; 5 doubles + exists) read, a 64-byte record written;
+# end of step: exists + position read; cell keys: exists + radius + position read, key + value + cell written;
+# a radix pass: key + value read and written (histogram: the key read).
+MESH_KERNEL_BYTES = {"k_kick": 76, "k_drift": 76, "k_mesh_records": 132, "k_grav_records": 112, "k_eot_flag": 28,
+                     "k_mesh_keys": 48, "k_radix_scatter": 16, "k_radix_hist": 4}
+
+
+def mesh_kernel_times(prof, n, calls):
+    """Per-kernel device time of a profiled mesh run, per call (the steps, the warm-up and the half kick),
+    with the algorithmic bytes per second of the O(N) kernels at n bodies."""
+    tot = {}
+    for e in prof.events():
+        if e.device_type.name != "CUDA":
+            continue
+        k = e.name.replace("(anonymous namespace)::", "").replace("ncg::", "").replace("void ", "").split("(")[0]
+        c = tot.setdefault(k, [0, 0.0])
+        c[0] += 1
+        c[1] += e.device_time_total
+    out = {}
+    for k, (cnt, us) in sorted(tot.items(), key=lambda kv: -kv[1][1]):
+        d = {"launches": cnt, "us_per_launch": us / cnt}
+        if k in MESH_KERNEL_BYTES:
+            d["alg_gb_per_s"] = MESH_KERNEL_BYTES[k] * n / (us / cnt * 1e-6) / 1e9
+        out[k] = d
+    return out
+
+
 def mesh_cpu_reference(nsteps=3):
     """The reference's mesh() + mesh gravity loop (oracle/_ref/mesh_merge_1m,
     1 thread, 8.6 GB hash table) for a few steps of the same disk."""
@@ -599,6 +628,9 @@ def main(argv=None):
     ap.add_argument("--mesh-steps", type=int, default=MESH_STEPS)
     ap.add_argument("--mesh-only", action="store_true",
                     help="profiling aid: only the mesh section (fast mode), its own JSON line")
+    ap.add_argument("--kernel-times", action="store_true",
+                    help="with --mesh-only: per-kernel device times of the timed steps (CUPTI tracing through "
+                         "torch.profiler) and each one's algorithmic bytes per second")
     a = ap.parse_args(argv)
     a.warmup = max(a.warmup, 3)
     ws, rank, local = dist_info()
@@ -619,7 +651,13 @@ def main(argv=None):
     lib = api.load()
 
     if a.mesh_only:
-        r = bench_mesh(lib, api, torch, api.GRAVITY_MIXED, a.mesh_steps, a.warmup, a.mesh_n, a.mesh_cells)
+        if a.kernel_times:
+            from torch.profiler import profile, ProfilerActivity
+            with profile(activities=[ProfilerActivity.CUDA]) as prof:
+                r = bench_mesh(lib, api, torch, api.GRAVITY_MIXED, a.mesh_steps, a.warmup, a.mesh_n, a.mesh_cells)
+            r["kernel_times"] = mesh_kernel_times(prof, a.mesh_n, a.mesh_steps + a.warmup + 1)
+        else:
+            r = bench_mesh(lib, api, torch, api.GRAVITY_MIXED, a.mesh_steps, a.warmup, a.mesh_n, a.mesh_cells)
         if rank == 0:
             print(json.dumps({"metric": f"mesh collision steps/s at N={a.mesh_n} (fast mode)",
                               "value": r["steps_per_s"], "unit": "steps/s", "n_gpus": ws, "steps": a.mesh_steps,

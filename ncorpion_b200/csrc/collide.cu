@@ -267,10 +267,9 @@ int collide_brute_state()
             NCG_CK(cudaMemsetAsync(c.scal + S_NEV, 0, sizeof(int), st));
             return sync_scalars();
       }
-      int zero[3] = {0, 0, 0};
       // S_NHITS, S_NEV, S_NDIRTY = 0
-      NCG_CK(cudaMemcpyAsync(c.scal + S_NHITS, zero, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
-      NCG_CK(cudaMemcpyAsync(c.scal + S_NDIRTY, zero, sizeof(int), cudaMemcpyHostToDevice, st));
+      NCG_CK(cudaMemsetAsync(c.scal + S_NHITS, 0, 2 * sizeof(int), st));
+      NCG_CK(cudaMemsetAsync(c.scal + S_NDIRTY, 0, sizeof(int), st));
       DevState S = dev_state();
       const int nt = (lid + BT) / BT;
       dim3 grid(nt, nt);

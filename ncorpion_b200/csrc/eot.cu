@@ -29,17 +29,31 @@ __global__ void k_eot_flag(const DevState S, int lid, const double *__restrict__
 {
       int j = blockIdx.x * blockDim.x + threadIdx.x;
       int f = 0;
+      bool stays = false;
       if (j <= lid && S.ex[j]) {
             double XX = central ? cm[0] : 0., YY = central ? cm[1] : 0., ZZ = central ? cm[2] : 0.;
             double DX = DSUB(S.x[j], XX), DY = DSUB(S.y[j], YY), DZ = DSUB(S.z[j], ZZ);
             double r2 = DADD(DADD(DMUL(DX, DX), DMUL(DY, DY)), DMUL(DZ, DZ));
             if (r2 < DMUL(dis, dis) && central) f = 1;
             else if (r2 > DMUL(high, high)) f = 2;
-            else atomicAdd(S.scal + S_HM, 1);
+            else stays = true;
       }
       if (j <= lid) flag[j] = f;
-      unsigned m = __ballot_sync(0xffffffffu, f != 0);
-      if ((threadIdx.x & 31) == 0 && m) atomicAdd(S.scal + S_NFLAG, __popc(m));
+      // counts summed per block: one atomic on each counter per block instead of
+      // one per body (atomics on one address are serialised at the L2)
+      __shared__ int cnt[2];
+      if (threadIdx.x < 2) cnt[threadIdx.x] = 0;
+      __syncthreads();
+      const unsigned m = __ballot_sync(0xffffffffu, f != 0), ms = __ballot_sync(0xffffffffu, stays);
+      if ((threadIdx.x & 31) == 0) {
+            if (m) atomicAdd(&cnt[0], __popc(m));
+            if (ms) atomicAdd(&cnt[1], __popc(ms));
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+            if (cnt[0]) atomicAdd(S.scal + S_NFLAG, cnt[0]);
+            if (cnt[1]) atomicAdd(S.scal + S_HM, cnt[1]);
+      }
 }
 
 // The flagged bodies, in slot order (list from an order-preserving compaction).
@@ -236,8 +250,7 @@ int eot_state(int *hm_out)
       const int lid = c.largest_id;
       c.eot_lid = lid;  // largest_id before tidy_up, which end_of_timestep prints
       DevState S = dev_state();
-      int zero[2] = {0, 0};
-      NCG_CK(cudaMemcpyAsync(c.scal + S_HM, zero, 2 * sizeof(int), cudaMemcpyHostToDevice, st));
+      NCG_CK(cudaMemsetAsync(c.scal + S_HM, 0, 2 * sizeof(int), st));  // HM, NFLAG
       const int nb = lid >= 0 ? (lid + 256) / 256 : 1;
       int *flag = c.exs;
       k_eot_flag<<<nb, 256, 0, st>>>(S, lid, c.cm, P.par_central_mass_bool, P.par_disruption_threshold,

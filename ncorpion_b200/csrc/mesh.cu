@@ -851,10 +851,10 @@ int mesh_pass(double gam, int test)
       NCG_TRY(mesh_reset_state());
       const int lid = c.largest_id;
       const int n = lid + 1;
-      int zero[S_COUNT] = {0};
-      NCG_CK(cudaMemcpyAsync(c.scal + S_NHITS, zero, 2 * sizeof(int), cudaMemcpyHostToDevice, st));  // NHITS, NEV
-      NCG_CK(cudaMemcpyAsync(c.scal + S_NBIG, zero, 3 * sizeof(int), cudaMemcpyHostToDevice, st));   // NBIG, NDROP, NINS
-      NCG_CK(cudaMemcpyAsync(c.scal + S_NXPAIRS, zero, 3 * sizeof(int), cudaMemcpyHostToDevice, st));  // NXPAIRS, NSKIP, NFEV
+      // counters of the pass cleared on the device (no host copy on the step's path)
+      NCG_CK(cudaMemsetAsync(c.scal + S_NHITS, 0, 2 * sizeof(int), st));    // NHITS, NEV
+      NCG_CK(cudaMemsetAsync(c.scal + S_NBIG, 0, 3 * sizeof(int), st));     // NBIG, NDROP, NINS
+      NCG_CK(cudaMemsetAsync(c.scal + S_NXPAIRS, 0, 3 * sizeof(int), st));  // NXPAIRS, NSKIP, NFEV
       c.n_cand = c.n_pairs = 0;
       c.total_neighbours = 0;
       c.how_many_small = c.how_many_big = 0;
