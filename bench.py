@@ -309,16 +309,65 @@ def bench_output(lib, api, torch, reps=5, cpu=True):
         t0 = time.perf_counter()
         one()
         times.append(time.perf_counter() - t0)
-    lib.ncgpu_host_unregister(api.ptr(text))
-    api.finalize()
     text_bytes = int(sum(lens))
     nvals = int(np.count_nonzero(text[:text_bytes] == ord(" ")))
+
+    # the elliptic files (write_elliptic_bool, mass and radius with them): the
+    # device's cart2ell, the C library's atan2 on host threads, the device's text
+    nb_cap = n + n // 20 + 1
+    yx, F = np.empty(2 * nb_cap), np.empty(nb_cap)
+    for a_ in (yx, F):
+        api.check(lib.ncgpu_host_register(api.ptr(a_), a_.nbytes), "register")
+    hidx, hrec, alk = np.empty(nb_cap, np.int32), np.empty((nb_cap, 8)), np.zeros((nb_cap, 6))
+    nbod, nhost = C.c_int(0), C.c_int(0)
+    t_atan2 = []
+
+    def one_ell():
+        api.snapshot_begin()
+        api.set_timestep(MESH_DT / -2.0)
+        api.three_largest()
+        api.mesh(gam, False)
+        api.kick()
+        api.check(lib.ncgpu_output_stats(api.ptr(stats), api.ptr(idx), api.ptr(cmo), api.ptr(two)), "stats")
+        api.check(lib.ncgpu_elliptic_begin(C.c_double(1.0 * cmo[6]), api.ptr(yx), yx.size, C.byref(nbod),
+                                           api.ptr(hidx), api.ptr(hrec), nb_cap, C.byref(nhost)), "elliptic begin")
+        t0 = time.perf_counter()
+        api.check(lib.ncgpu_host_atan2(api.ptr(yx), api.ptr(F), nbod.value), "atan2")
+        t_atan2.append(time.perf_counter() - t0)
+        # listed bodies (hyperbolic, cart2ell's warning, NaNs) would go through the
+        # caller's cart2ell here; this disk has none (checked below)
+        api.check(lib.ncgpu_format_elliptic(api.ptr(F), api.ptr(alk), nhost.value, 1, api.ptr(text), cap, lens),
+                  "elliptic text")
+        api.snapshot_end()
+        api.mesh_reset()
+        api.set_timestep(MESH_DT)
+
+    one_ell()
+    times_ell = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        one_ell()
+        times_ell.append(time.perf_counter() - t0)
+    ell_bytes = int(sum(lens))
+    for a_ in (text, yx, F):
+        lib.ncgpu_host_unregister(api.ptr(a_))
+    api.finalize()
     ms = 1e3 * float(np.median(times))
+    ms_ell = 1e3 * float(np.median(times_ell))
     out = {"metric": "output step of the mesh driver at N=1,048,576 (cartesian files)", "ms": ms, "values": nvals,
            "text_bytes": text_bytes, "values_per_s": nvals / (ms * 1e-3),
            "note": "snapshot, half backward kick (three largest, neighbours, mesh gravity), device formatting, "
                    "statistics, the text copied into a host buffer through the C ABI; host wall clock, median of "
-                   "%d" % reps}
+                   "%d" % reps,
+           "elliptic": {"ms": ms_ell, "bodies": nbod.value, "listed_bodies": nhost.value, "text_bytes": ell_bytes,
+                        "host_atan2_ms": 1e3 * float(np.median(t_atan2)),
+                        "note": "the same output step with the elliptic files (a, lambda, k, h, q, p, mass, "
+                                "radius): cart2ell on the device, atan2 by the C library on host threads, "
+                                "device formatting; host wall clock, median of %d" % reps}}
+    if nhost.value:
+        out["elliptic"]["ms"] = None
+        out["elliptic"]["note"] += "; not timed: bodies listed for the caller's cart2ell"
     if cpu:
         try:
             import tempfile
@@ -335,6 +384,24 @@ def bench_output(lib, api, torch, reps=5, cpu=True):
             out["cpu_baseline"] = {"value": dt * 1e3, "unit": "ms", "cores": 1, "kind": "port",
                                    "sample": f'fprintf "%.14lf " of {len(vals)} values (display()\'s formatting '
                                              "alone, without the host copy's backward kick), one core"}
+            # the elliptic files: cart2ell of every body, then the same formatting
+            port.orc_cart2ell_all.restype = Cc.c_long
+            port.orc_cart2ell_all.argtypes = [Cc.c_int, Cc.c_void_p, Cc.c_void_p, Cc.c_void_p, Cc.c_double,
+                                              Cc.c_void_p, Cc.c_double, Cc.c_void_p, Cc.c_long]
+            pe = mesh_params(api.GRAVITY_MIXED)
+            ell = np.empty((8, n))
+            t0 = time.perf_counter()
+            port.orc_cart2ell_all(n - 1, b.ctypes.data, ex.ctypes.data, cm.ctypes.data, 1.0, Cc.byref(pe), 0.0,
+                                  ell.ctypes.data, 6 * n)
+            t_c2e = time.perf_counter() - t0
+            ell[6], ell[7] = b[:, 6], b[:, 7]
+            t0 = time.perf_counter()
+            port.orc_fprintf_values(ell.ctypes.data, ell.size, os.path.join(d, "ell.txt").encode())
+            t_pr = time.perf_counter() - t0
+            out["elliptic"]["cpu_baseline"] = {
+                "value": (t_c2e + t_pr) * 1e3, "unit": "ms", "cores": 1, "kind": "port",
+                "cart2ell_ms": t_c2e * 1e3,
+                "sample": f'cart2ell of {n} bodies and fprintf "%.14lf " of their {ell.size} values, one core'}
         except Exception as e:  # noqa: BLE001
             out["cpu_baseline"] = {"value": None, "unit": "ms", "cores": 1, "kind": "port", "sample": f"unavailable: {e}"}
     return out

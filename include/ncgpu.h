@@ -309,6 +309,40 @@ int ncgpu_snapshot_end(void);
    (the caller prints that output itself). */
 int ncgpu_format_cartesian(char *text, unsigned long cap, unsigned long *lens);
 unsigned long ncgpu_format_cartesian_cap(void);
+/* The elliptic files of this output (display() with write_elliptic_bool,
+   src/display.c:340-347: cart2ell, src/structure.c:172-284, of every existing
+   body in slot order with mu + G*m), in two calls around the caller's libm.
+   ncgpu_elliptic_begin computes on the device, in the reference's operation
+   order, a, k, h, q, p and the two arguments of the mean longitude's atan2
+   (src/structure.c:268-271): yx[2j], yx[2j+1] = sinF, cosF of the j-th
+   existing body (0, 0 where the longitude is 0: R or V2 zero), yx_cap >= 2 *
+   *n_bodies.  Bodies that cart2ell takes out of that branch -- hyperbolic
+   (src/structure.c:274-279), printing its (k, h) warning (src/structure.c:
+   253-255) or giving a NaN -- are listed: host_idx their slots (ascending),
+   host_rec their records; the caller converts them with its cart2ell, which
+   prints the warnings as display() does.  NCGPU_E_CAPACITY when *n_host >
+   host_cap.  mu is display()'s mu (G times the central mass or M_unit); the
+   central body, J2_bool, J2 (the one in force), R_unit and G come from the
+   state and the parameters.
+   ncgpu_format_elliptic takes F[j] = atan2(yx[2j], yx[2j+1]) for every body
+   (entries of listed bodies are ignored) and host_alkhqp[6k .. 6k+5], cart2ell's
+   alkhqp of listed body k, and returns the texts of a, lambda, k, h, q, p (then
+   mass and radius when mass_radius) like ncgpu_format_cartesian, lens[6] or
+   lens[8], with the same capacity bound and NCGPU_E_UNSUPPORTED rule.  After it,
+   ncgpu_elliptic_values copies the elements and the bodies' masses and radii
+   (8 blocks of *n_bodies doubles, cap >= 8 * *n_bodies) for a caller that
+   prints them itself.  No state change may come between the calls. */
+int ncgpu_elliptic_begin(double mu, double *yx, unsigned long yx_cap, int *n_bodies, int *host_idx,
+                         struct ncgpu_body *host_rec, int host_cap, int *n_host);
+int ncgpu_format_elliptic(const double *F, const double *host_alkhqp, int n_host, int mass_radius, char *text,
+                          unsigned long cap, unsigned long *lens);
+int ncgpu_elliptic_values(double *values, unsigned long cap);
+/* F[j] = atan2(yx[2j], yx[2j+1]) for j < n with the C library's atan2 (the
+   function cart2ell calls; glibc's is not correctly rounded in every case, so
+   the files' bytes need that very function), on up to 16 host threads: the
+   loop between ncgpu_elliptic_begin and ncgpu_format_elliptic, for callers
+   that have none of their own. */
+int ncgpu_host_atan2(const double *yx, double *F, long n);
 /* display()'s statistics of the current state (src/display.c:303-379):
    stats[0] the total mass of the bodies summed in slot order, stats[1..2] and
    idx[0..1] the masses M1, M2 and slots of the two most massive bodies as its

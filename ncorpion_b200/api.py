@@ -129,6 +129,10 @@ EXPORTS = {
     "ncgpu_format_cartesian": (C.c_int, [P, C.c_ulong, P]),
     "ncgpu_format_cartesian_cap": (C.c_ulong, []),
     "ncgpu_output_stats": (C.c_int, [P, P, P, P]),
+    "ncgpu_elliptic_begin": (C.c_int, [C.c_double, P, C.c_ulong, P, P, P, C.c_int, P]),
+    "ncgpu_format_elliptic": (C.c_int, [P, P, C.c_int, C.c_int, P, C.c_ulong, P]),
+    "ncgpu_elliptic_values": (C.c_int, [P, C.c_ulong]),
+    "ncgpu_host_atan2": (C.c_int, [P, P, C.c_long]),
     "ncgpu_set_sideral_omega": (C.c_int, [C.c_double]),
     "ncgpu_probe_pow_third": (C.c_int, [P, P, C.c_int]),
     "ncgpu_probe_div": (C.c_int, [P, P, P, C.c_int]),
@@ -433,6 +437,60 @@ def format_cartesian() -> list:
     return out
 
 
+def elliptic_begin(mu: float):
+    """cart2ell on the device up to the mean longitude's atan2: returns
+    (yx (n, 2): the atan2 arguments of the existing bodies in slot order,
+    host_idx: the slots of the bodies the caller converts itself, host_rec
+    (k, 8): their records)."""
+    lib = load()
+    lid = C.c_int(0)
+    check(lib.ncgpu_get_largest_id(C.byref(lid), None), "ncgpu_get_largest_id")
+    n_slots = max(1, lid.value + 1)
+    yx = np.zeros((n_slots, 2))
+    n_b, n_h = C.c_int(0), C.c_int(0)
+    idx = np.zeros(n_slots, np.int32)
+    rec = np.zeros((n_slots, 8))
+    check(lib.ncgpu_elliptic_begin(C.c_double(mu), ptr(yx), 2 * n_slots, C.byref(n_b), ptr(idx), ptr(rec), n_slots,
+                                   C.byref(n_h)), "ncgpu_elliptic_begin")
+    return yx[:n_b.value].copy(), idx[:n_h.value].copy(), rec[:n_h.value].copy()
+
+
+def host_atan2(yx: np.ndarray) -> np.ndarray:
+    """atan2(y, x) of each row with the C library's atan2 (ncgpu_host_atan2)."""
+    yx = np.ascontiguousarray(yx, np.float64)
+    F = np.zeros(len(yx))
+    check(load().ncgpu_host_atan2(ptr(yx), ptr(F), len(yx)), "ncgpu_host_atan2")
+    return F
+
+
+def format_elliptic(F, host_alkhqp, mass_radius: bool = False) -> list:
+    """The texts of a, lambda, k, h, q, p (then mass and radius) after
+    elliptic_begin, from F = atan2 of its arguments and the caller's elements
+    of the listed bodies ((k, 6))."""
+    lib = load()
+    F = np.ascontiguousarray(F, np.float64)
+    alk = np.ascontiguousarray(np.asarray(host_alkhqp, np.float64).reshape(-1, 6))
+    cap = lib.ncgpu_format_cartesian_cap()
+    buf = C.create_string_buffer(cap)
+    nf = 8 if mass_radius else 6
+    lens = (C.c_ulong * 8)()
+    check(lib.ncgpu_format_elliptic(ptr(F), ptr(alk), len(alk), int(mass_radius), buf, cap, lens),
+          "ncgpu_format_elliptic")
+    raw = buf.raw
+    out, pos = [], 0
+    for f in range(nf):
+        out.append(raw[pos:pos + lens[f]].decode())
+        pos += lens[f]
+    return out
+
+
+def elliptic_values(n: int) -> np.ndarray:
+    """(8, n): a, lambda, k, h, q, p, mass, radius of the last elliptic output."""
+    v = np.zeros((8, max(n, 1)))
+    check(load().ncgpu_elliptic_values(ptr(v), v.size), "ncgpu_elliptic_values")
+    return v.reshape(-1)[:8 * n].reshape(8, n)
+
+
 def output_stats():
     """(stats (total_mass, M1, M2), (i1, i2), cm (8), two bodies (2 x 8)) as display() computes them."""
     lib = load()
@@ -442,6 +500,13 @@ def output_stats():
     two = np.zeros((2, 8))
     check(lib.ncgpu_output_stats(ptr(stats), ptr(idx), ptr(cm), ptr(two)), "ncgpu_output_stats")
     return stats, idx, cm, two
+
+
+def get_j2() -> float:
+    """The J2 in force of the device state (0 without J2)."""
+    j = C.c_double(0.0)
+    check(load().ncgpu_get_j2(C.byref(j), None), "ncgpu_get_j2")
+    return j.value
 
 
 def get_sideral_omega() -> float:

@@ -291,6 +291,17 @@ struct Ctx {
       char *fmt_slots = nullptr, *fmt_text = nullptr;
       int *fmt_len = nullptr;
       size_t fmt_cap = 0;
+      // elliptic output (output.cu): per existing body a, lambda, k, h, q, p
+      // (6 blocks), the atan2 arguments (2), the caller's atan2 (1), the caller's
+      // elements of the bodies it converts itself (6 a body), a branch code
+      // a body and the list of those bodies
+      double *ell = nullptr;
+      size_t ell_cap = 0;          // bodies
+      unsigned char *ell_code = nullptr;
+      int *ell_list = nullptr;     // [0]: count, then compact indices
+      int ell_n = -1;              // bodies of the pending elliptic output (-1: none)
+      int ell_nhost = 0;
+      int ell_done = 0;            // lambda finished from the caller's atan2
       double *cm_acc = nullptr;    // 3 doubles
       double dt = 0.0;
 

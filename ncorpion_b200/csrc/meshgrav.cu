@@ -506,8 +506,10 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
 // of the cell-sorted bodies: a body walks 9 ranges.  The warp's bodies queue
 // their partners (record positions, per lane in shared memory) during the
 // walk; then the warp evaluates the queued pair terms 32 at a time, every lane
-// busy whatever the lengths of the bodies' lists, and each body adds its own
-// terms in its queue's order (deterministic).  The pair term is FP64 with one
+// busy whatever the lengths of the bodies' lists.  A round's terms of one body
+// sit in adjacent lanes: a segmented scan over the warp (five shuffle steps)
+// leaves each list's sum in its last lane, which the body adds to its own sums
+// (a fixed order: deterministic).  The pair term is FP64 with one
 // reciprocal square root (G m dx / D^3 = G m dx (1/D)^3); against the exact
 // mode, only its rounding and the order of the sum differ.
 constexpr int FGW = 4;   // warps per block
@@ -543,7 +545,6 @@ __global__ void __launch_bounds__(FGW * 32, 8) k_mesh_grav_fast(DevState S, MGAr
 {
       __shared__ int qb[FGW][32 * FGQ];
       __shared__ unsigned char owner[FGW][32 * FGQ];
-      __shared__ double tb[FGW][3][32];
       __shared__ int pre[FGW][32];
       const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       const int t = blockIdx.x * blockDim.x + threadIdx.x;  // cell order
@@ -590,26 +591,42 @@ __global__ void __launch_bounds__(FGW * 32, 8) k_mesh_grav_fast(DevState S, MGAr
             __syncwarp();
             for (int f0 = 0; f0 < total; f0 += 32) {
                   const int fi = f0 + lane;
+                  double tx = 0., ty = 0., tz = 0.;
+                  int a = lane;  // the lane where this entry's list starts in the round
                   if (fi < total) {
                         const int o = owner[w][fi];
                         const int q = qb[w][o * FGQ + fi - pre[w][o]];
                         const double2 *ow = reinterpret_cast<const double2 *>(grec + t0 + o);
                         const double2 oxy = ow[0], oz = ow[1];
-                        double tx, ty, tz;
                         term_fast(oxy.x, oxy.y, oz.x, A.soft ? grec[t0 + o].R : 0., grec, q, A, tx, ty, tz);
-                        tb[w][0][lane] = tx;
-                        tb[w][1][lane] = ty;
-                        tb[w][2][lane] = tz;
+                        a = max(pre[w][o] - f0, 0);
                   }
-                  __syncwarp();
+                  // segmented inclusive scan over the round (the lists are contiguous in
+                  // lane order): the last lane of a list then holds the list's sum
+#pragma unroll
+                  for (int dl = 1; dl < 32; dl <<= 1) {
+                        const double ux = __shfl_up_sync(0xffffffffu, tx, dl);
+                        const double uy = __shfl_up_sync(0xffffffffu, ty, dl);
+                        const double uz = __shfl_up_sync(0xffffffffu, tz, dl);
+                        if (lane - dl >= a) {
+                              tx += ux;
+                              ty += uy;
+                              tz += uz;
+                        }
+                  }
+                  // each body takes its list's sum of this round from the list's last lane
                   const int i0 = max(mine, f0), i1 = min(mine + cnt, f0 + 32);
-                  for (int i = i0; i < i1; ++i) {
-                        a_x += tb[w][0][i - f0];
-                        a_y += tb[w][1][i - f0];
-                        a_z += tb[w][2][i - f0];
+                  const int src = i1 > i0 ? i1 - 1 - f0 : lane;
+                  const double sx = __shfl_sync(0xffffffffu, tx, src);
+                  const double sy = __shfl_sync(0xffffffffu, ty, src);
+                  const double sz = __shfl_sync(0xffffffffu, tz, src);
+                  if (i1 > i0) {
+                        a_x += sx;
+                        a_y += sy;
+                        a_z += sz;
                   }
-                  __syncwarp();
             }
+            __syncwarp();
             skip += FGQ;
       }
       if (walk || (act && me.ex && b > 2)) {

@@ -19,7 +19,13 @@
 // fits a 128-bit integer, the power of two is a shift, and the rounding of a
 // right shift is exact integer arithmetic.  Values whose |x| 10^14 reaches 2^127
 // (|x| > 1.7e24) are not formatted (NCGPU_E_UNSUPPORTED; the caller prints them).
+#include <algorithm>
+#include <cmath>
+#include <thread>
+#include <vector>
+
 #include "common.cuh"
+#include "physics.cuh"
 
 namespace ncg {
 
@@ -86,35 +92,56 @@ __device__ int fmt_fixed14(double v, char *out)
       return k;
 }
 
-// Value j of file f (0..5: x y z vx vy vz with the central body first when
-// `central`; 6, 7: mass and radius of the bodies only).
-__device__ __forceinline__ double out_value(const BodyView &S, const double *cm, const int *cidx, int central, int f,
-                                            int j)
-{
-      const int c = f < 6 ? central : 0;
-      if (j < c) return cm[f];
-      const long s = (long)cidx[j - c] * S.stride;
-      const double *a[8] = {S.x, S.y, S.z, S.vx, S.vy, S.vz, S.m, S.R};
-      return a[f][s];
-}
+// The values of the cartesian files, value i of the concatenation: files 0..5
+// (x y z vx vy vz, the central body first when `central`), then 6, 7 (mass and
+// radius of the bodies only).
+struct CartValues {
+      BodyView S;
+      const double *cm;
+      const int *cidx;
+      int n, central;
+      __device__ __forceinline__ double operator()(long i) const
+      {
+            const int per = n + central;
+            int f, j;
+            if (i < 6L * per) {
+                  f = (int)(i / per);
+                  j = (int)(i % per);
+            } else {
+                  f = 6 + (int)((i - 6L * per) / n);
+                  j = (int)((i - 6L * per) % n);
+            }
+            const int c = f < 6 ? central : 0;
+            if (j < c) return cm[f];
+            const long s = (long)cidx[j - c] * S.stride;
+            const double *a[8] = {S.x, S.y, S.z, S.vx, S.vy, S.vz, S.m, S.R};
+            return a[f][s];
+      }
+};
+
+// The values of the elliptic files: a, lambda, k, h, q, p of the bodies (six
+// blocks of n), then their masses and radii.
+struct EllValues {
+      BodyView S;
+      const double *ell;  // six blocks, `stride` doubles apart
+      const int *cidx;
+      int n;
+      long stride;
+      __device__ __forceinline__ double operator()(long i) const
+      {
+            const int f = (int)(i / n), j = (int)(i % n);
+            if (f < 6) return ell[f * stride + j];
+            return (f == 6 ? S.m : S.R)[(long)cidx[j] * S.stride];
+      }
+};
 
 // One thread per value: formatted into its slot, the length into len.
-__global__ void k_fmt_values(BodyView S, const double *__restrict__ cm, const int *__restrict__ cidx, int n,
-                             int central, char *__restrict__ slots, int *__restrict__ len, unsigned *err)
+template <class Values>
+__global__ void k_fmt_values(Values val, long total, char *__restrict__ slots, int *__restrict__ len, unsigned *err)
 {
       const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-      const int per = n + central;  // values in files 0..5
-      const long total = 6L * per + 2L * n;
       if (i >= total) return;
-      int f, j;
-      if (i < 6L * per) {
-            f = (int)(i / per);
-            j = (int)(i % per);
-      } else {
-            f = 6 + (int)((i - 6L * per) / n);
-            j = (int)((i - 6L * per) % n);
-      }
-      const int L = fmt_fixed14(out_value(S, cm, cidx, central, f, j), slots + (size_t)i * SLOT);
+      const int L = fmt_fixed14(val(i), slots + (size_t)i * SLOT);
       if (L < 0) atomicOr(err, ERR_INTERNAL);
       len[i] = L < 0 ? 0 : L;
 }
@@ -175,11 +202,176 @@ __global__ void k_gather_mass(BodyView S, const int *__restrict__ cidx, int n, d
       if (q < n) m[q] = S.m[(long)cidx[q] * S.stride];
 }
 
+__global__ void k_gather_radius(BodyView S, const int *__restrict__ cidx, int n, double *__restrict__ r)
+{
+      const int q = blockIdx.x * blockDim.x + threadIdx.x;
+      if (q < n) r[q] = S.R[(long)cidx[q] * S.stride];
+}
+
 __global__ void __launch_bounds__(32) k_chain_total(const double *__restrict__ m, int n, double *__restrict__ out)
 {
       __shared__ __align__(16) double stage[CHN];
       const double s = warp_chain_sum(m, n, 0., stage);
       if (threadIdx.x == 0) out[0] = s;
+}
+
+// ---- elliptic elements (cart2ell, src/structure.c:172-284) ----------------
+
+enum { ELL_ATAN2 = 0, ELL_ZERO = 1, ELL_HOST = 2 };
+
+// cart2ell of one body up to its mean longitude's atan2, in the reference's
+// operation order with round-to-nearest FP64 intrinsics (no FMA
+// contraction), so that a, k, h, q, p and the atan2 arguments are the
+// reference's bit for bit.  code:
+//   ELL_ATAN2  the elliptic branch: lambda = atan2(sinF, cosF) - l, the atan2
+//              left to the caller's libm (the function the reference calls);
+//   ELL_ZERO   R or V2 zero: lambda = 0 (src/structure.c:262-264);
+//   ELL_HOST   the caller converts the body with the reference's cart2ell: the
+//              hyperbolic branch (atanh, sinh; src/structure.c:274-279), the
+//              (k, h) warning the reference prints (src/structure.c:253-255),
+//              or a NaN anywhere (the device's NaNs do not carry the host's
+//              signs, which printf shows).
+struct Ell {
+      double a, l, k, h, q, p, sinF, cosF;
+      int code;
+};
+
+__device__ Ell d_cart2ell(double X, double Y, double Z, double vX, double vY, double vZ, const double *cmb,
+                          bool central, bool j2, double J2, double R_unit, double mu)
+{
+      Ell e;
+      e.l = e.sinF = e.cosF = 0.;
+      e.code = ELL_ATAN2;
+      X = DSUB(X, central ? cmb[0] : 0.);
+      Y = DSUB(Y, central ? cmb[1] : 0.);
+      Z = DSUB(Z, central ? cmb[2] : 0.);
+      vX = DSUB(vX, central ? cmb[3] : 0.);
+      vY = DSUB(vY, central ? cmb[4] : 0.);
+      vZ = DSUB(vZ, central ? cmb[5] : 0.);
+      // semi-major axis, with the J2 correction of Kepler's third law
+      const double R = __dsqrt_rn(DADD(DADD(DMUL(X, X), DMUL(Y, Y)), DMUL(Z, Z)));
+      double V2 = DADD(DADD(DMUL(vX, vX), DMUL(vY, vY)), DMUL(vZ, vZ));
+      double AA = DDIV(DMUL(R, mu), DSUB(DMUL(2., mu), DMUL(R, V2)));
+      if (j2 && AA > 0.) {
+            mu = DMUL(mu, DADD(1., DDIV(DMUL(DMUL(DMUL(1., J2), R_unit), R_unit), DMUL(AA, AA))));
+            AA = DDIV(DMUL(R, mu), DSUB(DMUL(2., mu), DMUL(R, V2)));
+      }
+      e.a = AA;
+      // velocities in units of sqrt(mu), angular momentum
+      const double SMU = __dsqrt_rn(mu);
+      vX = DDIV(vX, SMU);
+      vY = DDIV(vY, SMU);
+      vZ = DDIV(vZ, SMU);
+      V2 = DADD(DADD(DMUL(vX, vX), DMUL(vY, vY)), DMUL(vZ, vZ));
+      const double RV = DADD(DADD(DMUL(X, vX), DMUL(Y, vY)), DMUL(Z, vZ));
+      const double C1 = DSUB(DMUL(Y, vZ), DMUL(Z, vY));
+      const double C2 = DSUB(DMUL(Z, vX), DMUL(X, vZ));
+      const double C3 = DSUB(DMUL(X, vY), DMUL(Y, vX));
+      const double CC = DADD(DADD(DMUL(C1, C1), DMUL(C2, C2)), DMUL(C3, C3));
+      const double DC = __dsqrt_rn(CC);
+      // (q, p)
+      const double aux0 = __dsqrt_rn(DMUL(2., DADD(CC, DMUL(DC, C3))));
+      e.q = aux0 == 0. ? 0. : DDIV(-C2, aux0);
+      e.p = aux0 == 0. ? 0. : DDIV(C1, aux0);
+      if (R == 0. || V2 == 0.) {
+            e.k = e.h = 0.;
+            e.code = ELL_ZERO;
+      } else {
+            // (k, h)
+            const double a11 = DSUB(V2, DDIV(1., R));
+            const double a12 = DDIV(RV, DMUL(R, DC));
+            const double a21 = -RV;
+            const double a22 = DSUB(DC, DDIV(R, DC));
+            const double c11 = DADD(DMUL(X, a11), DMUL(vX, a21));
+            const double c12 = DADD(DMUL(X, a12), DMUL(vX, a22));
+            const double c21 = DADD(DMUL(Y, a11), DMUL(vY, a21));
+            const double c22 = DADD(DMUL(Y, a12), DMUL(vY, a22));
+            const double FAC1 = DDIV(C1, DADD(DC, C3));
+            const double FAC2 = DDIV(C2, DADD(DC, C3));
+            const double K1 = DSUB(c11, DMUL(FAC1, DADD(DMUL(Z, a11), DMUL(vZ, a21))));
+            const double H1 = DADD(-c12, DMUL(FAC1, DADD(DMUL(Z, a12), DMUL(vZ, a22))));
+            const double H2 = DSUB(c21, DMUL(FAC2, DADD(DMUL(Z, a11), DMUL(vZ, a21))));
+            const double K2 = DSUB(c22, DMUL(FAC2, DADD(DMUL(Z, a12), DMUL(vZ, a22))));
+            const bool warn = DADD(fabs(DSUB(H1, H2)), fabs(DSUB(K1, K2))) > 1.e-6;
+            e.k = DMUL(0.5, DADD(K1, K2));
+            e.h = DMUL(0.5, DADD(H1, H2));
+            // mean longitude, elliptic branch (sqrt of a negative is NaN: hyperbolic)
+            const double USQA = __dsqrt_rn(DSUB(DDIV(2., R), V2));
+            if (USQA >= 0. && !warn) {
+                  const double b12 = DSUB(vX, DMUL(FAC1, vZ));
+                  const double b22 = DSUB(vY, DMUL(FAC2, vZ));
+                  const double aux1 = DDIV(DSUB(DMUL(R, V2), 1.), DADD(1., DMUL(DC, USQA)));
+                  e.sinF = DADD(DMUL(DMUL(-b12, R), USQA), DMUL(e.h, aux1));
+                  e.cosF = DADD(DMUL(DMUL(b22, R), USQA), DMUL(e.k, aux1));
+                  e.l = DMUL(RV, USQA);
+            } else {
+                  e.code = ELL_HOST;
+            }
+      }
+      if (isnan(e.a) || isnan(e.k) || isnan(e.h) || isnan(e.q) || isnan(e.p) || isnan(e.l) || isnan(e.sinF) ||
+          isnan(e.cosF))
+            e.code = ELL_HOST;
+      return e;
+}
+
+// One thread per existing body j (slot cidx[j]), with display()'s
+// mu + G m (src/display.c:341).  Writes the six element blocks, N doubles
+// apart (lambda's block holds l until k_ell_lambda), the atan2 arguments
+// (y, x) and the branch code,
+// and lists the ELL_HOST bodies (list[0]: their count).
+__global__ void k_cart2ell(BodyView S, const double *__restrict__ cmb, const int *__restrict__ cidx, int n,
+                           double mu, double G, int central, int j2, double J2, double R_unit,
+                           double *__restrict__ ell, long N, double *__restrict__ yx,
+                           unsigned char *__restrict__ code, int *__restrict__ list)
+{
+      const int j = blockIdx.x * blockDim.x + threadIdx.x;
+      if (j >= n) return;
+      const long s = (long)cidx[j] * S.stride;
+      const Ell e = d_cart2ell(S.x[s], S.y[s], S.z[s], S.vx[s], S.vy[s], S.vz[s], cmb, central != 0, j2 != 0, J2,
+                               R_unit, DADD(mu, DMUL(G, S.m[s])));
+      ell[j] = e.a;
+      ell[N + j] = e.l;
+      ell[2 * N + j] = e.k;
+      ell[3 * N + j] = e.h;
+      ell[4 * N + j] = e.q;
+      ell[5 * N + j] = e.p;
+      yx[2 * (long)j] = e.sinF;
+      yx[2 * (long)j + 1] = e.cosF;
+      code[j] = (unsigned char)e.code;
+      if (e.code == ELL_HOST) list[1 + atomicAdd(list, 1)] = j;
+}
+
+// The records and slots of the listed bodies, for the caller's cart2ell.
+__global__ void k_ell_gather(BodyView S, const int *__restrict__ cidx, const int *__restrict__ list, int nh,
+                             double *__restrict__ rec, int *__restrict__ slot)
+{
+      const int k = blockIdx.x * blockDim.x + threadIdx.x;
+      if (k >= nh) return;
+      const int b = cidx[list[k]];
+      const long s = (long)b * S.stride;
+      double *r = rec + 8 * (long)k;
+      r[0] = S.x[s]; r[1] = S.y[s]; r[2] = S.z[s]; r[3] = S.vx[s]; r[4] = S.vy[s]; r[5] = S.vz[s];
+      r[6] = S.m[s]; r[7] = S.R[s];
+      slot[k] = b;
+}
+
+// lambda = F - RV USQA (src/structure.c:272) from the caller's F = atan2(sinF, cosF).
+__global__ void k_ell_lambda(const double *__restrict__ F, const unsigned char *__restrict__ code,
+                             double *__restrict__ lam, int n)
+{
+      const int j = blockIdx.x * blockDim.x + threadIdx.x;
+      if (j < n && code[j] == ELL_ATAN2) lam[j] = DSUB(F[j], lam[j]);
+}
+
+// The caller's elements of the listed bodies (six a body, alkhqp order) into
+// the element blocks, `stride` doubles apart.
+__global__ void k_ell_host(const int *__restrict__ list, const double *__restrict__ alk, int nh,
+                           double *__restrict__ ell, long stride)
+{
+      const int k = blockIdx.x * blockDim.x + threadIdx.x;
+      if (k >= nh) return;
+      const long j = list[k];
+      for (int f = 0; f < 6; f++) ell[f * stride + j] = alk[6 * (long)k + f];
 }
 
 }  // namespace
@@ -247,17 +439,19 @@ extern "C" unsigned long ncgpu_format_cartesian_cap(void)
       return 8ul * ((unsigned long)c.n_max + 1ul) * 42ul;
 }
 
-extern "C" int ncgpu_format_cartesian(char *text, unsigned long cap, unsigned long *lens)
+namespace ncg {
+namespace {
+
+// Formats `total` values (file f: values first[f] .. first[f + 1] - 1) and
+// copies the files' texts, one after the other, into text; lens[f] receives
+// each file's length.  NCGPU_E_UNSUPPORTED when a value is beyond the
+// formatter's range (nothing copied), NCGPU_E_CAPACITY when cap is too small.
+template <class Values>
+int format_files(const Values &val, int nfiles, const long *first, char *text, unsigned long cap, unsigned long *lens)
 {
       Ctx &c = ctx();
-      reset_launches();
-      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
-      if (!text || !lens) return NCGPU_E_ARG;
       cudaStream_t st = c.s;
-      int n = 0;
-      NCG_TRY(compact_existing(c.ex, c.largest_id, &n, st));
-      const int central = c.P.par_central_mass_bool ? 1 : 0;
-      const long per = n + central, total = 6 * per + 2L * n;
+      const long total = first[nfiles];
       if (total >= 0x7fffffffL / SLOT) return NCGPU_E_CAPACITY;
       const size_t need = (size_t)(total > 0 ? total : 1) * SLOT;
       if (need > c.fmt_cap) {  // slots, packed text, lengths + offsets, scan sums
@@ -275,18 +469,15 @@ extern "C" int ncgpu_format_cartesian(char *text, unsigned long cap, unsigned lo
       }
       const size_t vals = c.fmt_cap / SLOT;
       int *len = c.fmt_len, *off = c.fmt_len + vals + 1, *sums = c.fmt_len + 2 * vals + 2;
-      BodyView S = state_view();
-      int h[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      int h[16] = {0};
       if (total > 0) {
             const int nb = (int)((total + 255) / 256);
-            k_fmt_values<<<nb, 256, 0, st>>>(S, c.cm, c.cidx, n, central, c.fmt_slots, len, c.err);
+            k_fmt_values<<<nb, 256, 0, st>>>(val, total, c.fmt_slots, len, c.err);
             NCG_LAUNCHED();
             NCG_TRY(scan_exclusive(len, off, (int)total, sums, st));
             k_fmt_pack<<<nb, 256, 0, st>>>(c.fmt_slots, off, total, c.fmt_text);
             NCG_LAUNCHED();
-            // each file's first value (files 0..5: per values; 6, 7: n values)
-            const long first[9] = {0, per, 2 * per, 3 * per, 4 * per, 5 * per, 6 * per, 6 * per + n, total};
-            for (int f = 0; f < 9; f++)
+            for (int f = 0; f <= nfiles; f++)
                   NCG_CK(cudaMemcpyAsync(&h[f], off + first[f], sizeof(int), cudaMemcpyDeviceToHost, st));
       }
       unsigned herr = 0;
@@ -297,12 +488,186 @@ extern "C" int ncgpu_format_cartesian(char *text, unsigned long cap, unsigned lo
             return NCGPU_E_UNSUPPORTED;
       }
       if (herr) return check_err_word();
-      if ((unsigned long)h[8] > cap) return NCGPU_E_CAPACITY;
-      if (h[8] > 0) {
-            NCG_CK(cudaMemcpyAsync(text, c.fmt_text, (size_t)h[8], cudaMemcpyDeviceToHost, st));
+      if ((unsigned long)h[nfiles] > cap) return NCGPU_E_CAPACITY;
+      if (h[nfiles] > 0) {
+            NCG_CK(cudaMemcpyAsync(text, c.fmt_text, (size_t)h[nfiles], cudaMemcpyDeviceToHost, st));
             NCG_CK(cudaStreamSynchronize(st));
       }
-      for (int f = 0; f < 8; f++) lens[f] = (unsigned long)(h[f + 1] - h[f]);
+      for (int f = 0; f < nfiles; f++) lens[f] = (unsigned long)(h[f + 1] - h[f]);
+      return NCGPU_OK;
+}
+
+}  // namespace
+}  // namespace ncg
+
+extern "C" int ncgpu_format_cartesian(char *text, unsigned long cap, unsigned long *lens)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      if (!text || !lens) return NCGPU_E_ARG;
+      int n = 0;
+      NCG_TRY(compact_existing(c.ex, c.largest_id, &n, c.s));
+      const int central = c.P.par_central_mass_bool ? 1 : 0;
+      const long per = n + central;
+      const long first[9] = {0, per, 2 * per, 3 * per, 4 * per, 5 * per, 6 * per, 6 * per + n, 6 * per + 2L * n};
+      return format_files(CartValues{state_view(), c.cm, c.cidx, n, central}, 8, first, text, cap, lens);
+}
+
+namespace ncg {
+namespace {
+
+// The elliptic buffers for n bodies: ell (6n doubles: a, lambda, k, h, q, p),
+// yx (2n: the atan2 arguments, then the caller's F), h (8n: the listed bodies'
+// records, then the caller's elements), codes, the list (1 + n ints) and the
+// listed bodies' slots (n ints).
+int ensure_ell(size_t n)
+{
+      Ctx &c = ctx();
+      if (n <= c.ell_cap && c.ell) return NCGPU_OK;
+      if (c.ell) cudaFree(c.ell);
+      if (c.ell_code) cudaFree(c.ell_code);
+      if (c.ell_list) cudaFree(c.ell_list);
+      c.ell = nullptr;
+      c.ell_code = nullptr;
+      c.ell_list = nullptr;
+      c.ell_cap = 0;
+      const size_t cap = std::max<size_t>(n, (size_t)c.n_max + 1);
+      NCG_CK(cudaMalloc(&c.ell, 16 * cap * sizeof(double)));
+      NCG_CK(cudaMalloc(&c.ell_code, cap));
+      NCG_CK(cudaMalloc(&c.ell_list, (2 * cap + 1) * sizeof(int)));
+      c.ell_cap = cap;
+      return NCGPU_OK;
+}
+
+}  // namespace
+}  // namespace ncg
+
+extern "C" int ncgpu_elliptic_begin(double mu, double *yx, unsigned long yx_cap, int *n_bodies, int *host_idx,
+                                    struct ncgpu_body *host_rec, int host_cap, int *n_host)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      c.ell_n = -1;
+      if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
+      if (!yx || !n_bodies || !n_host || host_cap < 0 || (host_cap > 0 && (!host_idx || !host_rec)))
+            return NCGPU_E_ARG;
+      cudaStream_t st = c.s;
+      int n = 0;
+      NCG_TRY(compact_existing(c.ex, c.largest_id, &n, st));
+      *n_bodies = n;
+      *n_host = 0;
+      if (2ul * (unsigned long)n > yx_cap) return NCGPU_E_CAPACITY;
+      NCG_TRY(ensure_ell((size_t)n));
+      const size_t N = c.ell_cap;
+      double *ell = c.ell, *dyx = c.ell + 6 * N, *hrec = c.ell + 8 * N;
+      int *list = c.ell_list, *slots = c.ell_list + 1 + N;
+      NCG_CK(cudaMemsetAsync(list, 0, sizeof(int), st));
+      const bool j2 = c.P.par_J2_bool && c.P.par_central_mass_bool;
+      if (n > 0) {
+            k_cart2ell<<<(n + 255) / 256, 256, 0, st>>>(state_view(), c.cm, c.cidx, n, mu, c.P.par_G,
+                                                         c.P.par_central_mass_bool ? 1 : 0, j2 ? 1 : 0, c.j2,
+                                                         c.P.par_R_unit, ell, (long)N, dyx, c.ell_code, list);
+            NCG_LAUNCHED();
+      }
+      int nh = 0;
+      NCG_CK(cudaMemcpyAsync(&nh, list, sizeof(int), cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      *n_host = nh;
+      if (nh > host_cap) return NCGPU_E_CAPACITY;
+      if (nh > 0) {  // in slot order, as display()'s loop meets them
+            std::vector<int> h((size_t)nh);
+            NCG_CK(cudaMemcpyAsync(h.data(), list + 1, sizeof(int) * nh, cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaStreamSynchronize(st));
+            std::sort(h.begin(), h.end());
+            NCG_CK(cudaMemcpyAsync(list + 1, h.data(), sizeof(int) * nh, cudaMemcpyHostToDevice, st));
+            k_ell_gather<<<(nh + 255) / 256, 256, 0, st>>>(state_view(), c.cidx, list + 1, nh, hrec, slots);
+            NCG_LAUNCHED();
+            NCG_CK(cudaMemcpyAsync(host_rec, hrec, sizeof(double) * 8 * nh, cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaMemcpyAsync(host_idx, slots, sizeof(int) * nh, cudaMemcpyDeviceToHost, st));
+      }
+      if (n > 0) NCG_CK(cudaMemcpyAsync(yx, dyx, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, st));
+      NCG_CK(cudaStreamSynchronize(st));
+      c.ell_n = n;
+      c.ell_nhost = nh;
+      c.ell_done = 0;
+      return NCGPU_OK;
+}
+
+extern "C" int ncgpu_format_elliptic(const double *F, const double *host_alkhqp, int n_host, int mass_radius,
+                                     char *text, unsigned long cap, unsigned long *lens)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited || !c.uploaded || c.ell_n < 0) return NCGPU_E_STATE;
+      const int n = c.ell_n;
+      if (!text || !lens || n_host != c.ell_nhost || (n > 0 && !F) || (n_host > 0 && !host_alkhqp))
+            return NCGPU_E_ARG;
+      cudaStream_t st = c.s;
+      const size_t N = c.ell_cap;
+      if (!c.ell_done) {
+            double *ell = c.ell, *dF = c.ell + 6 * N, *halk = c.ell + 8 * N;
+            if (n > 0) {
+                  NCG_CK(cudaMemcpyAsync(dF, F, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+                  k_ell_lambda<<<(n + 255) / 256, 256, 0, st>>>(dF, c.ell_code, ell + N, n);
+                  NCG_LAUNCHED();
+            }
+            if (n_host > 0) {
+                  NCG_CK(cudaMemcpyAsync(halk, host_alkhqp, sizeof(double) * 6 * n_host, cudaMemcpyHostToDevice, st));
+                  k_ell_host<<<(n_host + 255) / 256, 256, 0, st>>>(c.ell_list + 1, halk, n_host, ell, (long)N);
+                  NCG_LAUNCHED();
+            }
+            c.ell_done = 1;
+      }
+      const long first[9] = {0, n, 2L * n, 3L * n, 4L * n, 5L * n, 6L * n, 7L * n, 8L * n};
+      // the element blocks are N apart: format them from a compact view
+      return format_files(EllValues{state_view(), c.ell, c.cidx, n, (long)N}, mass_radius ? 8 : 6, first, text, cap,
+                          lens);
+}
+
+extern "C" int ncgpu_elliptic_values(double *values, unsigned long cap)
+{
+      Ctx &c = ctx();
+      reset_launches();
+      if (!c.inited || !c.uploaded || c.ell_n < 0 || !c.ell_done) return NCGPU_E_STATE;
+      if (!values) return NCGPU_E_ARG;
+      const int n = c.ell_n;
+      if (8ul * (unsigned long)n > cap) return NCGPU_E_CAPACITY;
+      cudaStream_t st = c.s;
+      const size_t N = c.ell_cap;
+      for (int f = 0; f < 6 && n > 0; f++)
+            NCG_CK(cudaMemcpyAsync(values + (size_t)f * n, c.ell + f * N, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                   st));
+      if (n > 0) {  // masses and radii, gathered through the compacted slots
+            double *g = c.ell + 8 * N;
+            k_gather_mass<<<(n + 255) / 256, 256, 0, st>>>(state_view(), c.cidx, n, g);
+            NCG_LAUNCHED();
+            NCG_CK(cudaMemcpyAsync(values + 6 * (size_t)n, g, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+            k_gather_radius<<<(n + 255) / 256, 256, 0, st>>>(state_view(), c.cidx, n, g + N);
+            NCG_LAUNCHED();
+            NCG_CK(cudaMemcpyAsync(values + 7 * (size_t)n, g + N, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+      }
+      NCG_CK(cudaStreamSynchronize(st));
+      return NCGPU_OK;
+}
+
+extern "C" int ncgpu_host_atan2(const double *yx, double *F, long n)
+{
+      if (n < 0 || (n > 0 && (!yx || !F))) return NCGPU_E_ARG;
+      const long per = 1L << 16;
+      const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+      const int T = (int)std::min<long>(std::min<long>(hw, 16), (n + per - 1) / per);
+      auto run = [&](long lo, long hi) {
+            for (long j = lo; j < hi; j++) F[j] = atan2(yx[2 * j], yx[2 * j + 1]);
+      };
+      if (T <= 1) {
+            run(0, n);
+            return NCGPU_OK;
+      }
+      std::vector<std::thread> th;
+      const long chunk = (n + T - 1) / T;
+      for (int t = 0; t < T; t++) th.emplace_back(run, std::min(n, t * chunk), std::min(n, (t + 1) * chunk));
+      for (auto &x : th) x.join();
       return NCGPU_OK;
 }
 

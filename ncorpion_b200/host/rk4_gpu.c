@@ -169,18 +169,25 @@ static void gpu_collision_records(double t_now)
 }
 
 /* display() (src/display.c:239-451) of the device state -- the output step's
-   copy -- for the cartesian files: their text comes formatted from the device
-   (ncgpu_format_cartesian), stat.txt's line is printed here from the device's
-   statistics with the reference's own cart2ell, and collision.txt from the
-   host's records, every line as display() prints it.  CM_buffer receives the
-   copy's central body.  Returns 0 (nothing written) when the host must print
-   this output itself: elliptic elements, or a value beyond the device
-   formatter's range. */
+   copy.  The cartesian files' text comes formatted from the device
+   (ncgpu_format_cartesian).  The elliptic files' elements come from the
+   device's cart2ell (ncgpu_elliptic_begin): the mean longitude's atan2 is this
+   C library's (ncgpu_host_atan2), and the bodies the device lists (hyperbolic
+   orbits, the (k, h) warning, NaNs) go through the reference's own cart2ell,
+   which prints its warnings in slot order as display()'s loop does; the device
+   then formats the six files (ncgpu_format_elliptic).  stat.txt's line is
+   printed here from the device's statistics with the reference's own cart2ell,
+   and collision.txt from the host's records, every line as display() prints
+   it.  CM_buffer receives the copy's central body.  Returns 0 (nothing
+   written) when the host must print this output itself: a cartesian value
+   beyond the device formatter's range. */
 static int gpu_display_device(void)
 {
       static char *text = NULL;
       static unsigned long cap = 0;
-      if (!write_cartesian_bool || write_elliptic_bool) return 0;
+      static double *yx = NULL, *F = NULL, *halk = NULL;
+      static struct moonlet *hrec = NULL;
+      static int *hidx = NULL;
       if (cap < ncgpu_format_cartesian_cap()) {  /* one pinned buffer for the whole run */
             if (text) {
                   ncgpu_host_unregister(text);
@@ -194,10 +201,27 @@ static int gpu_display_device(void)
             }
             gpu_check(ncgpu_host_register(text, cap), "host register");
       }
+      if (write_elliptic_bool && yx == NULL) {  /* per body: atan2 arguments and results, listed bodies */
+            const size_t nb = (size_t)N_max + 1;
+            yx = (double *)malloc(2 * nb * sizeof(double));
+            F = (double *)malloc(nb * sizeof(double));
+            halk = (double *)malloc(6 * nb * sizeof(double));
+            hrec = (struct moonlet *)malloc(nb * sizeof(struct moonlet));
+            hidx = (int *)malloc(nb * sizeof(int));
+            if (!yx || !F || !halk || !hrec || !hidx) {
+                  fprintf(stderr, "Error : Can't allocate the elliptic output buffers.\n");
+                  abort();
+            }
+            gpu_check(ncgpu_host_register(yx, 2 * nb * sizeof(double)), "host register");
+            gpu_check(ncgpu_host_register(F, nb * sizeof(double)), "host register");
+      }
       unsigned long lens[8];
-      int st = ncgpu_format_cartesian(text, cap, lens);
-      if (st == NCGPU_E_UNSUPPORTED) return 0;
-      gpu_check(st, "output text");
+      int st;
+      if (write_cartesian_bool) {
+            st = ncgpu_format_cartesian(text, cap, lens);
+            if (st == NCGPU_E_UNSUPPORTED) return 0;
+            gpu_check(st, "output text");
+      }
       double stats[3];
       int idx[2];
       struct moonlet two[2];
@@ -207,20 +231,57 @@ static int gpu_display_device(void)
 
       int collision = collision_bool && write_collisions_bool ? 1 : 0;
       FILE *filestat = *files;
-      FILE *out[8];  /* in the device's order: x y z vx vy vz mass radius */
-      for (int f = 0; f < 6; f++) out[f] = *(files + 3 + collision + f);
-      out[6] = *(files + 1 + collision);
-      out[7] = *(files + 2 + collision);
-      unsigned long pos = 0;
-      for (int f = 0; f < 8; f++) {
-            fwrite(text + pos, 1, lens[f], out[f]);
-            pos += lens[f];
+      FILE *out[8];   /* in the device's order: x y z vx vy vz mass radius */
+      FILE *eout[6];  /* a lambda k h q p */
+      if (write_cartesian_bool || write_elliptic_bool) {
+            out[6] = *(files + 1 + collision);
+            out[7] = *(files + 2 + collision);
+      }
+      if (write_cartesian_bool) {
+            for (int f = 0; f < 6; f++) out[f] = *(files + 3 + collision + f);
+            unsigned long pos = 0;
+            for (int f = 0; f < 8; f++) {
+                  fwrite(text + pos, 1, lens[f], out[f]);
+                  pos += lens[f];
+            }
       }
 
       typ total_mass = stats[0], M1 = stats[1], M2 = stats[2];
       typ mu, R1, R2, a1, a2, l1, l2, K1, K2, H1, H2, Q1, Q2, P1, P2, inner_fluid_disk_mass;
       typ alkhqp[6];
       mu = central_mass_bool ? CM_buffer.mass : M_unit;  mu += inner_fluid_disk_bool ? fluid_disk_Sigma*M_PI*(Rout*Rout - R_unit*R_unit) : 0.;  mu *= G;
+      if (write_elliptic_bool) {
+            const int first = write_cartesian_bool ? 9 : 3;
+            for (int f = 0; f < 6; f++) eout[f] = *(files + first + collision + f);
+            int nb = 0, nh = 0;
+            gpu_check(ncgpu_elliptic_begin(mu, yx, 2ul * ((unsigned long)N_max + 1ul), &nb, hidx,
+                                           (struct ncgpu_body *)hrec, N_max + 1, &nh), "elliptic elements");
+            gpu_check(ncgpu_host_atan2(yx, F, nb), "atan2");
+            for (int k = 0; k < nh; k++) cart2ell(hrec, k, halk + 6 * k, mu + G*hrec[k].mass);
+            const int mr = write_cartesian_bool ? 0 : 1;  /* mass.txt and radius.txt, unless written above */
+            st = ncgpu_format_elliptic(F, halk, nh, mr, text, cap, lens);
+            if (st == NCGPU_E_UNSUPPORTED) {  /* a value beyond the formatter's range: print them here */
+                  double *v = (double *)malloc(8 * ((size_t)nb + 1) * sizeof(double));
+                  if (v == NULL) {
+                        fprintf(stderr, "Error : Can't allocate the elliptic values.\n");
+                        abort();
+                  }
+                  gpu_check(ncgpu_elliptic_values(v, 8ul * ((unsigned long)nb + 1ul)), "elliptic values");
+                  for (int f = 0; f < 6 + 2 * mr; f++) {
+                        FILE *o = f < 6 ? eout[f] : out[f];
+                        for (int j = 0; j < nb; j++) fprintf(o, "%.14lf ", v[(size_t)f * nb + j]);
+                  }
+                  free(v);
+            }
+            else {
+                  gpu_check(st, "elliptic text");
+                  unsigned long pos = 0;
+                  for (int f = 0; f < 6 + 2 * mr; f++) {
+                        fwrite(text + pos, 1, lens[f], f < 6 ? eout[f] : out[f]);
+                        pos += lens[f];
+                  }
+            }
+      }
       if (how_many_moonlets == 0){
             M1 = 0.; M2 = 0.; R1 = 0.; R2 = 0.; a1 = 0.; a2 = 0.; l1 = 0.; l2 = 0.; K1 = 0.; K2 = 0.; H1 = 0.; H2 = 0.; Q1 = 0.; Q2 = 0.; P1 = 0.; P2 = 0.;
       }
@@ -251,7 +312,12 @@ static int gpu_display_device(void)
       fprintf(filestat, " %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf %.14lf",
       M1, M2, R1, R2, a1, a2, l1, l2, K1, K2, H1, H2, Q1, Q2, P1, P2);
       fprintf(filestat, "\n");
-      for (int f = 0; f < 8; f++) fprintf(out[f], "\n");
+      if (write_cartesian_bool) for (int f = 0; f < 6; f++) fprintf(out[f], "\n");
+      if (write_elliptic_bool) for (int f = 0; f < 6; f++) fprintf(eout[f], "\n");
+      if (write_cartesian_bool || write_elliptic_bool) {
+            fprintf(out[7], "\n");  /* radius.txt, then mass.txt, as display() ends them */
+            fprintf(out[6], "\n");
+      }
       if (collision){
             FILE *filecol = *(files + 1);
             for (int p = 0; p < indexCollision; p ++){

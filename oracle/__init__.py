@@ -43,6 +43,10 @@ class Port:
         L.orc_vector_field.argtypes = [C.c_int, P, P, P, P, P, P]
         L.orc_kick.argtypes = [C.c_int, P, P, P, C.c_double, P]
         L.orc_drift.argtypes = [C.c_int, P, P, P, C.c_double, P]
+        L.orc_cart2ell.argtypes = [P, P, C.c_double, P, C.c_double, P]
+        L.orc_cart2ell.restype = C.c_int
+        L.orc_cart2ell_all.argtypes = [C.c_int, P, P, P, C.c_double, P, C.c_double, P, C.c_long]
+        L.orc_cart2ell_all.restype = C.c_long
 
     def vector_field(self, bodies, exists, cm, params):
         b = np.ascontiguousarray(bodies, np.float64)
@@ -60,6 +64,26 @@ class Port:
         ex = np.ascontiguousarray(exists, np.int32)
         self.lib.orc_kick(b.shape[0] - 1, _p(b), _p(ex), _p(cmv), C.c_double(dt), C.byref(params))
         return b, cmv
+
+    def cart2ell(self, rec, cm, mu, params, j2=0.0):
+        """cart2ell of one record: (alkhqp (6), whether it printed the (k, h) warning)."""
+        r = np.ascontiguousarray(rec, np.float64)
+        cmv = np.ascontiguousarray(cm, np.float64)
+        out = np.zeros(6)
+        w = self.lib.orc_cart2ell(_p(r), _p(cmv), C.c_double(mu), C.byref(params), C.c_double(j2), _p(out))
+        return out, bool(w)
+
+    def cart2ell_all(self, bodies, exists, cm, mu, params, j2=0.0):
+        """display()'s elliptic values of the existing bodies: (6, n)."""
+        b = np.ascontiguousarray(bodies, np.float64)
+        ex = np.ascontiguousarray(exists, np.int32)
+        cmv = np.ascontiguousarray(cm, np.float64)
+        n = int(np.count_nonzero(ex))
+        out = np.zeros((6, max(n, 1)))
+        got = self.lib.orc_cart2ell_all(b.shape[0] - 1, _p(b), _p(ex), _p(cmv), C.c_double(mu), C.byref(params),
+                                        C.c_double(j2), _p(out), out.size)
+        assert got == n
+        return out[:, :n].copy()
 
     def drift(self, bodies, exists, cm, dt, params):
         b = np.ascontiguousarray(bodies, np.float64).copy()
@@ -109,6 +133,8 @@ class Ref:
         L.orc_set_free.argtypes = [C.c_int, P]
         if hasattr(L, "orc_frag_counts"):
             L.orc_frag_counts.argtypes = [P]
+        if hasattr(L, "orc_cart2ell"):
+            L.orc_cart2ell.argtypes = [P, P, C.c_double, C.c_double, P]
         if L.orc_init() != 0:
             raise MemoryError("reference init failed")
         self.n_max = L.orc_n_max()
@@ -136,6 +162,15 @@ class Ref:
         cma = np.zeros(3)
         self.lib.orc_vector_field(_p(acc), _p(cma))
         return acc, cma
+
+    def cart2ell(self, rec, cm, mu, j2=0.0):
+        """The reference's cart2ell of one record (its globals CM_buffer = cm,
+        J2 = j2): alkhqp (6)."""
+        r = np.ascontiguousarray(rec, np.float64)
+        cmv = np.ascontiguousarray(cm, np.float64)
+        out = np.zeros(6)
+        self.lib.orc_cart2ell(_p(r), _p(cmv), C.c_double(j2), C.c_double(mu), _p(out))
+        return out
 
     def fragment_counts(self):
         """(merger, super-catastrophic, partial, full) since the last reset."""

@@ -1063,3 +1063,95 @@ long orc_fprintf_values(const double *v, long n, const char *path)
       fclose(f);
       return bytes;
 }
+
+/* ---- elliptic elements (cart2ell, src/structure.c:172-284) ---------------- */
+
+/* cart2ell of body b with the central body cm (CM_buffer) and the
+   parameter mu, into alkhqp (a, lambda, k, h, q, p), operation for operation;
+   J2 is the J2 in force (the reference's global).  Prints the reference's
+   (k, h) warning to stdout when it would (src/structure.c:253-255) and
+   returns 1 then, else 0. */
+int orc_cart2ell(const body *b, const body *cm, double mu, const struct ncgpu_params *P, double J2, double *alkhqp)
+{
+      const int central = P->par_central_mass_bool != 0;
+      double X = b->x - (central ? cm->x : 0.), Y = b->y - (central ? cm->y : 0.), Z = b->z - (central ? cm->z : 0.);
+      double vX = b->vx - (central ? cm->vx : 0.), vY = b->vy - (central ? cm->vy : 0.);
+      double vZ = b->vz - (central ? cm->vz : 0.);
+      int warned = 0;
+      /* semi-major axis, Kepler's third law corrected for J2 on elliptic orbits */
+      const double R = sqrt(X * X + Y * Y + Z * Z);
+      double V2 = vX * vX + vY * vY + vZ * vZ;
+      double AA = R * mu / (2. * mu - R * V2);
+      if (P->par_J2_bool && AA > 0. && central) {
+            mu *= 1. + 1. * J2 * P->par_R_unit * P->par_R_unit / (AA * AA);
+            AA = R * mu / (2. * mu - R * V2);
+      }
+      alkhqp[0] = AA;
+      /* velocities in units of sqrt(mu); angular momentum C */
+      const double SMU = sqrt(mu);
+      vX /= SMU;
+      vY /= SMU;
+      vZ /= SMU;
+      V2 = vX * vX + vY * vY + vZ * vZ;
+      const double RV = X * vX + Y * vY + Z * vZ;
+      const double C1 = Y * vZ - Z * vY, C2 = Z * vX - X * vZ, C3 = X * vY - Y * vX;
+      const double CC = C1 * C1 + C2 * C2 + C3 * C3;
+      const double DC = sqrt(CC);
+      const double aux0 = sqrt(2. * (CC + DC * C3));
+      alkhqp[4] = aux0 == 0. ? 0. : -C2 / aux0;
+      alkhqp[5] = aux0 == 0. ? 0. : C1 / aux0;
+      if (R == 0. || V2 == 0.) {
+            alkhqp[1] = alkhqp[2] = alkhqp[3] = 0.;
+            return 0;
+      }
+      const double a11 = V2 - 1. / R, a12 = RV / (R * DC), a21 = -RV, a22 = DC - R / DC;
+      const double c11 = X * a11 + vX * a21, c12 = X * a12 + vX * a22;
+      const double c21 = Y * a11 + vY * a21, c22 = Y * a12 + vY * a22;
+      const double FAC1 = C1 / (DC + C3), FAC2 = C2 / (DC + C3);
+      const double K1 = c11 - FAC1 * (Z * a11 + vZ * a21);
+      const double H1 = -c12 + FAC1 * (Z * a12 + vZ * a22);
+      const double H2 = c21 - FAC2 * (Z * a11 + vZ * a21);
+      const double K2 = c22 - FAC2 * (Z * a12 + vZ * a22);
+      if (fabs(H1 - H2) + fabs(K1 - K2) > 1.e-6) {
+            printf("Warning : Bad computation of (k,h) in function cart2ell. (K1 - K2, H1 - H2) = (%.13lf, %.13lf)\n",
+                   K1 - K2, H1 - H2);
+            warned = 1;
+      }
+      const double K = 0.5 * (K1 + K2), H = 0.5 * (H1 + H2);
+      alkhqp[2] = K;
+      alkhqp[3] = H;
+      /* mean longitude: elliptic branch, else (NaN square root) hyperbolic */
+      double USQA = sqrt(2. / R - V2);
+      if (USQA >= 0.) {
+            const double b12 = vX - FAC1 * vZ, b22 = vY - FAC2 * vZ;
+            const double aux1 = (R * V2 - 1.) / (1. + DC * USQA);
+            const double sinF = -b12 * R * USQA + H * aux1, cosF = b22 * R * USQA + K * aux1;
+            alkhqp[1] = atan2(sinF, cosF) - RV * USQA;
+      } else {
+            USQA = sqrt(-(2. / R - V2));
+            const double E = atanh(RV * USQA / (R * V2 - 1.));
+            alkhqp[1] = sqrt(K * K + H * H) * sinh(E) - E + atan2(H, K);
+      }
+      return warned;
+}
+
+/* display()'s elliptic values (src/display.c:321-347): cart2ell of every
+   existing slot <= lid with mu + G m, into out (six blocks a, lambda, k, h,
+   q, p of n_existing values).  Returns n_existing. */
+long orc_cart2ell_all(int lid, const body *b, const int *ex, const body *cm, double mu,
+                      const struct ncgpu_params *P, double J2, double *out, long cap)
+{
+      long n = 0;
+      for (int p = 0; p <= lid; p++) n += ex[p] ? 1 : 0;
+      if (6 * n > cap) return -1;
+      long j = 0;
+      for (int p = 0; p <= lid; p++) {
+            if (!ex[p]) continue;
+            double alk[6];
+            orc_cart2ell(b + p, cm, mu + P->par_G * b[p].mass, P, J2, alk);
+            for (int f = 0; f < 6; f++) out[f * n + j] = alk[f];
+            j++;
+      }
+      fflush(stdout);
+      return n;
+}

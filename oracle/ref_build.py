@@ -177,6 +177,16 @@ PROFILES = {
     "mesh_naive_resume": dict(MESH, collision_bool="1", instant_merger_bool="1", collision_cube_cells="256",
                               switch_to_brute_force="5000", N_max="4096", N_0="2000", t_end="0.05",
                               time_step="0.001", resume_simulation_bool="1"),
+    # whole-program runs with the elliptic files (cart2ell, src/structure.c:172-284):
+    # the brute-force driver with both coordinate sets and the fluid-body J2 (the
+    # J2 correction of the semi-major axis), the mesh driver with elliptic files only
+    "bf_merge_ell": dict(BF, collision_bool="1", instant_merger_bool="1", J2_bool="1", J2_value="0.", Tearth="25.",
+                         N_max="4096", N_0="2000", t_end="0.2", time_step="0.001", output_step="50",
+                         write_to_files_bool="1", write_cartesian_bool="1", write_elliptic_bool="1",
+                         write_collisions_bool="1"),
+    "mesh_prog_ell": dict(MESH, collision_bool="1", instant_merger_bool="1", collision_cube_cells="256",
+                          N_max="30000", N_0="20000", t_end="0.05", time_step="0.0005", output_step="25",
+                          write_to_files_bool="1", write_elliptic_bool="1", write_collisions_bool="1"),
     # the N = 1,048,576 mesh workload: 1024 cells per side (8.6 GB hash table)
     "mesh_merge_1m": dict(MESH, collision_bool="1", instant_merger_bool="1",
                           collision_cube_cells="1024", N_max="1100000", N_0="1048576",

@@ -256,3 +256,16 @@ void orc_step_mesh(void)
       end_of_timestep(B, 0);
 }
 #endif
+
+/* cart2ell (src/structure.c:172-284) of one record with the central body cm
+   as CM_buffer and the J2 in force j2 (the global J2 it reads), as display()
+   calls it; the reference prints its warnings to stdout. */
+void orc_cart2ell(const double *rec, const double *cm, double j2, double mu, double *alkhqp)
+{
+      struct moonlet m;
+      memcpy(&m, rec, sizeof m);
+      memcpy(&CM_buffer, cm, sizeof CM_buffer);
+      J2 = j2;
+      cart2ell(&m, 0, alkhqp, mu);
+      fflush(stdout);
+}

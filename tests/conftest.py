@@ -79,3 +79,45 @@ def make_params(**kw):
             continue
         setattr(p, k, v)
     return p
+
+
+def elliptic_cases(n=3000, seed=0, cm_at_rest=False):
+    """Bodies for cart2ell (src/structure.c:172-284) with every branch of it:
+    a disk of elliptic orbits (retrograde ones at small inclinations from 180
+    degrees, where its two estimates of (k, h) part and it prints its warning),
+    hyperbolic orbits (the atanh / sinh branch), a body on the central body
+    (R = 0), one at rest relative to it (V2 = 0), a radial orbit (zero angular
+    momentum: NaN elements), a parabolic orbit (2 mu = R V2: a = inf) and an
+    exactly retrograde planar one (0 / 0).  The special bodies sit at dyadic
+    offsets from the central body, so that cart2ell's subtractions are exact.
+    Returns (bodies, exists, cm): G = 1, central mass 1, body masses 1e-9 (0
+    for the parabolic and the planar retrograde bodies); the central body moves
+    off the origin unless cm_at_rest."""
+    from ncorpion_b200 import disks
+    rng = np.random.default_rng(seed)
+    cm = np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0]) if cm_at_rest else \
+        np.array([2.0 ** -10, -2.0 ** -11, 2.0 ** -12, 2.0 ** -9, 2.0 ** -10, -2.0 ** -11, 1.0, 1.0])
+    b = disks.gravity_disk(n, seed=seed)
+    b[:, :6] += cm[:6]
+    b[:, 6] = 1e-9
+    k = n // 50
+    hyp = rng.choice(np.arange(40, n), k, replace=False)
+    b[hyp, 3:6] = cm[3:6] + (b[hyp, 3:6] - cm[3:6]) * rng.uniform(1.5, 3.0, (k, 1))
+    special = [
+        ([0.0, 0.0, 0.0], [0.0, 0.0, 0.0], 1e-9),            # on the central body
+        ([0.5, -0.25, 0.0], [0.0, 0.0, 0.0], 1e-9),          # at rest relative to it
+        ([0.5, 0.25, 0.125], [0.25, 0.125, 0.0625], 1e-9),   # radial
+        ([2.0, 0.0, 0.0], [0.0, 1.0, 0.0], 0.0),             # parabolic (mu = 1)
+        ([1.0, 0.0, 0.0], [0.0, -1.0, 0.0], 0.0),            # retrograde, planar
+    ]
+    # retrograde at inclinations 1e-2 .. 1e-7 from 180 degrees, eccentric
+    for q, dz in enumerate(10.0 ** -np.arange(2, 8)):
+        for e in (0.0, 0.25, 0.5):
+            special.append(([1.0 + 0.125 * q, 0.0, 0.0], [0.0, -(1.0 + e) ** 0.5, dz], 1e-9))
+    for s_, (r, v, m) in enumerate(special):
+        b[s_, :3] = cm[:3] + np.array(r)
+        b[s_, 3:6] = cm[3:6] + np.array(v)
+        b[s_, 6] = m
+    ex = np.ones(n, np.int32)
+    ex[rng.choice(np.arange(40, n), n // 40, replace=False)] = 0
+    return b, ex, cm

@@ -279,6 +279,7 @@ def tides_mesh_case(profile, n, seed, nsteps, gam, dt):
 
 OUTPUT_FILES = ["stat.txt", "collision.txt", "mass.txt", "radius.txt", "x.txt", "y.txt", "z.txt", "vx.txt",
                 "vy.txt", "vz.txt", "readme.txt"]
+ELLIPTIC_FILES = ["a.txt", "lambda.txt", "k.txt", "h.txt", "q.txt", "p.txt"]
 
 
 def filtered_stdout(text):
@@ -306,7 +307,10 @@ def program_run_case(profile, bodies, bodies_from=None, disk=None):
         out = dict(bodies_from=np.array(bodies_from))
     else:
         out = dict(bodies=bodies)
-    for f in OUTPUT_FILES:
+    files = [f for f in OUTPUT_FILES + ELLIPTIC_FILES if os.path.exists(os.path.join(d, f))]
+    if files != OUTPUT_FILES:
+        out["files"] = np.array(files)
+    for f in files:
         data = open(os.path.join(d, f), "rb").read()
         out["digest_" + f] = digest(np.frombuffer(data, np.uint8))
     out["digest_stdout"] = digest(np.frombuffer(filtered_stdout(r.stdout).encode(), np.uint8))
@@ -394,6 +398,12 @@ def main(names=None):
     # the mesh driver on 200,000 bodies of the mesh workload's disk, 20 steps
     out["program_mesh_merge_200k"] = lambda: program_run_case("mesh_prog_200k", disks.mesh_disk(200000, seed=0),
                                                               disk=("mesh_disk", 200000, 0))
+    # both drivers with the elliptic files (brute force: with the cartesian ones
+    # and the fluid-body J2; mesh: elliptic only)
+    out["program_bf_merge_ell"] = lambda: program_run_case("bf_merge_ell", disks.bf_collide_disk(2000, seed=0),
+                                                           bodies_from="program_bf_merge")
+    out["program_mesh_merge_ell"] = lambda: program_run_case("mesh_prog_ell", big_disk(20000, 7)[0],
+                                                             bodies_from="program_mesh_merge")
     # both drivers without output files, with the resuming files at the end; the
     # mesh driver also in its brute-force regime (below switch_to_brute_force)
     out["program_bf_merge_resume"] = lambda: program_resume_case("bf_merge_resume", disks.bf_collide_disk(2000, seed=0),

@@ -33,7 +33,8 @@ pytestmark = pytest.mark.gpu
 PROGRAMS = [("bf_merge", "program_bf_merge"), ("mesh_prog", "program_mesh_merge"),
             ("bf_merge_j2", "program_bf_merge_j2"), ("mesh_prog_j2", "program_mesh_merge_j2"),
             ("bf_merge_tides", "program_bf_merge_tides"), ("mesh_prog_tides", "program_mesh_merge_tides"),
-            ("mesh_prog_200k", "program_mesh_merge_200k")]
+            ("mesh_prog_200k", "program_mesh_merge_200k"), ("bf_merge_ell", "program_bf_merge_ell"),
+            ("mesh_prog_ell", "program_mesh_merge_ell")]
 
 
 def _digest(b):
@@ -63,7 +64,7 @@ def test_dropin_program_matches_reference_outputs(lib, profile, fixture):
     r = subprocess.run([exe], cwd=d, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     bad = []
-    for f in OUTPUT_FILES:
+    for f in ([str(x) for x in g["files"]] if "files" in g else OUTPUT_FILES):
         data = open(os.path.join(d, f), "rb").read()
         if not np.array_equal(_digest(data), g["digest_" + f]):
             bad.append(f)

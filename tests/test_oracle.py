@@ -289,3 +289,34 @@ def test_port_tides_mesh_steps_match_golden():
     b, ex, cm = w.get_state()
     assert np.array_equal(_digest(b), g["out_digest"]) and np.array_equal(_digest(ex), g["out_exists_digest"])
     assert np.array_equal(cm, g["out_cm"])
+
+
+# ---- elliptic elements (cart2ell, src/structure.c:172-284) -----------------
+
+@pytest.mark.parametrize("profile,at_rest", [("bf_grav_s05", False), ("bf_grav_s05", True), ("bf_grav_j2", False)])
+def test_port_cart2ell_vs_reference(port, capfd, profile, at_rest):
+    """The port's cart2ell against the reference's on every branch
+    (conftest.elliptic_cases): the six elements bit for bit (NaNs with their
+    signs: printf shows them), and the (k, h) warnings printed alike.  The J2
+    profile holds a constant J2 of 0.0125, which corrects a on elliptic orbits."""
+    if not oracle.ref_available(profile):
+        pytest.skip("reference not compiled here")
+    from conftest import elliptic_cases
+    b, ex, cm = elliptic_cases(1500, seed=4, cm_at_rest=at_rest)
+    j2 = 0.0125 if profile == "bf_grav_j2" else 0.0
+    p = make_params(J2_bool=1, J2=j2) if j2 else make_params()
+    ref = oracle.Ref(profile)
+    mu = 1.0 * cm[6]
+    live = np.flatnonzero(ex)
+    capfd.readouterr()
+    got = np.array([port.cart2ell(b[i], cm, mu + 1.0 * b[i, 6], p, j2)[0] for i in live])
+    out_port = capfd.readouterr().out
+    want = np.array([ref.cart2ell(b[i], cm, mu + 1.0 * b[i, 6], j2) for i in live])
+    out_ref = capfd.readouterr().out
+    assert np.array_equal(got.view(np.int64), want.view(np.int64))
+    assert out_port == out_ref
+    assert out_ref.count("Warning : Bad computation of (k,h)") >= 3
+    assert got[0, 1] == 0.0 and got[1, 1] == 0.0      # R = 0, V2 = 0: lambda = 0
+    assert np.isnan(got[2]).any() and np.isnan(got[4]).any()  # radial, planar retrograde
+    assert got[3, 0] == np.inf                         # parabolic
+    assert (got[:, 0] < 0).sum() >= 10                 # hyperbolic branch

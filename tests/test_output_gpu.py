@@ -138,3 +138,107 @@ def test_snapshot_leaves_the_bodies(gpu):
     assert not np.array_equal(copy[0], before[0])
     assert np.array_equal(after[0], before[0]) and np.array_equal(after[2], before[2])
     assert w1 != w0 and api.get_sideral_omega() == w1
+
+
+# ---- elliptic files (cart2ell, src/structure.c:172-284) ---------------------
+
+def _fmt_c(v):
+    """glibc's "%.14lf " of v, NaNs with their signs."""
+    if np.isnan(v):
+        return "-nan " if np.signbit(v) else "nan "
+    return _fmt(v)
+
+
+def _elliptic_on_device(api, port, b, ex, cm, params, j2, mass_radius):
+    """Both halves of the device's elliptic output, the caller's part done as
+    the drop-in does it: atan2 by the C library (ncgpu_host_atan2), the listed
+    bodies through cart2ell (the oracle's, pinned to the reference's)."""
+    mu = 1.0 * cm[6]
+    yx, hidx, hrec = api.elliptic_begin(mu)
+    F = api.host_atan2(yx)
+    alk = np.array([port.cart2ell(r, cm, mu + 1.0 * r[6], params, j2)[0] for r in hrec]).reshape(-1, 6)
+    return yx, hidx, hrec, F, alk
+
+
+@pytest.mark.parametrize("at_rest,j2", [(False, 0.0), (True, 0.0), (False, 0.0125)])
+def test_format_elliptic_matches_cart2ell_and_printf(gpu, port, capfd, at_rest, j2):
+    """The six elliptic files (and mass, radius) against the oracle's cart2ell
+    of every existing body, text for text; the bodies the device lists are
+    exactly those cart2ell takes out of the elliptic branch (hyperbolic, its
+    (k, h) warning, NaNs), in slot order, and converting them prints the
+    reference's warnings as display()'s loop would."""
+    from conftest import elliptic_cases
+    b, ex, cm = elliptic_cases(3000, seed=6, cm_at_rest=at_rest)
+    params = dict(J2_bool=1, J2=j2) if j2 else {}
+    api = gpu(4000, **params)
+    p = make_params(**params)
+    api.upload(b, ex, cm)
+    assert api.get_j2() == j2
+    capfd.readouterr()
+    yx, hidx, hrec, F, alk = _elliptic_on_device(api, port, b, ex, cm, p, j2, True)
+    printed = capfd.readouterr().out
+    files = api.format_elliptic(F, alk, mass_radius=True)
+    live = np.flatnonzero(ex)
+    want = port.cart2ell_all(b, ex, cm, 1.0 * cm[6], p, j2)
+    want_printed = capfd.readouterr().out
+    assert printed == want_printed and printed.count("Warning") >= 3
+    for f in range(6):
+        assert files[f] == "".join(_fmt_c(v) for v in want[f]), f"file {f}"
+    assert files[6] == "".join(_fmt(v) for v in b[live, 6])
+    assert files[7] == "".join(_fmt(v) for v in b[live, 7])
+    # the listed bodies: slots ascending, records as uploaded
+    assert np.all(np.diff(hidx) > 0) and np.array_equal(hrec, b[hidx])
+    expect = []
+    for i in live:
+        a, warned = port.cart2ell(b[i], cm, 1.0 * cm[6] + 1.0 * b[i, 6], p, j2)
+        if warned or np.isnan(a).any() or a[0] < 0:
+            expect.append(i)
+    capfd.readouterr()
+    hyp_or_nan = set(expect)
+    assert hyp_or_nan <= set(hidx.tolist())
+    assert len(hidx) >= 30 and len(hidx) < len(live) // 10
+    # a second format call gives the same texts; values agree with the texts' numbers
+    assert api.format_elliptic(F, alk, mass_radius=False) == files[:6]
+    v = api.elliptic_values(len(live))
+    assert np.array_equal(v[:6].view(np.int64), want.view(np.int64))
+    assert np.array_equal(v[6], b[live, 6]) and np.array_equal(v[7], b[live, 7])
+
+
+def test_format_elliptic_out_of_range_values(gpu, port):
+    """A value beyond the formatter's range (a = R / 2 = 5e29 for a far body at
+    rest): NCGPU_E_UNSUPPORTED, and the values are there for the caller to
+    print, equal to cart2ell's."""
+    from ncorpion_b200 import api as A
+    from conftest import elliptic_cases
+    b, ex, cm = elliptic_cases(200, seed=7)
+    b[6, :3] = cm[:3] + np.array([1e30, 0.0, 0.0])
+    b[6, 3:6] = cm[3:6]
+    api = gpu(256)
+    p = make_params()
+    api.upload(b, ex, cm)
+    yx, hidx, hrec, F, alk = _elliptic_on_device(api, port, b, ex, cm, p, 0.0, False)
+    with pytest.raises(A.NcgpuError) as e:
+        api.format_elliptic(F, alk)
+    assert e.value.status == A.E_UNSUPPORTED
+    live = np.flatnonzero(ex)
+    v = api.elliptic_values(len(live))
+    want = port.cart2ell_all(b, ex, cm, 1.0, p, 0.0)
+    assert np.array_equal(v[:6].view(np.int64), want.view(np.int64))
+    assert v[0, 6] == 5e29
+
+
+def test_elliptic_state_rules(gpu):
+    """format_elliptic needs a begin first and the same listed-body count."""
+    from ncorpion_b200 import api as A
+    from conftest import elliptic_cases
+    b, ex, cm = elliptic_cases(100, seed=8)
+    api = gpu(128)
+    api.upload(b, ex, cm)
+    with pytest.raises(A.NcgpuError) as e:
+        api.format_elliptic(np.zeros(int(ex.sum())), np.zeros((0, 6)))
+    assert e.value.status == A.E_STATE
+    yx, hidx, hrec = api.elliptic_begin(1.0)
+    assert len(hidx) > 0
+    with pytest.raises(A.NcgpuError) as e:
+        api.format_elliptic(np.zeros(len(yx)), np.zeros((0, 6)))
+    assert e.value.status == A.E_ARG
