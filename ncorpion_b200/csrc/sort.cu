@@ -71,26 +71,30 @@ __global__ void k_scatter_flags(const int *__restrict__ ex, int n, const int *__
 
 // ---- radix sort -------------------------------------------------------------
 constexpr int RT = 256;           // threads per block
-constexpr int RK = 8;             // keys per thread
-constexpr int RB = RT * RK;       // keys per block
+constexpr int RK = 8;             // keys per thread (large sorts; small ones take fewer, RK_ template)
 constexpr int RADIX = 256;
 
+// Per-block digit counts: hist[digit][block] (digit-major, the order of the
+// global offsets a scan gives), or hist[block][digit] when block_major (read by
+// k_radix_scatter_inline, one coalesced row per block).
+template <int RK_>
 __global__ void k_radix_hist(const uint32_t *__restrict__ keys, int n, int shift,
-                             int *__restrict__ hist, int nblocks)
+                             int *__restrict__ hist, int nblocks, bool block_major)
 {
       __shared__ int h[RADIX];
       h[threadIdx.x] = 0;
       __syncthreads();
-      int base = blockIdx.x * RB;
+      int base = blockIdx.x * RT * RK_;
 #pragma unroll
-      for (int r = 0; r < RK; r++) {
+      for (int r = 0; r < RK_; r++) {
             int i = base + r * RT + threadIdx.x;
             if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xffu], 1);
       }
       __syncthreads();
-      hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+      hist[block_major ? blockIdx.x * RADIX + threadIdx.x : threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
+template <int RK_>
 __global__ void k_radix_scatter(const uint32_t *__restrict__ kin, const int *__restrict__ vin,
                                 uint32_t *__restrict__ kout, int *__restrict__ vout, int n,
                                 int shift, const int *__restrict__ hist, int nblocks)
@@ -101,19 +105,24 @@ __global__ void k_radix_scatter(const uint32_t *__restrict__ kin, const int *__r
       int t = threadIdx.x, lane = t & 31, w = t >> 5;
       run[t] = 0;
       gofs[t] = hist[t * nblocks + blockIdx.x];
-      int base = blockIdx.x * RB;
-      for (int r = 0; r < RK; r++) {
+      int base = blockIdx.x * RT * RK_;
+      // the thread's keys and values of all rounds, loaded up front (independent loads)
+      uint32_t kr[RK_];
+      int vr[RK_];
+#pragma unroll
+      for (int r = 0; r < RK_; r++) {
+            const int i = base + r * RT + t;
+            kr[r] = i < n ? kin[i] : 0u;
+            vr[r] = i < n ? vin[i] : 0;
+      }
+#pragma unroll
+      for (int r = 0; r < RK_; r++) {
             for (int q = 0; q < RT / 32; q++) wc[q][t] = 0;
             __syncthreads();
-            int i = base + r * RT + t;
-            uint32_t key = 0;
-            int val = 0;
-            int d = RADIX;  // sentinel: no key
-            if (i < n) {
-                  key = kin[i];
-                  val = vin[i];
-                  d = (key >> shift) & 0xffu;
-            }
+            const int i = base + r * RT + t;
+            const uint32_t key = kr[r];
+            const int val = vr[r];
+            const int d = i < n ? (int)((key >> shift) & 0xffu) : RADIX;  // RADIX: no key
             unsigned peers = __match_any_sync(0xffffffffu, d);
             int rk = __popc(peers & ((1u << lane) - 1u));
             int leader = __ffs(peers) - 1;
@@ -139,10 +148,11 @@ __global__ void k_radix_scatter(const uint32_t *__restrict__ kin, const int *__r
       }
 }
 
-// k_radix_scatter for a few blocks (n up to 64 RB keys): each block finds its
+// k_radix_scatter for up to 128 blocks: each block finds its
 // digits' global offsets from the unscanned histograms itself (the totals of
 // every digit over all blocks, scanned across the block's 256 threads, plus the
 // counts of the blocks before it), which saves the histogram scan's launches.
+template <int RK_>
 __global__ void k_radix_scatter_inline(const uint32_t *__restrict__ kin, const int *__restrict__ vin,
                                        uint32_t *__restrict__ kout, int *__restrict__ vout, int n, int shift,
                                        const int *__restrict__ hist, int nblocks)
@@ -153,8 +163,9 @@ __global__ void k_radix_scatter_inline(const uint32_t *__restrict__ kin, const i
       __shared__ int wsum[RT / 32];
       int t = threadIdx.x, lane = t & 31, w = t >> 5;
       int tot = 0, pre = 0;
-      for (int b = 0; b < nblocks; b++) {
-            const int v = hist[t * nblocks + b];
+#pragma unroll 8
+      for (int b = 0; b < nblocks; b++) {  // block-major: one coalesced row per block
+            const int v = hist[b * RADIX + t];
             tot += v;
             if (b < (int)blockIdx.x) pre += v;
       }
@@ -169,19 +180,24 @@ __global__ void k_radix_scatter_inline(const uint32_t *__restrict__ kin, const i
       for (int q = 0; q < w; q++) before += wsum[q];
       gofs[t] = before + x - tot + pre;
       run[t] = 0;
-      int base = blockIdx.x * RB;
-      for (int r = 0; r < RK; r++) {
+      int base = blockIdx.x * RT * RK_;
+      // the thread's keys and values of all rounds, loaded up front (independent loads)
+      uint32_t kr[RK_];
+      int vr[RK_];
+#pragma unroll
+      for (int r = 0; r < RK_; r++) {
+            const int i = base + r * RT + t;
+            kr[r] = i < n ? kin[i] : 0u;
+            vr[r] = i < n ? vin[i] : 0;
+      }
+#pragma unroll
+      for (int r = 0; r < RK_; r++) {
             for (int q = 0; q < RT / 32; q++) wc[q][t] = 0;
             __syncthreads();
-            int i = base + r * RT + t;
-            uint32_t key = 0;
-            int val = 0;
-            int d = RADIX;  // sentinel: no key
-            if (i < n) {
-                  key = kin[i];
-                  val = vin[i];
-                  d = (key >> shift) & 0xffu;
-            }
+            const int i = base + r * RT + t;
+            const uint32_t key = kr[r];
+            const int val = vr[r];
+            const int d = i < n ? (int)((key >> shift) & 0xffu) : RADIX;  // RADIX: no key
             unsigned peers = __match_any_sync(0xffffffffu, d);
             int rk = __popc(peers & ((1u << lane) - 1u));
             int leader = __ffs(peers) - 1;
@@ -303,7 +319,16 @@ int radix_sort_pairs(uint32_t *keys, int *vals, int n, int bits, cudaStream_t st
 {
       Ctx &c = ctx();
       if (n <= 1) return NCGPU_OK;
-      int nb = (n + RB - 1) / RB;
+      // keys per thread: the fewest (1, 2, 4) that keep a small sort within 128
+      // blocks, else 8; up to 128 blocks the scatter scans the histograms itself
+      // (two launches a pass), beyond that a scan runs between the two kernels
+      int kpt = RK;
+      for (int k = 1; k < RK; k <<= 1)
+            if ((n + RT * k - 1) / (RT * k) <= 128) {
+                  kpt = k;
+                  break;
+            }
+      const int nb = (n + RT * kpt - 1) / (RT * kpt);
       size_t need = (size_t)RADIX * nb;
       if (need > c.hist_cap) return NCGPU_E_CAPACITY;
       uint32_t *ka = keys, *kb = c.keys2;
@@ -312,16 +337,23 @@ int radix_sort_pairs(uint32_t *keys, int *vals, int n, int bits, cudaStream_t st
       int passes = (bits + 7) / 8;
       for (int p = 0; p < passes; p++) {
             int shift = 8 * p;
-            k_radix_hist<<<nb, RT, 0, st>>>(ka, n, shift, c.hist, nb);
-            NCG_LAUNCHED();
-            if (nb <= 64) {  // two launches a pass: the scatter scans the histograms itself
-                  k_radix_scatter_inline<<<nb, RT, 0, st>>>(ka, va, kb, vb, n, shift, c.hist, nb);
-                  NCG_LAUNCHED();
-            } else {
-                  NCG_TRY(scan_exclusive(c.hist, c.hist, (int)need, c.cnt, st));
-                  k_radix_scatter<<<nb, RT, 0, st>>>(ka, va, kb, vb, n, shift, c.hist, nb);
-                  NCG_LAUNCHED();
-            }
+#define NCG_RADIX_PASS(K)                                                                       \
+      do {                                                                                      \
+            k_radix_hist<K><<<nb, RT, 0, st>>>(ka, n, shift, c.hist, nb, nb <= 128);           \
+            NCG_LAUNCHED();                                                                     \
+            if (nb <= 128) {                                                                    \
+                  k_radix_scatter_inline<K><<<nb, RT, 0, st>>>(ka, va, kb, vb, n, shift, c.hist, nb); \
+            } else {                                                                            \
+                  NCG_TRY(scan_exclusive(c.hist, c.hist, (int)need, c.cnt, st));                \
+                  k_radix_scatter<K><<<nb, RT, 0, st>>>(ka, va, kb, vb, n, shift, c.hist, nb);  \
+            }                                                                                   \
+            NCG_LAUNCHED();                                                                     \
+      } while (0)
+            if (kpt == 1) NCG_RADIX_PASS(1);
+            else if (kpt == 2) NCG_RADIX_PASS(2);
+            else if (kpt == 4) NCG_RADIX_PASS(4);
+            else NCG_RADIX_PASS(RK);
+#undef NCG_RADIX_PASS
             uint32_t *tk = ka; ka = kb; kb = tk;
             int *tv = va; va = vb; vb = tv;
       }
