@@ -641,6 +641,7 @@ def mesh_kernel_times(prof, n, calls):
         if e.device_type.name != "CUDA":
             continue
         k = e.name.replace("(anonymous namespace)::", "").replace("ncg::", "").replace("void ", "").split("(")[0]
+        k = k.split("<")[0]  # template arguments apart
         c = tot.setdefault(k, [0, 0.0])
         c[0] += 1
         c[1] += e.device_time_total
