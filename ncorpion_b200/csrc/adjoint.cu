@@ -251,17 +251,17 @@ __global__ void __launch_bounds__(AT) k_pairs_mx(Src s, int n, int tpc, const do
                   const f2 XT = f2_pack(xr, xr), YT = f2_pack(yr, yr), ZT = f2_pack(zr, zr), RT = f2_pack(rkf, rkf);
                   const f2 MK = f2_pack(mkf, mkf), NLX = f2_pack(-lxkf, -lxkf), NLY = f2_pack(-lykf, -lykf),
                            NLZ = f2_pack(-lzkf, -lzkf), NEG3 = f2_pack(-3.f, -3.f);
-                  const int ce = (cnt + 1) & ~1;
+                  // sources q, q + 1 packed, four per 128-bit shared load (a far tile is
+                  // padded with far, massless sources up to a multiple of four)
+                  const int ce = (cnt + 3) & ~3;
                   for (int q0 = 0; q0 < ce; q0 += 64) {
                         f2 P0 = 0ull, P1 = 0ull, P2 = 0ull, P3 = 0ull;
                         const int qe = min(ce, q0 + 64);
-#pragma unroll 2
-                        for (int q = q0; q < qe; q += 2) {
-                              const f2 rx = f2_sub(*(const f2 *)&fx[q], XT), ry = f2_sub(*(const f2 *)&fy[q], YT);
-                              const f2 rz = f2_sub(*(const f2 *)&fz[q], ZT);
+                        auto term = [&](f2 XS, f2 YS, f2 ZS, f2 RS, f2 mj, f2 LX, f2 LY, f2 LZ) {
+                              const f2 rx = f2_sub(XS, XT), ry = f2_sub(YS, YT), rz = f2_sub(ZS, ZT);
                               f2 d2;
                               if (SOFT) {
-                                    const f2 e = f2_add(*(const f2 *)&fr[q], RT);
+                                    const f2 e = f2_add(RS, RT);
                                     d2 = f2_fma(rx, rx, f2_mul(e, e));
                               } else {
                                     d2 = f2_mul(rx, rx);
@@ -271,8 +271,6 @@ __global__ void __launch_bounds__(AT) k_pairs_mx(Src s, int n, int tpc, const do
                               const f2 ri = f2_rsqrt(d2);
                               const f2 r2i = f2_mul(ri, ri);
                               const f2 i3 = f2_mul(r2i, ri), i5 = f2_mul(i3, r2i);
-                              const f2 mj = *(const f2 *)&fm[q];
-                              const f2 LX = *(const f2 *)&flx[q], LY = *(const f2 *)&fly[q], LZ = *(const f2 *)&flz[q];
                               // w = m_k lambda_j - m_j lambda_k
                               const f2 wx = f2_fma(mj, NLX, f2_mul(MK, LX)), wy = f2_fma(mj, NLY, f2_mul(MK, LY));
                               const f2 wz = f2_fma(mj, NLZ, f2_mul(MK, LZ));
@@ -283,6 +281,17 @@ __global__ void __launch_bounds__(AT) k_pairs_mx(Src s, int n, int tpc, const do
                               P2 = f2_fma(wz, i3, f2_fma(rz, nc, P2));
                               const f2 lr = f2_fma(LZ, rz, f2_fma(LY, ry, f2_mul(LX, rx)));
                               P3 = f2_sub(P3, f2_mul(lr, i3));
+                        };
+#pragma unroll 1
+                        for (int q = q0; q < qe; q += 4) {
+                              const ulonglong2 X = *(const ulonglong2 *)&fx[q], Y = *(const ulonglong2 *)&fy[q];
+                              const ulonglong2 Z = *(const ulonglong2 *)&fz[q], M = *(const ulonglong2 *)&fm[q];
+                              const ulonglong2 LX = *(const ulonglong2 *)&flx[q], LY = *(const ulonglong2 *)&fly[q];
+                              const ulonglong2 LZ = *(const ulonglong2 *)&flz[q];
+                              ulonglong2 R = make_ulonglong2(0ull, 0ull);
+                              if (SOFT) R = *(const ulonglong2 *)&fr[q];
+                              term(X.x, Y.x, Z.x, R.x, M.x, LX.x, LY.x, LZ.x);
+                              term(X.y, Y.y, Z.y, R.y, M.y, LX.y, LY.y, LZ.y);
                         }
                         float lo, hi;
                         f2_unpack(P0, lo, hi); o0 += (double)lo + (double)hi;
