@@ -34,7 +34,8 @@ extern "C" {
                                   operation sequence: bit-identical to vector_field  */
 #define NCGPU_GRAVITY_FP64 1   /* FP64, space-filling-curve tiles, one rsqrt per pair */
 #define NCGPU_GRAVITY_MIXED 2  /* FP32 pair terms on tile-relative coordinates,
-                                  near tiles in FP64, compensated sums folded to FP64 */
+                                  near tiles in FP64, FP32 runs of 64 sources folded
+                                  into FP64 sums */
 
 /* Collision resolution types, numbered as collision_treatment's
    type_of_collision (src/physics.c:1043-1050). */
@@ -432,7 +433,9 @@ struct ncgpu_leapfrog_args {
 
 /* The brute-force integrator without collisions (src/rk4.c:873-936): half
    drift, nsteps x (kick, drift), half back-drift of the output, the central
-   mass integrated as a body.  FP64 pair sums, one rsqrt per pair. */
+   mass integrated as a body.  FP64 pair sums, one rsqrt per pair (par_gravity_mode
+   MIXED: far tile pairs in FP32).  The three calls share one device buffer, grown
+   when a call needs more and kept until ncgpu_finalize. */
 int ncgpu_leapfrog(const struct ncgpu_leapfrog_args *args);
 
 /* Reverse mode through ncgpu_leapfrog: given dL/dx_final returns dL/dx0,

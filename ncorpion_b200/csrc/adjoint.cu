@@ -332,37 +332,65 @@ __global__ void __launch_bounds__(AT) k_pairs_mx(Src s, int n, int tpc, const do
 }  // namespace
 
 namespace {
+constexpr int SB = 256;  // threads of the fold kernels and of the two-level sums
+
+// The block's sums of three per-body terms (zero past n): part[3 b + d] for
+// block b; k_sum3f then adds the blocks' sums in block order (deterministic).
+__device__ __forceinline__ void block_sum3(double v0, double v1, double v2, double *__restrict__ part)
+{
+      __shared__ double sh[3][SB];
+      sh[0][threadIdx.x] = v0;
+      sh[1][threadIdx.x] = v1;
+      sh[2][threadIdx.x] = v2;
+      __syncthreads();
+      for (int o = SB / 2; o > 0; o >>= 1) {
+            if (threadIdx.x < o)
+                  for (int d = 0; d < 3; d++) sh[d][threadIdx.x] += sh[d][threadIdx.x + o];
+            __syncthreads();
+      }
+      if (threadIdx.x < 3) part[blockIdx.x * 3 + threadIdx.x] = sh[threadIdx.x][0];
+}
+
 
 // acc = G * sum of chunk partials + central term; per-body CM_acc terms.
-__global__ void k_force_final(const double *__restrict__ part, int nch, long stride, Src s, int n,
-                              const double *__restrict__ cm, double G, double M, int central, double *ax, double *ay,
-                              double *az, double *cterm)
+__global__ void __launch_bounds__(SB) k_force_final(const double *__restrict__ part, int nch, long stride, Src s,
+                                                    int n, const double *__restrict__ cm, double G, double M,
+                                                    int central, double *ax, double *ay, double *az,
+                                                    double *__restrict__ red)
 {
-      int k = blockIdx.x * blockDim.x + threadIdx.x;
-      if (k >= n) return;
-      double a[3] = {0., 0., 0.};
-      for (int c = 0; c < nch; c++)
-            for (int d = 0; d < 3; d++) a[d] += part[(size_t)c * 3 * stride + d * stride + k];
-      for (int d = 0; d < 3; d++) a[d] *= G;
-      if (central) {
-            double sx = s.x[k] - cm[0], sy = s.y[k] - cm[1], sz = s.z[k] - cm[2];
-            double r2 = sx * sx + sy * sy + sz * sz;
-            double ri = rsqrt(r2), i3 = ri * ri * ri;
-            a[0] -= G * M * sx * i3; a[1] -= G * M * sy * i3; a[2] -= G * M * sz * i3;
-            double g = G * s.m[k] * i3;
-            cterm[k] = g * sx; cterm[n + k] = g * sy; cterm[2 * n + k] = g * sz;
+      const int k = blockIdx.x * blockDim.x + threadIdx.x;
+      double c[3] = {0., 0., 0.};
+      if (k < n) {
+            double a[3] = {0., 0., 0.};
+#pragma unroll 8  // the chunks' loads in flight together (sums still in chunk order)
+            for (int ch = 0; ch < nch; ch++)
+                  for (int d = 0; d < 3; d++) a[d] += part[(size_t)ch * 3 * stride + d * stride + k];
+            for (int d = 0; d < 3; d++) a[d] *= G;
+            if (central) {
+                  double sx = s.x[k] - cm[0], sy = s.y[k] - cm[1], sz = s.z[k] - cm[2];
+                  double r2 = sx * sx + sy * sy + sz * sz;
+                  double ri = rsqrt(r2), i3 = ri * ri * ri;
+                  a[0] -= G * M * sx * i3; a[1] -= G * M * sy * i3; a[2] -= G * M * sz * i3;
+                  double g = G * s.m[k] * i3;
+                  c[0] = g * sx; c[1] = g * sy; c[2] = g * sz;
+            }
+            ax[k] = a[0]; ay[k] = a[1]; az[k] = a[2];
       }
-      ax[k] = a[0]; ay[k] = a[1]; az[k] = a[2];
+      if (central) block_sum3(c[0], c[1], c[2], red);  // the CM_acc terms (central is uniform)
 }
 
 // VJP outputs: mu (3), nu (1) per body; per-body terms of the CM-position VJP.
-__global__ void k_vjp_final(const double *__restrict__ part, int nch, long stride, Src s, int n,
-                            const double *__restrict__ cm, const double *__restrict__ Lam, double G, double M,
-                            int central, double *mux, double *muy, double *muz, double *nu, double *xterm)
+__global__ void __launch_bounds__(SB) k_vjp_final(const double *__restrict__ part, int nch, long stride, Src s,
+                                                  int n, const double *__restrict__ cm,
+                                                  const double *__restrict__ Lam, double G, double M, int central,
+                                                  double *mux, double *muy, double *muz, double *nu,
+                                                  double *__restrict__ red)
 {
-      int k = blockIdx.x * blockDim.x + threadIdx.x;
-      if (k >= n) return;
+      const int k = blockIdx.x * blockDim.x + threadIdx.x;
+      double xt[3] = {0., 0., 0.};
+      if (k < n) {
       double o[4] = {0., 0., 0., 0.};
+#pragma unroll 8  // the chunks' loads in flight together (sums still in chunk order)
       for (int c = 0; c < nch; c++)
             for (int d = 0; d < 4; d++) o[d] += part[(size_t)c * 4 * stride + d * stride + k];
       for (int d = 0; d < 4; d++) o[d] *= G;
@@ -379,22 +407,27 @@ __global__ void k_vjp_final(const double *__restrict__ part, int nch, long strid
             for (int d = 0; d < 3; d++) Jw[d] = w[d] * i3 - 3.0 * sv[d] * sw * i5;
             for (int d = 0; d < 3; d++) {
                   o[d] += G * Jw[d];
-                  xterm[d * n + k] = -G * Jw[d];  // G J (M lambda - m Lambda)
+                  xt[d] = -G * Jw[d];  // G J (M lambda - m Lambda)
             }
             o[3] += G * (Lam[0] * sv[0] + Lam[1] * sv[1] + Lam[2] * sv[2]) * i3;
       }
       mux[k] = o[0]; muy[k] = o[1]; muz[k] = o[2]; nu[k] = o[3];
+      }
+      if (central) block_sum3(xt[0], xt[1], xt[2], red);  // the CM-position VJP's terms
 }
 
 // JVP: d a = G * sum of chunk partials - G M J_k (dx_k - dX); per-body terms
 // of d A_cm = sum_k G [dm_k s_k/|s|^3 + m_k J_k (dx_k - dX)].
-__global__ void k_jvp_final(const double *__restrict__ part, int nch, long stride, Src s, int n,
-                            const double *__restrict__ cm, const double *__restrict__ dX, double G, double M,
-                            int central, double *dax, double *day, double *daz, double *cterm)
+__global__ void __launch_bounds__(SB) k_jvp_final(const double *__restrict__ part, int nch, long stride, Src s,
+                                                  int n, const double *__restrict__ cm,
+                                                  const double *__restrict__ dX, double G, double M, int central,
+                                                  double *dax, double *day, double *daz, double *__restrict__ red)
 {
-      int k = blockIdx.x * blockDim.x + threadIdx.x;
-      if (k >= n) return;
+      const int k = blockIdx.x * blockDim.x + threadIdx.x;
+      double ct[3] = {0., 0., 0.};
+      if (k < n) {
       double o[3] = {0., 0., 0.};
+#pragma unroll 8  // the chunks' loads in flight together (sums still in chunk order)
       for (int c = 0; c < nch; c++)
             for (int d = 0; d < 3; d++) o[d] += part[(size_t)c * 3 * stride + d * stride + k];
       for (int d = 0; d < 3; d++) o[d] *= G;
@@ -409,30 +442,16 @@ __global__ void k_jvp_final(const double *__restrict__ part, int nch, long strid
             const double mk = s.m[k], dmk = s.dm[k];
             for (int d = 0; d < 3; d++) {
                   o[d] -= G * M * Ju[d];
-                  cterm[d * n + k] = G * (dmk * sv[d] * i3 + mk * Ju[d]);
+                  ct[d] = G * (dmk * sv[d] * i3 + mk * Ju[d]);
             }
       }
       dax[k] = o[0]; day[k] = o[1]; daz[k] = o[2];
-}
-
-constexpr int SB = 256;
-// out[d] = sum_k v[d*n + k], deterministic two levels (d < 3)
-__global__ void k_sum3p(const double *__restrict__ v, int n, double *__restrict__ part)
-{
-      __shared__ double sh[3][SB];
-      double a[3] = {0., 0., 0.};
-      for (int k = blockIdx.x * SB + threadIdx.x; k < n; k += gridDim.x * SB)
-            for (int d = 0; d < 3; d++) a[d] += v[(size_t)d * n + k];
-      for (int d = 0; d < 3; d++) sh[d][threadIdx.x] = a[d];
-      __syncthreads();
-      for (int o = SB / 2; o > 0; o >>= 1) {
-            if (threadIdx.x < o)
-                  for (int d = 0; d < 3; d++) sh[d][threadIdx.x] += sh[d][threadIdx.x + o];
-            __syncthreads();
       }
-      if (threadIdx.x < 3) part[blockIdx.x * 3 + threadIdx.x] = sh[threadIdx.x][0];
+      if (central) block_sum3(ct[0], ct[1], ct[2], red);  // the terms of d A_cm
 }
 
+// out[d] = the sum of the blocks' partial sums part[3 b + d] (block_sum3), in
+// block order (d < 3)
 __global__ void k_sum3f(const double *__restrict__ part, int np, double *__restrict__ out)
 {
       int d = threadIdx.x;
@@ -466,27 +485,32 @@ struct LF {
       int n, ntiles, tpc, nch, np;
       bool soft, central;
       double G, M;
-      double *X, *V, *m, *sR, *cm, *acc, *cterm, *part, *red, *acm;
-      double *lx, *lv, *LX, *LV, *mu, *nu, *gm, *xterm, *muX;
+      double *X, *V, *m, *sR, *cm, *acc, *part, *red, *acm;
+      double *lx, *lv, *LX, *LV, *mu, *nu, *gm, *muX;
       double *ckpt, *seg;
       double *tx, *tv, *tm, *tX, *da, *dA;  // tangents (JVP)
       int C, ncp;
       bool mixed;                  // MIXED gravity mode: k_pairs_mx with tile boxes
       double theta, *box;
+      double *boxseg;              // mixed mode: the tile boxes of a segment's recomputed steps
       cudaStream_t st;
 };
 
-// the pair sums of OP over positions pos (tile boxes first in the mixed mode)
+// the pair sums of OP over positions pos; the mixed mode's tile boxes in box
+// (null: L.box), computed from pos first unless `have_box`
 template <int OP>
-int lf_pairs(LF &L, const Src &s, const double *pos)
+int lf_pairs(LF &L, const Src &s, const double *pos, double *box = nullptr, bool have_box = false)
 {
       const int n = L.n;
       dim3 grid(L.nch, L.ntiles);
       if (L.mixed) {
-            k_adj_tilebox<<<(L.ntiles * 32 + 255) / 256, 256, 0, L.st>>>(pos, n, L.ntiles, L.box);
-            NCG_LAUNCHED();
-            if (L.soft) k_pairs_mx<OP, true><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.box, L.theta, L.part, n);
-            else k_pairs_mx<OP, false><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.box, L.theta, L.part, n);
+            if (!box) box = L.box;
+            if (!have_box) {
+                  k_adj_tilebox<<<(L.ntiles * 32 + 255) / 256, 256, 0, L.st>>>(pos, n, L.ntiles, box);
+                  NCG_LAUNCHED();
+            }
+            if (L.soft) k_pairs_mx<OP, true><<<grid, AT, 0, L.st>>>(s, n, L.tpc, box, L.theta, L.part, n);
+            else k_pairs_mx<OP, false><<<grid, AT, 0, L.st>>>(s, n, L.tpc, box, L.theta, L.part, n);
       } else {
             if (L.soft) k_pairs<OP, true><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
             else k_pairs<OP, false><<<grid, AT, 0, L.st>>>(s, n, L.tpc, L.part, n);
@@ -495,27 +519,27 @@ int lf_pairs(LF &L, const Src &s, const double *pos)
       return NCGPU_OK;
 }
 
-int lf_force(LF &L, const double *pos, const double *cmpos)
+int lf_force(LF &L, const double *pos, const double *cmpos, double *box = nullptr)
 {
       const int n = L.n;
       Src s{pos, pos + n, pos + 2 * n, L.m, L.sR, nullptr, nullptr, nullptr};
-      NCG_TRY(lf_pairs<0>(L, s, pos));
-      k_force_final<<<(n + 255) / 256, 256, 0, L.st>>>(L.part, L.nch, n, s, n, cmpos, L.G, L.M, L.central, L.acc,
-                                                       L.acc + n, L.acc + 2 * n, L.cterm);
+      NCG_TRY(lf_pairs<0>(L, s, pos, box));
+      const int nb = (n + SB - 1) / SB;
+      k_force_final<<<nb, SB, 0, L.st>>>(L.part, L.nch, n, s, n, cmpos, L.G, L.M, L.central, L.acc, L.acc + n,
+                                         L.acc + 2 * n, L.red);
       NCG_LAUNCHED();
       if (L.central) {
-            k_sum3p<<<L.np, SB, 0, L.st>>>(L.cterm, n, L.red);
-            NCG_LAUNCHED();
-            k_sum3f<<<1, 32, 0, L.st>>>(L.red, L.np, L.acm);
+            k_sum3f<<<1, 32, 0, L.st>>>(L.red, nb, L.acm);
             NCG_LAUNCHED();
       }
       return NCGPU_OK;
 }
 
-// kick (v += dt a, CM too) then drift (x += dt v, CM too)
-int lf_step(LF &L, double dt)
+// kick (v += dt a, CM too) then drift (x += dt v, CM too); box: where the
+// force's tile boxes go (null: L.box)
+int lf_step(LF &L, double dt, double *box = nullptr)
 {
-      NCG_TRY(lf_force(L, L.X, L.cm));
+      NCG_TRY(lf_force(L, L.X, L.cm, box));
       const int n = L.n, nb = (n + 255) / 256;
       k_axpy3<<<nb, 256, 0, L.st>>>(dt, L.acc, L.V, n, n, L.acm, L.central ? L.cm + 3 : nullptr);
       NCG_LAUNCHED();
@@ -524,18 +548,18 @@ int lf_step(LF &L, double dt)
       return NCGPU_OK;
 }
 
-int lf_vjp(LF &L, const double *pos, const double *cmpos)
+// box: the tile boxes of pos when known (null: computed)
+int lf_vjp(LF &L, const double *pos, const double *cmpos, double *box = nullptr)
 {
       const int n = L.n;
       Src s{pos, pos + n, pos + 2 * n, L.m, L.sR, L.lv, L.lv + n, L.lv + 2 * n};
-      NCG_TRY(lf_pairs<1>(L, s, pos));
-      k_vjp_final<<<(n + 255) / 256, 256, 0, L.st>>>(L.part, L.nch, n, s, n, cmpos, L.LV, L.G, L.M, L.central, L.mu,
-                                                     L.mu + n, L.mu + 2 * n, L.nu, L.xterm);
+      NCG_TRY(lf_pairs<1>(L, s, pos, box, box != nullptr));
+      const int nb = (n + SB - 1) / SB;
+      k_vjp_final<<<nb, SB, 0, L.st>>>(L.part, L.nch, n, s, n, cmpos, L.LV, L.G, L.M, L.central, L.mu, L.mu + n,
+                                       L.mu + 2 * n, L.nu, L.red);
       NCG_LAUNCHED();
       if (L.central) {
-            k_sum3p<<<L.np, SB, 0, L.st>>>(L.xterm, n, L.red);
-            NCG_LAUNCHED();
-            k_sum3f<<<1, 32, 0, L.st>>>(L.red, L.np, L.muX);
+            k_sum3f<<<1, 32, 0, L.st>>>(L.red, nb, L.muX);
             NCG_LAUNCHED();
       }
       return NCGPU_OK;
@@ -548,13 +572,12 @@ int lf_step_jvp(LF &L, double dt)
       NCG_TRY(lf_force(L, L.X, L.cm));
       Src s{L.X, L.X + n, L.X + 2 * n, L.m, L.sR, L.tx, L.tx + n, L.tx + 2 * n, L.tm};
       NCG_TRY(lf_pairs<2>(L, s, L.X));
-      k_jvp_final<<<nb, 256, 0, L.st>>>(L.part, L.nch, n, s, n, L.cm, L.tX, L.G, L.M, L.central, L.da, L.da + n,
-                                        L.da + 2 * n, L.xterm);
+      const int nbs = (n + SB - 1) / SB;
+      k_jvp_final<<<nbs, SB, 0, L.st>>>(L.part, L.nch, n, s, n, L.cm, L.tX, L.G, L.M, L.central, L.da, L.da + n,
+                                        L.da + 2 * n, L.red);
       NCG_LAUNCHED();
       if (L.central) {
-            k_sum3p<<<L.np, SB, 0, L.st>>>(L.xterm, n, L.red);
-            NCG_LAUNCHED();
-            k_sum3f<<<1, 32, 0, L.st>>>(L.red, L.np, L.dA);
+            k_sum3f<<<1, 32, 0, L.st>>>(L.red, nbs, L.dA);
             NCG_LAUNCHED();
       }
       k_axpy3<<<nb, 256, 0, L.st>>>(dt, L.acc, L.V, n, n, L.acm, L.central ? L.cm + 3 : nullptr);
@@ -626,29 +649,36 @@ int lf_core(const struct ncgpu_leapfrog_args *a, int mode, bool mixed)
       }
       L.tpc = (L.ntiles + L.nch - 1) / L.nch;
       L.nch = (L.ntiles + L.tpc - 1) / L.tpc;
-      L.np = std::min(128, (n + SB - 1) / SB);
+      L.np = (n + SB - 1) / SB;  // blocks of the fold kernels: their CM sums in red
       L.mixed = mixed;
       L.theta = c.P.par_near_theta > 0. ? c.P.par_near_theta : 0.15;
       L.C = a->checkpoint > 0 ? a->checkpoint : 32;
       L.ncp = (a->nsteps + L.C - 1) / L.C + 1;
       const size_t N = (size_t)n, st = 6 * N + 6;
-      size_t total = 3 * N * 2 + 2 * N + 6 + 3 * N + 3 * N + 4 * N * L.nch + 3 * 128 + 3  // X V m sR cm acc cterm part red acm
-                     + 3 * N * 2 + 6 + 3 * N + N + N + 3 * N + 3                     // lx lv LX LV mu nu gm xterm muX
+      size_t total = 3 * N * 2 + 2 * N + 6 + 3 * N + 4 * N * L.nch + 3 * (size_t)L.np + 3  // X V m sR cm acc part red acm
+                     + 3 * N * 2 + 6 + 3 * N + N + N + 3                              // lx lv LX LV mu nu gm muX
                      + st * L.ncp + (size_t)L.C * (3 * N + 3)                         // checkpoints, segment
                      + 3 * N * 3 + N + 6 + 3                                          // tx tv tm tX da dA
-                     + 6 * (size_t)L.ntiles;                                          // tile boxes
-      double *buf = nullptr;
-      NCG_CK(cudaMalloc(&buf, total * sizeof(double)));
-      double *p = buf;
+                     + 6 * (size_t)L.ntiles                                           // tile boxes
+                     + (mixed && vjp ? 6 * (size_t)L.ntiles * L.C : 0);               // a segment's boxes
+      if (total > c.lf_cap) {  // grown when needed, kept for the next call
+            if (c.lf_buf) cudaFree(c.lf_buf);
+            c.lf_buf = nullptr;
+            c.lf_cap = 0;
+            NCG_CK(cudaMalloc(&c.lf_buf, total * sizeof(double)));
+            c.lf_cap = total;
+      }
+      double *p = c.lf_buf;
       auto take = [&](size_t k) { double *q = p; p += k; return q; };
       L.X = take(3 * N); L.V = take(3 * N); L.m = take(N); L.sR = take(N); L.cm = take(6);
-      L.acc = take(3 * N); L.cterm = take(3 * N); L.part = take(4 * N * L.nch); L.red = take(3 * 128);
+      L.acc = take(3 * N); L.part = take(4 * N * L.nch); L.red = take(3 * (size_t)L.np);
       L.acm = take(3);
       L.lx = take(3 * N); L.lv = take(3 * N); L.LX = take(3); L.LV = take(3); L.mu = take(3 * N); L.nu = take(N);
-      L.gm = take(N); L.xterm = take(3 * N); L.muX = take(3);
+      L.gm = take(N); L.muX = take(3);
       L.ckpt = take(st * L.ncp); L.seg = take((size_t)L.C * (3 * N + 3));
       L.tx = take(3 * N); L.tv = take(3 * N); L.tm = take(N); L.tX = take(6); L.da = take(3 * N); L.dA = take(3);
       L.box = take(6 * (size_t)L.ntiles);
+      L.boxseg = take(mixed && vjp ? 6 * (size_t)L.ntiles * L.C : 0);
       int status = NCGPU_OK;
       cudaError_t e = cudaSuccess;
       const double h = a->dt / 2.0, dt = a->dt;
@@ -659,10 +689,7 @@ int lf_core(const struct ncgpu_leapfrog_args *a, int mode, bool mixed)
       if (e == cudaSuccess) e = cudaMemcpyAsync(L.sR, a->R, sizeof(double) * N, cudaMemcpyHostToDevice, L.st);
       if (e == cudaSuccess) e = cudaMemcpyAsync(L.cm, a->cm, 6 * sizeof(double), cudaMemcpyHostToDevice, L.st);
       if (e == cudaSuccess) e = cudaMemsetAsync(L.acm, 0, 3 * sizeof(double), L.st);
-      if (e != cudaSuccess) {
-            cudaFree(buf);
-            return cuda_fail(e, "leapfrog upload", __FILE__, __LINE__);
-      }
+      if (e != cudaSuccess) return cuda_fail(e, "leapfrog upload", __FILE__, __LINE__);
 #define LF_TRY(call)                         \
       do {                                   \
             if ((status = (call)) != NCGPU_OK) goto done; \
@@ -732,7 +759,7 @@ int lf_core(const struct ncgpu_leapfrog_args *a, int mode, bool mixed)
                         e = cudaMemcpyAsync(sg, L.X, sizeof(double) * 3 * N, cudaMemcpyDeviceToDevice, L.st);
                         if (e == cudaSuccess) e = cudaMemcpyAsync(sg + 3 * N, L.cm, 3 * sizeof(double), cudaMemcpyDeviceToDevice, L.st);
                         if (e != cudaSuccess) { status = cuda_fail(e, "segment", __FILE__, __LINE__); goto done; }
-                        LF_TRY(lf_step(L, dt));
+                        LF_TRY(lf_step(L, dt, L.mixed ? L.boxseg + (size_t)(s - s0) * 6 * L.ntiles : nullptr));
                   }
                   for (int s = s1 - 1; s >= s0; s--) {
                         const double *sg = L.seg + (size_t)(s - s0) * (3 * N + 3);
@@ -740,7 +767,8 @@ int lf_core(const struct ncgpu_leapfrog_args *a, int mode, bool mixed)
                         k_axpy3<<<nb, 256, 0, L.st>>>(dt, L.lx, L.lv, n, n, L.LX, L.LV);
                         LF_LAUNCHED();
                         // kick v_{s+1} = v_s + dt a(x_s)
-                        LF_TRY(lf_vjp(L, sg, sg + 3 * N));
+                        // (the recomputation's boxes of these positions)
+                        LF_TRY(lf_vjp(L, sg, sg + 3 * N, L.mixed ? L.boxseg + (size_t)(s - s0) * 6 * L.ntiles : nullptr));
                         k_axpy3<<<nb, 256, 0, L.st>>>(dt, L.mu, L.lx, n, n, L.muX, L.central ? L.LX : nullptr);
                         LF_LAUNCHED();
                         k_axpy1<<<nb, 256, 0, L.st>>>(dt, L.nu, L.gm, n);
@@ -760,7 +788,6 @@ int lf_core(const struct ncgpu_leapfrog_args *a, int mode, bool mixed)
 #undef LF_LAUNCHED
 done:
       cudaStreamSynchronize(L.st);
-      cudaFree(buf);
       return status;
 }
 

@@ -71,7 +71,7 @@ void free_all()
                       c.keys, c.keys2, c.vals, c.vals2, c.hist, c.red, c.err, c.aos, c.exs,
                       c.did, c.dirty, c.dlist, c.free_idx, c.scal, c.hi, c.hj, c.ev, c.evrec,
                       c.snap[0], c.snap[1], c.snap[2], c.snap[3], c.snap[4], c.snap[5], c.snap[6], c.snap[7],
-                      c.snap_cm, c.fmt_slots, c.fmt_text, c.fmt_len, c.ell, c.ell_code, c.ell_list};
+                      c.snap_cm, c.fmt_slots, c.fmt_text, c.fmt_len, c.ell, c.ell_code, c.ell_list, c.lf_buf};
       for (void *p : ptrs)
             if (p) cudaFree(p);
       if (c.pinned) cudaFreeHost(c.pinned);

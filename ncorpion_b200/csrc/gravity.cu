@@ -604,8 +604,11 @@ __global__ void k_grav_final(const double *__restrict__ partial, int nchunks, lo
       if (q >= n) return;
       const bool own = q >= q_lo && q < q_hi;  // this part's targets (sorted order)
       double m[3] = {0., 0., 0.};
-      for (int c = 0; own && c < nchunks; c++)
-            for (int d = 0; d < 3; d++) m[d] += partial[(size_t)c * 3 * npad + d * npad + q];
+      if (own) {
+#pragma unroll 8  // the chunks' loads in flight together (sums still in chunk order)
+            for (int c = 0; c < nchunks; c++)
+                  for (int d = 0; d < 3; d++) m[d] += partial[(size_t)c * 3 * npad + d * npad + q];
+      }
       D4 s = s64[q];
       double a[3] = {G * m[0], G * m[1], G * m[2]};
       if (central) {
