@@ -88,8 +88,11 @@ __global__ void k_cell_clear(const uint32_t *__restrict__ keys, int n, int2 *__r
 
 // number of candidates of body k (lo <= k < hi): existing bodies of lower
 // index in its 27 cells; 0 outside [lo, hi)
-// Cell-ordered copy of the fields the pass reads: record q is body vals[q].
-__global__ void k_mesh_records(const DevState S, const int *__restrict__ vals, int n, MRec *__restrict__ rec)
+// Cell-ordered copy of the fields the pass reads: record q is body vals[q];
+// pv[q] is vals[q] for an existing body, INT_MAX otherwise, so that "p < k and
+// p exists" is one compact load (pv[q] < k).
+__global__ void k_mesh_records(const DevState S, const int *__restrict__ vals, int n, MRec *__restrict__ rec,
+                               int *__restrict__ pv)
 {
       int q = blockIdx.x * blockDim.x + threadIdx.x;
       if (q >= n) return;
@@ -100,6 +103,7 @@ __global__ void k_mesh_records(const DevState S, const int *__restrict__ vals, i
       r.ex = S.ex[b];
       r.did = S.did[b];
       rec[q] = r;
+      pv[q] = r.ex ? b : 0x7fffffff;
 }
 
 // The 27 neighbour cells as 9 rows of three consecutive linear indices
@@ -107,7 +111,7 @@ __global__ void k_mesh_records(const DevState S, const int *__restrict__ vals, i
 // cell slots l = 26..0 of the pop order are the rows r = 8..0, each from x + 1
 // down to x - 1.
 
-__global__ void k_mesh_count(const MRec *__restrict__ rec, const int *__restrict__ ckey,
+__global__ void k_mesh_count(const int *__restrict__ pv, const int *__restrict__ ckey,
                              const int *__restrict__ vals, const int2 *__restrict__ crange, int lid, int lo, int hi,
                              int d, long long cap, int *__restrict__ cnt)
 {
@@ -127,7 +131,7 @@ __global__ void k_mesh_count(const MRec *__restrict__ rec, const int *__restrict
                   int s, e;
                   if (!row_range(crange, mid, cap, &s, &e)) continue;
                   for (int q = s; q < e; ++q)
-                        if (vals[q] < k && rec[q].ex) c++;  // a body removed earlier in the pass is not pushed
+                        if (pv[q] < k) c++;  // (a body removed earlier in the pass is not pushed)
             }
       }
       cnt[k] = c;
@@ -151,7 +155,8 @@ constexpr int MWW = 4;   // warps per block
 constexpr int MWQ = 32;  // queued entries per lane and round
 
 __global__ void __launch_bounds__(MWW * 32) k_mesh_write(const MRec *__restrict__ rec, const int *__restrict__ ckey,
-                                                        const int *__restrict__ vals, const int2 *__restrict__ crange,
+                                                        const int *__restrict__ vals, const int *__restrict__ pv,
+                                                        const int2 *__restrict__ crange,
                                                         const int *__restrict__ off, int lid, int lo, int hi, int d,
                                                         long long cap, double dt, int test, int *__restrict__ ck,
                                                         int *__restrict__ cp, unsigned char *__restrict__ cflag,
@@ -217,8 +222,8 @@ __global__ void __launch_bounds__(MWW * 32) k_mesh_write(const MRec *__restrict_
                         o = owner[w][fi];
                         q = qb[w][o * MWQ + fi - pre[w][o]];
                         kk = okk[w][o] & 0x7fffffff;
-                        p = vals[q];
-                        cand = p < kk && rec[q].ex;  // a body removed earlier in the pass is not pushed
+                        p = pv[q];
+                        cand = p < kk;  // (a body removed earlier in the pass is not pushed)
                   }
                   const unsigned m = __ballot_sync(0xffffffffu, cand);
                   // this entry's list starts at lane a of the round (the lists are contiguous, in lane order)
@@ -679,6 +684,7 @@ static int mesh_alloc(int d)
             size_t N = (size_t)c.n_max;
             NCG_CK(cudaMalloc(&c.mkeys, sizeof(uint32_t) * (N + 1)));
             NCG_CK(cudaMalloc(&c.mvals, sizeof(int) * N));
+            NCG_CK(cudaMalloc(&c.mpv, sizeof(int) * N));
             NCG_CK(cudaMalloc(&c.ckey, sizeof(int) * N));
             NCG_CK(cudaMalloc(&c.mcnt, sizeof(int) * (N + 1)));
             NCG_CK(cudaMalloc(&c.moff, sizeof(int) * (N + 2)));
@@ -706,7 +712,7 @@ static int mesh_alloc(int d)
 void mesh_free()
 {
       Ctx &c = ctx();
-      void *ptrs[] = {c.crange, c.mkeys, c.mvals, c.ckey, c.mcnt, c.moff, c.cand_k, c.cand_p, c.cflag, c.cpos,
+      void *ptrs[] = {c.crange, c.mkeys, c.mvals, c.mpv, c.ckey, c.mcnt, c.moff, c.cand_k, c.cand_p, c.cflag, c.cpos,
                       c.occ, c.msums, c.evx, c.xpairs, c.xhead, c.fev, c.vis, c.mrec};
       for (void *p : ptrs)
             if (p) cudaFree(p);
@@ -753,9 +759,9 @@ static int mesh_segment_launch(const DevState &S, int lid, int lo, int hi, long 
       const int nb = (n + 255) / 256;
       const int d = c.P.par_collision_cube_cells;
       MRec *rec = (MRec *)c.mrec;
-      k_mesh_records<<<nb, 256, 0, st>>>(S, c.mvals, n, rec);
+      k_mesh_records<<<nb, 256, 0, st>>>(S, c.mvals, n, rec, c.mpv);
       NCG_LAUNCHED();
-      k_mesh_count<<<nb, 256, 0, st>>>(rec, c.ckey, c.mvals, c.crange, lid, lo, hi, d,
+      k_mesh_count<<<nb, 256, 0, st>>>(c.mpv, c.ckey, c.mvals, c.crange, lid, lo, hi, d,
                                        (long long)c.cell_cap, c.mcnt);
       NCG_LAUNCHED();
       NCG_TRY(scan_exclusive(c.mcnt, c.moff, n, c.cnt, st));
@@ -766,7 +772,7 @@ static int mesh_segment_launch(const DevState &S, int lid, int lo, int hi, long 
       NCG_CK(cudaMemsetAsync(c.scal + S_NHITS, 0, sizeof(int), st));
       // (positions at or past pair_cap are not written: the kernel records the
       // overflow and the host returns NCGPU_E_CAPACITY)
-      k_mesh_write<<<(n + MWW * 32 - 1) / (MWW * 32), MWW * 32, 0, st>>>(rec, c.ckey, c.mvals, c.crange, c.moff, lid, lo, hi, d,
+      k_mesh_write<<<(n + MWW * 32 - 1) / (MWW * 32), MWW * 32, 0, st>>>(rec, c.ckey, c.mvals, c.mpv, c.crange, c.moff, lid, lo, hi, d,
                                        (long long)c.cell_cap, c.dt, test, c.cand_k, c.cand_p, c.cflag, c.hi, c.hit_cap,
                                        c.scal + S_NHITS, c.pair_cap, c.err);
       NCG_LAUNCHED();
