@@ -350,6 +350,7 @@ struct Ctx {
       uint32_t *mkeys = nullptr;   // cell index per sorted body (n + 1, sentinel)
       int *mvals = nullptr;        // body index per sorted position
       int *mpv = nullptr;          // per sorted position: the body index if it exists, else INT_MAX
+      double *gpart = nullptr;     // mesh gravity: per sorted position x, y, z, partner mass (4 doubles)
       double *lf_buf = nullptr;    // the differentiable leapfrog's buffers (kept between calls)
       size_t lf_cap = 0;           // doubles
       int *ckey = nullptr;         // insertion cell per slot (-1: not inserted)

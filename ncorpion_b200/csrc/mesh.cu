@@ -705,6 +705,7 @@ static int mesh_alloc(int d)
             NCG_CK(cudaMalloc(&c.fev, sizeof(int) * (size_t)c.ev_cap));
             NCG_CK(cudaMalloc(&c.vis, sizeof(int) * 3 * (size_t)MAX_VISITS));
             NCG_CK(cudaMalloc(&c.mrec, sizeof(MRec) * N));
+            NCG_CK(cudaMalloc(&c.gpart, 4 * sizeof(double) * N));
       }
       return NCGPU_OK;
 }
@@ -712,7 +713,7 @@ static int mesh_alloc(int d)
 void mesh_free()
 {
       Ctx &c = ctx();
-      void *ptrs[] = {c.crange, c.mkeys, c.mvals, c.mpv, c.ckey, c.mcnt, c.moff, c.cand_k, c.cand_p, c.cflag, c.cpos,
+      void *ptrs[] = {c.crange, c.mkeys, c.mvals, c.mpv, c.gpart, c.ckey, c.mcnt, c.moff, c.cand_k, c.cand_p, c.cflag, c.cpos,
                       c.occ, c.msums, c.evx, c.xpairs, c.xhead, c.fev, c.vis, c.mrec};
       for (void *p : ptrs)
             if (p) cudaFree(p);

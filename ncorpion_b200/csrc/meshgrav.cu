@@ -221,7 +221,10 @@ struct __align__(16) GRec {
       int ex, partner;
 };
 
-__global__ void k_grav_records(const DevState S, const int *__restrict__ vals, int n, GRec *__restrict__ rec)
+// gp (when not null): the partners' x, y, z and partner mass alone, 32 bytes a
+// position, which the fast walk reads for every pair term.
+__global__ void k_grav_records(const DevState S, const int *__restrict__ vals, int n, GRec *__restrict__ rec,
+                               double4 *__restrict__ gp)
 {
       int q = blockIdx.x * blockDim.x + threadIdx.x;
       if (q >= n) return;
@@ -233,6 +236,7 @@ __global__ void k_grav_records(const DevState S, const int *__restrict__ vals, i
       r.partner = (b > 2 && r.ex) ? 1 : 0;
       r.mp = r.partner ? r.m : 0.;
       rec[q] = r;
+      if (gp) gp[q] = make_double4(r.x, r.y, r.z, r.mp);
 }
 
 // pair_add with the partner's fields from its record (same operations)
@@ -515,13 +519,14 @@ __global__ void k_mesh_grav(DevState S, MGArgs A, const int *__restrict__ ckey, 
 constexpr int FGW = 4;   // warps per block
 constexpr int FGQ = 32;  // queued partners per lane and round
 
-// The partner's record (position q) against a body at (xb, yb, zb) of radius
-// Rb: the partner's x, y, z and partner mass come in two 16-byte loads of its
-// record's first 32 bytes (a zero mass for bodies that add no term).
-__device__ __forceinline__ void term_fast(double xb, double yb, double zb, double Rb, const GRec *__restrict__ grec,
-                                          int q, const MGArgs &A, double &tx, double &ty, double &tz)
+// The partner at position q against a body at (xb, yb, zb) of radius Rb: the
+// partner's x, y, z and partner mass in two 16-byte loads of the compact gp
+// array (a zero mass for bodies that add no term), its radius from its record.
+__device__ __forceinline__ void term_fast(double xb, double yb, double zb, double Rb, const double4 *__restrict__ gp,
+                                          const GRec *__restrict__ grec, int q, const MGArgs &A, double &tx,
+                                          double &ty, double &tz)
 {
-      const double2 *r = reinterpret_cast<const double2 *>(grec + q);
+      const double2 *r = reinterpret_cast<const double2 *>(gp + q);
       const double2 xy = r[0], zm = r[1];
       const double dx = xy.x - xb, dy = xy.y - yb, dz = zm.x - zb;
       double r2 = dx * dx + dy * dy + dz * dz;
@@ -539,7 +544,8 @@ __device__ __forceinline__ void term_fast(double xb, double yb, double zb, doubl
 __global__ void __launch_bounds__(FGW * 32, 8) k_mesh_grav_fast(DevState S, MGArgs A, const uint32_t *__restrict__ keys,
                                                                const int *__restrict__ vals,
                                                                const int2 *__restrict__ crange,
-                                                               const GRec *__restrict__ grec, double *__restrict__ ax,
+                                                               const GRec *__restrict__ grec,
+                                                               const double4 *__restrict__ gp, double *__restrict__ ax,
                                                                double *__restrict__ ay, double *__restrict__ az,
                                                                double *__restrict__ terms, long N)
 {
@@ -598,7 +604,7 @@ __global__ void __launch_bounds__(FGW * 32, 8) k_mesh_grav_fast(DevState S, MGAr
                         const int q = qb[w][o * FGQ + fi - pre[w][o]];
                         const double2 *ow = reinterpret_cast<const double2 *>(grec + t0 + o);
                         const double2 oxy = ow[0], oz = ow[1];
-                        term_fast(oxy.x, oxy.y, oz.x, A.soft ? grec[t0 + o].R : 0., grec, q, A, tx, ty, tz);
+                        term_fast(oxy.x, oxy.y, oz.x, A.soft ? grec[t0 + o].R : 0., gp, grec, q, A, tx, ty, tz);
                         a = max(pre[w][o] - f0, 0);
                   }
                   // segmented inclusive scan over the round (the lists are contiguous in
@@ -796,16 +802,19 @@ int mesh_gravity_state(const J2Arg &j2)
       double *ax = c.acc, *ay = c.acc + N, *az = c.acc + 2 * N;
       if (lid >= 0) {
             GRec *grec = (GRec *)c.mrec;
-            if (c.mesh_valid) {
-                  k_grav_records<<<(c.mesh_n + 255) / 256, 256, 0, st>>>(S, c.mvals, c.mesh_n, grec);
-                  NCG_LAUNCHED();
-            }
+            double4 *gp = (double4 *)c.gpart;
             // the fast modes' order-free kernel where a body's pairs are exactly its
             // 27-cell neighbours (no big bodies' visits, no fragments appended)
             const bool fast = A.cellterms && c.mesh_valid && A.nvis == 0 && A.nfev == 0 && lid == A.lid0;
+            if (c.mesh_valid) {
+                  k_grav_records<<<(c.mesh_n + 255) / 256, 256, 0, st>>>(S, c.mvals, c.mesh_n, grec,
+                                                                         fast ? gp : nullptr);
+                  NCG_LAUNCHED();
+            }
             if (fast)
                   k_mesh_grav_fast<<<(lid + FGW * 32) / (FGW * 32), FGW * 32, 0, st>>>(S, A, c.mkeys, c.mvals, c.crange,
-                                                                                     grec, ax, ay, az, c.partial, N);
+                                                                                     grec, gp, ax, ay, az, c.partial,
+                                                                                     N);
             else
                   k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.crange, c.mesh_valid,
                                                                 grec, ax, ay, az, c.partial, N);
