@@ -82,9 +82,26 @@ __global__ void k_top3_part(const DevState S, int lid, const int *__restrict__ f
       Top3 t;
       for (int q = 0; q < 3; q++) { t.R[q] = 0.; t.i[q] = -1; }
       const int start = first3[2] + 1;
-      if (first3[2] >= 0)
-            for (int j = start + blockIdx.x * TB + threadIdx.x; j <= lid; j += gridDim.x * TB)
+      if (first3[2] >= 0) {
+            // four slots a round, their loads issued together (the top three of a
+            // total order do not depend on the order of the insertions)
+            const int stride = gridDim.x * TB;
+            int j = start + blockIdx.x * TB + threadIdx.x;
+            for (; j + 3 * stride <= lid; j += 4 * stride) {
+                  int e[4];
+                  double r[4];
+#pragma unroll
+                  for (int u = 0; u < 4; u++) {
+                        e[u] = S.ex[j + u * stride];
+                        r[u] = S.R[j + u * stride];
+                  }
+#pragma unroll
+                  for (int u = 0; u < 4; u++)
+                        if (e[u]) t3_insert(t, r[u], j + u * stride);
+            }
+            for (; j <= lid; j += stride)
                   if (S.ex[j]) t3_insert(t, S.R[j], j);
+      }
       for (int q = 0; q < 3; q++) { sR[q][threadIdx.x] = t.R[q]; si[q][threadIdx.x] = t.i[q]; }
       __syncthreads();
       for (int o = TB / 2; o > 0; o >>= 1) {
@@ -315,14 +332,20 @@ __device__ __forceinline__ void tail_terms(const DevState &S, const MGArgs &A, i
 // largest bodies 0..2 (b's acceleration from them, their terms from b), with
 // the reference's operations.  Writes the per-body terms at ti; returns false
 // when the body has nothing more to add (empty slot, or one of bodies 0..2).
+// tv (when not null): the body's terms of the 12 chains (bodies 0..2's
+// components, then CM_acc's, the J2 term added to the central one) returned
+// instead of stored in terms; zero where the body adds none.
 __device__ __forceinline__ bool body_prologue(const DevState &S, const MGArgs &A, const GRec &me, int b, long ti,
                                               double *__restrict__ terms, long N, double *__restrict__ ax,
                                               double *__restrict__ ay, double *__restrict__ az, double &a_x,
-                                              double &a_y, double &a_z)
+                                              double &a_y, double &a_z, double *tv = nullptr)
 {
       const int f = A.j2.on ? 2 : 1;
       a_x = a_y = a_z = 0.;
+      if (tv)
+            for (int w = 0; w < 12; w++) tv[w] = 0.;
       if (!me.ex) {
+            if (tv) return false;
             // an empty slot adds +0.0 to every chain (they then read all terms
             // without looking at exists[])
             for (int w = 0; w < 9; w++) terms[(size_t)w * N + ti] = 0.;
@@ -340,18 +363,22 @@ __device__ __forceinline__ bool body_prologue(const DevState &S, const MGArgs &A
             a_y = div_by_recip(DMUL(-mu, DY), r3, y3);
             a_z = div_by_recip(DMUL(-mu, DZ), r3, y3);
             double g = DMUL(A.G, me.m);
-            cm_chain(terms, A, N, 0)[f * ti] = div_by_recip(DMUL(g, DX), r3, y3);
-            cm_chain(terms, A, N, 1)[f * ti] = div_by_recip(DMUL(g, DY), r3, y3);
-            cm_chain(terms, A, N, 2)[f * ti] = div_by_recip(DMUL(g, DZ), r3, y3);
-            if (A.j2.on) {  // src/physics.c:149-160
-                  double cj[3];
-                  d_j2(A.j2, mu, DX, DY, DZ, rk, r3, me.m, a_x, a_y, a_z, cj);
-                  for (int c = 0; c < 3; c++) cm_chain(terms, A, N, c)[2 * ti + 1] = cj[c];
+            const double cc[3] = {div_by_recip(DMUL(g, DX), r3, y3), div_by_recip(DMUL(g, DY), r3, y3),
+                                  div_by_recip(DMUL(g, DZ), r3, y3)};
+            double cj[3] = {0., 0., 0.};
+            if (A.j2.on) d_j2(A.j2, mu, DX, DY, DZ, rk, r3, me.m, a_x, a_y, a_z, cj);  // src/physics.c:149-160
+            for (int c = 0; c < 3; c++) {
+                  if (tv) {
+                        tv[9 + c] = A.j2.on ? cc[c] + cj[c] : cc[c];
+                  } else {
+                        cm_chain(terms, A, N, c)[f * ti] = cc[c];
+                        if (A.j2.on) cm_chain(terms, A, N, c)[2 * ti + 1] = cj[c];
+                  }
             }
       }
       if (b <= 2) {  // bodies 0..2: central term only here
             ax[b] = a_x; ay[b] = a_y; az[b] = a_z;
-            if (A.cellterms)  // (the parallel sums read every position)
+            if (A.cellterms && !tv)  // (the parallel sums read every position)
                   for (int w = 0; w < 9; w++) terms[(size_t)w * N + ti] = 0.;
             return false;
       }
@@ -375,9 +402,13 @@ __device__ __forceinline__ bool body_prologue(const DevState &S, const MGArgs &A
                   a_x = DADD(a_x, div_by_recip(DMUL(gi, dx), D3, y));
                   a_y = DADD(a_y, div_by_recip(DMUL(gi, dy), D3, y));
                   a_z = DADD(a_z, div_by_recip(DMUL(gi, dz), D3, y));
-                  terms[(3 * i) * N + ti] = div_by_recip(DMUL(gb, DSUB(xb, S.x[i])), D3, y);
-                  terms[(3 * i + 1) * N + ti] = div_by_recip(DMUL(gb, DSUB(yb, S.y[i])), D3, y);
-                  terms[(3 * i + 2) * N + ti] = div_by_recip(DMUL(gb, DSUB(zb, S.z[i])), D3, y);
+                  const double t3[3] = {div_by_recip(DMUL(gb, DSUB(xb, S.x[i])), D3, y),
+                                        div_by_recip(DMUL(gb, DSUB(yb, S.y[i])), D3, y),
+                                        div_by_recip(DMUL(gb, DSUB(zb, S.z[i])), D3, y)};
+                  for (int c = 0; c < 3; c++) {
+                        if (tv) tv[3 * i + c] = t3[c];
+                        else terms[(3 * i + c) * N + ti] = t3[c];
+                  }
             }
       }
       return true;
@@ -547,11 +578,13 @@ __global__ void __launch_bounds__(FGW * 32, 8) k_mesh_grav_fast(DevState S, MGAr
                                                                const GRec *__restrict__ grec,
                                                                const double4 *__restrict__ gp, double *__restrict__ ax,
                                                                double *__restrict__ ay, double *__restrict__ az,
-                                                               double *__restrict__ terms, long N)
+                                                               double *__restrict__ terms, long N,
+                                                               double *__restrict__ cpart)
 {
       __shared__ int qb[FGW][32 * FGQ];
       __shared__ unsigned char owner[FGW][32 * FGQ];
       __shared__ int pre[FGW][32];
+      __shared__ double csum[12][FGW];
       const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
       const int t = blockIdx.x * blockDim.x + threadIdx.x;  // cell order
       const int t0 = t - lane;                               // the warp's first record
@@ -562,7 +595,28 @@ __global__ void __launch_bounds__(FGW * 32, 8) k_mesh_grav_fast(DevState S, MGAr
       me.ex = 0;
       if (act) me = grec[t];
       double a_x = 0., a_y = 0., a_z = 0.;
-      bool walk = act && body_prologue(S, A, me, b, t, terms, N, ax, ay, az, a_x, a_y, a_z) && A.mutual;
+      bool walk = false;
+      {
+            // the bodies' terms of the 12 chains (bodies 0..2, CM_acc), summed over
+            // the block in a fixed shape: cpart[12 block + chain]
+            double tv[12];
+            if (act) {
+                  walk = body_prologue(S, A, me, b, t, terms, N, ax, ay, az, a_x, a_y, a_z, tv) && A.mutual;
+            } else {
+                  for (int c = 0; c < 12; c++) tv[c] = 0.;
+            }
+            for (int c = 0; c < 12; c++) {
+                  double v = tv[c];
+                  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                  if (lane == 0) csum[c][w] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x < 12) {
+                  double v = 0.;
+                  for (int q = 0; q < FGW; q++) v += csum[threadIdx.x][q];
+                  cpart[12 * (size_t)blockIdx.x + threadIdx.x] = v;
+            }
+      }
       const uint32_t L = act ? keys[t] : 0xffffffffu;
       walk = walk && L != 0xffffffffu;  // outside the collision cube: no pairs
       const long long dd = (long long)A.d * A.d;
@@ -712,17 +766,28 @@ __global__ void k_mesh_chains_part(DevState S, MGArgs A, const double *__restric
       }
 }
 
-// One warp per chain: a fixed-shape (deterministic) fold of the block partials.
-__global__ void k_mesh_chains_fold(DevState S, MGArgs A, const double *__restrict__ part, int nparts,
-                                   const double *__restrict__ ax, const double *__restrict__ ay,
-                                   const double *__restrict__ az, double *__restrict__ tot)
+// The block partials folded in a fixed shape (deterministic): thread i of
+// CHF (a multiple of 12) takes chain i % 12 of partials i / 12, i / 12 + CHF / 12,
+// ... -- consecutive threads read consecutive doubles -- and each chain's
+// CHF / 12 sums are added in order.
+constexpr int CHF = 768;
+__global__ void __launch_bounds__(CHF) k_mesh_chains_fold(DevState S, MGArgs A, const double *__restrict__ part,
+                                                         int nparts, const double *__restrict__ ax,
+                                                         const double *__restrict__ ay, const double *__restrict__ az,
+                                                         double *__restrict__ tot)
 {
-      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-      if (w >= 12) return;
+      constexpr int L = CHF / 12;
+      __shared__ double sh[12][L];
+      const int i = threadIdx.x, w = i % 12, l = i / 12;
       double s = 0.;
-      for (int b = lane; b < nparts; b += 32) s += part[12 * b + w];
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) tot[w] = chain_live(w, S, A) ? chain_init(w, ax, ay, az) + s : chain_init(w, ax, ay, az);
+      for (int b = l; b < nparts; b += L) s += part[12 * (size_t)b + w];
+      sh[w][l] = s;
+      __syncthreads();
+      if (i < 12) {
+            double v = 0.;
+            for (int q = 0; q < L; q++) v += sh[i][q];
+            tot[i] = chain_live(i, S, A) ? chain_init(i, ax, ay, az) + v : chain_init(i, ax, ay, az);
+      }
 }
 
 // CM_acc and bodies 0..2: chain totals, then the (0,1), (0,2), (1,2) pairs
@@ -791,7 +856,11 @@ int mesh_gravity_state(const J2Arg &j2)
       const int lid = c.largest_id;
       const long N = c.n_max;
       constexpr int MAXP = 1184;  // block partials of the parallel chain sums (8 per SM)
-      NCG_TRY(ensure_partial((size_t)(j2.on ? 15 : 12) * N + 12 * MAXP));
+      // (fast kernel: its blocks' chain sums after the terms' room)
+      const int nfast = lid >= 0 ? (lid + FGW * 32) / (FGW * 32) : 1;
+      NCG_TRY(ensure_partial((size_t)(j2.on ? 15 : 12) * N + 12 * (size_t)std::max(MAXP, nfast)));
+      double *cpart = c.partial + (size_t)(j2.on ? 15 : 12) * N;
+      bool fast_done = false;
       DevState S = dev_state();
       MGArgs A{lid, c.P.par_collision_cube_cells, c.P.par_central_mass_bool, c.P.par_mutual_bool,
                c.P.par_softening_parameter != 0., (long long)c.cell_cap, c.P.par_G, c.P.par_softening_parameter,
@@ -811,10 +880,10 @@ int mesh_gravity_state(const J2Arg &j2)
                                                                          fast ? gp : nullptr);
                   NCG_LAUNCHED();
             }
+            fast_done = fast;
             if (fast)
-                  k_mesh_grav_fast<<<(lid + FGW * 32) / (FGW * 32), FGW * 32, 0, st>>>(S, A, c.mkeys, c.mvals, c.crange,
-                                                                                     grec, gp, ax, ay, az, c.partial,
-                                                                                     N);
+                  k_mesh_grav_fast<<<nfast, FGW * 32, 0, st>>>(S, A, c.mkeys, c.mvals, c.crange, grec, gp, ax, ay, az,
+                                                               c.partial, N, cpart);
             else
                   k_mesh_grav<<<(lid + 256) / 256, 256, 0, st>>>(S, A, c.ckey, c.mkeys, c.mvals, c.crange, c.mesh_valid,
                                                                 grec, ax, ay, az, c.partial, N);
@@ -824,12 +893,14 @@ int mesh_gravity_state(const J2Arg &j2)
       if (c.P.par_gravity_mode == NCGPU_GRAVITY_EXACT) {
             k_mesh_chains<<<12, 32, 0, st>>>(S, A, c.partial, N, ax, ay, az, tot);
             NCG_LAUNCHED();
+      } else if (fast_done) {  // the fast kernel's block sums
+            k_mesh_chains_fold<<<1, CHF, 0, st>>>(S, A, cpart, nfast, ax, ay, az, tot);
+            NCG_LAUNCHED();
       } else {
             const int np = std::min(MAXP, std::max(1, (lid + RB12) / RB12));
-            double *part = c.partial + (size_t)(j2.on ? 15 : 12) * N;  // after the terms
-            k_mesh_chains_part<<<np, RB12, 0, st>>>(S, A, c.partial, N, part);
+            k_mesh_chains_part<<<np, RB12, 0, st>>>(S, A, c.partial, N, cpart);
             NCG_LAUNCHED();
-            k_mesh_chains_fold<<<1, 384, 0, st>>>(S, A, part, np, ax, ay, az, tot);
+            k_mesh_chains_fold<<<1, CHF, 0, st>>>(S, A, cpart, np, ax, ay, az, tot);
             NCG_LAUNCHED();
       }
       k_mesh_big3<<<1, 32, 0, st>>>(S, A, tot, ax, ay, az, c.cm_acc);
