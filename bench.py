@@ -592,7 +592,7 @@ def bench_bf_collide(lib, api, torch, cpu_ref):
     return out
 
 
-def bench_adjoint(lib, api, torch):
+def bench_adjoint(lib, api, torch, nsteps=ADJ_STEPS):
     """C4: forward + adjoint of the differentiable leapfrog (ncgpu_leapfrog_vjp:
     forward with checkpoints every 32 steps, then the reverse sweep with
     recomputation) at N=16,384 for the workload's 1,000 steps, in the MIXED
@@ -601,10 +601,10 @@ def bench_adjoint(lib, api, torch):
     from ncorpion_b200 import disks
     b, cm = disks.reduce_to_com(disks.adjoint_disk(ADJ_N, 0), np.array([0, 0, 0, 0, 0, 0, 1.0, 1.0]))
     adj = np.random.default_rng(0).normal(size=(ADJ_N, 3))
-    args = (b[:, :3], b[:, 3:6], b[:, 6], b[:, 7], cm, 1e-3, ADJ_STEPS, adj)
-    out = {"metric": "forward+adjoint leapfrog steps/s at N=16,384", "checkpoint": 32, "steps": ADJ_STEPS,
+    args = (b[:, :3], b[:, 3:6], b[:, 6], b[:, 7], cm, 1e-3, nsteps, adj)
+    out = {"metric": "forward+adjoint leapfrog steps/s at N=16,384", "checkpoint": 32, "steps": nsteps,
            "workload": "gravity-only disk, N=16,384, log-uniform masses, R=1e-2, softening 0.5 (R_k+R_p), dt=1e-3, "
-                       f"{ADJ_STEPS} steps: forward with checkpoints, reverse sweep with recomputation"}
+                       f"{nsteps} steps: forward with checkpoints, reverse sweep with recomputation"}
     for name, mode in (("mixed", api.GRAVITY_MIXED), ("fp64", api.GRAVITY_EXACT)):
         api.init(ADJ_N, api.default_params(G=1.0, softening_parameter=0.5, collision_bool=0, gravity_mode=mode))
         api.leapfrog_vjp(*args)  # warm-up: the same call (the library keeps its buffers for the next one)
@@ -617,7 +617,7 @@ def bench_adjoint(lib, api, torch):
         e1.synchronize()
         t = e0.elapsed_time(e1) / 1e3
         api.finalize()
-        out[name] = {"steps_per_s": ADJ_STEPS / t, "ms_per_step": 1e3 * t / ADJ_STEPS}
+        out[name] = {"steps_per_s": nsteps / t, "ms_per_step": 1e3 * t / nsteps}
     out["steps_per_s"] = out["mixed"]["steps_per_s"]
     out["ms_per_step"] = out["mixed"]["ms_per_step"]
     return out
@@ -693,6 +693,8 @@ def main(argv=None):
     ap.add_argument("--mesh-n", type=int, default=MESH_N, help="mesh workload bodies (smaller cases for profiling)")
     ap.add_argument("--mesh-cells", type=int, default=1024)
     ap.add_argument("--mesh-steps", type=int, default=MESH_STEPS)
+    ap.add_argument("--adj-steps", type=int, default=ADJ_STEPS,
+                    help="steps of the forward+adjoint section (the workload's 1,000; fewer for profiling)")
     ap.add_argument("--mesh-only", action="store_true",
                     help="profiling aid: only the mesh section (fast mode), its own JSON line")
     ap.add_argument("--kernel-times", action="store_true",
@@ -888,7 +890,7 @@ def main(argv=None):
                 "cpu_baseline": mesh_cpu_reference() if (rank == 0 and ws == 1 and not a.no_cpu_baseline
                                                          and a.mesh_n == MESH_N) else None}
     bf = None if a.no_bf else bench_bf_collide(lib, api, torch, rank == 0 and ws == 1 and not a.no_cpu_baseline)
-    adjoint = None if a.no_adjoint else bench_adjoint(lib, api, torch)
+    adjoint = None if a.no_adjoint else bench_adjoint(lib, api, torch, a.adj_steps)
     central = None if a.no_central else bench_central(lib, api, torch)
     output = None if a.no_output else bench_output(lib, api, torch, cpu=(rank == 0 and ws == 1 and not a.no_cpu_baseline))
     programs = bench_programs() if (rank == 0 and ws == 1 and not a.no_programs and not a.no_cpu_baseline) else None
