@@ -44,8 +44,9 @@ FLOP_PER_INTERACTION = 20  # 3 sub, 3 FMA (r^2+eps^2), rsqrt (2), 3 mul, 3 FMA a
 # (the written bytes are the per-chunk partial sums: 103 source chunks x 3 x 65,536 doubles).
 MIXED_DRAM_BYTES = 109.33e6
 # DRAM bytes of one mesh step's two main kernels (k_mesh_write + k_mesh_grav_fast) captured at N=262,144
-# (profiles/mesh_step_kernels_n262144.txt: 34.1 MB + 29.3 MB), scaled by the bodies to N=1,048,576.
-MESH_DRAM_BYTES_262K = 63.4e6
+# (profiles/mesh_step_kernels_n262144.txt, current version: 40.3 MB + 36.0 MB), scaled by the bodies to
+# N=1,048,576.
+MESH_DRAM_BYTES_262K = 76.3e6
 METRIC = "Pair-interactions/s mixed vs FP64 (rel err<1e-6); mesh collision steps/s at N=1M"
 WORKLOAD = ("gravity-only single-step accelerations, N=65,536 disk (a~U[0.8,1.2], e~Rayleigh 0.01, "
             "i~Rayleigh 0.005), masses log-uniform [1e-9,1e-6], R=1e-5, softening 0.5*(R_k+R_p)")
