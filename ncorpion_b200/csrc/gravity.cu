@@ -33,6 +33,7 @@ namespace {
 
 constexpr int T = 128;        // bodies per tile
 constexpr int EXB = 128;      // threads per block, exact kernel
+constexpr int EXACT_SMALL_N = 8192;  // up to this many bodies the exact terms are computed by whole CTAs
 constexpr int MXB = 64;       // threads per block, tiled kernels (2 targets each)
 
 struct alignas(16) D4 { double x, y, z, w; };
@@ -177,6 +178,124 @@ __global__ void __launch_bounds__(EXB) k_grav_exact(const D4 *__restrict__ src, 
             ax[slot] = own ? a_x : -0.0;
             ay[slot] = own ? a_y : -0.0;
             az[slot] = own ? a_z : -0.0;
+      }
+}
+
+// k_grav_exact for few bodies.  One thread a target leaves most of the SMs
+// idle below ~19,000 bodies (128 targets a CTA), so here a CTA holds XT
+// targets and computes their pair terms with all its threads, XS sources a
+// round, into shared memory; then one thread per target and component adds the
+// round's terms in source order.  The terms (k_grav_exact's operation
+// sequence) and the order of the additions are k_grav_exact's, so the sums
+// are bit-identical.
+constexpr int XT = 8;     // targets a CTA
+constexpr int XS = 64;    // sources a round
+constexpr int XTH = 128;  // threads a CTA: XTH / XT source lanes a target
+
+template <bool SOFT>
+__global__ void __launch_bounds__(XTH) k_grav_exact_small(const D4 *__restrict__ src, const double *__restrict__ srcR,
+                                                          const int *__restrict__ cidx, int n, double cmx, double cmy,
+                                                          double cmz, double mu, double sp, int central, J2Arg j2,
+                                                          BodyView bv, int p_lo, int p_hi, double *__restrict__ ax,
+                                                          double *__restrict__ ay, double *__restrict__ az,
+                                                          double *__restrict__ cterm)
+{
+      __shared__ double tm[3][XS][XT + 1];  // the round's terms (padded rows)
+      __shared__ D4 ss[XS];
+      __shared__ double sR[XS];
+      __shared__ double a0[3][XT];           // the targets' starting sums (central terms)
+      const int tid = threadIdx.x;
+      const int pbase = blockIdx.x * XT;
+      if (tid < XT) {
+            const int p = pbase + tid;
+            double a[3] = {0., 0., 0.};
+            if (central && p < n) {  // as k_grav_exact (src/physics.c:123-160)
+                  const D4 me = src[p];
+                  double DX = __dsub_rn(me.x, cmx), DY = __dsub_rn(me.y, cmy), DZ = __dsub_rn(me.z, cmz);
+                  double rk = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(DX, DX), __dmul_rn(DY, DY)), __dmul_rn(DZ, DZ)));
+                  double r3 = __dmul_rn(__dmul_rn(rk, rk), rk);
+                  const double y3 = __drcp_rn(r3);
+                  a[0] = div_by_recip(__dmul_rn(-mu, DX), r3, y3);
+                  a[1] = div_by_recip(__dmul_rn(-mu, DY), r3, y3);
+                  a[2] = div_by_recip(__dmul_rn(-mu, DZ), r3, y3);
+                  const int f = j2.on ? 2 : 1;
+                  const size_t nf = (size_t)f * n;
+                  cterm[f * p] = div_by_recip(__dmul_rn(me.w, DX), r3, y3);
+                  cterm[nf + f * p] = div_by_recip(__dmul_rn(me.w, DY), r3, y3);
+                  cterm[2 * nf + f * p] = div_by_recip(__dmul_rn(me.w, DZ), r3, y3);
+                  if (j2.on) {
+                        double cj[3];
+                        d_j2(j2, mu, DX, DY, DZ, rk, r3, bv.m[(long)cidx[p] * bv.stride], a[0], a[1], a[2], cj);
+                        cterm[2 * p + 1] = cj[0];
+                        cterm[nf + 2 * p + 1] = cj[1];
+                        cterm[2 * nf + 2 * p + 1] = cj[2];
+                  }
+            }
+            for (int c = 0; c < 3; c++) a0[c][tid] = a[c];
+      }
+      // the part's targets; a CTA without any writes -0.0 (the identity of the
+      // sum that combines the parts) and leaves
+      const bool any_own = pbase < n && pbase + XT > p_lo && pbase < p_hi;
+      if (!any_own) {
+            __syncthreads();
+            if (tid < XT && pbase + tid < n) {
+                  const int slot = cidx[pbase + tid];
+                  ax[slot] = -0.0; ay[slot] = -0.0; az[slot] = -0.0;
+            }
+            return;
+      }
+      // this thread's target for the terms, and (threads < 3 XT) its sum
+      const int tt = tid % XT, lane = tid / XT;
+      const int pt = pbase + tt;
+      const D4 me = src[pt < n ? pt : 0];
+      const double Ri = SOFT ? srcR[pt < n ? pt : 0] : 0.;
+      const bool summer = tid < 3 * XT;
+      const int sc = tid / XT, st = tid % XT, ps = pbase + st;
+      __syncthreads();
+      double acc = summer ? a0[sc][st] : 0.;
+      for (int j0 = 0; j0 < n; j0 += XS) {
+            if (tid < XS && j0 + tid < n) {
+                  ss[tid] = src[j0 + tid];
+                  if (SOFT) sR[tid] = srcR[j0 + tid];
+            }
+            __syncthreads();
+            for (int j = lane; j < XS; j += XTH / XT) {
+                  const int q = j0 + j;
+                  double tx = 0., ty = 0., tz = 0.;
+                  if (q < n && q != pt && pt < n) {
+                        const D4 sj = ss[j];
+                        double dx = __dsub_rn(sj.x, me.x);
+                        double dy = __dsub_rn(sj.y, me.y);
+                        double dz = __dsub_rn(sj.z, me.z);
+                        double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                        if (SOFT) {
+                              double sf = __dmul_rn(sp, __dadd_rn(Ri, sR[j]));
+                              r2 = __dadd_rn(r2, __dmul_rn(sf, sf));
+                        }
+                        double D = __dsqrt_rn(r2);
+                        double D3 = __dmul_rn(__dmul_rn(D, D), D);
+                        const double y = __drcp_rn(D3);
+                        tx = div_by_recip(__dmul_rn(sj.w, dx), D3, y);
+                        ty = div_by_recip(__dmul_rn(sj.w, dy), D3, y);
+                        tz = div_by_recip(__dmul_rn(sj.w, dz), D3, y);
+                  }
+                  tm[0][j][tt] = tx;
+                  tm[1][j][tt] = ty;
+                  tm[2][j][tt] = tz;
+            }
+            __syncthreads();
+            if (summer && ps < n) {
+                  const int je = min(XS, n - j0);
+                  for (int j = 0; j < je; ++j)
+                        if (j0 + j != ps) acc = __dadd_rn(acc, tm[sc][j][st]);
+            }
+            __syncthreads();
+      }
+      if (summer && ps < n) {
+            const bool own = ps >= p_lo && ps < p_hi;
+            const int slot = cidx[ps];
+            double *out = sc == 0 ? ax : sc == 1 ? ay : az;
+            out[slot] = own ? acc : -0.0;
       }
 }
 
@@ -764,7 +883,17 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
             int nb = (n + EXB - 1) / EXB;
             const int p_lo = (int)((long)n * part / nparts), p_hi = (int)((long)n * (part + 1) / nparts);
             NCG_CK(cudaEventRecord(c.kev0, st));
-            if (soft)
+            if (n <= EXACT_SMALL_N) {  // few bodies: the terms computed by whole CTAs
+                  const int nbs = (n + XT - 1) / XT;
+                  if (soft)
+                        k_grav_exact_small<true><<<nbs, XTH, 0, st>>>(src, c.srcR, c.cidx, n, cmh[0], cmh[1], cmh[2],
+                                                                     mu, sp, central, j2, cv, p_lo, p_hi, ax, ay, az,
+                                                                     c.cmterm);
+                  else
+                        k_grav_exact_small<false><<<nbs, XTH, 0, st>>>(src, c.srcR, c.cidx, n, cmh[0], cmh[1], cmh[2],
+                                                                      mu, sp, central, j2, cv, p_lo, p_hi, ax, ay, az,
+                                                                      c.cmterm);
+            } else if (soft)
                   k_grav_exact<true><<<nb, EXB, 0, st>>>(src, c.srcR, c.cidx, n, ntiles, cmh[0], cmh[1], cmh[2], mu,
                                                          sp, central, j2, cv, p_lo, p_hi, ax, ay, az, c.cmterm,
                                                          c.err);
