@@ -52,16 +52,35 @@ __device__ __forceinline__ void append_hit(bool hit, int i, int j, int *hi, int 
 __global__ void __launch_bounds__(BT) k_bf_hits(DevState S, int lid, double dt, int *hi, int *hj, int cap,
                                                 unsigned *err)
 {
-      int ti = blockIdx.y, tj = blockIdx.x;
+      // tile (ti, tj), tj >= ti: body i of the thread against the tile's bodies j
+      // staged in shared memory (closest_approach's test on the same values)
+      __shared__ double sj[7][BT];
+      __shared__ int sv[BT];
+      const int ti = blockIdx.y, tj = blockIdx.x;
       if (tj < ti) return;
-      int i = ti * BT + threadIdx.x;
-      bool vi = i <= lid && S.ex[i] && !S.did[i];
-      int j0 = tj * BT;
-      int jn = min(BT, lid + 1 - j0);
+      const int i = ti * BT + threadIdx.x;
+      const bool vi = i <= lid && S.ex[i] && !S.did[i];
+      double xi = 0., yi = 0., zi = 0., vxi = 0., vyi = 0., vzi = 0., Ri = 0.;
+      if (vi) {
+            xi = S.x[i]; yi = S.y[i]; zi = S.z[i]; vxi = S.vx[i]; vyi = S.vy[i]; vzi = S.vz[i]; Ri = S.R[i];
+      }
+      const int j0 = tj * BT;
+      const int jn = min(BT, lid + 1 - j0);
+      if ((int)threadIdx.x < jn) {
+            const int j = j0 + threadIdx.x;
+            sj[0][threadIdx.x] = S.x[j]; sj[1][threadIdx.x] = S.y[j]; sj[2][threadIdx.x] = S.z[j];
+            sj[3][threadIdx.x] = S.vx[j]; sj[4][threadIdx.x] = S.vy[j]; sj[5][threadIdx.x] = S.vz[j];
+            sj[6][threadIdx.x] = S.R[j];
+            sv[threadIdx.x] = S.ex[j] && !S.did[j];
+      }
+      __syncthreads();
       for (int jj = 0; jj < jn; ++jj) {
-            int j = j0 + jj;
+            const int j = j0 + jj;
             bool hit = false;
-            if (vi && j > i && S.ex[j] && !S.did[j]) hit = d_approach(S, i, j, dt, nullptr);
+            double t;
+            if (vi && j > i && sv[jj])
+                  hit = d_contact(xi, yi, zi, vxi, vyi, vzi, Ri, sj[0][jj], sj[1][jj], sj[2][jj], sj[3][jj], sj[4][jj],
+                                  sj[5][jj], sj[6][jj], dt, &t);
             append_hit(hit, i, j, hi, hj, S.scal + S_NHITS, cap, err);
       }
 }
