@@ -206,15 +206,17 @@ int kick_state()
       const int nslots = c.largest_id + 1;
       const bool mesh_grav = c.P.par_mesh_bool && !c.force_naive && !c.P.par_mesh_brute_gravity;
       // the central mass's state on the host: for the brute-force gravity's
-      // arguments and the J2 term; mesh gravity reads it from device memory
+      // arguments and the J2 term; mesh gravity, and the exact brute force on a
+      // few thousand bodies, read it from device memory
+      const bool exact_small = c.P.par_gravity_mode == NCGPU_GRAVITY_EXACT && nslots <= EXACT_SMALL_N;
       double cm9[9] = {0.};
-      if (!mesh_grav || c.P.par_J2_bool) NCG_TRY(state_cm_host(cm9));
+      if ((!mesh_grav && !exact_small) || c.P.par_J2_bool) NCG_TRY(state_cm_host(cm9));
       const J2Arg j2 = j2_arg(c.P, cm9[6], c.j2);
       if (mesh_grav)
             NCG_TRY(mesh_gravity_state(j2));
       else
             NCG_TRY(gravity_eval(state_view(), c.largest_id, cm9, j2, c.acc, c.n_max, c.cm_acc, c.P.par_gravity_mode,
-                                 c.s));
+                                 c.s, 0, 1, c.cm));
       if (c.P.par_central_tides_bool && c.P.par_central_mass_bool) NCG_TRY(tides_state(c.acc, c.n_max, c.cm_acc));
       int nb = nslots > 0 ? (nslots + 255) / 256 : 1;
       k_kick<<<nb, 256, 0, c.s>>>(c.ex, nslots, c.dt, c.acc, c.acc + c.n_max, c.acc + 2 * (size_t)c.n_max, c.vx,

@@ -434,8 +434,12 @@ int sync_scalars_h(int *h);  // device scalars into c.* and h[S_COUNT], error wo
 // Morton-ordered target blocks in the tiled modes); every other row gets -0.0
 // (+0.0 for empty slots from part 0), so that the sum over the parts is the
 // full field, bit for bit.  CM_acc is the full one in every part.
+// cm_dev (may be null): the central body in device memory; the exact mode up to
+// EXACT_SMALL_N body slots then runs without reading anything back.
+constexpr int EXACT_SMALL_N = 8192;
 int gravity_eval(const BodyView &bv, int largest_id, const double *cm_host8, const J2Arg &j2, double *d_acc,
-                 long acc_stride_block, double *d_cm_acc, int mode, cudaStream_t st, int part = 0, int nparts = 1);
+                 long acc_stride_block, double *d_cm_acc, int mode, cudaStream_t st, int part = 0, int nparts = 1,
+                 const double *cm_dev = nullptr);
 
 // Sequential FP64 sums, in index order, of the 3 arrays terms[c*n .. c*n + n),
 // starting from init[c] (0 when init is null); out may alias init.

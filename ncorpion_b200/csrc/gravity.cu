@@ -33,7 +33,6 @@ namespace {
 
 constexpr int T = 128;        // bodies per tile
 constexpr int EXB = 128;      // threads per block, exact kernel
-constexpr int EXACT_SMALL_N = 8192;  // up to this many bodies the exact terms are computed by whole CTAs
 constexpr int MXB = 64;       // threads per block, tiled kernels (2 targets each)
 
 struct alignas(16) D4 { double x, y, z, w; };
@@ -41,9 +40,10 @@ struct alignas(16) D4 { double x, y, z, w; };
 // ---------------------------------------------------------------- packing --
 
 __global__ void k_pack_exact(BodyView bv, const int *__restrict__ cidx, int n, int npad, double G,
-                             D4 *__restrict__ src, double *__restrict__ srcR)
+                             D4 *__restrict__ src, double *__restrict__ srcR, const int *__restrict__ n_dev = nullptr)
 {
       int p = blockIdx.x * blockDim.x + threadIdx.x;
+      if (n_dev) n = *n_dev;  // the count on the device (npad bounds it)
       if (p >= npad) return;
       if (p < n) {
             long s = (long)cidx[p] * bv.stride;
@@ -194,12 +194,18 @@ constexpr int XTH = 128;  // threads a CTA: XTH / XT source lanes a target
 
 template <bool SOFT>
 __global__ void __launch_bounds__(XTH) k_grav_exact_small(const D4 *__restrict__ src, const double *__restrict__ srcR,
-                                                          const int *__restrict__ cidx, int n, double cmx, double cmy,
-                                                          double cmz, double mu, double sp, int central, J2Arg j2,
-                                                          BodyView bv, int p_lo, int p_hi, double *__restrict__ ax,
-                                                          double *__restrict__ ay, double *__restrict__ az,
-                                                          double *__restrict__ cterm)
+                                                          const int *__restrict__ cidx, const int *__restrict__ n_dev,
+                                                          const double *__restrict__ cmd, double G, double sp,
+                                                          int central, J2Arg j2, BodyView bv, int part, int nparts,
+                                                          double *__restrict__ ax, double *__restrict__ ay,
+                                                          double *__restrict__ az, double *__restrict__ cterm)
 {
+      // the count and the central body from device memory (the grid covers every
+      // slot; the part's slice as the host would cut it)
+      const int n = *n_dev;
+      const int p_lo = (int)((long)n * part / nparts), p_hi = (int)((long)n * (part + 1) / nparts);
+      const double cmx = cmd[0], cmy = cmd[1], cmz = cmd[2];
+      const double mu = G * cmd[6];
       __shared__ double tm[3][XS][XT + 1];  // the round's terms (padded rows)
       __shared__ D4 ss[XS];
       __shared__ double sR[XS];
@@ -304,8 +310,9 @@ __global__ void __launch_bounds__(XTH) k_grav_exact_small(const D4 *__restrict__
 // without init), one CTA (one warp) per component, so the result matches the
 // reference bit for bit.  out may alias init.
 __global__ void __launch_bounds__(32) k_seq_sum3(const double *__restrict__ cterm, int n, const double *init,
-                                                 double *out)
+                                                 double *out, const int *__restrict__ n_dev = nullptr, int f = 1)
 {
+      if (n_dev) n = f * *n_dev;  // (f terms a body)
       __shared__ __align__(16) double stage[CHN];
       const int w = blockIdx.x;
       const double s = warp_chain_sum(cterm + (size_t)w * n, n, init ? init[w] : 0., stage);
@@ -817,7 +824,7 @@ int seq_sum3(const double *terms, int n, const double *init, double *out, cudaSt
 }
 
 int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2Arg &j2, double *d_acc, long bs,
-                 double *d_cm_acc, int mode, cudaStream_t st, int part, int nparts)
+                 double *d_cm_acc, int mode, cudaStream_t st, int part, int nparts, const double *cm_dev)
 {
       Ctx &c = ctx();
       const ncgpu_params &P = c.P;
@@ -833,6 +840,46 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
       int n = 0;
       const bool tiled = mode == NCGPU_GRAVITY_FP64 || mode == NCGPU_GRAVITY_MIXED;
       double rr[2] = {0., 0.};  // radius range of the existing bodies (tiled modes)
+      if (!tiled && nslots <= EXACT_SMALL_N) {
+            // few bodies, exact: the count stays on the device, the kernels read it
+            // (grids sized for every slot) and the central body from device memory
+            if (nslots == 0) {
+                  k_set3<<<1, 1, 0, st>>>(d_cm_acc, 0., 0., 0.);
+                  NCG_LAUNCHED();
+                  return NCGPU_OK;
+            }
+            NCG_TRY(compact_existing_dev(bv.ex, largest_id, st));
+            const double *cmd = cm_dev;
+            if (!cmd) {
+                  NCG_CK(cudaMemcpyAsync(c.red + 4064, cmh, 8 * sizeof(double), cudaMemcpyHostToDevice, st));
+                  cmd = c.red + 4064;
+            }
+            const int npad_max = (nslots + T - 1) / T * T;
+            D4 *src = (D4 *)c.src64;
+            k_pack_exact<<<(npad_max + 255) / 256, 256, 0, st>>>(bv, c.cidx, 0, npad_max, P.par_G, src, c.srcR,
+                                                                 c.n_dev);
+            NCG_LAUNCHED();
+            const double sp = P.par_softening_parameter;
+            const int central = P.par_central_mass_bool;
+            const int nbs = (nslots + XT - 1) / XT;
+            NCG_CK(cudaEventRecord(c.kev0, st));
+            if (sp != 0.)
+                  k_grav_exact_small<true><<<nbs, XTH, 0, st>>>(src, c.srcR, c.cidx, c.n_dev, cmd, P.par_G, sp, central,
+                                                               j2, bv, part, nparts, ax, ay, az, c.cmterm);
+            else
+                  k_grav_exact_small<false><<<nbs, XTH, 0, st>>>(src, c.srcR, c.cidx, c.n_dev, cmd, P.par_G, sp,
+                                                                central, j2, bv, part, nparts, ax, ay, az, c.cmterm);
+            NCG_LAUNCHED();
+            NCG_CK(cudaEventRecord(c.kev1, st));
+            c.kev_valid = 1;
+            if (central) {
+                  k_seq_sum3<<<3, 32, 0, st>>>(c.cmterm, 0, nullptr, d_cm_acc, c.n_dev, j2.on ? 2 : 1);
+            } else {
+                  k_set3<<<1, 1, 0, st>>>(d_cm_acc, 0., 0., 0.);
+            }
+            NCG_LAUNCHED();
+            return NCGPU_OK;
+      }
       if (!tiled) {
             NCG_TRY(compact_existing(bv.ex, largest_id, &n, st));
       } else if (nslots > 0) {
@@ -883,17 +930,7 @@ int gravity_eval(const BodyView &bv, int largest_id, const double *cmh, const J2
             int nb = (n + EXB - 1) / EXB;
             const int p_lo = (int)((long)n * part / nparts), p_hi = (int)((long)n * (part + 1) / nparts);
             NCG_CK(cudaEventRecord(c.kev0, st));
-            if (n <= EXACT_SMALL_N) {  // few bodies: the terms computed by whole CTAs
-                  const int nbs = (n + XT - 1) / XT;
-                  if (soft)
-                        k_grav_exact_small<true><<<nbs, XTH, 0, st>>>(src, c.srcR, c.cidx, n, cmh[0], cmh[1], cmh[2],
-                                                                     mu, sp, central, j2, cv, p_lo, p_hi, ax, ay, az,
-                                                                     c.cmterm);
-                  else
-                        k_grav_exact_small<false><<<nbs, XTH, 0, st>>>(src, c.srcR, c.cidx, n, cmh[0], cmh[1], cmh[2],
-                                                                      mu, sp, central, j2, cv, p_lo, p_hi, ax, ay, az,
-                                                                      c.cmterm);
-            } else if (soft)
+            if (soft)
                   k_grav_exact<true><<<nb, EXB, 0, st>>>(src, c.srcR, c.cidx, n, ntiles, cmh[0], cmh[1], cmh[2], mu,
                                                          sp, central, j2, cv, p_lo, p_hi, ax, ay, az, c.cmterm,
                                                          c.err);
