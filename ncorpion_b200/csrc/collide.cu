@@ -277,7 +277,10 @@ int sync_scalars_h(int *h)
       return check_err_word();  // reads, clears and maps the recorded error
 }
 
-int collide_brute_state()
+// defer: leave the scalars' read-back to the caller's next synchronisation
+// (the end of step's), for the collision types that append no body (largest_id
+// cannot change).
+int collide_brute_state(bool defer)
 {
       Ctx &c = ctx();
       cudaStream_t st = c.s;
@@ -308,6 +311,7 @@ int collide_brute_state()
       NCG_LAUNCHED();
       k_clear_dirty<<<32, 256, 0, st>>>(c.dirty, c.dlist, c.scal);
       NCG_LAUNCHED();
+      if (defer && E.type != NCGPU_COLLISION_FRAGMENTATION) return NCGPU_OK;
       return sync_scalars();
 }
 
@@ -331,7 +335,7 @@ extern "C" int ncgpu_collide_brute(int *n_events)
       Ctx &c = ctx();
       reset_launches();
       if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
-      NCG_TRY(collide_brute_state());
+      NCG_TRY(collide_brute_state(false));
       if (n_events) *n_events = c.n_events;
       return NCGPU_OK;
 }

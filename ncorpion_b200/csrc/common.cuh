@@ -351,6 +351,10 @@ struct Ctx {
       int *mvals = nullptr;        // body index per sorted position
       int *mpv = nullptr;          // per sorted position: the body index if it exists, else INT_MAX
       double *gpart = nullptr;     // mesh gravity: per sorted position x, y, z, partner mass (4 doubles)
+      // a mesh pass whose counts come back with the end of step's read (its
+      // candidates' total, the small bodies' total before the drops)
+      int mesh_pending = 0;
+      long mesh_base = 0, mesh_small_total = 0;
       double *lf_buf = nullptr;    // the differentiable leapfrog's buffers (kept between calls)
       size_t lf_cap = 0;           // doubles
       int *ckey = nullptr;         // insertion cell per slot (-1: not inserted)

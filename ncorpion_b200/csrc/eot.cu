@@ -15,9 +15,10 @@ DevState dev_state();
 int sync_scalars();
 int kick_state();
 int drift_state();
-int collide_brute_state();
+int collide_brute_state(bool defer);
 int mesh_reset_state();
-int mesh_pass(double gam, int test);
+int mesh_pass(double gam, int test, bool defer);
+void mesh_counts_finish(const int *h);
 int three_largest_state(int *idx);
 
 namespace {
@@ -262,6 +263,9 @@ int eot_state(int *hm_out)
       NCG_CK(cudaMemcpyAsync(&e, c.err, sizeof e, cudaMemcpyDeviceToHost, st));
       NCG_CK(cudaStreamSynchronize(st));
       if (e) NCG_TRY(check_err_word());
+      c.n_events = h[S_NEV];  // (a collision pass of this step may have left these to us)
+      c.collision_count = h[S_CCOUNT];
+      mesh_counts_finish(h);
       const int hm = h[S_HM];
       const bool changed = h[S_NFLAG] > 0 || hm < 9 * lid / 10;  // dumping or tidy_up change the scalars
       if (h[S_NFLAG] > 0) {
@@ -348,7 +352,7 @@ extern "C" int ncgpu_step_brute_force(int *how_many_moonlets)
       reset_launches();
       if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
       NCG_TRY(kick_state());
-      if (c.P.par_collision_bool) NCG_TRY(collide_brute_state());
+      if (c.P.par_collision_bool) NCG_TRY(collide_brute_state(true));  // its counts come back with the end of step's
       NCG_TRY(drift_state());
       return eot_state(how_many_moonlets);
 }
@@ -364,20 +368,21 @@ extern "C" int ncgpu_step_mesh(double gam, int *how_many_moonlets, long *total_n
       long tn = 0;
       if (c.P.par_collision_bool) {
             if (c.force_naive) {
-                  NCG_TRY(collide_brute_state());
+                  NCG_TRY(collide_brute_state(false));
             } else {
                   NCG_TRY(three_largest_state(nullptr));
-                  NCG_TRY(mesh_pass(gam, 1));
-                  tn = c.total_neighbours;
+                  NCG_TRY(mesh_pass(gam, 1, true));  // its counts come back with the end of step's
             }
       }
       NCG_TRY(drift_state());
       if (!c.P.par_collision_bool && !c.force_naive) {
             NCG_TRY(three_largest_state(nullptr));
-            NCG_TRY(mesh_pass(gam, 0));
+            NCG_TRY(mesh_pass(gam, 0, false));
             tn = c.total_neighbours;
       }
       NCG_TRY(kick_state());
+      const int st = eot_state(how_many_moonlets);
+      if (c.P.par_collision_bool && !c.force_naive) tn = c.total_neighbours;  // (set by the end of step's read)
       if (total_neighbours) *total_neighbours = tn;
-      return eot_state(how_many_moonlets);
+      return st;
 }

@@ -750,6 +750,16 @@ __global__ void k_clear_dirty_events(unsigned char *dirty, const int *ev, int n)
       }
 }
 
+// The same for the events [0, min(*nev, cap)) counted on the device (grid-stride).
+__global__ void k_clear_dirty_events_dev(unsigned char *dirty, const int *ev, const int *nev, int cap)
+{
+      const int n = min(*nev, cap);
+      for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+            dirty[ev[3 * e]] = 0;
+            dirty[ev[3 * e + 1]] = 0;
+      }
+}
+
 // Candidates of the bodies k in [lo, hi) (pop order, positions from base) and
 // their hits against the current state: the kernels, without waiting.
 static int mesh_segment_launch(const DevState &S, int lid, int lo, int hi, long base, int test)
@@ -849,7 +859,10 @@ static int read_scal(int idx, int *out)
 // parallel candidate machinery) separated by the big bodies' visits (one CTA
 // each); a visit that resolved collisions re-keys the bodies after it, whose
 // positions and radii at their turn may have changed.
-int mesh_pass(double gam, int test)
+// defer: for collision types that append no body, leave the pass's counts
+// (events, dropped pairs, total_neighbours) to the end of step's read instead
+// of reading them back here (mesh_counts_finish).
+int mesh_pass(double gam, int test, bool defer)
 {
       Ctx &c = ctx();
       cudaStream_t st = c.s;
@@ -960,6 +973,18 @@ int mesh_pass(double gam, int test)
                   NCG_CK(cudaMemcpyAsync(c.vis, c.vis_host, sizeof(int) * 3 * (size_t)c.mesh_nvis,
                                          cudaMemcpyHostToDevice, st));
       }
+      if (defer && test && nbig == 0 && E.type != NCGPU_COLLISION_FRAGMENTATION) {
+            k_clear_dirty_events_dev<<<32, 256, 0, st>>>(c.dirty, c.ev, c.scal + S_NEV, c.ev_cap);
+            NCG_LAUNCHED();
+            c.n_cand = (int)base;
+            c.mesh_nfev = 0;  // (no fragments without the fragmentation model)
+            c.mesh_nx = 0;
+            c.how_many_big = 0;
+            c.mesh_pending = 1;
+            c.mesh_base = base;
+            c.mesh_small_total = small_total;
+            return NCGPU_OK;
+      }
       int h[S_COUNT];
       NCG_TRY(sync_scalars_h(h));
       NCG_TRY(clear_dirty(c.n_events));
@@ -973,6 +998,19 @@ int mesh_pass(double gam, int test)
       return NCGPU_OK;
 }
 
+// The counts of a deferred mesh pass from the device scalars h (S_COUNT ints).
+void mesh_counts_finish(const int *h)
+{
+      Ctx &c = ctx();
+      if (!c.mesh_pending) return;
+      c.mesh_pending = 0;
+      c.n_events = h[S_NEV];
+      c.collision_count = h[S_CCOUNT];
+      c.mesh_nev = min(c.n_events, c.ev_cap);
+      c.total_neighbours = c.mesh_small_total - h[S_NDROP];
+      c.n_pairs = c.P.par_mutual_bool ? (int)(c.mesh_base - h[S_NDROP] - h[S_NSKIP] + h[S_NXPAIRS]) : 0;
+}
+
 }  // namespace ncg
 
 using namespace ncg;
@@ -983,7 +1021,7 @@ extern "C" int ncgpu_mesh(double gam, int with_collisions, int *n_pairs, int *n_
       reset_launches();
       if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
       if (!(gam > 0.)) return NCGPU_E_ARG;
-      NCG_TRY(mesh_pass(gam, with_collisions ? 1 : 0));
+      NCG_TRY(mesh_pass(gam, with_collisions ? 1 : 0, false));
       if (n_pairs) *n_pairs = c.n_pairs;
       if (n_events) *n_events = with_collisions ? c.n_events : 0;
       if (total_neighbours) *total_neighbours = c.total_neighbours;
