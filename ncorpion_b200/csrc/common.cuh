@@ -208,47 +208,158 @@ __device__ __forceinline__ bool row_range(const int2 *__restrict__ crange, long 
       return true;
 }
 
-// Sequential FP64 sum s + t[0] + t[1] + ... + t[n-1], in that order with IEEE
-// rounding, by one warp (the result is lane 0's): the lanes stage CHN terms at
-// a time in shared memory (`stage`, CHN doubles, 16-byte aligned) with
-// coalesced loads, the next block in flight while lane 0 adds, two terms per
-// shared load.  Launched as one warp per CTA, so that every chain has an SM's
-// FP64 pipe to itself.
-constexpr int CHN = 512;
+// Sequential FP64 sum s + t[0] + t[1] + ... + t[n-1]: the bits of the plain
+// loop, rounded to nearest after every addition, by one warp (every lane
+// returns it).  While the running sum is a normal number of binade e (|s| in
+// [2^e, 2^(e+1))) it is an integer multiple T of u = 2^(e-52), and s + x
+// rounds to (T + R)u, R the integer nearest x/u, as long as T + R stays inside
+// the binade with a unit to spare (2^52 < |T + R| < 2^53, or |T + R| = 2^52
+// with x/u - R pointing away from zero) and x/u is not an odd multiple of 1/2
+// (a tie, whose rounding would depend on T's last bit).  So a window's terms
+// are rounded to the spacing independently, their integer prefix sums checked
+// against the binade, and every term before the first one that breaks a
+// condition is taken at once.  That term (a binade change, a tie, a NaN or an
+// infinity, a term of 2^47 units or more, a sum that is zero, subnormal or
+// beyond 2^+-969) is added by itself with one rounded addition, and the pass
+// resumes after it; after a short run the next SEQ_RUN terms go one by one, so
+// that a sum that keeps changing binade costs little more than the plain loop.
+// Windows of SQW terms are copied into shared memory (`stage`, CHN doubles)
+// SQD windows ahead with cp.async, lane L's 32 consecutive terms in row L.
+// Launched as one warp per CTA.
+constexpr int SQD = 4, SQR = 33, SQW = 1024;
+constexpr int CHN = SQD * 32 * SQR;
+constexpr int SEQ_SHORT = 64, SEQ_RUN = 256;
+constexpr double SEQ_MAG = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds |q| < 2^51 to an integer
+
+struct SeqBin {
+      long long T;  // s = T * u
+      double u, inv;
+      bool ok;
+};
+
+__device__ __forceinline__ SeqBin seq_bin(double s)
+{
+      SeqBin b;
+      const unsigned long long w = (unsigned long long)__double_as_longlong(s);
+      const int ef = (int)((w >> 52) & 0x7ff);
+      b.ok = ef >= 54 && ef <= 2023;  // u = 2^(ef-1075) and 1/u both normal
+      const long long M = (long long)((w & 0xfffffffffffffull) | 0x10000000000000ull);
+      b.T = (w >> 63) ? -M : M;
+      b.u = __longlong_as_double((long long)((unsigned long long)(unsigned)(ef - 52) << 52));
+      b.inv = __longlong_as_double((long long)((unsigned long long)(unsigned)(2098 - ef) << 52));
+      return b;
+}
+
+__device__ __forceinline__ void seq_issue(const double *t, long n, long w, double *stage, int lane)
+{
+      const long base = w * SQW;
+      if (base < n) {
+            const unsigned d0 = (unsigned)__cvta_generic_to_shared(stage + (int)(w % SQD) * (32 * SQR));
+#pragma unroll 8
+            for (int i = 0; i < 32; i++) {  // window term i*32 + lane into row i, column lane
+                  const long k = base + i * 32 + lane;
+                  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d0 + (unsigned)(i * SQR + lane) * 8u),
+                               "l"(t + (k < n ? k : base)), "r"(k < n ? 8 : 0)
+                               : "memory");
+            }
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
 __device__ __forceinline__ double warp_chain_sum(const double *__restrict__ t, long n, double s, double *stage)
 {
       const int lane = threadIdx.x & 31;
-      double v[CHN / 32];
-#pragma unroll
-      for (int u = 0; u < CHN / 32; u++) {
-            const long k = (long)u * 32 + lane;
-            v[u] = k < n ? t[k] : 0.;
-      }
-      for (long base = 0; base < n; base += CHN) {
-#pragma unroll
-            for (int u = 0; u < CHN / 32; u++) stage[u * 32 + lane] = v[u];
+      const long nw = (n + SQW - 1) / SQW;
+      for (int w = 0; w < SQD; w++) seq_issue(t, n, w, stage, lane);
+      SeqBin b = seq_bin(s);
+      for (long w = 0; w < nw; w++) {
+            asm volatile("cp.async.wait_group %0;" ::"n"(SQD - 1) : "memory");
             __syncwarp();
-#pragma unroll
-            for (int u = 0; u < CHN / 32; u++) {  // the next block, in flight during the sums
-                  const long k = base + CHN + (long)u * 32 + lane;
-                  v[u] = k < n ? t[k] : 0.;
-            }
-            if (lane == 0) {
-                  const long m = n - base < CHN ? n - base : CHN;
-                  if (m == CHN) {  // full block: fixed trip count
-                        const double2 *st2 = reinterpret_cast<const double2 *>(stage);
-#pragma unroll 16
-                        for (int q = 0; q < CHN / 2; q++) {
-                              const double2 pr = st2[q];
-                              s = __dadd_rn(s, pr.x);
-                              s = __dadd_rn(s, pr.y);
-                        }
-                  } else {
-                        for (int q = 0; q < m; q++) s = __dadd_rn(s, stage[q]);
+            const double *buf = stage + (int)(w % SQD) * (32 * SQR);
+            const int wl = (int)(n - w * SQW < SQW ? n - w * SQW : SQW);
+            const int p0 = lane * 32;
+            int o = 0;
+            while (o < wl) {
+                  if (!b.ok) {  // no binade: the next term by itself
+                        s = __dadd_rn(s, buf[(o >> 5) * SQR + (o & 31)]);
+                        o++;
+                        b = seq_bin(s);
+                        continue;
                   }
+                  const bool pos = b.T > 0;
+                  double acc = 0., mn = 0., mx = 0., P[32];
+                  unsigned bad = 0u, dok = 0u;
+#pragma unroll
+                  for (int j = 0; j < 32; j++) {
+                        const double x = buf[lane * SQR + j];
+                        const bool live = p0 + j >= o && p0 + j < wl;
+                        const double y = __fma_rn(x, b.inv, SEQ_MAG);
+                        const double r = __dsub_rn(y, SEQ_MAG);  // x/u rounded (exact while |x/u| < 2^51)
+                        const double d = __fma_rn(x, b.inv, -r);  // x/u - r, exact
+                        const bool good = fabs(r) < 0x1p47 && fabs(d) != 0.5;
+                        acc = __dadd_rn(acc, live && good ? r : 0.);  // integers below 2^52: exact
+                        P[j] = acc;
+                        mn = fmin(mn, acc);
+                        mx = fmax(mx, acc);
+                        bad |= (unsigned)(live && !good) << j;
+                        dok |= (unsigned)(pos ? d >= 0. : d <= 0.) << j;
+                  }
+                  const long long tot = __double2ll_rn(acc);
+                  long long inc = tot;
+#pragma unroll
+                  for (int k = 1; k < 32; k <<= 1) {
+                        const long long v = __shfl_up_sync(0xffffffffu, inc, k);
+                        if (lane >= k) inc += v;
+                  }
+                  const long long T0 = b.T + (inc - tot);  // the sum before this lane's terms
+                  const long long wsum = __shfl_sync(0xffffffffu, inc, 31);
+                  const long long LO1 = pos ? (1LL << 52) + 1 : -((1LL << 53) - 1);
+                  const long long HI1 = pos ? (1LL << 53) - 1 : -((1LL << 52) + 1);
+                  const bool lane_ok =
+                      !bad && T0 + __double2ll_rn(mn) >= LO1 && T0 + __double2ll_rn(mx) <= HI1;
+                  if (__all_sync(0xffffffffu, lane_ok)) {  // the whole window
+                        b.T += wsum;
+                        s = __dmul_rn(__ll2double_rn(b.T), b.u);
+                        break;
+                  }
+                  // the first term that breaks a condition, and the sum before it
+                  const long long LOe = pos ? (1LL << 52) : -((1LL << 53) - 1);
+                  const long long HIe = pos ? (1LL << 53) - 1 : -(1LL << 52);
+                  const long long EDGE = pos ? LOe : HIe;
+                  int jf = 32;
+#pragma unroll
+                  for (int j = 31; j >= 0; j--) {
+                        const bool live = p0 + j >= o && p0 + j < wl;
+                        const long long Tj = T0 + __double2ll_rn(P[j]);
+                        const bool brk = live && (((bad >> j) & 1u) || Tj < LOe || Tj > HIe ||
+                                                  (Tj == EDGE && !((dok >> j) & 1u)));
+                        jf = brk ? j : jf;
+                  }
+                  long long Tb = T0;
+#pragma unroll
+                  for (int j = 0; j < 31; j++) Tb = j + 1 == jf ? T0 + __double2ll_rn(P[j]) : Tb;
+                  const unsigned bm = __ballot_sync(0xffffffffu, jf < 32);
+                  if (!bm) {
+                        b.T += wsum;
+                        s = __dmul_rn(__ll2double_rn(b.T), b.u);
+                        break;
+                  }
+                  const int lf = __ffs(bm) - 1;
+                  const int pf = lf * 32 + __shfl_sync(0xffffffffu, jf, lf);
+                  s = __dmul_rn(__ll2double_rn(__shfl_sync(0xffffffffu, Tb, lf)), b.u);
+                  s = __dadd_rn(s, buf[(pf >> 5) * SQR + (pf & 31)]);
+                  const int taken = pf - o;
+                  o = pf + 1;
+                  if (taken < SEQ_SHORT) {
+                        const int e = wl < o + SEQ_RUN ? wl : o + SEQ_RUN;
+                        for (; o < e; o++) s = __dadd_rn(s, buf[(o >> 5) * SQR + (o & 31)]);
+                  }
+                  b = seq_bin(s);
             }
             __syncwarp();
+            seq_issue(t, n, w + SQD, stage, lane);
       }
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
       return s;
 }
 

@@ -163,36 +163,71 @@ __global__ void k_fmt_pack(const char *__restrict__ slots, const int *__restrict
 // summed in slot order, and the two most massive bodies as its loop picks them
 // (strictly greater replaces, so the first of equal masses wins; i1 = i2 = 0 and
 // M = 0 when there are fewer positive masses).  One warp.
-__global__ void k_out_stats(BodyView S, const int *__restrict__ cidx, int n, double *__restrict__ out_mass,
-                            int *__restrict__ out_idx)
+// display()'s two most massive bodies (src/display.c:353-363): the reference scans the
+// slots in ascending order from M = 0 with strict comparisons, which keeps the
+// first two positive masses of the order (mass descending, slot ascending).
+// That order is total, so the scan is a reduction: each thread keeps the first
+// two of its bodies, then threads, warps and blocks merge their pairs.
+struct Top2 {
+      double M1, M2;
+      int i1, i2;
+};
+
+__device__ __forceinline__ bool top_before(double a, int i, double b, int j) { return a > b || (a == b && i < j); }
+
+__device__ __forceinline__ void top2_insert(Top2 &t, double m, int p)
 {
-      // per lane, then merged: the first (m desc, slot asc) and the first of the
-      // others; only positive masses take part (the loop starts from M = 0)
-      double M1 = 0., M2 = 0.;
-      int i1 = 0x7fffffff, i2 = 0x7fffffff;
-      for (int q = threadIdx.x; q < n; q += 32) {
-            const int p = cidx[q];  // ascending within a lane
-            const double m = S.m[(long)p * S.stride];
-            if (m > M1) { M2 = M1; i2 = i1; M1 = m; i1 = p; }
-            else if (m > M2) { M2 = m; i2 = p; }
+      if (top_before(m, p, t.M1, t.i1)) {
+            t.M2 = t.M1;
+            t.i2 = t.i1;
+            t.M1 = m;
+            t.i1 = p;
+      } else if (top_before(m, p, t.M2, t.i2)) {
+            t.M2 = m;
+            t.i2 = p;
       }
+}
+
+__device__ __forceinline__ void top2_warp(Top2 &t)
+{
       for (int o = 16; o > 0; o >>= 1) {
-            double a1 = M1, a2 = M2, b1 = __shfl_xor_sync(0xffffffffu, M1, o), b2 = __shfl_xor_sync(0xffffffffu, M2, o);
-            int j1 = i1, j2 = i2, k1 = __shfl_xor_sync(0xffffffffu, i1, o), k2 = __shfl_xor_sync(0xffffffffu, i2, o);
-            if (b1 > a1 || (b1 == a1 && k1 < j1)) {  // the other list leads
-                  double t = a1; a1 = b1; b1 = t; t = a2; a2 = b2; b2 = t;
-                  int u = j1; j1 = k1; k1 = u; u = j2; j2 = k2; k2 = u;
-            }
-            const bool bsec = b1 > a2 || (b1 == a2 && k1 < j2);  // second: the better of a2 and b1
-            M1 = a1; i1 = j1;
-            M2 = bsec ? b1 : a2;
-            i2 = bsec ? k1 : j2;
+            const double b1 = __shfl_xor_sync(0xffffffffu, t.M1, o), b2 = __shfl_xor_sync(0xffffffffu, t.M2, o);
+            const int k1 = __shfl_xor_sync(0xffffffffu, t.i1, o), k2 = __shfl_xor_sync(0xffffffffu, t.i2, o);
+            top2_insert(t, b1, k1);
+            top2_insert(t, b2, k2);
       }
-      if (threadIdx.x == 0) {
-            out_mass[1] = M1;
-            out_mass[2] = M2;
-            out_idx[0] = M1 > 0. ? i1 : 0;
-            out_idx[1] = M2 > 0. ? i2 : 0;
+}
+
+constexpr int TOP_T = 256, TOP_MAXB = 148 * 8;
+
+// The compacted masses m[q] = S.m[cidx[q]] (the sequential total's input) and
+// each block's first two bodies: pm[2b], pm[2b+1] with slots pi[2b], pi[2b+1]
+// (mass 0 and slot INT_MAX for an empty entry).
+__global__ void __launch_bounds__(TOP_T) k_out_top2(BodyView S, const int *__restrict__ cidx, int n,
+                                                    double *__restrict__ m, double *__restrict__ pm,
+                                                    int *__restrict__ pi)
+{
+      __shared__ Top2 wt[TOP_T / 32];
+      Top2 t{0., 0., 0x7fffffff, 0x7fffffff};
+      for (int q = blockIdx.x * TOP_T + threadIdx.x; q < n; q += gridDim.x * TOP_T) {
+            const int p = cidx[q];
+            const double v = S.m[(long)p * S.stride];
+            m[q] = v;
+            if (v > 0.) top2_insert(t, v, p);
+      }
+      top2_warp(t);
+      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      if (lane == 0) wt[w] = t;
+      __syncthreads();
+      if (w == 0) {
+            t = lane < TOP_T / 32 ? wt[lane] : Top2{0., 0., 0x7fffffff, 0x7fffffff};
+            top2_warp(t);
+            if (lane == 0) {
+                  pm[2 * blockIdx.x] = t.M1;
+                  pm[2 * blockIdx.x + 1] = t.M2;
+                  pi[2 * blockIdx.x] = t.i1;
+                  pi[2 * blockIdx.x + 1] = t.i2;
+            }
       }
 }
 
@@ -208,9 +243,23 @@ __global__ void k_gather_radius(BodyView S, const int *__restrict__ cidx, int n,
       if (q < n) r[q] = S.R[(long)cidx[q] * S.stride];
 }
 
-__global__ void __launch_bounds__(32) k_chain_total(const double *__restrict__ m, int n, double *__restrict__ out)
+// The blocks' pairs merged (out[1], out[2]; the slots in out_idx, 0 when a
+// mass is absent, as the reference leaves them), then the total mass out[0]:
+// the masses summed in slot order with round-to-nearest, the reference's sum.
+__global__ void __launch_bounds__(32) k_chain_total(const double *__restrict__ m, int n, double *__restrict__ out,
+                                                    const double *__restrict__ pm, const int *__restrict__ pi,
+                                                    int nb, int *__restrict__ out_idx)
 {
       __shared__ __align__(16) double stage[CHN];
+      Top2 t{0., 0., 0x7fffffff, 0x7fffffff};
+      for (int k = threadIdx.x; k < 2 * nb; k += 32) top2_insert(t, pm[k], pi[k]);
+      top2_warp(t);
+      if (threadIdx.x == 0) {
+            out[1] = t.M1;
+            out[2] = t.M2;
+            out_idx[0] = t.M1 > 0. ? t.i1 : 0;
+            out_idx[1] = t.M2 > 0. ? t.i2 : 0;
+      }
       const double s = warp_chain_sum(m, n, 0., stage);
       if (threadIdx.x == 0) out[0] = s;
 }
@@ -680,17 +729,15 @@ extern "C" int ncgpu_output_stats(double *stats, int *idx, struct ncgpu_body *cm
       cudaStream_t st = c.s;
       int n = 0;
       NCG_TRY(compact_existing(c.ex, c.largest_id, &n, st));
-      NCG_TRY(ensure_partial((size_t)n + 8));
+      const size_t mcap = ((size_t)n + 8) & ~(size_t)7;
+      NCG_TRY(ensure_partial(mcap + 3 * TOP_MAXB));
       BodyView S = state_view();
-      double *m = c.partial, *res = c.red + 3900;
-      int *didx = (int *)(c.red + 3904);
-      if (n > 0) {
-            k_gather_mass<<<(n + 255) / 256, 256, 0, st>>>(S, c.cidx, n, m);
-            NCG_LAUNCHED();
-      }
-      k_chain_total<<<1, 32, 0, st>>>(m, n, res);
+      double *m = c.partial, *pm = c.partial + mcap, *res = c.red + 3900;
+      int *pi = (int *)(pm + 2 * TOP_MAXB), *didx = (int *)(c.red + 3904);
+      const int nb = (int)std::min<long>(std::max<long>(((long)n + TOP_T - 1) / TOP_T, 1), TOP_MAXB);
+      k_out_top2<<<nb, TOP_T, 0, st>>>(S, c.cidx, n, m, pm, pi);
       NCG_LAUNCHED();
-      k_out_stats<<<1, 32, 0, st>>>(S, c.cidx, n, res, didx);
+      k_chain_total<<<1, 32, 0, st>>>(m, n, res, pm, pi, nb, didx);
       NCG_LAUNCHED();
       int hidx[2];
       NCG_CK(cudaMemcpyAsync(stats, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
