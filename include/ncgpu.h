@@ -247,10 +247,12 @@ int ncgpu_probe_pow_third(const double *x, double *out, int n);
 int ncgpu_probe_div(const double *a, const double *b, double *out, int n);
 /* Diagnostic: out[c] = s0[c] + x[c*n] + x[c*n + 1] + ... + x[c*n + n-1] for the
    `chains` chains, added in that order with round-to-nearest after every
-   addition (the plain loop's bits), by the device routine that forms every
-   reference-order sum here (total mass, momentum, the central body's
-   acceleration, the mesh's chains).  Host buffers. */
-int ncgpu_probe_seq_sum(const double *x, long n, const double *s0, double *out, int chains);
+   addition (the plain loop's bits), by the device routines that form the
+   reference-order sums here: the one that takes whole runs of terms within a
+   binade (runs != 0; display()'s total mass of 65,536 bodies or more) or the
+   staged one-add-at-a-time loop (runs == 0; every other such sum).  Host
+   buffers. */
+int ncgpu_probe_seq_sum(const double *x, long n, const double *s0, double *out, int chains, int runs);
 
 /* ---- device-resident integrator state ------------------------------------ */
 

@@ -136,7 +136,7 @@ EXPORTS = {
     "ncgpu_set_sideral_omega": (C.c_int, [C.c_double]),
     "ncgpu_probe_pow_third": (C.c_int, [P, P, C.c_int]),
     "ncgpu_probe_div": (C.c_int, [P, P, P, C.c_int]),
-    "ncgpu_probe_seq_sum": (C.c_int, [P, C.c_long, P, P, C.c_int]),
+    "ncgpu_probe_seq_sum": (C.c_int, [P, C.c_long, P, P, C.c_int, C.c_int]),
     "ncgpu_get_events": (C.c_int, [P, P, C.c_int, P]),
     "ncgpu_end_of_timestep": (C.c_int, [P]),
     "ncgpu_step_brute_force": (C.c_int, [P]),

@@ -19,7 +19,14 @@ int cuda_fail(cudaError_t e, const char *what, const char *file, int line)
       return NCGPU_E_CUDA;
 }
 void note_launch() { ++g_launches; }
-void reset_launches() { g_launches = 0; }
+void reset_launches()
+{
+      g_launches = 0;
+      if (g_ctx.stats_pre) {  // statistics still running on the second stream: later work waits for them
+            cudaStreamWaitEvent(g_ctx.s, g_ctx.sev1, 0);
+            g_ctx.stats_pre = 0;
+      }
+}
 int launches() { return g_launches; }
 
 int ensure_partial(size_t doubles)
@@ -77,6 +84,9 @@ void free_all()
       if (c.pinned) cudaFreeHost(c.pinned);
       if (c.kev0) cudaEventDestroy(c.kev0);
       if (c.kev1) cudaEventDestroy(c.kev1);
+      if (c.sev0) cudaEventDestroy(c.sev0);
+      if (c.sev1) cudaEventDestroy(c.sev1);
+      if (c.s2) cudaStreamDestroy(c.s2);
       if (c.s) cudaStreamDestroy(c.s);
       c = Ctx{};
 }
@@ -389,7 +399,10 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
             free_all();
             return NCGPU_E_CUDA;
       }
-      if (cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking) != cudaSuccess) {
+      if (cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaStreamCreateWithFlags(&c.s2, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&c.sev0, cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&c.sev1, cudaEventDisableTiming) != cudaSuccess) {
             free_all();
             return NCGPU_E_CUDA;
       }

@@ -208,26 +208,73 @@ __device__ __forceinline__ bool row_range(const int2 *__restrict__ crange, long 
       return true;
 }
 
-// Sequential FP64 sum s + t[0] + t[1] + ... + t[n-1]: the bits of the plain
-// loop, rounded to nearest after every addition, by one warp (every lane
-// returns it).  While the running sum is a normal number of binade e (|s| in
-// [2^e, 2^(e+1))) it is an integer multiple T of u = 2^(e-52), and s + x
-// rounds to (T + R)u, R the integer nearest x/u, as long as T + R stays inside
-// the binade with a unit to spare (2^52 < |T + R| < 2^53, or |T + R| = 2^52
-// with x/u - R pointing away from zero) and x/u is not an odd multiple of 1/2
-// (a tie, whose rounding would depend on T's last bit).  So a window's terms
-// are rounded to the spacing independently, their integer prefix sums checked
-// against the binade, and every term before the first one that breaks a
-// condition is taken at once.  That term (a binade change, a tie, a NaN or an
-// infinity, a term of 2^47 units or more, a sum that is zero, subnormal or
-// beyond 2^+-969) is added by itself with one rounded addition, and the pass
-// resumes after it; after a short run the next SEQ_RUN terms go one by one, so
-// that a sum that keeps changing binade costs little more than the plain loop.
-// Windows of SQW terms are copied into shared memory (`stage`, CHN doubles)
-// SQD windows ahead with cp.async, lane L's 32 consecutive terms in row L.
-// Launched as one warp per CTA.
+
+// Sequential FP64 sum s + t[0] + t[1] + ... + t[n-1], in that order with IEEE
+// rounding, by one warp (the result is lane 0's): the lanes stage CHN terms at
+// a time in shared memory (`stage`, CHN doubles, 16-byte aligned) with
+// coalesced loads, the next block in flight while lane 0 adds, two terms per
+// shared load.  Launched as one warp per CTA, so that every chain has an SM's
+// FP64 pipe to itself.
+constexpr int CHN = 512;
+__device__ __forceinline__ double warp_chain_sum(const double *__restrict__ t, long n, double s, double *stage)
+{
+      const int lane = threadIdx.x & 31;
+      double v[CHN / 32];
+#pragma unroll
+      for (int u = 0; u < CHN / 32; u++) {
+            const long k = (long)u * 32 + lane;
+            v[u] = k < n ? t[k] : 0.;
+      }
+      for (long base = 0; base < n; base += CHN) {
+#pragma unroll
+            for (int u = 0; u < CHN / 32; u++) stage[u * 32 + lane] = v[u];
+            __syncwarp();
+#pragma unroll
+            for (int u = 0; u < CHN / 32; u++) {  // the next block, in flight during the sums
+                  const long k = base + CHN + (long)u * 32 + lane;
+                  v[u] = k < n ? t[k] : 0.;
+            }
+            if (lane == 0) {
+                  const long m = n - base < CHN ? n - base : CHN;
+                  if (m == CHN) {  // full block: fixed trip count
+                        const double2 *st2 = reinterpret_cast<const double2 *>(stage);
+#pragma unroll 16
+                        for (int q = 0; q < CHN / 2; q++) {
+                              const double2 pr = st2[q];
+                              s = __dadd_rn(s, pr.x);
+                              s = __dadd_rn(s, pr.y);
+                        }
+                  } else {
+                        for (int q = 0; q < m; q++) s = __dadd_rn(s, stage[q]);
+                  }
+            }
+            __syncwarp();
+      }
+      return s;
+}
+
+
+// The same sum, taking whole runs of terms at once (display()'s total mass of
+// up to millions of positive masses).  While the running sum is a normal number
+// of binade e (|s| in [2^e, 2^(e+1))) it is an integer multiple T of
+// u = 2^(e-52), and s + x rounds to (T + R)u, R the integer nearest x/u, as
+// long as T + R stays inside the binade with a unit to spare
+// (2^52 < |T + R| < 2^53, or |T + R| = 2^52 with x/u - R pointing away from
+// zero) and x/u is not an odd multiple of 1/2 (a tie, whose rounding would
+// depend on T's last bit).  So a window's terms are rounded to the spacing
+// independently, their integer prefix sums checked against the binade, and
+// every term before the first one that breaks a condition is taken at once.
+// That term (a binade change, a tie, a NaN or an infinity, a term of 2^47
+// units or more, a sum that is zero, subnormal or beyond 2^+-969) is added by
+// itself with one rounded addition, and the pass resumes after it; after a
+// short run the next SEQ_RUN terms go one by one.  Windows of SQW terms are
+// copied into shared memory (`stage`, RUN_STAGE doubles) SQD windows ahead
+// with cp.async, lane L's 32 consecutive terms in row L.  One warp per CTA.
+// About 2.2 ns a term for positive masses against 5 ns for warp_chain_sum;
+// sums whose running value keeps changing binade (zero-mean terms) are
+// slower, so the other reference-order sums keep warp_chain_sum.
 constexpr int SQD = 4, SQR = 33, SQW = 1024;
-constexpr int CHN = SQD * 32 * SQR;
+constexpr int RUN_STAGE = SQD * 32 * SQR;
 constexpr int SEQ_SHORT = 64, SEQ_RUN = 256;
 constexpr double SEQ_MAG = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds |q| < 2^51 to an integer
 
@@ -266,7 +313,7 @@ __device__ __forceinline__ void seq_issue(const double *t, long n, long w, doubl
       asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
-__device__ __forceinline__ double warp_chain_sum(const double *__restrict__ t, long n, double s, double *stage)
+__device__ __forceinline__ double warp_run_sum(const double *__restrict__ t, long n, double s, double *stage)
 {
       const int lane = threadIdx.x & 31;
       const long nw = (n + SQW - 1) / SQW;
@@ -439,6 +486,13 @@ struct Ctx {
       double *pinned = nullptr;    // pinned host staging (8 * n_max doubles)
       cudaEvent_t kev0 = nullptr, kev1 = nullptr;  // bracket the dominant kernel
       int kev_valid = 0;
+      // display()'s statistics, started by ncgpu_format_cartesian on a second
+      // stream while its text crosses to the host; ncgpu_output_stats takes
+      // them when no other entry point ran in between (any other one first
+      // makes the main stream wait for them and drops them)
+      cudaStream_t s2 = nullptr;
+      cudaEvent_t sev0 = nullptr, sev1 = nullptr;
+      int stats_pre = 0;
 
       // collision state (device)
       int *did = nullptr;          // did_collide[] (src/structure.c)

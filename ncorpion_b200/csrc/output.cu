@@ -245,12 +245,14 @@ __global__ void k_gather_radius(BodyView S, const int *__restrict__ cidx, int n,
 
 // The blocks' pairs merged (out[1], out[2]; the slots in out_idx, 0 when a
 // mass is absent, as the reference leaves them), then the total mass out[0]:
-// the masses summed in slot order with round-to-nearest, the reference's sum.
+// the masses summed in slot order with round-to-nearest, the reference's sum
+// (taken in runs from RUN_SUM_MIN bodies on).
+constexpr int RUN_SUM_MIN = 65536;
 __global__ void __launch_bounds__(32) k_chain_total(const double *__restrict__ m, int n, double *__restrict__ out,
                                                     const double *__restrict__ pm, const int *__restrict__ pi,
                                                     int nb, int *__restrict__ out_idx)
 {
-      __shared__ __align__(16) double stage[CHN];
+      __shared__ __align__(16) double stage[RUN_STAGE];
       Top2 t{0., 0., 0x7fffffff, 0x7fffffff};
       for (int k = threadIdx.x; k < 2 * nb; k += 32) top2_insert(t, pm[k], pi[k]);
       top2_warp(t);
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(32) k_chain_total(const double *__restrict__ m
             out_idx[0] = t.M1 > 0. ? t.i1 : 0;
             out_idx[1] = t.M2 > 0. ? t.i2 : 0;
       }
-      const double s = warp_chain_sum(m, n, 0., stage);
+      const double s = n >= RUN_SUM_MIN ? warp_run_sum(m, n, 0., stage) : warp_chain_sum(m, n, 0., stage);
       if (threadIdx.x == 0) out[0] = s;
 }
 
@@ -549,6 +551,30 @@ int format_files(const Values &val, int nfiles, const long *first, char *text, u
 }  // namespace
 }  // namespace ncg
 
+namespace ncg {
+namespace {
+
+// display()'s statistics of the n compacted bodies on stream st: the total mass
+// and the two most massive bodies into c.red[3900..2], their slots into the
+// two ints at c.red + 3904.
+int stats_launch(int n, cudaStream_t st)
+{
+      Ctx &c = ctx();
+      const size_t mcap = ((size_t)n + 8) & ~(size_t)7;
+      NCG_TRY(ensure_partial(mcap + 3 * TOP_MAXB));
+      double *m = c.partial, *pm = c.partial + mcap, *res = c.red + 3900;
+      int *pi = (int *)(pm + 2 * TOP_MAXB), *didx = (int *)(c.red + 3904);
+      const int nb = (int)std::min<long>(std::max<long>(((long)n + TOP_T - 1) / TOP_T, 1), TOP_MAXB);
+      k_out_top2<<<nb, TOP_T, 0, st>>>(state_view(), c.cidx, n, m, pm, pi);
+      NCG_LAUNCHED();
+      k_chain_total<<<1, 32, 0, st>>>(m, n, res, pm, pi, nb, didx);
+      NCG_LAUNCHED();
+      return NCGPU_OK;
+}
+
+}  // namespace
+}  // namespace ncg
+
 extern "C" int ncgpu_format_cartesian(char *text, unsigned long cap, unsigned long *lens)
 {
       Ctx &c = ctx();
@@ -557,6 +583,13 @@ extern "C" int ncgpu_format_cartesian(char *text, unsigned long cap, unsigned lo
       if (!text || !lens) return NCGPU_E_ARG;
       int n = 0;
       NCG_TRY(compact_existing(c.ex, c.largest_id, &n, c.s));
+      // display()'s statistics on the second stream, while the text is formatted
+      // and copied out; ncgpu_output_stats, called next, takes them
+      NCG_CK(cudaEventRecord(c.sev0, c.s));
+      NCG_CK(cudaStreamWaitEvent(c.s2, c.sev0, 0));
+      NCG_TRY(stats_launch(n, c.s2));
+      NCG_CK(cudaEventRecord(c.sev1, c.s2));
+      c.stats_pre = 1;
       const int central = c.P.par_central_mass_bool ? 1 : 0;
       const long per = n + central;
       const long first[9] = {0, per, 2 * per, 3 * per, 4 * per, 5 * per, 6 * per, 6 * per + n, 6 * per + 2L * n};
@@ -723,22 +756,21 @@ extern "C" int ncgpu_host_atan2(const double *yx, double *F, long n)
 extern "C" int ncgpu_output_stats(double *stats, int *idx, struct ncgpu_body *cm, struct ncgpu_body *two)
 {
       Ctx &c = ctx();
+      const int pre = c.stats_pre;  // started by ncgpu_format_cartesian just before
+      c.stats_pre = 0;
       reset_launches();
       if (!c.inited || !c.uploaded) return NCGPU_E_STATE;
       if (!stats || !idx || !cm || !two) return NCGPU_E_ARG;
       cudaStream_t st = c.s;
-      int n = 0;
-      NCG_TRY(compact_existing(c.ex, c.largest_id, &n, st));
-      const size_t mcap = ((size_t)n + 8) & ~(size_t)7;
-      NCG_TRY(ensure_partial(mcap + 3 * TOP_MAXB));
-      BodyView S = state_view();
-      double *m = c.partial, *pm = c.partial + mcap, *res = c.red + 3900;
-      int *pi = (int *)(pm + 2 * TOP_MAXB), *didx = (int *)(c.red + 3904);
-      const int nb = (int)std::min<long>(std::max<long>(((long)n + TOP_T - 1) / TOP_T, 1), TOP_MAXB);
-      k_out_top2<<<nb, TOP_T, 0, st>>>(S, c.cidx, n, m, pm, pi);
-      NCG_LAUNCHED();
-      k_chain_total<<<1, 32, 0, st>>>(m, n, res, pm, pi, nb, didx);
-      NCG_LAUNCHED();
+      if (pre) {
+            NCG_CK(cudaStreamWaitEvent(st, c.sev1, 0));
+      } else {
+            int n = 0;
+            NCG_TRY(compact_existing(c.ex, c.largest_id, &n, st));
+            NCG_TRY(stats_launch(n, st));
+      }
+      const double *res = c.red + 3900;
+      const int *didx = (const int *)(c.red + 3904);
       int hidx[2];
       NCG_CK(cudaMemcpyAsync(stats, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
       NCG_CK(cudaMemcpyAsync(hidx, didx, sizeof hidx, cudaMemcpyDeviceToHost, st));

@@ -217,19 +217,20 @@ extern "C" int ncgpu_probe_div(const double *a, const double *b, double *out, in
 namespace ncg {
 namespace {
 // out[c] = s0[c] + x[c*n] + ... + x[c*n + n-1], one warp per chain, by the
-// sequential sum every reference-order reduction here uses.
+// run-taking sum (runs != 0) or the plain staged loop.
 __global__ void __launch_bounds__(32) k_seq_probe(const double *__restrict__ x, long n, const double *__restrict__ s0,
-                                                  double *__restrict__ out)
+                                                  double *__restrict__ out, int runs)
 {
-      __shared__ __align__(16) double stage[CHN];
+      __shared__ __align__(16) double stage[RUN_STAGE];
       const int c = blockIdx.x;
-      const double s = warp_chain_sum(x + (size_t)c * n, n, s0[c], stage);
+      const double *t = x + (size_t)c * n;
+      const double s = runs ? warp_run_sum(t, n, s0[c], stage) : warp_chain_sum(t, n, s0[c], stage);
       if (threadIdx.x == 0) out[c] = s;
 }
 }  // namespace
 }  // namespace ncg
 
-extern "C" int ncgpu_probe_seq_sum(const double *x, long n, const double *s0, double *out, int chains)
+extern "C" int ncgpu_probe_seq_sum(const double *x, long n, const double *s0, double *out, int chains, int runs)
 {
       if (!x || !s0 || !out || n < 0 || chains <= 0 || chains > 65535) return NCGPU_E_ARG;
       const size_t nx = (size_t)n * (size_t)chains;
@@ -237,7 +238,7 @@ extern "C" int ncgpu_probe_seq_sum(const double *x, long n, const double *s0, do
       NCG_CK(cudaMalloc(&d, sizeof(double) * (nx + 2 * (size_t)chains)));
       if (nx) NCG_CK(cudaMemcpy(d, x, sizeof(double) * nx, cudaMemcpyHostToDevice));
       NCG_CK(cudaMemcpy(d + nx, s0, sizeof(double) * (size_t)chains, cudaMemcpyHostToDevice));
-      ncg::k_seq_probe<<<chains, 32>>>(d, n, d + nx, d + nx + chains);
+      ncg::k_seq_probe<<<chains, 32>>>(d, n, d + nx, d + nx + chains, runs);
       NCG_LAUNCHED();
       NCG_CK(cudaMemcpy(out, d + nx + chains, sizeof(double) * (size_t)chains, cudaMemcpyDeviceToHost));
       NCG_CK(cudaFree(d));

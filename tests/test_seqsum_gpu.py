@@ -1,10 +1,10 @@
-"""The device's sequential FP64 sum (every reference-order reduction: display()'s
-total mass, src/display.c:352; total_momentum, src/structure.c:1193-1227; the
-central body's acceleration, src/physics.c:137-139; the mesh's chains) against
-the plain loop, through the C ABI.
+"""The device's sequential FP64 sums against the plain loop, through the C ABI:
+the staged one-add-at-a-time loop (total_momentum, src/structure.c:1193-1227;
+the central body's acceleration, src/physics.c:137-139; the mesh's chains) and
+the routine that takes whole runs of terms at once while the running sum stays
+in one binade (display()'s total mass, src/display.c:352).
 
-The device takes whole runs of terms at once while the running sum stays in one
-binade, so the cases aim at the places where that could go wrong: binade
+For the second, the cases aim at the places where that could go wrong: binade
 changes up and down, ties (terms that are odd multiples of half the sum's
 spacing), a sum that is an exact power of two, sign changes, zeros, subnormal
 and huge values, infinities and NaNs, and sizes that end inside a window.
@@ -21,12 +21,13 @@ def _plain(x, s0):
     return np.add.accumulate(np.concatenate([[s0], x]))[-1] if len(x) else np.float64(s0)
 
 
-def _device(lib, api, chains, s0):
+def _device(lib, api, chains, s0, runs=1):
     n = len(chains[0])
     x = np.ascontiguousarray(np.concatenate(chains)) if n else np.zeros(1)
     s = np.ascontiguousarray(s0, dtype=np.float64)
     out = np.empty(len(chains))
-    api.check(lib.ncgpu_probe_seq_sum(api.ptr(x), n, api.ptr(s), api.ptr(out), len(chains)), "ncgpu_probe_seq_sum")
+    api.check(lib.ncgpu_probe_seq_sum(api.ptr(x), n, api.ptr(s), api.ptr(out), len(chains), runs),
+              "ncgpu_probe_seq_sum")
     return out
 
 
@@ -64,8 +65,9 @@ def _cases(rng, n):
     ]
 
 
+@pytest.mark.parametrize("runs", [1, 0])
 @pytest.mark.parametrize("n", [0, 1, 31, 1000, 1024, 1025, 5000, 33_000])
-def test_seq_sum_matches_the_plain_loop(lib, n):
+def test_seq_sum_matches_the_plain_loop(lib, n, runs):
     from ncorpion_b200 import api
     rng = np.random.default_rng(n + 11)
     cases = _cases(rng, n)
@@ -80,12 +82,13 @@ def test_seq_sum_matches_the_plain_loop(lib, n):
         cases.append(("nan", x, 0.0))
     with np.errstate(over="ignore", invalid="ignore"):
         want = [_plain(x, s0) for _, x, s0 in cases]
-        got = _device(lib, api, [x for _, x, _ in cases], [s0 for _, _, s0 in cases])
+        got = _device(lib, api, [x for _, x, _ in cases], [s0 for _, _, s0 in cases], runs)
     bad = [name for (name, _, _), w, g in zip(cases, want, got) if not _same(w, g)]
     assert not bad, bad
 
 
-def test_seq_sum_long_chains(lib):
+@pytest.mark.parametrize("runs", [1, 0])
+def test_seq_sum_long_chains(lib, runs):
     """Chains of 2^20 terms, the mesh workload's size, in the shapes its sums
     take: positive masses, a zero-mean walk (the central body's acceleration
     from a symmetric disk), heavy-tailed terms (a moonlet's acceleration)."""
@@ -96,5 +99,5 @@ def test_seq_sum_long_chains(lib):
               1e-3 * rng.standard_cauchy(n), 1e-3 * rng.standard_normal(n) + 1e-6]
     s0 = [0.0, 0.0, 0.0, 0.25]
     want = [_plain(x, s) for x, s in zip(chains, s0)]
-    got = _device(lib, api, chains, s0)
+    got = _device(lib, api, chains, s0, runs)
     assert all(_same(w, g) for w, g in zip(want, got))
