@@ -315,7 +315,9 @@ int ncgpu_snapshot_end(void);
    in `text` (no newlines; display() ends each line with one) and lens[8]
    receives their byte counts.  cap >= ncgpu_format_cartesian_cap() always
    suffices.  NCGPU_E_UNSUPPORTED when a value exceeds 1.7e24 in magnitude
-   (the caller prints that output itself). */
+   (the caller prints that output itself).  It also starts the statistics of
+   ncgpu_output_stats on a second stream, so that a call of that function
+   right after this one (as display() makes them) finds them computed. */
 int ncgpu_format_cartesian(char *text, unsigned long cap, unsigned long *lens);
 unsigned long ncgpu_format_cartesian_cap(void);
 /* The elliptic files of this output (display() with write_elliptic_bool,
@@ -356,7 +358,8 @@ int ncgpu_host_atan2(const double *yx, double *F, long n);
    stats[0] the total mass of the bodies summed in slot order, stats[1..2] and
    idx[0..1] the masses M1, M2 and slots of the two most massive bodies as its
    loop picks them (0 when absent), two[0..1] those slots' records, cm the
-   central body. */
+   central body.  Computed here, or taken from the preceding call when that was
+   ncgpu_format_cartesian on the same state. */
 int ncgpu_output_stats(double *stats, int *idx, struct ncgpu_body *cm, struct ncgpu_body *two);
 /* The barycentre end_of_timestep prints at a progress step (src/rk4.c:202-222,
    333): zeros right after an ncgpu_end_of_timestep that reduced the barycentre
