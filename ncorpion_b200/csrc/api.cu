@@ -87,6 +87,8 @@ void free_all()
       if (c.sev0) cudaEventDestroy(c.sev0);
       if (c.sev1) cudaEventDestroy(c.sev1);
       if (c.s2) cudaStreamDestroy(c.s2);
+      if (c.cev) cudaEventDestroy(c.cev);
+      if (c.s3) cudaStreamDestroy(c.s3);
       if (c.s) cudaStreamDestroy(c.s);
       c = Ctx{};
 }
@@ -401,6 +403,8 @@ int ncgpu_init(int n_max, const struct ncgpu_params *params)
       }
       if (cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking) != cudaSuccess ||
           cudaStreamCreateWithFlags(&c.s2, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaStreamCreateWithFlags(&c.s3, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&c.cev, cudaEventDisableTiming) != cudaSuccess ||
           cudaEventCreateWithFlags(&c.sev0, cudaEventDisableTiming) != cudaSuccess ||
           cudaEventCreateWithFlags(&c.sev1, cudaEventDisableTiming) != cudaSuccess) {
             free_all();

@@ -492,6 +492,9 @@ struct Ctx {
       // makes the main stream wait for them and drops them)
       cudaStream_t s2 = nullptr;
       cudaEvent_t sev0 = nullptr, sev1 = nullptr;
+      // the output text's copies to the host, chunk by chunk behind the formatting
+      cudaStream_t s3 = nullptr;
+      cudaEvent_t cev = nullptr;
       int stats_pre = 0;
 
       // collision state (device)

@@ -137,22 +137,24 @@ struct EllValues {
 
 // One thread per value: formatted into its slot, the length into len.
 template <class Values>
-__global__ void k_fmt_values(Values val, long total, char *__restrict__ slots, int *__restrict__ len, unsigned *err)
+__global__ void k_fmt_values(Values val, long lo, long hi, char *__restrict__ slots, int *__restrict__ len,
+                             unsigned *err)
 {
-      const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-      if (i >= total) return;
+      const long i = lo + (long)blockIdx.x * blockDim.x + threadIdx.x;
+      if (i >= hi) return;
       const int L = fmt_fixed14(val(i), slots + (size_t)i * SLOT);
       if (L < 0) atomicOr(err, ERR_INTERNAL);
       len[i] = L < 0 ? 0 : L;
 }
 
-// Copies the slots to their places in the packed text (offsets: exclusive
-// scan of the lengths; the files' texts follow one another, without newlines).
-__global__ void k_fmt_pack(const char *__restrict__ slots, const int *__restrict__ off, long total,
+// Copies the slots of values lo .. hi-1 to their places in the packed text
+// (offsets: exclusive scan of those values' lengths, from text; the files'
+// texts follow one another, without newlines).
+__global__ void k_fmt_pack(const char *__restrict__ slots, const int *__restrict__ off, long lo, long hi,
                            char *__restrict__ text)
 {
-      const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-      if (i >= total) return;
+      const long i = lo + (long)blockIdx.x * blockDim.x + threadIdx.x;
+      if (i >= hi) return;
       const int L = off[i + 1] - off[i];
       const char *src = slots + (size_t)i * SLOT;
       char *dst = text + off[i];
@@ -495,8 +497,12 @@ namespace {
 
 // Formats `total` values (file f: values first[f] .. first[f + 1] - 1) and
 // copies the files' texts, one after the other, into text; lens[f] receives
-// each file's length.  NCGPU_E_UNSUPPORTED when a value is beyond the
-// formatter's range (nothing copied), NCGPU_E_CAPACITY when cap is too small.
+// each file's length.  In chunks of FMT_CHUNK values: a chunk's text crosses to
+// the host on the copy stream while the next chunk is formatted.
+// NCGPU_E_UNSUPPORTED when a value is beyond the formatter's range,
+// NCGPU_E_CAPACITY when cap is too small (text then holds an unspecified
+// prefix).
+constexpr long FMT_CHUNK = 1L << 20;
 template <class Values>
 int format_files(const Values &val, int nfiles, const long *first, char *text, unsigned long cap, unsigned long *lens)
 {
@@ -520,30 +526,52 @@ int format_files(const Values &val, int nfiles, const long *first, char *text, u
       }
       const size_t vals = c.fmt_cap / SLOT;
       int *len = c.fmt_len, *off = c.fmt_len + vals + 1, *sums = c.fmt_len + 2 * vals + 2;
-      int h[16] = {0};
-      if (total > 0) {
-            const int nb = (int)((total + 255) / 256);
-            k_fmt_values<<<nb, 256, 0, st>>>(val, total, c.fmt_slots, len, c.err);
-            NCG_LAUNCHED();
-            NCG_TRY(scan_exclusive(len, off, (int)total, sums, st));
-            k_fmt_pack<<<nb, 256, 0, st>>>(c.fmt_slots, off, total, c.fmt_text);
-            NCG_LAUNCHED();
-            for (int f = 0; f <= nfiles; f++)
-                  NCG_CK(cudaMemcpyAsync(&h[f], off + first[f], sizeof(int), cudaMemcpyDeviceToHost, st));
-      }
+      long h[16] = {0};
+      int rel[17] = {0};  // [0..nfiles]: boundary offsets within their chunk; [16]: the chunk's length
       unsigned herr = 0;
-      NCG_CK(cudaMemcpyAsync(&herr, c.err, sizeof herr, cudaMemcpyDeviceToHost, st));
-      NCG_CK(cudaStreamSynchronize(st));
+      long base = 0;
+      int st_ret = NCGPU_OK;
+      for (long lo = 0; lo < total; lo += FMT_CHUNK) {
+            const long hi = std::min(total, lo + FMT_CHUNK);
+            const int nb = (int)((hi - lo + 255) / 256);
+            k_fmt_values<<<nb, 256, 0, st>>>(val, lo, hi, c.fmt_slots, len, c.err);
+            NCG_LAUNCHED();
+            // chunk-relative offsets; off[hi] is the chunk's length until the next chunk's scan
+            NCG_TRY(scan_exclusive(len + lo, off + lo, (int)(hi - lo), sums, st));
+            k_fmt_pack<<<nb, 256, 0, st>>>(c.fmt_slots, off, lo, hi, c.fmt_text + base);
+            NCG_LAUNCHED();
+            for (int f = 0; f <= nfiles; f++)  // each boundary read with the chunk that starts at or holds it
+                  if ((first[f] >= lo && first[f] < hi) || (first[f] == total && hi == total))
+                        NCG_CK(cudaMemcpyAsync(&rel[f], off + first[f], sizeof(int), cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaMemcpyAsync(&rel[16], off + hi, sizeof(int), cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaMemcpyAsync(&herr, c.err, sizeof herr, cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaStreamSynchronize(st));
+            if (herr) break;
+            for (int f = 0; f <= nfiles; f++)
+                  if ((first[f] >= lo && first[f] < hi) || (first[f] == total && hi == total)) h[f] = base + rel[f];
+            if ((unsigned long)(base + rel[16]) > cap) {
+                  st_ret = NCGPU_E_CAPACITY;
+                  break;
+            }
+            if (rel[16] > 0) {  // this chunk's text to the host, behind the previous chunks' copies
+                  NCG_CK(cudaEventRecord(c.cev, st));
+                  NCG_CK(cudaStreamWaitEvent(c.s3, c.cev, 0));
+                  NCG_CK(cudaMemcpyAsync(text + base, c.fmt_text + base, (size_t)rel[16], cudaMemcpyDeviceToHost,
+                                         c.s3));
+            }
+            base += rel[16];
+      }
+      NCG_CK(cudaStreamSynchronize(c.s3));
+      if (total <= 0) {
+            NCG_CK(cudaMemcpyAsync(&herr, c.err, sizeof herr, cudaMemcpyDeviceToHost, st));
+            NCG_CK(cudaStreamSynchronize(st));
+      }
       if (herr & ERR_INTERNAL) {  // a value beyond the formatter's range
             NCG_CK(cudaMemsetAsync(c.err, 0, sizeof(unsigned), st));
             return NCGPU_E_UNSUPPORTED;
       }
       if (herr) return check_err_word();
-      if ((unsigned long)h[nfiles] > cap) return NCGPU_E_CAPACITY;
-      if (h[nfiles] > 0) {
-            NCG_CK(cudaMemcpyAsync(text, c.fmt_text, (size_t)h[nfiles], cudaMemcpyDeviceToHost, st));
-            NCG_CK(cudaStreamSynchronize(st));
-      }
+      if (st_ret != NCGPU_OK) return st_ret;
       for (int f = 0; f < nfiles; f++) lens[f] = (unsigned long)(h[f + 1] - h[f]);
       return NCGPU_OK;
 }
