@@ -261,20 +261,24 @@ __device__ __forceinline__ double warp_chain_sum(const double *__restrict__ t, l
 // long as T + R stays inside the binade with a unit to spare
 // (2^52 < |T + R| < 2^53, or |T + R| = 2^52 with x/u - R pointing away from
 // zero) and x/u is not an odd multiple of 1/2 (a tie, whose rounding would
-// depend on T's last bit).  So a window's terms are rounded to the spacing
-// independently, their integer prefix sums checked against the binade, and
-// every term before the first one that breaks a condition is taken at once.
-// That term (a binade change, a tie, a NaN or an infinity, a term of 2^47
-// units or more, a sum that is zero, subnormal or beyond 2^+-969) is added by
-// itself with one rounded addition, and the pass resumes after it; after a
-// short run the next SEQ_RUN terms go one by one.  Windows of SQW terms are
-// copied into shared memory (`stage`, RUN_STAGE doubles) SQD windows ahead
-// with cp.async, lane L's 32 consecutive terms in row L.  One warp per CTA.
-// About 2.2 ns a term for positive masses against 5 ns for warp_chain_sum;
-// sums whose running value keeps changing binade (zero-mean terms) are
-// slower, so the other reference-order sums keep warp_chain_sum.
-constexpr int SQD = 4, SQR = 33, SQW = 1024;
-constexpr int RUN_STAGE = SQD * 32 * SQR;
+// depend on T's last bit).  So terms are rounded to the spacing independently
+// and their integer prefix sums checked against the binade.
+//
+// A block of RUN_NW warps takes RUN_NW windows of RUN_W terms a round: each
+// warp stages its window in shared memory (lane L's RUN_Q consecutive terms in
+// row L) and sums it for the binade the round starts in, with the range of its
+// prefix sums; warp 0 then accepts the windows in order while they keep the
+// sum inside the binade, and walks the first one that does not term by term
+// (run_window: every term before the first that breaks a condition taken at
+// once, that term -- a binade change, a tie, a NaN or an infinity, a term of
+// 2^47 units or more, a sum that is zero, subnormal or beyond 2^+-969 -- added
+// by itself, and the pass resumed after it; after a short run the next
+// SEQ_RUN terms go one by one).  The next round starts after that window.
+// Sums whose running value keeps changing binade (zero-mean terms) gain
+// nothing, so the other reference-order sums keep warp_chain_sum.
+constexpr int RUN_Q = 16, RUN_NW = 16, RUN_W = 32 * RUN_Q;
+constexpr int RUN_ROW = RUN_Q + 1;                  // padded row: conflict-free transposed reads
+constexpr int RUN_STAGE = RUN_NW * 32 * RUN_ROW;    // doubles of dynamic shared memory
 constexpr int SEQ_SHORT = 64, SEQ_RUN = 256;
 constexpr double SEQ_MAG = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds |q| < 2^51 to an integer
 
@@ -297,116 +301,200 @@ __device__ __forceinline__ SeqBin seq_bin(double s)
       return b;
 }
 
-__device__ __forceinline__ void seq_issue(const double *t, long n, long w, double *stage, int lane)
+__device__ __forceinline__ double run_term(const double *buf, int p)
 {
-      const long base = w * SQW;
-      if (base < n) {
-            const unsigned d0 = (unsigned)__cvta_generic_to_shared(stage + (int)(w % SQD) * (32 * SQR));
-#pragma unroll 8
-            for (int i = 0; i < 32; i++) {  // window term i*32 + lane into row i, column lane
-                  const long k = base + i * 32 + lane;
-                  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d0 + (unsigned)(i * SQR + lane) * 8u),
-                               "l"(t + (k < n ? k : base)), "r"(k < n ? 8 : 0)
-                               : "memory");
-            }
-      }
-      asm volatile("cp.async.commit_group;" ::: "memory");
+      return buf[(p / RUN_Q) * RUN_ROW + p % RUN_Q];
 }
 
-__device__ __forceinline__ double warp_run_sum(const double *__restrict__ t, long n, double s, double *stage)
+// One warp walks window buf (terms 0 .. wl-1) from term o on, from the sum s.
+__device__ __forceinline__ double run_window(const double *buf, int o, int wl, double s)
 {
-      const int lane = threadIdx.x & 31;
-      const long nw = (n + SQW - 1) / SQW;
-      for (int w = 0; w < SQD; w++) seq_issue(t, n, w, stage, lane);
+      const int lane = threadIdx.x & 31, p0 = lane * RUN_Q;
       SeqBin b = seq_bin(s);
-      for (long w = 0; w < nw; w++) {
-            asm volatile("cp.async.wait_group %0;" ::"n"(SQD - 1) : "memory");
-            __syncwarp();
-            const double *buf = stage + (int)(w % SQD) * (32 * SQR);
-            const int wl = (int)(n - w * SQW < SQW ? n - w * SQW : SQW);
-            const int p0 = lane * 32;
-            int o = 0;
-            while (o < wl) {
-                  if (!b.ok) {  // no binade: the next term by itself
-                        s = __dadd_rn(s, buf[(o >> 5) * SQR + (o & 31)]);
-                        o++;
-                        b = seq_bin(s);
-                        continue;
-                  }
-                  const bool pos = b.T > 0;
-                  double acc = 0., mn = 0., mx = 0., P[32];
-                  unsigned bad = 0u, dok = 0u;
-#pragma unroll
-                  for (int j = 0; j < 32; j++) {
-                        const double x = buf[lane * SQR + j];
-                        const bool live = p0 + j >= o && p0 + j < wl;
-                        const double y = __fma_rn(x, b.inv, SEQ_MAG);
-                        const double r = __dsub_rn(y, SEQ_MAG);  // x/u rounded (exact while |x/u| < 2^51)
-                        const double d = __fma_rn(x, b.inv, -r);  // x/u - r, exact
-                        const bool good = fabs(r) < 0x1p47 && fabs(d) != 0.5;
-                        acc = __dadd_rn(acc, live && good ? r : 0.);  // integers below 2^52: exact
-                        P[j] = acc;
-                        mn = fmin(mn, acc);
-                        mx = fmax(mx, acc);
-                        bad |= (unsigned)(live && !good) << j;
-                        dok |= (unsigned)(pos ? d >= 0. : d <= 0.) << j;
-                  }
-                  const long long tot = __double2ll_rn(acc);
-                  long long inc = tot;
-#pragma unroll
-                  for (int k = 1; k < 32; k <<= 1) {
-                        const long long v = __shfl_up_sync(0xffffffffu, inc, k);
-                        if (lane >= k) inc += v;
-                  }
-                  const long long T0 = b.T + (inc - tot);  // the sum before this lane's terms
-                  const long long wsum = __shfl_sync(0xffffffffu, inc, 31);
-                  const long long LO1 = pos ? (1LL << 52) + 1 : -((1LL << 53) - 1);
-                  const long long HI1 = pos ? (1LL << 53) - 1 : -((1LL << 52) + 1);
-                  const bool lane_ok =
-                      !bad && T0 + __double2ll_rn(mn) >= LO1 && T0 + __double2ll_rn(mx) <= HI1;
-                  if (__all_sync(0xffffffffu, lane_ok)) {  // the whole window
-                        b.T += wsum;
-                        s = __dmul_rn(__ll2double_rn(b.T), b.u);
-                        break;
-                  }
-                  // the first term that breaks a condition, and the sum before it
-                  const long long LOe = pos ? (1LL << 52) : -((1LL << 53) - 1);
-                  const long long HIe = pos ? (1LL << 53) - 1 : -(1LL << 52);
-                  const long long EDGE = pos ? LOe : HIe;
-                  int jf = 32;
-#pragma unroll
-                  for (int j = 31; j >= 0; j--) {
-                        const bool live = p0 + j >= o && p0 + j < wl;
-                        const long long Tj = T0 + __double2ll_rn(P[j]);
-                        const bool brk = live && (((bad >> j) & 1u) || Tj < LOe || Tj > HIe ||
-                                                  (Tj == EDGE && !((dok >> j) & 1u)));
-                        jf = brk ? j : jf;
-                  }
-                  long long Tb = T0;
-#pragma unroll
-                  for (int j = 0; j < 31; j++) Tb = j + 1 == jf ? T0 + __double2ll_rn(P[j]) : Tb;
-                  const unsigned bm = __ballot_sync(0xffffffffu, jf < 32);
-                  if (!bm) {
-                        b.T += wsum;
-                        s = __dmul_rn(__ll2double_rn(b.T), b.u);
-                        break;
-                  }
-                  const int lf = __ffs(bm) - 1;
-                  const int pf = lf * 32 + __shfl_sync(0xffffffffu, jf, lf);
-                  s = __dmul_rn(__ll2double_rn(__shfl_sync(0xffffffffu, Tb, lf)), b.u);
-                  s = __dadd_rn(s, buf[(pf >> 5) * SQR + (pf & 31)]);
-                  const int taken = pf - o;
-                  o = pf + 1;
-                  if (taken < SEQ_SHORT) {
-                        const int e = wl < o + SEQ_RUN ? wl : o + SEQ_RUN;
-                        for (; o < e; o++) s = __dadd_rn(s, buf[(o >> 5) * SQR + (o & 31)]);
-                  }
+      while (o < wl) {
+            if (!b.ok) {  // no binade: the next term by itself
+                  s = __dadd_rn(s, run_term(buf, o));
+                  o++;
                   b = seq_bin(s);
+                  continue;
+            }
+            const bool pos = b.T > 0;
+            double acc = 0., mn = 0., mx = 0., P[RUN_Q];
+            unsigned bad = 0u, dok = 0u;
+#pragma unroll
+            for (int j = 0; j < RUN_Q; j++) {
+                  const double x = buf[lane * RUN_ROW + j];
+                  const bool live = p0 + j >= o && p0 + j < wl;
+                  const double y = __fma_rn(x, b.inv, SEQ_MAG);
+                  const double r = __dsub_rn(y, SEQ_MAG);  // x/u rounded (exact while |x/u| < 2^51)
+                  const double d = __fma_rn(x, b.inv, -r);  // x/u - r, exact
+                  const bool good = fabs(r) < 0x1p47 && fabs(d) != 0.5;
+                  acc = __dadd_rn(acc, live && good ? r : 0.);  // integers below 2^52: exact
+                  P[j] = acc;
+                  mn = fmin(mn, acc);
+                  mx = fmax(mx, acc);
+                  bad |= (unsigned)(live && !good) << j;
+                  dok |= (unsigned)(pos ? d >= 0. : d <= 0.) << j;
+            }
+            const long long tot = __double2ll_rn(acc);
+            long long inc = tot;
+#pragma unroll
+            for (int k = 1; k < 32; k <<= 1) {
+                  const long long v = __shfl_up_sync(0xffffffffu, inc, k);
+                  if (lane >= k) inc += v;
+            }
+            const long long T0 = b.T + (inc - tot);  // the sum before this lane's terms
+            const long long wsum = __shfl_sync(0xffffffffu, inc, 31);
+            const long long LO1 = pos ? (1LL << 52) + 1 : -((1LL << 53) - 1);
+            const long long HI1 = pos ? (1LL << 53) - 1 : -((1LL << 52) + 1);
+            const bool lane_ok = !bad && T0 + __double2ll_rn(mn) >= LO1 && T0 + __double2ll_rn(mx) <= HI1;
+            if (__all_sync(0xffffffffu, lane_ok)) {  // the rest of the window
+                  s = __dmul_rn(__ll2double_rn(b.T + wsum), b.u);
+                  break;
+            }
+            // the first term that breaks a condition, and the sum before it
+            const long long LOe = pos ? (1LL << 52) : -((1LL << 53) - 1);
+            const long long HIe = pos ? (1LL << 53) - 1 : -(1LL << 52);
+            const long long EDGE = pos ? LOe : HIe;
+            int jf = RUN_Q;
+#pragma unroll
+            for (int j = RUN_Q - 1; j >= 0; j--) {
+                  const bool live = p0 + j >= o && p0 + j < wl;
+                  const long long Tj = T0 + __double2ll_rn(P[j]);
+                  const bool brk = live && (((bad >> j) & 1u) || Tj < LOe || Tj > HIe ||
+                                            (Tj == EDGE && !((dok >> j) & 1u)));
+                  jf = brk ? j : jf;
+            }
+            long long Tb = T0;
+#pragma unroll
+            for (int j = 0; j < RUN_Q - 1; j++) Tb = j + 1 == jf ? T0 + __double2ll_rn(P[j]) : Tb;
+            const unsigned bm = __ballot_sync(0xffffffffu, jf < RUN_Q);
+            if (!bm) {
+                  s = __dmul_rn(__ll2double_rn(b.T + wsum), b.u);
+                  break;
+            }
+            const int lf = __ffs(bm) - 1;
+            const int pf = lf * RUN_Q + __shfl_sync(0xffffffffu, jf, lf);
+            s = __dmul_rn(__ll2double_rn(__shfl_sync(0xffffffffu, Tb, lf)), b.u);
+            s = __dadd_rn(s, run_term(buf, pf));
+            const int taken = pf - o;
+            o = pf + 1;
+            if (taken < SEQ_SHORT) {
+                  const int e = wl < o + SEQ_RUN ? wl : o + SEQ_RUN;
+                  for (; o < e; o++) s = __dadd_rn(s, run_term(buf, o));
+            }
+            b = seq_bin(s);
+      }
+      return s;
+}
+
+// A window's integer sum at the spacing of binade b, the range of its prefix
+// sums (the empty prefix included) and whether a term cannot be taken.
+struct RunPart {
+      long long tot, mn, mx;
+      int bad;
+};
+
+__device__ __forceinline__ RunPart run_part(const double *buf, int wl, const SeqBin &b)
+{
+      const int lane = threadIdx.x & 31, p0 = lane * RUN_Q;
+      double acc = 0., mn = 0., mx = 0.;
+      bool bad = false;
+#pragma unroll
+      for (int j = 0; j < RUN_Q; j++) {
+            const double x = buf[lane * RUN_ROW + j];
+            const bool live = p0 + j < wl;
+            const double y = __fma_rn(x, b.inv, SEQ_MAG);
+            const double r = __dsub_rn(y, SEQ_MAG);
+            const double d = __fma_rn(x, b.inv, -r);
+            const bool good = fabs(r) < 0x1p47 && fabs(d) != 0.5;
+            acc = __dadd_rn(acc, live && good ? r : 0.);
+            mn = fmin(mn, acc);
+            mx = fmax(mx, acc);
+            bad |= live && !good;
+      }
+      const long long tot = __double2ll_rn(acc);
+      long long inc = tot;
+#pragma unroll
+      for (int k = 1; k < 32; k <<= 1) {
+            const long long v = __shfl_up_sync(0xffffffffu, inc, k);
+            if (lane >= k) inc += v;
+      }
+      long long lo = inc - tot + __double2ll_rn(mn), hi = inc - tot + __double2ll_rn(mx);
+#pragma unroll
+      for (int k = 16; k > 0; k >>= 1) {
+            const long long a = __shfl_xor_sync(0xffffffffu, lo, k), c = __shfl_xor_sync(0xffffffffu, hi, k);
+            lo = a < lo ? a : lo;
+            hi = c > hi ? c : hi;
+      }
+      RunPart r;
+      r.tot = __shfl_sync(0xffffffffu, inc, 31);
+      r.mn = lo;
+      r.mx = hi;
+      r.bad = __any_sync(0xffffffffu, bad);
+      return r;
+}
+
+// s + t[0] + ... + t[n-1] by the whole block (RUN_NW warps; every thread
+// returns it); stage: RUN_STAGE doubles of shared memory.
+__device__ __forceinline__ double block_run_sum(const double *__restrict__ t, long n, double s, double *stage)
+{
+      __shared__ RunPart part[RUN_NW];
+      __shared__ double sh_s;
+      __shared__ long sh_pos;
+      const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+      double *buf = stage + w * 32 * RUN_ROW;
+      long pos = 0;
+      while (pos < n) {
+            const SeqBin b = seq_bin(s);
+            const long start = pos + (long)w * RUN_W;
+            const long left = n - start;
+            const int wl = left <= 0 ? 0 : left < RUN_W ? (int)left : RUN_W;
+#pragma unroll 4
+            for (int i = 0; i < RUN_Q; i++) {  // window term i*32 + lane: row (i*32 + lane) / RUN_Q
+                  const int p = i * 32 + lane;
+                  buf[(p / RUN_Q) * RUN_ROW + p % RUN_Q] = p < wl ? t[start + p] : 0.;
             }
             __syncwarp();
-            seq_issue(t, n, w + SQD, stage, lane);
+            RunPart r{0, 0, 0, 0};
+            if (b.ok && wl > 0) r = run_part(buf, wl, b);
+            if (lane == 0) part[w] = r;
+            __syncthreads();
+            if (w == 0) {
+                  double s2 = s;
+                  long p2;
+                  if (b.ok) {
+                        const bool pos_s = b.T > 0;
+                        const long long LO1 = pos_s ? (1LL << 52) + 1 : -((1LL << 53) - 1);
+                        const long long HI1 = pos_s ? (1LL << 53) - 1 : -((1LL << 52) + 1);
+                        long long T = b.T;
+                        int k = 0;
+                        for (; k < RUN_NW && pos + (long)k * RUN_W < n; k++) {  // windows taken whole
+                              const RunPart q = part[k];
+                              if (q.bad || T + q.mn < LO1 || T + q.mx > HI1) break;
+                              T += q.tot;
+                        }
+                        s2 = __dmul_rn(__ll2double_rn(T), b.u);
+                        p2 = pos + (long)k * RUN_W;
+                        if (k < RUN_NW && p2 < n) {  // window k walked term by term
+                              const int wk = n - p2 < RUN_W ? (int)(n - p2) : RUN_W;
+                              s2 = run_window(stage + k * 32 * RUN_ROW, 0, wk, s2);
+                              p2 += wk;
+                        }
+                  } else {
+                        s2 = run_window(stage, 0, wl, s);  // this warp's window 0
+                        p2 = pos + wl;
+                  }
+                  if (lane == 0) {
+                        sh_s = s2;
+                        sh_pos = p2 < n ? p2 : n;
+                  }
+            }
+            __syncthreads();
+            s = sh_s;
+            pos = sh_pos;
+            __syncthreads();
       }
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
       return s;
 }
 

@@ -250,22 +250,30 @@ __global__ void k_gather_radius(BodyView S, const int *__restrict__ cidx, int n,
 // the masses summed in slot order with round-to-nearest, the reference's sum
 // (taken in runs from RUN_SUM_MIN bodies on).
 constexpr int RUN_SUM_MIN = 65536;
-__global__ void __launch_bounds__(32) k_chain_total(const double *__restrict__ m, int n, double *__restrict__ out,
-                                                    const double *__restrict__ pm, const int *__restrict__ pi,
-                                                    int nb, int *__restrict__ out_idx)
+__global__ void __launch_bounds__(RUN_NW * 32) k_chain_total(const double *__restrict__ m, int n,
+                                                             double *__restrict__ out, const double *__restrict__ pm,
+                                                             const int *__restrict__ pi, int nb,
+                                                             int *__restrict__ out_idx)
 {
-      __shared__ __align__(16) double stage[RUN_STAGE];
-      Top2 t{0., 0., 0x7fffffff, 0x7fffffff};
-      for (int k = threadIdx.x; k < 2 * nb; k += 32) top2_insert(t, pm[k], pi[k]);
-      top2_warp(t);
-      if (threadIdx.x == 0) {
-            out[1] = t.M1;
-            out[2] = t.M2;
-            out_idx[0] = t.M1 > 0. ? t.i1 : 0;
-            out_idx[1] = t.M2 > 0. ? t.i2 : 0;
+      extern __shared__ __align__(16) double stage[];  // RUN_STAGE doubles
+      if (threadIdx.x < 32) {
+            Top2 t{0., 0., 0x7fffffff, 0x7fffffff};
+            for (int k = threadIdx.x; k < 2 * nb; k += 32) top2_insert(t, pm[k], pi[k]);
+            top2_warp(t);
+            if (threadIdx.x == 0) {
+                  out[1] = t.M1;
+                  out[2] = t.M2;
+                  out_idx[0] = t.M1 > 0. ? t.i1 : 0;
+                  out_idx[1] = t.M2 > 0. ? t.i2 : 0;
+            }
       }
-      const double s = n >= RUN_SUM_MIN ? warp_run_sum(m, n, 0., stage) : warp_chain_sum(m, n, 0., stage);
-      if (threadIdx.x == 0) out[0] = s;
+      if (n >= RUN_SUM_MIN) {
+            const double s = block_run_sum(m, n, 0., stage);
+            if (threadIdx.x == 0) out[0] = s;
+      } else if (threadIdx.x < 32) {
+            const double s = warp_chain_sum(m, n, 0., stage);
+            if (threadIdx.x == 0) out[0] = s;
+      }
 }
 
 // ---- elliptic elements (cart2ell, src/structure.c:172-284) ----------------
@@ -595,7 +603,9 @@ int stats_launch(int n, cudaStream_t st)
       const int nb = (int)std::min<long>(std::max<long>(((long)n + TOP_T - 1) / TOP_T, 1), TOP_MAXB);
       k_out_top2<<<nb, TOP_T, 0, st>>>(state_view(), c.cidx, n, m, pm, pi);
       NCG_LAUNCHED();
-      k_chain_total<<<1, 32, 0, st>>>(m, n, res, pm, pi, nb, didx);
+      constexpr int smem = RUN_STAGE * (int)sizeof(double);
+      NCG_CK(cudaFuncSetAttribute(k_chain_total, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      k_chain_total<<<1, RUN_NW * 32, smem, st>>>(m, n, res, pm, pi, nb, didx);
       NCG_LAUNCHED();
       return NCGPU_OK;
 }

@@ -218,14 +218,20 @@ namespace ncg {
 namespace {
 // out[c] = s0[c] + x[c*n] + ... + x[c*n + n-1], one warp per chain, by the
 // run-taking sum (runs != 0) or the plain staged loop.
-__global__ void __launch_bounds__(32) k_seq_probe(const double *__restrict__ x, long n, const double *__restrict__ s0,
-                                                  double *__restrict__ out, int runs)
+__global__ void __launch_bounds__(RUN_NW * 32) k_seq_probe(const double *__restrict__ x, long n,
+                                                           const double *__restrict__ s0, double *__restrict__ out,
+                                                           int runs)
 {
-      __shared__ __align__(16) double stage[RUN_STAGE];
+      extern __shared__ __align__(16) double stage[];  // RUN_STAGE doubles
       const int c = blockIdx.x;
       const double *t = x + (size_t)c * n;
-      const double s = runs ? warp_run_sum(t, n, s0[c], stage) : warp_chain_sum(t, n, s0[c], stage);
-      if (threadIdx.x == 0) out[c] = s;
+      if (runs) {
+            const double s = block_run_sum(t, n, s0[c], stage);
+            if (threadIdx.x == 0) out[c] = s;
+      } else if (threadIdx.x < 32) {
+            const double s = warp_chain_sum(t, n, s0[c], stage);
+            if (threadIdx.x == 0) out[c] = s;
+      }
 }
 }  // namespace
 }  // namespace ncg
@@ -238,7 +244,9 @@ extern "C" int ncgpu_probe_seq_sum(const double *x, long n, const double *s0, do
       NCG_CK(cudaMalloc(&d, sizeof(double) * (nx + 2 * (size_t)chains)));
       if (nx) NCG_CK(cudaMemcpy(d, x, sizeof(double) * nx, cudaMemcpyHostToDevice));
       NCG_CK(cudaMemcpy(d + nx, s0, sizeof(double) * (size_t)chains, cudaMemcpyHostToDevice));
-      ncg::k_seq_probe<<<chains, 32>>>(d, n, d + nx, d + nx + chains, runs);
+      constexpr int smem = ncg::RUN_STAGE * (int)sizeof(double);
+      NCG_CK(cudaFuncSetAttribute(ncg::k_seq_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      ncg::k_seq_probe<<<chains, ncg::RUN_NW * 32, smem>>>(d, n, d + nx, d + nx + chains, runs);
       NCG_LAUNCHED();
       NCG_CK(cudaMemcpy(out, d + nx + chains, sizeof(double) * (size_t)chains, cudaMemcpyDeviceToHost));
       NCG_CK(cudaFree(d));
