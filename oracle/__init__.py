@@ -135,6 +135,8 @@ class Ref:
             L.orc_frag_counts.argtypes = [P]
         if hasattr(L, "orc_cart2ell"):
             L.orc_cart2ell.argtypes = [P, P, C.c_double, C.c_double, P]
+        if hasattr(L, "orc_tree_build"):
+            L.orc_tree_build.restype = C.c_int
         if L.orc_init() != 0:
             raise MemoryError("reference init failed")
         self.n_max = L.orc_n_max()
@@ -162,6 +164,25 @@ class Ref:
         cma = np.zeros(3)
         self.lib.orc_vector_field(_p(acc), _p(cma))
         return acc, cma
+
+    def tree_field(self, slot_order=True):
+        """falcON's field of the current state (a falcON profile): the tree
+        built as the tree driver builds it before a kick (src/rk4.c:576-586),
+        vector_field on it, the tree released (src/rk4.c:337-346).  With
+        slot_order the bodies enter the tree in slot order, as in a run's first
+        tree; otherwise in the previous tree's Peano-Hilbert order, as in every
+        later one.  Returns (acc, cm_acc, cells)."""
+        if not getattr(self, "_tree_tables", False):
+            self.lib.orc_tree_tables()
+            self._tree_tables = True
+        if slot_order:
+            self.lib.orc_tree_slot_order()
+        cells = self.lib.orc_tree_build()
+        try:
+            acc, cma = self.vector_field()
+        finally:
+            self.lib.orc_tree_free()
+        return acc, cma, cells
 
     def cart2ell(self, rec, cm, mu, j2=0.0):
         """The reference's cart2ell of one record (its globals CM_buffer = cm,

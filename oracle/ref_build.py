@@ -92,6 +92,10 @@ PROFILES = {
                        t_end="0.01", time_step="0.001"),
     "bf_grav_s05": dict(BF, collision_bool="0", softening_parameter="0.5", N_max="70000",
                         N_0="2000", t_end="0.01", time_step="0.001"),
+    # falcON gravity only (src/ffm.c, Dehnen 2002; the reference's default module): expansion order 3,
+    # theta_min 0.45, the parameters.h defaults
+    "tree_grav": dict(COMMON, falcON_bool="1", collision_bool="0", N_max="70000", N_0="2000",
+                      t_end="0.01", time_step="0.001"),
     # brute-force gravity + brute-force collisions, instant merger: N=2000, 200 steps
     "bf_merge": dict(BF, collision_bool="1", instant_merger_bool="1", N_max="4096", N_0="2000",
                      t_end="0.2", time_step="0.001", output_step="50",

@@ -16,6 +16,8 @@
  *   three_largest_*        src/structure.c:914, src/structure.c:1005
  *   collision_treatment    src/physics.c:1043 (wrapped with -Wl,--wrap to log events)
  *   fragmentation counters src/structure.h:148-151
+ *   falcON tree            src/ffm.c (tables src/main.c:118-125, build
+ *                          src/rk4.c:576-586, release src/rk4.c:337-346)
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -26,6 +28,7 @@
 #include "physics.h"
 #include "collision.h"
 #include "rk4.h"
+#include "ffm.h"
 
 static struct moonlet *B = NULL;    /* the body array handed to the reference */
 static int *ev_log = NULL;          /* (a, b, type) per collision_treatment call */
@@ -140,6 +143,58 @@ void orc_vector_field(double *acc, double *cm_acc)
       cm_acc[0] = CM_acc[0];
       cm_acc[1] = CM_acc[1];
       cm_acc[2] = CM_acc[2];
+}
+
+/* falcON: the multipole index tables main() fills once (src/main.c:118-125). */
+void orc_tree_tables(void)
+{
+      k_from_s2s3_init();
+      s1s2s3_from_kn_init();
+      s2s3_from_k_init();
+      k_from_ijklmn_init();
+      ijklmn_from_kn_init();
+      perm_from_kn_init();
+      q1fromq2q3_init();
+}
+
+/* The tree of the current state, as the tree driver builds it before its kick
+   (src/rk4.c:576-586); vector_field then runs falcON on it.  Returns the
+   number of cells. */
+int orc_tree_build(void)
+{
+      struct boxdot *root = root_cell(B);
+      FlatTree = flattree_init(root);
+      clear_boxdot(&root);
+      com_flattree(FlatTree, B);
+      Mtot = FlatTree->M0;
+      rmax_flattree(FlatTree, B);
+      rcrit_flattree(FlatTree);
+      tensor_initialization(FlatTree);
+#if expansion_order > 2
+      multipole_flattree(FlatTree, B);
+#endif
+      return cell_id;
+}
+
+/* The next tree takes the bodies in slot order, as the first tree of a run
+   does (IndexPeanoHilbertOrder at its initial 0); every later tree takes them
+   in the previous tree's Peano-Hilbert order first (src/ffm.c:350-361,
+   421-479), which changes the order of the sums in its leaves. */
+void orc_tree_slot_order(void) { IndexPeanoHilbertOrder = 0; }
+
+/* Releases the tree as end_of_timestep does (src/rk4.c:337-346). */
+void orc_tree_free(void)
+{
+      int j;
+      if (FlatTree == NULL) return;
+      for (j = 0; j < cell_id; j++) {
+            free((FlatTree + j)->dots);
+            (FlatTree + j)->dots = NULL;
+      }
+      free(FlatTree);
+      FlatTree = NULL;
+      how_many_cells = 0;
+      cell_id = 0;
 }
 
 void orc_kick(void) { kick(B, &CM, vector_field); }

@@ -282,6 +282,24 @@ OUTPUT_FILES = ["stat.txt", "collision.txt", "mass.txt", "radius.txt", "x.txt", 
 ELLIPTIC_FILES = ["a.txt", "lambda.txt", "k.txt", "h.txt", "q.txt", "p.txt"]
 
 
+def tree_case(profile, n, seed, holes=()):
+    """falcON's field (src/ffm.c; the tree as the tree driver builds it before a
+    kick, then vector_field) of one disk, with the exact brute-force field of
+    the same state beside it."""
+    b = disks.gravity_disk(n, seed=seed)
+    ex = np.ones(n, np.int32)
+    ex[list(holes)] = 0
+    cm = cm_state(seed)
+    ref = oracle.Ref(profile)
+    ref.set_state(b, ex, cm)
+    acc, cma, cells = ref.tree_field()
+    exact = oracle.Ref("bf_grav_s0")
+    exact.set_state(b, ex, cm)
+    acc_x, cma_x = exact.vector_field()
+    return dict(bodies=b, exists=ex, cm=cm, acc=acc, cm_acc=cma, cells=np.int64(cells), acc_exact=acc_x,
+                cm_acc_exact=cma_x)
+
+
 def filtered_stdout(text):
     """The program's console output without its wall-clock timing line."""
     return "\n".join(l for l in text.splitlines() if "integration took" not in l)
@@ -413,6 +431,8 @@ def main(names=None):
     out["program_mesh_naive_resume"] = lambda: program_resume_case("mesh_naive_resume",
                                                                    disks.bf_collide_disk(2000, seed=0),
                                                                    "program_bf_merge")
+    # falcON (expansion order 3, theta_min 0.45), the reference's default gravity module
+    out["tree_n4096"] = lambda: tree_case("tree_grav", 4096, 51, holes=(5, 77, 4000))
     for k, make in out.items():
         if names and k not in names:
             continue
