@@ -164,8 +164,8 @@ __global__ void k_fmt_pack(const char *__restrict__ slots, const int *__restrict
 // display()'s statistics of the bodies (src/display.c:303-379): the total mass,
 // summed in slot order, and the two most massive bodies as its loop picks them
 // (strictly greater replaces, so the first of equal masses wins; i1 = i2 = 0 and
-// M = 0 when there are fewer positive masses).  One warp.
-// display()'s two most massive bodies (src/display.c:353-363): the reference scans the
+// M = 0 when there are fewer positive masses).
+// The two most massive bodies (src/display.c:353-363): the reference scans the
 // slots in ascending order from M = 0 with strict comparisons, which keeps the
 // first two positive masses of the order (mass descending, slot ascending).
 // That order is total, so the scan is a reduction: each thread keeps the first
